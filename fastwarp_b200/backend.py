@@ -1,0 +1,400 @@
+"""Python mirror of the engine interface the reference's loops drive, over the C ABI.
+
+`CudaBackend` has the operations of trait `Backend` (crates/fastwarp-reg/src/backend.rs:39-305)
+under the same names and argument meanings, and `CudaLinearEngine` those of `LinearEngine` /
+`LinearMetric` (crates/fastwarp-reg/src/linear.rs:288-320, optimizer.rs:60-65). Images and fields
+are opaque device buffers; host arrays are numpy:
+
+  - images: float arrays shaped (nz, ny, nx) (x fastest in memory, as `Volume`);
+  - fields: float64 arrays shaped (nz, ny, nx, 3), AoS LPS millimetres (as `VectorField`).
+
+Errors raise `FastwarpError` with the reference's message text (RegError::Invalid etc.).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from ._native import FastwarpError, check, lib
+
+SYN_INVERT = (20, 0.001, 0.1, True)  # InvertParams::SYN, field_ops.rs:290-295
+
+
+def make_grid(size, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0), direction=None) -> N.Grid:
+    """An ITK grid: size (nx, ny, nz), spacing and origin in mm, direction 3x3 (axis columns)."""
+    g = N.Grid()
+    d = np.eye(3) if direction is None else np.asarray(direction, dtype=np.float64)
+    for a in range(3):
+        g.size[a] = int(size[a])
+        g.spacing[a] = float(spacing[a])
+        g.origin[a] = float(origin[a])
+    for k in range(9):
+        g.direction[k] = float(d.reshape(-1)[k])
+    return g
+
+
+def grid_shape(g: N.Grid):
+    return (int(g.size[2]), int(g.size[1]), int(g.size[0]))
+
+
+def make_affine(matrix=None, offset=(0.0, 0.0, 0.0)) -> N.Affine:
+    """y = matrix @ p + offset."""
+    a = N.Affine()
+    m = np.eye(3) if matrix is None else np.asarray(matrix, dtype=np.float64)
+    for k in range(9):
+        a.matrix[k] = float(m.reshape(-1)[k])
+    for k in range(3):
+        a.offset[k] = float(offset[k])
+    return a
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Image:
+    """An image buffer on the device (float32)."""
+
+    def __init__(self, backend, handle):
+        self.backend = backend
+        self.handle = handle
+
+    @property
+    def grid(self) -> N.Grid:
+        g = N.Grid()
+        check(lib().fw_image_grid(self.handle, C.byref(g)))
+        return g
+
+    def download(self) -> np.ndarray:
+        out = np.empty(grid_shape(self.grid), np.float32)
+        check(lib().fw_image_download(self.backend.ctx, self.handle, _ptr(out)))
+        return out
+
+    def free(self):
+        if self.handle:
+            lib().fw_image_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Field:
+    """A displacement-field buffer on the device (float32 SoA planes)."""
+
+    def __init__(self, backend, handle):
+        self.backend = backend
+        self.handle = handle
+
+    @property
+    def grid(self) -> N.Grid:
+        g = N.Grid()
+        check(lib().fw_field_grid(self.handle, C.byref(g)))
+        return g
+
+    def free(self):
+        if self.handle:
+            lib().fw_field_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class CudaBackend:
+    """trait Backend on one CUDA context (one stream; synchronous calls)."""
+
+    def __init__(self, device: int = 0):
+        ctx = C.c_void_p()
+        check(lib().fw_ctx_create(int(device), C.byref(ctx)))
+        self.ctx = ctx
+        self.device = device
+
+    def close(self):
+        if self.ctx:
+            lib().fw_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def name(self) -> str:
+        return lib().fw_backend_name().decode()
+
+    def stats(self) -> dict:
+        s = N.Stats()
+        check(lib().fw_ctx_stats(self.ctx, C.byref(s)))
+        return {k: int(getattr(s, k)) for k, _ in N.Stats._fields_}
+
+    def reset_stats(self):
+        lib().fw_ctx_reset_stats(self.ctx)
+
+    def synchronize(self):
+        check(lib().fw_ctx_synchronize(self.ctx))
+
+    # -- buffers (backend.rs:52-79)
+    def upload_image(self, grid: N.Grid, data) -> Image:
+        h = C.c_void_p()
+        if isinstance(data, np.ndarray) and data.dtype == np.float32:
+            a = np.ascontiguousarray(data)
+            check(lib().fw_image_upload_f32(self.ctx, C.byref(grid), _ptr(a), C.byref(h)))
+        else:
+            a = np.ascontiguousarray(data, dtype=np.float64)
+            check(lib().fw_image_upload(self.ctx, C.byref(grid), _ptr(a), C.byref(h)))
+        return Image(self, h)
+
+    def zero_field(self, grid: N.Grid) -> Field:
+        h = C.c_void_p()
+        check(lib().fw_field_zero(self.ctx, C.byref(grid), C.byref(h)))
+        return Field(self, h)
+
+    def upload_field(self, grid: N.Grid, data) -> Field:
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        h = C.c_void_p()
+        check(lib().fw_field_upload(self.ctx, C.byref(grid), _ptr(a), C.byref(h)))
+        return Field(self, h)
+
+    def download_field(self, field: Field) -> np.ndarray:
+        out = np.empty(grid_shape(field.grid) + (3,), np.float64)
+        check(lib().fw_field_download(self.ctx, field.handle, _ptr(out)))
+        return out
+
+    def field_grid(self, field: Field) -> N.Grid:
+        return field.grid
+
+    def copy_field(self, field: Field) -> Field:
+        h = C.c_void_p()
+        check(lib().fw_field_copy(self.ctx, field.handle, C.byref(h)))
+        return Field(self, h)
+
+    # -- operations (backend.rs:75-304)
+    def warp_through_field(self, source: Image, field: Field, pre: Field | None = None,
+                           affine: N.Affine | None = None) -> Image:
+        h = C.c_void_p()
+        check(lib().fw_warp_through_field(self.ctx, source.handle, field.handle,
+                                          None if pre is None else pre.handle,
+                                          None if affine is None else C.byref(affine),
+                                          C.byref(h)))
+        return Image(self, h)
+
+    def warp_mask_through_field(self, mask: Image, field: Field, pre: Field | None = None,
+                                affine: N.Affine | None = None,
+                                product: Image | None = None) -> Image:
+        h = C.c_void_p()
+        check(lib().fw_warp_mask_through_field(self.ctx, mask.handle, field.handle,
+                                               None if pre is None else pre.handle,
+                                               None if affine is None else C.byref(affine),
+                                               None if product is None else product.handle,
+                                               C.byref(h)))
+        if product is not None:
+            return product
+        return Image(self, h)
+
+    def cc_value_derivative(self, fixed: Image, moving: Image, radius: int):
+        v = C.c_double()
+        h = C.c_void_p()
+        check(lib().fw_cc_value_derivative(self.ctx, fixed.handle, moving.handle,
+                                           C.c_int32(radius), C.byref(v), C.byref(h)))
+        return v.value, Field(self, h)
+
+    def cc_value_derivative_pair(self, fixed: Image, moving: Image, radius: int):
+        vals = (C.c_double * 2)()
+        a, b = C.c_void_p(), C.c_void_p()
+        check(lib().fw_cc_value_derivative_pair(self.ctx, fixed.handle, moving.handle,
+                                                C.c_int32(radius), vals, C.byref(a), C.byref(b)))
+        return (vals[0], Field(self, a)), (vals[1], Field(self, b))
+
+    def cc_value_derivative_pair_with_norms(self, fixed: Image, moving: Image, radius: int):
+        vals = (C.c_double * 2)()
+        norms = (C.c_double * 2)()
+        a, b = C.c_void_p(), C.c_void_p()
+        check(lib().fw_cc_value_derivative_pair_with_norms(
+            self.ctx, fixed.handle, moving.handle, C.c_int32(radius), vals, C.byref(a),
+            C.byref(b), norms))
+        return ((vals[0], Field(self, a)), (vals[1], Field(self, b))), [norms[0], norms[1]]
+
+    def smooth_field(self, field: Field, variance: float) -> Field:
+        check(lib().fw_smooth_field(self.ctx, field.handle, C.c_double(variance)))
+        return field
+
+    def max_scaled_norm(self, field: Field) -> float:
+        v = C.c_double()
+        check(lib().fw_max_scaled_norm(self.ctx, field.handle, C.byref(v)))
+        return v.value
+
+    def max_scaled_norm_pair(self, a: Field, b: Field):
+        out = (C.c_double * 2)()
+        check(lib().fw_max_scaled_norm_pair(self.ctx, a.handle, b.handle, out))
+        return out[0], out[1]
+
+    def l2_norm(self, field: Field) -> float:
+        v = C.c_double()
+        check(lib().fw_l2_norm(self.ctx, field.handle, C.byref(v)))
+        return v.value
+
+    def scale(self, field: Field, s: float) -> None:
+        check(lib().fw_scale(self.ctx, field.handle, C.c_double(s)))
+
+    def axpy(self, acc: Field, a: float, x: Field) -> None:
+        check(lib().fw_axpy(self.ctx, acc.handle, C.c_double(a), x.handle))
+
+    def compose(self, displacement: Field, warping: Field) -> Field:
+        h = C.c_void_p()
+        check(lib().fw_compose(self.ctx, displacement.handle, warping.handle, C.byref(h)))
+        return Field(self, h)
+
+    def invert(self, field: Field, initial: Field, params=SYN_INVERT):
+        prm = N.InvertParams(int(params[0]), float(params[1]), float(params[2]),
+                             int(bool(params[3])))
+        st = N.InvertStats()
+        check(lib().fw_invert(self.ctx, field.handle, initial.handle, C.byref(prm),
+                              C.byref(st)))
+        return initial, (st.iterations, st.mean_error_norm, st.max_error_norm)
+
+    def invert_pair(self, field: Field, inverse: Field, params=SYN_INVERT):
+        prm = N.InvertParams(int(params[0]), float(params[1]), float(params[2]),
+                             int(bool(params[3])))
+        st = (N.InvertStats * 2)()
+        check(lib().fw_invert_pair(self.ctx, field.handle, inverse.handle, C.byref(prm), st))
+        s = [(x.iterations, x.mean_error_norm, x.max_error_norm) for x in st]
+        return (inverse, s[0]), (field, s[1])
+
+    def resample_field(self, field: Field, grid: N.Grid) -> Field:
+        h = C.c_void_p()
+        check(lib().fw_resample_field(self.ctx, field.handle, C.byref(grid), C.byref(h)))
+        return Field(self, h)
+
+    # -- pyramid
+    def smooth_recursive(self, image: Image, sigma_mm) -> Image:
+        h = C.c_void_p()
+        s = (C.c_double * 3)(*[float(x) for x in sigma_mm])
+        check(lib().fw_smooth_recursive(self.ctx, image.handle, s, C.byref(h)))
+        return Image(self, h)
+
+
+def shrink_factors(factor: int, spacing):
+    out = (C.c_uint32 * 3)()
+    check(lib().fw_shrink_factors(C.c_uint32(factor), (C.c_double * 3)(*spacing), out))
+    return tuple(out)
+
+
+def shrink_grid(grid: N.Grid, factors) -> N.Grid:
+    out = N.Grid()
+    check(lib().fw_shrink_grid(C.byref(grid), (C.c_uint32 * 3)(*factors), C.byref(out)))
+    return out
+
+
+def linear_transform(kind="euler", parameters=None, center=(0, 0, 0), zyx=False,
+                     outer_matrix=None, outer_translation=(0, 0, 0),
+                     outer_center=(0, 0, 0)) -> N.LinearTransform:
+    """LinearMovingTransform (transform/param.rs:392-420): outer(optimised(p))."""
+    t = N.LinearTransform()
+    om = np.eye(3) if outer_matrix is None else np.asarray(outer_matrix, np.float64)
+    for k in range(9):
+        t.outer_matrix[k] = float(om.reshape(-1)[k])
+    for k in range(3):
+        t.outer_translation[k] = float(outer_translation[k])
+        t.outer_center[k] = float(outer_center[k])
+        t.center[k] = float(center[k])
+    t.kind = 0 if kind == "euler" else 1
+    t.zyx = int(bool(zyx))
+    if parameters is None:
+        parameters = [0.0] * 6 if kind == "euler" else list(np.eye(3).reshape(-1)) + [0, 0, 0]
+    for k, v in enumerate(parameters):
+        t.parameters[k] = float(v)
+    return t
+
+
+def binning_from_ranges(bins, fixed_range, moving_range) -> N.MiBinning:
+    """MiBinning::from_ranges (metric/mi.rs:229-262)."""
+    fmin, fmax = map(float, fixed_range)
+    mmin, mmax = map(float, moving_range)
+    if bins <= 4:
+        raise FastwarpError(N.FW_ERR_INVALID, "at least five histogram bins are required")
+    if fmax - fmin <= np.finfo(np.float64).eps:
+        raise FastwarpError(N.FW_ERR_INVALID, "the fixed image is constant")
+    if mmax - mmin <= np.finfo(np.float64).eps:
+        raise FastwarpError(N.FW_ERR_INVALID, "the moving image is constant")
+    b = N.MiBinning()
+    span = float(bins - 4)
+    b.bins = int(bins)
+    b.fixed_min, b.fixed_max, b.moving_min, b.moving_max = fmin, fmax, mmin, mmax
+    b.fixed_bin_size = (fmax - fmin) / span
+    b.moving_bin_size = (mmax - mmin) / span
+    b.fixed_normalized_min = fmin / b.fixed_bin_size - 2.0
+    b.moving_normalized_min = mmin / b.moving_bin_size - 2.0
+    return b
+
+
+class MiLevel:
+    """LinearMetric of one prepared level (GpuMiLevel's role): -MI and its gradient."""
+
+    def __init__(self, backend: CudaBackend, handle):
+        self.backend = backend
+        self.handle = handle
+
+    def value(self, t: N.LinearTransform) -> float:
+        v = C.c_double()
+        check(lib().fw_mi_level_value(self.handle, C.byref(t), C.byref(v)))
+        return v.value
+
+    def values(self, ts) -> list:
+        arr = (N.LinearTransform * len(ts))(*ts)
+        out = (C.c_double * len(ts))()
+        check(lib().fw_mi_level_values(self.handle, arr, C.c_int32(len(ts)), out))
+        return list(out)
+
+    def value_and_derivative(self, t: N.LinearTransform):
+        v = C.c_double()
+        d = (C.c_double * 12)()
+        check(lib().fw_mi_level_value_and_derivative(self.handle, C.byref(t), C.byref(v), d))
+        n = 6 if t.kind == 0 else 12
+        return v.value, np.array(d[:n])
+
+    def num_valid(self) -> int:
+        v = C.c_int64()
+        check(lib().fw_mi_level_num_valid(self.handle, C.byref(v)))
+        return v.value
+
+    def free(self):
+        if self.handle:
+            lib().fw_mi_level_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class CudaLinearEngine:
+    """trait LinearEngine: prepare_level uploads the moving level image and the samples."""
+
+    def __init__(self, backend: CudaBackend):
+        self.backend = backend
+
+    def name(self) -> str:
+        return self.backend.name() + " Mattes MI"
+
+    def prepare_level(self, moving_grid: N.Grid, moving, points, fixed_bin,
+                      binning: N.MiBinning) -> MiLevel:
+        m = np.ascontiguousarray(moving, np.float64)
+        p = np.ascontiguousarray(points, np.float64)
+        fb = np.ascontiguousarray(fixed_bin, np.uint32)
+        h = C.c_void_p()
+        check(lib().fw_mi_level_prepare(self.backend.ctx, C.byref(moving_grid), _ptr(m), _ptr(p),
+                                        _ptr(fb), C.c_int64(p.shape[0]), C.byref(binning),
+                                        C.byref(h)))
+        return MiLevel(self.backend, h)

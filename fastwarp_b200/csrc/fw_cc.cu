@@ -1,0 +1,443 @@
+// fw_cc.cu -- ANTs neighbourhood cross-correlation, both directions in one pass.
+//
+// Restates metric/cc.rs:170-321 (CcMetric::evaluate_masked with identity transforms on one grid,
+// what cpu/mod.rs:299-331 runs for Backend::cc_value_derivative_pair): the six window sums over a
+// clamped (2r+1)^3 box, local CC = sFM^2 / (sFF sMM), value = -mean(localCC), and the derivative
+// coefficient * grad(moving) by ITK's half-spacing central difference (interp.rs:96-120).
+//
+// Kernel design (sm_100a): one CTA owns a TX x TY column tile and marches along z over a chunk
+// of slices. Each input slice (with an r-voxel halo in x and y) is staged in shared memory; the
+// x and y box passes run in shared memory and the z window is a running sum over a ring of the
+// per-slice xy sums. Sums are float64: products of float32 voxels are exact in float64, so the
+// centred second moments (sum f^2 - (sum f)^2 / n) keep their precision in flat bright regions
+// where float32 cancels. The window planes never touch HBM: the kernel reads the two images once
+// (plus halo re-reads that hit L2) and writes the two derivative fields.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstring>
+
+#include "fw_internal.cuh"
+
+namespace fw {
+
+namespace {
+
+constexpr int TX = 32;
+
+struct CcArgs {
+    DevGrid g;
+    long long ps;       // plane stride of the derivative fields
+    int zchunk;         // slices per CTA
+    int identity_dir;   // direction is the identity: axis-aligned probes
+    double probe[3][3]; // index offset of +half a spacing along physical axis d: probe[d][r]
+};
+
+// Exact float64 emulation of the oracle's probe position (index_to_point, offset along the
+// physical axis, point_to_index) -- no fused multiply-adds, so the inside test at the faces
+// rounds as the reference's f64 code does.
+__device__ __forceinline__ void probe_index(const DevGrid& g, int i, int j, int k, int d,
+                                            double sign, double c[3]) {
+    double s0 = __dmul_rn((double)i, g.sp[0]);
+    double s1 = __dmul_rn((double)j, g.sp[1]);
+    double s2 = __dmul_rn((double)k, g.sp[2]);
+    double p[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        double rot = __dadd_rn(__dadd_rn(__dmul_rn(g.dir[r * 3 + 0], s0),
+                                         __dmul_rn(g.dir[r * 3 + 1], s1)),
+                               __dmul_rn(g.dir[r * 3 + 2], s2));
+        p[r] = __dadd_rn(g.org[r], rot);
+    }
+    double off = __dmul_rn(0.5, g.sp[d]);
+    p[d] = sign > 0 ? __dadd_rn(p[d], off) : __dsub_rn(p[d], off);
+    double e0 = __dsub_rn(p[0], g.org[0]), e1 = __dsub_rn(p[1], g.org[1]),
+           e2 = __dsub_rn(p[2], g.org[2]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        c[r] = __dadd_rn(__dadd_rn(__dmul_rn(g.inv[r * 3], e0), __dmul_rn(g.inv[r * 3 + 1], e1)),
+                         __dmul_rn(g.inv[r * 3 + 2], e2));
+}
+
+// interp.rs:96-120 at voxel (i, j, k) from global memory, general direction.
+__device__ void central_difference_exact(const float* __restrict__ img, const DevGrid& g, int i,
+                                         int j, int k, float out[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double c1[3], c2[3];
+        probe_index(g, i, j, k, d, -1.0, c1);
+        probe_index(g, i, j, k, d, +1.0, c2);
+        out[d] = 0.0f;
+        if (!inside_index(c1[0], c1[1], c1[2], g.nx, g.ny, g.nz) ||
+            !inside_index(c2[0], c2[1], c2[2], g.nx, g.ny, g.nz))
+            continue;
+        float v1 = lin_at_index(img, g.nx, g.ny, g.nz, c1[0], c1[1], c1[2]);
+        float v2 = lin_at_index(img, g.nx, g.ny, g.nz, c2[0], c2[1], c2[2]);
+        out[d] = (float)((double)(v2 - v1) / g.sp[d]);
+    }
+}
+
+// Whether the probe of voxel coordinate `i` (axis d, direction `sign`) is inside the buffer,
+// for an identity direction: only the two face voxels can round either way.
+__device__ __forceinline__ bool axis_probe_inside(const DevGrid& g, int i, int j, int k, int d,
+                                                  double sign, int n) {
+    int q = d == 0 ? i : (d == 1 ? j : k);
+    if (sign < 0 && q > 0) return true;
+    if (sign > 0 && q < n - 1) return true;
+    double c[3];
+    probe_index(g, i, j, k, d, sign, c);
+    return c[d] >= -0.5 && c[d] < (double)n - 0.5;
+}
+
+// Shared-memory layout (dynamic): input ring [D][HY][HX] float2 (f, m); x sums [5][HY][TX]
+// double; xy-sum ring [2R+1][5][TX*TY] double.
+template <int R, int TY>
+struct Layout {
+    static constexpr int HX = TX + 2 * R;
+    static constexpr int HY = TY + 2 * R;
+    static constexpr int D = R + 2;        // input slices kept: k-R-1 .. k
+    static constexpr int W = 2 * R + 1;    // z window
+    static constexpr int NT = TX * TY;
+    static constexpr size_t in_bytes = sizeof(float2) * D * HY * HX;
+    static constexpr size_t xs_bytes = sizeof(double) * 5 * HY * TX;
+    static constexpr size_t ring_bytes = sizeof(double) * W * 5 * NT;
+    static constexpr size_t bytes = in_bytes + xs_bytes + ring_bytes + 64 * sizeof(double);
+};
+
+template <int R, int TY>
+__global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __restrict__ fimg,
+                                                     const float* __restrict__ mimg,
+                                                     float* __restrict__ d_fixed,
+                                                     float* __restrict__ d_moving,
+                                                     double* __restrict__ partials,
+                                                     unsigned int* __restrict__ counter,
+                                                     double* __restrict__ result, int want_norms) {
+    using L = Layout<R, TY>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2* in = reinterpret_cast<float2*>(smem);
+    double* xs = reinterpret_cast<double*>(smem + L::in_bytes);
+    double* ring = reinterpret_cast<double*>(smem + L::in_bytes + L::xs_bytes);
+    double* red = ring + L::W * 5 * L::NT;
+
+    const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
+    const int tid = threadIdx.x;
+    const int tx = tid % TX, ty = tid / TX;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int z0 = blockIdx.z * a.zchunk;
+    const int z1 = min(z0 + a.zchunk, nz);
+    const int x = x0 + tx, y = y0 + ty;
+    const bool own = x < nx && y < ny;
+    const long long sxy = (long long)nx * ny;
+
+    for (int s = tid; s < L::W * 5 * L::NT; s += L::NT) ring[s] = 0.0;
+    double S[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double acc_cc = 0.0, acc_nf = 0.0, acc_nm = 0.0;
+
+    // analytic voxel counts of the clamped window along x and y
+    const int cxn = own ? (min(x + R, nx - 1) - max(x - R, 0) + 1) : 0;
+    const int cyn = own ? (min(y + R, ny - 1) - max(y - R, 0) + 1) : 0;
+
+    const int kbeg = max(z0 - R, 0);
+    const int kend = min(z1 + R, nz);  // slices that exist and are needed (exclusive)
+    for (int k = kbeg; k < z1 + R; ++k) {
+        __syncthreads();  // previous slice's readers are done with the slot and the x sums
+        double P[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        const bool have = k < kend;
+        if (have) {
+            float2* slot = in + (k % L::D) * (L::HY * L::HX);
+            const long long zoff = (long long)k * sxy;
+            for (int s = tid; s < L::HY * L::HX; s += L::NT) {
+                int hy = s / L::HX, hx = s - hy * L::HX;
+                int gx = x0 - R + hx, gy = y0 - R + hy;
+                float2 v = make_float2(0.0f, 0.0f);
+                if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) {
+                    long long o = zoff + (long long)gy * nx + gx;
+                    v = make_float2(__ldg(fimg + o), __ldg(mimg + o));
+                }
+                slot[s] = v;
+            }
+            __syncthreads();
+            // x pass: every (halo row, output column) pair
+            for (int s = tid; s < L::HY * TX; s += L::NT) {
+                int hy = s / TX, cx = s - hy * TX;
+                const float2* row = slot + hy * L::HX + cx;
+                double q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0;
+#pragma unroll
+                for (int t = 0; t <= 2 * R; ++t) {
+                    float2 v = row[t];
+                    double f = v.x, m = v.y;
+                    q0 += f;
+                    q1 += m;
+                    q2 += f * f;
+                    q3 += m * m;
+                    q4 += f * m;
+                }
+                xs[(0 * L::HY + hy) * TX + cx] = q0;
+                xs[(1 * L::HY + hy) * TX + cx] = q1;
+                xs[(2 * L::HY + hy) * TX + cx] = q2;
+                xs[(3 * L::HY + hy) * TX + cx] = q3;
+                xs[(4 * L::HY + hy) * TX + cx] = q4;
+            }
+            __syncthreads();
+            // y pass for the thread's own column
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                double s = 0.0;
+#pragma unroll
+                for (int t = 0; t <= 2 * R; ++t) s += xs[(q * L::HY + ty + t) * TX + tx];
+                P[q] = s;
+            }
+        }
+        // z window: running sum over the ring of xy sums (entering k, leaving k - 2R - 1)
+        double* rs = ring + (k % L::W) * 5 * L::NT + tid;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            double old = rs[q * L::NT];
+            S[q] += P[q] - old;
+            rs[q * L::NT] = P[q];
+        }
+        const int z = k - R;
+        if (z < z0 || z >= z1 || !own) continue;
+
+        // ---- output voxel (x, y, z) ----
+        const int czn = min(z + R, nz - 1) - max(z - R, 0) + 1;
+        const double cnt = (double)(cxn * cyn * czn);
+        const float2* cs = in + (z % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R);
+        const float fv = cs[0].x, mv = cs[0].y;
+        // metric/cc.rs:267-302 (same expression order)
+        const double sum_f = S[0], sum_m = S[1], sum_f2 = S[2], sum_m2 = S[3], sum_fm = S[4];
+        const double fmean = sum_f / cnt, mmean = sum_m / cnt;
+        const double s_ff = sum_f2 - fmean * sum_f - fmean * sum_f + cnt * fmean * fmean;
+        const double s_mm = sum_m2 - mmean * sum_m - mmean * sum_m + cnt * mmean * mmean;
+        const double s_fm = sum_fm - mmean * sum_f - fmean * sum_m + cnt * mmean * fmean;
+        const double fi = (double)fv - fmean, mi = (double)mv - mmean;
+        const double product = s_ff * s_mm;
+        double cc = 1.0;
+        if (fabs(product) > DBL_EPSILON) cc = s_fm * s_fm / product;
+        acc_cc += cc;
+        double cf = 0.0, cm = 0.0;
+        if (s_ff > DBL_EPSILON && s_mm > DBL_EPSILON) {
+            cf = 2.0 * s_fm / product * (fi - s_fm / s_mm * mi);  // (fixed, moving)
+            cm = 2.0 * s_fm / product * (mi - s_fm / s_ff * fi);  // (moving, fixed)
+        }
+        // gradients of moving (for the first direction) and of fixed (for the second)
+        float gm[3], gf[3];
+        if (a.identity_dir) {
+            const int nn[3] = {nx, ny, nz};
+            const int pos[3] = {x, y, z};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                gm[d] = 0.0f;
+                gf[d] = 0.0f;
+                if (!axis_probe_inside(a.g, x, y, z, d, -1.0, nn[d]) ||
+                    !axis_probe_inside(a.g, x, y, z, d, +1.0, nn[d]))
+                    continue;
+                // neighbours along d inside the staged tile / ring
+                float2 lo, hi;
+                const float2* c0 = cs;
+                if (d == 0) {
+                    lo = c0[-1];
+                    hi = c0[1];
+                } else if (d == 1) {
+                    lo = c0[-L::HX];
+                    hi = c0[L::HX];
+                } else {
+                    lo = (z > 0) ? in[((z - 1) % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R)]
+                                 : cs[0];
+                    hi = (z < nz - 1) ? in[((z + 1) % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R)]
+                                      : cs[0];
+                }
+                const int p = pos[d];
+                // upper probe at p + 0.5: lerp to p + 1 unless p is the last voxel
+                float m2 = p < nn[d] - 1 ? fmaf(hi.y - mv, 0.5f, mv) : mv;
+                float f2 = p < nn[d] - 1 ? fmaf(hi.x - fv, 0.5f, fv) : fv;
+                // lower probe at p - 0.5: base p - 1 with weight 0.5, or the first voxel itself
+                float m1 = p > 0 ? fmaf(mv - lo.y, 0.5f, lo.y) : mv;
+                float f1 = p > 0 ? fmaf(fv - lo.x, 0.5f, lo.x) : fv;
+                gm[d] = (float)((double)(m2 - m1) / a.g.sp[d]);
+                gf[d] = (float)((double)(f2 - f1) / a.g.sp[d]);
+            }
+        } else {
+            central_difference_exact(mimg, a.g, x, y, z, gm);
+            central_difference_exact(fimg, a.g, x, y, z, gf);
+        }
+        const long long l = (long long)z * sxy + (long long)y * nx + x;
+        const float fcf = (float)cf, fcm = (float)cm;
+        float dfx = fcf * gm[0], dfy = fcf * gm[1], dfz = fcf * gm[2];
+        float dmx = fcm * gf[0], dmy = fcm * gf[1], dmz = fcm * gf[2];
+        d_fixed[l] = dfx;
+        d_fixed[l + a.ps] = dfy;
+        d_fixed[l + 2 * a.ps] = dfz;
+        d_moving[l] = dmx;
+        d_moving[l + a.ps] = dmy;
+        d_moving[l + 2 * a.ps] = dmz;
+        if (want_norms) {
+            acc_nf += (double)dfx * dfx + (double)dfy * dfy + (double)dfz * dfz;
+            acc_nm += (double)dmx * dmx + (double)dmy * dmy + (double)dmz * dmz;
+        }
+    }
+
+    // block partials, then the fixed-order last-block reduction
+    acc_cc = warp_sum_d(acc_cc);
+    acc_nf = warp_sum_d(acc_nf);
+    acc_nm = warp_sum_d(acc_nm);
+    __syncthreads();
+    const int warps = L::NT / 32;
+    if ((tid & 31) == 0) {
+        red[(tid >> 5) * 3 + 0] = acc_cc;
+        red[(tid >> 5) * 3 + 1] = acc_nf;
+        red[(tid >> 5) * 3 + 2] = acc_nm;
+    }
+    __syncthreads();
+    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (tid < 3) {
+        double s = 0.0;
+        for (int w = 0; w < warps; ++w) s += red[w * 3 + tid];
+        partials[(size_t)bid * 3 + tid] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    __shared__ bool last;
+    if (tid == 0) last = atomicAdd(counter, 1u) == nblocks - 1;
+    __syncthreads();
+    if (!last) return;
+    if (tid < 32) {
+        for (int q = 0; q < 3; ++q) {
+            double s = 0.0;
+            for (unsigned int b = tid; b < nblocks; b += 32) s += __ldcg(partials + (size_t)b * 3 + q);
+            s = warp_sum_d(s);
+            if (tid == 0) {
+                if (q == 0) result[0] = -s / (double)a.g.n;
+                else result[q] = s;
+            }
+        }
+        if (tid == 0) *counter = 0;
+    }
+}
+
+template <int R, int TY>
+int launch_r(fw_ctx* ctx, const CcArgs& a0, const float* f, const float* m, float* df, float* dm,
+             double* d_result, int want_norms) {
+    using L = Layout<R, TY>;
+    CcArgs a = a0;
+    dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, 1);
+    // z chunks: enough CTAs to fill the GPU a few times over, chunks no thinner than 4R slices
+    long long tiles = (long long)grid.x * grid.y;
+    int want = (int)std::max<long long>(1, (4LL * ctx->num_sms + tiles - 1) / tiles);
+    int chunk = (a.g.nz + want - 1) / want;
+    chunk = std::max(chunk, std::min(a.g.nz, 4 * R + 4));
+    a.zchunk = chunk;
+    grid.z = (a.g.nz + chunk - 1) / chunk;
+    unsigned int nblocks = grid.x * grid.y * grid.z;
+    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 3 * (size_t)nblocks + 16));
+    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)L::bytes));
+    k_cc_pair<R, TY><<<grid, L::NT, L::bytes, ctx->stream>>>(
+        a, f, m, df, dm, ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 1, d_result, want_norms);
+    return check_launch(ctx, "k_cc_pair");
+}
+
+}  // namespace
+
+// d_result receives [value, sum |d_fixed|^2, sum |d_moving|^2].
+int launch_cc_pair_impl(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
+                        fw_field* d_fixed, fw_field* d_moving, double* d_result, int want_norms) {
+    CcArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = dev_grid(fixed->grid);
+    a.ps = d_fixed->ps;
+    const HostGrid& g = fixed->grid;
+    a.identity_dir = 1;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            if (g.dir[r * 3 + c] != (r == c ? 1.0 : 0.0)) a.identity_dir = 0;
+    const float* f = fixed->d;
+    const float* m = moving->d;
+    switch (radius) {
+        case 1: return launch_r<1, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
+        case 2: return launch_r<2, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
+        case 3: return launch_r<3, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
+        case 4: return launch_r<4, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
+        case 5: return launch_r<5, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
+        case 6: return launch_r<6, 4>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
+        case 7: return launch_r<7, 4>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
+        case 8: return launch_r<8, 4>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
+        default:
+            return fail(FW_ERR_INVALID, "cc metric: radius must be in 1..=8 (BOX_RADIUS_MAX)");
+    }
+}
+
+int launch_cc_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
+                   fw_field* d_fixed, fw_field* d_moving, double* d_value, double* d_norms) {
+    (void)d_norms;
+    return launch_cc_pair_impl(ctx, fixed, moving, radius, d_fixed, d_moving, d_value,
+                               d_norms != nullptr);
+}
+
+}  // namespace fw
+
+using namespace fw;
+
+extern "C" {
+
+static int cc_pair_common(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                          int32_t radius, double values[2], fw_field** d_fixed,
+                          fw_field** d_moving, double norms[2]) {
+    FW_CHECK(ctx && fixed && moving && values && d_fixed && d_moving, "null argument");
+    if (!fixed->grid.same(moving->grid))
+        return fail(FW_ERR_INVALID, "cc metric: the images are not on one grid");
+    fw_field *a = nullptr, *b = nullptr;
+    FW_TRY(new_field(ctx, fixed->grid, &a));
+    int rc = new_field(ctx, fixed->grid, &b);
+    if (rc) {
+        fw_field_free(a);
+        return rc;
+    }
+    double* slot = ctx->d_scratch + SLOT_CC_VALUE;  // [value, nf, nm] at SLOT_CC_VALUE.. +2
+    rc = launch_cc_pair_impl(ctx, fixed, moving, radius, a, b, slot, 1);
+    double r[3] = {0, 0, 0};
+    if (!rc) rc = read_back(ctx, slot, 3, r);
+    if (rc) {
+        fw_field_free(a);
+        fw_field_free(b);
+        return rc;
+    }
+    values[0] = r[0];
+    values[1] = r[0];
+    if (norms) {
+        norms[0] = std::sqrt(r[1]);
+        norms[1] = std::sqrt(r[2]);
+    }
+    *d_fixed = a;
+    *d_moving = b;
+    return 0;
+}
+
+int fw_cc_value_derivative_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                                int32_t radius, double values[2], fw_field** d_fixed,
+                                fw_field** d_moving) {
+    return cc_pair_common(ctx, fixed, moving, radius, values, d_fixed, d_moving, nullptr);
+}
+
+int fw_cc_value_derivative_pair_with_norms(fw_ctx* ctx, const fw_image* fixed,
+                                           const fw_image* moving, int32_t radius,
+                                           double values[2], fw_field** d_fixed,
+                                           fw_field** d_moving, double norms[2]) {
+    FW_CHECK(norms, "null norms");
+    return cc_pair_common(ctx, fixed, moving, radius, values, d_fixed, d_moving, norms);
+}
+
+int fw_cc_value_derivative(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                           int32_t radius, double* value, fw_field** derivative) {
+    FW_CHECK(value && derivative, "null argument");
+    double v[2];
+    fw_field *a = nullptr, *b = nullptr;
+    FW_TRY(cc_pair_common(ctx, fixed, moving, radius, v, &a, &b, nullptr));
+    fw_field_free(b);
+    *value = v[0];
+    *derivative = a;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,288 @@
+// fw_internal.cuh -- shared declarations of the sm_100a registration engine.
+//
+// Device layout: images are float32 arrays of n = nx*ny*nz voxels (x fastest); fields are three
+// float32 planes (x | y | z) of `ps` floats each, ps = n rounded up to 64 so every plane starts
+// on a 256-byte boundary and 16-byte vector accesses stay aligned.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <cmath>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fastwarp_cuda.h"
+
+namespace fw {
+
+// ---- errors ---------------------------------------------------------------------------------
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define FW_CUDA(call)                                              \
+    do {                                                           \
+        cudaError_t fw_e_ = (call);                                \
+        if (fw_e_ != cudaSuccess) return ::fw::cuda_fail(fw_e_, #call); \
+    } while (0)
+
+#define FW_CHECK(cond, msg)                                        \
+    do {                                                           \
+        if (!(cond)) return ::fw::fail(FW_ERR_INVALID, (msg));     \
+    } while (0)
+
+#define FW_TRY(call)                  \
+    do {                              \
+        int fw_rc_ = (call);          \
+        if (fw_rc_ != 0) return fw_rc_; \
+    } while (0)
+
+// ---- host grid math (grid.rs:45-161) -------------------------------------------------------
+
+struct HostGrid {
+    int64_t n[3];
+    double sp[3], org[3], dir[9];
+    double ds[9];   // direction * diag(spacing): index -> offset
+    double inv[9];  // its inverse: offset -> index
+    int64_t count() const { return n[0] * n[1] * n[2]; }
+    bool same(const HostGrid& o) const;
+};
+
+bool mat3_inverse(const double m[9], double out[9]);
+void mat3_mul(const double a[9], const double b[9], double out[9]);
+void mat3_vec(const double m[9], const double v[3], double out[3]);
+int make_grid(const fw_grid* g, HostGrid& out);
+fw_grid to_c(const HostGrid& g);
+
+// ---- device grid ---------------------------------------------------------------------------
+
+struct DevGrid {
+    int nx, ny, nz;
+    long long n;
+    double org[3];
+    double ds[9];
+    double inv[9];
+    double sp[3];
+    double dir[9];
+};
+
+DevGrid dev_grid(const HostGrid& g);
+
+inline int64_t plane_stride(int64_t n) { return (n + 63) / 64 * 64; }
+
+// ---- context and buffers -------------------------------------------------------------------
+
+}  // namespace fw
+
+struct fw_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    // scratch: reduction partials, small device scalars and a pinned host mirror
+    double* d_scratch = nullptr;     // device scratch doubles
+    size_t scratch_doubles = 0;
+    unsigned int* d_counter = nullptr;  // last-block counters (zeroed after use)
+    double* h_pinned = nullptr;      // pinned host scalars for read-backs
+    fw_stats stats{};
+    std::atomic<uint64_t> live_bytes{0};
+    const volatile int32_t* cancel = nullptr;
+    bool capturing = false;          // a graph capture is in progress on `stream`
+    cudaStream_t aux = nullptr;      // second stream for capturing conditional bodies
+};
+
+struct fw_image {
+    fw_ctx* ctx;
+    fw::HostGrid grid;
+    float* d;
+    size_t bytes;
+};
+
+struct fw_field {
+    fw_ctx* ctx;
+    fw::HostGrid grid;
+    float* d;       // plane 0; planes at d, d + ps, d + 2 ps
+    int64_t ps;     // plane stride in floats
+    size_t bytes;
+};
+
+namespace fw {
+
+// stream-ordered allocation from the device's memory pool (kept cached: the buffer pool)
+int dev_alloc(fw_ctx* ctx, size_t bytes, void** out);
+void dev_free(fw_ctx* ctx, void* p, size_t bytes);
+int new_image(fw_ctx* ctx, const HostGrid& g, fw_image** out);
+int new_field(fw_ctx* ctx, const HostGrid& g, fw_field** out);
+int sync(fw_ctx* ctx);
+int check_launch(fw_ctx* ctx, const char* what);
+int ensure_scratch(fw_ctx* ctx, size_t doubles);
+
+// ---- device helpers: ITK interpolation rules (interp.rs:43-120, field_ops.rs:143-181) -----
+
+// ITK IsInsideBuffer on a continuous index: every coordinate in [-0.5, n - 0.5).
+__device__ __forceinline__ bool inside_index(double cx, double cy, double cz, int nx, int ny,
+                                             int nz) {
+    return cx >= -0.5 && cx < (double)nx - 0.5 && cy >= -0.5 && cy < (double)ny - 0.5 &&
+           cz >= -0.5 && cz < (double)nz - 0.5;
+}
+
+// One axis of ITK's scalar linear interpolation: base clamped into the buffer, no weight when
+// the distance is not positive or the upper neighbour is past the last voxel.
+__device__ __forceinline__ void lin_axis(double c, int n, int& b, float& w) {
+    double fl = floor(c);
+    long long bb = fl < 0.0 ? 0 : (long long)fmin(fl, (double)(n - 1));
+    double d = c - (double)bb;
+    b = (int)bb;
+    w = (d <= 0.0 || bb + 1 > n - 1) ? 0.0f : (float)d;
+}
+
+// interp.rs:43-85: LinearInterpolateImageFunction::EvaluateAtContinuousIndex (no bounds check).
+__device__ __forceinline__ float lin_at_index(const float* __restrict__ img, int nx, int ny,
+                                              int nz, double cx, double cy, double cz) {
+    int bx, by, bz;
+    float wx, wy, wz;
+    lin_axis(cx, nx, bx, wx);
+    lin_axis(cy, ny, by, wy);
+    lin_axis(cz, nz, bz, wz);
+    const long long sy = nx, sz = (long long)nx * ny;
+    const float* p = img + bx + sy * by + sz * bz;
+    int ox = wx > 0.0f ? 1 : 0;
+    long long oy = wy > 0.0f ? sy : 0;
+    long long oz = wz > 0.0f ? sz : 0;
+    float v000 = __ldg(p), v100 = __ldg(p + ox);
+    float v010 = __ldg(p + oy), v110 = __ldg(p + oy + ox);
+    float x0 = fmaf(v100 - v000, wx, v000);
+    float x1 = fmaf(v110 - v010, wx, v010);
+    float y0 = fmaf(x1 - x0, wy, x0);
+    if (wz > 0.0f) {
+        float v001 = __ldg(p + oz), v101 = __ldg(p + oz + ox);
+        float v011 = __ldg(p + oz + oy), v111 = __ldg(p + oz + oy + ox);
+        float x2 = fmaf(v101 - v001, wx, v001);
+        float x3 = fmaf(v111 - v011, wx, v011);
+        float y1 = fmaf(x3 - x2, wy, x2);
+        return fmaf(y1 - y0, wz, y0);
+    }
+    return y0;
+}
+
+// field_ops.rs:143-172: VectorLinearInterpolateImageFunction (neighbours clamped, weights 1-d, d)
+// of a SoA field at a continuous index.
+__device__ __forceinline__ void vec_at_index(const float* __restrict__ f, long long ps, int nx,
+                                             int ny, int nz, double cx, double cy, double cz,
+                                             float out[3]) {
+    double fx = floor(cx), fy = floor(cy), fz = floor(cz);
+    float dx = (float)(cx - fx), dy = (float)(cy - fy), dz = (float)(cz - fz);
+    int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+    int xa = min(max(x0, 0), nx - 1), xb = min(max(x0 + 1, 0), nx - 1);
+    int ya = min(max(y0, 0), ny - 1), yb = min(max(y0 + 1, 0), ny - 1);
+    int za = min(max(z0, 0), nz - 1), zb = min(max(z0 + 1, 0), nz - 1);
+    const long long sy = nx, sz = (long long)nx * ny;
+    long long i000 = xa + sy * ya + sz * za, i100 = xb + sy * ya + sz * za;
+    long long i010 = xa + sy * yb + sz * za, i110 = xb + sy * yb + sz * za;
+    long long i001 = xa + sy * ya + sz * zb, i101 = xb + sy * ya + sz * zb;
+    long long i011 = xa + sy * yb + sz * zb, i111 = xb + sy * yb + sz * zb;
+    float w[2][3] = {{1.0f - dx, 1.0f - dy, 1.0f - dz}, {dx, dy, dz}};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float* p = f + c * ps;
+        float acc = 0.0f;
+        float o;
+        o = w[0][0] * w[0][1] * w[0][2]; if (o != 0.0f) acc += o * __ldg(p + i000);
+        o = w[1][0] * w[0][1] * w[0][2]; if (o != 0.0f) acc += o * __ldg(p + i100);
+        o = w[0][0] * w[1][1] * w[0][2]; if (o != 0.0f) acc += o * __ldg(p + i010);
+        o = w[1][0] * w[1][1] * w[0][2]; if (o != 0.0f) acc += o * __ldg(p + i110);
+        o = w[0][0] * w[0][1] * w[1][2]; if (o != 0.0f) acc += o * __ldg(p + i001);
+        o = w[1][0] * w[0][1] * w[1][2]; if (o != 0.0f) acc += o * __ldg(p + i101);
+        o = w[0][0] * w[1][1] * w[1][2]; if (o != 0.0f) acc += o * __ldg(p + i011);
+        o = w[1][0] * w[1][1] * w[1][2]; if (o != 0.0f) acc += o * __ldg(p + i111);
+        out[c] = acc;
+    }
+}
+
+__device__ __forceinline__ void voxel_ijk(long long l, int nx, int ny, int& i, int& j, int& k) {
+    long long q = l / nx;
+    i = (int)(l - q * nx);
+    k = (int)(q / ny);
+    j = (int)(q - (long long)k * ny);
+}
+
+// non-negative float max via integer compare; NaN (canonical, positive) wins.
+__device__ __forceinline__ float nan_canon(float v) {
+    return isnan(v) ? __int_as_float(0x7fffffff) : v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_max_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        float w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = __int_as_float(max(__float_as_int(v), __float_as_int(w)));
+    }
+    return v;
+}
+
+// ---- internal kernels launched by the SyN driver -------------------------------------------
+
+// Device loop state of one inversion (fw_invert.cu).
+struct InvState {
+    double mean;         // MeanErrorNorm of the last measurement
+    double max;          // MaxErrorNorm of the last measurement
+    int executed;        // bodies executed
+    int k;               // index of the next body
+    int go;              // whether body k runs
+    int max_iterations;
+    double mean_tol, max_tol;
+    int enforce;
+    int pad;
+};
+
+int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
+                             const fw_invert_params& prm, InvState* st,
+                             cudaGraphConditionalHandle handle, int use_handle);
+int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, InvState* st,
+                           cudaGraphConditionalHandle handle, int use_handle);
+int read_back(fw_ctx* ctx, const double* d, int k, double* out);
+int launch_cc_pair_impl(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
+                        fw_field* d_fixed, fw_field* d_moving, double* d_result, int want_norms);
+
+// Gaussian taps of ITK's GaussianOperator (field_ops.rs:478-506), f64.
+std::vector<double> gaussian_taps(double variance, double max_error, int64_t max_width);
+
+// Reduction slots in ctx->d_scratch (doubles).
+enum Slot : int {
+    SLOT_MAX_A = 0,      // float bits of max |u/sp| (field a), as uint in a double slot
+    SLOT_MAX_B = 1,
+    SLOT_CC_VALUE = 2,   // -mean(localCC)
+    SLOT_NORM_A = 3,     // sum u.u of derivative a
+    SLOT_NORM_B = 4,
+    SLOT_INV = 8,        // inversion state (8 doubles)
+    SLOT_MI = 32,        // MI scalars
+    SLOT_PARTIALS = 128, // block partials follow
+};
+
+int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const fw_field* pre,
+                const fw_affine* affine, float* out, bool mask, const float* product);
+int launch_cc_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
+                   fw_field* d_fixed, fw_field* d_moving, double* d_value, double* d_norms);
+int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double variance,
+                  unsigned int* d_max_bits);
+int launch_max_norm(fw_ctx* ctx, const fw_field* f, unsigned int* d_max_bits);
+int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, fw_field* out,
+                   const unsigned int* d_scale_max_bits, double step);
+int launch_scale_by_max(fw_ctx* ctx, fw_field* f, const unsigned int* d_max_bits, double step);
+int invert_field(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
+                 const fw_invert_params& prm, fw_invert_stats* stats);
+int launch_resample(fw_ctx* ctx, const fw_field* f, fw_field* out);
+int launch_smooth_recursive(fw_ctx* ctx, const fw_image* img, const double sigma_mm[3],
+                            fw_image* out);
+int reduce_l2(fw_ctx* ctx, const fw_field* f, double* d_out);
+
+}  // namespace fw

@@ -1,0 +1,306 @@
+// fw_invert.cu -- ITK InvertDisplacementFieldImageFilter as SyN runs it (field_ops.rs:309-392).
+//
+// The reference loop is: while (iteration < max && max_error > max_tol && mean_error > mean_tol)
+// { e = psi + f(x + psi); measure mean and max of |e/sp|; psi += eps * clamp(-e) with
+// eps = 0.75 on the first body and 0.5 after; faces of psi to zero }.
+//
+// Device design: the error at voxel x depends only on psi(x) and the read-only field f, so one
+// sweep can apply body k's update to psi(x) and at once measure body k+1's error at the same
+// voxel. Each body is therefore ONE sweep (read psi, gather f, write psi, gather f again for the
+// next measurement) plus a fixed-order reduction done by the last block to finish. The loop
+// state (errors of the last measurement, body index, whether the next body runs) lives in device
+// memory and is updated by that last block, so the loop needs no host read-back: the SyN driver
+// runs it inside a CUDA graph WHILE node whose condition the last block sets.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstring>
+
+#include "fw_internal.cuh"
+
+namespace fw {
+
+struct InvArgs {
+    DevGrid g;
+    long long ps_f, ps_psi;
+    float isx, isy, isz;
+};
+
+__device__ __forceinline__ void residual(const InvArgs& a, const float* __restrict__ f,
+                                         long long l, int i, int j, int k, float px, float py,
+                                         float pz, float e[3]) {
+    double c0 = i + (a.g.inv[0] * px + a.g.inv[1] * py + a.g.inv[2] * pz);
+    double c1 = j + (a.g.inv[3] * px + a.g.inv[4] * py + a.g.inv[5] * pz);
+    double c2 = k + (a.g.inv[6] * px + a.g.inv[7] * py + a.g.inv[8] * pz);
+    float d[3] = {0.0f, 0.0f, 0.0f};
+    if (inside_index(c0, c1, c2, a.g.nx, a.g.ny, a.g.nz))
+        vec_at_index(f, a.ps_f, a.g.nx, a.g.ny, a.g.nz, c0, c1, c2, d);
+    e[0] = px + d[0];
+    e[1] = py + d[1];
+    e[2] = pz + d[2];
+}
+
+// Block sums (f64) and maxima -> partials; the last block reduces them in block order and
+// updates the loop state through `finish`.
+template <typename Finish>
+__device__ void reduce_and_finish(double sum, float mx, double* __restrict__ partials,
+                                  unsigned int* __restrict__ counter, Finish finish) {
+    __shared__ double rs[32];
+    __shared__ float rm[32];
+    __shared__ bool last;
+    sum = warp_sum_d(sum);
+    mx = warp_max_f(mx);
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        rs[w] = sum;
+        rm[w] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        float m = 0.0f;
+        for (int q = 0; q < nw; ++q) {
+            s += rs[q];
+            m = __int_as_float(max(__float_as_int(m), __float_as_int(rm[q])));
+        }
+        partials[2 * blockIdx.x] = s;
+        partials[2 * blockIdx.x + 1] = (double)m;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    if (threadIdx.x < 32) {
+        double s = 0.0, m = 0.0;
+        for (unsigned int b = threadIdx.x; b < gridDim.x; b += 32) {
+            s += __ldcg(partials + 2 * b);
+            double mb = __ldcg(partials + 2 * b + 1);
+            m = (mb > m || mb != mb) ? mb : m;
+        }
+        s = warp_sum_d(s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double t = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (t > m || t != t) ? t : m;
+        }
+        if (threadIdx.x == 0) {
+            finish(s, m);
+            *counter = 0;
+        }
+    }
+}
+
+// First measurement (body 0's error) of psi against f.
+__global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __restrict__ f,
+                                                     const float* __restrict__ psi,
+                                                     double* __restrict__ partials,
+                                                     unsigned int* __restrict__ counter,
+                                                     InvState* __restrict__ st,
+                                                     cudaGraphConditionalHandle handle,
+                                                     int use_handle) {
+    double sum = 0.0;
+    float mx = 0.0f;
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < a.g.n;
+         l += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
+        float e[3];
+        residual(a, f, l, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
+        float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
+        float nrm = nan_canon(sqrtf(x * x + y * y + z * z));
+        sum += (double)nrm;
+        mx = __int_as_float(max(__float_as_int(mx), __float_as_int(nrm)));
+    }
+    const double count = (double)a.g.n;
+    reduce_and_finish(sum, mx, partials, counter, [&](double s, double m) {
+        st->mean = s / count;
+        st->max = m;
+        st->executed = 0;
+        st->k = 0;
+        st->go = st->max_iterations > 0 ? 1 : 0;
+        if (use_handle) cudaGraphSetConditional(handle, st->go ? 1u : 0u);
+    });
+}
+
+// One body: the update with eps (0.75 on body 0, else 0.5) and limit eps * max of the last
+// measurement, faces to zero, then -- when the next body will run -- its measurement.
+__global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __restrict__ f,
+                                                  float* __restrict__ psi,
+                                                  double* __restrict__ partials,
+                                                  unsigned int* __restrict__ counter,
+                                                  InvState* __restrict__ st,
+                                                  cudaGraphConditionalHandle handle,
+                                                  int use_handle) {
+    const int go = st->go;
+    if (!go) {  // uniform: the state only changes in the last block of this grid
+        // keep a WHILE loop from spinning should its condition ever disagree with the state
+        if (use_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
+        return;
+    }
+    const int kb = st->k;
+    const double mean = st->mean, mxe = st->max;
+    const float eps = kb == 0 ? 0.75f : 0.5f;
+    const float limit = eps * (float)mxe;
+    const bool next = (kb + 1 < st->max_iterations) && mxe > st->max_tol && mean > st->mean_tol;
+    const bool enforce = st->enforce != 0;
+    double sum = 0.0;
+    float mx = 0.0f;
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < a.g.n;
+         l += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
+        float px = psi[l], py = psi[l + a.ps_psi], pz = psi[l + 2 * a.ps_psi];
+        float e[3];
+        residual(a, f, l, i, j, k, px, py, pz, e);
+        float ex = e[0] * a.isx, ey = e[1] * a.isy, ez = e[2] * a.isz;
+        float nrm = sqrtf(ex * ex + ey * ey + ez * ez);
+        float ux = -e[0], uy = -e[1], uz = -e[2];
+        if (nrm > limit) {
+            float fct = limit / nrm;
+            ux *= fct;
+            uy *= fct;
+            uz *= fct;
+        }
+        px = px + ux * eps;
+        py = py + uy * eps;
+        pz = pz + uz * eps;
+        const bool face = i == 0 || j == 0 || k == 0 || i == a.g.nx - 1 || j == a.g.ny - 1 ||
+                          k == a.g.nz - 1;
+        if (enforce && face) px = py = pz = 0.0f;
+        psi[l] = px;
+        psi[l + a.ps_psi] = py;
+        psi[l + 2 * a.ps_psi] = pz;
+        if (next) {
+            residual(a, f, l, i, j, k, px, py, pz, e);
+            float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
+            float n2 = nan_canon(sqrtf(x * x + y * y + z * z));
+            sum += (double)n2;
+            mx = __int_as_float(max(__float_as_int(mx), __float_as_int(n2)));
+        }
+    }
+    const double count = (double)a.g.n;
+    reduce_and_finish(sum, mx, partials, counter, [&](double s, double m) {
+        st->executed = kb + 1;
+        if (next) {
+            st->mean = s / count;
+            st->max = m;
+            st->k = kb + 1;
+        }
+        st->go = next ? 1 : 0;
+        if (use_handle) cudaGraphSetConditional(handle, next ? 1u : 0u);
+    });
+}
+
+__global__ void k_inv_init(InvState* st, fw_invert_params p) {
+    st->mean = DBL_MAX;
+    st->max = DBL_MAX;
+    st->executed = 0;
+    st->k = 0;
+    st->go = 0;
+    st->max_iterations = p.max_iterations;
+    st->mean_tol = p.mean_error_tolerance;
+    st->max_tol = p.max_error_tolerance;
+    st->enforce = p.enforce_boundary_condition;
+}
+
+static InvArgs inv_args(const fw_field* field, const fw_field* inverse) {
+    InvArgs a;
+    a.g = dev_grid(field->grid);
+    a.ps_f = field->ps;
+    a.ps_psi = inverse->ps;
+    a.isx = (float)(1.0 / field->grid.sp[0]);
+    a.isy = (float)(1.0 / field->grid.sp[1]);
+    a.isz = (float)(1.0 / field->grid.sp[2]);
+    return a;
+}
+
+static unsigned int inv_blocks(fw_ctx* ctx, long long n) {
+    long long b = (n + 255) / 256;
+    return (unsigned int)std::max<long long>(1, std::min<long long>(b, 8LL * ctx->num_sms));
+}
+
+// Launches the whole inversion on the stream: init, first measurement and `bodies` body kernels
+// (each returns at once after the loop has ended). Used by graph capture with bodies = 0.
+int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
+                             const fw_invert_params& prm, InvState* st,
+                             cudaGraphConditionalHandle handle, int use_handle) {
+    InvArgs a = inv_args(field, inverse);
+    unsigned int blocks = inv_blocks(ctx, a.g.n);
+    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 2 * (size_t)blocks + 16));
+    k_inv_init<<<1, 1, 0, ctx->stream>>>(st, prm);
+    FW_TRY(check_launch(ctx, "k_inv_init"));
+    k_inv_measure<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d,
+                                                   ctx->d_scratch + SLOT_PARTIALS,
+                                                   ctx->d_counter + 2, st, handle, use_handle);
+    return check_launch(ctx, "k_inv_measure");
+}
+
+int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, InvState* st,
+                           cudaGraphConditionalHandle handle, int use_handle) {
+    InvArgs a = inv_args(field, inverse);
+    unsigned int blocks = inv_blocks(ctx, a.g.n);
+    k_inv_body<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d,
+                                                ctx->d_scratch + SLOT_PARTIALS,
+                                                ctx->d_counter + 2, st, handle, use_handle);
+    return check_launch(ctx, "k_inv_body");
+}
+
+// Host-driven loop (Backend::invert): one read-back of the loop flag per body.
+int invert_field(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
+                 const fw_invert_params& prm, fw_invert_stats* stats) {
+    InvState* st = reinterpret_cast<InvState*>(ctx->d_scratch + SLOT_INV);
+    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, prm, st, 0, 0));
+    InvState h;
+    for (int body = 0; body < std::max(prm.max_iterations, 0); ++body) {
+        FW_TRY(enqueue_inversion_body(ctx, field, inverse, st, 0, 0));
+        FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, st, sizeof(InvState), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        FW_TRY(sync(ctx));
+        std::memcpy(&h, ctx->h_pinned, sizeof(h));
+        if (!h.go) break;
+    }
+    FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, st, sizeof(InvState), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    FW_TRY(sync(ctx));
+    std::memcpy(&h, ctx->h_pinned, sizeof(h));
+    stats->iterations = h.executed;
+    stats->mean_error_norm = h.executed == 0 ? 0.0 : h.mean;
+    stats->max_error_norm = h.executed == 0 ? 0.0 : h.max;
+    return 0;
+}
+
+size_t inv_state_bytes() { return sizeof(InvState); }
+
+void inv_state_read(const void* raw, fw_invert_stats* stats) {
+    InvState h;
+    std::memcpy(&h, raw, sizeof(h));
+    stats->iterations = h.executed;
+    stats->mean_error_norm = h.executed == 0 ? 0.0 : h.mean;
+    stats->max_error_norm = h.executed == 0 ? 0.0 : h.max;
+}
+
+}  // namespace fw
+
+using namespace fw;
+
+extern "C" {
+
+int fw_invert(fw_ctx* ctx, const fw_field* field, fw_field* initial,
+              const fw_invert_params* params, fw_invert_stats* stats) {
+    FW_CHECK(ctx && field && initial && params && stats, "null argument");
+    if (!field->grid.same(initial->grid))
+        return fail(FW_ERR_INVALID, "invert: initial estimate grid differs");
+    return invert_field(ctx, field, initial, *params, stats);
+}
+
+int fw_invert_pair(fw_ctx* ctx, fw_field* field, fw_field* inverse,
+                   const fw_invert_params* params, fw_invert_stats stats[2]) {
+    FW_CHECK(ctx && field && inverse && params && stats, "null argument");
+    if (!field->grid.same(inverse->grid))
+        return fail(FW_ERR_INVALID, "invert: initial estimate grid differs");
+    FW_TRY(invert_field(ctx, field, inverse, *params, &stats[0]));
+    return invert_field(ctx, inverse, field, *params, &stats[1]);
+}
+
+}  // extern "C"

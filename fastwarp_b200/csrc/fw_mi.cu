@@ -1,0 +1,611 @@
+// fw_mi.cu -- sampled Mattes mutual information of the Rigid/Affine stages: the joint Parzen
+// histogram, ITK's ComputeResults and the parameter gradient (metric/mi.rs:364-511, 702-768;
+// GPU counterpart GpuMiLevel, crates/fastwarp-gpu/src/wgpu_backend/mi.rs:144-491).
+//
+// Device design:
+//  - samples are resident as 16-byte records (x, y, z relative to the cloud centre as float32,
+//    fixed bin as u32): one vector load per sample;
+//  - the histogram is accumulated in 2^-32 fixed point as u64 in block-private shared memory
+//    and merged with u64 atomics: integer sums do not depend on order, so a rerun is
+//    bit-identical, and the normalising sum is exact (no Kahan sum needed);
+//  - ComputeResults (normalisation, marginals, -MI, the per-cell ratio) runs on the device in
+//    float64, one thread per cell, so value_and_derivative needs a single read-back;
+//  - the derivative is linear in the Jacobian, which is affine in the sample point for Euler3D and
+//    affine transforms: col_mu(p) = G_mu [p; 1]. The kernel therefore reduces only the twelve
+//    moments M_ij = sum_s w_s grad_i(s) [r_s; 1]_j (w_s = sum_k B3'(k - term) ratio[f, k]) and the
+//    host contracts them with every parameter's G_mu in float64 -- the same sum as the
+//    reference's sum_cell dpdf[cell] * ratio[cell], reordered.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstring>
+#include <vector>
+
+#include "fw_internal.cuh"
+
+struct fw_mi_level {
+    fw_ctx* ctx;
+    fw_image* moving;
+    bool own_moving;
+    float4* d_rec;
+    int64_t n;
+    double center[3];
+    fw_mi_binning binning;
+    unsigned long long* d_hist;  // [T][bins*bins + bins]
+    double* d_ratio;             // [bins*bins]
+    double* d_out;               // [T][4]: value, num_valid, status, pad
+    double* d_mom;               // [12]
+    double* d_part;              // block partials
+    unsigned int* d_counter;
+    unsigned int blocks;
+    int64_t last_valid;
+    size_t rec_bytes;
+};
+
+namespace fw {
+
+namespace {
+
+constexpr int MI_THREADS = 256;
+constexpr int MAX_BINS = 32;  // one thread per joint cell in k_mi_finish
+constexpr double FIXED = 4294967296.0;  // 2^32
+
+struct MiMap {
+    double a[9];   // moving index from relative sample point
+    double b[3];
+    double h[3][3];  // index offset of +half a spacing along physical axis d (central difference)
+    DevGrid m;
+    int bins;
+    double mmin, mmax, mbin, mnmin;
+};
+
+__device__ __forceinline__ double bspline3(double u) {
+    double a = fabs(u);
+    if (a < 1.0) {
+        double s = a * a;
+        return (4.0 - 6.0 * s + 3.0 * s * a) / 6.0;
+    }
+    if (a < 2.0) {
+        double s = a * a;
+        return (8.0 - 12.0 * a + 6.0 * s - s * a) / 6.0;
+    }
+    return 0.0;
+}
+
+__device__ __forceinline__ double bspline3_derivative(double u) {
+    if (u >= 0.0 && u < 1.0) return -2.0 * u + 1.5 * u * u;
+    if (u > -1.0 && u < 0.0) return -2.0 * u - 1.5 * u * u;
+    if (u >= 1.0 && u < 2.0) return -2.0 + 2.0 * u - 0.5 * u * u;
+    if (u > -2.0 && u <= -1.0) return 2.0 + 2.0 * u + 0.5 * u * u;
+    return 0.0;
+}
+
+__device__ __forceinline__ int clamp_bin(double term, int bins) {
+    long long idx = isnan(term) ? 0 : (long long)term;  // truncation toward zero
+    return (int)min(max(idx, 2LL), (long long)bins - 3);
+}
+
+// The moving sample: index, interpolated value and its Parzen term; false when the sample does
+// not contribute (outside the buffer, not finite, or outside the moving range).
+__device__ __forceinline__ bool sample_value(const MiMap& mp, const float* __restrict__ img,
+                                             float4 r, double c[3], double& mv, double& term,
+                                             int& mbin) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        c[q] = mp.a[q * 3] * r.x + mp.a[q * 3 + 1] * r.y + mp.a[q * 3 + 2] * r.z + mp.b[q];
+    if (!inside_index(c[0], c[1], c[2], mp.m.nx, mp.m.ny, mp.m.nz)) return false;
+    float v = lin_at_index(img, mp.m.nx, mp.m.ny, mp.m.nz, c[0], c[1], c[2]);
+    mv = (double)v;
+    if (!isfinite(v) || mv < mp.mmin || mv > mp.mmax) return false;
+    term = mv / mp.mbin - mp.mnmin;
+    mbin = clamp_bin(term, mp.bins);
+    return true;
+}
+
+// Joint histogram of transform blockIdx.y over a chunk of samples per block.
+__global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict__ maps,
+                                                        const float4* __restrict__ rec,
+                                                        long long n,
+                                                        const float* __restrict__ img,
+                                                        unsigned long long* __restrict__ hist) {
+    const MiMap& mp = maps[blockIdx.y];
+    const int bins = mp.bins;
+    const int cells = bins * bins + bins;
+    extern __shared__ unsigned long long sh[];
+    for (int s = threadIdx.x; s < cells; s += blockDim.x) sh[s] = 0ULL;
+    __syncthreads();
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        float4 r = __ldg(rec + i);
+        double c[3], mv, term;
+        int mbin;
+        if (!sample_value(mp, img, r, c, mv, term, mbin)) continue;
+        const int fbin = (int)__float_as_uint(r.w);
+        atomicAdd(&sh[bins * bins + fbin], 1ULL);
+#pragma unroll
+        for (int pm = -1; pm <= 2; ++pm) {
+            double w = bspline3((double)(mbin + pm) - term);
+            unsigned long long q = (unsigned long long)__double2ll_rn(w * FIXED);
+            if (q) atomicAdd(&sh[fbin * bins + mbin + pm], q);
+        }
+    }
+    __syncthreads();
+    unsigned long long* out = hist + (size_t)blockIdx.y * cells;
+    for (int s = threadIdx.x; s < cells; s += blockDim.x)
+        if (sh[s]) atomicAdd(&out[s], sh[s]);
+}
+
+// ComputeResults (metric/mi.rs:702-768) for transform blockIdx.x: one thread per cell.
+// out[t*4 + 0] = -MI, [1] = valid samples, [2] = status (0 ok, 1 no valid sample, 2 zero PDF).
+__global__ void __launch_bounds__(1024) k_mi_finish(const unsigned long long* __restrict__ hist,
+                                                    int bins, double moving_bin_size,
+                                                    double* __restrict__ ratio,
+                                                    double* __restrict__ out, int want_ratio) {
+    const int cells = bins * bins + bins;
+    const unsigned long long* h = hist + (size_t)blockIdx.x * cells;
+    double* o = out + 4 * blockIdx.x;
+    __shared__ unsigned long long s_int[1024];
+    __shared__ double s_d[1024];
+    __shared__ double fmarg[MAX_BINS], mmarg[MAX_BINS];
+    __shared__ double norm_s;
+    __shared__ unsigned long long valid_s;
+    const int t = threadIdx.x;
+    const int nc = bins * bins;
+    // exact integer totals: the joint sum and the number of valid samples
+    unsigned long long js = 0, vs = 0;
+    for (int s = t; s < nc; s += blockDim.x) js += h[s];
+    for (int s = t; s < bins; s += blockDim.x) vs += h[nc + s];
+    s_int[t] = js;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w) s_int[t] += s_int[t + w];
+        __syncthreads();
+    }
+    if (t == 0) norm_s = (double)s_int[0] / FIXED;
+    __syncthreads();
+    s_int[t] = vs;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w) s_int[t] += s_int[t + w];
+        __syncthreads();
+    }
+    if (t == 0) valid_s = s_int[0];
+    __syncthreads();
+    const double pdf_sum = norm_s;
+    const unsigned long long num_valid = valid_s;
+    if (num_valid == 0 || pdf_sum < DBL_EPSILON) {
+        if (t == 0) {
+            o[0] = 0.0;
+            o[1] = (double)num_valid;
+            o[2] = num_valid == 0 ? 1.0 : 2.0;
+        }
+        return;
+    }
+    const double norm = 1.0 / pdf_sum;
+    if (t < bins) fmarg[t] = (double)h[nc + t] * norm;
+    if (t < bins) {
+        double s = 0.0;
+        for (int row = 0; row < bins; ++row) s += ((double)h[row * bins + t] / FIXED) * norm;
+        mmarg[t] = s;
+    }
+    __syncthreads();
+    const double n_factor = -1.0 / (moving_bin_size * (double)num_valid);
+    double contrib = 0.0;
+    if (t < nc) {
+        int f = t / bins, m = t - f * bins;
+        double fm = fmarg[f], mm = mmarg[m];
+        double jv = ((double)h[t] / FIXED) * norm;
+        double r = 0.0;
+        if (fm > DBL_EPSILON && mm > DBL_EPSILON && jv > DBL_EPSILON) {
+            double pr = log(jv / mm);
+            contrib = jv * (pr - log(fm));
+            r = n_factor * pr;
+        }
+        if (want_ratio) ratio[t] = r;
+    }
+    s_d[t] = contrib;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w) s_d[t] += s_d[t + w];
+        __syncthreads();
+    }
+    if (t == 0) {
+        o[0] = -s_d[0];
+        o[1] = (double)num_valid;
+        o[2] = 0.0;
+    }
+}
+
+// Derivative moments M[i][j] = sum_s w_s grad_i [r; 1]_j with a fixed-order last-block reduction.
+__global__ void __launch_bounds__(MI_THREADS) k_mi_deriv(const MiMap* __restrict__ maps,
+                                                         const float4* __restrict__ rec,
+                                                         long long n,
+                                                         const float* __restrict__ img,
+                                                         const double* __restrict__ ratio,
+                                                         double* __restrict__ partials,
+                                                         unsigned int* __restrict__ counter,
+                                                         double* __restrict__ mom) {
+    const MiMap& mp = maps[0];
+    const int bins = mp.bins;
+    __shared__ double sratio[MAX_BINS * MAX_BINS];
+    for (int s = threadIdx.x; s < bins * bins; s += blockDim.x) sratio[s] = ratio[s];
+    __syncthreads();
+    double acc[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) acc[q] = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        float4 r = __ldg(rec + i);
+        double c[3], mv, term;
+        int mbin;
+        if (!sample_value(mp, img, r, c, mv, term, mbin)) continue;
+        const int fbin = (int)__float_as_uint(r.w);
+        double w = 0.0;
+#pragma unroll
+        for (int pm = -1; pm <= 2; ++pm)
+            w += bspline3_derivative((double)(mbin + pm) - term) * sratio[fbin * bins + mbin + pm];
+        if (w == 0.0) continue;
+        // interp.rs:96-120: half-spacing central difference along the physical axes
+        double g[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double c1x = c[0] - mp.h[d][0], c1y = c[1] - mp.h[d][1], c1z = c[2] - mp.h[d][2];
+            double c2x = c[0] + mp.h[d][0], c2y = c[1] + mp.h[d][1], c2z = c[2] + mp.h[d][2];
+            g[d] = 0.0;
+            if (!inside_index(c1x, c1y, c1z, mp.m.nx, mp.m.ny, mp.m.nz) ||
+                !inside_index(c2x, c2y, c2z, mp.m.nx, mp.m.ny, mp.m.nz))
+                continue;
+            float v1 = lin_at_index(img, mp.m.nx, mp.m.ny, mp.m.nz, c1x, c1y, c1z);
+            float v2 = lin_at_index(img, mp.m.nx, mp.m.ny, mp.m.nz, c2x, c2y, c2z);
+            g[d] = (double)(v2 - v1) / mp.m.sp[d];
+        }
+        if (!(isfinite(g[0]) && isfinite(g[1]) && isfinite(g[2]))) g[0] = g[1] = g[2] = 0.0;
+        const double p[4] = {(double)r.x, (double)r.y, (double)r.z, 1.0};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a * 4 + b] += w * g[a] * p[b];
+    }
+    __shared__ double red[12][MI_THREADS / 32];
+    __shared__ bool last;
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+        double v = warp_sum_d(acc[q]);
+        if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        double s = 0.0;
+        for (int w = 0; w < MI_THREADS / 32; ++w) s += red[threadIdx.x][w];
+        partials[(size_t)blockIdx.x * 12 + threadIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    if (threadIdx.x < 12) {
+        double s = 0.0;
+        for (unsigned int b = 0; b < gridDim.x; ++b) s += __ldcg(partials + (size_t)b * 12 + threadIdx.x);
+        mom[threadIdx.x] = s;
+    }
+    if (threadIdx.x == 0) *counter = 0;
+}
+
+// ---- host: transform maps and Jacobian matrices (transform/param.rs, affine.rs) -------------
+
+void parametric_affine(const fw_linear_transform* t, double M[9], double off[3]) {
+    double tr[3];
+    if (t->kind == 0) {
+        const double* p = t->parameters;
+        double cx = std::cos(p[0]), sx = std::sin(p[0]);
+        double cy = std::cos(p[1]), sy = std::sin(p[1]);
+        double cz = std::cos(p[2]), sz = std::sin(p[2]);
+        double rx[9] = {1, 0, 0, 0, cx, -sx, 0, sx, cx};
+        double ry[9] = {cy, 0, sy, 0, 1, 0, -sy, 0, cy};
+        double rz[9] = {cz, -sz, 0, sz, cz, 0, 0, 0, 1};
+        double tmp[9];
+        if (t->zyx) {
+            mat3_mul(rz, ry, tmp);
+            mat3_mul(tmp, rx, M);
+        } else {
+            mat3_mul(rz, rx, tmp);
+            mat3_mul(tmp, ry, M);
+        }
+        tr[0] = p[3];
+        tr[1] = p[4];
+        tr[2] = p[5];
+    } else {
+        for (int k = 0; k < 9; ++k) M[k] = t->parameters[k];
+        tr[0] = t->parameters[9];
+        tr[1] = t->parameters[10];
+        tr[2] = t->parameters[11];
+    }
+    double mc[3];
+    mat3_vec(M, t->center, mc);
+    for (int r = 0; r < 3; ++r) off[r] = tr[r] + t->center[r] - mc[r];
+}
+
+void linear_map(const fw_linear_transform* t, double Mout[9], double off_out[3]) {
+    double M[9], off[3];
+    parametric_affine(t, M, off);
+    double oc[3], ooff[3];
+    mat3_vec(t->outer_matrix, t->outer_center, oc);
+    for (int r = 0; r < 3; ++r) ooff[r] = t->outer_translation[r] + t->outer_center[r] - oc[r];
+    mat3_mul(t->outer_matrix, M, Mout);
+    double mo[3];
+    mat3_vec(t->outer_matrix, off, mo);
+    for (int r = 0; r < 3; ++r) off_out[r] = mo[r] + ooff[r];
+}
+
+// transform/param.rs:188-288, 448-457: Jacobian columns at p (outer matrix applied).
+int jacobian_columns(const fw_linear_transform* t, const double p[3], double cols[36]) {
+    for (int k = 0; k < 36; ++k) cols[k] = 0.0;
+    int np;
+    if (t->kind == 0) {
+        const double* q = t->parameters;
+        double cx = std::cos(q[0]), sx = std::sin(q[0]);
+        double cy = std::cos(q[1]), sy = std::sin(q[1]);
+        double cz = std::cos(q[2]), sz = std::sin(q[2]);
+        double px = p[0] - t->center[0], py = p[1] - t->center[1], pz = p[2] - t->center[2];
+        double *o0 = cols, *o1 = cols + 3, *o2 = cols + 6;
+        if (t->zyx) {
+            o0[0] = (cz * sy * cx + sz * sx) * py + (-cz * sy * sx + sz * cx) * pz;
+            o0[1] = (sz * sy * cx - cz * sx) * py + (-sz * sy * sx - cz * cx) * pz;
+            o0[2] = (cy * cx) * py + (-cy * sx) * pz;
+            o1[0] = (-cz * sy) * px + (cz * cy * sx) * py + (cz * cy * cx) * pz;
+            o1[1] = (-sz * sy) * px + (sz * cy * sx) * py + (sz * cy * cx) * pz;
+            o1[2] = (-cy) * px + (-sy * sx) * py + (-sy * cx) * pz;
+            o2[0] = (-sz * cy) * px + (-sz * sy * sx - cz * cx) * py + (-sz * sy * cx + cz * sx) * pz;
+            o2[1] = (cz * cy) * px + (cz * sy * sx - sz * cx) * py + (cz * sy * cx + sz * sx) * pz;
+        } else {
+            o0[0] = (-sz * cx * sy) * px + (sz * sx) * py + (sz * cx * cy) * pz;
+            o0[1] = (cz * cx * sy) * px + (-cz * sx) * py + (-cz * cx * cy) * pz;
+            o0[2] = (sx * sy) * px + cx * py + (-sx * cy) * pz;
+            o1[0] = (-cz * sy - sz * sx * cy) * px + (cz * cy - sz * sx * sy) * pz;
+            o1[1] = (-sz * sy + cz * sx * cy) * px + (sz * cy + cz * sx * sy) * pz;
+            o1[2] = (-cx * cy) * px + (-cx * sy) * pz;
+            o2[0] = (-sz * cy - cz * sx * sy) * px + (-cz * cx) * py + (-sz * sy + cz * sx * cy) * pz;
+            o2[1] = (cz * cy - sz * sx * sy) * px + (-sz * cx) * py + (cz * sy + sz * sx * cy) * pz;
+        }
+        for (int d = 0; d < 3; ++d) cols[3 * (3 + d) + d] = 1.0;
+        np = 6;
+    } else {
+        for (int r = 0; r < 3; ++r) {
+            for (int c = 0; c < 3; ++c) cols[3 * (r * 3 + c) + r] = p[c] - t->center[c];
+            cols[3 * (9 + r) + r] = 1.0;
+        }
+        np = 12;
+    }
+    for (int k = 0; k < np; ++k) {
+        double v[3] = {cols[3 * k], cols[3 * k + 1], cols[3 * k + 2]}, o[3];
+        mat3_vec(t->outer_matrix, v, o);
+        for (int r = 0; r < 3; ++r) cols[3 * k + r] = o[r];
+    }
+    return np;
+}
+
+MiMap make_map(const fw_mi_level* L, const fw_linear_transform* t) {
+    MiMap mp;
+    std::memset(&mp, 0, sizeof(mp));
+    const HostGrid& g = L->moving->grid;
+    double M[9], off[3];
+    linear_map(t, M, off);
+    // index = inv (M (centre + r) + off - org) = (inv M) r + inv (M centre + off - org)
+    mat3_mul(g.inv, M, mp.a);
+    double mc[3];
+    mat3_vec(M, L->center, mc);
+    double v[3] = {mc[0] + off[0] - g.org[0], mc[1] + off[1] - g.org[1], mc[2] + off[2] - g.org[2]};
+    mat3_vec(g.inv, v, mp.b);
+    for (int d = 0; d < 3; ++d)
+        for (int r = 0; r < 3; ++r) mp.h[d][r] = 0.5 * g.sp[d] * g.inv[r * 3 + d];
+    mp.m = dev_grid(g);
+    mp.bins = L->binning.bins;
+    mp.mmin = L->binning.moving_min;
+    mp.mmax = L->binning.moving_max;
+    mp.mbin = L->binning.moving_bin_size;
+    mp.mnmin = L->binning.moving_normalized_min;
+    return mp;
+}
+
+int hist_and_finish(fw_mi_level* L, const fw_linear_transform* ts, int count, bool want_ratio) {
+    fw_ctx* ctx = L->ctx;
+    const int bins = L->binning.bins;
+    const int cells = bins * bins + bins;
+    std::vector<MiMap> maps(count);
+    for (int t = 0; t < count; ++t) maps[t] = make_map(L, &ts[t]);
+    MiMap* d_maps = reinterpret_cast<MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
+    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (sizeof(MiMap) * count + 7) / 8 + 16));
+    d_maps = reinterpret_cast<MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
+    FW_CUDA(cudaMemcpyAsync(d_maps, maps.data(), sizeof(MiMap) * count, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    FW_CUDA(cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells * count, ctx->stream));
+    size_t sh = sizeof(unsigned long long) * cells;
+    dim3 grid(L->blocks, count);
+    k_mi_hist<<<grid, MI_THREADS, sh, ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d, L->d_hist);
+    FW_TRY(check_launch(ctx, "k_mi_hist"));
+    k_mi_finish<<<count, 1024, 0, ctx->stream>>>(L->d_hist, bins, L->binning.moving_bin_size,
+                                                 L->d_ratio, L->d_out, want_ratio ? 1 : 0);
+    return check_launch(ctx, "k_mi_finish");
+}
+
+int check_status(fw_mi_level* L, const double* out) {
+    L->last_valid = (int64_t)out[1];
+    if (out[2] == 1.0) return fail(FW_ERR_INVALID, "mattes: all samples map outside the moving image buffer");
+    if (out[2] == 2.0) return fail(FW_ERR_INVALID, "mattes: joint PDF summed to zero");
+    return 0;
+}
+
+}  // namespace
+
+}  // namespace fw
+
+using namespace fw;
+
+extern "C" {
+
+static int mi_prepare_common(fw_ctx* ctx, fw_image* moving, bool own, const double* points,
+                             const uint32_t* fixed_bin, int64_t n, const fw_mi_binning* binning,
+                             fw_mi_level** out) {
+    if (n <= 0) {
+        if (own) fw_image_free(moving);
+        return fail(FW_ERR_INVALID, "mattes: no samples inside the fixed image");
+    }
+    if (binning->bins <= 4 || binning->bins > MAX_BINS) {
+        if (own) fw_image_free(moving);
+        return fail(FW_ERR_INVALID, "mattes: bins must be in 5..=32");
+    }
+    fw_mi_level* L = new fw_mi_level();
+    L->ctx = ctx;
+    L->moving = moving;
+    L->own_moving = own;
+    L->n = n;
+    L->binning = *binning;
+    // the cloud centre in float64; records hold float32 offsets from it
+    double c[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) c[a] += points[3 * i + a];
+    for (int a = 0; a < 3; ++a) L->center[a] = c[a] / (double)n;
+    std::vector<float4> rec((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        if (fixed_bin[i] >= (uint32_t)binning->bins) {
+            if (own) fw_image_free(moving);
+            delete L;
+            return fail(FW_ERR_INVALID, "mattes: a fixed bin is out of range");
+        }
+        rec[i].x = (float)(points[3 * i] - L->center[0]);
+        rec[i].y = (float)(points[3 * i + 1] - L->center[1]);
+        rec[i].z = (float)(points[3 * i + 2] - L->center[2]);
+        uint32_t b = fixed_bin[i];
+        std::memcpy(&rec[i].w, &b, 4);
+    }
+    L->rec_bytes = sizeof(float4) * (size_t)n;
+    const int cells = binning->bins * binning->bins + binning->bins;
+    const int max_t = 16;
+    L->blocks = (unsigned int)std::max<long long>(
+        1, std::min<long long>((n + MI_THREADS - 1) / MI_THREADS, 4LL * ctx->num_sms));
+    int rc = dev_alloc(ctx, L->rec_bytes, (void**)&L->d_rec);
+    if (!rc) rc = dev_alloc(ctx, sizeof(unsigned long long) * cells * max_t, (void**)&L->d_hist);
+    if (!rc) rc = dev_alloc(ctx, sizeof(double) * binning->bins * binning->bins, (void**)&L->d_ratio);
+    if (!rc) rc = dev_alloc(ctx, sizeof(double) * 4 * max_t, (void**)&L->d_out);
+    if (!rc) rc = dev_alloc(ctx, sizeof(double) * 16, (void**)&L->d_mom);
+    if (!rc) rc = dev_alloc(ctx, sizeof(double) * 12 * L->blocks, (void**)&L->d_part);
+    if (!rc) rc = dev_alloc(ctx, sizeof(unsigned int) * 4, (void**)&L->d_counter);
+    if (!rc) {
+        cudaError_t e = cudaMemsetAsync(L->d_counter, 0, sizeof(unsigned int) * 4, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(L->d_rec, rec.data(), L->rec_bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "mi level upload");
+        ctx->stats.bytes_uploaded += L->rec_bytes;
+    }
+    if (!rc) rc = sync(ctx);
+    if (rc) {
+        fw_mi_level_free(L);
+        return rc;
+    }
+    *out = L;
+    return 0;
+}
+
+int fw_mi_level_prepare(fw_ctx* ctx, const fw_grid* moving_grid, const double* moving,
+                        const double* points, const uint32_t* fixed_bin, int64_t n,
+                        const fw_mi_binning* binning, fw_mi_level** out) {
+    FW_CHECK(ctx && moving_grid && moving && points && fixed_bin && binning && out, "null argument");
+    fw_image* img;
+    FW_TRY(fw_image_upload(ctx, moving_grid, moving, &img));
+    return mi_prepare_common(ctx, img, true, points, fixed_bin, n, binning, out);
+}
+
+int fw_mi_level_prepare_image(fw_ctx* ctx, const fw_image* moving, const double* points,
+                              const uint32_t* fixed_bin, int64_t n,
+                              const fw_mi_binning* binning, fw_mi_level** out) {
+    FW_CHECK(ctx && moving && points && fixed_bin && binning && out, "null argument");
+    return mi_prepare_common(ctx, const_cast<fw_image*>(moving), false, points, fixed_bin, n,
+                             binning, out);
+}
+
+int fw_mi_level_value(fw_mi_level* L, const fw_linear_transform* t, double* value) {
+    FW_CHECK(L && t && value, "null argument");
+    FW_TRY(hist_and_finish(L, t, 1, false));
+    double out[3];
+    FW_TRY(read_back(L->ctx, L->d_out, 3, out));
+    FW_TRY(check_status(L, out));
+    *value = out[0];
+    return 0;
+}
+
+int fw_mi_level_values(fw_mi_level* L, const fw_linear_transform* ts, int32_t count,
+                       double* values) {
+    FW_CHECK(L && ts && values, "null argument");
+    FW_CHECK(count >= 1 && count <= 16, "mattes: 1..=16 transforms per batch");
+    FW_TRY(hist_and_finish(L, ts, count, false));
+    std::vector<double> out(4 * count);
+    FW_TRY(read_back(L->ctx, L->d_out, 4 * count, out.data()));
+    for (int t = 0; t < count; ++t) {
+        FW_TRY(check_status(L, &out[4 * t]));
+        values[t] = out[4 * t];
+    }
+    return 0;
+}
+
+int fw_mi_level_value_and_derivative(fw_mi_level* L, const fw_linear_transform* t,
+                                     double* value, double* derivative) {
+    FW_CHECK(L && t && value && derivative, "null argument");
+    fw_ctx* ctx = L->ctx;
+    FW_TRY(hist_and_finish(L, t, 1, true));
+    const MiMap* d_maps = reinterpret_cast<const MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
+    k_mi_deriv<<<L->blocks, MI_THREADS, 0, ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d,
+                                                          L->d_ratio, L->d_part, L->d_counter,
+                                                          L->d_mom);
+    FW_TRY(check_launch(ctx, "k_mi_deriv"));
+    // one read-back: status block (value, valid, status) and the twelve moments
+    FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, L->d_out, sizeof(double) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    FW_CUDA(cudaMemcpyAsync(ctx->h_pinned + 4, L->d_mom, sizeof(double) * 12, cudaMemcpyDeviceToHost, ctx->stream));
+    FW_TRY(sync(ctx));
+    double out[4], mom[12];
+    std::memcpy(out, ctx->h_pinned, sizeof(out));
+    std::memcpy(mom, ctx->h_pinned + 4, sizeof(mom));
+    FW_TRY(check_status(L, out));
+    *value = out[0];
+    // G_mu in relative coordinates: col_mu(c + r) = J(c) + (J(c + e_j) - J(c)) r_j
+    double j0[36], je[3][36];
+    FW_TRY(0);
+    int np = jacobian_columns(t, L->center, j0);
+    for (int j = 0; j < 3; ++j) {
+        double p[3] = {L->center[0], L->center[1], L->center[2]};
+        p[j] += 1.0;
+        jacobian_columns(t, p, je[j]);
+    }
+    for (int mu = 0; mu < np; ++mu) {
+        double s = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            for (int j = 0; j < 3; ++j) s += (je[j][3 * mu + i] - j0[3 * mu + i]) * mom[i * 4 + j];
+            s += j0[3 * mu + i] * mom[i * 4 + 3];
+        }
+        derivative[mu] = s;
+    }
+    return 0;
+}
+
+int fw_mi_level_num_valid(const fw_mi_level* L, int64_t* out) {
+    FW_CHECK(L && out, "null argument");
+    *out = L->last_valid;
+    return 0;
+}
+
+void fw_mi_level_free(fw_mi_level* L) {
+    if (!L) return;
+    fw_ctx* ctx = L->ctx;
+    const int cells = L->binning.bins * L->binning.bins + L->binning.bins;
+    dev_free(ctx, L->d_rec, L->rec_bytes);
+    dev_free(ctx, L->d_hist, sizeof(unsigned long long) * cells * 16);
+    dev_free(ctx, L->d_ratio, sizeof(double) * L->binning.bins * L->binning.bins);
+    dev_free(ctx, L->d_out, sizeof(double) * 4 * 16);
+    dev_free(ctx, L->d_mom, sizeof(double) * 16);
+    dev_free(ctx, L->d_part, sizeof(double) * 12 * L->blocks);
+    dev_free(ctx, L->d_counter, sizeof(unsigned int) * 4);
+    if (L->own_moving) fw_image_free(L->moving);
+    delete L;
+}
+
+}  // extern "C"

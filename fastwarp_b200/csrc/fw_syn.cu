@@ -1,0 +1,847 @@
+// fw_syn.cu -- the SyN stage driver (syn.rs:337-445, 776-986) on the device.
+//
+// One iteration (syn.rs:890-958): warp fixed and moving through F^-1 and affine(M^-1); the CC
+// pair (window sums shared by both directions); for several channels the multi-metric
+// combination (syn.rs:203-282); Gaussian smoothing of both gradients with the max |u/sp| fused;
+// F <- F + (step / max) u(x + F) (scale fused into the composition, done in place because every
+// voxel reads only its own F); optional total-field smoothing; the inversion pair
+// F^-1 = invert(F, init F^-1), F = invert(F^-1, init F) in place; then the energy enters the
+// window convergence monitor (convergence.rs:47-126).
+//
+// Graph design: every buffer of a level is allocated once, so the kernel sequence of an
+// iteration is the same every time. The whole level is captured as ONE CUDA graph: an outer
+// WHILE node whose body is the iteration, with each of the four inversions an inner WHILE node
+// whose condition the inversion's last block sets (no host read-back inside the loop). A
+// single-thread record kernel at the end of the body runs the convergence monitor on the device,
+// writes the iteration record and sets the outer condition. The host launches one graph and
+// reads the records back once per level.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fw_internal.cuh"
+
+namespace fw {
+
+namespace {
+
+constexpr int MAX_WINDOW = 64;
+
+struct SynDev {
+    int it;          // iterations done in this level
+    int limit;       // iteration limit of this level
+    int converged;
+    int status;      // 0 ok, 1 gradient not finite, 2 field not finite, 3 cancelled
+    int level;
+    int window;
+    int count;       // values in the window
+    int head;
+    double total;    // running sum of |energy| of every value added
+    double values[MAX_WINDOW];
+    double threshold;
+    double step;
+    int channels;
+    int pad;
+    double wnorm[FW_MAX_CHANNELS];
+};
+
+// convergence.rs:91-126, the closed form of the two-control-point fit.
+__device__ double convergence_value(const SynDev& s) {
+    if (s.count < s.window) return DBL_MAX;
+    if (s.window < 2) return 0.0;
+    const double spline_eps = 1e-3, domain_spacing = 0.1, domain_size = 11.0;
+    double r = 1.0 / ((domain_size - 1.0) * domain_spacing);
+    double epsilon = r * domain_spacing * spline_eps;
+    double delta[2] = {0, 0}, omega[2] = {0, 0};
+    for (int k = 0; k < s.count; ++k) {
+        double e = s.values[(s.head + k) % s.window];
+        double p = ((double)k / (double)(s.window - 1)) * r;
+        if (fabs(p - 1.0) <= epsilon) p = 1.0 - epsilon;
+        if (p < 0.0 && fabs(p) <= epsilon) p = 0.0;
+        double t = p - floor(p);
+        double w[2] = {1.0 - t, t};
+        double w2 = w[0] * w[0] + w[1] * w[1];
+        double v = e / s.total;
+        for (int j = 0; j < 2; ++j) {
+            omega[j] += w[j] * w[j];
+            delta[j] += v * (w[j] * w[j] * w[j] / w2);
+        }
+    }
+    double phi[2] = {0, 0};
+    for (int j = 0; j < 2; ++j) {
+        if (fabs(omega[j]) > DBL_EPSILON) {
+            double q = delta[j] / omega[j];
+            phi[j] = isfinite(q) ? q : 0.0;
+        }
+    }
+    return phi[0] - phi[1];
+}
+
+__global__ void k_syn_level_init(SynDev* s, int level, int limit) {
+    s->it = 0;
+    s->limit = limit;
+    s->converged = 0;
+    s->status = 0;
+    s->level = level;
+    s->count = 0;
+    s->head = 0;
+    s->total = 0.0;
+}
+
+// cc: [channel][value, |dF|^2, |dM|^2]; max_bits: [F side, M side]; inv: 4 loop states.
+__global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
+                             const unsigned int* __restrict__ max_bits,
+                             const InvState* __restrict__ inv, fw_syn_iteration* trace,
+                             int trace_cap, const volatile int* cancel,
+                             cudaGraphConditionalHandle handle, int use_handle) {
+    double vF = cc[0], vM = cc[0];  // the CC value is symmetric in its two images
+    double weighted = 0.0;
+    for (int c = 0; c < s->channels; ++c) weighted += cc[3 * c] * s->wnorm[c];
+    if (s->channels == 1) weighted = vF;
+    for (int c = 0; c < s->channels && s->channels > 1; ++c)
+        if (!isfinite(cc[3 * c + 1]) || !isfinite(cc[3 * c + 2])) s->status = 1;
+    float mF = __uint_as_float(max_bits[0]), mM = __uint_as_float(max_bits[1]);
+    if (!isfinite(mF) || !isfinite(mM)) s->status = 1;
+    for (int q = 0; q < 4; ++q)
+        if (!isfinite(inv[q].mean) || !isfinite(inv[q].max)) s->status = s->status ? s->status : 2;
+    double energy = 0.5 * (vF + vM);
+    // WindowConvergenceMonitor::add_energy_value
+    if (s->count < s->window) {
+        s->values[(s->head + s->count) % s->window] = energy;
+        s->count++;
+    } else {
+        s->values[s->head] = energy;
+        s->head = (s->head + 1) % s->window;
+    }
+    s->total += fabs(energy);
+    double cv = convergence_value(*s);
+    if (cv < s->threshold) s->converged = 1;
+    int it = s->it;
+    if (it < trace_cap) {
+        fw_syn_iteration r;
+        r.level = s->level;
+        r.energy = energy;
+        r.energy_weighted = 0.5 * (weighted + weighted);
+        r.convergence_value = cv;
+        r.fixed_update_scale = mF > 0.0f ? s->step / (double)mF : s->step;
+        r.moving_update_scale = mM > 0.0f ? s->step / (double)mM : s->step;
+        for (int q = 0; q < 4; ++q) {
+            r.inversions[q].iterations = inv[q].executed;
+            r.inversions[q].mean_error_norm = inv[q].executed ? inv[q].mean : 0.0;
+            r.inversions[q].max_error_norm = inv[q].executed ? inv[q].max : 0.0;
+        }
+        trace[it] = r;
+    }
+    s->it = it + 1;
+    if (cancel && *cancel) s->status = 3;
+    int more = (s->it < s->limit) && !s->converged && s->status == 0;
+    if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// acc += (w / |x|) x when |x| > eps (syn.rs:233-240), |x|^2 read from the device.
+__global__ void k_axpy_norm(float4* __restrict__ acc, const float4* __restrict__ x, long long n4,
+                            const double* __restrict__ nsq, double w) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n4) return;
+    double mag = sqrt(*nsq);
+    if (!(mag > DBL_EPSILON)) return;
+    float a = (float)(w / mag);
+    float4 v = acc[l], u = x[l];
+    v.x = fmaf(a, u.x, v.x);
+    v.y = fmaf(a, u.y, v.y);
+    v.z = fmaf(a, u.z, v.z);
+    v.w = fmaf(a, u.w, v.w);
+    acc[l] = v;
+}
+
+// acc *= sum_c |d_c| / C (syn.rs:259-263); `which` selects |dF|^2 (1) or |dM|^2 (2).
+__global__ void k_scale_norms(float4* __restrict__ acc, long long n4, const double* __restrict__ cc,
+                              int channels, int which) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n4) return;
+    double tot = 0.0;
+    for (int c = 0; c < channels; ++c) tot += sqrt(cc[3 * c + which]);
+    float s = (float)(tot / channels);
+    float4 v = acc[l];
+    v.x *= s;
+    v.y *= s;
+    v.z *= s;
+    v.w *= s;
+    acc[l] = v;
+}
+
+struct Level {
+    HostGrid grid;
+    int channels = 1;
+    fw_field *F = nullptr, *Fi = nullptr, *M = nullptr, *Mi = nullptr;
+    std::vector<fw_image*> fmid, mmid;
+    fw_field *dF = nullptr, *dM = nullptr;      // raw CC derivatives
+    fw_field *accF = nullptr, *accM = nullptr;  // multichannel combination
+    fw_field *sF = nullptr, *sM = nullptr;      // smoothed updates
+    fw_field* T = nullptr;                      // total-field smoothing
+};
+
+void free_level_work(Level& L) {
+    for (auto* im : L.fmid) fw_image_free(im);
+    for (auto* im : L.mmid) fw_image_free(im);
+    L.fmid.clear();
+    L.mmid.clear();
+    fw_field* fs[] = {L.dF, L.dM, L.accF, L.accM, L.sF, L.sM, L.T};
+    for (auto* f : fs) fw_field_free(f);
+    L.dF = L.dM = L.accF = L.accM = L.sF = L.sM = L.T = nullptr;
+}
+
+int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
+    for (int c = 0; c < L.channels; ++c) {
+        fw_image *a, *b;
+        FW_TRY(new_image(ctx, L.grid, &a));
+        L.fmid.push_back(a);
+        FW_TRY(new_image(ctx, L.grid, &b));
+        L.mmid.push_back(b);
+    }
+    FW_TRY(new_field(ctx, L.grid, &L.dF));
+    FW_TRY(new_field(ctx, L.grid, &L.dM));
+    if (L.channels > 1) {
+        FW_TRY(new_field(ctx, L.grid, &L.accF));
+        FW_TRY(new_field(ctx, L.grid, &L.accM));
+    }
+    if (r->update_field_variance > 0.0) {
+        FW_TRY(new_field(ctx, L.grid, &L.sF));
+        FW_TRY(new_field(ctx, L.grid, &L.sM));
+    }
+    if (r->total_field_variance > 0.0) FW_TRY(new_field(ctx, L.grid, &L.T));
+    return 0;
+}
+
+// Device scalars of a run.
+struct RunDev {
+    SynDev* syn;
+    double* cc;              // [channels][3]
+    unsigned int* max_bits;  // [2]
+    InvState* inv;           // [4]
+    fw_syn_iteration* trace;
+    int trace_cap;
+};
+
+const fw_invert_params kSynInvert = {20, 0.001, 0.1, 1};
+
+// Adds a WHILE node at the capture position of `s` and returns its body graph.
+int add_while(cudaStream_t s, unsigned int default_value, unsigned int flags,
+              cudaGraphConditionalHandle* handle, cudaGraph_t* body) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps;
+    size_t ndeps;
+    FW_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, &g, &deps, &ndeps));
+    FW_CHECK(status == cudaStreamCaptureStatusActive, "graph capture is not active");
+    FW_CUDA(cudaGraphConditionalHandleCreate(handle, g, default_value, flags));
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = *handle;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    FW_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &p));
+    *body = p.conditional.phGraph_out[0];
+    FW_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return 0;
+}
+
+// One inversion: in graph mode a WHILE node around the body kernel; in direct mode a host loop.
+int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inverse,
+                   InvState* st) {
+    if (!graph) {
+        FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, kSynInvert, st, 0, 0));
+        InvState h;
+        for (int body = 0; body < kSynInvert.max_iterations; ++body) {
+            FW_TRY(enqueue_inversion_body(ctx, field, inverse, st, 0, 0));
+            FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, st, sizeof(InvState), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+            FW_TRY(sync(ctx));
+            std::memcpy(&h, ctx->h_pinned, sizeof(h));
+            if (!h.go) break;
+        }
+        return 0;
+    }
+    // the handle lives in the graph being captured; the measure kernel sets it
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps;
+    size_t ndeps;
+    FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
+    cudaGraphConditionalHandle h;
+    FW_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, kSynInvert, st, h, 1));
+    FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    FW_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &p));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    FW_CUDA(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1,
+                                                cudaStreamSetCaptureDependencies));
+    // capture the body on the auxiliary stream
+    cudaStream_t main = ctx->stream;
+    FW_CUDA(cudaStreamBeginCaptureToGraph(ctx->aux, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed));
+    ctx->stream = ctx->aux;
+    int rc = enqueue_inversion_body(ctx, field, inverse, st, h, 1);
+    ctx->stream = main;
+    cudaGraph_t out;
+    cudaError_t e = cudaStreamEndCapture(ctx->aux, &out);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "inversion body capture");
+    return 0;
+}
+
+unsigned int blocks256(long long n) { return (unsigned int)((n + 255) / 256); }
+
+// The kernels of one iteration (syn.rs:890-958) on ctx->stream.
+int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
+                      const std::vector<const fw_image*>& fs,
+                      const std::vector<const fw_image*>& ms, const fw_affine* initial,
+                      const RunDev& d) {
+    const int C = L.channels;
+    FW_CUDA(cudaMemsetAsync(d.max_bits, 0, 2 * sizeof(unsigned int), ctx->stream));
+    if (C > 1) {
+        FW_CUDA(cudaMemsetAsync(L.accF->d, 0, L.accF->bytes, ctx->stream));
+        FW_CUDA(cudaMemsetAsync(L.accM->d, 0, L.accM->bytes, ctx->stream));
+    }
+    double wsum = 0.0;
+    for (int c = 0; c < C; ++c) wsum += r->channel_weights[c];
+    const long long n4 = 3 * L.dF->ps / 4;
+    for (int c = 0; c < C; ++c) {
+        FW_TRY(launch_warp(ctx, fs[c], L.Fi, nullptr, nullptr, L.fmid[c]->d, false, nullptr));
+        FW_TRY(launch_warp(ctx, ms[c], L.Mi, nullptr, initial, L.mmid[c]->d, false, nullptr));
+        FW_TRY(launch_cc_pair_impl(ctx, L.fmid[c], L.mmid[c], r->cc_radius, L.dF, L.dM,
+                                   d.cc + 3 * c, C > 1 ? 1 : 0));
+        if (C > 1) {
+            double wn = r->channel_weights[c] / wsum;
+            k_axpy_norm<<<blocks256(n4), 256, 0, ctx->stream>>>((float4*)L.accF->d,
+                                                                (const float4*)L.dF->d, n4,
+                                                                d.cc + 3 * c + 1, wn);
+            FW_TRY(check_launch(ctx, "k_axpy_norm"));
+            k_axpy_norm<<<blocks256(n4), 256, 0, ctx->stream>>>((float4*)L.accM->d,
+                                                                (const float4*)L.dM->d, n4,
+                                                                d.cc + 3 * c + 2, wn);
+            FW_TRY(check_launch(ctx, "k_axpy_norm"));
+        }
+    }
+    fw_field* gF = L.dF;
+    fw_field* gM = L.dM;
+    if (C > 1) {
+        k_scale_norms<<<blocks256(n4), 256, 0, ctx->stream>>>((float4*)L.accF->d, n4, d.cc, C, 1);
+        FW_TRY(check_launch(ctx, "k_scale_norms"));
+        k_scale_norms<<<blocks256(n4), 256, 0, ctx->stream>>>((float4*)L.accM->d, n4, d.cc, C, 2);
+        FW_TRY(check_launch(ctx, "k_scale_norms"));
+        gF = L.accF;
+        gM = L.accM;
+    }
+    // smooth_field(update variance) with the max norm fused; without smoothing, the max alone
+    if (r->update_field_variance > 0.0) {
+        FW_TRY(launch_smooth(ctx, gF, L.sF, r->update_field_variance, d.max_bits));
+        FW_TRY(launch_smooth(ctx, gM, L.sM, r->update_field_variance, d.max_bits + 1));
+        gF = L.sF;
+        gM = L.sM;
+    } else {
+        FW_TRY(launch_max_norm(ctx, gF, d.max_bits));
+        FW_TRY(launch_max_norm(ctx, gM, d.max_bits + 1));
+    }
+    // update_total_field for both sides (syn.rs:422-445)
+    struct Side {
+        fw_field* u;
+        fw_field* field;
+        fw_field* inverse;
+        const unsigned int* max;
+        InvState* st;
+    } sides[2] = {{gF, L.F, L.Fi, d.max_bits, d.inv}, {gM, L.M, L.Mi, d.max_bits + 1, d.inv + 2}};
+    for (auto& s : sides) {
+        // compose in place: every voxel reads its own field value and the update elsewhere
+        FW_TRY(launch_compose(ctx, s.u, s.field, s.field, s.max, r->gradient_step));
+        if (r->total_field_variance > 0.0) {
+            FW_TRY(launch_smooth(ctx, s.field, L.T, r->total_field_variance, nullptr));
+            FW_CUDA(cudaMemcpyAsync(s.field->d, L.T->d, s.field->bytes, cudaMemcpyDeviceToDevice,
+                                    ctx->stream));
+        }
+        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, s.st));      // inverse = invert(field)
+        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, s.st + 1));  // field = invert(inverse)
+    }
+    return 0;
+}
+
+int syn_validate(const fw_syn_recipe* r) {
+    FW_CHECK(r, "null recipe");
+    FW_CHECK(r->levels >= 1 && r->levels <= FW_MAX_LEVELS, "syn recipe: no levels");
+    FW_CHECK(r->channels >= 1 && r->channels <= FW_MAX_CHANNELS, "syn recipe: 1..=4 channels");
+    double ws = 0.0;
+    for (int c = 0; c < r->channels; ++c) {
+        FW_CHECK(std::isfinite(r->channel_weights[c]) && r->channel_weights[c] >= 0.0,
+                 "syn recipe: channel weights must be non-negative with a positive sum");
+        ws += r->channel_weights[c];
+    }
+    FW_CHECK(ws > DBL_EPSILON, "syn recipe: channel weights must be non-negative with a positive sum");
+    for (int l = 0; l < r->levels; ++l) FW_CHECK(r->shrink_factors[l] > 0, "syn recipe: shrink factor 0");
+    FW_CHECK(std::isfinite(r->gradient_step) && r->gradient_step > 0.0,
+             "syn recipe: gradient step must be positive");
+    FW_CHECK(r->cc_radius >= 1 && r->cc_radius <= 8, "syn recipe: CC radius must be in 1..=8");
+    FW_CHECK(r->convergence_window >= 1 && r->convergence_window <= MAX_WINDOW,
+             "syn recipe: convergence window must be in 1..=64");
+    FW_CHECK(std::isfinite(r->update_field_variance) && std::isfinite(r->total_field_variance),
+             "syn recipe: variances must be finite");
+    return 0;
+}
+
+// pyramid.rs:58-93
+void shrink_factors(uint32_t factor, const double sp[3], uint32_t out[3]) {
+    factor = std::max(factor, 1u);
+    int mi = 0;
+    double ms = sp[0];
+    for (int n = 1; n < 3; ++n)
+        if (ms > sp[n]) {
+            ms = sp[n];
+            mi = n;
+        }
+    double target = sp[mi] * (double)factor;
+    out[0] = out[1] = out[2] = 0;
+    out[mi] = factor;
+    for (int n = 0; n < 3; ++n) {
+        if (out[n] != 0) continue;
+        double best_diff = std::fabs(sp[n] * (double)factor - target);
+        uint32_t best = factor;
+        for (uint32_t f = factor - 1; f >= 1; --f) {
+            double diff = std::fabs(sp[n] * (double)f - target);
+            if (diff <= best_diff) {
+                best_diff = diff;
+                best = f;
+            }
+        }
+        out[n] = best;
+    }
+}
+
+// pyramid.rs:99-129
+int shrink_grid(const HostGrid& g, const uint32_t f[3], HostGrid& out) {
+    fw_grid o = to_c(g);
+    for (int a = 0; a < 3; ++a) {
+        uint32_t fa = std::max(f[a], 1u);
+        o.spacing[a] = g.sp[a] * (double)fa;
+        o.size[a] = std::max((int64_t)std::floor((double)g.n[a] / (double)fa), (int64_t)1);
+    }
+    double ic[3], oc[3], ip[3], op[3];
+    for (int a = 0; a < 3; ++a) {
+        ic[a] = ((double)g.n[a] - 1.0) / 2.0;
+        oc[a] = ((double)o.size[a] - 1.0) / 2.0;
+    }
+    auto index_to_point = [](const HostGrid& gg, const double c[3], double p[3]) {
+        double s[3] = {c[0] * gg.sp[0], c[1] * gg.sp[1], c[2] * gg.sp[2]};
+        for (int r = 0; r < 3; ++r)
+            p[r] = gg.org[r] + (gg.dir[r * 3] * s[0] + gg.dir[r * 3 + 1] * s[1] + gg.dir[r * 3 + 2] * s[2]);
+    };
+    index_to_point(g, ic, ip);
+    HostGrid prov;
+    FW_TRY(make_grid(&o, prov));
+    index_to_point(prov, oc, op);
+    for (int a = 0; a < 3; ++a) o.origin[a] = g.org[a] + (ip[a] - op[a]);
+    return make_grid(&o, out);
+}
+
+int level_grid(const fw_syn_recipe* r, const HostGrid& fixed, int level, HostGrid& out) {
+    uint32_t f[3];
+    shrink_factors(r->shrink_factors[level], fixed.sp, f);
+    return shrink_grid(fixed, f, out);
+}
+
+struct RunScratch {
+    fw_ctx* ctx = nullptr;
+    void* base = nullptr;
+    size_t bytes = 0;
+    RunDev d{};
+    ~RunScratch() {
+        if (base) dev_free(ctx, base, bytes);
+    }
+    int init(fw_ctx* c, int channels, int trace_cap) {
+        ctx = c;
+        size_t off_syn = 0;
+        size_t off_cc = off_syn + ((sizeof(SynDev) + 255) / 256) * 256;
+        size_t off_max = off_cc + 256;
+        size_t off_inv = off_max + 256;
+        size_t off_trace = off_inv + ((4 * sizeof(InvState) + 255) / 256) * 256;
+        bytes = off_trace + sizeof(fw_syn_iteration) * (size_t)std::max(trace_cap, 1);
+        (void)channels;
+        FW_TRY(dev_alloc(ctx, bytes, &base));
+        char* b = static_cast<char*>(base);
+        d.syn = reinterpret_cast<SynDev*>(b + off_syn);
+        d.cc = reinterpret_cast<double*>(b + off_cc);
+        d.max_bits = reinterpret_cast<unsigned int*>(b + off_max);
+        d.inv = reinterpret_cast<InvState*>(b + off_inv);
+        d.trace = reinterpret_cast<fw_syn_iteration*>(b + off_trace);
+        d.trace_cap = trace_cap;
+        FW_CUDA(cudaMemsetAsync(base, 0, bytes, ctx->stream));
+        return 0;
+    }
+};
+
+int upload_syn_dev(fw_ctx* ctx, const fw_syn_recipe* r, SynDev* d) {
+    SynDev h;
+    std::memset(&h, 0, sizeof(h));
+    h.window = r->convergence_window;
+    h.threshold = r->convergence_threshold;
+    h.step = r->gradient_step;
+    h.channels = r->channels;
+    double ws = 0.0;
+    for (int c = 0; c < r->channels; ++c) ws += r->channel_weights[c];
+    for (int c = 0; c < r->channels; ++c) h.wnorm[c] = r->channel_weights[c] / ws;
+    FW_CUDA(cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
+    return sync(ctx);  // h lives on this stack frame
+}
+
+struct GraphGuard {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ~GraphGuard() {
+        if (e) cudaGraphExecDestroy(e);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+
+// Captures the level's iteration loop as one graph, launches it and waits.
+int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
+                    const std::vector<const fw_image*>& fs, const std::vector<const fw_image*>& ms,
+                    const fw_affine* initial, const RunDev& d, int level, int limit,
+                    fw_syn_iteration* trace_dev_base) {
+    GraphGuard G;
+    FW_CUDA(cudaGraphCreate(&G.g, 0));
+    FW_CUDA(cudaStreamBeginCaptureToGraph(ctx->stream, G.g, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed));
+    ctx->capturing = true;
+    int rc = 0;
+    cudaGraphConditionalHandle h_it = 0;
+    cudaGraph_t body = nullptr;
+    k_syn_level_init<<<1, 1, 0, ctx->stream>>>(d.syn, level, limit);
+    rc = check_launch(ctx, "k_syn_level_init");
+    if (!rc) rc = add_while(ctx->stream, limit > 0 ? 1u : 0u, cudaGraphCondAssignDefault, &h_it, &body);
+    cudaGraph_t top;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &top);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "level graph capture");
+    if (!rc) {
+        e = cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed);
+        if (e != cudaSuccess) rc = cuda_fail(e, "iteration capture");
+        if (!rc) {
+            rc = enqueue_iteration(ctx, true, r, L, fs, ms, initial, d);
+            if (!rc) {
+                k_syn_record<<<1, 1, 0, ctx->stream>>>(d.syn, d.cc, d.max_bits, d.inv,
+                                                      trace_dev_base, d.trace_cap, nullptr, h_it, 1);
+                rc = check_launch(ctx, "k_syn_record");
+            }
+            cudaGraph_t b2;
+            e = cudaStreamEndCapture(ctx->stream, &b2);
+            if (!rc && e != cudaSuccess) rc = cuda_fail(e, "iteration capture end");
+        }
+    }
+    ctx->capturing = false;
+    if (rc) {
+        cudaGetLastError();
+        return rc;
+    }
+    FW_CUDA(cudaGraphInstantiate(&G.e, G.g, 0));
+    FW_CUDA(cudaGraphLaunch(G.e, ctx->stream));
+    ctx->stats.graph_launches++;
+    return sync(ctx);
+}
+
+int check_status(int status) {
+    switch (status) {
+        case 0: return 0;
+        case 1: return fail(FW_ERR_NOT_FINITE, "syn: the metric gradient is not finite");
+        case 2: return fail(FW_ERR_NOT_FINITE, "syn: the displacement field is not finite");
+        case 3: return fail(FW_ERR_CANCELLED, "registration cancelled");
+        default: return fail(FW_ERR_INVALID, "syn: unknown device status");
+    }
+}
+
+// Kernels per iteration outside the inversion bodies (for the launch counter).
+int kernels_per_iteration(const fw_syn_recipe* r) {
+    int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) + 2 /*smooth or max*/ +
+            2 /*compose*/ + (r->total_field_variance > 0.0 ? 2 : 0) + 4 * 2 /*inv init+measure*/ +
+            1 /*record*/;
+    return k;
+}
+
+}  // namespace
+
+int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
+                   const fw_image* const* moving, const fw_affine* initial, fw_field** warp,
+                   fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
+                   int64_t* count) {
+    FW_TRY(syn_validate(r));
+    const int C = r->channels;
+    for (int c = 0; c < C; ++c) FW_CHECK(fixed[c] && moving[c], "syn: null channel image");
+    const HostGrid fg = fixed[0]->grid;
+    for (int c = 1; c < C; ++c)
+        if (!fixed[c]->grid.same(fg)) return fail(FW_ERR_INVALID, "syn: fixed images of the channels differ in grid");
+    int total_iters = 0;
+    for (int l = 0; l < r->levels; ++l) total_iters += (int)r->iterations[l];
+    // scratch for every reduction of the biggest level, before any capture
+    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)(1 << 20)));
+    RunScratch rs;
+    FW_TRY(rs.init(ctx, C, std::max(total_iters, 1)));
+    FW_TRY(upload_syn_dev(ctx, r, rs.d.syn));
+    Level L;
+    L.channels = C;
+    HostGrid prev;
+    bool have_prev = false;
+    std::vector<fw_image*> owned;
+    auto free_owned = [&]() {
+        for (auto* im : owned) fw_image_free(im);
+        owned.clear();
+    };
+    auto free_state = [&]() {
+        fw_field* st[] = {L.F, L.Fi, L.M, L.Mi};
+        for (auto* f : st) fw_field_free(f);
+        L.F = L.Fi = L.M = L.Mi = nullptr;
+    };
+    int rc = 0;
+    int done = 0;
+    for (int level = 0; level < r->levels && !rc; ++level) {
+        if (ctx->cancel && *ctx->cancel) {
+            rc = fail(FW_ERR_CANCELLED, "registration cancelled");
+            break;
+        }
+        HostGrid lg;
+        rc = level_grid(r, fg, level, lg);
+        if (rc) break;
+        // level smoothing of the full-resolution images (pyramid.rs:446-460), on the device
+        std::vector<const fw_image*> fs(C), ms(C);
+        double sigma = r->smoothing_sigmas[level];
+        free_owned();
+        for (int c = 0; c < C && !rc; ++c) {
+            if (sigma > 0.0) {
+                double sf[3], sm[3];
+                for (int a = 0; a < 3; ++a) {
+                    sf[a] = r->sigma_units_mm ? sigma : sigma * fixed[c]->grid.sp[a];
+                    sm[a] = r->sigma_units_mm ? sigma : sigma * moving[c]->grid.sp[a];
+                }
+                fw_image *a = nullptr, *b = nullptr;
+                rc = new_image(ctx, fixed[c]->grid, &a);
+                if (!rc) owned.push_back(a);
+                if (!rc) rc = launch_smooth_recursive(ctx, fixed[c], sf, a);
+                if (!rc) rc = new_image(ctx, moving[c]->grid, &b);
+                if (!rc) owned.push_back(b);
+                if (!rc) rc = launch_smooth_recursive(ctx, moving[c], sm, b);
+                fs[c] = a;
+                ms[c] = b;
+            } else {
+                fs[c] = fixed[c];
+                ms[c] = moving[c];
+            }
+        }
+        if (rc) break;
+        // state fields: zero on the first level, resampled afterwards (syn.rs:850-884)
+        fw_field* st[4] = {L.F, L.Fi, L.M, L.Mi};
+        fw_field* nx[4] = {nullptr, nullptr, nullptr, nullptr};
+        for (int q = 0; q < 4 && !rc; ++q) {
+            rc = new_field(ctx, lg, &nx[q]);
+            if (rc) break;
+            if (!have_prev) {
+                FW_CUDA(cudaMemsetAsync(nx[q]->d, 0, nx[q]->bytes, ctx->stream));
+            } else if (prev.same(lg)) {
+                FW_CUDA(cudaMemcpyAsync(nx[q]->d, st[q]->d, nx[q]->bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+            } else {
+                rc = launch_resample(ctx, st[q], nx[q]);
+            }
+        }
+        if (rc) {
+            for (auto* f : nx) fw_field_free(f);
+            break;
+        }
+        free_state();
+        L.F = nx[0];
+        L.Fi = nx[1];
+        L.M = nx[2];
+        L.Mi = nx[3];
+        L.grid = lg;
+        prev = lg;
+        have_prev = true;
+        free_level_work(L);
+        rc = alloc_level_work(ctx, r, L);
+        if (rc) break;
+        int limit = (int)r->iterations[level];
+        if (limit > 0) {
+            rc = run_level_graph(ctx, r, L, fs, ms, initial, rs.d, level, limit, rs.d.trace + done);
+            if (rc) break;
+            // the level's records and the device status
+            SynDev h;
+            FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, rs.d.syn, sizeof(SynDev), cudaMemcpyDeviceToHost, ctx->stream));
+            rc = sync(ctx);
+            if (rc) break;
+            std::memcpy(&h, ctx->h_pinned, sizeof(h));
+            int ran = h.it;
+            if (records && done < cap) {
+                int k = (int)std::min<int64_t>(ran, cap - done);
+                FW_CUDA(cudaMemcpy(records + done, rs.d.trace + done, sizeof(fw_syn_iteration) * k,
+                                   cudaMemcpyDeviceToHost));
+                // inversion bodies ran inside the graph: count them as launches
+                for (int q = 0; q < k; ++q)
+                    for (int s = 0; s < 4; ++s)
+                        ctx->stats.kernel_launches += records[done + q].inversions[s].iterations;
+            }
+            ctx->stats.kernel_launches += (uint64_t)ran * kernels_per_iteration(r) + 1;
+            done += ran;
+            rc = check_status(h.status);
+        }
+    }
+    free_level_work(L);
+    free_owned();
+    if (!rc) {
+        // syn.rs:969-970: forward = F + Minv(x + F), inverse = M + Finv(x + M)
+        fw_field *w = nullptr, *iw = nullptr;
+        rc = new_field(ctx, L.grid, &w);
+        if (!rc) rc = new_field(ctx, L.grid, &iw);
+        if (!rc) rc = launch_compose(ctx, L.Mi, L.F, w, nullptr, 1.0);
+        if (!rc) rc = launch_compose(ctx, L.Fi, L.M, iw, nullptr, 1.0);
+        if (!rc) rc = sync(ctx);
+        if (rc) {
+            fw_field_free(w);
+            fw_field_free(iw);
+        } else {
+            *warp = w;
+            *inverse_warp = iw;
+        }
+    }
+    free_state();
+    if (count) *count = done;
+    return rc;
+}
+
+}  // namespace fw
+
+using namespace fw;
+
+extern "C" {
+
+int fw_shrink_factors(uint32_t factor, const double spacing[3], uint32_t out[3]) {
+    FW_CHECK(spacing && out, "null argument");
+    shrink_factors(factor, spacing, out);
+    return 0;
+}
+
+int fw_shrink_grid(const fw_grid* grid, const uint32_t factors[3], fw_grid* out) {
+    FW_CHECK(grid && factors && out, "null argument");
+    HostGrid g, o;
+    FW_TRY(make_grid(grid, g));
+    FW_TRY(shrink_grid(g, factors, o));
+    *out = to_c(o);
+    return 0;
+}
+
+int fw_syn_level_grid(const fw_syn_recipe* recipe, const fw_grid* fixed_grid, int32_t level,
+                      fw_grid* out) {
+    FW_CHECK(recipe && fixed_grid && out, "null argument");
+    FW_TRY(syn_validate(recipe));
+    FW_CHECK(level >= 0 && level < recipe->levels, "syn: level out of range");
+    HostGrid g, o;
+    FW_TRY(make_grid(fixed_grid, g));
+    FW_TRY(level_grid(recipe, g, level, o));
+    *out = to_c(o);
+    return 0;
+}
+
+int fw_syn_step(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const* fixed,
+                const fw_image* const* moving, const fw_affine* initial, fw_field* f2m,
+                fw_field* f2m_inv, fw_field* m2m, fw_field* m2m_inv, double* fixed_update,
+                double* moving_update, fw_syn_iteration* record) {
+    FW_CHECK(ctx && recipe && fixed && moving && f2m && f2m_inv && m2m && m2m_inv, "null argument");
+    FW_TRY(syn_validate(recipe));
+    const HostGrid& g = f2m->grid;
+    FW_CHECK(f2m_inv->grid.same(g) && m2m->grid.same(g) && m2m_inv->grid.same(g),
+             "syn: the state fields differ in grid");
+    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)(1 << 20)));
+    Level L;
+    L.channels = recipe->channels;
+    L.grid = g;
+    L.F = f2m;
+    L.Fi = f2m_inv;
+    L.M = m2m;
+    L.Mi = m2m_inv;
+    int rc = alloc_level_work(ctx, recipe, L);
+    RunScratch rs;
+    if (!rc) rc = rs.init(ctx, L.channels, 1);
+    if (!rc) rc = upload_syn_dev(ctx, recipe, rs.d.syn);
+    std::vector<const fw_image*> fs(fixed, fixed + L.channels), ms(moving, moving + L.channels);
+    if (!rc) {
+        k_syn_level_init<<<1, 1, 0, ctx->stream>>>(rs.d.syn, 0, 1);
+        rc = check_launch(ctx, "k_syn_level_init");
+    }
+    if (!rc) rc = enqueue_iteration(ctx, false, recipe, L, fs, ms, initial, rs.d);
+    if (!rc) {
+        k_syn_record<<<1, 1, 0, ctx->stream>>>(rs.d.syn, rs.d.cc, rs.d.max_bits, rs.d.inv, rs.d.trace, 1,
+                                              nullptr, 0, 0);
+        rc = check_launch(ctx, "k_syn_record");
+    }
+    // the scaled updates of both sides (what the reference passes to compose)
+    for (int side = 0; side < 2 && !rc; ++side) {
+        double* out = side == 0 ? fixed_update : moving_update;
+        if (!out) continue;
+        fw_field* u = side == 0 ? (L.sF ? L.sF : (L.accF ? L.accF : L.dF))
+                                : (L.sM ? L.sM : (L.accM ? L.accM : L.dM));
+        rc = launch_scale_by_max(ctx, u, rs.d.max_bits + side, recipe->gradient_step);
+        if (!rc) rc = fw_field_download(ctx, u, out);
+    }
+    if (!rc) rc = sync(ctx);
+    if (!rc && record) {
+        FW_CUDA(cudaMemcpy(record, rs.d.trace, sizeof(fw_syn_iteration), cudaMemcpyDeviceToHost));
+        record->convergence_value = DBL_MAX;
+    }
+    if (!rc) {
+        SynDev h;
+        FW_CUDA(cudaMemcpy(&h, rs.d.syn, sizeof(h), cudaMemcpyDeviceToHost));
+        rc = check_status(h.status);
+    }
+    L.F = L.Fi = L.M = L.Mi = nullptr;  // owned by the caller
+    free_level_work(L);
+    return rc;
+}
+
+int fw_syn_run_device(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const* fixed,
+                      const fw_image* const* moving, const fw_affine* initial,
+                      fw_field** warp, fw_field** inverse_warp, fw_syn_iteration* records,
+                      int64_t cap, int64_t* count) {
+    FW_CHECK(ctx && recipe && fixed && moving && warp && inverse_warp, "null argument");
+    return syn_run_device(ctx, recipe, fixed, moving, initial, warp, inverse_warp, records, cap,
+                          count);
+}
+
+int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_grid,
+               const float* const* fixed, const fw_grid* moving_grid, const float* const* moving,
+               const fw_affine* initial, float* warp, float* inverse_warp,
+               fw_syn_iteration* records, int64_t cap, int64_t* count) {
+    FW_CHECK(ctx && recipe && fixed_grid && fixed && moving_grid && moving && warp && inverse_warp,
+             "null argument");
+    FW_TRY(syn_validate(recipe));
+    const int C = recipe->channels;
+    std::vector<fw_image*> fi(C, nullptr), mi(C, nullptr);
+    int rc = 0;
+    for (int c = 0; c < C && !rc; ++c) {
+        rc = fw_image_upload_f32(ctx, fixed_grid, fixed[c], &fi[c]);
+        if (!rc) rc = fw_image_upload_f32(ctx, moving_grid, moving[c], &mi[c]);
+    }
+    fw_field *w = nullptr, *iw = nullptr;
+    if (!rc) {
+        std::vector<const fw_image*> cf(fi.begin(), fi.end()), cm(mi.begin(), mi.end());
+        rc = syn_run_device(ctx, recipe, cf.data(), cm.data(), initial, &w, &iw, records, cap, count);
+    }
+    if (!rc) rc = fw_field_download_f32(ctx, w, warp);
+    if (!rc) rc = fw_field_download_f32(ctx, iw, inverse_warp);
+    fw_field_free(w);
+    fw_field_free(iw);
+    for (auto* im : fi) fw_image_free(im);
+    for (auto* im : mi) fw_image_free(im);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,323 @@
+/*
+ * fastwarp_cuda.h -- C ABI of the B200 (sm_100a) registration engine.
+ *
+ * This is the drop-in boundary for the hot path of WyssCenter/fastwarp: every entry point
+ * replaces one operation of the engine interface that the registration loops drive,
+ *   - trait `Backend`      crates/fastwarp-reg/src/backend.rs:39-305 (SyN loop),
+ *   - trait `LinearEngine` crates/fastwarp-reg/src/linear.rs:288-320 and
+ *     trait `LinearMetric` crates/fastwarp-reg/src/optimizer.rs:60-65 (Rigid/Affine Mattes MI),
+ * and the SyN stage driver `syn_fields` crates/fastwarp-reg/src/syn.rs:776-986.
+ * The reference declaration each function replaces is cited beside it.
+ *
+ * Conventions
+ *  - Grids are ITK LPS grids (crates/fastwarp-reg/src/grid.rs:33-40): size, spacing (mm),
+ *    origin (mm) and the 3x3 direction matrix row-major with the axis directions as columns.
+ *    Voxels are x-fastest.
+ *  - Images live on the device as float32 (one value per voxel). Fields live on the device as
+ *    float32 SoA planes x | y | z of LPS millimetre displacements. Host-side fields are AoS
+ *    (x, y, z per voxel), float64 (`VectorField`, field_ops.rs:58-64) or float32
+ *    (`DisplacementField`).
+ *  - Every call returns 0 on success and a negative status on failure; fw_last_error() gives
+ *    the message of the last failure on the calling thread (RegError::Invalid's text where the
+ *    reference has one).
+ *  - One CUDA stream per context. Every call is synchronous from the caller's view (its results
+ *    are ready when it returns), as the reference's native futures are ready on first poll
+ *    (crates/fastwarp-reg/src/exec.rs:14-30). Contexts are independent and may be used from
+ *    different threads at the same time; one context must not be used by two threads at once.
+ *  - Nothing falls back to the CPU: a call on a machine without a usable sm_100 GPU fails.
+ */
+#ifndef FASTWARP_CUDA_H
+#define FASTWARP_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FW_OK 0
+#define FW_ERR_INVALID -1   /* RegError::Invalid: bad argument, mismatched grids, no overlap */
+#define FW_ERR_CUDA -2      /* a CUDA runtime error */
+#define FW_ERR_MEMORY -3    /* device allocation failed or the HBM budget is exhausted */
+#define FW_ERR_NOT_FINITE -4 /* "the metric gradient is not finite" / "the displacement field is not finite" */
+#define FW_ERR_TIMEOUT -5   /* a bounded device-side wait ran out */
+#define FW_ERR_CANCELLED -6 /* RegError::Cancelled (syn.rs:826, 891) */
+
+typedef struct fw_ctx fw_ctx;
+typedef struct fw_image fw_image;
+typedef struct fw_field fw_field;
+typedef struct fw_mi_level fw_mi_level;
+
+/* crates/fastwarp-reg/src/grid.rs:33-40 */
+typedef struct fw_grid {
+    int64_t size[3];
+    double spacing[3];
+    double origin[3];
+    double direction[9];
+} fw_grid;
+
+/* AffineTransform as one map y = matrix * p + offset (transform/affine.rs:77-86). */
+typedef struct fw_affine {
+    double matrix[9];
+    double offset[3];
+} fw_affine;
+
+/* InvertParams, field_ops.rs:276-296 (SyN: 20, 0.001, 0.1, true). */
+typedef struct fw_invert_params {
+    int32_t max_iterations;
+    double mean_error_tolerance;
+    double max_error_tolerance;
+    int32_t enforce_boundary_condition;
+} fw_invert_params;
+
+/* InvertStats, field_ops.rs:300-307. */
+typedef struct fw_invert_stats {
+    int32_t iterations;
+    double mean_error_norm;
+    double max_error_norm;
+} fw_invert_stats;
+
+/* MiBinning, metric/mi.rs:117-137. */
+typedef struct fw_mi_binning {
+    int32_t bins;
+    double fixed_min, fixed_max, moving_min, moving_max;
+    double fixed_bin_size, moving_bin_size;
+    double fixed_normalized_min, moving_normalized_min;
+} fw_mi_binning;
+
+/* LinearMovingTransform, transform/param.rs:392-420: outer(optimised(p)).
+ * kind 0 = Euler3DTransform (parameters: angles x, y, z in radians, then translation; zyx
+ * selects the Rz Ry Rx composition), kind 1 = AffineTransform (matrix row-major, then
+ * translation). `center` is the optimised transform's centre. */
+typedef struct fw_linear_transform {
+    double outer_matrix[9];
+    double outer_translation[3];
+    double outer_center[3];
+    int32_t kind;
+    int32_t zyx;
+    double parameters[12];
+    double center[3];
+} fw_linear_transform;
+
+/* SynRecipe, recipe.rs:52-100 (CC channels, no masks). */
+#define FW_MAX_LEVELS 8
+#define FW_MAX_CHANNELS 4
+typedef struct fw_syn_recipe {
+    double gradient_step;
+    double update_field_variance;
+    double total_field_variance;
+    int32_t cc_radius;
+    int32_t levels;
+    uint32_t iterations[FW_MAX_LEVELS];
+    uint32_t shrink_factors[FW_MAX_LEVELS];
+    double smoothing_sigmas[FW_MAX_LEVELS];
+    int32_t sigma_units_mm;
+    double convergence_threshold;
+    int32_t convergence_window;
+    int32_t channels;
+    double channel_weights[FW_MAX_CHANNELS];
+} fw_syn_recipe;
+
+/* SynIteration, syn.rs:96-113. */
+typedef struct fw_syn_iteration {
+    int32_t level;
+    double energy;
+    double energy_weighted;
+    double convergence_value;
+    double fixed_update_scale;
+    double moving_update_scale;
+    fw_invert_stats inversions[4];
+} fw_syn_iteration;
+
+/* Counters of BackendStats (crates/fastwarp-gpu/src/wgpu_backend.rs:209-220) plus device
+ * launches. */
+typedef struct fw_stats {
+    uint64_t kernel_launches;
+    uint64_t graph_launches;
+    uint64_t host_syncs;
+    uint64_t bytes_uploaded;
+    uint64_t bytes_downloaded;
+    uint64_t peak_device_bytes;
+    uint64_t live_device_bytes;
+} fw_stats;
+
+/* ---- errors, context ------------------------------------------------------------------- */
+
+/* The message of the last failure on this thread (RegError's Display text). */
+const char* fw_last_error(void);
+
+/* Opens a context on `device` with its own stream. Fails on a GPU that is not sm_100.
+ * Replaces the device open of the wgpu engine (crates/fastwarp-gpu/src/device.rs). */
+int fw_ctx_create(int device, fw_ctx** out);
+void fw_ctx_destroy(fw_ctx* ctx);
+/* The context's cudaStream_t, for callers that interleave their own device work. */
+void* fw_ctx_stream(fw_ctx* ctx);
+int fw_ctx_synchronize(fw_ctx* ctx);
+int fw_ctx_stats(const fw_ctx* ctx, fw_stats* out);
+void fw_ctx_reset_stats(fw_ctx* ctx);
+/* Free and total device memory (cudaMemGetInfo): the capacity budget that engine.rs:843-861
+ * builds from its device caps. */
+int fw_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes);
+/* Backend::name (backend.rs:46). */
+const char* fw_backend_name(void);
+
+/* ---- images and fields (backend.rs:52-87) ----------------------------------------------- */
+
+/* Backend::upload_image (backend.rs:53): a float64 volume, stored as float32. */
+int fw_image_upload(fw_ctx* ctx, const fw_grid* grid, const double* host, fw_image** out);
+/* The same from float32 host data (no conversion). */
+int fw_image_upload_f32(fw_ctx* ctx, const fw_grid* grid, const float* host, fw_image** out);
+int fw_image_download(fw_ctx* ctx, const fw_image* img, float* host);
+int fw_image_grid(const fw_image* img, fw_grid* out);
+/* Device address of the float32 voxels (for zero-copy interop). */
+void* fw_image_device_ptr(fw_image* img);
+void fw_image_free(fw_image* img);
+
+/* Backend::zero_field (backend.rs:61). */
+int fw_field_zero(fw_ctx* ctx, const fw_grid* grid, fw_field** out);
+/* Backend::upload_field (backend.rs:64): AoS float64 (VectorField). */
+int fw_field_upload(fw_ctx* ctx, const fw_grid* grid, const double* aos, fw_field** out);
+/* Backend::download_field (backend.rs:67): AoS float64 (VectorField). */
+int fw_field_download(fw_ctx* ctx, const fw_field* field, double* aos);
+/* The same as AoS float32 (DisplacementField, what run_syn returns). */
+int fw_field_download_f32(fw_ctx* ctx, const fw_field* field, float* aos);
+/* Backend::field_grid (backend.rs:70). */
+int fw_field_grid(const fw_field* field, fw_grid* out);
+/* Backend::copy_field (backend.rs:73). */
+int fw_field_copy(fw_ctx* ctx, const fw_field* field, fw_field** out);
+/* Device address of plane 0 and the plane stride in floats (planes x | y | z). */
+void* fw_field_device_ptr(fw_field* field, int64_t* plane_stride);
+void fw_field_free(fw_field* field);
+
+/* ---- SyN operations (backend.rs:75-304) ------------------------------------------------- */
+
+/* Backend::warp_through_field (backend.rs:82-88): out(x) = source(affine(q + pre(q))),
+ * q = x + field(x), trilinear with ITK's buffer rule, zero outside. pre and affine may be NULL.
+ * The result lives on the grid of `field`. */
+int fw_warp_through_field(fw_ctx* ctx, const fw_image* source, const fw_field* field,
+                          const fw_field* pre, const fw_affine* affine, fw_image** out);
+
+/* Backend::warp_mask_through_field (backend.rs:98-105): nearest neighbour (half up), 1 where the
+ * mask is not zero; with `product` the result is multiplied into it and returned in it
+ * (*out == product). */
+int fw_warp_mask_through_field(fw_ctx* ctx, const fw_image* mask, const fw_field* field,
+                               const fw_field* pre, const fw_affine* affine, fw_image* product,
+                               fw_image** out);
+
+/* Backend::cc_value_derivative (backend.rs:110-115). */
+int fw_cc_value_derivative(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                           int32_t radius, double* value, fw_field** derivative);
+
+/* Backend::cc_value_derivative_pair (backend.rs:120-130): both directions from one set of
+ * window sums; values[0] = (fixed, moving), values[1] = (moving, fixed). */
+int fw_cc_value_derivative_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                                int32_t radius, double values[2], fw_field** d_fixed,
+                                fw_field** d_moving);
+
+/* Backend::cc_value_derivative_pair_with_norms (backend.rs:164-177): plus both L2 norms. */
+int fw_cc_value_derivative_pair_with_norms(fw_ctx* ctx, const fw_image* fixed,
+                                           const fw_image* moving, int32_t radius,
+                                           double values[2], fw_field** d_fixed,
+                                           fw_field** d_moving, double norms[2]);
+
+/* Backend::smooth_field (backend.rs:249): in place; variance <= 0 leaves the field unchanged. */
+int fw_smooth_field(fw_ctx* ctx, fw_field* field, double variance);
+
+/* Backend::max_scaled_norm / max_scaled_norm_pair (backend.rs:252-262). */
+int fw_max_scaled_norm(fw_ctx* ctx, const fw_field* field, double* out);
+int fw_max_scaled_norm_pair(fw_ctx* ctx, const fw_field* a, const fw_field* b, double out[2]);
+
+/* Backend::l2_norm (backend.rs:265). */
+int fw_l2_norm(fw_ctx* ctx, const fw_field* field, double* out);
+
+/* Backend::scale (backend.rs:268) and Backend::axpy (backend.rs:271). */
+int fw_scale(fw_ctx* ctx, fw_field* field, double s);
+int fw_axpy(fw_ctx* ctx, fw_field* acc, double a, const fw_field* x);
+
+/* Backend::compose (backend.rs:275-279): out(x) = warping(x) + displacement(x + warping(x)). */
+int fw_compose(fw_ctx* ctx, const fw_field* displacement, const fw_field* warping,
+               fw_field** out);
+
+/* Backend::invert (backend.rs:283-288): `initial` is updated in place and is the inverse. */
+int fw_invert(fw_ctx* ctx, const fw_field* field, fw_field* initial,
+              const fw_invert_params* params, fw_invert_stats* stats);
+
+/* Backend::invert_pair (backend.rs:293-302): inverse = invert(field, init = inverse), then
+ * field = invert(inverse, init = field), both in place; stats in call order. */
+int fw_invert_pair(fw_ctx* ctx, fw_field* field, fw_field* inverse,
+                   const fw_invert_params* params, fw_invert_stats stats[2]);
+
+/* Backend::resample_field (backend.rs:305). */
+int fw_resample_field(fw_ctx* ctx, const fw_field* field, const fw_grid* grid, fw_field** out);
+
+/* ---- level pyramid (pyramid.rs:58-129, 418-460) ---------------------------------------- */
+
+/* shrink_factors_per_dimension (pyramid.rs:58-93). */
+int fw_shrink_factors(uint32_t factor, const double spacing[3], uint32_t out[3]);
+/* level_virtual_grid / shrink_grid (pyramid.rs:99-158). */
+int fw_shrink_grid(const fw_grid* grid, const uint32_t factors[3], fw_grid* out);
+/* smooth_recursive_gaussian (pyramid.rs:418-427) on the device: a new image. */
+int fw_smooth_recursive(fw_ctx* ctx, const fw_image* img, const double sigma_mm[3],
+                        fw_image** out);
+
+/* ---- Mattes MI of the linear stages (linear.rs:288-320, optimizer.rs:60-65) ------------- */
+
+/* LinearEngine::prepare_level (linear.rs:303-308): the moving level image and the prepared
+ * samples (points in LPS mm, n x 3; fixed bins; binning) become device-resident. */
+int fw_mi_level_prepare(fw_ctx* ctx, const fw_grid* moving_grid, const double* moving,
+                        const double* points, const uint32_t* fixed_bin, int64_t n,
+                        const fw_mi_binning* binning, fw_mi_level** out);
+/* The same with the moving image already on the device (no upload). */
+int fw_mi_level_prepare_image(fw_ctx* ctx, const fw_image* moving, const double* points,
+                              const uint32_t* fixed_bin, int64_t n,
+                              const fw_mi_binning* binning, fw_mi_level** out);
+/* LinearMetric::value (optimizer.rs:61): -MI. */
+int fw_mi_level_value(fw_mi_level* level, const fw_linear_transform* t, double* value);
+/* LinearMetric::value_and_derivative (optimizer.rs:62-64): -MI and +dMI/dtheta (6 or 12). */
+int fw_mi_level_value_and_derivative(fw_mi_level* level, const fw_linear_transform* t,
+                                     double* value, double* derivative);
+/* Several value() evaluations in one pass over the samples (a line search's bracket). */
+int fw_mi_level_values(fw_mi_level* level, const fw_linear_transform* ts, int32_t count,
+                       double* values);
+/* Samples that contributed to the last evaluation. */
+int fw_mi_level_num_valid(const fw_mi_level* level, int64_t* out);
+void fw_mi_level_free(fw_mi_level* level);
+
+/* ---- SyN stage (syn.rs:776-986) --------------------------------------------------------- */
+
+/* The virtual grid of one level of `recipe` on the fixed grid. */
+int fw_syn_level_grid(const fw_syn_recipe* recipe, const fw_grid* fixed_grid, int32_t level,
+                      fw_grid* out);
+
+/* One SyN iteration (syn.rs:890-958) on device-resident state: f2m, f2m_inv, m2m, m2m_inv are
+ * replaced in place; fixed/moving are the level-smoothed full-resolution images (one per
+ * channel). Optional outputs: the two scaled update fields (host AoS float64, may be NULL). */
+int fw_syn_step(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const* fixed,
+                const fw_image* const* moving, const fw_affine* initial, fw_field* f2m,
+                fw_field* f2m_inv, fw_field* m2m, fw_field* m2m_inv, double* fixed_update,
+                double* moving_update, fw_syn_iteration* record);
+
+/* run_syn (syn.rs:555-564) from device-resident full-resolution images (one per channel):
+ * the forward and inverse SyN fields on the grid of the last level (new fields) and the
+ * per-iteration records (up to cap; *count = all iterations). */
+int fw_syn_run_device(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const* fixed,
+                      const fw_image* const* moving, const fw_affine* initial,
+                      fw_field** warp, fw_field** inverse_warp, fw_syn_iteration* records,
+                      int64_t cap, int64_t* count);
+
+/* run_syn from host float32 images: uploads, runs, and writes the two fields as AoS float32
+ * (DisplacementField) on the grid of the last level (fw_syn_level_grid). */
+int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_grid,
+               const float* const* fixed, const fw_grid* moving_grid, const float* const* moving,
+               const fw_affine* initial, float* warp, float* inverse_warp,
+               fw_syn_iteration* records, int64_t cap, int64_t* count);
+
+/* Sets a flag polled before every level and iteration (SynOptions::cancel, syn.rs:80-85);
+ * a run that sees it set fails with FW_ERR_CANCELLED. Pass NULL to clear. */
+int fw_ctx_set_cancel_flag(fw_ctx* ctx, const volatile int32_t* flag);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

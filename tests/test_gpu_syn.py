@@ -1,0 +1,129 @@
+"""The SyN step and the whole SyN stage on the GPU against the f64 oracle.
+
+Bars: a single SyN step matches to 1e-5 relative on the CC value and 1e-4 voxel on both update
+fields; a full registration matches to 0.05 mm RMS displacement and 1e-4 relative final CC.
+The oracle runs the same seeded 64^3 blob pair (config 1: CC radius 2, gradient step 0.25,
+update variance 3, total variance 0, 30 iterations, convergence threshold -1 so that both
+engines run every iteration, as crates/fastwarp-gpu/tests/syn_parity.rs:244-260 pins it).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from fastwarp_b200 import SynRecipe, run_syn, syn_step
+from fastwarp_b200.phantoms import blob_pair
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pair():
+    return blob_pair(64)
+
+
+def config1(iterations=30):
+    return SynRecipe(gradient_step=0.25, update_field_variance=3.0, total_field_variance=0.0,
+                     cc_radius=2, iterations=[iterations], shrink_factors=[1],
+                     smoothing_sigmas=[0.0], convergence_threshold=-1.0, convergence_window=10,
+                     channel_weights=[1.0])
+
+
+def oracle_recipe(r: SynRecipe):
+    return O.syn_recipe(r.gradient_step, r.update_field_variance, r.total_field_variance,
+                        r.cc_radius, r.iterations, r.shrink_factors, r.smoothing_sigmas,
+                        r.sigma_units_mm, r.convergence_threshold, r.convergence_window,
+                        r.channel_weights)
+
+
+def ogrid(g):
+    return O.make_grid(tuple(g.size), tuple(g.spacing), tuple(g.origin),
+                       np.array(g.direction[:]).reshape(3, 3))
+
+
+def test_one_syn_step_from_zero_matches(backend, pair):
+    g, fixed, moving = pair
+    r = config1(1)
+    og = ogrid(g)
+    fi = backend.upload_image(g, fixed)
+    mi = backend.upload_image(g, moving)
+    state = {k: backend.zero_field(g) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    rec, fu, mu = syn_step(backend, r, [fi], [mi], None, state)
+    ostate = {k: np.zeros((64, 64, 64, 3)) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    orec, ofu, omu = O.syn_step(oracle_recipe(r), og, og, [fixed], og, [moving], None, ostate)
+    assert abs(rec["energy"] - orec.energy) <= 1e-5 * abs(orec.energy)
+    assert np.abs(fu - ofu).max() <= 1e-4
+    assert np.abs(mu - omu).max() <= 1e-4
+    for k in state:
+        assert np.abs(backend.download_field(state[k]) - ostate[k]).max() <= 1e-4
+    assert [s[0] for s in rec["inversions"]] == [s.iterations for s in orec.inversions]
+
+
+def test_a_syn_step_from_a_deformed_state_matches(backend, pair):
+    """The oracle runs five iterations; both engines then take the sixth from that state."""
+    g, fixed, moving = pair
+    r = config1(1)
+    og = ogrid(g)
+    ostate = {k: np.zeros((64, 64, 64, 3)) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    for _ in range(5):
+        O.syn_step(oracle_recipe(r), og, og, [fixed], og, [moving], None, ostate)
+    fi = backend.upload_image(g, fixed)
+    mi = backend.upload_image(g, moving)
+    state = {k: backend.upload_field(g, v) for k, v in ostate.items()}
+    rec, fu, mu = syn_step(backend, r, [fi], [mi], None, state)
+    orec, ofu, omu = O.syn_step(oracle_recipe(r), og, og, [fixed], og, [moving], None, ostate)
+    assert abs(rec["energy"] - orec.energy) <= 1e-5 * abs(orec.energy)
+    assert np.abs(fu - ofu).max() <= 1e-4
+    assert np.abs(mu - omu).max() <= 1e-4
+
+
+def test_full_registration_matches_the_oracle(backend, pair):
+    g, fixed, moving = pair
+    r = config1(30)
+    og = ogrid(g)
+    res = run_syn(backend, r, g, [fixed], g, [moving])
+    ow, oinv, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed], og, [moving])
+    assert len(res.iterations) == len(orecs) == 30
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    rms_inv = np.sqrt(((res.inverse_warp.astype(np.float64) - oinv) ** 2).sum(-1).mean())
+    assert rms <= 0.05 and rms_inv <= 0.05, (rms, rms_inv)
+    e, oe = res.iterations[-1]["energy"], orecs[-1].energy
+    assert abs(e - oe) <= 1e-4 * abs(oe)
+    assert res.iterations[-1]["energy"] < res.iterations[0]["energy"]
+
+
+def test_multilevel_registration_with_pyramid_smoothing_matches(backend):
+    g, fixed, moving = blob_pair(48, seed=77)
+    r = SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2,
+                  iterations=[8, 6], shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0],
+                  convergence_threshold=-1.0)
+    og = ogrid(g)
+    res = run_syn(backend, r, g, [fixed], g, [moving])
+    ow, oinv, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed], og, [moving])
+    assert len(res.iterations) == len(orecs) == 14
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    assert rms <= 0.05, rms
+    assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
+
+
+def test_two_channel_registration_matches(backend):
+    g, fixed, moving = blob_pair(40, seed=91)
+    r = SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2, iterations=[6],
+                  shrink_factors=[1], smoothing_sigmas=[0.0], convergence_threshold=-1.0,
+                  channel_weights=[0.5, 0.5])
+    f2, m2 = 1.0 - fixed, 1.0 - moving  # inverted contrast (T2-like)
+    og = ogrid(g)
+    res = run_syn(backend, r, g, [fixed, f2], g, [moving, m2])
+    ow, _, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed, f2], og, [moving, m2])
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    assert rms <= 0.05, rms
+    assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
+
+
+def test_convergence_monitor_stops_the_level_on_the_device(backend, pair):
+    g, fixed, moving = pair
+    r = config1(60)
+    r.convergence_threshold = 1e-3  # loose: the monitor stops the level early
+    og = ogrid(g)
+    res = run_syn(backend, r, g, [fixed], g, [moving])
+    ow, _, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed], og, [moving])
+    assert len(res.iterations) == len(orecs) < 60
