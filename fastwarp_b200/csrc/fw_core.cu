@@ -314,12 +314,9 @@ __global__ void __launch_bounds__(256) k_resample(DevGrid d, DevGrid s, const fl
     if (l >= d.n) return;
     int i, j, k;
     voxel_ijk(l, d.nx, d.ny, i, j, k);
-    double p[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) p[r] = d.org[r] + (d.ds[r * 3] * i + d.ds[r * 3 + 1] * j + d.ds[r * 3 + 2] * k) - s.org[r];
-    double c[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) c[r] = s.inv[r * 3] * p[0] + s.inv[r * 3 + 1] * p[1] + s.inv[r * 3 + 2] * p[2];
+    double p[3], c[3];
+    exact_point(d, i, j, k, p);
+    exact_index(s, p, c);
     bool in = inside_index(c[0], c[1], c[2], s.nx, s.ny, s.nz);
 #pragma unroll
     for (int q = 0; q < 3; ++q)

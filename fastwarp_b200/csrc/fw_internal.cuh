@@ -202,6 +202,28 @@ __device__ __forceinline__ void vec_at_index(const float* __restrict__ f, long l
     }
 }
 
+// Grid::index_to_point then another grid's Grid::point_to_index (grid.rs:131-156) in the
+// reference's float64 operation order with no fused multiply-adds, so points on a buffer edge
+// (-0.5 or n - 0.5) fall on the same side as in the reference.
+__device__ __forceinline__ void exact_point(const DevGrid& g, double i, double j, double k,
+                                            double p[3]) {
+    double s0 = __dmul_rn(i, g.sp[0]), s1 = __dmul_rn(j, g.sp[1]), s2 = __dmul_rn(k, g.sp[2]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        p[r] = __dadd_rn(g.org[r], __dadd_rn(__dadd_rn(__dmul_rn(g.dir[r * 3], s0),
+                                                       __dmul_rn(g.dir[r * 3 + 1], s1)),
+                                             __dmul_rn(g.dir[r * 3 + 2], s2)));
+}
+
+__device__ __forceinline__ void exact_index(const DevGrid& g, const double p[3], double c[3]) {
+    double e0 = __dsub_rn(p[0], g.org[0]), e1 = __dsub_rn(p[1], g.org[1]),
+           e2 = __dsub_rn(p[2], g.org[2]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        c[r] = __dadd_rn(__dadd_rn(__dmul_rn(g.inv[r * 3], e0), __dmul_rn(g.inv[r * 3 + 1], e1)),
+                         __dmul_rn(g.inv[r * 3 + 2], e2));
+}
+
 __device__ __forceinline__ void voxel_ijk(long long l, int nx, int ny, int& i, int& j, int& k) {
     long long q = l / nx;
     i = (int)(l - q * nx);
