@@ -1,0 +1,445 @@
+#!/usr/bin/env python
+"""Benchmark: SyN registrations/hour of the config-2 workload on B200.
+
+Workload ("head-1mm"): the SyN stage of the brain-template-shape pipeline, a seeded
+193 x 229 x 193 float32 phantom pair at 1 mm (nested ellipsoids 0.2/0.5/0.8, +-20 % bias,
+Rician-like noise 0.02; moving = rigid + affine + smooth field of the fixed image), CC radius 4,
+shrink 4/2/1, smoothing sigma 2/1/0 voxels, iterations 70/50/20, gradient step 0.1, update
+variance 3, total variance 0, convergence 1e-6 over a window of 10 (the cohort recipe). The
+linear part of the phantom's map is the SyN stage's initial transform (a converged linear stage).
+
+One step = one batch of `--concurrency` registrations served together (continuous batching: each
+registration on its own stream, admitted as slots free up; `--mode sequential` runs them one at a
+time). `value` is registrations/hour with the images resident in HBM, timed with CUDA events on the
+engines' streams between barriers, max over ranks; `e2e` is the same through the public host API
+(`run_syn`: pinned host images in, AoS float32 fields out, copies inside the timed region).
+Every working set here (fields of 100 MB, images of 34 MB per registration) exceeds the 126 MB L2
+many times over, so no L2 flush is needed between steps.
+
+`--impl reference` times the reference's CPU engine restated as the f64 oracle (the Rust
+reference cannot be built here) on all host cores, on a bounded sample: one SyN iteration per
+level plus the level smoothing, extrapolated to the recipe's iteration counts.
+"""
+import argparse
+import faulthandler
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+faulthandler.enable()
+
+
+def log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+ITERATIONS = [70, 50, 20]
+SHRINK = [4, 2, 1]
+SIGMAS = [2.0, 1.0, 0.0]
+SHAPE = (193, 229, 193)
+METRIC = "SyN registrations/hour (served vs sequential, same CC); p50/p99 latency"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--mode", choices=["served", "sequential"], default="served")
+    p.add_argument("--concurrency", type=int, default=4)
+    p.add_argument("--shape", type=str, default=None, help="override nx,ny,nz (tests)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def recipe():
+    from fastwarp_b200 import SynRecipe
+    return SynRecipe(gradient_step=0.1, update_field_variance=3.0, total_field_variance=0.0,
+                     cc_radius=4, iterations=list(ITERATIONS), shrink_factors=list(SHRINK),
+                     smoothing_sigmas=list(SIGMAS), convergence_threshold=1e-6,
+                     convergence_window=10, channel_weights=[1.0])
+
+
+def dist_init(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def kernel_traffic():
+    """dram bytes per voxel of each kernel from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "kernel_traffic.json")
+    try:
+        return json.load(open(path))
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+
+def run_ours(args, rank, world, local):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from fastwarp_b200 import CudaBackend, run_syn, run_syn_device
+    from fastwarp_b200 import _native as N
+    from fastwarp_b200.phantoms import head_pair
+
+    shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else SHAPE
+    log(f"generating the {shape} phantom pair")
+    g, fixed, mg, moving, initial = head_pair(shape, seed=20_260_910 + 2 + rank)
+    rec = recipe()
+    log("creating contexts")
+    conc = 1 if args.mode == "sequential" else max(1, args.concurrency)
+    backends = [CudaBackend(local) for _ in range(conc)]
+    fimgs = [b.upload_image(g, fixed) for b in backends]
+    mimgs = [b.upload_image(mg, moving) for b in backends]
+    streams = [torch.cuda.ExternalStream(N.lib().fw_ctx_stream(b.ctx), device=local)
+               for b in backends]
+    results = [None] * conc
+    lat = []
+
+    def one(i):
+        t0 = time.perf_counter()
+        w, iw, recs = run_syn_device(backends[i], rec, [fimgs[i]], [mimgs[i]], initial)
+        results[i] = (recs, w, iw)
+        lat.append(time.perf_counter() - t0)
+
+    def batch():
+        if conc == 1:
+            one(0)
+            return
+        th = [threading.Thread(target=one, args=(i,)) for i in range(conc)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+
+    log("warm-up")
+    for _ in range(args.warmup):
+        batch()
+    log("timed steps")
+    lat.clear()
+    for b in backends:
+        b.reset_stats()
+    clocks = Clocks(local)
+    torch.cuda.synchronize(local)
+    barrier(world)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in streams]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in streams]
+    for e, s in zip(starts, streams):
+        e.record(s)
+    clocks.start()
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch()
+    for e, s in zip(ends, streams):
+        e.record(s)
+    torch.cuda.synchronize(local)
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    barrier(world)
+    # device time of the job: first start to last end over the engines' streams
+    t_dev = max(starts[0].elapsed_time(e) for e in ends) / 1000.0
+    t_dev = max(t_dev, max(s.elapsed_time(e) for s, e in zip(starts, ends)) / 1000.0)
+    t_max = max_over_ranks(t_dev, world)
+    regs = args.steps * conc
+    total_regs = sum_over_ranks(regs, world)
+    value = total_regs / t_max * 3600.0
+    launches = sum(b.stats()["kernel_launches"] for b in backends)
+    graphs = sum(b.stats()["graph_launches"] for b in backends)
+    recs0 = results[0][0]
+    iters = len(recs0)
+    final_cc = recs0[-1]["energy"]
+    lat_sorted = sorted(lat)
+
+    def pct(p):
+        return lat_sorted[min(len(lat_sorted) - 1, int(round(p / 100.0 * (len(lat_sorted) - 1))))]
+
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "registrations/hour",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t_max / args.steps * 1000.0, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded phantom pair, no dataset)",
+        "config": {"workload": f"head-1mm SyN stage {shape[0]}x{shape[1]}x{shape[2]} CC r4 "
+                               f"shrink 4/2/1 sigma 2/1/0 iters 70/50/20",
+                   "mode": args.mode, "concurrency": conc,
+                   "registrations_per_step": conc, "iterations_run": iters,
+                   "final_cc_energy": final_cc, "l2_flush": "not needed: working set >> L2",
+                   "parallelism": f"replicas x{world}"},
+        "latency_s": {"p50": round(pct(50), 4), "p95": round(pct(95), 4),
+                      "p99": round(pct(99), 4)},
+        "gpu_launches": int(launches), "graph_launches": int(graphs),
+    }
+    if clk:
+        out["clocks"] = clk
+    # per-kernel roofline at the finest level (CUDA events on the engine stream)
+    b0 = backends[0]
+    ms = (C.c_double * 6)()
+    by = (C.c_double * 6)()
+    fi = fimgs[0]
+    mw = b0.upload_image(g, fixed)  # a second image on the fixed grid
+    N.check(N.lib().fw_time_kernels(b0.ctx, fi.handle, mw.handle, C.c_int32(4), C.c_double(3.0),
+                                    C.c_int32(20), ms, by))
+    names = ["warp", "cc_pair", "smooth", "compose", "inv_measure", "inv_body"]
+    per_iter = {"warp": 2, "cc_pair": 1, "smooth": 2, "compose": 2, "inv_measure": 4,
+                "inv_body": 4}
+    share = {k: ms[i] * per_iter[k] for i, k in enumerate(names)}
+    dom = max(share, key=share.get)
+    di = names.index(dom)
+    peak, src = peaks()
+    achieved = by[di] / (ms[di] / 1000.0) / 1e9
+    traffic = None
+    kt = kernel_traffic()
+    nvox = shape[0] * shape[1] * shape[2]
+    if kt and dom in kt.get("dram_bytes_per_voxel", {}):
+        traffic = kt["dram_bytes_per_voxel"][dom] * nvox
+    out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
+                       "peak": peak, "peak_source": f"{src} hbm_gbs (copy, burst)",
+                       "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                       "algorithmic_bytes_per_launch": by[di], "ms_per_launch": ms[di],
+                       "kernels_ms": {k: round(ms[i], 4) for i, k in enumerate(names)},
+                       "kernels_gbs": {k: round(by[i] / (ms[i] / 1000.0) / 1e9, 1)
+                                       for i, k in enumerate(names)}}
+    # end to end through the public host API (pinned host images in, fields out)
+    if not args.no_e2e:
+        pin_f = torch.from_numpy(fixed).pin_memory()
+        pin_m = torch.from_numpy(moving).pin_memory()
+        fe = pin_f.numpy()
+        me = pin_m.numpy()
+        t0 = time.perf_counter()
+        e_steps = max(1, min(args.steps, 3))
+        res = None
+        for _ in range(e_steps):
+            if conc == 1:
+                res = run_syn(backends[0], rec, g, [fe], mg, [me], initial)
+            else:
+                rs = [None] * conc
+
+                def e2e_one(i):
+                    rs[i] = run_syn(backends[i], rec, g, [fe], mg, [me], initial)
+
+                th = [threading.Thread(target=e2e_one, args=(i,)) for i in range(conc)]
+                for t in th:
+                    t.start()
+                for t in th:
+                    t.join()
+                res = rs[0]
+        te = max_over_ranks(time.perf_counter() - t0, world)
+        e_regs = sum_over_ranks(e_steps * conc, world)
+        out["e2e"] = {"value": round(e_regs / te * 3600.0, 1), "unit": "registrations/hour",
+                      "h2d_bytes_per_step": int((fixed.nbytes + moving.nbytes) * conc),
+                      "d2h_bytes_per_step": int((res.warp.nbytes + res.inverse_warp.nbytes) * conc),
+                      "timing": "wall clock around run_syn calls (host conversion included)"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_sample(g, fixed, mg, moving, initial, rec, shape)
+    for b in backends:
+        b.close()
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# the CPU engine (oracle restatement of the reference's engine="cpu")
+
+def cpu_sample(g, fixed, mg, moving, initial, rec, shape):
+    """One SyN iteration per level and the level smoothing, timed on the oracle and extrapolated
+    to the recipe's iteration counts (the CPU engine's time is linear in the iterations)."""
+    import numpy as np
+
+    import oracle as O
+
+    def og(grid):
+        return O.make_grid(tuple(grid.size), tuple(grid.spacing), tuple(grid.origin),
+                           np.array(grid.direction[:]).reshape(3, 3))
+
+    ofg, omg = og(g), og(mg)
+    oaff = O.make_affine(np.array(initial.matrix[:]).reshape(3, 3), tuple(initial.offset))
+    r = O.syn_recipe(rec.gradient_step, rec.update_field_variance, rec.total_field_variance,
+                     rec.cc_radius, rec.iterations, rec.shrink_factors, rec.smoothing_sigmas,
+                     False, rec.convergence_threshold, rec.convergence_window, [1.0])
+    f64, m64 = fixed.astype(np.float64), moving.astype(np.float64)
+    total = 0.0
+    parts = []
+    t_all = time.perf_counter()
+    for level in range(len(rec.iterations)):
+        lg = O.syn_level_grid(r, ofg, level)
+        t0 = time.perf_counter()
+        s = rec.smoothing_sigmas[level]
+        fs = O.smooth_recursive(ofg, f64, (s, s, s)) if s > 0 else f64
+        ms = O.smooth_recursive(omg, m64, (s, s, s)) if s > 0 else m64
+        t_smooth = time.perf_counter() - t0
+        shp = O.grid_shape(lg) + (3,)
+        state = {k: np.zeros(shp) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+        t0 = time.perf_counter()
+        O.syn_step(r, lg, ofg, [fs], omg, [ms], oaff, state)
+        t_it = time.perf_counter() - t0
+        total += t_smooth + rec.iterations[level] * t_it
+        parts.append(f"L{level} {tuple(lg.size)}: {t_it:.3f}s/iter")
+    sample = time.perf_counter() - t_all
+    return {"value": round(3600.0 / total, 3), "unit": "registrations/hour",
+            "cores": O.num_threads(), "kind": "port",
+            "sample": f"one SyN iteration per level + level smoothing ({sample:.1f}s of CPU work), "
+                      f"extrapolated to 70/50/20 iterations: " + "; ".join(parts),
+            "seconds_per_registration": round(total, 2)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import numpy as np
+
+    from fastwarp_b200.phantoms import head_pair
+    shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else SHAPE
+    g, fixed, mg, moving, initial = head_pair(shape)
+    rec = recipe()
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        cpu_sample(g, fixed, mg, moving, initial, rec, shape)
+    vals = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_sample(g, fixed, mg, moving, initial, rec, shape)
+        vals.append(last["value"])
+    v = statistics.mean(vals)
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3),
+        "unit": "registrations/hour", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(last["seconds_per_registration"] * 1000, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded phantom pair, no dataset)",
+        "config": {"workload": f"head-1mm SyN stage {shape[0]}x{shape[1]}x{shape[2]} CC r4 "
+                               f"shrink 4/2/1 sigma 2/1/0 iters 70/50/20",
+                   "engine": "f64 CPU oracle restating the reference's engine=cpu "
+                             "(the Rust reference cannot be built here)"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "registrations/hour",
+                         "cores": last["cores"], "kind": "port", "sample": last["sample"]},
+        "e2e": {"value": round(v, 3), "unit": "registrations/hour", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args)
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_ours(args, rank, world, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -13,6 +13,7 @@ Errors raise `FastwarpError` with the reference's message text (RegError::Invali
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -60,6 +61,7 @@ class Image:
     def __init__(self, backend, handle):
         self.backend = backend
         self.handle = handle
+        backend._live.add(self)
 
     @property
     def grid(self) -> N.Grid:
@@ -90,6 +92,7 @@ class Field:
     def __init__(self, backend, handle):
         self.backend = backend
         self.handle = handle
+        backend._live.add(self)
 
     @property
     def grid(self) -> N.Grid:
@@ -117,9 +120,13 @@ class CudaBackend:
         check(lib().fw_ctx_create(int(device), C.byref(ctx)))
         self.ctx = ctx
         self.device = device
+        self._live = weakref.WeakSet()  # buffers to free before the context goes
 
     def close(self):
+        """Frees every buffer still alive on this context, then the context itself."""
         if self.ctx:
+            for buf in list(self._live):
+                buf.free()
             lib().fw_ctx_destroy(self.ctx)
             self.ctx = None
 
@@ -343,6 +350,7 @@ class MiLevel:
     def __init__(self, backend: CudaBackend, handle):
         self.backend = backend
         self.handle = handle
+        backend._live.add(self)
 
     def value(self, t: N.LinearTransform) -> float:
         v = C.c_double()

@@ -150,6 +150,8 @@ const char* fw_last_error(void);
 /* Opens a context on `device` with its own stream. Fails on a GPU that is not sm_100.
  * Replaces the device open of the wgpu engine (crates/fastwarp-gpu/src/device.rs). */
 int fw_ctx_create(int device, fw_ctx** out);
+/* Destroys the context and its stream. Free every image, field and MI level made on it first:
+ * their free functions use the context's stream. */
 void fw_ctx_destroy(fw_ctx* ctx);
 /* The context's cudaStream_t, for callers that interleave their own device work. */
 void* fw_ctx_stream(fw_ctx* ctx);
@@ -312,6 +314,15 @@ int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_gr
                const float* const* fixed, const fw_grid* moving_grid, const float* const* moving,
                const fw_affine* initial, float* warp, float* inverse_warp,
                fw_syn_iteration* records, int64_t cap, int64_t* count);
+
+/* ---- profiling (crates/fastwarp-gpu/src/profiler.rs:8-60: per-op device timestamps) ----- */
+
+/* Times `reps` launches of each kernel of one SyN iteration on the grid of `fixed` with CUDA
+ * events on the context's stream: mean ms per launch and algorithmic bytes per launch of
+ * [0] warp, [1] CC pair, [2] Gaussian smoothing + max norm, [3] compose + scale,
+ * [4] inversion measure, [5] inversion body (update + next measurement). */
+int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int32_t radius,
+                    double variance, int32_t reps, double ms[6], double bytes[6]);
 
 /* Sets a flag polled before every level and iteration (SynOptions::cancel, syn.rs:80-85);
  * a run that sees it set fails with FW_ERR_CANCELLED. Pass NULL to clear. */

@@ -238,6 +238,16 @@ def test_recursive_gaussian_matches(backend, name):
     assert worst(got, want) <= 1e-5 * np.abs(want).max()
 
 
+def test_closing_a_context_frees_its_buffers_first():
+    from fastwarp_b200 import CudaBackend
+    b = CudaBackend(0)
+    g = make_grid((9, 8, 7))
+    kept = [b.zero_field(g), b.upload_image(g, np.ones((7, 8, 9), np.float32))]
+    b.close()
+    assert all(x.handle is None for x in kept)
+    del kept  # no use of the destroyed context
+
+
 def test_errors_carry_the_reference_messages(backend):
     g1 = make_grid((8, 8, 8))
     g2 = make_grid((8, 8, 9))
