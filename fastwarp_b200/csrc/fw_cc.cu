@@ -441,3 +441,111 @@ int fw_cc_value_derivative(fw_ctx* ctx, const fw_image* fixed, const fw_image* m
 }
 
 }  // extern "C"
+
+// ---- allocation-free variant of the CC pair ---------------------------------------------------
+//
+// For callers that cannot allocate device memory: code that records its work inside a CUDA
+// stream capture (allocating there breaks the capture), hosts that hand every byte of the GPU to
+// their own pool allocator (a deep-learning framework's caching allocator, a serving process
+// with a fixed HBM budget) and real-time pipelines that plan all memory before they start. The
+// caller passes the images, the two derivative fields and a 3-double result on the device; the
+// kernel's only scratch -- the block partials and the last-block counter -- lives in the
+// file-scope array below, which every GPU that loads this library holds until the process exits.
+
+namespace fw {
+namespace {
+
+struct NoAllocScratch {
+    double partials[3 * FW_NOALLOC_MAX_BLOCKS];
+    unsigned int counter[64];
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_ptr[128] = {};
+
+// The array's device address on `device` (current), looked up once per device: in host code the
+// symbol is only a host-side stand-in, not an address a kernel may use.
+int noalloc_scratch(int device, NoAllocScratch** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (device < 0 || device >= 128) return fail(FW_ERR_INVALID, "cc pair (no alloc): device index out of range");
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_ptr[device] = static_cast<NoAllocScratch*>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return 0;
+}
+
+template <int R, int TY>
+int noalloc_launch(const CcArgs& a0, int num_sms, const float* f, const float* m, float* df,
+                   float* dm, double* result, NoAllocScratch* s, cudaStream_t stream) {
+    using L = Layout<R, TY>;
+    CcArgs a = a0;
+    dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, 1);
+    long long tiles = (long long)grid.x * grid.y;
+    int want = (int)std::max<long long>(1, (4LL * num_sms + tiles - 1) / tiles);
+    int chunk = (a.g.nz + want - 1) / want;
+    chunk = std::max(chunk, std::min(a.g.nz, 4 * R + 4));
+    a.zchunk = chunk;
+    grid.z = (a.g.nz + chunk - 1) / chunk;
+    long long nblocks = (long long)grid.x * grid.y * grid.z;
+    if (nblocks > FW_NOALLOC_MAX_BLOCKS)
+        return fail(FW_ERR_INVALID,
+                    "cc pair (no alloc): the grid needs " + std::to_string(nblocks) +
+                        " thread blocks, more than the " + std::to_string(FW_NOALLOC_MAX_BLOCKS) +
+                        " the static scratch holds (use fw_cc_value_derivative_pair)");
+    // the last-block counter must start at zero whatever the previous call left
+    FW_CUDA(cudaMemsetAsync(s->counter, 0, sizeof(unsigned int), stream));
+    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)L::bytes));
+    k_cc_pair<R, TY><<<grid, L::NT, L::bytes, stream>>>(a, f, m, df, dm, s->partials, s->counter,
+                                                         result, 1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "k_cc_pair (no alloc)");
+    return 0;
+}
+
+}  // namespace
+}  // namespace fw
+
+extern "C" int fw_cc_value_derivative_pair_noalloc(const fw_grid* grid, const float* fixed,
+                                                   const float* moving, int32_t radius,
+                                                   float* d_fixed, float* d_moving,
+                                                   int64_t plane_stride, double* result,
+                                                   void* stream) {
+    FW_CHECK(grid && fixed && moving && d_fixed && d_moving && result, "null argument");
+    HostGrid g;
+    FW_TRY(make_grid(grid, g));
+    FW_CHECK(plane_stride >= g.count(), "cc pair (no alloc): plane stride below the voxel count");
+    int device = 0;
+    FW_CUDA(cudaGetDevice(&device));
+    int num_sms = 0;
+    FW_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    NoAllocScratch* s = nullptr;
+    FW_TRY(noalloc_scratch(device, &s));
+    CcArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = dev_grid(g);
+    a.ps = plane_stride;
+    a.identity_dir = 1;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            if (g.dir[r * 3 + c] != (r == c ? 1.0 : 0.0)) a.identity_dir = 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch (radius) {
+        case 1: return noalloc_launch<1, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 2: return noalloc_launch<2, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 3: return noalloc_launch<3, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 4: return noalloc_launch<4, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 5: return noalloc_launch<5, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 6: return noalloc_launch<6, 4>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 7: return noalloc_launch<7, 4>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 8: return noalloc_launch<8, 4>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        default:
+            return fail(FW_ERR_INVALID, "cc metric: radius must be in 1..=8 (BOX_RADIUS_MAX)");
+    }
+}

@@ -223,6 +223,27 @@ int fw_cc_value_derivative_pair_with_norms(fw_ctx* ctx, const fw_image* fixed,
                                            double values[2], fw_field** d_fixed,
                                            fw_field** d_moving, double norms[2]);
 
+/* No counterpart in the reference. The CC pair above for callers that cannot allocate device
+ * memory: code recording into a CUDA stream capture (an allocation there breaks the capture),
+ * hosts whose own pool allocator owns the GPU's memory (a framework's caching allocator, a server
+ * under a fixed HBM budget) and real-time pipelines that plan all memory up front. This call
+ * allocates nothing and needs no context: `fixed` and `moving` are float32 device images on
+ * `grid`, `d_fixed` / `d_moving` receive the two derivative fields as three float32 planes of
+ * `plane_stride` (>= voxel count) floats, and `result` (device, 3 doubles) receives the value,
+ * sum |d_fixed|^2 and sum |d_moving|^2. It runs asynchronously on `stream` (a cudaStream_t;
+ * NULL = the default stream) of the current device and does not wait for it.
+ * Its scratch is a static device array compiled into the library (block partials for at most
+ * FW_NOALLOC_MAX_BLOCKS thread blocks, about 196 KB, held on every GPU that loads the library
+ * until the process exits); a grid that needs more blocks is rejected with FW_ERR_INVALID. The
+ * first call on a device looks the array's address up, so make it before any stream capture.
+ * All calls share the array: calls whose kernels overlap on the GPU race and must be ordered
+ * on one stream (or otherwise serialised) by the caller. */
+#define FW_NOALLOC_MAX_BLOCKS 8192
+int fw_cc_value_derivative_pair_noalloc(const fw_grid* grid, const float* fixed,
+                                        const float* moving, int32_t radius, float* d_fixed,
+                                        float* d_moving, int64_t plane_stride, double* result,
+                                        void* stream);
+
 /* Backend::smooth_field (backend.rs:249): in place; variance <= 0 leaves the field unchanged. */
 int fw_smooth_field(fw_ctx* ctx, fw_field* field, double variance);
 
