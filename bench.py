@@ -57,7 +57,38 @@ def parse():
     p.add_argument("--shape", type=str, default=None, help="override nx,ny,nz (tests)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--kernels-only", action="store_true",
+                   help="time the kernels of one finest-level iteration only (profiling target)")
+    p.add_argument("--reps", type=int, default=20)
     return p.parse_args()
+
+
+def time_kernels(b, fimg, mimg, reps):
+    """Per-kernel mean ms and algorithmic bytes at the grid of the images (CUDA events on the
+    engine's stream)."""
+    import ctypes as C
+
+    from fastwarp_b200 import _native as N
+    ms = (C.c_double * 6)()
+    by = (C.c_double * 6)()
+    N.check(N.lib().fw_time_kernels(b.ctx, fimg.handle, mimg.handle, C.c_int32(4),
+                                    C.c_double(3.0), C.c_int32(reps), ms, by))
+    names = ["warp", "cc_pair", "smooth", "compose", "inv_measure", "inv_body"]
+    return {k: (ms[i], by[i]) for i, k in enumerate(names)}
+
+
+def run_kernels_only(args, local):
+    from fastwarp_b200 import CudaBackend
+    from fastwarp_b200.phantoms import head_phantom
+    shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else SHAPE
+    from fastwarp_b200 import make_grid
+    g = make_grid(shape)
+    fixed = head_phantom(shape)
+    moving = head_phantom(shape, seed=7)
+    with CudaBackend(local) as b:
+        t = time_kernels(b, b.upload_image(g, fixed), b.upload_image(g, moving), args.reps)
+    return {"kernels": {k: {"ms": round(v[0], 4), "gbs": round(v[1] / (v[0] / 1000) / 1e9, 1)}
+                        for k, v in t.items()}, "shape": shape}
 
 
 def recipe():
@@ -429,7 +460,9 @@ def run_reference(args, rank, world):
 def main():
     args = parse()
     rank, world, local = dist_init(args)
-    if args.impl == "reference":
+    if args.kernels_only:
+        out = run_kernels_only(args, local)
+    elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:
         out = run_ours(args, rank, world, local)

@@ -139,44 +139,66 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
 
     const int kbeg = max(z0 - R, 0);
     const int kend = min(z1 + R, nz);  // slices that exist and are needed (exclusive)
+    // slice-invariant prefetch slots: offset inside a slice (-1 outside the image in x or y)
+    constexpr int PERC = (L::HY * L::HX + L::NT - 1) / L::NT;
+    int src_off[PERC];
+#pragma unroll
+    for (int q = 0; q < PERC; ++q) {
+        int s = tid + q * L::NT;
+        src_off[q] = -1;
+        if (s < L::HY * L::HX) {
+            int hy = s / L::HX, hx = s - hy * L::HX;
+            int gx = x0 - R + hx, gy = y0 - R + hy;
+            if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) src_off[q] = gy * nx + gx;
+        }
+    }
+    float2 pre[PERC];
+    auto fetch = [&](int k) {
+        const long long zoff = (long long)k * sxy;
+#pragma unroll
+        for (int q = 0; q < PERC; ++q)
+            pre[q] = src_off[q] >= 0 ? make_float2(__ldg(fimg + zoff + src_off[q]),
+                                                   __ldg(mimg + zoff + src_off[q]))
+                                     : make_float2(0.0f, 0.0f);
+    };
+    if (kbeg < kend) fetch(kbeg);
     for (int k = kbeg; k < z1 + R; ++k) {
         __syncthreads();  // previous slice's readers are done with the slot and the x sums
         double P[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         const bool have = k < kend;
         if (have) {
             float2* slot = in + (k % L::D) * (L::HY * L::HX);
-            const long long zoff = (long long)k * sxy;
-            for (int s = tid; s < L::HY * L::HX; s += L::NT) {
-                int hy = s / L::HX, hx = s - hy * L::HX;
-                int gx = x0 - R + hx, gy = y0 - R + hy;
-                float2 v = make_float2(0.0f, 0.0f);
-                if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) {
-                    long long o = zoff + (long long)gy * nx + gx;
-                    v = make_float2(__ldg(fimg + o), __ldg(mimg + o));
-                }
-                slot[s] = v;
+#pragma unroll
+            for (int q = 0; q < PERC; ++q) {
+                int s = tid + q * L::NT;
+                if (s < L::HY * L::HX) slot[s] = pre[q];
             }
             __syncthreads();
-            // x pass: every (halo row, output column) pair
-            for (int s = tid; s < L::HY * TX; s += L::NT) {
-                int hy = s / TX, cx = s - hy * TX;
-                const float2* row = slot + hy * L::HX + cx;
-                double q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0;
+            if (k + 1 < kend) fetch(k + 1);  // in flight while this slice is summed
+            // x pass: each item makes the sums of two adjacent columns from one window of
+            // 2r + 2 voxels (the 2r in the middle are shared)
+            for (int s = tid; s < L::HY * (TX / 2); s += L::NT) {
+                int hy = s / (TX / 2), cp = s - hy * (TX / 2);
+                const float2* row = slot + hy * L::HX + 2 * cp;
+                double c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0;
 #pragma unroll
-                for (int t = 0; t <= 2 * R; ++t) {
+                for (int t = 1; t <= 2 * R; ++t) {
                     float2 v = row[t];
                     double f = v.x, m = v.y;
-                    q0 += f;
-                    q1 += m;
-                    q2 += f * f;
-                    q3 += m * m;
-                    q4 += f * m;
+                    c0 += f;
+                    c1 += m;
+                    c2 += f * f;
+                    c3 += m * m;
+                    c4 += f * m;
                 }
-                xs[(0 * L::HY + hy) * TX + cx] = q0;
-                xs[(1 * L::HY + hy) * TX + cx] = q1;
-                xs[(2 * L::HY + hy) * TX + cx] = q2;
-                xs[(3 * L::HY + hy) * TX + cx] = q3;
-                xs[(4 * L::HY + hy) * TX + cx] = q4;
+                float2 va = row[0], vb = row[2 * R + 1];
+                double fa = va.x, ma = va.y, fb = vb.x, mb = vb.y;
+                double* o = xs + hy * TX + 2 * cp;
+                *reinterpret_cast<double2*>(o + 0 * L::HY * TX) = make_double2(c0 + fa, c0 + fb);
+                *reinterpret_cast<double2*>(o + 1 * L::HY * TX) = make_double2(c1 + ma, c1 + mb);
+                *reinterpret_cast<double2*>(o + 2 * L::HY * TX) = make_double2(c2 + fa * fa, c2 + fb * fb);
+                *reinterpret_cast<double2*>(o + 3 * L::HY * TX) = make_double2(c3 + ma * ma, c3 + mb * mb);
+                *reinterpret_cast<double2*>(o + 4 * L::HY * TX) = make_double2(c4 + fa * ma, c4 + fb * mb);
             }
             __syncthreads();
             // y pass for the thread's own column

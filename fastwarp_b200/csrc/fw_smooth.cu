@@ -196,6 +196,163 @@ __global__ void __launch_bounds__(SNT) k_smooth(SmoothArgs a, const float* __res
     }
 }
 
+// Fixed-radius variant (the same radius on the three axes, the usual case): taps unrolled from
+// the parameter bank, the x pass vectorised (each item reads a 4 + 2r window as float4 and makes
+// four outputs), the z window kept as a register ring shifted once per slice, and the next slice
+// prefetched into registers while the current one is filtered. Two 256-thread CTAs per SM.
+constexpr int RTX = 32;
+constexpr int RTY = 8;
+constexpr int RNT = RTX * RTY;
+
+template <int R>
+__global__ void __launch_bounds__(RNT, 2) k_smooth_r(SmoothArgs a, const float* __restrict__ in,
+                                                     float* __restrict__ out,
+                                                     unsigned int* __restrict__ max_bits) {
+    constexpr int HX = RTX + 2 * R, HY = RTY + 2 * R, W = 2 * R + 1;
+    constexpr int HXP = (HX + 3) & ~3;             // row stride: rows start on 16 bytes
+    constexpr int TILE = HY * HXP;
+    constexpr int NV = (4 + 2 * R + 3) / 4;        // float4 loads per x-pass window
+    constexpr int PER = (3 * HY * HX + RNT - 1) / RNT;  // prefetched values per thread
+    __shared__ __align__(16) float tile[3 * TILE + 4 * NV];
+    __shared__ __align__(16) float xs[3 * HY * RTX];
+    const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
+    const int tid = threadIdx.x, tx = tid % RTX, ty = tid / RTX;
+    const int x0 = blockIdx.x * RTX, y0 = blockIdx.y * RTY;
+    const int z0 = blockIdx.z * a.zchunk, z1 = min(z0 + a.zchunk, nz);
+    const int x = x0 + tx, y = y0 + ty;
+    const bool own = x < nx && y < ny;
+    const long long sxy = (long long)nx * ny;
+    const float* taps = a.tx_;  // identical on the three axes here
+    float ring[W][3];
+#pragma unroll
+    for (int t = 0; t < W; ++t) ring[t][0] = ring[t][1] = ring[t][2] = 0.0f;
+    float pre[PER];
+    // the slice-invariant part of every prefetch: offset in the slice (clamped x, y; component
+    // plane) and destination in the tile (-1: no value for this thread)
+    int src_off[PER], dst_off[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        int s = tid + q * RNT;
+        src_off[q] = 0;
+        dst_off[q] = -1;
+        if (s < 3 * HY * HX) {
+            int c = s / (HY * HX), rr = s - c * (HY * HX);
+            int hy = rr / HX, hx = rr - hy * HX;
+            int gx = min(max(x0 - R + hx, 0), nx - 1);
+            int gy = min(max(y0 - R + hy, 0), ny - 1);
+            src_off[q] = gy * nx + gx + c * (int)a.ps_in;
+            dst_off[q] = c * TILE + hy * HXP + hx;
+        }
+    }
+    auto fetch = [&](int k) {
+        const int kz = min(max(k, 0), nz - 1);  // edge replication along z
+        const float* base = in + (long long)kz * sxy;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) pre[q] = dst_off[q] >= 0 ? __ldg(base + src_off[q]) : 0.0f;
+    };
+    float vmax = 0.0f;
+    const float isx = (float)(1.0 / a.g.sp[0]), isy = (float)(1.0 / a.g.sp[1]),
+                isz = (float)(1.0 / a.g.sp[2]);
+    int k = z0 - R;
+    fetch(k);
+    for (; k < z1 + R; ++k) {
+        __syncthreads();  // the previous slice's passes are done with tile and xs
+#pragma unroll
+        for (int q = 0; q < PER; ++q)
+            if (dst_off[q] >= 0) tile[dst_off[q]] = pre[q];
+        __syncthreads();
+        if (k + 1 < z1 + R) fetch(k + 1);  // in flight while this slice is filtered
+        // x pass: (component, halo row, group of four output columns)
+        for (int s = tid; s < 3 * HY * (RTX / 4); s += RNT) {
+            int c = s / (HY * (RTX / 4)), rr = s - c * (HY * (RTX / 4));
+            int hy = rr / (RTX / 4), g4 = rr - hy * (RTX / 4);
+            const float4* row = reinterpret_cast<const float4*>(tile + c * TILE + hy * HXP) + g4;
+            float win[4 * NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                float4 q4 = row[v];
+                win[4 * v] = q4.x;
+                win[4 * v + 1] = q4.y;
+                win[4 * v + 2] = q4.z;
+                win[4 * v + 3] = q4.w;
+            }
+            float4 o;
+            float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f, acc3 = 0.0f;
+#pragma unroll
+            for (int t = 0; t < W; ++t) {
+                const float w = taps[t];
+                acc0 = fmaf(w, win[t], acc0);
+                acc1 = fmaf(w, win[t + 1], acc1);
+                acc2 = fmaf(w, win[t + 2], acc2);
+                acc3 = fmaf(w, win[t + 3], acc3);
+            }
+            o.x = acc0;
+            o.y = acc1;
+            o.z = acc2;
+            o.w = acc3;
+            reinterpret_cast<float4*>(xs + c * HY * RTX + hy * RTX)[g4] = o;
+        }
+        __syncthreads();
+        // y pass for the thread's own column, then shift it into the z ring
+#pragma unroll
+        for (int t = 0; t < W - 1; ++t) {
+            ring[t][0] = ring[t + 1][0];
+            ring[t][1] = ring[t + 1][1];
+            ring[t][2] = ring[t + 1][2];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float* col = xs + c * HY * RTX + ty * RTX + tx;
+            float acc = 0.0f;
+#pragma unroll
+            for (int t = 0; t < W; ++t) acc = fmaf(taps[t], col[t * RTX], acc);
+            ring[W - 1][c] = acc;
+        }
+        const int z = k - R;
+        if (z < z0 || !own) continue;
+        float v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int t = 0; t < W; ++t) acc = fmaf(taps[t], ring[t][c], acc);
+            v[c] = acc;
+        }
+        const long long l = (long long)z * sxy + (long long)y * nx + x;
+        const bool face = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
+        float o[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float orig = a.w2 != 0.0f ? __ldg(in + l + c * a.ps_in) : 0.0f;
+            o[c] = face ? 0.0f : (a.w2 != 0.0f ? v[c] * a.w1 + orig * a.w2 : v[c]);
+            out[l + c * a.ps_out] = o[c];
+        }
+        if (max_bits) {
+            float px = o[0] * isx, py = o[1] * isy, pz = o[2] * isz;
+            vmax = __int_as_float(max(__float_as_int(vmax),
+                                      __float_as_int(nan_canon(sqrtf(px * px + py * py + pz * pz)))));
+        }
+    }
+    if (max_bits) {
+        vmax = warp_max_f(vmax);
+        if ((tid & 31) == 0 && vmax > 0.0f) atomicMax(max_bits, __float_as_uint(vmax));
+    }
+}
+
+template <int R>
+int launch_smooth_r(fw_ctx* ctx, SmoothArgs a, const fw_field* in, fw_field* out,
+                    unsigned int* d_max_bits) {
+    dim3 grid((a.g.nx + RTX - 1) / RTX, (a.g.ny + RTY - 1) / RTY, 1);
+    long long tiles = (long long)grid.x * grid.y;
+    int want = (int)std::max<long long>(1, (3LL * ctx->num_sms + tiles - 1) / tiles);
+    int chunk = (a.g.nz + want - 1) / want;
+    chunk = std::max(chunk, std::min(a.g.nz, 4 * R + 8));
+    a.zchunk = chunk;
+    grid.z = (a.g.nz + chunk - 1) / chunk;
+    k_smooth_r<R><<<grid, RNT, 0, ctx->stream>>>(a, in->d, out->d, d_max_bits);
+    return check_launch(ctx, "k_smooth_r");
+}
+
 // ---- Deriche recursive Gaussian (pyramid.rs:186-300, 418-427) --------------------------------
 
 struct Deriche {
@@ -374,6 +531,26 @@ int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double varianc
     double w1 = variance < 0.5 ? 1.0 - variance / 0.5 : 1.0;
     a.w1 = (float)w1;
     a.w2 = (float)(1.0 - w1);
+    bool same = r[0] == r[1] && r[1] == r[2] && 3 * in->ps < 2147483647LL;  // int32 offsets
+    for (int t = 0; same && t <= 2 * r[0]; ++t)
+        same = a.tx_[t] == a.ty_[t] && a.ty_[t] == a.tz_[t];
+    if (same) {
+        switch (r[0]) {
+            case 1: return launch_smooth_r<1>(ctx, a, in, out, d_max_bits);
+            case 2: return launch_smooth_r<2>(ctx, a, in, out, d_max_bits);
+            case 3: return launch_smooth_r<3>(ctx, a, in, out, d_max_bits);
+            case 4: return launch_smooth_r<4>(ctx, a, in, out, d_max_bits);
+            case 5: return launch_smooth_r<5>(ctx, a, in, out, d_max_bits);
+            case 6: return launch_smooth_r<6>(ctx, a, in, out, d_max_bits);
+            case 7: return launch_smooth_r<7>(ctx, a, in, out, d_max_bits);
+            case 8: return launch_smooth_r<8>(ctx, a, in, out, d_max_bits);
+            case 9: return launch_smooth_r<9>(ctx, a, in, out, d_max_bits);
+            case 10: return launch_smooth_r<10>(ctx, a, in, out, d_max_bits);
+            case 11: return launch_smooth_r<11>(ctx, a, in, out, d_max_bits);
+            case 12: return launch_smooth_r<12>(ctx, a, in, out, d_max_bits);
+            default: break;
+        }
+    }
     dim3 grid((a.g.nx + STX - 1) / STX, (a.g.ny + STY - 1) / STY, 1);
     long long tiles = (long long)grid.x * grid.y;
     int want = (int)std::max<long long>(1, (4LL * ctx->num_sms + tiles - 1) / tiles);
