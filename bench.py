@@ -215,85 +215,63 @@ def kernel_traffic():
 # our arm
 
 def run_ours(args, rank, world, local):
-    import ctypes as C
-
     import numpy as np
     import torch
 
-    from fastwarp_b200 import CudaBackend, run_syn, run_syn_device
-    from fastwarp_b200 import _native as N
+    from fastwarp_b200 import CudaBackend
     from fastwarp_b200.phantoms import head_pair
+    from fastwarp_b200.serve import Server
 
     shape = tuple(int(x) for x in args.shape.split(",")) if args.shape else SHAPE
     log(f"generating the {shape} phantom pair")
     g, fixed, mg, moving, initial = head_pair(shape, seed=20_260_910 + 2 + rank)
     rec = recipe()
-    log("creating contexts")
     conc = 1 if args.mode == "sequential" else max(1, args.concurrency)
-    backends = [CudaBackend(local) for _ in range(conc)]
-    fimgs = [b.upload_image(g, fixed) for b in backends]
-    mimgs = [b.upload_image(mg, moving) for b in backends]
-    streams = [torch.cuda.ExternalStream(N.lib().fw_ctx_stream(b.ctx), device=local)
-               for b in backends]
-    results = [None] * conc
-    lat = []
+    b = CudaBackend(local)
+    fi, mi = b.upload_image(g, fixed), b.upload_image(mg, moving)
 
-    def one(i):
-        t0 = time.perf_counter()
-        w, iw, recs = run_syn_device(backends[i], rec, [fimgs[i]], [mimgs[i]], initial)
-        results[i] = (recs, w, iw)
-        lat.append(time.perf_counter() - t0)
+    def batch(server, n, device=True):
+        if device:
+            ts = [server.submit(rec, g, [fi], mg, [mi], initial, keep_on_device=True)
+                  for _ in range(n)]
+        else:
+            ts = [server.submit(rec, g, [fixed], mg, [moving], initial) for _ in range(n)]
+        outs = [server.wait(t) for t in ts]
+        for o in outs:
+            if o["status"] != 0:
+                raise RuntimeError(o["error"])
+            Server.free_device_fields(o)
+        return outs
 
-    def batch():
-        if conc == 1:
-            one(0)
-            return
-        th = [threading.Thread(target=one, args=(i,)) for i in range(conc)]
-        for t in th:
-            t.start()
-        for t in th:
-            t.join()
+    def span_ms(outs):
+        return max(o["device_end_ms"] for o in outs) - min(o["device_start_ms"] for o in outs)
 
-    log("warm-up")
+    log(f"server with {conc} slots; warm-up")
+    srv = Server(local, slots=conc)
     for _ in range(args.warmup):
-        batch()
-    log("timed steps")
-    lat.clear()
-    for b in backends:
-        b.reset_stats()
+        batch(srv, conc)
+    launches0 = srv.stats()["kernel_launches"]
+    graphs0 = srv.stats()["graph_launches"]
+    n = args.steps * conc
+    log(f"timed: {n} registrations")
     clocks = Clocks(local)
     torch.cuda.synchronize(local)
     barrier(world)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in streams]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in streams]
-    for e, s in zip(starts, streams):
-        e.record(s)
     clocks.start()
-    wall0 = time.perf_counter()
-    for _ in range(args.steps):
-        batch()
-    for e, s in zip(ends, streams):
-        e.record(s)
-    torch.cuda.synchronize(local)
-    wall = time.perf_counter() - wall0
+    srv.mark()
+    outs = batch(srv, n)
     clk = clocks.stop()
     barrier(world)
-    # device time of the job: first start to last end over the engines' streams
-    t_dev = max(starts[0].elapsed_time(e) for e in ends) / 1000.0
-    t_dev = max(t_dev, max(s.elapsed_time(e) for s, e in zip(starts, ends)) / 1000.0)
+    t_dev = span_ms(outs) / 1000.0
     t_max = max_over_ranks(t_dev, world)
-    regs = args.steps * conc
-    total_regs = sum_over_ranks(regs, world)
-    value = total_regs / t_max * 3600.0
-    launches = sum(b.stats()["kernel_launches"] for b in backends)
-    graphs = sum(b.stats()["graph_launches"] for b in backends)
-    recs0 = results[0][0]
-    iters = len(recs0)
-    final_cc = recs0[-1]["energy"]
-    lat_sorted = sorted(lat)
+    value = sum_over_ranks(n, world) / t_max * 3600.0
+    st = srv.stats()
+    launches = st["kernel_launches"] - launches0
+    graphs = st["graph_launches"] - graphs0
+    lat = sorted(o["queued_s"] + o["run_s"] for o in outs)
 
     def pct(p):
-        return lat_sorted[min(len(lat_sorted) - 1, int(round(p / 100.0 * (len(lat_sorted) - 1))))]
+        return lat[min(len(lat) - 1, int(round(p / 100.0 * (len(lat) - 1))))]
 
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "registrations/hour",
@@ -303,9 +281,12 @@ def run_ours(args, rank, world, local):
         "data": "synthetic (seeded phantom pair, no dataset)",
         "config": {"workload": f"head-1mm SyN stage {shape[0]}x{shape[1]}x{shape[2]} CC r4 "
                                f"shrink 4/2/1 sigma 2/1/0 iters 70/50/20",
-                   "mode": args.mode, "concurrency": conc,
-                   "registrations_per_step": conc, "iterations_run": iters,
-                   "final_cc_energy": final_cc, "l2_flush": "not needed: working set >> L2",
+                   "mode": args.mode, "slots": conc, "registrations_per_step": conc,
+                   "iterations_run": outs[0]["iterations"],
+                   "final_cc_energy": outs[0]["final_energy"],
+                   "device_bytes_per_registration": outs[0]["device_bytes"],
+                   "peak_reserved_bytes": st["peak_reserved_bytes"],
+                   "l2_flush": "not needed: working set >> L2",
                    "parallelism": f"replicas x{world}"},
         "latency_s": {"p50": round(pct(50), 4), "p95": round(pct(95), 4),
                       "p99": round(pct(99), 4)},
@@ -313,22 +294,30 @@ def run_ours(args, rank, world, local):
     }
     if clk:
         out["clocks"] = clk
+    srv.close()
+    # the same registrations one at a time on the same kernels (served vs sequential)
+    if conc > 1:
+        log("sequential comparison")
+        seq = Server(local, slots=1)
+        batch(seq, 1)
+        seq.mark()
+        so = batch(seq, max(2, min(n, 2 * conc)))
+        t_seq = span_ms(so) / 1000.0
+        seq_value = len(so) / t_seq * 3600.0
+        seq.close()
+        out["config"]["sequential_value"] = round(seq_value, 1)
+        out["config"]["served_over_sequential"] = round(value / world / seq_value, 3)
+        out["config"]["sequential_latency_s"] = round(statistics.median(
+            o["run_s"] for o in so), 4)
     # per-kernel roofline at the finest level (CUDA events on the engine stream)
-    b0 = backends[0]
-    ms = (C.c_double * 6)()
-    by = (C.c_double * 6)()
-    fi = fimgs[0]
-    mw = b0.upload_image(g, fixed)  # a second image on the fixed grid
-    N.check(N.lib().fw_time_kernels(b0.ctx, fi.handle, mw.handle, C.c_int32(4), C.c_double(3.0),
-                                    C.c_int32(20), ms, by))
-    names = ["warp", "cc_pair", "smooth", "compose", "inv_measure", "inv_body"]
+    log("kernel timing")
+    t = time_kernels(b, fi, b.upload_image(g, fixed), 20)
     per_iter = {"warp": 2, "cc_pair": 1, "smooth": 2, "compose": 2, "inv_measure": 4,
                 "inv_body": 4}
-    share = {k: ms[i] * per_iter[k] for i, k in enumerate(names)}
-    dom = max(share, key=share.get)
-    di = names.index(dom)
+    dom = max(per_iter, key=lambda k: t[k][0] * per_iter[k])
+    ms, by = t[dom]
     peak, src = peaks()
-    achieved = by[di] / (ms[di] / 1000.0) / 1e9
+    achieved = by / (ms / 1000.0) / 1e9
     traffic = None
     kt = kernel_traffic()
     nvox = shape[0] * shape[1] * shape[2]
@@ -337,44 +326,31 @@ def run_ours(args, rank, world, local):
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1),
                        "peak": peak, "peak_source": f"{src} hbm_gbs (copy, burst)",
                        "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                       "algorithmic_bytes_per_launch": by[di], "ms_per_launch": ms[di],
-                       "kernels_ms": {k: round(ms[i], 4) for i, k in enumerate(names)},
-                       "kernels_gbs": {k: round(by[i] / (ms[i] / 1000.0) / 1e9, 1)
-                                       for i, k in enumerate(names)}}
-    # end to end through the public host API (pinned host images in, fields out)
+                       "algorithmic_bytes_per_launch": by, "ms_per_launch": round(ms, 4),
+                       "kernels_ms": {k: round(v[0], 4) for k, v in t.items()},
+                       "kernels_gbs": {k: round(v[1] / (v[0] / 1000.0) / 1e9, 1)
+                                       for k, v in t.items()}}
+    # end to end through the public host API: host images in (copied at submit), AoS float32
+    # fields out; wall clock from the first submit to the last result
     if not args.no_e2e:
-        pin_f = torch.from_numpy(fixed).pin_memory()
-        pin_m = torch.from_numpy(moving).pin_memory()
-        fe = pin_f.numpy()
-        me = pin_m.numpy()
+        log("end to end")
+        e2e = Server(local, slots=conc)
+        batch(e2e, conc, device=False)
+        ne = max(conc, min(n, 2 * conc))
         t0 = time.perf_counter()
-        e_steps = max(1, min(args.steps, 3))
-        res = None
-        for _ in range(e_steps):
-            if conc == 1:
-                res = run_syn(backends[0], rec, g, [fe], mg, [me], initial)
-            else:
-                rs = [None] * conc
-
-                def e2e_one(i):
-                    rs[i] = run_syn(backends[i], rec, g, [fe], mg, [me], initial)
-
-                th = [threading.Thread(target=e2e_one, args=(i,)) for i in range(conc)]
-                for t in th:
-                    t.start()
-                for t in th:
-                    t.join()
-                res = rs[0]
+        eo = batch(e2e, ne, device=False)
         te = max_over_ranks(time.perf_counter() - t0, world)
-        e_regs = sum_over_ranks(e_steps * conc, world)
-        out["e2e"] = {"value": round(e_regs / te * 3600.0, 1), "unit": "registrations/hour",
+        e2e.close()
+        shape3 = (rec_grid_voxels := int(np.prod([eo[0]["grid"].size[a] for a in range(3)])))
+        out["e2e"] = {"value": round(sum_over_ranks(ne, world) / te * 3600.0, 1),
+                      "unit": "registrations/hour",
                       "h2d_bytes_per_step": int((fixed.nbytes + moving.nbytes) * conc),
-                      "d2h_bytes_per_step": int((res.warp.nbytes + res.inverse_warp.nbytes) * conc),
-                      "timing": "wall clock around run_syn calls (host conversion included)"}
+                      "d2h_bytes_per_step": int(2 * 12 * shape3 * conc),
+                      "timing": "wall clock, first submit to last result (host copies included)"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        log("CPU baseline sample")
         out["cpu_baseline"] = cpu_sample(g, fixed, mg, moving, initial, rec, shape)
-    for b in backends:
-        b.close()
+    b.close()
     return out
 
 

@@ -1,0 +1,394 @@
+// fw_serve.cu -- the continuous-batching registration server (include/fastwarp_serve.h).
+//
+// N execution slots, each a thread with its own context (stream, scratch). A FIFO queue of
+// requests; a slot takes the first queued request whose device-memory estimate fits in what is
+// left of the HBM budget (smaller requests may pass a large one that does not fit yet), runs the
+// whole SyN stage (one CUDA graph per level), releases the memory, and takes the next. Several
+// slots run at once, so the latency-bound coarse levels of one registration overlap the
+// bandwidth-bound fine levels of another.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/fastwarp_serve.h"
+#include "fw_internal.cuh"
+
+namespace fw {
+int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
+                   const fw_image* const* moving, const fw_affine* initial, fw_field** warp,
+                   fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
+                   int64_t* count);
+}
+
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+struct Job {
+    uint64_t ticket = 0;
+    fw_syn_request req{};
+    std::vector<std::vector<float>> fixed_host, moving_host;
+    std::vector<const fw_image*> fixed_dev, moving_dev;
+    uint64_t bytes = 0;
+    Clock::time_point submitted;
+    fw_syn_result result{};
+    bool done = false;
+    bool taken = false;
+};
+
+int estimate(const fw_syn_request* q, uint64_t* out) {
+    using namespace fw;
+    HostGrid fg, mg;
+    FW_TRY(make_grid(&q->fixed_grid, fg));
+    FW_TRY(make_grid(&q->moving_grid, mg));
+    const fw_syn_recipe* r = &q->recipe;
+    FW_CHECK(r->levels >= 1 && r->levels <= FW_MAX_LEVELS, "serve: recipe has no levels");
+    FW_CHECK(r->channels >= 1 && r->channels <= FW_MAX_CHANNELS, "serve: 1..=4 channels");
+    fw_grid last;
+    FW_TRY(fw_syn_level_grid(r, &q->fixed_grid, r->levels - 1, &last));
+    int64_t n = 1, nprev = 0;
+    for (int a = 0; a < 3; ++a) n *= last.size[a];
+    if (r->levels > 1) {
+        fw_grid prev;
+        FW_TRY(fw_syn_level_grid(r, &q->fixed_grid, r->levels - 2, &prev));
+        nprev = prev.size[0] * prev.size[1] * prev.size[2];
+    }
+    const uint64_t C = (uint64_t)r->channels;
+    const uint64_t nf = (uint64_t)fg.count(), nm = (uint64_t)mg.count();
+    const uint64_t ps = (uint64_t)plane_stride(n), psp = (uint64_t)plane_stride(nprev);
+    bool smooth = false;
+    for (int l = 0; l < r->levels; ++l) smooth = smooth || r->smoothing_sigmas[l] > 0.0;
+    uint64_t b = 0;
+    if (q->fixed == nullptr) b += 0;
+    else b += 4 * C * (nf + nm);                       // uploaded inputs
+    if (smooth) b += 4 * C * (nf + nm) + 24 * std::max(nf, nm);  // smoothed copies + Deriche temp
+    int fields = 4 + 2 + (r->update_field_variance > 0 ? 2 : 0) + (C > 1 ? 2 : 0) +
+                 (r->total_field_variance > 0 ? 1 : 0) + 2 /* outputs */;
+    b += 12 * ps * (uint64_t)fields;
+    b += 4 * (uint64_t)n * 2 * C;                      // warped images
+    b += 12 * psp * 4;                                 // state of the previous level at a transition
+    b += 2u << 20;                                     // records and scalars
+    *out = b;
+    return 0;
+}
+
+}  // namespace
+
+struct fw_server {
+    int device = 0;
+    uint64_t budget = 0;
+    int slots = 0;
+    std::vector<fw_ctx*> ctxs;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Job*> queue;
+    std::map<uint64_t, Job*> jobs;
+    uint64_t next_ticket = 1;
+    uint64_t reserved = 0, peak = 0;
+    uint64_t submitted = 0, completed = 0, failed = 0, active = 0;
+    bool stopping = false;
+    cudaEvent_t epoch = nullptr;
+    bool epoch_set = false;
+};
+
+namespace {
+
+void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
+    using namespace fw;
+    fw_syn_result& res = j->result;
+    res.tag = j->req.tag;
+    res.device_bytes = j->bytes;
+    const fw_syn_request& q = j->req;
+    const int C = q.recipe.channels;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ctx->stream);
+    std::vector<fw_image*> up;
+    std::vector<const fw_image*> fi(C), mi(C);
+    int rc = 0;
+    if (!j->fixed_dev.empty()) {
+        for (int c = 0; c < C; ++c) {
+            fi[c] = j->fixed_dev[c];
+            mi[c] = j->moving_dev[c];
+        }
+    } else {
+        for (int c = 0; c < C && !rc; ++c) {
+            fw_image *a = nullptr, *b = nullptr;
+            rc = fw_image_upload_f32(ctx, &q.fixed_grid, j->fixed_host[c].data(), &a);
+            if (!rc) up.push_back(a);
+            if (!rc) rc = fw_image_upload_f32(ctx, &q.moving_grid, j->moving_host[c].data(), &b);
+            if (!rc) up.push_back(b);
+            fi[c] = a;
+            mi[c] = b;
+        }
+        j->fixed_host.clear();
+        j->moving_host.clear();
+    }
+    int64_t cap = 0;
+    for (int l = 0; l < q.recipe.levels; ++l) cap += q.recipe.iterations[l];
+    std::vector<fw_syn_iteration> recs((size_t)std::max<int64_t>(cap, 1));
+    int64_t count = 0;
+    fw_field *w = nullptr, *iw = nullptr;
+    if (!rc)
+        rc = syn_run_device(ctx, &q.recipe, fi.data(), mi.data(), q.has_initial ? &q.initial : nullptr,
+                            &w, &iw, recs.data(), (int64_t)recs.size(), &count);
+    for (auto* im : up) fw_image_free(im);
+    if (!rc) {
+        res.iterations = count;
+        res.final_energy = count > 0 ? recs[(size_t)std::min<int64_t>(count, cap) - 1].energy : 0.0;
+        res.grid = to_c(w->grid);
+        if (q.keep_on_device) {
+            res.warp_dev = w;
+            res.inverse_dev = iw;
+            w = iw = nullptr;
+        } else {
+            size_t n3 = 3 * (size_t)w->grid.count();
+            res.warp = static_cast<float*>(std::malloc(n3 * sizeof(float)));
+            res.inverse_warp = static_cast<float*>(std::malloc(n3 * sizeof(float)));
+            if (!res.warp || !res.inverse_warp) rc = fail(FW_ERR_MEMORY, "serve: host allocation failed");
+            if (!rc) rc = fw_field_download_f32(ctx, w, res.warp);
+            if (!rc) rc = fw_field_download_f32(ctx, iw, res.inverse_warp);
+        }
+    }
+    fw_field_free(w);
+    fw_field_free(iw);
+    cudaEventRecord(e1, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->epoch_set) {
+            float a = 0.0f, b = 0.0f;
+            cudaEventElapsedTime(&a, s->epoch, e0);
+            cudaEventElapsedTime(&b, s->epoch, e1);
+            res.device_start_ms = a;
+            res.device_end_ms = b;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    res.status = rc;
+    if (rc) {
+        std::strncpy(res.error, fw_last_error(), sizeof(res.error) - 1);
+        std::free(res.warp);
+        std::free(res.inverse_warp);
+        res.warp = res.inverse_warp = nullptr;
+        fw_field_free(res.warp_dev);
+        fw_field_free(res.inverse_dev);
+        res.warp_dev = res.inverse_dev = nullptr;
+    }
+}
+
+void worker(fw_server* s, int slot) {
+    cudaSetDevice(s->device);
+    fw_ctx* ctx = s->ctxs[slot];
+    for (;;) {
+        Job* j = nullptr;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            for (;;) {
+                for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+                    if (s->reserved + (*it)->bytes <= s->budget) {
+                        j = *it;
+                        s->queue.erase(it);
+                        break;
+                    }
+                }
+                if (j || (s->stopping && s->queue.empty())) break;
+                s->cv_work.wait(lock);
+            }
+            if (!j) return;
+            s->reserved += j->bytes;
+            s->peak = std::max(s->peak, s->reserved);
+            s->active++;
+        }
+        auto t0 = Clock::now();
+        j->result.queued_s = std::chrono::duration<double>(t0 - j->submitted).count();
+        run_job(s, ctx, j);
+        j->result.run_s = std::chrono::duration<double>(Clock::now() - t0).count();
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            s->reserved -= j->bytes;
+            s->active--;
+            if (j->result.status) s->failed++;
+            else s->completed++;
+            j->done = true;
+        }
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();
+    }
+}
+
+}  // namespace
+
+using namespace fw;
+
+extern "C" {
+
+int fw_server_estimate(const fw_syn_request* req, uint64_t* bytes) {
+    FW_CHECK(req && bytes, "null argument");
+    return estimate(req, bytes);
+}
+
+int fw_server_create(int device, uint64_t hbm_budget, int32_t slots, fw_server** out) {
+    FW_CHECK(out && slots >= 1 && slots <= 64, "serve: 1..=64 slots");
+    *out = nullptr;
+    fw_server* s = new fw_server();
+    s->device = device;
+    s->slots = slots;
+    for (int i = 0; i < slots; ++i) {
+        fw_ctx* c = nullptr;
+        int rc = fw_ctx_create(device, &c);
+        if (!rc) rc = ensure_scratch(c, SLOT_PARTIALS + (size_t)(1 << 20));
+        if (rc) {
+            if (c) fw_ctx_destroy(c);
+            for (auto* x : s->ctxs) fw_ctx_destroy(x);
+            delete s;
+            return rc;
+        }
+        s->ctxs.push_back(c);
+    }
+    if (hbm_budget == 0) {
+        size_t f = 0, t = 0;
+        cudaMemGetInfo(&f, &t);
+        hbm_budget = (uint64_t)(0.9 * (double)f);
+    }
+    s->budget = hbm_budget;
+    cudaEventCreate(&s->epoch);
+    for (int i = 0; i < slots; ++i) s->threads.emplace_back(worker, s, i);
+    *out = s;
+    return 0;
+}
+
+int fw_server_submit(fw_server* s, const fw_syn_request* req, uint64_t* ticket) {
+    FW_CHECK(s && req && ticket, "null argument");
+    const int C = req->recipe.channels;
+    FW_CHECK(C >= 1 && C <= FW_MAX_CHANNELS, "serve: 1..=4 channels");
+    bool host = req->fixed && req->moving;
+    bool dev = req->fixed_dev && req->moving_dev;
+    FW_CHECK(host != dev, "serve: give either host or device images");
+    uint64_t bytes = 0;
+    FW_TRY(estimate(req, &bytes));
+    if (bytes > s->budget)
+        return fail(FW_ERR_MEMORY, "serve: the request needs " + std::to_string(bytes) +
+                                       " bytes of device memory, more than the budget of " +
+                                       std::to_string(s->budget));
+    Job* j = new Job();
+    j->req = *req;
+    j->bytes = bytes;
+    HostGrid fg, mg;
+    int rc = make_grid(&req->fixed_grid, fg);
+    if (!rc) rc = make_grid(&req->moving_grid, mg);
+    if (rc) {
+        delete j;
+        return rc;
+    }
+    if (host) {
+        for (int c = 0; c < C; ++c) {
+            j->fixed_host.emplace_back(req->fixed[c], req->fixed[c] + fg.count());
+            j->moving_host.emplace_back(req->moving[c], req->moving[c] + mg.count());
+        }
+    } else {
+        for (int c = 0; c < C; ++c) {
+            j->fixed_dev.push_back(req->fixed_dev[c]);
+            j->moving_dev.push_back(req->moving_dev[c]);
+        }
+    }
+    j->req.fixed = j->req.moving = nullptr;
+    j->req.fixed_dev = j->req.moving_dev = nullptr;
+    j->submitted = Clock::now();
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        j->ticket = s->next_ticket++;
+        s->jobs[j->ticket] = j;
+        s->queue.push_back(j);
+        s->submitted++;
+    }
+    s->cv_work.notify_all();
+    *ticket = j->ticket;
+    return 0;
+}
+
+int fw_server_wait(fw_server* s, uint64_t ticket, double timeout_s, fw_syn_result* out) {
+    FW_CHECK(s && out, "null argument");
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return fail(FW_ERR_INVALID, "serve: unknown or already taken ticket");
+    Job* j = it->second;
+    auto ready = [&] { return j->done; };
+    if (timeout_s < 0) {
+        s->cv_done.wait(lock, ready);
+    } else if (!s->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), ready)) {
+        return fail(FW_ERR_TIMEOUT, "serve: the request is not done yet");
+    }
+    *out = j->result;
+    s->jobs.erase(it);
+    delete j;
+    return 0;
+}
+
+void fw_server_result_free(fw_syn_result* r) {
+    if (!r) return;
+    std::free(r->warp);
+    std::free(r->inverse_warp);
+    r->warp = r->inverse_warp = nullptr;
+}
+
+int fw_server_mark(fw_server* s) {
+    FW_CHECK(s, "null server");
+    cudaSetDevice(s->device);
+    std::lock_guard<std::mutex> lock(s->mu);
+    FW_CUDA(cudaEventRecord(s->epoch, s->ctxs[0]->stream));
+    FW_CUDA(cudaEventSynchronize(s->epoch));
+    s->epoch_set = true;
+    return 0;
+}
+
+int fw_server_stats_get(fw_server* s, fw_server_stats* out) {
+    FW_CHECK(s && out, "null argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    out->submitted = s->submitted;
+    out->completed = s->completed;
+    out->failed = s->failed;
+    out->active = s->active;
+    out->queued = s->queue.size();
+    out->reserved_bytes = s->reserved;
+    out->peak_reserved_bytes = s->peak;
+    out->budget_bytes = s->budget;
+    out->kernel_launches = out->graph_launches = 0;
+    for (auto* c : s->ctxs) {
+        out->kernel_launches += c->stats.kernel_launches;
+        out->graph_launches += c->stats.graph_launches;
+    }
+    return 0;
+}
+
+void fw_server_destroy(fw_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stopping = true;
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->threads) t.join();
+    for (auto& kv : s->jobs) {
+        fw_server_result_free(&kv.second->result);
+        fw_field_free(kv.second->result.warp_dev);
+        fw_field_free(kv.second->result.inverse_dev);
+        delete kv.second;
+    }
+    if (s->epoch) cudaEventDestroy(s->epoch);
+    for (auto* c : s->ctxs) fw_ctx_destroy(c);
+    delete s;
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+"""The continuous-batching registration server (include/fastwarp_serve.h) from Python.
+
+A `Server` owns N execution slots on one GPU (each a context with its own stream). Requests are
+queued at once and admitted as slots free up and their device-memory estimate fits the HBM
+budget; admitted registrations run concurrently and their kernels overlap on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from ._native import check, lib
+from .backend import Field, Image, grid_shape
+from .syn import SynRecipe
+
+
+class SynRequest(C.Structure):
+    _fields_ = [("recipe", N.SynRecipe), ("fixed_grid", N.Grid), ("moving_grid", N.Grid),
+                ("fixed", C.c_void_p), ("moving", C.c_void_p), ("fixed_dev", C.c_void_p),
+                ("moving_dev", C.c_void_p), ("initial", N.Affine), ("has_initial", C.c_int32),
+                ("keep_on_device", C.c_int32), ("tag", C.c_uint64)]
+
+
+class SynResultC(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("status", C.c_int32), ("error", C.c_char * 256),
+                ("grid", N.Grid), ("warp", C.c_void_p), ("inverse_warp", C.c_void_p),
+                ("warp_dev", C.c_void_p), ("inverse_dev", C.c_void_p),
+                ("iterations", C.c_int64), ("final_energy", C.c_double),
+                ("device_bytes", C.c_uint64), ("queued_s", C.c_double), ("run_s", C.c_double),
+                ("device_start_ms", C.c_double), ("device_end_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in (
+        "submitted", "completed", "failed", "active", "queued", "reserved_bytes",
+        "peak_reserved_bytes", "budget_bytes", "kernel_launches", "graph_launches")]
+
+
+class Server:
+    def __init__(self, device: int = 0, budget_bytes: int = 0, slots: int = 4):
+        h = C.c_void_p()
+        check(lib().fw_server_create(int(device), C.c_uint64(int(budget_bytes)), C.c_int32(slots),
+                                     C.byref(h)))
+        self.handle = h
+        self._keep = {}
+
+    def close(self):
+        if self.handle:
+            lib().fw_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _request(self, recipe: SynRecipe, fixed_grid, fixed, moving_grid, moving, initial, tag,
+                 keep_on_device):
+        q = SynRequest()
+        q.recipe = recipe.to_c()
+        q.fixed_grid = fixed_grid
+        q.moving_grid = moving_grid
+        keep = []
+        if isinstance(fixed[0], Image):
+            fp = (C.c_void_p * len(fixed))(*[im.handle.value for im in fixed])
+            mp = (C.c_void_p * len(moving))(*[im.handle.value for im in moving])
+            q.fixed_dev = C.cast(fp, C.c_void_p)
+            q.moving_dev = C.cast(mp, C.c_void_p)
+            keep = [fp, mp, fixed, moving]
+        else:
+            fs = [np.ascontiguousarray(a, np.float32) for a in fixed]
+            ms = [np.ascontiguousarray(a, np.float32) for a in moving]
+            fp = (C.c_void_p * len(fs))(*[a.ctypes.data for a in fs])
+            mp = (C.c_void_p * len(ms))(*[a.ctypes.data for a in ms])
+            q.fixed = C.cast(fp, C.c_void_p)
+            q.moving = C.cast(mp, C.c_void_p)
+            keep = [fp, mp, fs, ms]
+        if initial is not None:
+            q.initial = initial
+            q.has_initial = 1
+        q.keep_on_device = int(bool(keep_on_device))
+        q.tag = int(tag)
+        return q, keep
+
+    def estimate(self, recipe, fixed_grid, fixed, moving_grid, moving, initial=None) -> int:
+        q, _ = self._request(recipe, fixed_grid, fixed, moving_grid, moving, initial, 0, False)
+        b = C.c_uint64()
+        check(lib().fw_server_estimate(C.byref(q), C.byref(b)))
+        return int(b.value)
+
+    def submit(self, recipe: SynRecipe, fixed_grid, fixed, moving_grid, moving, initial=None,
+               tag=0, keep_on_device=False) -> int:
+        """Queues one SyN registration; `fixed`/`moving` are lists (one per channel) of host
+        float arrays or of device `Image`s. Returns the ticket."""
+        q, keep = self._request(recipe, fixed_grid, fixed, moving_grid, moving, initial, tag,
+                                keep_on_device)
+        t = C.c_uint64()
+        check(lib().fw_server_submit(self.handle, C.byref(q), C.byref(t)))
+        if isinstance(fixed[0], Image):
+            self._keep[int(t.value)] = keep  # device images must outlive the request
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout: float = -1.0) -> dict:
+        r = SynResultC()
+        check(lib().fw_server_wait(self.handle, C.c_uint64(ticket), C.c_double(timeout),
+                                   C.byref(r)))
+        self._keep.pop(ticket, None)
+        out = {"tag": r.tag, "status": r.status, "error": r.error.decode(errors="replace"),
+               "iterations": r.iterations, "final_energy": r.final_energy,
+               "device_bytes": r.device_bytes, "queued_s": r.queued_s, "run_s": r.run_s,
+               "latency_s": r.queued_s + r.run_s, "device_start_ms": r.device_start_ms,
+               "device_end_ms": r.device_end_ms, "grid": r.grid}
+        if r.status == 0 and r.warp:
+            shape = grid_shape(r.grid) + (3,)
+            n = int(np.prod(shape))
+            out["warp"] = np.ctypeslib.as_array((C.c_float * n).from_address(r.warp)).reshape(shape).copy()
+            out["inverse_warp"] = np.ctypeslib.as_array(
+                (C.c_float * n).from_address(r.inverse_warp)).reshape(shape).copy()
+        out["warp_dev"], out["inverse_dev"] = r.warp_dev, r.inverse_dev
+        lib().fw_server_result_free(C.byref(r))
+        return out
+
+    @staticmethod
+    def free_device_fields(result: dict):
+        for k in ("warp_dev", "inverse_dev"):
+            if result.get(k):
+                lib().fw_field_free(C.c_void_p(result[k]))
+                result[k] = None
+
+    def mark(self):
+        check(lib().fw_server_mark(self.handle))
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(lib().fw_server_stats_get(self.handle, C.byref(s)))
+        return {k: int(getattr(s, k)) for k, _ in ServerStats._fields_}

@@ -1,0 +1,88 @@
+/*
+ * fastwarp_serve.h -- continuous-batching registration server on one GPU.
+ *
+ * The reference runs several registrations on one device at once only in `register_atlases`
+ * (crates/fastwarp-cli/src/engine.rs:1016-1072: up to four at a time, admitted by a memory
+ * budget). This server generalises that path: requests of any grid size arrive at any time, are
+ * admitted as soon as an execution slot is free and their device-memory estimate fits the HBM
+ * budget, and then run concurrently -- each on its own context and stream, each level of each
+ * registration one CUDA graph -- so their kernels overlap on the GPU. Results do not depend on
+ * what else is running: every kernel is deterministic and no state is shared between requests.
+ */
+#ifndef FASTWARP_SERVE_H
+#define FASTWARP_SERVE_H
+
+#include "fastwarp_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fw_server fw_server;
+
+/* One SyN-stage request (run_syn, syn.rs:555-564). Images are either host float32 volumes
+ * (copied at submit, so the caller may free them at once) or device images made on any context
+ * of the same device (used in place; they must stay alive until the request completes). */
+typedef struct fw_syn_request {
+    fw_syn_recipe recipe;
+    fw_grid fixed_grid;
+    fw_grid moving_grid;
+    const float* const* fixed;         /* host, one per channel, or NULL */
+    const float* const* moving;
+    const fw_image* const* fixed_dev;  /* device, one per channel, or NULL */
+    const fw_image* const* moving_dev;
+    fw_affine initial;
+    int32_t has_initial;
+    int32_t keep_on_device;  /* 1: the fields stay on the device (warp_dev / inverse_dev) */
+    uint64_t tag;
+} fw_syn_request;
+
+typedef struct fw_syn_result {
+    uint64_t tag;
+    int32_t status;            /* FW_OK or an FW_ERR_* code */
+    char error[256];
+    fw_grid grid;              /* the last level grid of the fields */
+    float* warp;               /* host AoS float32 (keep_on_device == 0), else NULL */
+    float* inverse_warp;
+    fw_field* warp_dev;        /* keep_on_device == 1; free with fw_field_free before the server */
+    fw_field* inverse_dev;
+    int64_t iterations;
+    double final_energy;
+    uint64_t device_bytes;     /* the admission estimate of this request */
+    double queued_s;           /* submit -> start (host clock) */
+    double run_s;              /* start -> done (host clock) */
+    double device_start_ms;    /* device clock, relative to the last fw_server_mark */
+    double device_end_ms;
+} fw_syn_result;
+
+typedef struct fw_server_stats {
+    uint64_t submitted, completed, failed;
+    uint64_t active, queued;
+    uint64_t reserved_bytes, peak_reserved_bytes, budget_bytes;
+    uint64_t kernel_launches, graph_launches;
+} fw_server_stats;
+
+/* A server on `device` with `slots` execution slots (each its own context and stream) that
+ * admits requests while the sum of their device-memory estimates stays within `hbm_budget`
+ * bytes (0: 90 % of the device's free memory). */
+int fw_server_create(int device, uint64_t hbm_budget, int32_t slots, fw_server** out);
+/* Queues a request; returns at once with its ticket. Fails with FW_ERR_MEMORY when the request
+ * alone exceeds the budget. */
+int fw_server_submit(fw_server* s, const fw_syn_request* req, uint64_t* ticket);
+/* Waits for a ticket (timeout_s < 0: forever) and moves its result to `out`; FW_ERR_TIMEOUT when
+ * it is not done in time. A ticket's result can be taken once. */
+int fw_server_wait(fw_server* s, uint64_t ticket, double timeout_s, fw_syn_result* out);
+/* Frees the host buffers of a result (not the device fields). */
+void fw_server_result_free(fw_syn_result* r);
+/* Records the device-clock origin of device_start_ms / device_end_ms. */
+int fw_server_mark(fw_server* s);
+int fw_server_stats_get(fw_server* s, fw_server_stats* out);
+/* The device-memory estimate the server admits a request by. */
+int fw_server_estimate(const fw_syn_request* req, uint64_t* bytes);
+/* Waits for every queued and running request, then stops the slots. */
+void fw_server_destroy(fw_server* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,85 @@
+"""The continuous-batching server: each result is the same alone and in a mix, admission follows
+the HBM budget, and requests that cannot fit are refused before any work."""
+import numpy as np
+import pytest
+
+from fastwarp_b200 import CudaBackend, FastwarpError, SynRecipe
+from fastwarp_b200.phantoms import blob_pair
+from fastwarp_b200.serve import Server
+
+pytestmark = pytest.mark.gpu
+
+
+def small_recipe():
+    return SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2,
+                     iterations=[6, 4], shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0],
+                     convergence_threshold=-1.0)
+
+
+@pytest.fixture(scope="module")
+def pairs():
+    return [blob_pair(40, seed=101), blob_pair(48, seed=202), blob_pair(32, seed=303)]
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix(pairs):
+    r = small_recipe()
+    alone = []
+    with Server(0, slots=1) as s:
+        for g, f, m in pairs:
+            res = s.wait(s.submit(r, g, [f], g, [m]))
+            assert res["status"] == 0, res["error"]
+            alone.append(res)
+    with Server(0, slots=4) as s:
+        tickets = []
+        for rep in range(3):
+            for i, (g, f, m) in enumerate(pairs):
+                tickets.append((i, s.submit(r, g, [f], g, [m], tag=10 * rep + i)))
+        for i, t in tickets:
+            res = s.wait(t)
+            assert res["status"] == 0, res["error"]
+            assert np.array_equal(res["warp"], alone[i]["warp"])
+            assert np.array_equal(res["inverse_warp"], alone[i]["inverse_warp"])
+            assert res["final_energy"] == alone[i]["final_energy"]
+            assert res["iterations"] == 10
+        st = s.stats()
+        assert st["completed"] == 9 and st["failed"] == 0
+
+
+def test_admission_keeps_the_reserved_memory_within_the_budget(pairs):
+    r = small_recipe()
+    g, f, m = pairs[1]
+    with Server(0, slots=4) as probe:
+        one = probe.estimate(r, g, [f], g, [m])
+    budget = int(1.5 * one)  # room for one request at a time
+    with Server(0, budget_bytes=budget, slots=4) as s:
+        ts = [s.submit(r, g, [f], g, [m]) for _ in range(4)]
+        outs = [s.wait(t) for t in ts]
+        st = s.stats()
+    assert all(o["status"] == 0 for o in outs)
+    assert st["peak_reserved_bytes"] <= budget
+    # one at a time: each started after the previous finished
+    starts = sorted(o["queued_s"] for o in outs)
+    assert starts[-1] > 0.0
+
+
+def test_a_request_larger_than_the_budget_is_refused(pairs):
+    r = small_recipe()
+    g, f, m = pairs[0]
+    with Server(0, budget_bytes=1 << 20, slots=2) as s:
+        with pytest.raises(FastwarpError, match="budget"):
+            s.submit(r, g, [f], g, [m])
+
+
+def test_device_resident_images_and_fields(pairs):
+    r = small_recipe()
+    g, f, m = pairs[2]
+    with CudaBackend(0) as b:
+        fi, mi = b.upload_image(g, f), b.upload_image(g, m)
+        with Server(0, slots=2) as s:
+            host = s.wait(s.submit(r, g, [f], g, [m]))
+            s.mark()
+            dev = s.wait(s.submit(r, g, [fi], g, [mi], keep_on_device=True))
+            assert dev["status"] == 0, dev["error"]
+            assert dev["warp_dev"] and dev["device_end_ms"] > dev["device_start_ms"] >= 0.0
+            assert dev["final_energy"] == host["final_energy"]
+            Server.free_device_fields(dev)
