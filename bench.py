@@ -309,6 +309,15 @@ def run_ours(args, rank, world, local):
         out["config"]["served_over_sequential"] = round(value / world / seq_value, 3)
         out["config"]["sequential_latency_s"] = round(statistics.median(
             o["run_s"] for o in so), 4)
+        # the reference's execution shape: the loop drives one synchronous Backend op at a time
+        from fastwarp_b200.syn import run_syn_ops
+        log("op-by-op comparison")
+        run_syn_ops(b, rec, g, [fixed], mg, [moving], initial)
+        t0 = time.perf_counter()
+        run_syn_ops(b, rec, g, [fixed], mg, [moving], initial)
+        t_ops = time.perf_counter() - t0
+        out["config"]["op_by_op_value"] = round(3600.0 / t_ops, 1)
+        out["config"]["served_over_op_by_op"] = round(value / world / (3600.0 / t_ops), 3)
     # per-kernel roofline at the finest level (CUDA events on the engine stream)
     log("kernel timing")
     t = time_kernels(b, fi, b.upload_image(g, fixed), 20)

@@ -135,6 +135,143 @@ def run_syn_device(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
     return Field(backend, w), Field(backend, iw), _records(recs, min(count.value, cap))
 
 
+class WindowConvergenceMonitor:
+    """ITK's window convergence monitor (convergence.rs:47-126), on the host."""
+
+    def __init__(self, window: int):
+        self.window = window
+        self.values = []
+        self.total = 0.0
+
+    def add(self, v: float):
+        self.values.append(v)
+        if len(self.values) > self.window:
+            self.values.pop(0)
+        self.total += abs(v)
+
+    def value(self) -> float:
+        if len(self.values) < self.window:
+            return float(np.finfo(np.float64).max)
+        if self.window < 2:
+            return 0.0
+        r = 1.0 / ((11.0 - 1.0) * 0.1)
+        eps = r * 0.1 * 1e-3
+        delta, omega = [0.0, 0.0], [0.0, 0.0]
+        for n, e in enumerate(self.values):
+            p = (n / (self.window - 1)) * r
+            if abs(p - 1.0) <= eps:
+                p = 1.0 - eps
+            if p < 0.0 and abs(p) <= eps:
+                p = 0.0
+            t = p - np.floor(p)
+            w = (1.0 - t, t)
+            w2 = w[0] * w[0] + w[1] * w[1]
+            v = e / self.total
+            for j in range(2):
+                omega[j] += w[j] * w[j]
+                delta[j] += v * (w[j] ** 3 / w2)
+        phi = [0.0, 0.0]
+        for j in range(2):
+            if abs(omega[j]) > np.finfo(np.float64).eps:
+                q = delta[j] / omega[j]
+                phi[j] = q if np.isfinite(q) else 0.0
+        return phi[0] - phi[1]
+
+
+def run_syn_ops(backend: CudaBackend, recipe: SynRecipe, fixed_grid: N.Grid, fixed: list,
+                moving_grid: N.Grid, moving: list, initial: N.Affine | None = None):
+    """syn_fields (syn.rs:776-986) driven op by op through the Backend operations, every op a
+    synchronous call -- how the reference's loop drives an engine. Returns (warp, inverse_warp,
+    records) with the fields as host AoS float64 on the last level grid."""
+    from .backend import shrink_factors, shrink_grid
+    b = backend
+    C_ = len(recipe.channel_weights)
+    wsum = sum(recipe.channel_weights)
+    wn = [w / wsum for w in recipe.channel_weights]
+    fi = [b.upload_image(fixed_grid, np.ascontiguousarray(a, np.float32)) for a in fixed]
+    mi = [b.upload_image(moving_grid, np.ascontiguousarray(a, np.float32)) for a in moving]
+    F = Fi = M = Mi = None
+    records = []
+    eps = np.finfo(np.float64).eps
+    for level, limit in enumerate(recipe.iterations):
+        grid = shrink_grid(fixed_grid, shrink_factors(recipe.shrink_factors[level],
+                                                      tuple(fixed_grid.spacing)))
+        sigma = recipe.smoothing_sigmas[level]
+        if sigma > 0:
+            def sig(g):
+                return [sigma if recipe.sigma_units_mm else sigma * g.spacing[a] for a in range(3)]
+            fs = [b.smooth_recursive(im, sig(fixed_grid)) for im in fi]
+            ms = [b.smooth_recursive(im, sig(moving_grid)) for im in mi]
+        else:
+            fs, ms = fi, mi
+        if F is None:
+            F, Fi, M, Mi = (b.zero_field(grid) for _ in range(4))
+        else:
+            F, Fi, M, Mi = (b.resample_field(x, grid) for x in (F, Fi, M, Mi))
+        monitor = WindowConvergenceMonitor(recipe.convergence_window)
+        current, converged = 0, False
+        while current < limit and not converged:
+            current += 1
+            fmid = [b.warp_through_field(fs[c], Fi) for c in range(C_)]
+            mmid = [b.warp_through_field(ms[c], Mi, None, initial) for c in range(C_)]
+            sides = []
+            for side in range(2):
+                sides.append({"values": [], "grad": None, "mag": 0.0})
+            for c in range(C_):
+                if C_ == 1:
+                    (vf, df), (vm, dm) = b.cc_value_derivative_pair(fmid[c], mmid[c],
+                                                                    recipe.cc_radius)
+                    sides[0]["values"].append(vf)
+                    sides[1]["values"].append(vm)
+                    sides[0]["grad"], sides[1]["grad"] = df, dm
+                else:
+                    ((vf, df), (vm, dm)), norms = b.cc_value_derivative_pair_with_norms(
+                        fmid[c], mmid[c], recipe.cc_radius)
+                    for side, (v, d, nrm) in enumerate([(vf, df, norms[0]), (vm, dm, norms[1])]):
+                        s = sides[side]
+                        s["values"].append(v)
+                        if s["grad"] is None:
+                            s["grad"] = b.zero_field(grid)
+                        if not np.isfinite(nrm):
+                            raise N.FastwarpError(N.FW_ERR_NOT_FINITE,
+                                                  "syn: the metric gradient is not finite")
+                        s["mag"] += nrm
+                        if nrm > eps:
+                            b.axpy(s["grad"], wn[c] / nrm, d)
+            for s in sides:
+                if C_ > 1:
+                    b.scale(s["grad"], s["mag"] / C_)
+                s["grad"] = b.smooth_field(s["grad"], recipe.update_field_variance)
+            mF, mM = b.max_scaled_norm_pair(sides[0]["grad"], sides[1]["grad"])
+            if not (np.isfinite(mF) and np.isfinite(mM)):
+                raise N.FastwarpError(N.FW_ERR_NOT_FINITE, "syn: the metric gradient is not finite")
+            scales = []
+            for s, mx in zip(sides, (mF, mM)):
+                sc = recipe.gradient_step / mx if mx > 0.0 else recipe.gradient_step
+                b.scale(s["grad"], sc)
+                scales.append(sc)
+            stats = []
+            for side, (field, inverse) in enumerate([(F, Fi), (M, Mi)]):
+                composed = b.compose(sides[side]["grad"], field)
+                tmp = b.smooth_field(composed, recipe.total_field_variance)
+                (new_inv, s1), (new_field, s2) = b.invert_pair(tmp, inverse)
+                stats += [s1, s2]
+                if side == 0:
+                    F, Fi = new_field, new_inv
+                else:
+                    M, Mi = new_field, new_inv
+            energy = 0.5 * (sides[0]["values"][0] + sides[1]["values"][0])
+            monitor.add(energy)
+            cv = monitor.value()
+            converged = cv < recipe.convergence_threshold
+            records.append({"level": level, "energy": energy, "convergence_value": cv,
+                            "fixed_update_scale": scales[0], "moving_update_scale": scales[1],
+                            "inversions": stats})
+    warp = b.download_field(b.compose(Mi, F))
+    inverse = b.download_field(b.compose(Fi, M))
+    return warp, inverse, records
+
+
 def syn_step(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image], moving: List[Image],
              initial: N.Affine | None, state: dict, want_updates: bool = True):
     """One SyN iteration (syn.rs:890-958) on device-resident state fields f2m, f2m_inv, m2m,

@@ -119,6 +119,25 @@ def test_two_channel_registration_matches(backend):
     assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
 
 
+def test_the_op_by_op_loop_over_the_backend_matches_the_graph_driver(backend):
+    """The reference's loop shape (syn.rs:776-986: one synchronous Backend op at a time) on this
+    engine gives the graph-captured driver's result."""
+    from fastwarp_b200.syn import run_syn_ops
+    g, fixed, moving = blob_pair(40, seed=55)
+    r = SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2,
+                  iterations=[5, 4], shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0],
+                  convergence_threshold=-1.0)
+    res = run_syn(backend, r, g, [fixed], g, [moving])
+    w, iw, recs = run_syn_ops(backend, r, g, [fixed], g, [moving])
+    assert len(recs) == len(res.iterations) == 9
+    assert np.sqrt(((w - res.warp) ** 2).sum(-1).mean()) <= 1e-3
+    assert np.sqrt(((iw - res.inverse_warp) ** 2).sum(-1).mean()) <= 1e-3
+    assert abs(recs[-1]["energy"] - res.iterations[-1]["energy"]) <= 1e-5 * abs(recs[-1]["energy"])
+    og = ogrid(g)
+    ow, _, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed], og, [moving])
+    assert np.sqrt(((w - ow) ** 2).sum(-1).mean()) <= 0.05
+
+
 def test_convergence_monitor_stops_the_level_on_the_device(backend, pair):
     g, fixed, moving = pair
     r = config1(60)
