@@ -270,6 +270,48 @@ __global__ void __launch_bounds__(256) k_warp(WarpArgs a, const float* __restric
     out[l] = v;
 }
 
+// The plain warp (no earlier field, linear interpolation) -- the SyN loop's two per-iteration
+// warps -- with VPT voxels per thread, 256 apart, so their independent gathers are in flight
+// together.
+template <int VPT>
+__global__ void __launch_bounds__(256) k_warp_v(WarpArgs a, const float* __restrict__ u,
+                                                const float* __restrict__ src,
+                                                float* __restrict__ out) {
+    const long long base = (long long)blockIdx.x * (256 * VPT) + threadIdx.x;
+    float ux[VPT], uy[VPT], uz[VPT];
+#pragma unroll
+    for (int v = 0; v < VPT; ++v) {
+        long long l = base + v * 256;
+        ux[v] = uy[v] = uz[v] = 0.0f;
+        if (l < a.g.n) {
+            ux[v] = u[l];
+            uy[v] = u[l + a.fps];
+            uz[v] = u[l + 2 * a.fps];
+        }
+    }
+    float val[VPT];
+#pragma unroll
+    for (int v = 0; v < VPT; ++v) {
+        long long l = base + v * 256;
+        val[v] = 0.0f;
+        if (l >= a.g.n) continue;
+        int i, j, k;
+        voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
+        double c[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+            c[r] = a.q[r * 3] * i + a.q[r * 3 + 1] * j + a.q[r * 3 + 2] * k + a.q0[r] +
+                   (a.r[r * 3] * ux[v] + a.r[r * 3 + 1] * uy[v] + a.r[r * 3 + 2] * uz[v]);
+        if (inside_index(c[0], c[1], c[2], a.s.nx, a.s.ny, a.s.nz))
+            val[v] = lin_at_index(src, a.s.nx, a.s.ny, a.s.nz, c[0], c[1], c[2]);
+    }
+#pragma unroll
+    for (int v = 0; v < VPT; ++v) {
+        long long l = base + v * 256;
+        if (l < a.g.n) out[l] = val[v];
+    }
+}
+
 struct FieldArgs {
     DevGrid g;
     long long ps;
@@ -277,9 +319,10 @@ struct FieldArgs {
 
 // field_ops.rs:251-272 with the scale of syn.rs:285-298 fused: out(x) = w(x) + s * u(x + w(x)),
 // s = step / max |u/sp| (step when the max is 0) or 1 without a max.
+// `w` and `out` may be the same buffer (the SyN loop composes in place: a voxel reads only its
+// own value of `w`), so neither is declared __restrict__.
 __global__ void __launch_bounds__(256) k_compose(FieldArgs a, const float* __restrict__ u,
-                                                 const float* __restrict__ w,
-                                                 float* __restrict__ out,
+                                                 const float* w, float* out,
                                                  const unsigned int* __restrict__ max_bits,
                                                  double step) {
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -459,6 +502,10 @@ int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const f
         mat3_vec(s.inv, t, a.q0);
     }
     long long n = a.g.n;
+    if (!pre && !mask) {
+        k_warp_v<4><<<blocks_for(n, 1024), 256, 0, ctx->stream>>>(a, field->d, src->d, out);
+        return check_launch(ctx, "k_warp_v");
+    }
     k_warp<<<blocks_for(n), 256, 0, ctx->stream>>>(a, field->d, pre ? pre->d : nullptr, src->d,
                                                    product, out);
     return check_launch(ctx, "k_warp");

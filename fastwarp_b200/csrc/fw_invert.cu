@@ -101,16 +101,23 @@ __global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __r
                                                      int use_handle) {
     double sum = 0.0;
     float mx = 0.0f;
-    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < a.g.n;
-         l += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
-        float e[3];
-        residual(a, f, l, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
-        float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
-        float nrm = nan_canon(sqrtf(x * x + y * y + z * z));
-        sum += (double)nrm;
-        mx = __int_as_float(max(__float_as_int(mx), __float_as_int(nrm)));
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // two voxels a step, `stride` apart: their gathers are in flight together
+    for (long long l0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; l0 < a.g.n;
+         l0 += 2 * stride) {
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            long long l = l0 + v * stride;
+            if (l >= a.g.n) continue;
+            int i, j, k;
+            voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
+            float e[3];
+            residual(a, f, l, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
+            float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
+            float nrm = nan_canon(sqrtf(x * x + y * y + z * z));
+            sum += (double)nrm;
+            mx = __int_as_float(max(__float_as_int(mx), __float_as_int(nrm)));
+        }
     }
     const double count = (double)a.g.n;
     reduce_and_finish(sum, mx, partials, counter, [&](double s, double m) {
@@ -146,37 +153,61 @@ __global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __rest
     const bool enforce = st->enforce != 0;
     double sum = 0.0;
     float mx = 0.0f;
-    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < a.g.n;
-         l += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
-        float px = psi[l], py = psi[l + a.ps_psi], pz = psi[l + 2 * a.ps_psi];
-        float e[3];
-        residual(a, f, l, i, j, k, px, py, pz, e);
-        float ex = e[0] * a.isx, ey = e[1] * a.isy, ez = e[2] * a.isz;
-        float nrm = sqrtf(ex * ex + ey * ey + ez * ez);
-        float ux = -e[0], uy = -e[1], uz = -e[2];
-        if (nrm > limit) {
-            float fct = limit / nrm;
-            ux *= fct;
-            uy *= fct;
-            uz *= fct;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // two voxels a step, `stride` apart: their gathers are in flight together
+    for (long long l0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; l0 < a.g.n;
+         l0 += 2 * stride) {
+        float px[2], py[2], pz[2];
+        int ii[2], jj[2], kk[2];
+        bool ok[2];
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            long long l = l0 + v * stride;
+            ok[v] = l < a.g.n;
+            if (!ok[v]) continue;
+            voxel_ijk(l, a.g.nx, a.g.ny, ii[v], jj[v], kk[v]);
+            px[v] = psi[l];
+            py[v] = psi[l + a.ps_psi];
+            pz[v] = psi[l + 2 * a.ps_psi];
         }
-        px = px + ux * eps;
-        py = py + uy * eps;
-        pz = pz + uz * eps;
-        const bool face = i == 0 || j == 0 || k == 0 || i == a.g.nx - 1 || j == a.g.ny - 1 ||
-                          k == a.g.nz - 1;
-        if (enforce && face) px = py = pz = 0.0f;
-        psi[l] = px;
-        psi[l + a.ps_psi] = py;
-        psi[l + 2 * a.ps_psi] = pz;
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            if (!ok[v]) continue;
+            long long l = l0 + v * stride;
+            const int i = ii[v], j = jj[v], k = kk[v];
+            float e[3];
+            residual(a, f, l, i, j, k, px[v], py[v], pz[v], e);
+            float ex = e[0] * a.isx, ey = e[1] * a.isy, ez = e[2] * a.isz;
+            float nrm = sqrtf(ex * ex + ey * ey + ez * ez);
+            float ux = -e[0], uy = -e[1], uz = -e[2];
+            if (nrm > limit) {
+                float fct = limit / nrm;
+                ux *= fct;
+                uy *= fct;
+                uz *= fct;
+            }
+            px[v] = px[v] + ux * eps;
+            py[v] = py[v] + uy * eps;
+            pz[v] = pz[v] + uz * eps;
+            const bool face = i == 0 || j == 0 || k == 0 || i == a.g.nx - 1 ||
+                              j == a.g.ny - 1 || k == a.g.nz - 1;
+            if (enforce && face) px[v] = py[v] = pz[v] = 0.0f;
+            psi[l] = px[v];
+            psi[l + a.ps_psi] = py[v];
+            psi[l + 2 * a.ps_psi] = pz[v];
+        }
         if (next) {
-            residual(a, f, l, i, j, k, px, py, pz, e);
-            float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
-            float n2 = nan_canon(sqrtf(x * x + y * y + z * z));
-            sum += (double)n2;
-            mx = __int_as_float(max(__float_as_int(mx), __float_as_int(n2)));
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+                if (!ok[v]) continue;
+                long long l = l0 + v * stride;
+                float e[3];
+                residual(a, f, l, ii[v], jj[v], kk[v], px[v], py[v], pz[v], e);
+                float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
+                float n2 = nan_canon(sqrtf(x * x + y * y + z * z));
+                sum += (double)n2;
+                mx = __int_as_float(max(__float_as_int(mx), __float_as_int(n2)));
+            }
         }
     }
     const double count = (double)a.g.n;

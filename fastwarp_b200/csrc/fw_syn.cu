@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -509,6 +510,36 @@ struct GraphGuard {
 };
 
 // Captures the level's iteration loop as one graph, launches it and waits.
+// FASTWARP_SYN_GRAPHS=0 launches the same kernels straight onto the stream, the loops driven by
+// the host (one read-back per inversion body and per iteration): for profilers that cannot look
+// inside graphs with conditional nodes, and for debugging. The default is the graph.
+bool use_graphs() {
+    const char* v = std::getenv("FASTWARP_SYN_GRAPHS");
+    return !(v && v[0] == '0');
+}
+
+int run_level_direct(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
+                     const std::vector<const fw_image*>& fs, const std::vector<const fw_image*>& ms,
+                     const fw_affine* initial, const RunDev& d, int level, int limit,
+                     fw_syn_iteration* trace_dev_base) {
+    k_syn_level_init<<<1, 1, 0, ctx->stream>>>(d.syn, level, limit);
+    FW_TRY(check_launch(ctx, "k_syn_level_init"));
+    for (int it = 0; it < limit; ++it) {
+        if (ctx->cancel && *ctx->cancel) return fail(FW_ERR_CANCELLED, "registration cancelled");
+        FW_TRY(enqueue_iteration(ctx, false, r, L, fs, ms, initial, d));
+        k_syn_record<<<1, 1, 0, ctx->stream>>>(d.syn, d.cc, d.max_bits, d.inv, trace_dev_base,
+                                              d.trace_cap, nullptr, 0, 0);
+        FW_TRY(check_launch(ctx, "k_syn_record"));
+        FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, d.syn, sizeof(SynDev), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        FW_TRY(sync(ctx));
+        SynDev h;
+        std::memcpy(&h, ctx->h_pinned, sizeof(h));
+        if (h.converged || h.status) break;
+    }
+    return 0;
+}
+
 int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
                     const std::vector<const fw_image*>& fs, const std::vector<const fw_image*>& ms,
                     const fw_affine* initial, const RunDev& d, int level, int limit,
@@ -672,7 +703,10 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
         if (rc) break;
         int limit = (int)r->iterations[level];
         if (limit > 0) {
-            rc = run_level_graph(ctx, r, L, fs, ms, initial, rs.d, level, limit, rs.d.trace + done);
+            if (use_graphs())
+                rc = run_level_graph(ctx, r, L, fs, ms, initial, rs.d, level, limit, rs.d.trace + done);
+            else
+                rc = run_level_direct(ctx, r, L, fs, ms, initial, rs.d, level, limit, rs.d.trace + done);
             if (rc) break;
             // the level's records and the device status
             SynDev h;
