@@ -31,6 +31,7 @@ struct CcArgs {
     int zchunk;         // slices per CTA
     int identity_dir;   // direction is the identity: axis-aligned probes
     double probe[3][3]; // index offset of +half a spacing along physical axis d: probe[d][r]
+    double isp[3];      // 1 / spacing (the central difference's denominator)
 };
 
 // Exact float64 emulation of the oracle's probe position (index_to_point, offset along the
@@ -180,17 +181,29 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
             for (int s = tid; s < L::HY * (TX / 2); s += L::NT) {
                 int hy = s / (TX / 2), cp = s - hy * (TX / 2);
                 const float2* row = slot + hy * L::HX + 2 * cp;
+                // two interleaved partial sums per plane: half-length add chains
                 double c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0;
+                double e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0;
 #pragma unroll
-                for (int t = 1; t <= 2 * R; ++t) {
-                    float2 v = row[t];
-                    double f = v.x, m = v.y;
+                for (int t = 1; t <= 2 * R; t += 2) {
+                    float2 v = row[t], w = row[t + 1];
+                    double f = v.x, m = v.y, g = w.x, n = w.y;
                     c0 += f;
                     c1 += m;
                     c2 += f * f;
                     c3 += m * m;
                     c4 += f * m;
+                    e0 += g;
+                    e1 += n;
+                    e2 += g * g;
+                    e3 += n * n;
+                    e4 += g * n;
                 }
+                c0 += e0;
+                c1 += e1;
+                c2 += e2;
+                c3 += e3;
+                c4 += e4;
                 float2 va = row[0], vb = row[2 * R + 1];
                 double fa = va.x, ma = va.y, fb = vb.x, mb = vb.y;
                 double* o = xs + hy * TX + 2 * cp;
@@ -204,10 +217,13 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
             // y pass for the thread's own column
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                double s = 0.0;
+                double s = 0.0, s2 = 0.0;  // two partial sums: half-length add chains
 #pragma unroll
-                for (int t = 0; t <= 2 * R; ++t) s += xs[(q * L::HY + ty + t) * TX + tx];
-                P[q] = s;
+                for (int t = 0; t < 2 * R; t += 2) {
+                    s += xs[(q * L::HY + ty + t) * TX + tx];
+                    s2 += xs[(q * L::HY + ty + t + 1) * TX + tx];
+                }
+                P[q] = s + s2 + xs[(q * L::HY + ty + 2 * R) * TX + tx];
             }
         }
         // z window: running sum over the ring of xy sums (entering k, leaving k - 2R - 1)
@@ -228,20 +244,25 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
         const float fv = cs[0].x, mv = cs[0].y;
         // metric/cc.rs:267-302 (same expression order)
         const double sum_f = S[0], sum_m = S[1], sum_f2 = S[2], sum_m2 = S[3], sum_fm = S[4];
-        const double fmean = sum_f / cnt, mmean = sum_m / cnt;
+        const double icnt = 1.0 / cnt;
+        const double fmean = sum_f * icnt, mmean = sum_m * icnt;
         const double s_ff = sum_f2 - fmean * sum_f - fmean * sum_f + cnt * fmean * fmean;
         const double s_mm = sum_m2 - mmean * sum_m - mmean * sum_m + cnt * mmean * mmean;
         const double s_fm = sum_fm - mmean * sum_f - fmean * sum_m + cnt * mmean * fmean;
         const double fi = (double)fv - fmean, mi = (double)mv - mmean;
         const double product = s_ff * s_mm;
-        double cc = 1.0;
-        if (fabs(product) > DBL_EPSILON) cc = s_fm * s_fm / product;
-        acc_cc += cc;
-        double cf = 0.0, cm = 0.0;
-        if (s_ff > DBL_EPSILON && s_mm > DBL_EPSILON) {
-            cf = 2.0 * s_fm / product * (fi - s_fm / s_mm * mi);  // (fixed, moving)
-            cm = 2.0 * s_fm / product * (mi - s_fm / s_ff * fi);  // (moving, fixed)
+        double cc = 1.0, cf = 0.0, cm = 0.0;
+        const bool prod_ok = fabs(product) > DBL_EPSILON;
+        const bool coef_ok = s_ff > DBL_EPSILON && s_mm > DBL_EPSILON;  // implies product > 0
+        // one reciprocal: 1 / sMM = sFF / product and 1 / sFF = sMM / product
+        const double ip = (prod_ok || coef_ok) ? 1.0 / product : 0.0;
+        if (prod_ok) cc = s_fm * s_fm * ip;
+        if (coef_ok) {
+            const double k2 = 2.0 * s_fm * ip;
+            cf = k2 * (fi - s_fm * s_ff * ip * mi);  // (fixed, moving)
+            cm = k2 * (mi - s_fm * s_mm * ip * fi);  // (moving, fixed)
         }
+        acc_cc += cc;
         // gradients of moving (for the first direction) and of fixed (for the second)
         float gm[3], gf[3];
         if (a.identity_dir) {
@@ -276,8 +297,8 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
                 // lower probe at p - 0.5: base p - 1 with weight 0.5, or the first voxel itself
                 float m1 = p > 0 ? fmaf(mv - lo.y, 0.5f, lo.y) : mv;
                 float f1 = p > 0 ? fmaf(fv - lo.x, 0.5f, lo.x) : fv;
-                gm[d] = (float)((double)(m2 - m1) / a.g.sp[d]);
-                gf[d] = (float)((double)(f2 - f1) / a.g.sp[d]);
+                gm[d] = (float)((double)(m2 - m1) * a.isp[d]);
+                gf[d] = (float)((double)(f2 - f1) * a.isp[d]);
             }
         } else {
             central_difference_exact(mimg, a.g, x, y, z, gm);
@@ -370,6 +391,7 @@ int launch_cc_pair_impl(fw_ctx* ctx, const fw_image* fixed, const fw_image* movi
     a.g = dev_grid(fixed->grid);
     a.ps = d_fixed->ps;
     const HostGrid& g = fixed->grid;
+    for (int d = 0; d < 3; ++d) a.isp[d] = 1.0 / g.sp[d];
     a.identity_dir = 1;
     for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c)
@@ -553,6 +575,7 @@ extern "C" int fw_cc_value_derivative_pair_noalloc(const fw_grid* grid, const fl
     std::memset(&a, 0, sizeof(a));
     a.g = dev_grid(g);
     a.ps = plane_stride;
+    for (int d = 0; d < 3; ++d) a.isp[d] = 1.0 / g.sp[d];
     a.identity_dir = 1;
     for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c)
