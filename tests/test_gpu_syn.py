@@ -146,3 +146,19 @@ def test_convergence_monitor_stops_the_level_on_the_device(backend, pair):
     res = run_syn(backend, r, g, [fixed], g, [moving])
     ow, _, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed], og, [moving])
     assert len(res.iterations) == len(orecs) < 60
+
+
+def test_direct_launch_mode_gives_the_graph_result(backend, monkeypatch):
+    """FASTWARP_SYN_GRAPHS=0 launches the same kernels straight onto the stream with the loops on
+    the host (the profiling mode); it must give the graph driver's result bit for bit."""
+    g, fixed, moving = blob_pair(40, seed=56)
+    r = SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2,
+                  iterations=[5, 4], shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0],
+                  convergence_threshold=1e-3, convergence_window=3)
+    res = run_syn(backend, r, g, [fixed], g, [moving])
+    monkeypatch.setenv("FASTWARP_SYN_GRAPHS", "0")
+    direct = run_syn(backend, r, g, [fixed], g, [moving])
+    assert len(direct.iterations) == len(res.iterations)
+    assert np.array_equal(direct.warp, res.warp)
+    assert np.array_equal(direct.inverse_warp, res.inverse_warp)
+    assert direct.iterations[-1]["energy"] == res.iterations[-1]["energy"]
