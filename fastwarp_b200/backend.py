@@ -231,6 +231,27 @@ class CudaBackend:
             C.byref(b), norms))
         return ((vals[0], Field(self, a)), (vals[1], Field(self, b))), [norms[0], norms[1]]
 
+    def cc_value_derivative_pair_masked(self, fixed: Image, moving: Image, valid: Image,
+                                        radius: int):
+        """Backend::cc_value_derivative_pair_masked (backend.rs:128-140): only voxels where
+        `valid` is not zero count; raises FastwarpError naming NO_VOXEL_IN_MASKS when none does."""
+        vals = (C.c_double * 2)()
+        a, b = C.c_void_p(), C.c_void_p()
+        check(lib().fw_cc_value_derivative_pair_masked(
+            self.ctx, fixed.handle, moving.handle, valid.handle, C.c_int32(radius), vals,
+            C.byref(a), C.byref(b)))
+        return (vals[0], Field(self, a)), (vals[1], Field(self, b))
+
+    def cc_value_derivative_pair_masked_with_norms(self, fixed: Image, moving: Image,
+                                                   valid: Image, radius: int):
+        vals = (C.c_double * 2)()
+        norms = (C.c_double * 2)()
+        a, b = C.c_void_p(), C.c_void_p()
+        check(lib().fw_cc_value_derivative_pair_masked_with_norms(
+            self.ctx, fixed.handle, moving.handle, valid.handle, C.c_int32(radius), vals,
+            C.byref(a), C.byref(b), norms))
+        return ((vals[0], Field(self, a)), (vals[1], Field(self, b))), [norms[0], norms[1]]
+
     def smooth_field(self, field: Field, variance: float) -> Field:
         check(lib().fw_smooth_field(self.ctx, field.handle, C.c_double(variance)))
         return field

@@ -90,35 +90,50 @@ __device__ __forceinline__ bool axis_probe_inside(const DevGrid& g, int i, int j
     return c[d] >= -0.5 && c[d] < (double)n - 0.5;
 }
 
-// Shared-memory layout (dynamic): input ring [D][HY][HX] float2 (f, m); x sums [5][HY][TX]
-// double; xy-sum ring [2R+1][5][TX*TY] double.
-template <int R, int TY>
+// Shared-memory layout (dynamic): input ring [D][HY][HX] float2 (f, m); with a mask, its flags
+// [D][HY][HX] bytes; x sums [5][HY][TX] double (+ [HY][TX] int counts); xy-sum ring
+// [2R+1][5][TX*TY] double (+ [2R+1][TX*TY] int counts); block-reduction space.
+template <int R, int TY, bool MK>
 struct Layout {
     static constexpr int HX = TX + 2 * R;
     static constexpr int HY = TY + 2 * R;
     static constexpr int D = R + 2;        // input slices kept: k-R-1 .. k
     static constexpr int W = 2 * R + 1;    // z window
     static constexpr int NT = TX * TY;
+    static constexpr int NP = MK ? 4 : 3;  // block partials: cc, |dF|^2, |dM|^2 (+ valid voxels)
     static constexpr size_t in_bytes = sizeof(float2) * D * HY * HX;
+    static constexpr size_t vin_bytes = MK ? (size_t)(D * HY * HX + 15) / 16 * 16 : 0;
     static constexpr size_t xs_bytes = sizeof(double) * 5 * HY * TX;
+    static constexpr size_t xc_bytes = MK ? sizeof(int) * HY * TX : 0;
     static constexpr size_t ring_bytes = sizeof(double) * W * 5 * NT;
-    static constexpr size_t bytes = in_bytes + xs_bytes + ring_bytes + 64 * sizeof(double);
+    static constexpr size_t rc_bytes = MK ? sizeof(int) * W * NT : 0;
+    static constexpr size_t bytes =
+        in_bytes + vin_bytes + xs_bytes + xc_bytes + ring_bytes + rc_bytes + 64 * sizeof(double);
 };
 
-template <int R, int TY>
+// MK: masked (cpu/mod.rs:134-163 -> evaluate_masked with Some(valid)): a voxel counts only where
+// `vimg` is not zero; invalid voxels add nothing to any window sum, the count is the number of
+// valid voxels in the window, their outputs are zero and the value is the mean over the valid
+// voxels (result[3] receives their number; zero means no voxel in the masks).
+template <int R, int TY, bool MK>
 __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __restrict__ fimg,
                                                      const float* __restrict__ mimg,
+                                                     const float* __restrict__ vimg,
                                                      float* __restrict__ d_fixed,
                                                      float* __restrict__ d_moving,
                                                      double* __restrict__ partials,
                                                      unsigned int* __restrict__ counter,
                                                      double* __restrict__ result, int want_norms) {
-    using L = Layout<R, TY>;
+    using L = Layout<R, TY, MK>;
     extern __shared__ __align__(16) unsigned char smem[];
     float2* in = reinterpret_cast<float2*>(smem);
-    double* xs = reinterpret_cast<double*>(smem + L::in_bytes);
-    double* ring = reinterpret_cast<double*>(smem + L::in_bytes + L::xs_bytes);
-    double* red = ring + L::W * 5 * L::NT;
+    unsigned char* vin = smem + L::in_bytes;
+    double* xs = reinterpret_cast<double*>(smem + L::in_bytes + L::vin_bytes);
+    int* xc = reinterpret_cast<int*>(smem + L::in_bytes + L::vin_bytes + L::xs_bytes);
+    double* ring = reinterpret_cast<double*>(smem + L::in_bytes + L::vin_bytes + L::xs_bytes +
+                                             L::xc_bytes);
+    int* rcn = reinterpret_cast<int*>(ring + L::W * 5 * L::NT);
+    double* red = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(rcn) + L::rc_bytes);
 
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
     const int tid = threadIdx.x;
@@ -131,8 +146,11 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
     const long long sxy = (long long)nx * ny;
 
     for (int s = tid; s < L::W * 5 * L::NT; s += L::NT) ring[s] = 0.0;
+    if constexpr (MK)
+        for (int s = tid; s < L::W * L::NT; s += L::NT) rcn[s] = 0;
     double S[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    double acc_cc = 0.0, acc_nf = 0.0, acc_nm = 0.0;
+    int Sc = 0;  // valid voxels in the window (masked)
+    double acc_cc = 0.0, acc_nf = 0.0, acc_nm = 0.0, acc_nv = 0.0;
 
     // analytic voxel counts of the clamped window along x and y
     const int cxn = own ? (min(x + R, nx - 1) - max(x - R, 0) + 1) : 0;
@@ -154,25 +172,34 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
         }
     }
     float2 pre[PERC];
+    unsigned char prev[PERC];
     auto fetch = [&](int k) {
         const long long zoff = (long long)k * sxy;
 #pragma unroll
-        for (int q = 0; q < PERC; ++q)
+        for (int q = 0; q < PERC; ++q) {
             pre[q] = src_off[q] >= 0 ? make_float2(__ldg(fimg + zoff + src_off[q]),
                                                    __ldg(mimg + zoff + src_off[q]))
                                      : make_float2(0.0f, 0.0f);
+            if constexpr (MK)
+                prev[q] = src_off[q] >= 0 ? (__ldg(vimg + zoff + src_off[q]) != 0.0f) : 0;
+        }
     };
     if (kbeg < kend) fetch(kbeg);
     for (int k = kbeg; k < z1 + R; ++k) {
         __syncthreads();  // previous slice's readers are done with the slot and the x sums
         double P[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        int Pc = 0;
         const bool have = k < kend;
         if (have) {
             float2* slot = in + (k % L::D) * (L::HY * L::HX);
+            unsigned char* vslot = vin + (k % L::D) * (L::HY * L::HX);
 #pragma unroll
             for (int q = 0; q < PERC; ++q) {
                 int s = tid + q * L::NT;
-                if (s < L::HY * L::HX) slot[s] = pre[q];
+                if (s < L::HY * L::HX) {
+                    slot[s] = pre[q];
+                    if constexpr (MK) vslot[s] = prev[q];
+                }
             }
             __syncthreads();
             if (k + 1 < kend) fetch(k + 1);  // in flight while this slice is summed
@@ -181,12 +208,27 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
             for (int s = tid; s < L::HY * (TX / 2); s += L::NT) {
                 int hy = s / (TX / 2), cp = s - hy * (TX / 2);
                 const float2* row = slot + hy * L::HX + 2 * cp;
+                const unsigned char* vrow = vslot + hy * L::HX + 2 * cp;
+                // a masked-out voxel enters every sum as zero
+                auto val = [&](int t) {
+                    float2 v = row[t];
+                    if constexpr (MK)
+                        if (!vrow[t]) v = make_float2(0.0f, 0.0f);
+                    return v;
+                };
+                if constexpr (MK) {
+                    int cn = 0;
+#pragma unroll
+                    for (int t = 1; t <= 2 * R; ++t) cn += vrow[t];
+                    xc[hy * TX + 2 * cp] = cn + vrow[0];
+                    xc[hy * TX + 2 * cp + 1] = cn + vrow[2 * R + 1];
+                }
                 // two interleaved partial sums per plane: half-length add chains
                 double c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0;
                 double e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0;
 #pragma unroll
                 for (int t = 1; t <= 2 * R; t += 2) {
-                    float2 v = row[t], w = row[t + 1];
+                    float2 v = val(t), w = val(t + 1);
                     double f = v.x, m = v.y, g = w.x, n = w.y;
                     c0 += f;
                     c1 += m;
@@ -204,7 +246,7 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
                 c2 += e2;
                 c3 += e3;
                 c4 += e4;
-                float2 va = row[0], vb = row[2 * R + 1];
+                float2 va = val(0), vb = val(2 * R + 1);
                 double fa = va.x, ma = va.y, fb = vb.x, mb = vb.y;
                 double* o = xs + hy * TX + 2 * cp;
                 *reinterpret_cast<double2*>(o + 0 * L::HY * TX) = make_double2(c0 + fa, c0 + fb);
@@ -225,6 +267,10 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
                 }
                 P[q] = s + s2 + xs[(q * L::HY + ty + 2 * R) * TX + tx];
             }
+            if constexpr (MK) {
+#pragma unroll
+                for (int t = 0; t <= 2 * R; ++t) Pc += xc[(ty + t) * TX + tx];
+            }
         }
         // z window: running sum over the ring of xy sums (entering k, leaving k - 2R - 1)
         double* rs = ring + (k % L::W) * 5 * L::NT + tid;
@@ -234,12 +280,29 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
             S[q] += P[q] - old;
             rs[q * L::NT] = P[q];
         }
+        if constexpr (MK) {
+            int* rc = rcn + (k % L::W) * L::NT + tid;
+            Sc += Pc - *rc;
+            *rc = Pc;
+        }
         const int z = k - R;
         if (z < z0 || z >= z1 || !own) continue;
 
         // ---- output voxel (x, y, z) ----
-        const int czn = min(z + R, nz - 1) - max(z - R, 0) + 1;
-        const double cnt = (double)(cxn * cyn * czn);
+        const long long l = (long long)z * sxy + (long long)y * nx + x;
+        double cnt;
+        if constexpr (MK) {
+            if (!vin[(z % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R)]) {
+                d_fixed[l] = d_fixed[l + a.ps] = d_fixed[l + 2 * a.ps] = 0.0f;
+                d_moving[l] = d_moving[l + a.ps] = d_moving[l + 2 * a.ps] = 0.0f;
+                continue;
+            }
+            cnt = (double)Sc;  // >= 1: the centre is valid
+            acc_nv += 1.0;
+        } else {
+            const int czn = min(z + R, nz - 1) - max(z - R, 0) + 1;
+            cnt = (double)(cxn * cyn * czn);
+        }
         const float2* cs = in + (z % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R);
         const float fv = cs[0].x, mv = cs[0].y;
         // metric/cc.rs:267-302 (same expression order)
@@ -304,7 +367,6 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
             central_difference_exact(mimg, a.g, x, y, z, gm);
             central_difference_exact(fimg, a.g, x, y, z, gf);
         }
-        const long long l = (long long)z * sxy + (long long)y * nx + x;
         const float fcf = (float)cf, fcm = (float)cm;
         float dfx = fcf * gm[0], dfy = fcf * gm[1], dfz = fcf * gm[2];
         float dmx = fcm * gf[0], dmy = fcm * gf[1], dmz = fcm * gf[2];
@@ -321,23 +383,23 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
     }
 
     // block partials, then the fixed-order last-block reduction
-    acc_cc = warp_sum_d(acc_cc);
-    acc_nf = warp_sum_d(acc_nf);
-    acc_nm = warp_sum_d(acc_nm);
+    constexpr int NP = L::NP;
+    double acc[4] = {acc_cc, acc_nf, acc_nm, acc_nv};
+#pragma unroll
+    for (int q = 0; q < NP; ++q) acc[q] = warp_sum_d(acc[q]);
     __syncthreads();
     const int warps = L::NT / 32;
     if ((tid & 31) == 0) {
-        red[(tid >> 5) * 3 + 0] = acc_cc;
-        red[(tid >> 5) * 3 + 1] = acc_nf;
-        red[(tid >> 5) * 3 + 2] = acc_nm;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) red[(tid >> 5) * NP + q] = acc[q];
     }
     __syncthreads();
     const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
     const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (tid < 3) {
+    if (tid < NP) {
         double s = 0.0;
-        for (int w = 0; w < warps; ++w) s += red[w * 3 + tid];
-        partials[(size_t)bid * 3 + tid] = s;
+        for (int w = 0; w < warps; ++w) s += red[w * NP + tid];
+        partials[(size_t)bid * NP + tid] = s;
     }
     __threadfence();
     __syncthreads();
@@ -346,23 +408,28 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
     __syncthreads();
     if (!last) return;
     if (tid < 32) {
-        for (int q = 0; q < 3; ++q) {
+        double tot[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
             double s = 0.0;
-            for (unsigned int b = tid; b < nblocks; b += 32) s += __ldcg(partials + (size_t)b * 3 + q);
-            s = warp_sum_d(s);
-            if (tid == 0) {
-                if (q == 0) result[0] = -s / (double)a.g.n;
-                else result[q] = s;
-            }
+            for (unsigned int b = tid; b < nblocks; b += 32) s += __ldcg(partials + (size_t)b * NP + q);
+            tot[q] = warp_sum_d(s);
         }
-        if (tid == 0) *counter = 0;
+        if (tid == 0) {
+            // the mean over the valid voxels (all voxels without a mask); no valid voxel: NaN
+            result[0] = -tot[0] / (MK ? tot[3] : (double)a.g.n);
+            result[1] = tot[1];
+            result[2] = tot[2];
+            if constexpr (MK) result[3] = tot[3];
+            *counter = 0;
+        }
     }
 }
 
-template <int R, int TY>
-int launch_r(fw_ctx* ctx, const CcArgs& a0, const float* f, const float* m, float* df, float* dm,
-             double* d_result, int want_norms) {
-    using L = Layout<R, TY>;
+template <int R, int TY, bool MK>
+int launch_r(fw_ctx* ctx, const CcArgs& a0, const float* f, const float* m, const float* v,
+             float* df, float* dm, double* d_result, int want_norms) {
+    using L = Layout<R, TY, MK>;
     CcArgs a = a0;
     dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, 1);
     // z chunks: enough CTAs to fill the GPU a few times over, chunks no thinner than 4R slices
@@ -373,19 +440,39 @@ int launch_r(fw_ctx* ctx, const CcArgs& a0, const float* f, const float* m, floa
     a.zchunk = chunk;
     grid.z = (a.g.nz + chunk - 1) / chunk;
     unsigned int nblocks = grid.x * grid.y * grid.z;
-    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 3 * (size_t)nblocks + 16));
-    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)L::bytes));
-    k_cc_pair<R, TY><<<grid, L::NT, L::bytes, ctx->stream>>>(
-        a, f, m, df, dm, ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 1, d_result, want_norms);
+    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)L::NP * nblocks + 16));
+    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY, MK>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes));
+    k_cc_pair<R, TY, MK><<<grid, L::NT, L::bytes, ctx->stream>>>(
+        a, f, m, v, df, dm, ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 1, d_result,
+        want_norms);
     return check_launch(ctx, "k_cc_pair");
+}
+
+template <bool MK>
+int launch_radius(fw_ctx* ctx, const CcArgs& a, int radius, const float* f, const float* m,
+                  const float* v, float* df, float* dm, double* d_result, int want_norms) {
+    switch (radius) {
+        case 1: return launch_r<1, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 2: return launch_r<2, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 3: return launch_r<3, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 4: return launch_r<4, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 5: return launch_r<5, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 6: return launch_r<6, 4, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 7: return launch_r<7, 4, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 8: return launch_r<8, 4, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        default:
+            return fail(FW_ERR_INVALID, "cc metric: radius must be in 1..=8 (BOX_RADIUS_MAX)");
+    }
 }
 
 }  // namespace
 
-// d_result receives [value, sum |d_fixed|^2, sum |d_moving|^2].
+// d_result receives [value, sum |d_fixed|^2, sum |d_moving|^2] and, with `valid`, the number of
+// valid voxels in d_result[3].
 int launch_cc_pair_impl(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
-                        fw_field* d_fixed, fw_field* d_moving, double* d_result, int want_norms) {
+                        fw_field* d_fixed, fw_field* d_moving, double* d_result, int want_norms,
+                        const fw_image* valid) {
     CcArgs a;
     std::memset(&a, 0, sizeof(a));
     a.g = dev_grid(fixed->grid);
@@ -396,20 +483,11 @@ int launch_cc_pair_impl(fw_ctx* ctx, const fw_image* fixed, const fw_image* movi
     for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c)
             if (g.dir[r * 3 + c] != (r == c ? 1.0 : 0.0)) a.identity_dir = 0;
-    const float* f = fixed->d;
-    const float* m = moving->d;
-    switch (radius) {
-        case 1: return launch_r<1, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
-        case 2: return launch_r<2, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
-        case 3: return launch_r<3, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
-        case 4: return launch_r<4, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
-        case 5: return launch_r<5, 8>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
-        case 6: return launch_r<6, 4>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
-        case 7: return launch_r<7, 4>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
-        case 8: return launch_r<8, 4>(ctx, a, f, m, d_fixed->d, d_moving->d, d_result, want_norms);
-        default:
-            return fail(FW_ERR_INVALID, "cc metric: radius must be in 1..=8 (BOX_RADIUS_MAX)");
-    }
+    if (valid)
+        return launch_radius<true>(ctx, a, radius, fixed->d, moving->d, valid->d, d_fixed->d,
+                                   d_moving->d, d_result, want_norms);
+    return launch_radius<false>(ctx, a, radius, fixed->d, moving->d, nullptr, d_fixed->d,
+                                d_moving->d, d_result, want_norms);
 }
 
 int launch_cc_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
@@ -426,11 +504,13 @@ using namespace fw;
 extern "C" {
 
 static int cc_pair_common(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
-                          int32_t radius, double values[2], fw_field** d_fixed,
-                          fw_field** d_moving, double norms[2]) {
+                          const fw_image* valid, int32_t radius, double values[2],
+                          fw_field** d_fixed, fw_field** d_moving, double norms[2]) {
     FW_CHECK(ctx && fixed && moving && values && d_fixed && d_moving, "null argument");
     if (!fixed->grid.same(moving->grid))
         return fail(FW_ERR_INVALID, "cc metric: the images are not on one grid");
+    if (valid && !valid->grid.same(fixed->grid))
+        return fail(FW_ERR_INVALID, "cc metric: the mask is not on the virtual grid");
     fw_field *a = nullptr, *b = nullptr;
     FW_TRY(new_field(ctx, fixed->grid, &a));
     int rc = new_field(ctx, fixed->grid, &b);
@@ -438,10 +518,12 @@ static int cc_pair_common(fw_ctx* ctx, const fw_image* fixed, const fw_image* mo
         fw_field_free(a);
         return rc;
     }
-    double* slot = ctx->d_scratch + SLOT_CC_VALUE;  // [value, nf, nm] at SLOT_CC_VALUE.. +2
-    rc = launch_cc_pair_impl(ctx, fixed, moving, radius, a, b, slot, 1);
-    double r[3] = {0, 0, 0};
-    if (!rc) rc = read_back(ctx, slot, 3, r);
+    // [value, nf, nm, valid voxels] at SLOT_CC_VALUE .. SLOT_CC_VALID
+    double* slot = ctx->d_scratch + SLOT_CC_VALUE;
+    rc = launch_cc_pair_impl(ctx, fixed, moving, radius, a, b, slot, 1, valid);
+    double r[4] = {0, 0, 0, 0};
+    if (!rc) rc = read_back(ctx, slot, valid ? 4 : 3, r);
+    if (!rc && valid && r[3] == 0.0) rc = fail(FW_ERR_INVALID, std::string("cc metric: ") + FW_NO_VOXEL_IN_MASKS);
     if (rc) {
         fw_field_free(a);
         fw_field_free(b);
@@ -461,7 +543,7 @@ static int cc_pair_common(fw_ctx* ctx, const fw_image* fixed, const fw_image* mo
 int fw_cc_value_derivative_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
                                 int32_t radius, double values[2], fw_field** d_fixed,
                                 fw_field** d_moving) {
-    return cc_pair_common(ctx, fixed, moving, radius, values, d_fixed, d_moving, nullptr);
+    return cc_pair_common(ctx, fixed, moving, nullptr, radius, values, d_fixed, d_moving, nullptr);
 }
 
 int fw_cc_value_derivative_pair_with_norms(fw_ctx* ctx, const fw_image* fixed,
@@ -469,7 +551,23 @@ int fw_cc_value_derivative_pair_with_norms(fw_ctx* ctx, const fw_image* fixed,
                                            double values[2], fw_field** d_fixed,
                                            fw_field** d_moving, double norms[2]) {
     FW_CHECK(norms, "null norms");
-    return cc_pair_common(ctx, fixed, moving, radius, values, d_fixed, d_moving, norms);
+    return cc_pair_common(ctx, fixed, moving, nullptr, radius, values, d_fixed, d_moving, norms);
+}
+
+int fw_cc_value_derivative_pair_masked(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                                       const fw_image* valid, int32_t radius, double values[2],
+                                       fw_field** d_fixed, fw_field** d_moving) {
+    FW_CHECK(valid, "null mask");
+    return cc_pair_common(ctx, fixed, moving, valid, radius, values, d_fixed, d_moving, nullptr);
+}
+
+int fw_cc_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* fixed,
+                                                  const fw_image* moving, const fw_image* valid,
+                                                  int32_t radius, double values[2],
+                                                  fw_field** d_fixed, fw_field** d_moving,
+                                                  double norms[2]) {
+    FW_CHECK(valid && norms, "null argument");
+    return cc_pair_common(ctx, fixed, moving, valid, radius, values, d_fixed, d_moving, norms);
 }
 
 int fw_cc_value_derivative(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
@@ -477,7 +575,7 @@ int fw_cc_value_derivative(fw_ctx* ctx, const fw_image* fixed, const fw_image* m
     FW_CHECK(value && derivative, "null argument");
     double v[2];
     fw_field *a = nullptr, *b = nullptr;
-    FW_TRY(cc_pair_common(ctx, fixed, moving, radius, v, &a, &b, nullptr));
+    FW_TRY(cc_pair_common(ctx, fixed, moving, nullptr, radius, v, &a, &b, nullptr));
     fw_field_free(b);
     *value = v[0];
     *derivative = a;
@@ -527,7 +625,7 @@ int noalloc_scratch(int device, NoAllocScratch** out) {
 template <int R, int TY>
 int noalloc_launch(const CcArgs& a0, int num_sms, const float* f, const float* m, float* df,
                    float* dm, double* result, NoAllocScratch* s, cudaStream_t stream) {
-    using L = Layout<R, TY>;
+    using L = Layout<R, TY, false>;
     CcArgs a = a0;
     dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, 1);
     long long tiles = (long long)grid.x * grid.y;
@@ -544,10 +642,10 @@ int noalloc_launch(const CcArgs& a0, int num_sms, const float* f, const float* m
                         " the static scratch holds (use fw_cc_value_derivative_pair)");
     // the last-block counter must start at zero whatever the previous call left
     FW_CUDA(cudaMemsetAsync(s->counter, 0, sizeof(unsigned int), stream));
-    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)L::bytes));
-    k_cc_pair<R, TY><<<grid, L::NT, L::bytes, stream>>>(a, f, m, df, dm, s->partials, s->counter,
-                                                         result, 1);
+    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes));
+    k_cc_pair<R, TY, false><<<grid, L::NT, L::bytes, stream>>>(a, f, m, nullptr, df, dm,
+                                                                s->partials, s->counter, result, 1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_cc_pair (no alloc)");
     return 0;

@@ -272,8 +272,18 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
 int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, InvState* st,
                            cudaGraphConditionalHandle handle, int use_handle);
 int read_back(fw_ctx* ctx, const double* d, int k, double* out);
+// The SyN stage on device images (fw_syn.cu); masks may be null.
+int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
+                   const fw_image* const* moving, const fw_image* fixed_mask,
+                   const fw_image* moving_mask, const fw_affine* initial, fw_field** warp,
+                   fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
+                   int64_t* count);
+
+// d_result: [value, sum |d_fixed|^2, sum |d_moving|^2] and, with `valid` (the masked metric:
+// voxels where it is not zero), the number of valid voxels at d_result[3].
 int launch_cc_pair_impl(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
-                        fw_field* d_fixed, fw_field* d_moving, double* d_result, int want_norms);
+                        fw_field* d_fixed, fw_field* d_moving, double* d_result, int want_norms,
+                        const fw_image* valid = nullptr);
 
 // Gaussian taps of ITK's GaussianOperator (field_ops.rs:478-506), f64.
 std::vector<double> gaussian_taps(double variance, double max_error, int64_t max_width);
@@ -285,6 +295,7 @@ enum Slot : int {
     SLOT_CC_VALUE = 2,   // -mean(localCC)
     SLOT_NORM_A = 3,     // sum u.u of derivative a
     SLOT_NORM_B = 4,
+    SLOT_CC_VALID = 5,   // valid voxels of the masked CC
     SLOT_INV = 8,        // inversion state (8 doubles)
     SLOT_MI = 32,        // MI scalars
     SLOT_PARTIALS = 128, // block partials follow

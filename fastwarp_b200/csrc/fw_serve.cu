@@ -21,13 +21,6 @@
 #include "../../include/fastwarp_serve.h"
 #include "fw_internal.cuh"
 
-namespace fw {
-int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
-                   const fw_image* const* moving, const fw_affine* initial, fw_field** warp,
-                   fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
-                   int64_t* count);
-}
-
 using Clock = std::chrono::steady_clock;
 
 namespace {
@@ -140,7 +133,8 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
     int64_t count = 0;
     fw_field *w = nullptr, *iw = nullptr;
     if (!rc)
-        rc = syn_run_device(ctx, &q.recipe, fi.data(), mi.data(), q.has_initial ? &q.initial : nullptr,
+        rc = syn_run_device(ctx, &q.recipe, fi.data(), mi.data(), nullptr, nullptr,
+                            q.has_initial ? &q.initial : nullptr,
                             &w, &iw, recs.data(), (int64_t)recs.size(), &count);
     for (auto* im : up) fw_image_free(im);
     if (!rc) {

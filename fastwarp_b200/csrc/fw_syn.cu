@@ -35,7 +35,8 @@ struct SynDev {
     int it;          // iterations done in this level
     int limit;       // iteration limit of this level
     int converged;
-    int status;      // 0 ok, 1 gradient not finite, 2 field not finite, 3 cancelled
+    int status;      // 0 ok, 1 gradient not finite, 2 field not finite, 3 cancelled,
+                     // 4 no voxel inside the masks
     int level;
     int window;
     int count;       // values in the window
@@ -45,7 +46,7 @@ struct SynDev {
     double threshold;
     double step;
     int channels;
-    int pad;
+    int masked;      // the CC pairs take the masks' valid voxels
     double wnorm[FW_MAX_CHANNELS];
 };
 
@@ -92,7 +93,8 @@ __global__ void k_syn_level_init(SynDev* s, int level, int limit) {
     s->total = 0.0;
 }
 
-// cc: [channel][value, |dF|^2, |dM|^2]; max_bits: [F side, M side]; inv: 4 loop states.
+// cc: [channel][value, |dF|^2, |dM|^2, valid voxels]; max_bits: [F side, M side]; inv: 4 loop
+// states.
 __global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
                              const unsigned int* __restrict__ max_bits,
                              const InvState* __restrict__ inv, fw_syn_iteration* trace,
@@ -100,10 +102,12 @@ __global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
                              cudaGraphConditionalHandle handle, int use_handle) {
     double vF = cc[0], vM = cc[0];  // the CC value is symmetric in its two images
     double weighted = 0.0;
-    for (int c = 0; c < s->channels; ++c) weighted += cc[3 * c] * s->wnorm[c];
+    for (int c = 0; c < s->channels; ++c) weighted += cc[4 * c] * s->wnorm[c];
     if (s->channels == 1) weighted = vF;
     for (int c = 0; c < s->channels && s->channels > 1; ++c)
-        if (!isfinite(cc[3 * c + 1]) || !isfinite(cc[3 * c + 2])) s->status = 1;
+        if (!isfinite(cc[4 * c + 1]) || !isfinite(cc[4 * c + 2])) s->status = 1;
+    for (int c = 0; c < s->channels && s->masked; ++c)
+        if (cc[4 * c + 3] == 0.0) s->status = 4;
     float mF = __uint_as_float(max_bits[0]), mM = __uint_as_float(max_bits[1]);
     if (!isfinite(mF) || !isfinite(mM)) s->status = 1;
     for (int q = 0; q < 4; ++q)
@@ -164,7 +168,7 @@ __global__ void k_scale_norms(float4* __restrict__ acc, long long n4, const doub
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= n4) return;
     double tot = 0.0;
-    for (int c = 0; c < channels; ++c) tot += sqrt(cc[3 * c + which]);
+    for (int c = 0; c < channels; ++c) tot += sqrt(cc[4 * c + which]);
     float s = (float)(tot / channels);
     float4 v = acc[l];
     v.x *= s;
@@ -183,6 +187,9 @@ struct Level {
     fw_field *accF = nullptr, *accM = nullptr;  // multichannel combination
     fw_field *sF = nullptr, *sM = nullptr;      // smoothed updates
     fw_field* T = nullptr;                      // total-field smoothing
+    const fw_image* fmask = nullptr;            // recipe masks on their own grids (or none)
+    const fw_image* mmask = nullptr;
+    fw_image* valid = nullptr;                  // the masks resolved on the level grid
 };
 
 void free_level_work(Level& L) {
@@ -190,6 +197,8 @@ void free_level_work(Level& L) {
     for (auto* im : L.mmid) fw_image_free(im);
     L.fmid.clear();
     L.mmid.clear();
+    fw_image_free(L.valid);
+    L.valid = nullptr;
     fw_field* fs[] = {L.dF, L.dM, L.accF, L.accM, L.sF, L.sM, L.T};
     for (auto* f : fs) fw_field_free(f);
     L.dF = L.dM = L.accF = L.accM = L.sF = L.sM = L.T = nullptr;
@@ -214,13 +223,14 @@ int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
         FW_TRY(new_field(ctx, L.grid, &L.sM));
     }
     if (r->total_field_variance > 0.0) FW_TRY(new_field(ctx, L.grid, &L.T));
+    if (L.fmask || L.mmask) FW_TRY(new_image(ctx, L.grid, &L.valid));
     return 0;
 }
 
 // Device scalars of a run.
 struct RunDev {
     SynDev* syn;
-    double* cc;              // [channels][3]
+    double* cc;              // [channels][4]
     unsigned int* max_bits;  // [2]
     InvState* inv;           // [4]
     fw_syn_iteration* trace;
@@ -315,20 +325,27 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
     double wsum = 0.0;
     for (int c = 0; c < C; ++c) wsum += r->channel_weights[c];
     const long long n4 = 3 * L.dF->ps / 4;
+    // syn.rs:555-580: the voxels of the level grid inside both masks (nearest voxel, half up):
+    // the fixed mask through F^-1, times the moving mask through affine(M^-1)
+    if (L.fmask)
+        FW_TRY(launch_warp(ctx, L.fmask, L.Fi, nullptr, nullptr, L.valid->d, true, nullptr));
+    if (L.mmask)
+        FW_TRY(launch_warp(ctx, L.mmask, L.Mi, nullptr, initial, L.valid->d, true,
+                           L.fmask ? L.valid->d : nullptr));
     for (int c = 0; c < C; ++c) {
         FW_TRY(launch_warp(ctx, fs[c], L.Fi, nullptr, nullptr, L.fmid[c]->d, false, nullptr));
         FW_TRY(launch_warp(ctx, ms[c], L.Mi, nullptr, initial, L.mmid[c]->d, false, nullptr));
         FW_TRY(launch_cc_pair_impl(ctx, L.fmid[c], L.mmid[c], r->cc_radius, L.dF, L.dM,
-                                   d.cc + 3 * c, C > 1 ? 1 : 0));
+                                   d.cc + 4 * c, C > 1 ? 1 : 0, L.valid));
         if (C > 1) {
             double wn = r->channel_weights[c] / wsum;
             k_axpy_norm<<<blocks256(n4), 256, 0, ctx->stream>>>((float4*)L.accF->d,
                                                                 (const float4*)L.dF->d, n4,
-                                                                d.cc + 3 * c + 1, wn);
+                                                                d.cc + 4 * c + 1, wn);
             FW_TRY(check_launch(ctx, "k_axpy_norm"));
             k_axpy_norm<<<blocks256(n4), 256, 0, ctx->stream>>>((float4*)L.accM->d,
                                                                 (const float4*)L.dM->d, n4,
-                                                                d.cc + 3 * c + 2, wn);
+                                                                d.cc + 4 * c + 2, wn);
             FW_TRY(check_launch(ctx, "k_axpy_norm"));
         }
     }
@@ -486,9 +503,10 @@ struct RunScratch {
     }
 };
 
-int upload_syn_dev(fw_ctx* ctx, const fw_syn_recipe* r, SynDev* d) {
+int upload_syn_dev(fw_ctx* ctx, const fw_syn_recipe* r, SynDev* d, bool masked) {
     SynDev h;
     std::memset(&h, 0, sizeof(h));
+    h.masked = masked ? 1 : 0;
     h.window = r->convergence_window;
     h.threshold = r->convergence_threshold;
     h.step = r->gradient_step;
@@ -591,25 +609,61 @@ int check_status(int status) {
         case 1: return fail(FW_ERR_NOT_FINITE, "syn: the metric gradient is not finite");
         case 2: return fail(FW_ERR_NOT_FINITE, "syn: the displacement field is not finite");
         case 3: return fail(FW_ERR_CANCELLED, "registration cancelled");
+        case 4: return fail(FW_ERR_INVALID, std::string("cc metric: ") + FW_NO_VOXEL_IN_MASKS);
         default: return fail(FW_ERR_INVALID, "syn: unknown device status");
     }
 }
 
 // Kernels per iteration outside the inversion bodies (for the launch counter).
-int kernels_per_iteration(const fw_syn_recipe* r) {
+int kernels_per_iteration(const fw_syn_recipe* r, int mask_warps) {
     int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) + 2 /*smooth or max*/ +
             2 /*compose*/ + (r->total_field_variance > 0.0 ? 2 : 0) + 4 * 2 /*inv init+measure*/ +
-            1 /*record*/;
+            1 /*record*/ + mask_warps;
     return k;
+}
+
+__global__ void k_count_nonzero(const float* __restrict__ a, long long n, unsigned int* count) {
+    unsigned int c = 0;
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < n;
+         l += (long long)gridDim.x * blockDim.x)
+        c += a[l] != 0.0f;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+// recipe.rs:239-246: a given mask must have a voxel inside.
+int check_masks(fw_ctx* ctx, const fw_image* fmask, const fw_image* mmask) {
+    const fw_image* ms[2] = {fmask, mmask};
+    const char* names[2] = {"fixed", "moving"};
+    for (int q = 0; q < 2; ++q) {
+        if (!ms[q]) continue;
+        unsigned int* cnt = ctx->d_counter + 48;
+        FW_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned int), ctx->stream));
+        long long n = ms[q]->grid.count();
+        unsigned int blocks = (unsigned int)std::min<long long>((n + 255) / 256, 4LL * ctx->num_sms);
+        k_count_nonzero<<<std::max(blocks, 1u), 256, 0, ctx->stream>>>(ms[q]->d, n, cnt);
+        FW_TRY(check_launch(ctx, "k_count_nonzero"));
+        FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, cnt, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        FW_TRY(sync(ctx));
+        unsigned int h = 0;
+        std::memcpy(&h, ctx->h_pinned, sizeof(h));
+        if (h == 0)
+            return fail(FW_ERR_INVALID, std::string("syn recipe: the ") + names[q] +
+                                            " mask has no voxel inside (every voxel is zero)");
+    }
+    return 0;
 }
 
 }  // namespace
 
 int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
-                   const fw_image* const* moving, const fw_affine* initial, fw_field** warp,
+                   const fw_image* const* moving, const fw_image* fixed_mask,
+                   const fw_image* moving_mask, const fw_affine* initial, fw_field** warp,
                    fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
                    int64_t* count) {
     FW_TRY(syn_validate(r));
+    FW_TRY(check_masks(ctx, fixed_mask, moving_mask));
     const int C = r->channels;
     for (int c = 0; c < C; ++c) FW_CHECK(fixed[c] && moving[c], "syn: null channel image");
     const HostGrid fg = fixed[0]->grid;
@@ -621,9 +675,11 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
     FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)(1 << 20)));
     RunScratch rs;
     FW_TRY(rs.init(ctx, C, std::max(total_iters, 1)));
-    FW_TRY(upload_syn_dev(ctx, r, rs.d.syn));
+    FW_TRY(upload_syn_dev(ctx, r, rs.d.syn, fixed_mask || moving_mask));
     Level L;
     L.channels = C;
+    L.fmask = fixed_mask;
+    L.mmask = moving_mask;
     HostGrid prev;
     bool have_prev = false;
     std::vector<fw_image*> owned;
@@ -724,7 +780,8 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
                     for (int s = 0; s < 4; ++s)
                         ctx->stats.kernel_launches += records[done + q].inversions[s].iterations;
             }
-            ctx->stats.kernel_launches += (uint64_t)ran * kernels_per_iteration(r) + 1;
+            ctx->stats.kernel_launches +=
+                (uint64_t)ran * kernels_per_iteration(r, (fixed_mask ? 1 : 0) + (moving_mask ? 1 : 0)) + 1;
             done += ran;
             rc = check_status(h.status);
         }
@@ -789,14 +846,26 @@ int fw_syn_step(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const*
                 const fw_image* const* moving, const fw_affine* initial, fw_field* f2m,
                 fw_field* f2m_inv, fw_field* m2m, fw_field* m2m_inv, double* fixed_update,
                 double* moving_update, fw_syn_iteration* record) {
+    return fw_syn_step_masked(ctx, recipe, fixed, moving, nullptr, nullptr, initial, f2m, f2m_inv,
+                              m2m, m2m_inv, fixed_update, moving_update, record);
+}
+
+int fw_syn_step_masked(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const* fixed,
+                       const fw_image* const* moving, const fw_image* fixed_mask,
+                       const fw_image* moving_mask, const fw_affine* initial, fw_field* f2m,
+                       fw_field* f2m_inv, fw_field* m2m, fw_field* m2m_inv, double* fixed_update,
+                       double* moving_update, fw_syn_iteration* record) {
     FW_CHECK(ctx && recipe && fixed && moving && f2m && f2m_inv && m2m && m2m_inv, "null argument");
     FW_TRY(syn_validate(recipe));
+    FW_TRY(check_masks(ctx, fixed_mask, moving_mask));
     const HostGrid& g = f2m->grid;
     FW_CHECK(f2m_inv->grid.same(g) && m2m->grid.same(g) && m2m_inv->grid.same(g),
              "syn: the state fields differ in grid");
     FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)(1 << 20)));
     Level L;
     L.channels = recipe->channels;
+    L.fmask = fixed_mask;
+    L.mmask = moving_mask;
     L.grid = g;
     L.F = f2m;
     L.Fi = f2m_inv;
@@ -805,7 +874,7 @@ int fw_syn_step(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const*
     int rc = alloc_level_work(ctx, recipe, L);
     RunScratch rs;
     if (!rc) rc = rs.init(ctx, L.channels, 1);
-    if (!rc) rc = upload_syn_dev(ctx, recipe, rs.d.syn);
+    if (!rc) rc = upload_syn_dev(ctx, recipe, rs.d.syn, fixed_mask || moving_mask);
     std::vector<const fw_image*> fs(fixed, fixed + L.channels), ms(moving, moving + L.channels);
     if (!rc) {
         k_syn_level_init<<<1, 1, 0, ctx->stream>>>(rs.d.syn, 0, 1);
@@ -846,8 +915,18 @@ int fw_syn_run_device(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* 
                       fw_field** warp, fw_field** inverse_warp, fw_syn_iteration* records,
                       int64_t cap, int64_t* count) {
     FW_CHECK(ctx && recipe && fixed && moving && warp && inverse_warp, "null argument");
-    return syn_run_device(ctx, recipe, fixed, moving, initial, warp, inverse_warp, records, cap,
-                          count);
+    return syn_run_device(ctx, recipe, fixed, moving, nullptr, nullptr, initial, warp,
+                          inverse_warp, records, cap, count);
+}
+
+int fw_syn_run_device_masked(fw_ctx* ctx, const fw_syn_recipe* recipe,
+                             const fw_image* const* fixed, const fw_image* const* moving,
+                             const fw_image* fixed_mask, const fw_image* moving_mask,
+                             const fw_affine* initial, fw_field** warp, fw_field** inverse_warp,
+                             fw_syn_iteration* records, int64_t cap, int64_t* count) {
+    FW_CHECK(ctx && recipe && fixed && moving && warp && inverse_warp, "null argument");
+    return syn_run_device(ctx, recipe, fixed, moving, fixed_mask, moving_mask, initial, warp,
+                          inverse_warp, records, cap, count);
 }
 
 int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_grid,
@@ -867,7 +946,8 @@ int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_gr
     fw_field *w = nullptr, *iw = nullptr;
     if (!rc) {
         std::vector<const fw_image*> cf(fi.begin(), fi.end()), cm(mi.begin(), mi.end());
-        rc = syn_run_device(ctx, recipe, cf.data(), cm.data(), initial, &w, &iw, records, cap, count);
+        rc = syn_run_device(ctx, recipe, cf.data(), cm.data(), nullptr, nullptr, initial, &w, &iw,
+                            records, cap, count);
     }
     if (!rc) rc = fw_field_download_f32(ctx, w, warp);
     if (!rc) rc = fw_field_download_f32(ctx, iw, inverse_warp);

@@ -96,8 +96,19 @@ def _records(recs, n):
 
 
 def run_syn(backend: CudaBackend, recipe: SynRecipe, fixed_grid: N.Grid, fixed: list,
-            moving_grid: N.Grid, moving: list, initial: N.Affine | None = None) -> SynResult:
-    """run_syn (syn.rs:555-564) from host images (one float array per channel)."""
+            moving_grid: N.Grid, moving: list, initial: N.Affine | None = None,
+            fixed_mask=None, moving_mask=None) -> SynResult:
+    """run_syn (syn.rs:555-564) from host images (one float array per channel). Masks are
+    (grid, array) pairs on any grid (recipe.rs fixed_mask / moving_mask) or None."""
+    if fixed_mask is not None or moving_mask is not None:
+        fi = [backend.upload_image(fixed_grid, a) for a in fixed]
+        mi = [backend.upload_image(moving_grid, a) for a in moving]
+        fm = None if fixed_mask is None else backend.upload_image(*fixed_mask)
+        mm = None if moving_mask is None else backend.upload_image(*moving_mask)
+        w, iw, recs = run_syn_device(backend, recipe, fi, mi, initial, fm, mm)
+        last = level_grid(recipe, fixed_grid, recipe.to_c().levels - 1)
+        return SynResult(backend.download_field(w).astype(np.float32),
+                         backend.download_field(iw).astype(np.float32), last, recs)
     r = recipe.to_c()
     fs = [np.ascontiguousarray(a, np.float32) for a in fixed]
     ms = [np.ascontiguousarray(a, np.float32) for a in moving]
@@ -119,7 +130,8 @@ def run_syn(backend: CudaBackend, recipe: SynRecipe, fixed_grid: N.Grid, fixed: 
 
 
 def run_syn_device(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
-                   moving: List[Image], initial: N.Affine | None = None):
+                   moving: List[Image], initial: N.Affine | None = None,
+                   fixed_mask: Image | None = None, moving_mask: Image | None = None):
     """The same on device-resident images; returns (warp Field, inverse Field, records)."""
     r = recipe.to_c()
     fp = (C.c_void_p * len(fixed))(*[im.handle.value for im in fixed])
@@ -128,10 +140,12 @@ def run_syn_device(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
     recs = (N.SynIteration * cap)()
     count = C.c_int64()
     w, iw = C.c_void_p(), C.c_void_p()
-    check(lib().fw_syn_run_device(backend.ctx, C.byref(r), fp, mp,
-                                  None if initial is None else C.byref(initial),
-                                  C.byref(w), C.byref(iw), recs, C.c_int64(cap),
-                                  C.byref(count)))
+    check(lib().fw_syn_run_device_masked(backend.ctx, C.byref(r), fp, mp,
+                                         None if fixed_mask is None else fixed_mask.handle,
+                                         None if moving_mask is None else moving_mask.handle,
+                                         None if initial is None else C.byref(initial),
+                                         C.byref(w), C.byref(iw), recs, C.c_int64(cap),
+                                         C.byref(count)))
     return Field(backend, w), Field(backend, iw), _records(recs, min(count.value, cap))
 
 
@@ -273,7 +287,8 @@ def run_syn_ops(backend: CudaBackend, recipe: SynRecipe, fixed_grid: N.Grid, fix
 
 
 def syn_step(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image], moving: List[Image],
-             initial: N.Affine | None, state: dict, want_updates: bool = True):
+             initial: N.Affine | None, state: dict, want_updates: bool = True,
+             fixed_mask: Image | None = None, moving_mask: Image | None = None):
     """One SyN iteration (syn.rs:890-958) on device-resident state fields f2m, f2m_inv, m2m,
     m2m_inv (updated in place). Returns (record, fixed_update, moving_update)."""
     r = recipe.to_c()
@@ -284,7 +299,9 @@ def syn_step(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image], moving
     fu = np.zeros(shape) if want_updates else None
     mu = np.zeros(shape) if want_updates else None
     rec = N.SynIteration()
-    check(lib().fw_syn_step(backend.ctx, C.byref(r), fp, mp,
+    check(lib().fw_syn_step_masked(backend.ctx, C.byref(r), fp, mp,
+                            None if fixed_mask is None else fixed_mask.handle,
+                            None if moving_mask is None else moving_mask.handle,
                             None if initial is None else C.byref(initial),
                             state["f2m"].handle, state["f2m_inv"].handle, state["m2m"].handle,
                             state["m2m_inv"].handle,

@@ -100,7 +100,7 @@ typedef struct fw_linear_transform {
     double center[3];
 } fw_linear_transform;
 
-/* SynRecipe, recipe.rs:52-100 (CC channels, no masks). */
+/* SynRecipe, recipe.rs:52-100 (CC channels; masks are passed beside it as images). */
 #define FW_MAX_LEVELS 8
 #define FW_MAX_CHANNELS 4
 typedef struct fw_syn_recipe {
@@ -223,6 +223,24 @@ int fw_cc_value_derivative_pair_with_norms(fw_ctx* ctx, const fw_image* fixed,
                                            double values[2], fw_field** d_fixed,
                                            fw_field** d_moving, double norms[2]);
 
+/* Backend::cc_value_derivative_pair_masked (backend.rs:128-140; cpu/mod.rs:134-163 ->
+ * metric/cc.rs:170-321 with Some(valid)): only voxels where `valid` (on the images' grid) is not
+ * zero enter the window sums and their count; other voxels get a zero derivative; each value is
+ * the mean over the valid voxels. No valid voxel: FW_ERR_INVALID with FW_NO_VOXEL_IN_MASKS in
+ * the message (metric/cc.rs:49-50). */
+#define FW_NO_VOXEL_IN_MASKS \
+    "no voxel of the registration level lies inside both the fixed and the moving mask"
+int fw_cc_value_derivative_pair_masked(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                                       const fw_image* valid, int32_t radius, double values[2],
+                                       fw_field** d_fixed, fw_field** d_moving);
+
+/* Backend::cc_value_derivative_pair_masked_with_norms (backend.rs:142-152). */
+int fw_cc_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* fixed,
+                                                  const fw_image* moving, const fw_image* valid,
+                                                  int32_t radius, double values[2],
+                                                  fw_field** d_fixed, fw_field** d_moving,
+                                                  double norms[2]);
+
 /* No counterpart in the reference. The CC pair above for callers that cannot allocate device
  * memory: code recording into a CUDA stream capture (an allocation there breaks the capture),
  * hosts whose own pool allocator owns the GPU's memory (a framework's caching allocator, a server
@@ -328,6 +346,22 @@ int fw_syn_run_device(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* 
                       const fw_image* const* moving, const fw_affine* initial,
                       fw_field** warp, fw_field** inverse_warp, fw_syn_iteration* records,
                       int64_t cap, int64_t* count);
+
+/* The same two with the recipe's masks (recipe.rs fixed_mask / moving_mask, each on its own
+ * grid, either may be NULL): every iteration resolves them on the level grid (syn.rs:555-580:
+ * the fixed mask through F^-1, times the moving mask through affine(M^-1), nearest voxel) and
+ * the CC pairs take only those voxels. A given mask without a non-zero voxel is refused
+ * (recipe.rs:239-246); a level grid without a valid voxel fails with FW_NO_VOXEL_IN_MASKS. */
+int fw_syn_step_masked(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const* fixed,
+                       const fw_image* const* moving, const fw_image* fixed_mask,
+                       const fw_image* moving_mask, const fw_affine* initial, fw_field* f2m,
+                       fw_field* f2m_inv, fw_field* m2m, fw_field* m2m_inv, double* fixed_update,
+                       double* moving_update, fw_syn_iteration* record);
+int fw_syn_run_device_masked(fw_ctx* ctx, const fw_syn_recipe* recipe,
+                             const fw_image* const* fixed, const fw_image* const* moving,
+                             const fw_image* fixed_mask, const fw_image* moving_mask,
+                             const fw_affine* initial, fw_field** warp, fw_field** inverse_warp,
+                             fw_syn_iteration* records, int64_t cap, int64_t* count);
 
 /* run_syn from host float32 images: uploads, runs, and writes the two fields as AoS float32
  * (DisplacementField) on the grid of the last level (fw_syn_level_grid). */

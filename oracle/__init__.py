@@ -401,8 +401,30 @@ def _ptrs(arrs):
     return (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
 
 
+class SynMasks(C.Structure):
+    _fields_ = [("fixed_grid", C.POINTER(Grid)), ("fixed", C.POINTER(C.c_double)),
+                ("moving_grid", C.POINTER(Grid)), ("moving", C.POINTER(C.c_double))]
+
+
+def _masks(masks):
+    """masks = None or dict(fixed_grid, fixed, moving_grid, moving) (either side may be None).
+    Returns (struct or None, arrays kept alive)."""
+    if masks is None:
+        return None, []
+    keep = []
+    m = SynMasks()
+    for side in ("fixed", "moving"):
+        data = masks.get(side)
+        if data is not None:
+            arr = _f64(data)
+            keep.append(arr)
+            setattr(m, side, arr.ctypes.data_as(C.POINTER(C.c_double)))
+            setattr(m, side + "_grid", C.pointer(masks[side + "_grid"]))
+    return m, keep
+
+
 def syn_step(recipe, level_grid, fixed_grid, fixed_smooth, moving_grid, moving_smooth, initial,
-             state):
+             state, masks=None):
     """One SyN iteration from ``state`` = dict(f2m, f2m_inv, m2m, m2m_inv) (updated in place).
     Returns (record, fixed_update, moving_update)."""
     fs = [_f64(a) for a in fixed_smooth]
@@ -412,15 +434,18 @@ def syn_step(recipe, level_grid, fixed_grid, fixed_smooth, moving_grid, moving_s
     rec = SynIteration()
     for k in ("f2m", "f2m_inv", "m2m", "m2m_inv"):
         state[k] = _f64(state[k])
-    _check(lib().fwo_syn_step(C.byref(recipe), C.byref(level_grid), C.byref(fixed_grid),
-                              _ptrs(fs), C.byref(moving_grid), _ptrs(ms),
-                              None if initial is None else C.byref(initial),
-                              _p(state["f2m"]), _p(state["f2m_inv"]), _p(state["m2m"]),
-                              _p(state["m2m_inv"]), _p(fu), _p(mu), C.byref(rec)))
+    cm, _keep = _masks(masks)
+    _check(lib().fwo_syn_step_masked(C.byref(recipe), C.byref(level_grid), C.byref(fixed_grid),
+                                     _ptrs(fs), C.byref(moving_grid), _ptrs(ms),
+                                     None if initial is None else C.byref(initial),
+                                     None if cm is None else C.byref(cm),
+                                     _p(state["f2m"]), _p(state["f2m_inv"]), _p(state["m2m"]),
+                                     _p(state["m2m_inv"]), _p(fu), _p(mu), C.byref(rec)))
     return rec, fu, mu
 
 
-def syn_run(recipe, fixed_grid, fixed, moving_grid, moving, initial=None, cap=100000):
+def syn_run(recipe, fixed_grid, fixed, moving_grid, moving, initial=None, cap=100000,
+            masks=None):
     """Whole SyN stage; fixed/moving are lists (one image per channel)."""
     fs = [_f64(a) for a in fixed]
     ms = [_f64(a) for a in moving]
@@ -429,10 +454,12 @@ def syn_run(recipe, fixed_grid, fixed, moving_grid, moving, initial=None, cap=10
     warp_out, inv_out = np.zeros(shape), np.zeros(shape)
     recs = (SynIteration * cap)()
     count = C.c_int64()
-    _check(lib().fwo_syn_run(C.byref(recipe), C.byref(fixed_grid), _ptrs(fs),
-                             C.byref(moving_grid), _ptrs(ms),
-                             None if initial is None else C.byref(initial), _p(warp_out),
-                             _p(inv_out), recs, C.c_int64(cap), C.byref(count)))
+    cm, _keep = _masks(masks)
+    _check(lib().fwo_syn_run_masked(C.byref(recipe), C.byref(fixed_grid), _ptrs(fs),
+                                    C.byref(moving_grid), _ptrs(ms),
+                                    None if initial is None else C.byref(initial),
+                                    None if cm is None else C.byref(cm), _p(warp_out),
+                                    _p(inv_out), recs, C.c_int64(cap), C.byref(count)))
     return warp_out, inv_out, [recs[i] for i in range(min(count.value, cap))], last
 
 

@@ -1610,11 +1610,13 @@ int fwo_syn_level_grid(const fwo_syn_recipe* r, const fwo_grid* fixed_grid, int3
 namespace {
 
 // syn.rs:337-420 (side_updates) + 422-445 (update_total_field) + 890-958 (one iteration).
+// With masks, syn.rs:555-580 (StageMasks::validity): the fixed mask resampled (nearest voxel)
+// through F^-1, times the moving mask through affine(M^-1); the CC pair takes only those voxels.
 int syn_iteration(const fwo_syn_recipe* r, const Grid& lg, const Grid& fg,
                   const double* const* fixed_s, const Grid& mg, const double* const* moving_s,
-                  const fwo_affine* initial, double* f2m, double* f2m_inv, double* m2m,
-                  double* m2m_inv, double* fixed_update_out, double* moving_update_out,
-                  fwo_syn_iteration* rec) {
+                  const fwo_affine* initial, const fwo_syn_masks* masks, double* f2m,
+                  double* f2m_inv, double* m2m, double* m2m_inv, double* fixed_update_out,
+                  double* moving_update_out, fwo_syn_iteration* rec) {
     int64_t n = lg.count();
     int channels = r->channels;
     double wsum = 0.0;
@@ -1625,14 +1627,26 @@ int syn_iteration(const fwo_syn_recipe* r, const Grid& lg, const Grid& fg,
     double totF = 0.0, totM = 0.0;
     std::vector<double> valsF, valsM;
     fwo_grid lgc = to_c(lg), fgc = to_c(fg), mgc = to_c(mg);
+    std::vector<double> valid;
+    const bool has_fm = masks && masks->fixed, has_mm = masks && masks->moving;
+    if (has_fm || has_mm) {
+        valid.resize(n);
+        if (has_fm && fwo_warp_mask(masks->fixed_grid, masks->fixed, &lgc, f2m_inv, nullptr,
+                                    nullptr, nullptr, nullptr, valid.data()))
+            return -1;
+        if (has_mm && fwo_warp_mask(masks->moving_grid, masks->moving, &lgc, m2m_inv, nullptr,
+                                    nullptr, initial, has_fm ? valid.data() : nullptr,
+                                    valid.data()))
+            return -1;
+    }
     for (int c = 0; c < channels; ++c) {
         if (fwo_warp(&fgc, fixed_s[c], &lgc, f2m_inv, nullptr, nullptr, nullptr, fmid.data()))
             return -1;
         if (fwo_warp(&mgc, moving_s[c], &lgc, m2m_inv, nullptr, nullptr, initial, mmid.data()))
             return -1;
         double vals[2];
-        if (fwo_cc_pair(&lgc, fmid.data(), mmid.data(), nullptr, r->cc_radius, vals, dF.data(),
-                        dM.data()))
+        if (fwo_cc_pair(&lgc, fmid.data(), mmid.data(), valid.empty() ? nullptr : valid.data(),
+                        r->cc_radius, vals, dF.data(), dM.data()))
             return -1;
         valsF.push_back(vals[0]);
         valsM.push_back(vals[1]);
@@ -1714,26 +1728,62 @@ int fwo_syn_step(const fwo_syn_recipe* r, const fwo_grid* level_grid,
                  const fwo_affine* initial, double* f2m, double* f2m_inv, double* m2m,
                  double* m2m_inv, double* fixed_update, double* moving_update,
                  fwo_syn_iteration* record) {
+    return fwo_syn_step_masked(r, level_grid, fixed_grid, fixed_smooth, moving_grid,
+                               moving_smooth, initial, nullptr, f2m, f2m_inv, m2m, m2m_inv,
+                               fixed_update, moving_update, record);
+}
+
+int fwo_syn_step_masked(const fwo_syn_recipe* r, const fwo_grid* level_grid,
+                        const fwo_grid* fixed_grid, const double* const* fixed_smooth,
+                        const fwo_grid* moving_grid, const double* const* moving_smooth,
+                        const fwo_affine* initial, const fwo_syn_masks* masks, double* f2m,
+                        double* f2m_inv, double* m2m, double* m2m_inv, double* fixed_update,
+                        double* moving_update, fwo_syn_iteration* record) {
     Grid lg, fg, mg;
     if (!make_grid(level_grid, lg) || !make_grid(fixed_grid, fg) || !make_grid(moving_grid, mg))
         return -1;
     fwo_syn_iteration rec{};
-    int rc = syn_iteration(r, lg, fg, fixed_smooth, mg, moving_smooth, initial, f2m, f2m_inv, m2m,
-                           m2m_inv, fixed_update, moving_update, &rec);
+    int rc = syn_iteration(r, lg, fg, fixed_smooth, mg, moving_smooth, initial, masks, f2m,
+                           f2m_inv, m2m, m2m_inv, fixed_update, moving_update, &rec);
     rec.convergence_value = DBL_MAX;
     if (record) *record = rec;
     return rc;
 }
 
-// syn.rs:776-986 -- syn_fields for a first SyN stage (no prior field, no masks).
+// syn.rs:776-986 -- syn_fields for a first SyN stage (no prior field).
 int fwo_syn_run(const fwo_syn_recipe* r, const fwo_grid* fixed_grid, const double* const* fixed,
                 const fwo_grid* moving_grid, const double* const* moving,
                 const fwo_affine* initial, double* warp, double* inverse_warp,
                 fwo_syn_iteration* records, int64_t cap, int64_t* count) {
+    return fwo_syn_run_masked(r, fixed_grid, fixed, moving_grid, moving, initial, nullptr, warp,
+                              inverse_warp, records, cap, count);
+}
+
+int fwo_syn_run_masked(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
+                       const double* const* fixed, const fwo_grid* moving_grid,
+                       const double* const* moving, const fwo_affine* initial,
+                       const fwo_syn_masks* masks, double* warp, double* inverse_warp,
+                       fwo_syn_iteration* records, int64_t cap, int64_t* count) {
     Grid fg, mg;
     if (!make_grid(fixed_grid, fg) || !make_grid(moving_grid, mg)) return -1;
     if (r->levels <= 0 || r->levels > FWO_MAX_LEVELS) return fail("bad level count");
     if (r->channels <= 0 || r->channels > FWO_MAX_CHANNELS) return fail("bad channel count");
+    // recipe.rs:239-246: a given mask must have a voxel inside
+    if (masks) {
+        const fwo_grid* mgs[2] = {masks->fixed_grid, masks->moving_grid};
+        const double* mds[2] = {masks->fixed, masks->moving};
+        const char* names[2] = {"fixed", "moving"};
+        for (int q = 0; q < 2; ++q) {
+            if (!mds[q]) continue;
+            Grid m;
+            if (!make_grid(mgs[q], m)) return -1;
+            bool any = false;
+            for (int64_t l = 0; l < m.count() && !any; ++l) any = mds[q][l] != 0.0;
+            if (!any)
+                return fail(std::string("syn recipe: the ") + names[q] +
+                            " mask has no voxel inside (every voxel is zero)");
+        }
+    }
     int channels = r->channels;
     std::vector<std::vector<double>> fs(channels), ms(channels);
     std::vector<double> f2m, f2m_inv, m2m, m2m_inv;
@@ -1787,7 +1837,7 @@ int fwo_syn_run(const fwo_syn_recipe* r, const fwo_grid* fixed_grid, const doubl
         while (current < r->iterations[level] && !converged) {
             ++current;
             fwo_syn_iteration rec{};
-            if (syn_iteration(r, lg, fg, fptr.data(), mg, mptr.data(), initial, f2m.data(),
+            if (syn_iteration(r, lg, fg, fptr.data(), mg, mptr.data(), initial, masks, f2m.data(),
                               f2m_inv.data(), m2m.data(), m2m_inv.data(), nullptr, nullptr, &rec))
                 return -1;
             monitor.add(rec.energy);

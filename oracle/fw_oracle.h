@@ -74,8 +74,8 @@ typedef struct fwo_linear_transform {
     double center[3];
 } fwo_linear_transform;
 
-/* SyN recipe, crates/fastwarp-reg/src/recipe.rs:52-100 (masks and Mattes channels are not part
- * of this restatement). */
+/* SyN recipe, crates/fastwarp-reg/src/recipe.rs:52-100 (Mattes channels are not part of this
+ * restatement; masks are passed beside it as fwo_syn_masks). */
 #define FWO_MAX_LEVELS 8
 #define FWO_MAX_CHANNELS 4
 typedef struct fwo_syn_recipe {
@@ -190,6 +190,26 @@ int fwo_syn_run(const fwo_syn_recipe* r, const fwo_grid* fixed_grid, const doubl
                 const fwo_grid* moving_grid, const double* const* moving,
                 const fwo_affine* initial, double* warp, double* inverse_warp,
                 fwo_syn_iteration* records, int64_t cap, int64_t* count);
+
+/* The recipe's fixed and moving masks (recipe.rs fixed_mask / moving_mask), each on its own grid
+ * (NULL data = not given); syn.rs:496-580 resolves them on the level grid every iteration. */
+typedef struct fwo_syn_masks {
+    const fwo_grid* fixed_grid;
+    const double* fixed;
+    const fwo_grid* moving_grid;
+    const double* moving;
+} fwo_syn_masks;
+int fwo_syn_step_masked(const fwo_syn_recipe* r, const fwo_grid* level_grid,
+                        const fwo_grid* fixed_grid, const double* const* fixed_smooth,
+                        const fwo_grid* moving_grid, const double* const* moving_smooth,
+                        const fwo_affine* initial, const fwo_syn_masks* masks, double* f2m,
+                        double* f2m_inv, double* m2m, double* m2m_inv, double* fixed_update,
+                        double* moving_update, fwo_syn_iteration* record);
+int fwo_syn_run_masked(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
+                       const double* const* fixed, const fwo_grid* moving_grid,
+                       const double* const* moving, const fwo_affine* initial,
+                       const fwo_syn_masks* masks, double* warp, double* inverse_warp,
+                       fwo_syn_iteration* records, int64_t cap, int64_t* count);
 
 #ifdef __cplusplus
 }

@@ -135,6 +135,80 @@ def test_cc_every_radius_path_matches(backend, radius):
     assert worst(backend.download_field(d2), e2) <= 1e-4 * np.abs(e2).max()
 
 
+def ball_mask(case):
+    """metric/cc.rs:465-473's mask shape on the case grid: out of a ball, the first x plane and a
+    corner strip; the inside value is 3 (any non-zero value counts)."""
+    nx, ny, nz = case["size"]
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    d = np.sqrt((i - nx / 2.0) ** 2 + (j - ny / 2.5) ** 2 + (k - nz / 1.8) ** 2)
+    out = (d < min(nx, ny, nz) / 3.5) | (i == 0) | ((j == ny - 1) & (k > nz // 2))
+    return np.where(out, 0.0, 3.0)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_masked_cc_pair_matches(backend, name):
+    case = CASES[name]
+    og, g = grid_of(case), fgrid(case)
+    fimg, mimg = image(case), image(case, seed_offset=5)
+    valid = ball_mask(case)
+    r = case["radius"]
+    fi = backend.upload_image(g, fimg.astype(np.float32))
+    mi = backend.upload_image(g, mimg.astype(np.float32))
+    vi = backend.upload_image(g, valid.astype(np.float32))
+    (v1, d1), (v2, d2) = backend.cc_value_derivative_pair_masked(fi, mi, vi, r)
+    (w1, e1), (w2, e2) = O.cc_pair(og, fimg, mimg, r, valid=valid)
+    assert rel(v1, w1) <= 1e-5 and rel(v2, w2) <= 1e-5
+    g1, g2 = backend.download_field(d1), backend.download_field(d2)
+    assert worst(g1, e1) <= 1e-4 * np.abs(e1).max()
+    assert worst(g2, e2) <= 1e-4 * np.abs(e2).max()
+    assert np.all(g1[valid == 0] == 0.0) and np.all(g2[valid == 0] == 0.0)
+    ((u1, c1), (u2, c2)), norms = backend.cc_value_derivative_pair_masked_with_norms(fi, mi, vi, r)
+    assert (u1, u2) == (v1, v2)
+    assert np.array_equal(backend.download_field(c1), g1)
+    assert rel(norms[0], np.sqrt((e1 ** 2).sum())) <= 1e-5
+    assert rel(norms[1], np.sqrt((e2 ** 2).sum())) <= 1e-5
+
+
+@pytest.mark.parametrize("radius", [1, 5, 6, 8])
+def test_masked_cc_every_radius_path_matches(backend, radius):
+    case = dict(CASES["awkward_aligned"], radius=radius)
+    og, g = grid_of(case), fgrid(case)
+    fimg, mimg = image(case), image(case, seed_offset=3)
+    valid = ball_mask(case)
+    fi = backend.upload_image(g, fimg.astype(np.float32))
+    mi = backend.upload_image(g, mimg.astype(np.float32))
+    vi = backend.upload_image(g, valid.astype(np.float32))
+    (v1, d1), (v2, d2) = backend.cc_value_derivative_pair_masked(fi, mi, vi, radius)
+    (w1, e1), (w2, e2) = O.cc_pair(og, fimg, mimg, radius, valid=valid)
+    assert rel(v1, w1) <= 1e-5
+    assert worst(backend.download_field(d1), e1) <= 1e-4 * np.abs(e1).max()
+    assert worst(backend.download_field(d2), e2) <= 1e-4 * np.abs(e2).max()
+
+
+def test_an_all_ones_mask_gives_the_unmasked_pair_bit_for_bit(backend):
+    """metric/cc.rs:540-552: a mask of ones is no mask."""
+    case = CASES["awkward_oblique"]
+    g = fgrid(case)
+    fi = backend.upload_image(g, image(case).astype(np.float32))
+    mi = backend.upload_image(g, image(case, seed_offset=5).astype(np.float32))
+    ones = backend.upload_image(g, np.ones(tuple(reversed(case["size"])), np.float32))
+    ((a, da), (b, db)), na = backend.cc_value_derivative_pair_with_norms(fi, mi, 4)
+    ((c, dc), (d, dd)), nc = backend.cc_value_derivative_pair_masked_with_norms(fi, mi, ones, 4)
+    assert (a, b) == (c, d) and na == nc
+    assert np.array_equal(backend.download_field(da), backend.download_field(dc))
+    assert np.array_equal(backend.download_field(db), backend.download_field(dd))
+
+
+def test_an_empty_mask_fails_with_no_voxel_in_masks(backend):
+    """metric/cc.rs:553-565."""
+    case = CASES["selftest"]
+    g = fgrid(case)
+    fi = backend.upload_image(g, image(case).astype(np.float32))
+    zeros = backend.upload_image(g, np.zeros(tuple(reversed(case["size"])), np.float32))
+    with pytest.raises(N.FastwarpError, match="no voxel of the registration level lies inside"):
+        backend.cc_value_derivative_pair_masked(fi, fi, zeros, 2)
+
+
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("variance", [3.0, 0.25, 8.0])
 def test_smooth_field_matches(backend, name, variance):

@@ -162,3 +162,86 @@ def test_direct_launch_mode_gives_the_graph_result(backend, monkeypatch):
     assert np.array_equal(direct.warp, res.warp)
     assert np.array_equal(direct.inverse_warp, res.inverse_warp)
     assert direct.iterations[-1]["energy"] == res.iterations[-1]["energy"]
+
+
+# ---- masks (syn.rs:496-580): the fixed mask through F^-1 times the moving mask through
+# affine(M^-1), nearest voxel, every iteration; the CC pairs take only those voxels ------------
+
+def masks_for(n):
+    """A fixed mask on the fixed grid (a ball left out, value 2: any non-zero is inside) and a
+    moving mask on its own coarser, shifted grid (a slab left out)."""
+    from fastwarp_b200.backend import make_grid
+    z, y, x = np.meshgrid(*[np.arange(n, dtype=float)] * 3, indexing="ij")
+    fm = np.where((x - 0.3 * n) ** 2 + (y - 0.6 * n) ** 2 + (z - 0.5 * n) ** 2 < (0.18 * n) ** 2,
+                  0.0, 2.0)
+    m_n = (n * 2) // 3 + 3
+    mgrid = make_grid((m_n, m_n, m_n), (1.5, 1.5, 1.5), (-1.2, -0.9, -1.05))
+    mz = np.arange(m_n) * 1.5 - 1.05
+    mm = np.ones((m_n, m_n, m_n))
+    mm[(mz > 0.65 * n) & (mz < 0.8 * n), :, :] = 0.0
+    return fm, mgrid, mm
+
+
+def test_one_masked_syn_step_matches(backend, pair):
+    g, fixed, moving = pair
+    r = config1(1)
+    og = ogrid(g)
+    fm, mgrid, mm = masks_for(64)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    fmi, mmi = backend.upload_image(g, fm), backend.upload_image(mgrid, mm)
+    state = {k: backend.zero_field(g) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    rec, fu, mu = syn_step(backend, r, [fi], [mi], None, state, fixed_mask=fmi, moving_mask=mmi)
+    ostate = {k: np.zeros((64, 64, 64, 3)) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    orec, ofu, omu = O.syn_step(oracle_recipe(r), og, og, [fixed], og, [moving], None, ostate,
+                                masks=dict(fixed_grid=og, fixed=fm, moving_grid=ogrid(mgrid),
+                                           moving=mm))
+    assert abs(rec["energy"] - orec.energy) <= 1e-5 * abs(orec.energy)
+    assert np.abs(fu - ofu).max() <= 1e-4
+    assert np.abs(mu - omu).max() <= 1e-4
+    # the mask changed the step: the unmasked oracle step differs
+    ustate = {k: np.zeros((64, 64, 64, 3)) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    urec, ufu, _ = O.syn_step(oracle_recipe(r), og, og, [fixed], og, [moving], None, ustate)
+    assert abs(urec.energy - orec.energy) > 1e-4
+
+
+def test_masked_registration_matches_the_oracle(backend):
+    g, fixed, moving = blob_pair(48, seed=78)
+    r = SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2,
+                  iterations=[8, 6], shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0],
+                  convergence_threshold=-1.0)
+    fm, mgrid, mm = masks_for(48)
+    og = ogrid(g)
+    res = run_syn(backend, r, g, [fixed], g, [moving], fixed_mask=(g, fm),
+                  moving_mask=(mgrid, mm))
+    ow, oinv, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed], og, [moving],
+                                   masks=dict(fixed_grid=og, fixed=fm, moving_grid=ogrid(mgrid),
+                                              moving=mm))
+    assert len(res.iterations) == len(orecs) == 14
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    rms_inv = np.sqrt(((res.inverse_warp.astype(np.float64) - oinv) ** 2).sum(-1).mean())
+    assert rms <= 0.05 and rms_inv <= 0.05, (rms, rms_inv)
+    assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
+
+
+def test_masks_of_ones_give_the_unmasked_run_bit_for_bit(backend):
+    """syn.rs:1239: masks of ones leave a run unchanged."""
+    g, fixed, moving = blob_pair(40, seed=57)
+    r = SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2,
+                  iterations=[4, 3], shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0],
+                  convergence_threshold=-1.0)
+    res = run_syn(backend, r, g, [fixed], g, [moving])
+    ones = np.ones((40, 40, 40))
+    masked = run_syn(backend, r, g, [fixed], g, [moving], fixed_mask=(g, ones),
+                     moving_mask=(g, ones))
+    assert np.array_equal(res.warp, masked.warp)
+    assert np.array_equal(res.inverse_warp, masked.inverse_warp)
+    assert [i["energy"] for i in res.iterations] == [i["energy"] for i in masked.iterations]
+
+
+def test_an_all_zero_mask_is_refused(backend):
+    """recipe.rs:239-246."""
+    from fastwarp_b200 import _native as N
+    g, fixed, moving = blob_pair(24, seed=58)
+    r = config1(2)
+    with pytest.raises(N.FastwarpError, match="moving mask has no voxel inside"):
+        run_syn(backend, r, g, [fixed], g, [moving], moving_mask=(g, np.zeros((24, 24, 24))))

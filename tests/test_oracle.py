@@ -504,3 +504,63 @@ def test_syn_loop_reduces_the_cc_energy_on_a_blob_pair():
     assert len(recs) == 15
     assert recs[-1].energy < recs[0].energy - 0.003
     assert all(s.iterations >= 1 for rec in recs for s in rec.inversions)
+
+
+# ---- masked SyN (syn.rs:496-580; syn.rs:1239-1300; syn_phantom.rs:290-380) ---------------------
+
+def _cavity_pair(n=24):
+    z, y, x = np.meshgrid(*[np.arange(n, dtype=float)] * 3, indexing="ij")
+    f = np.exp(-(((x - 11) / 5) ** 2 + ((y - 12) / 4) ** 2 + ((z - 12) / 6) ** 2)) + \
+        0.6 * np.exp(-(((x - 16) / 3) ** 2 + ((y - 8) / 3) ** 2 + ((z - 14) / 3) ** 2))
+    m = np.exp(-(((x - 12) / 5) ** 2 + ((y - 11.5) / 4) ** 2 + ((z - 12) / 6) ** 2)) + \
+        0.6 * np.exp(-(((x - 17) / 3) ** 2 + ((y - 8.5) / 3) ** 2 + ((z - 14) / 3) ** 2))
+    return f, m, (x, y, z)
+
+
+def test_masks_of_ones_leave_the_syn_run_unchanged():
+    n = 20
+    g = cube(n)
+    f, m, _ = _cavity_pair(n)
+    r = O.syn_recipe(gradient_step=0.25, update_variance=3.0, cc_radius=2, iterations=(4, 3),
+                     shrink=(2, 1), sigmas=(1.0, 0.0), convergence_threshold=-1.0)
+    w0, i0, r0, _ = O.syn_run(r, g, [f], g, [m])
+    ones = np.ones((n, n, n))
+    mg = O.make_grid((n + 4,) * 3, (1.0,) * 3, (-2.0,) * 3)
+    w1, i1, r1, _ = O.syn_run(r, g, [f], g, [m], masks=dict(
+        fixed_grid=g, fixed=ones, moving_grid=mg, moving=np.ones((n + 4,) * 3)))
+    assert np.array_equal(w0, w1) and np.array_equal(i0, i1)
+    assert [a.energy for a in r0] == [b.energy for b in r1]
+
+
+def test_a_moving_mask_keeps_a_cavity_from_driving_the_deformation():
+    n = 24
+    g = cube(n)
+    f, m, (x, y, z) = _cavity_pair(n)
+    centre = (8.0, 15.0, 12.0)
+    inside = (x - centre[0]) ** 2 + (y - centre[1]) ** 2 + (z - centre[2]) ** 2 < 4.0 ** 2
+    lesioned = np.where(inside, 0.9, m)
+    # the mask on its own coarser grid: 0 in a ball a little bigger than the cavity
+    mg = O.make_grid((17, 17, 17), (1.5, 1.5, 1.5), (0.0, 0.0, 0.0))
+    mz, my, mx = np.meshgrid(*[np.arange(17) * 1.5] * 3, indexing="ij")
+    keep = ((mx - centre[0]) ** 2 + (my - centre[1]) ** 2 + (mz - centre[2]) ** 2 >= 5.5 ** 2)
+    r = O.syn_recipe(gradient_step=0.25, update_variance=3.0, cc_radius=2, iterations=(12,),
+                     shrink=(1,), sigmas=(0.0,), convergence_threshold=-1.0)
+    clean, _, _, _ = O.syn_run(r, g, [f], g, [m])
+    unmasked, _, _, _ = O.syn_run(r, g, [f], g, [lesioned])
+    masked, _, _, _ = O.syn_run(r, g, [f], g, [lesioned],
+                                masks=dict(moving_grid=mg, moving=keep.astype(float)))
+    near = inside
+    dev_u = np.sqrt(((unmasked - clean) ** 2).sum(-1))[near].mean()
+    dev_m = np.sqrt(((masked - clean) ** 2).sum(-1))[near].mean()
+    assert dev_u > 0.05, dev_u
+    assert dev_m < 0.5 * dev_u, (dev_m, dev_u)
+
+
+def test_an_all_zero_mask_is_refused():
+    n = 12
+    g = cube(n)
+    f, m, _ = _cavity_pair(n)
+    r = O.syn_recipe(gradient_step=0.25, update_variance=3.0, cc_radius=2, iterations=(2,),
+                     shrink=(1,), sigmas=(0.0,), convergence_threshold=-1.0)
+    with pytest.raises(RuntimeError, match="fixed mask has no voxel inside"):
+        O.syn_run(r, g, [f], g, [m], masks=dict(fixed_grid=g, fixed=np.zeros((n, n, n))))
