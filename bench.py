@@ -69,11 +69,12 @@ def time_kernels(b, fimg, mimg, reps):
     import ctypes as C
 
     from fastwarp_b200 import _native as N
-    ms = (C.c_double * 6)()
-    by = (C.c_double * 6)()
+    ms = (C.c_double * 7)()
+    by = (C.c_double * 7)()
     N.check(N.lib().fw_time_kernels(b.ctx, fimg.handle, mimg.handle, C.c_int32(4),
                                     C.c_double(3.0), C.c_int32(reps), ms, by))
-    names = ["warp", "cc_pair", "smooth", "compose", "inv_measure", "inv_body"]
+    names = ["warp", "cc_pair", "smooth", "compose", "inv_measure", "inv_body_last",
+             "inv_body_next"]
     return {k: (ms[i], by[i]) for i, k in enumerate(names)}
 
 
@@ -308,6 +309,7 @@ def run_ours(args, rank, world, local):
         out["config"]["served_over_sequential"] = round(value / world / seq_value, 3)
         out["config"]["sequential_latency_s"] = round(statistics.median(
             o["run_s"] for o in so), 4)
+        out["config"]["sequential_run_s"] = [round(o["run_s"], 4) for o in so]
         # the reference's execution shape: the loop drives one synchronous Backend op at a time
         from fastwarp_b200.syn import run_syn_ops
         log("op-by-op comparison")
@@ -320,8 +322,10 @@ def run_ours(args, rank, world, local):
     # per-kernel roofline at the finest level (CUDA events on the engine stream)
     log("kernel timing")
     t = time_kernels(b, fi, b.upload_image(g, fixed), 20)
+    # launches per iteration (ncu launch list of a registration: 4 inversions, each one
+    # measurement and one last body, plus 0.4 bodies per iteration that measure again)
     per_iter = {"warp": 2, "cc_pair": 1, "smooth": 2, "compose": 2, "inv_measure": 4,
-                "inv_body": 4}
+                "inv_body_last": 4, "inv_body_next": 0.4}
     dom = max(per_iter, key=lambda k: t[k][0] * per_iter[k])
     ms, by = t[dom]
     peak, src = peaks()

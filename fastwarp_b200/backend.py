@@ -252,6 +252,33 @@ class CudaBackend:
             C.byref(a), C.byref(b), norms))
         return ((vals[0], Field(self, a)), (vals[1], Field(self, b))), [norms[0], norms[1]]
 
+    def _mi_pair(self, fixed, moving, fixed_mask, moving_mask, bins, norms):
+        vals = (C.c_double * 2)()
+        nrm = (C.c_double * 2)()
+        a, b = C.c_void_p(), C.c_void_p()
+        fm = None if fixed_mask is None else fixed_mask.handle
+        mm = None if moving_mask is None else moving_mask.handle
+        check(lib().fw_mi_value_derivative_pair_masked_with_norms(
+            self.ctx, fixed.handle, moving.handle, fm, mm, C.c_int32(bins), vals, C.byref(a),
+            C.byref(b), nrm))
+        pair = (vals[0], Field(self, a)), (vals[1], Field(self, b))
+        return (pair, [nrm[0], nrm[1]]) if norms else pair
+
+    def mi_value_derivative_pair(self, fixed: Image, moving: Image, bins: int):
+        """Backend::mi_value_derivative_pair (backend.rs:179-190): dense Mattes MI both ways."""
+        return self._mi_pair(fixed, moving, None, None, bins, False)
+
+    def mi_value_derivative_pair_masked(self, fixed: Image, moving: Image, fixed_mask, moving_mask,
+                                        bins: int):
+        return self._mi_pair(fixed, moving, fixed_mask, moving_mask, bins, False)
+
+    def mi_value_derivative_pair_with_norms(self, fixed: Image, moving: Image, bins: int):
+        return self._mi_pair(fixed, moving, None, None, bins, True)
+
+    def mi_value_derivative_pair_masked_with_norms(self, fixed: Image, moving: Image, fixed_mask,
+                                                   moving_mask, bins: int):
+        return self._mi_pair(fixed, moving, fixed_mask, moving_mask, bins, True)
+
     def smooth_field(self, field: Field, variance: float) -> Field:
         check(lib().fw_smooth_field(self.ctx, field.handle, C.c_double(variance)))
         return field

@@ -34,62 +34,6 @@ struct CcArgs {
     double isp[3];      // 1 / spacing (the central difference's denominator)
 };
 
-// Exact float64 emulation of the oracle's probe position (index_to_point, offset along the
-// physical axis, point_to_index) -- no fused multiply-adds, so the inside test at the faces
-// rounds as the reference's f64 code does.
-__device__ __forceinline__ void probe_index(const DevGrid& g, int i, int j, int k, int d,
-                                            double sign, double c[3]) {
-    double s0 = __dmul_rn((double)i, g.sp[0]);
-    double s1 = __dmul_rn((double)j, g.sp[1]);
-    double s2 = __dmul_rn((double)k, g.sp[2]);
-    double p[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        double rot = __dadd_rn(__dadd_rn(__dmul_rn(g.dir[r * 3 + 0], s0),
-                                         __dmul_rn(g.dir[r * 3 + 1], s1)),
-                               __dmul_rn(g.dir[r * 3 + 2], s2));
-        p[r] = __dadd_rn(g.org[r], rot);
-    }
-    double off = __dmul_rn(0.5, g.sp[d]);
-    p[d] = sign > 0 ? __dadd_rn(p[d], off) : __dsub_rn(p[d], off);
-    double e0 = __dsub_rn(p[0], g.org[0]), e1 = __dsub_rn(p[1], g.org[1]),
-           e2 = __dsub_rn(p[2], g.org[2]);
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-        c[r] = __dadd_rn(__dadd_rn(__dmul_rn(g.inv[r * 3], e0), __dmul_rn(g.inv[r * 3 + 1], e1)),
-                         __dmul_rn(g.inv[r * 3 + 2], e2));
-}
-
-// interp.rs:96-120 at voxel (i, j, k) from global memory, general direction.
-__device__ void central_difference_exact(const float* __restrict__ img, const DevGrid& g, int i,
-                                         int j, int k, float out[3]) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        double c1[3], c2[3];
-        probe_index(g, i, j, k, d, -1.0, c1);
-        probe_index(g, i, j, k, d, +1.0, c2);
-        out[d] = 0.0f;
-        if (!inside_index(c1[0], c1[1], c1[2], g.nx, g.ny, g.nz) ||
-            !inside_index(c2[0], c2[1], c2[2], g.nx, g.ny, g.nz))
-            continue;
-        float v1 = lin_at_index(img, g.nx, g.ny, g.nz, c1[0], c1[1], c1[2]);
-        float v2 = lin_at_index(img, g.nx, g.ny, g.nz, c2[0], c2[1], c2[2]);
-        out[d] = (float)((double)(v2 - v1) / g.sp[d]);
-    }
-}
-
-// Whether the probe of voxel coordinate `i` (axis d, direction `sign`) is inside the buffer,
-// for an identity direction: only the two face voxels can round either way.
-__device__ __forceinline__ bool axis_probe_inside(const DevGrid& g, int i, int j, int k, int d,
-                                                  double sign, int n) {
-    int q = d == 0 ? i : (d == 1 ? j : k);
-    if (sign < 0 && q > 0) return true;
-    if (sign > 0 && q < n - 1) return true;
-    double c[3];
-    probe_index(g, i, j, k, d, sign, c);
-    return c[d] >= -0.5 && c[d] < (double)n - 0.5;
-}
-
 // Shared-memory layout (dynamic): input ring [D][HY][HX] float2 (f, m); with a mask, its flags
 // [D][HY][HX] bytes; x sums [5][HY][TX] double (+ [HY][TX] int counts); xy-sum ring
 // [2R+1][5][TX*TY] double (+ [2R+1][TX*TY] int counts); block-reduction space.

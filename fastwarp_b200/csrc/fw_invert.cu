@@ -91,9 +91,11 @@ __device__ void reduce_and_finish(double sum, float mx, double* __restrict__ par
     }
 }
 
-// First measurement (body 0's error) of psi against f.
+// First measurement (body 0's error) of psi against f; the residual e = psi + f(x + psi) of
+// every voxel is kept in `res` for the body that follows.
 __global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __restrict__ f,
                                                      const float* __restrict__ psi,
+                                                     float* __restrict__ res,
                                                      double* __restrict__ partials,
                                                      unsigned int* __restrict__ counter,
                                                      InvState* __restrict__ st,
@@ -113,6 +115,9 @@ __global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __r
             voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
             float e[3];
             residual(a, f, l, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
+            res[l] = e[0];
+            res[l + a.ps_psi] = e[1];
+            res[l + 2 * a.ps_psi] = e[2];
             float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
             float nrm = nan_canon(sqrtf(x * x + y * y + z * z));
             sum += (double)nrm;
@@ -131,9 +136,12 @@ __global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __r
 }
 
 // One body: the update with eps (0.75 on body 0, else 0.5) and limit eps * max of the last
-// measurement, faces to zero, then -- when the next body will run -- its measurement.
+// measurement, from the residual that measurement kept in `res`; faces to zero; then -- when
+// the next body will run -- its measurement, whose residual replaces the voxel's in `res`.
+// Without a next body the sweep is elementwise (no gather).
 __global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __restrict__ f,
                                                   float* __restrict__ psi,
+                                                  float* __restrict__ res,
                                                   double* __restrict__ partials,
                                                   unsigned int* __restrict__ counter,
                                                   InvState* __restrict__ st,
@@ -154,10 +162,10 @@ __global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __rest
     double sum = 0.0;
     float mx = 0.0f;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    // two voxels a step, `stride` apart: their gathers are in flight together
+    // two voxels a step, `stride` apart: their loads are in flight together
     for (long long l0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; l0 < a.g.n;
          l0 += 2 * stride) {
-        float px[2], py[2], pz[2];
+        float px[2], py[2], pz[2], ex[2], ey[2], ez[2];
         int ii[2], jj[2], kk[2];
         bool ok[2];
 #pragma unroll
@@ -169,17 +177,18 @@ __global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __rest
             px[v] = psi[l];
             py[v] = psi[l + a.ps_psi];
             pz[v] = psi[l + 2 * a.ps_psi];
+            ex[v] = res[l];
+            ey[v] = res[l + a.ps_psi];
+            ez[v] = res[l + 2 * a.ps_psi];
         }
 #pragma unroll
         for (int v = 0; v < 2; ++v) {
             if (!ok[v]) continue;
             long long l = l0 + v * stride;
             const int i = ii[v], j = jj[v], k = kk[v];
-            float e[3];
-            residual(a, f, l, i, j, k, px[v], py[v], pz[v], e);
-            float ex = e[0] * a.isx, ey = e[1] * a.isy, ez = e[2] * a.isz;
-            float nrm = sqrtf(ex * ex + ey * ey + ez * ez);
-            float ux = -e[0], uy = -e[1], uz = -e[2];
+            float sx = ex[v] * a.isx, sy = ey[v] * a.isy, sz = ez[v] * a.isz;
+            float nrm = sqrtf(sx * sx + sy * sy + sz * sz);
+            float ux = -ex[v], uy = -ey[v], uz = -ez[v];
             if (nrm > limit) {
                 float fct = limit / nrm;
                 ux *= fct;
@@ -203,6 +212,9 @@ __global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __rest
                 long long l = l0 + v * stride;
                 float e[3];
                 residual(a, f, l, ii[v], jj[v], kk[v], px[v], py[v], pz[v], e);
+                res[l] = e[0];
+                res[l + a.ps_psi] = e[1];
+                res[l + 2 * a.ps_psi] = e[2];
                 float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
                 float n2 = nan_canon(sqrtf(x * x + y * y + z * z));
                 sum += (double)n2;
@@ -235,6 +247,18 @@ __global__ void k_inv_init(InvState* st, fw_invert_params p) {
     st->enforce = p.enforce_boundary_condition;
 }
 
+// Re-arms a finished loop for one more body from its last measurement (kernel timing).
+__global__ void k_inv_rearm(InvState* st, int max_iterations) {
+    st->go = 1;
+    st->k = 0;
+    st->max_iterations = max_iterations;
+}
+
+int enqueue_inversion_rearm(fw_ctx* ctx, InvState* st, int max_iterations) {
+    k_inv_rearm<<<1, 1, 0, ctx->stream>>>(st, max_iterations);
+    return check_launch(ctx, "k_inv_rearm");
+}
+
 static InvArgs inv_args(const fw_field* field, const fw_field* inverse) {
     InvArgs a;
     a.g = dev_grid(field->grid);
@@ -254,24 +278,26 @@ static unsigned int inv_blocks(fw_ctx* ctx, long long n) {
 // Launches the whole inversion on the stream: init, first measurement and `bodies` body kernels
 // (each returns at once after the loop has ended). Used by graph capture with bodies = 0.
 int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
-                             const fw_invert_params& prm, InvState* st,
+                             fw_field* res, const fw_invert_params& prm, InvState* st,
                              cudaGraphConditionalHandle handle, int use_handle) {
+    FW_CHECK(res->grid.same(inverse->grid) && res->ps == inverse->ps,
+             "invert: the residual buffer does not match the inverse");
     InvArgs a = inv_args(field, inverse);
     unsigned int blocks = inv_blocks(ctx, a.g.n);
     FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 2 * (size_t)blocks + 16));
     k_inv_init<<<1, 1, 0, ctx->stream>>>(st, prm);
     FW_TRY(check_launch(ctx, "k_inv_init"));
-    k_inv_measure<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d,
+    k_inv_measure<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
                                                    ctx->d_scratch + SLOT_PARTIALS,
                                                    ctx->d_counter + 2, st, handle, use_handle);
     return check_launch(ctx, "k_inv_measure");
 }
 
-int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, InvState* st,
-                           cudaGraphConditionalHandle handle, int use_handle) {
+int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
+                           InvState* st, cudaGraphConditionalHandle handle, int use_handle) {
     InvArgs a = inv_args(field, inverse);
     unsigned int blocks = inv_blocks(ctx, a.g.n);
-    k_inv_body<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d,
+    k_inv_body<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
                                                 ctx->d_scratch + SLOT_PARTIALS,
                                                 ctx->d_counter + 2, st, handle, use_handle);
     return check_launch(ctx, "k_inv_body");
@@ -281,10 +307,16 @@ int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse
 int invert_field(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
                  const fw_invert_params& prm, fw_invert_stats* stats) {
     InvState* st = reinterpret_cast<InvState*>(ctx->d_scratch + SLOT_INV);
-    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, prm, st, 0, 0));
+    fw_field* res = nullptr;  // the residual of the last measurement
+    FW_TRY(new_field(ctx, inverse->grid, &res));
+    struct Free {
+        fw_field* f;
+        ~Free() { fw_field_free(f); }
+    } guard{res};
+    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, prm, st, 0, 0));
     InvState h;
     for (int body = 0; body < std::max(prm.max_iterations, 0); ++body) {
-        FW_TRY(enqueue_inversion_body(ctx, field, inverse, st, 0, 0));
+        FW_TRY(enqueue_inversion_body(ctx, field, inverse, res, st, 0, 0));
         FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, st, sizeof(InvState), cudaMemcpyDeviceToHost,
                                 ctx->stream));
         FW_TRY(sync(ctx));

@@ -135,15 +135,20 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict_
         if (sh[s]) atomicAdd(&out[s], sh[s]);
 }
 
-// ComputeResults (metric/mi.rs:702-768) for transform blockIdx.x: one thread per cell.
-// out[t*4 + 0] = -MI, [1] = valid samples, [2] = status (0 ok, 1 no valid sample, 2 zero PDF).
+// ComputeResults (metric/mi.rs:702-768) for histogram blockIdx.x: one thread per cell.
+// out[t*4 + 0] = -MI, [1] = valid samples, [2] = status (0 ok, 1 no valid sample, 2 zero PDF);
+// ratio[t * bins * bins + cell] with want_ratio. The moving bin size is `moving_bin_size`, or
+// mbin_dev[t] when that is given (bin sizes measured on the device).
 __global__ void __launch_bounds__(1024) k_mi_finish(const unsigned long long* __restrict__ hist,
                                                     int bins, double moving_bin_size,
-                                                    double* __restrict__ ratio,
+                                                    const double* __restrict__ mbin_dev,
+                                                    double* __restrict__ ratio_all,
                                                     double* __restrict__ out, int want_ratio) {
     const int cells = bins * bins + bins;
     const unsigned long long* h = hist + (size_t)blockIdx.x * cells;
     double* o = out + 4 * blockIdx.x;
+    double* ratio = ratio_all + (size_t)blockIdx.x * bins * bins;
+    if (mbin_dev) moving_bin_size = mbin_dev[blockIdx.x];
     __shared__ unsigned long long s_int[1024];
     __shared__ double s_d[1024];
     __shared__ double fmarg[MAX_BINS], mmarg[MAX_BINS];
@@ -292,6 +297,242 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_deriv(const MiMap* __restrict
     if (threadIdx.x == 0) *counter = 0;
 }
 
+// ---- dense Mattes MI pair of two images on one grid (SyN Mattes channels) -----------------
+//
+// Backend::mi_value_derivative_pair[_masked] (backend.rs:179-205) as cpu/mod.rs:352-381 runs it:
+// MattesMi::evaluate_dense (metric/mi.rs:601-680) twice, (fixed, moving) then (moving, fixed),
+// with identity transforms and the masks (when given) on the images' grid. Both directions use
+// the same two Parzen terms per voxel (f / s_f - n_f and m / s_m - n_m), so one pass builds both
+// joint histograms and one pass writes both derivatives. The intensity ranges (MiBinning::dense,
+// mi.rs:276-295: each image over the voxels inside its own mask, non-finite voxels skipped) and
+// the bin geometry (MiBinning::from_ranges, mi.rs:238-274) are measured on the device.
+
+struct DenseState {
+    unsigned int key[4];    // order-preserving keys of f min, f max, m min, m max
+    unsigned int count[2];  // finite voxels inside each image's own mask
+    int status;             // 0 ok; 1 / 2 no finite fixed / moving voxel; 3 / 4 constant
+    int pad;
+    double fmin, fmax, mmin, mmax;
+    double sf, nf, sm, nm;  // bin size and normalised minimum of each image
+    double mbin[2];         // moving-axis bin size of direction 0 (m) and 1 (f)
+};
+
+__device__ __forceinline__ unsigned int order_key(float v) {
+    unsigned int b = __float_as_uint(v);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ float key_value(unsigned int k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void k_dense_init(DenseState* st) {
+    st->key[0] = st->key[2] = 0xffffffffu;
+    st->key[1] = st->key[3] = 0u;
+    st->count[0] = st->count[1] = 0u;
+    st->status = 0;
+}
+
+__global__ void __launch_bounds__(256) k_dense_range(const float* __restrict__ f,
+                                                     const float* __restrict__ m,
+                                                     const float* __restrict__ fm,
+                                                     const float* __restrict__ mm, long long n,
+                                                     DenseState* __restrict__ st) {
+    unsigned int kl[2] = {0xffffffffu, 0xffffffffu}, kh[2] = {0u, 0u}, cnt[2] = {0u, 0u};
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < n;
+         l += (long long)gridDim.x * blockDim.x) {
+        const float v[2] = {f[l], m[l]};
+        const bool in[2] = {!fm || fm[l] != 0.0f, !mm || mm[l] != 0.0f};
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (in[q] && isfinite(v[q])) {
+                const unsigned int k = order_key(v[q]);
+                kl[q] = min(kl[q], k);
+                kh[q] = max(kh[q], k);
+                ++cnt[q];
+            }
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            kl[q] = min(kl[q], __shfl_xor_sync(0xffffffffu, kl[q], o));
+            kh[q] = max(kh[q], __shfl_xor_sync(0xffffffffu, kh[q], o));
+            cnt[q] += __shfl_xor_sync(0xffffffffu, cnt[q], o);
+        }
+        if ((threadIdx.x & 31) == 0 && cnt[q]) {
+            atomicMin(&st->key[2 * q], kl[q]);
+            atomicMax(&st->key[2 * q + 1], kh[q]);
+            atomicAdd(&st->count[q], cnt[q]);
+        }
+    }
+}
+
+__global__ void k_dense_setup(DenseState* st, int bins) {
+    if (st->count[0] == 0) {
+        st->status = 1;
+        return;
+    }
+    if (st->count[1] == 0) {
+        st->status = 2;
+        return;
+    }
+    st->fmin = key_value(st->key[0]);
+    st->fmax = key_value(st->key[1]);
+    st->mmin = key_value(st->key[2]);
+    st->mmax = key_value(st->key[3]);
+    if (st->fmax - st->fmin <= DBL_EPSILON) {
+        st->status = 3;
+        return;
+    }
+    if (st->mmax - st->mmin <= DBL_EPSILON) {
+        st->status = 4;
+        return;
+    }
+    const double span = (double)(bins - 4);
+    st->sf = (st->fmax - st->fmin) / span;
+    st->sm = (st->mmax - st->mmin) / span;
+    st->nf = st->fmin / st->sf - 2.0;
+    st->nm = st->mmin / st->sm - 2.0;
+    st->mbin[0] = st->sm;
+    st->mbin[1] = st->sf;
+}
+
+// The voxel's two Parzen terms and bins; false when it does not contribute (mi.rs:560-595).
+__device__ __forceinline__ bool dense_voxel(const DenseState& st, int bins, float a, float b,
+                                            bool in, double& tf, double& tm, int& bf, int& bm) {
+    if (!in || !isfinite(a) || !isfinite(b)) return false;
+    const double fv = a, mv = b;
+    // each direction's moving value must lie in its range: m for (f, m), f for (m, f)
+    if (mv < st.mmin || mv > st.mmax || fv < st.fmin || fv > st.fmax) return false;
+    tf = fv / st.sf - st.nf;
+    tm = mv / st.sm - st.nm;
+    bf = clamp_bin(tf, bins);
+    bm = clamp_bin(tm, bins);
+    return true;
+}
+
+// Both joint histograms: [direction][bins*bins joint + bins fixed marginal] in 2^-32 fixed point.
+__global__ void __launch_bounds__(MI_THREADS) k_dense_hist(const float* __restrict__ f,
+                                                           const float* __restrict__ m,
+                                                           const float* __restrict__ fm,
+                                                           const float* __restrict__ mm,
+                                                           long long n, int bins,
+                                                           const DenseState* __restrict__ st,
+                                                           unsigned long long* __restrict__ hist) {
+    extern __shared__ unsigned long long sh[];
+    const int nc = bins * bins, cells = nc + bins;
+    for (int s = threadIdx.x; s < 2 * cells; s += blockDim.x) sh[s] = 0ULL;
+    __syncthreads();
+    const DenseState S = *st;
+    if (S.status == 0) {
+        for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < n;
+             l += (long long)gridDim.x * blockDim.x) {
+            double tf, tm;
+            int bf, bm;
+            const bool in = (!fm || fm[l] != 0.0f) && (!mm || mm[l] != 0.0f);
+            if (!dense_voxel(S, bins, f[l], m[l], in, tf, tm, bf, bm)) continue;
+            atomicAdd(&sh[nc + bf], 1ULL);
+            atomicAdd(&sh[cells + nc + bm], 1ULL);
+#pragma unroll
+            for (int k = -1; k <= 2; ++k) {
+                unsigned long long q0 =
+                    (unsigned long long)__double2ll_rn(bspline3((double)(bm + k) - tm) * FIXED);
+                unsigned long long q1 =
+                    (unsigned long long)__double2ll_rn(bspline3((double)(bf + k) - tf) * FIXED);
+                if (q0) atomicAdd(&sh[bf * bins + bm + k], q0);
+                if (q1) atomicAdd(&sh[cells + bm * bins + bf + k], q1);
+            }
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < 2 * cells; s += blockDim.x)
+        if (sh[s]) atomicAdd(&hist[s], sh[s]);
+}
+
+struct DenseArgs {
+    DevGrid g;
+    long long ps;
+    int bins;
+    int identity;
+    double isp[3];
+};
+
+// Both derivatives (mi.rs:655-672): sum_k B3'(k - term) ratio[fixed bin, k] * grad(moving image of
+// the direction), zero where the voxel does not contribute; result[0..1] = their sums of squares.
+__global__ void __launch_bounds__(MI_THREADS) k_dense_deriv(
+    DenseArgs a, const float* __restrict__ f, const float* __restrict__ m,
+    const float* __restrict__ fm, const float* __restrict__ mm, const DenseState* __restrict__ st,
+    const double* __restrict__ ratio, float* __restrict__ d0, float* __restrict__ d1,
+    double* __restrict__ partials, unsigned int* __restrict__ counter,
+    double* __restrict__ result) {
+    __shared__ double sr[2 * MAX_BINS * MAX_BINS];
+    const int bins = a.bins, nc = bins * bins;
+    for (int s = threadIdx.x; s < 2 * nc; s += blockDim.x) sr[s] = ratio[s];
+    __syncthreads();
+    const DenseState S = *st;
+    double n0 = 0.0, n1 = 0.0;
+    for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < a.g.n;
+         l += (long long)gridDim.x * blockDim.x) {
+        double tf, tm;
+        int bf, bm;
+        const bool in = (!fm || fm[l] != 0.0f) && (!mm || mm[l] != 0.0f);
+        float o0[3] = {0.0f, 0.0f, 0.0f}, o1[3] = {0.0f, 0.0f, 0.0f};
+        if (S.status == 0 && dense_voxel(S, bins, f[l], m[l], in, tf, tm, bf, bm)) {
+            double w0 = 0.0, w1 = 0.0;
+#pragma unroll
+            for (int k = -1; k <= 2; ++k) {
+                w0 += bspline3_derivative((double)(bm + k) - tm) * sr[bf * bins + bm + k];
+                w1 += bspline3_derivative((double)(bf + k) - tf) * sr[nc + bm * bins + bf + k];
+            }
+            int i, j, kz;
+            voxel_ijk(l, a.g.nx, a.g.ny, i, j, kz);
+            float gm[3], gf[3];
+            central_difference_voxel(m, a.g, a.identity != 0, a.isp, i, j, kz, gm);
+            central_difference_voxel(f, a.g, a.identity != 0, a.isp, i, j, kz, gf);
+            if (!(isfinite(gm[0]) && isfinite(gm[1]) && isfinite(gm[2]))) gm[0] = gm[1] = gm[2] = 0.0f;
+            if (!(isfinite(gf[0]) && isfinite(gf[1]) && isfinite(gf[2]))) gf[0] = gf[1] = gf[2] = 0.0f;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                o0[d] = (float)(w0 * (double)gm[d]);
+                o1[d] = (float)(w1 * (double)gf[d]);
+                n0 += (double)o0[d] * o0[d];
+                n1 += (double)o1[d] * o1[d];
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            d0[l + d * a.ps] = o0[d];
+            d1[l + d * a.ps] = o1[d];
+        }
+    }
+    __shared__ double red[2][MI_THREADS / 32];
+    __shared__ bool last;
+    n0 = warp_sum_d(n0);
+    n1 = warp_sum_d(n1);
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = n0;
+        red[1][threadIdx.x >> 5] = n1;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double s = 0.0;
+        for (int w = 0; w < MI_THREADS / 32; ++w) s += red[threadIdx.x][w];
+        partials[(size_t)blockIdx.x * 2 + threadIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    if (threadIdx.x < 2) {
+        double s = 0.0;
+        for (unsigned int b = 0; b < gridDim.x; ++b) s += __ldcg(partials + (size_t)b * 2 + threadIdx.x);
+        result[threadIdx.x] = s;
+    }
+    if (threadIdx.x == 0) *counter = 0;
+}
+
 // ---- host: transform maps and Jacobian matrices (transform/param.rs, affine.rs) -------------
 
 void parametric_affine(const fw_linear_transform* t, double M[9], double off[3]) {
@@ -425,7 +666,8 @@ int hist_and_finish(fw_mi_level* L, const fw_linear_transform* ts, int count, bo
     k_mi_hist<<<grid, MI_THREADS, sh, ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d, L->d_hist);
     FW_TRY(check_launch(ctx, "k_mi_hist"));
     k_mi_finish<<<count, 1024, 0, ctx->stream>>>(L->d_hist, bins, L->binning.moving_bin_size,
-                                                 L->d_ratio, L->d_out, want_ratio ? 1 : 0);
+                                                 nullptr, L->d_ratio, L->d_out,
+                                                 want_ratio ? 1 : 0);
     return check_launch(ctx, "k_mi_finish");
 }
 
@@ -606,6 +848,198 @@ void fw_mi_level_free(fw_mi_level* L) {
     dev_free(ctx, L->d_counter, sizeof(unsigned int) * 4);
     if (L->own_moving) fw_image_free(L->moving);
     delete L;
+}
+
+}  // extern "C"
+
+// ---- dense Mattes MI pair: host side -----------------------------------------------------------
+
+namespace fw {
+namespace {
+
+std::string empty_range_message(const char* role, bool masked) {
+    if (masked)
+        return std::string("no finite ") + role + "-image voxel lies inside the " + role + " mask";
+    return std::string("the ") + role + " image has no finite voxel";
+}
+
+// Device scratch of one dense pair: [state | out 2x4 | norms 2 | hist | ratio | partials].
+struct DenseScratch {
+    fw_ctx* ctx = nullptr;
+    void* base = nullptr;
+    size_t bytes = 0;
+    DenseState* st = nullptr;
+    double* out = nullptr;
+    double* norms = nullptr;
+    unsigned long long* hist = nullptr;
+    double* ratio = nullptr;
+    double* partials = nullptr;
+    unsigned int* counter = nullptr;
+    ~DenseScratch() {
+        if (base) dev_free(ctx, base, bytes);
+    }
+    static constexpr size_t head = 512;  // state + out + norms, read back in one copy
+    int init(fw_ctx* c, int bins, unsigned int blocks) {
+        ctx = c;
+        const size_t cells = (size_t)bins * bins + bins;
+        const size_t o_hist = head, o_ratio = o_hist + 16 * cells,
+                     o_part = o_ratio + 16 * (size_t)bins * bins,
+                     o_cnt = o_part + 16 * (size_t)blocks;
+        bytes = o_cnt + 256;
+        FW_TRY(dev_alloc(ctx, bytes, &base));
+        char* b = static_cast<char*>(base);
+        st = reinterpret_cast<DenseState*>(b);
+        out = reinterpret_cast<double*>(b + 256);
+        norms = reinterpret_cast<double*>(b + 256 + 64);
+        hist = reinterpret_cast<unsigned long long*>(b + o_hist);
+        ratio = reinterpret_cast<double*>(b + o_ratio);
+        partials = reinterpret_cast<double*>(b + o_part);
+        counter = reinterpret_cast<unsigned int*>(b + o_cnt);
+        FW_CUDA(cudaMemsetAsync(base, 0, bytes, ctx->stream));
+        return 0;
+    }
+};
+
+static_assert(sizeof(DenseState) <= 256, "dense state slot");
+
+int dense_pair(fw_ctx* ctx, const fw_image* f, const fw_image* m, const fw_image* fm,
+               const fw_image* mm, int bins, double values[2], fw_field** d_fixed,
+               fw_field** d_moving, double norms[2]) {
+    FW_CHECK(ctx && f && m && values && d_fixed && d_moving, "null argument");
+    if (!f->grid.same(m->grid)) return fail(FW_ERR_INVALID, "mattes: the images are not on one grid");
+    if ((fm && !fm->grid.same(f->grid)) || (mm && !mm->grid.same(f->grid)))
+        return fail(FW_ERR_INVALID, "mattes: a mask is not on the grid of the images");
+    if (bins <= 4) return fail(FW_ERR_INVALID, "mattes: at least five histogram bins are required");
+    if (bins > MAX_BINS) return fail(FW_ERR_INVALID, "mattes: bins must be in 5..=32");
+    const HostGrid& g = f->grid;
+    const long long n = g.count();
+    fw_field *a = nullptr, *b = nullptr;
+    FW_TRY(new_field(ctx, g, &a));
+    int rc = new_field(ctx, g, &b);
+    const unsigned int blocks =
+        (unsigned int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 2LL * ctx->num_sms));
+    DenseScratch sc;
+    if (!rc) rc = sc.init(ctx, bins, blocks);
+    const float* fmp = fm ? fm->d : nullptr;
+    const float* mmp = mm ? mm->d : nullptr;
+    if (!rc) {
+        k_dense_init<<<1, 1, 0, ctx->stream>>>(sc.st);
+        rc = check_launch(ctx, "k_dense_init");
+    }
+    if (!rc) {
+        k_dense_range<<<blocks, 256, 0, ctx->stream>>>(f->d, m->d, fmp, mmp, n, sc.st);
+        rc = check_launch(ctx, "k_dense_range");
+    }
+    if (!rc) {
+        k_dense_setup<<<1, 1, 0, ctx->stream>>>(sc.st, bins);
+        rc = check_launch(ctx, "k_dense_setup");
+    }
+    if (!rc) {
+        const size_t sh = 2 * sizeof(unsigned long long) * ((size_t)bins * bins + bins);
+        k_dense_hist<<<blocks, MI_THREADS, sh, ctx->stream>>>(f->d, m->d, fmp, mmp, n, bins, sc.st,
+                                                              sc.hist);
+        rc = check_launch(ctx, "k_dense_hist");
+    }
+    if (!rc) {
+        k_mi_finish<<<2, 1024, 0, ctx->stream>>>(sc.hist, bins, 0.0, sc.st->mbin, sc.ratio, sc.out,
+                                                 1);
+        rc = check_launch(ctx, "k_mi_finish");
+    }
+    if (!rc) {
+        DenseArgs da;
+        std::memset(&da, 0, sizeof(da));
+        da.g = dev_grid(g);
+        da.ps = a->ps;
+        da.bins = bins;
+        da.identity = 1;
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+                if (g.dir[r * 3 + c] != (r == c ? 1.0 : 0.0)) da.identity = 0;
+        for (int d = 0; d < 3; ++d) da.isp[d] = 1.0 / g.sp[d];
+        k_dense_deriv<<<blocks, MI_THREADS, 0, ctx->stream>>>(da, f->d, m->d, fmp, mmp, sc.st,
+                                                              sc.ratio, a->d, b->d, sc.partials,
+                                                              sc.counter, sc.norms);
+        rc = check_launch(ctx, "k_dense_deriv");
+    }
+    double headd[DenseScratch::head / sizeof(double)];  // copied bitwise, doubles or not
+    if (!rc) rc = read_back(ctx, static_cast<const double*>(sc.base), DenseScratch::head / 8, headd);
+    const unsigned char* head = reinterpret_cast<const unsigned char*>(headd);
+    if (!rc) {
+        DenseState st;
+        std::memcpy(&st, head, sizeof(st));
+        const double* out = reinterpret_cast<const double*>(head + 256);
+        const double* nr = reinterpret_cast<const double*>(head + 256 + 64);
+        switch (st.status) {
+            case 1: rc = fail(FW_ERR_INVALID, "mattes: " + empty_range_message("fixed", fm != nullptr)); break;
+            case 2: rc = fail(FW_ERR_INVALID, "mattes: " + empty_range_message("moving", mm != nullptr)); break;
+            case 3: rc = fail(FW_ERR_INVALID, "mattes: the fixed image is constant"); break;
+            case 4: rc = fail(FW_ERR_INVALID, "mattes: the moving image is constant"); break;
+            default: break;
+        }
+        for (int dir = 0; dir < 2 && !rc; ++dir) {
+            if (out[4 * dir + 2] == 1.0)
+                rc = fail(FW_ERR_INVALID, (fm || mm) ? std::string("mattes: ") + FW_NO_VOXEL_IN_MASKS
+                                                     : std::string("mattes: all samples map outside the moving image buffer"));
+            else if (out[4 * dir + 2] == 2.0)
+                rc = fail(FW_ERR_INVALID, "mattes: joint PDF summed to zero");
+        }
+        if (!rc) {
+            values[0] = out[0];
+            values[1] = out[4];
+            if (norms) {
+                norms[0] = std::sqrt(nr[0]);
+                norms[1] = std::sqrt(nr[1]);
+            }
+        }
+    }
+    if (rc) {
+        fw_field_free(a);
+        fw_field_free(b);
+        return rc;
+    }
+    *d_fixed = a;
+    *d_moving = b;
+    return 0;
+}
+
+}  // namespace
+}  // namespace fw
+
+extern "C" {
+
+int fw_mi_value_derivative_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                                int32_t bins, double values[2], fw_field** d_fixed,
+                                fw_field** d_moving) {
+    return fw::dense_pair(ctx, fixed, moving, nullptr, nullptr, bins, values, d_fixed, d_moving,
+                          nullptr);
+}
+
+int fw_mi_value_derivative_pair_masked(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                                       const fw_image* fixed_mask, const fw_image* moving_mask,
+                                       int32_t bins, double values[2], fw_field** d_fixed,
+                                       fw_field** d_moving) {
+    return fw::dense_pair(ctx, fixed, moving, fixed_mask, moving_mask, bins, values, d_fixed,
+                          d_moving, nullptr);
+}
+
+int fw_mi_value_derivative_pair_with_norms(fw_ctx* ctx, const fw_image* fixed,
+                                           const fw_image* moving, int32_t bins, double values[2],
+                                           fw_field** d_fixed, fw_field** d_moving,
+                                           double norms[2]) {
+    FW_CHECK(norms, "null norms");
+    return fw::dense_pair(ctx, fixed, moving, nullptr, nullptr, bins, values, d_fixed, d_moving,
+                          norms);
+}
+
+int fw_mi_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* fixed,
+                                                  const fw_image* moving,
+                                                  const fw_image* fixed_mask,
+                                                  const fw_image* moving_mask, int32_t bins,
+                                                  double values[2], fw_field** d_fixed,
+                                                  fw_field** d_moving, double norms[2]) {
+    FW_CHECK(norms, "null norms");
+    return fw::dense_pair(ctx, fixed, moving, fixed_mask, moving_mask, bins, values, d_fixed,
+                          d_moving, norms);
 }
 
 }  // extern "C"

@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -187,6 +189,7 @@ struct Level {
     fw_field *accF = nullptr, *accM = nullptr;  // multichannel combination
     fw_field *sF = nullptr, *sM = nullptr;      // smoothed updates
     fw_field* T = nullptr;                      // total-field smoothing
+    fw_field* R = nullptr;                      // inversion residual of the last measurement
     const fw_image* fmask = nullptr;            // recipe masks on their own grids (or none)
     const fw_image* mmask = nullptr;
     fw_image* valid = nullptr;                  // the masks resolved on the level grid
@@ -199,9 +202,9 @@ void free_level_work(Level& L) {
     L.mmid.clear();
     fw_image_free(L.valid);
     L.valid = nullptr;
-    fw_field* fs[] = {L.dF, L.dM, L.accF, L.accM, L.sF, L.sM, L.T};
+    fw_field* fs[] = {L.dF, L.dM, L.accF, L.accM, L.sF, L.sM, L.T, L.R};
     for (auto* f : fs) fw_field_free(f);
-    L.dF = L.dM = L.accF = L.accM = L.sF = L.sM = L.T = nullptr;
+    L.dF = L.dM = L.accF = L.accM = L.sF = L.sM = L.T = L.R = nullptr;
 }
 
 int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
@@ -214,6 +217,7 @@ int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
     }
     FW_TRY(new_field(ctx, L.grid, &L.dF));
     FW_TRY(new_field(ctx, L.grid, &L.dM));
+    FW_TRY(new_field(ctx, L.grid, &L.R));
     if (L.channels > 1) {
         FW_TRY(new_field(ctx, L.grid, &L.accF));
         FW_TRY(new_field(ctx, L.grid, &L.accM));
@@ -262,12 +266,12 @@ int add_while(cudaStream_t s, unsigned int default_value, unsigned int flags,
 
 // One inversion: in graph mode a WHILE node around the body kernel; in direct mode a host loop.
 int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inverse,
-                   InvState* st) {
+                   fw_field* res, InvState* st) {
     if (!graph) {
-        FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, kSynInvert, st, 0, 0));
+        FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, 0, 0));
         InvState h;
         for (int body = 0; body < kSynInvert.max_iterations; ++body) {
-            FW_TRY(enqueue_inversion_body(ctx, field, inverse, st, 0, 0));
+            FW_TRY(enqueue_inversion_body(ctx, field, inverse, res, st, 0, 0));
             FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, st, sizeof(InvState), cudaMemcpyDeviceToHost,
                                     ctx->stream));
             FW_TRY(sync(ctx));
@@ -284,7 +288,7 @@ int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inv
     FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
     cudaGraphConditionalHandle h;
     FW_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, kSynInvert, st, h, 1));
+    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, h, 1));
     FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
     cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
     p.conditional.handle = h;
@@ -300,7 +304,7 @@ int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inv
     FW_CUDA(cudaStreamBeginCaptureToGraph(ctx->aux, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
     ctx->stream = ctx->aux;
-    int rc = enqueue_inversion_body(ctx, field, inverse, st, h, 1);
+    int rc = enqueue_inversion_body(ctx, field, inverse, res, st, h, 1);
     ctx->stream = main;
     cudaGraph_t out;
     cudaError_t e = cudaStreamEndCapture(ctx->aux, &out);
@@ -385,8 +389,9 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
             FW_CUDA(cudaMemcpyAsync(s.field->d, L.T->d, s.field->bytes, cudaMemcpyDeviceToDevice,
                                     ctx->stream));
         }
-        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, s.st));      // inverse = invert(field)
-        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, s.st + 1));  // field = invert(inverse)
+        // inverse = invert(field), then field = invert(inverse)
+        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, L.R, s.st));
+        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, L.R, s.st + 1));
     }
     return 0;
 }
@@ -536,6 +541,21 @@ bool use_graphs() {
     return !(v && v[0] == '0');
 }
 
+// FASTWARP_TRACE=1: host-side phase times of every level on stderr (capture, instantiate, run).
+bool tracing() {
+    static const bool on = [] {
+        const char* v = std::getenv("FASTWARP_TRACE");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
 int run_level_direct(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
                      const std::vector<const fw_image*>& fs, const std::vector<const fw_image*>& ms,
                      const fw_affine* initial, const RunDev& d, int level, int limit,
@@ -563,6 +583,7 @@ int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
                     const fw_affine* initial, const RunDev& d, int level, int limit,
                     fw_syn_iteration* trace_dev_base) {
     GraphGuard G;
+    const double t0 = tracing() ? now_ms() : 0.0;
     FW_CUDA(cudaGraphCreate(&G.g, 0));
     FW_CUDA(cudaStreamBeginCaptureToGraph(ctx->stream, G.g, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
@@ -597,10 +618,16 @@ int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
         cudaGetLastError();
         return rc;
     }
+    const double t1 = tracing() ? now_ms() : 0.0;
     FW_CUDA(cudaGraphInstantiate(&G.e, G.g, 0));
+    const double t2 = tracing() ? now_ms() : 0.0;
     FW_CUDA(cudaGraphLaunch(G.e, ctx->stream));
     ctx->stats.graph_launches++;
-    return sync(ctx);
+    int rc2 = sync(ctx);
+    if (tracing())
+        std::fprintf(stderr, "[fastwarp] level %d (%lld voxels): capture %.2f ms, instantiate %.2f ms, "
+                     "run %.2f ms\n", level, (long long)L.grid.count(), t1 - t0, t2 - t1, now_ms() - t2);
+    return rc2;
 }
 
 int check_status(int status) {
@@ -663,6 +690,7 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
                    fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
                    int64_t* count) {
     FW_TRY(syn_validate(r));
+    const double t_start = tracing() ? now_ms() : 0.0;
     FW_TRY(check_masks(ctx, fixed_mask, moving_mask));
     const int C = r->channels;
     for (int c = 0; c < C; ++c) FW_CHECK(fixed[c] && moving[c], "syn: null channel image");
@@ -806,6 +834,9 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
     }
     free_state();
     if (count) *count = done;
+    if (tracing())
+        std::fprintf(stderr, "[fastwarp] registration: %d iterations, %.2f ms on the host\n", done,
+                     now_ms() - t_start);
     return rc;
 }
 

@@ -241,6 +241,35 @@ int fw_cc_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* f
                                                   fw_field** d_fixed, fw_field** d_moving,
                                                   double norms[2]);
 
+/* Backend::mi_value_derivative_pair (backend.rs:179-190; cpu/mod.rs:352-381 ->
+ * MattesMi::evaluate_dense, metric/mi.rs:601-680): dense Mattes MI of two images on one grid in
+ * both directions, (fixed, moving) then (moving, fixed). Each value is -MI; each derivative is
+ * sum_k B3'(k - term) ratio[fixed bin, k] * grad(moving image of the direction) per voxel. The
+ * intensity ranges of the bins are measured anew from the images on every call. bins 5..=32. */
+int fw_mi_value_derivative_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                                int32_t bins, double values[2], fw_field** d_fixed,
+                                fw_field** d_moving);
+
+/* Backend::mi_value_derivative_pair_masked (backend.rs:192-205): masks on the images' grid
+ * (NULL: not given); a voxel counts where both masks are not zero, each image's range is
+ * measured inside its own mask; no voxel inside both: FW_NO_VOXEL_IN_MASKS. */
+int fw_mi_value_derivative_pair_masked(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,
+                                       const fw_image* fixed_mask, const fw_image* moving_mask,
+                                       int32_t bins, double values[2], fw_field** d_fixed,
+                                       fw_field** d_moving);
+
+/* ..._with_norms (backend.rs:207-240): plus the L2 norms of both derivatives. */
+int fw_mi_value_derivative_pair_with_norms(fw_ctx* ctx, const fw_image* fixed,
+                                           const fw_image* moving, int32_t bins, double values[2],
+                                           fw_field** d_fixed, fw_field** d_moving,
+                                           double norms[2]);
+int fw_mi_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* fixed,
+                                                  const fw_image* moving,
+                                                  const fw_image* fixed_mask,
+                                                  const fw_image* moving_mask, int32_t bins,
+                                                  double values[2], fw_field** d_fixed,
+                                                  fw_field** d_moving, double norms[2]);
+
 /* No counterpart in the reference. The CC pair above for callers that cannot allocate device
  * memory: code recording into a CUDA stream capture (an allocation there breaks the capture),
  * hosts whose own pool allocator owns the GPU's memory (a framework's caching allocator, a server
@@ -375,9 +404,10 @@ int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_gr
 /* Times `reps` launches of each kernel of one SyN iteration on the grid of `fixed` with CUDA
  * events on the context's stream: mean ms per launch and algorithmic bytes per launch of
  * [0] warp, [1] CC pair, [2] Gaussian smoothing + max norm, [3] compose + scale,
- * [4] inversion measure, [5] inversion body (update + next measurement). */
+ * [4] inversion measure (keeps the residual), [5] last inversion body (update from the kept
+ * residual), [6] inversion body followed by the next measurement. */
 int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int32_t radius,
-                    double variance, int32_t reps, double ms[6], double bytes[6]);
+                    double variance, int32_t reps, double ms[7], double bytes[7]);
 
 /* Sets a flag polled before every level and iteration (SynOptions::cancel, syn.rs:80-85);
  * a run that sees it set fails with FW_ERR_CANCELLED. Pass NULL to clear. */

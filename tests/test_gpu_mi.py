@@ -85,3 +85,94 @@ def test_all_samples_outside_is_an_error(backend):
     far = linear_transform("euler", [0, 0, 0, 500.0, 0, 0])
     with pytest.raises(FastwarpError, match="all samples map outside"):
         level.value(far)
+
+
+# ---- dense Mattes MI pair of the SyN stage (Backend::mi_value_derivative_pair[_masked]) -------
+# cpu/mod.rs:352-381: evaluate_dense twice, (fixed, moving) then (moving, fixed), identity
+# transforms, masks on the images' grid. Oracle: the f64 dense restatement pinned against the
+# reference's ITK fixtures (tests/test_oracle.py::test_dense_mattes_matches_itk). Tolerances:
+# value 1e-5 relative, derivative 5e-4 of its largest component (parity.rs:45-48).
+
+def dense_case(size=(21, 19, 17), spacing=(1.2, 1.0, 1.4), direction=None, seed=5):
+    og = O.make_grid(size, spacing, (-4.0, 3.0, 1.5), direction)
+    g = make_grid(size, spacing, (-4.0, 3.0, 1.5), direction)
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = size
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    f = 2.0 + np.sin(0.33 * x) * np.cos(0.27 * y) + 0.7 * np.sin(0.21 * z + 0.1 * x)
+    m = 2.0 + np.sin(0.33 * (x - 0.6) + 0.1) * np.cos(0.27 * (y + 0.5)) + \
+        0.7 * np.sin(0.21 * (z - 0.3) + 0.1 * x) + 0.02 * rng.standard_normal(f.shape)
+    return og, g, f.astype(np.float32), m.astype(np.float32)
+
+
+def oracle_pair(og, f, m, bins, fm=None, mm=None):
+    zero = np.zeros(f.shape + (3,))
+    f64, m64 = f.astype(np.float64), m.astype(np.float64)
+    a = O.mi_dense(og, f64, og, m64, zero, bins, og if fm is not None else None, fm,
+                   og if mm is not None else None, mm)
+    b = O.mi_dense(og, m64, og, f64, zero, bins, og if mm is not None else None, mm,
+                   og if fm is not None else None, fm)
+    return a, b
+
+
+@pytest.mark.parametrize("bins", [32, 12])
+@pytest.mark.parametrize("oblique", [False, True])
+def test_dense_mi_pair_matches_the_oracle(backend, bins, oblique):
+    og, g, f, m = dense_case(direction=rot_z(0.2) @ rot_x(-0.1) if oblique else None)
+    fi, mi = backend.upload_image(g, f), backend.upload_image(g, m)
+    ((v0, d0), (v1, d1)), norms = backend.mi_value_derivative_pair_with_norms(fi, mi, bins)
+    (w0, n0, e0), (w1, n1, e1) = oracle_pair(og, f, m, bins)
+    assert abs(v0 - w0) <= 1e-5 * abs(w0) and abs(v1 - w1) <= 1e-5 * abs(w1)
+    g0, g1 = backend.download_field(d0), backend.download_field(d1)
+    assert np.abs(g0 - e0).max() <= 5e-4 * np.abs(e0).max()
+    assert np.abs(g1 - e1).max() <= 5e-4 * np.abs(e1).max()
+    assert abs(norms[0] - np.sqrt((e0 ** 2).sum())) <= 5e-4 * np.sqrt((e0 ** 2).sum())
+    (u0, c0), (u1, c1) = backend.mi_value_derivative_pair(fi, mi, bins)
+    assert (u0, u1) == (v0, v1)
+    assert np.array_equal(backend.download_field(c0), g0)
+
+
+def test_masked_dense_mi_pair_matches_the_oracle(backend):
+    og, g, f, m = dense_case(seed=9)
+    nz, ny, nx = f.shape
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    fm = ((x - 8) ** 2 + (y - 9) ** 2 + (z - 8) ** 2 > 16).astype(np.float64)
+    mm = (x < nx - 3).astype(np.float64) * 2.0  # any non-zero value is inside
+    fi, mi = backend.upload_image(g, f), backend.upload_image(g, m)
+    fmi, mmi = backend.upload_image(g, fm), backend.upload_image(g, mm)
+    (v0, d0), (v1, d1) = backend.mi_value_derivative_pair_masked(fi, mi, fmi, mmi, 32)
+    (w0, n0, e0), (w1, n1, e1) = oracle_pair(og, f, m, 32, fm, mm)
+    assert abs(v0 - w0) <= 1e-5 * abs(w0) and abs(v1 - w1) <= 1e-5 * abs(w1)
+    g0, g1 = backend.download_field(d0), backend.download_field(d1)
+    assert np.abs(g0 - e0).max() <= 5e-4 * np.abs(e0).max()
+    assert np.abs(g1 - e1).max() <= 5e-4 * np.abs(e1).max()
+    outside = (fm == 0) | (mm == 0)
+    assert np.all(g0[outside] == 0.0) and np.all(g1[outside] == 0.0)
+    # masks of ones are no masks
+    ones = backend.upload_image(g, np.ones(f.shape, np.float32))
+    (a0, b0), (a1, b1) = backend.mi_value_derivative_pair_masked(fi, mi, ones, ones, 32)
+    (p0, q0), (p1, q1) = backend.mi_value_derivative_pair(fi, mi, 32)
+    assert (a0, a1) == (p0, p1)
+    assert np.array_equal(backend.download_field(b0), backend.download_field(q0))
+
+
+def test_dense_mi_errors_carry_the_reference_messages(backend):
+    from fastwarp_b200 import FastwarpError
+    og, g, f, m = dense_case(size=(9, 8, 7))
+    fi, mi = backend.upload_image(g, f), backend.upload_image(g, m)
+    const = backend.upload_image(g, np.full(f.shape, 3.0, np.float32))
+    with pytest.raises(FastwarpError, match="the fixed image is constant"):
+        backend.mi_value_derivative_pair(const, mi, 32)
+    with pytest.raises(FastwarpError, match="the moving image is constant"):
+        backend.mi_value_derivative_pair(fi, const, 32)
+    with pytest.raises(FastwarpError, match="at least five histogram bins"):
+        backend.mi_value_derivative_pair(fi, mi, 4)
+    zeros = backend.upload_image(g, np.zeros(f.shape, np.float32))
+    with pytest.raises(FastwarpError, match="no finite fixed-image voxel lies inside the fixed mask"):
+        backend.mi_value_derivative_pair_masked(fi, mi, zeros, None, 32)
+    half = np.zeros(f.shape, np.float32)
+    half[:, :, :4] = 1.0
+    other = 1.0 - half
+    with pytest.raises(FastwarpError, match="no voxel of the registration level lies inside"):
+        backend.mi_value_derivative_pair_masked(fi, mi, backend.upload_image(g, half),
+                                                backend.upload_image(g, other), 32)
