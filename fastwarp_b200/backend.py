@@ -144,6 +144,16 @@ class CudaBackend:
         check(lib().fw_ctx_stats(self.ctx, C.byref(s)))
         return {k: int(getattr(s, k)) for k, _ in N.Stats._fields_}
 
+    def release_idle_buffers(self):
+        """Backend::release_idle_buffers (backend.rs:48-50): returns the buffers the context
+        keeps for reuse to the device."""
+        check(lib().fw_ctx_release_idle_buffers(self.ctx))
+
+    def cached_bytes(self) -> int:
+        v = C.c_uint64()
+        check(lib().fw_ctx_cached_bytes(self.ctx, C.byref(v)))
+        return int(v.value)
+
     def reset_stats(self):
         lib().fw_ctx_reset_stats(self.ctx)
 

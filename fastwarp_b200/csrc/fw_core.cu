@@ -123,16 +123,31 @@ DevGrid dev_grid(const HostGrid& g) {
 
 // ---- buffers --------------------------------------------------------------------------------
 
+// Sizes are rounded up to 4 KB so that buffers of nearby sizes share the cache.
+static size_t cache_size(size_t bytes) { return (std::max<size_t>(bytes, 256) + 4095) & ~(size_t)4095; }
+
 int dev_alloc(fw_ctx* ctx, size_t bytes, void** out) {
     *out = nullptr;
-    if (bytes == 0) bytes = 256;
-    cudaError_t e = cudaMallocAsync(out, bytes, ctx->stream);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(FW_ERR_MEMORY, std::string("device allocation of ") + std::to_string(bytes) +
-                                       " bytes failed: " + cudaGetErrorString(e));
+    const size_t sz = cache_size(bytes);
+    {
+        std::lock_guard<std::mutex> lock(ctx->cache_mu);
+        auto it = ctx->cache.find(sz);
+        if (it != ctx->cache.end()) {
+            *out = it->second;
+            ctx->cache.erase(it);
+            ctx->cached_bytes -= sz;
+        }
     }
-    uint64_t live = ctx->live_bytes.fetch_add(bytes) + bytes;
+    if (!*out) {
+        cudaError_t e = cudaMallocFromPoolAsync(out, sz, ctx->pool, ctx->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *out = nullptr;
+            return fail(FW_ERR_MEMORY, std::string("device allocation of ") + std::to_string(bytes) +
+                                           " bytes failed: " + cudaGetErrorString(e));
+        }
+    }
+    uint64_t live = ctx->live_bytes.fetch_add(sz) + sz;
     ctx->stats.live_device_bytes = live;
     if (live > ctx->stats.peak_device_bytes) ctx->stats.peak_device_bytes = live;
     return 0;
@@ -140,9 +155,28 @@ int dev_alloc(fw_ctx* ctx, size_t bytes, void** out) {
 
 void dev_free(fw_ctx* ctx, void* p, size_t bytes) {
     if (!p) return;
-    cudaFreeAsync(p, ctx->stream);
-    ctx->live_bytes.fetch_sub(bytes);
+    const size_t sz = cache_size(bytes);
+    {
+        std::lock_guard<std::mutex> lock(ctx->cache_mu);
+        ctx->cache.emplace(sz, p);
+        ctx->cached_bytes += sz;
+    }
+    ctx->live_bytes.fetch_sub(sz);
     ctx->stats.live_device_bytes = ctx->live_bytes.load();
+}
+
+// Returns the cached buffers to the pool and the pool's unused memory to the device.
+int trim_cache(fw_ctx* ctx) {
+    std::unordered_multimap<size_t, void*> drop;
+    {
+        std::lock_guard<std::mutex> lock(ctx->cache_mu);
+        drop.swap(ctx->cache);
+        ctx->cached_bytes = 0;
+    }
+    for (auto& kv : drop) cudaFreeAsync(kv.second, ctx->stream);
+    FW_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->pool) FW_CUDA(cudaMemPoolTrimTo(ctx->pool, 0));
+    return 0;
 }
 
 int new_image(fw_ctx* ctx, const HostGrid& g, fw_image** out) {
@@ -324,7 +358,7 @@ struct FieldArgs {
 __global__ void __launch_bounds__(256) k_compose(FieldArgs a, const float* __restrict__ u,
                                                  const float* w, float* out,
                                                  const unsigned int* __restrict__ max_bits,
-                                                 double step) {
+                                                 double step, float4* __restrict__ out4) {
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= a.g.n) return;
     float s = 1.0f;
@@ -343,9 +377,18 @@ __global__ void __launch_bounds__(256) k_compose(FieldArgs a, const float* __res
     float d[3] = {0.0f, 0.0f, 0.0f};
     if (inside_index(c[0], c[1], c[2], a.g.nx, a.g.ny, a.g.nz))
         vec_at_index(u, a.ps, a.g.nx, a.g.ny, a.g.nz, c[0], c[1], c[2], d);
-    out[l] = fmaf(s, d[0], wx);
-    out[l + a.ps] = fmaf(s, d[1], wy);
-    out[l + 2 * a.ps] = fmaf(s, d[2], wz);
+    const float ox = fmaf(s, d[0], wx), oy = fmaf(s, d[1], wy), oz = fmaf(s, d[2], wz);
+    out[l] = ox;
+    out[l + a.ps] = oy;
+    out[l + 2 * a.ps] = oz;
+    if (out4) out4[l] = make_float4(ox, oy, oz, 0.0f);
+}
+
+__global__ void __launch_bounds__(256) k_pack4(FieldArgs a, const float* __restrict__ f,
+                                               float4* __restrict__ out4) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= a.g.n) return;
+    out4[l] = make_float4(f[l], f[l + a.ps], f[l + 2 * a.ps], 0.0f);
 }
 
 // field_ops.rs:580-605: onto another grid, scalar linear interpolation per component, zero
@@ -512,11 +555,17 @@ int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const f
 }
 
 int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, fw_field* out,
-                   const unsigned int* d_scale_max_bits, double step) {
+                   const unsigned int* d_scale_max_bits, double step, float4* out4) {
     FieldArgs a{dev_grid(warping->grid), warping->ps};
     k_compose<<<blocks_for(a.g.n), 256, 0, ctx->stream>>>(a, disp->d, warping->d, out->d,
-                                                          d_scale_max_bits, step);
+                                                          d_scale_max_bits, step, out4);
     return check_launch(ctx, "k_compose");
+}
+
+int launch_pack4(fw_ctx* ctx, const fw_field* f, float4* out4) {
+    FieldArgs a{dev_grid(f->grid), f->ps};
+    k_pack4<<<blocks_for(a.g.n), 256, 0, ctx->stream>>>(a, f->d, out4);
+    return check_launch(ctx, "k_pack4");
 }
 
 int launch_max_norm(fw_ctx* ctx, const fw_field* f, unsigned int* d_max_bits) {
@@ -595,11 +644,24 @@ int fw_ctx_create(int device, fw_ctx** out) {
         delete ctx;
         return cuda_fail(e, "cudaStreamCreate");
     }
-    // keep freed blocks in the pool: the buffer pool of the wgpu engine (pool.rs)
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    // a memory pool of the context's own that keeps freed blocks (the buffer pool of the wgpu
+    // engine, pool.rs): every allocation and free is ordered on the context's stream, so after
+    // the first registration of a shape the next ones reuse the same blocks; a pool shared with
+    // other streams could not always reuse them and would grow instead
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    e = cudaMemPoolCreate(&ctx->pool, &props);
+    if (e == cudaSuccess) {
         uint64_t threshold = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+        e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fw_ctx_destroy(ctx);
+        return cuda_fail(e, "cudaMemPoolCreate");
     }
     if (cudaMalloc(&ctx->d_counter, 64 * sizeof(unsigned int)) != cudaSuccess ||
         cudaMemset(ctx->d_counter, 0, 64 * sizeof(unsigned int)) != cudaSuccess ||
@@ -620,13 +682,32 @@ int fw_ctx_create(int device, fw_ctx** out) {
 void fw_ctx_destroy(fw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& kv : ctx->cache) cudaFreeAsync(kv.second, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    ctx->cache.clear();
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->aux) cudaStreamDestroy(ctx->aux);
+    // the pool's blocks go back to the device; a buffer still outstanding keeps them until freed
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
+}
+
+int fw_ctx_release_idle_buffers(fw_ctx* ctx) {
+    FW_CHECK(ctx, "null context");
+    return trim_cache(ctx);
+}
+
+int fw_ctx_cached_bytes(const fw_ctx* ctx, uint64_t* out) {
+    FW_CHECK(ctx && out, "null argument");
+    std::lock_guard<std::mutex> lock(const_cast<fw_ctx*>(ctx)->cache_mu);
+    *out = ctx->cached_bytes;
+    return 0;
 }
 
 void* fw_ctx_stream(fw_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

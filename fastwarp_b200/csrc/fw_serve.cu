@@ -67,6 +67,7 @@ int estimate(const fw_syn_request* q, uint64_t* out) {
                  (C > 1 ? 2 : 0) + (r->total_field_variance > 0 ? 1 : 0) + 2 /* outputs */;
     b += 12 * ps * (uint64_t)fields;
     b += 4 * (uint64_t)n * 2 * C;                      // warped images
+    b += 16 * (uint64_t)n;                             // interleaved copy for the inversions
     b += 12 * psp * 4;                                 // state of the previous level at a transition
     b += 2u << 20;                                     // records and scalars
     *out = b;

@@ -196,161 +196,153 @@ __global__ void __launch_bounds__(SNT) k_smooth(SmoothArgs a, const float* __res
     }
 }
 
-// Fixed-radius variant (the same radius on the three axes, the usual case): taps unrolled from
-// the parameter bank, the x pass vectorised (each item reads a 4 + 2r window as float4 and makes
-// four outputs), the z window kept as a register ring shifted once per slice, and the next slice
-// prefetched into registers while the current one is filtered. Two 256-thread CTAs per SM.
-constexpr int RTX = 32;
-constexpr int RTY = 8;
-constexpr int RNT = RTX * RTY;
+// ---- fixed-radius path (the same taps on the three axes, the usual case) ----------------------
+//
+// The separable filter as two bandwidth-bound sweeps instead of one fused 2.5D kernel (whose z
+// ring of registers shifts every slice and whose x pass repeats the y halo rows): k_smooth_xy
+// filters each z slice along x then y through shared memory (32 x 32 output tile, clamped halo)
+// into a temporary field; k_smooth_z filters along z from a fixed-index register window of
+// Z_SEG + 2R values per column and applies the faces, the w1/w2 blend and the fused max norm.
+// Both passes accumulate taps in the reference's order (field_ops.rs:508-528), x then y then z.
+
+constexpr int XY_T = 32;     // output tile edge of the xy pass
+constexpr int XY_NT = 256;   // threads: 32 columns x 8 rows, 4 output rows each
+constexpr int Z_SEG = 16;    // z outputs per thread of the z pass
 
 template <int R>
-__global__ void __launch_bounds__(RNT, 2) k_smooth_r(SmoothArgs a, const float* __restrict__ in,
-                                                     float* __restrict__ out,
-                                                     unsigned int* __restrict__ max_bits) {
-    constexpr int HX = RTX + 2 * R, HY = RTY + 2 * R, W = 2 * R + 1;
-    constexpr int HXP = (HX + 3) & ~3;             // row stride: rows start on 16 bytes
-    constexpr int TILE = HY * HXP;
-    constexpr int NV = (4 + 2 * R + 3) / 4;        // float4 loads per x-pass window
-    constexpr int PER = (3 * HY * HX + RNT - 1) / RNT;  // prefetched values per thread
-    __shared__ __align__(16) float tile[3 * TILE + 4 * NV];
-    __shared__ __align__(16) float xs[3 * HY * RTX];
-    const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
-    const int tid = threadIdx.x, tx = tid % RTX, ty = tid / RTX;
-    const int x0 = blockIdx.x * RTX, y0 = blockIdx.y * RTY;
-    const int z0 = blockIdx.z * a.zchunk, z1 = min(z0 + a.zchunk, nz);
-    const int x = x0 + tx, y = y0 + ty;
-    const bool own = x < nx && y < ny;
-    const long long sxy = (long long)nx * ny;
-    const float* taps = a.tx_;  // identical on the three axes here
-    float ring[W][3];
-#pragma unroll
-    for (int t = 0; t < W; ++t) ring[t][0] = ring[t][1] = ring[t][2] = 0.0f;
-    float pre[PER];
-    // the slice-invariant part of every prefetch: offset in the slice (clamped x, y; component
-    // plane) and destination in the tile (-1: no value for this thread)
-    int src_off[PER], dst_off[PER];
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        int s = tid + q * RNT;
-        src_off[q] = 0;
-        dst_off[q] = -1;
-        if (s < 3 * HY * HX) {
-            int c = s / (HY * HX), rr = s - c * (HY * HX);
-            int hy = rr / HX, hx = rr - hy * HX;
-            int gx = min(max(x0 - R + hx, 0), nx - 1);
-            int gy = min(max(y0 - R + hy, 0), ny - 1);
-            src_off[q] = gy * nx + gx + c * (int)a.ps_in;
-            dst_off[q] = c * TILE + hy * HXP + hx;
+__global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* __restrict__ in,
+                                                     float* __restrict__ tmp, long long ps_tmp) {
+    constexpr int HX = XY_T + 2 * R, HY = XY_T + 2 * R;
+    constexpr int HXP = (HX + 3) & ~3;       // rows start on 16 bytes
+    constexpr int NV = (4 + 2 * R + 3) / 4;  // float4 loads per x window of four outputs
+    __shared__ __align__(16) float tile[HY * HXP + 4 * NV];
+    __shared__ __align__(16) float xs[HY * XY_T];
+    const int nx = a.g.nx, ny = a.g.ny;
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    const int x0 = blockIdx.x * XY_T, y0 = blockIdx.y * XY_T;
+    const long long zoff = (long long)blockIdx.z * nx * ny;
+    const int x = x0 + tx;
+    for (int c = 0; c < 3; ++c) {
+        const float* src = in + c * a.ps_in + zoff;
+        for (int s = tid; s < HY * HX; s += XY_NT) {
+            const int hy = s / HX, hx = s - hy * HX;
+            const int gx = min(max(x0 - R + hx, 0), nx - 1);  // edge replication
+            const int gy = min(max(y0 - R + hy, 0), ny - 1);
+            tile[hy * HXP + hx] = __ldg(src + (long long)gy * nx + gx);
         }
-    }
-    auto fetch = [&](int k) {
-        const int kz = min(max(k, 0), nz - 1);  // edge replication along z
-        const float* base = in + (long long)kz * sxy;
-#pragma unroll
-        for (int q = 0; q < PER; ++q) pre[q] = dst_off[q] >= 0 ? __ldg(base + src_off[q]) : 0.0f;
-    };
-    float vmax = 0.0f;
-    const float isx = (float)(1.0 / a.g.sp[0]), isy = (float)(1.0 / a.g.sp[1]),
-                isz = (float)(1.0 / a.g.sp[2]);
-    int k = z0 - R;
-    fetch(k);
-    for (; k < z1 + R; ++k) {
-        __syncthreads();  // the previous slice's passes are done with tile and xs
-#pragma unroll
-        for (int q = 0; q < PER; ++q)
-            if (dst_off[q] >= 0) tile[dst_off[q]] = pre[q];
         __syncthreads();
-        if (k + 1 < z1 + R) fetch(k + 1);  // in flight while this slice is filtered
-        // x pass: (component, halo row, group of four output columns)
-        for (int s = tid; s < 3 * HY * (RTX / 4); s += RNT) {
-            int c = s / (HY * (RTX / 4)), rr = s - c * (HY * (RTX / 4));
-            int hy = rr / (RTX / 4), g4 = rr - hy * (RTX / 4);
-            const float4* row = reinterpret_cast<const float4*>(tile + c * TILE + hy * HXP) + g4;
+        // x pass: (halo row, group of four output columns)
+        for (int s = tid; s < HY * (XY_T / 4); s += XY_NT) {
+            const int hy = s >> 3, g4 = s & 7;
+            const float4* row = reinterpret_cast<const float4*>(tile + hy * HXP) + g4;
             float win[4 * NV];
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                float4 q4 = row[v];
-                win[4 * v] = q4.x;
-                win[4 * v + 1] = q4.y;
-                win[4 * v + 2] = q4.z;
-                win[4 * v + 3] = q4.w;
+                const float4 q = row[v];
+                win[4 * v] = q.x;
+                win[4 * v + 1] = q.y;
+                win[4 * v + 2] = q.z;
+                win[4 * v + 3] = q.w;
             }
-            float4 o;
-            float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f, acc3 = 0.0f;
+            float4 o = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
-            for (int t = 0; t < W; ++t) {
-                const float w = taps[t];
-                acc0 = fmaf(w, win[t], acc0);
-                acc1 = fmaf(w, win[t + 1], acc1);
-                acc2 = fmaf(w, win[t + 2], acc2);
-                acc3 = fmaf(w, win[t + 3], acc3);
+            for (int t = 0; t <= 2 * R; ++t) {
+                const float w = a.tx_[t];
+                o.x = fmaf(w, win[t], o.x);
+                o.y = fmaf(w, win[t + 1], o.y);
+                o.z = fmaf(w, win[t + 2], o.z);
+                o.w = fmaf(w, win[t + 3], o.w);
             }
-            o.x = acc0;
-            o.y = acc1;
-            o.z = acc2;
-            o.w = acc3;
-            reinterpret_cast<float4*>(xs + c * HY * RTX + hy * RTX)[g4] = o;
+            reinterpret_cast<float4*>(xs + hy * XY_T)[g4] = o;
         }
         __syncthreads();
-        // y pass for the thread's own column, then shift it into the z ring
+        // y pass: four consecutive output rows of the thread's column
+        float col[4 + 2 * R];
 #pragma unroll
-        for (int t = 0; t < W - 1; ++t) {
-            ring[t][0] = ring[t + 1][0];
-            ring[t][1] = ring[t + 1][1];
-            ring[t][2] = ring[t + 1][2];
-        }
+        for (int t = 0; t < 4 + 2 * R; ++t) col[t] = xs[(ty * 4 + t) * XY_T + tx];
+        float* dst = tmp + c * ps_tmp + zoff;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float* col = xs + c * HY * RTX + ty * RTX + tx;
+        for (int q = 0; q < 4; ++q) {
             float acc = 0.0f;
 #pragma unroll
-            for (int t = 0; t < W; ++t) acc = fmaf(taps[t], col[t * RTX], acc);
-            ring[W - 1][c] = acc;
+            for (int t = 0; t <= 2 * R; ++t) acc = fmaf(a.ty_[t], col[q + t], acc);
+            const int y = y0 + ty * 4 + q;
+            if (x < nx && y < ny) dst[(long long)y * nx + x] = acc;
         }
-        const int z = k - R;
-        if (z < z0 || !own) continue;
-        float v[3];
+        __syncthreads();  // the next component overwrites tile and xs
+    }
+}
+
+// blockIdx.x: z segment (fastest, so neighbouring segments share their halo rows in L2),
+// blockIdx.y: 32 columns in x, blockIdx.z: 8 rows in y.
+template <int R>
+__global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __restrict__ tmp,
+                                                  long long ps_tmp, const float* in,
+                                                  float* out,
+                                                  unsigned int* __restrict__ max_bits) {
+    const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
+    const int x = blockIdx.y * 32 + (threadIdx.x & 31), y = blockIdx.z * 8 + (threadIdx.x >> 5);
+    const int zs = blockIdx.x * Z_SEG;
+    const long long sxy = (long long)nx * ny;
+    float vmax = 0.0f;
+    if (x < nx && y < ny) {
+        const long long col = (long long)y * nx + x;
+        const float isp[3] = {(float)(1.0 / a.g.sp[0]), (float)(1.0 / a.g.sp[1]),
+                              (float)(1.0 / a.g.sp[2])};
+        const bool edge_xy = x == 0 || y == 0 || x == nx - 1 || y == ny - 1;
+        float nsq[Z_SEG];
+#pragma unroll
+        for (int q = 0; q < Z_SEG; ++q) nsq[q] = 0.0f;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            float acc = 0.0f;
+            const float* src = tmp + c * ps_tmp + col;
+            float w[Z_SEG + 2 * R];
 #pragma unroll
-            for (int t = 0; t < W; ++t) acc = fmaf(taps[t], ring[t][c], acc);
-            v[c] = acc;
-        }
-        const long long l = (long long)z * sxy + (long long)y * nx + x;
-        const bool face = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
-        float o[3];
+            for (int t = 0; t < Z_SEG + 2 * R; ++t) {
+                const int zz = min(max(zs - R + t, 0), nz - 1);  // edge replication
+                w[t] = __ldg(src + zz * sxy);
+            }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            float orig = a.w2 != 0.0f ? __ldg(in + l + c * a.ps_in) : 0.0f;
-            o[c] = face ? 0.0f : (a.w2 != 0.0f ? v[c] * a.w1 + orig * a.w2 : v[c]);
-            out[l + c * a.ps_out] = o[c];
+            for (int q = 0; q < Z_SEG; ++q) {
+                const int z = zs + q;
+                if (z >= nz) break;
+                float v = 0.0f;
+#pragma unroll
+                for (int t = 0; t <= 2 * R; ++t) v = fmaf(a.tz_[t], w[q + t], v);
+                const long long l = (long long)z * sxy + col;
+                const bool face = edge_xy || z == 0 || z == nz - 1;
+                float o;
+                if (face) o = 0.0f;
+                else if (a.w2 != 0.0f) o = v * a.w1 + in[l + c * a.ps_in] * a.w2;
+                else o = v;
+                out[l + c * a.ps_out] = o;
+                const float p = o * isp[c];
+                nsq[q] = fmaf(p, p, nsq[q]);
+            }
         }
         if (max_bits) {
-            float px = o[0] * isx, py = o[1] * isy, pz = o[2] * isz;
-            vmax = __int_as_float(max(__float_as_int(vmax),
-                                      __float_as_int(nan_canon(sqrtf(px * px + py * py + pz * pz)))));
+#pragma unroll
+            for (int q = 0; q < Z_SEG; ++q)
+                if (zs + q < nz)
+                    vmax = __int_as_float(max(__float_as_int(vmax),
+                                              __float_as_int(nan_canon(sqrtf(nsq[q])))));
         }
     }
     if (max_bits) {
         vmax = warp_max_f(vmax);
-        if ((tid & 31) == 0 && vmax > 0.0f) atomicMax(max_bits, __float_as_uint(vmax));
+        if ((threadIdx.x & 31) == 0 && vmax > 0.0f) atomicMax(max_bits, __float_as_uint(vmax));
     }
 }
 
 template <int R>
-int launch_smooth_r(fw_ctx* ctx, SmoothArgs a, const fw_field* in, fw_field* out,
-                    unsigned int* d_max_bits) {
-    dim3 grid((a.g.nx + RTX - 1) / RTX, (a.g.ny + RTY - 1) / RTY, 1);
-    long long tiles = (long long)grid.x * grid.y;
-    int want = (int)std::max<long long>(1, (3LL * ctx->num_sms + tiles - 1) / tiles);
-    int chunk = (a.g.nz + want - 1) / want;
-    chunk = std::max(chunk, std::min(a.g.nz, 4 * R + 8));
-    a.zchunk = chunk;
-    grid.z = (a.g.nz + chunk - 1) / chunk;
-    k_smooth_r<R><<<grid, RNT, 0, ctx->stream>>>(a, in->d, out->d, d_max_bits);
-    return check_launch(ctx, "k_smooth_r");
+int launch_smooth_xyz(fw_ctx* ctx, const SmoothArgs& a, const fw_field* in, fw_field* out,
+                      fw_field* tmp, unsigned int* d_max_bits) {
+    dim3 g1((a.g.nx + XY_T - 1) / XY_T, (a.g.ny + XY_T - 1) / XY_T, a.g.nz);
+    k_smooth_xy<R><<<g1, XY_NT, 0, ctx->stream>>>(a, in->d, tmp->d, tmp->ps);
+    FW_TRY(check_launch(ctx, "k_smooth_xy"));
+    dim3 g2((a.g.nz + Z_SEG - 1) / Z_SEG, (a.g.nx + 31) / 32, (a.g.ny + 7) / 8);
+    k_smooth_z<R><<<g2, 256, 0, ctx->stream>>>(a, tmp->d, tmp->ps, in->d, out->d, d_max_bits);
+    return check_launch(ctx, "k_smooth_z");
 }
 
 // ---- Deriche recursive Gaussian (pyramid.rs:186-300, 418-427) --------------------------------
@@ -509,7 +501,7 @@ __global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b
 }  // namespace
 
 int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double variance,
-                  unsigned int* d_max_bits) {
+                  unsigned int* d_max_bits, fw_field* tmp) {
     SmoothArgs a;
     std::memset(&a, 0, sizeof(a));
     a.g = dev_grid(in->grid);
@@ -531,26 +523,29 @@ int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double varianc
     double w1 = variance < 0.5 ? 1.0 - variance / 0.5 : 1.0;
     a.w1 = (float)w1;
     a.w2 = (float)(1.0 - w1);
-    bool same = r[0] == r[1] && r[1] == r[2] && 3 * in->ps < 2147483647LL;  // int32 offsets
+    bool same = tmp != nullptr && r[0] == r[1] && r[1] == r[2];
     for (int t = 0; same && t <= 2 * r[0]; ++t)
         same = a.tx_[t] == a.ty_[t] && a.ty_[t] == a.tz_[t];
     if (same) {
+        FW_CHECK(tmp->grid.same(in->grid) && tmp != in && tmp != out,
+                 "smooth field: the temporary field must be a third field on the same grid");
         switch (r[0]) {
-            case 1: return launch_smooth_r<1>(ctx, a, in, out, d_max_bits);
-            case 2: return launch_smooth_r<2>(ctx, a, in, out, d_max_bits);
-            case 3: return launch_smooth_r<3>(ctx, a, in, out, d_max_bits);
-            case 4: return launch_smooth_r<4>(ctx, a, in, out, d_max_bits);
-            case 5: return launch_smooth_r<5>(ctx, a, in, out, d_max_bits);
-            case 6: return launch_smooth_r<6>(ctx, a, in, out, d_max_bits);
-            case 7: return launch_smooth_r<7>(ctx, a, in, out, d_max_bits);
-            case 8: return launch_smooth_r<8>(ctx, a, in, out, d_max_bits);
-            case 9: return launch_smooth_r<9>(ctx, a, in, out, d_max_bits);
-            case 10: return launch_smooth_r<10>(ctx, a, in, out, d_max_bits);
-            case 11: return launch_smooth_r<11>(ctx, a, in, out, d_max_bits);
-            case 12: return launch_smooth_r<12>(ctx, a, in, out, d_max_bits);
+            case 1: return launch_smooth_xyz<1>(ctx, a, in, out, tmp, d_max_bits);
+            case 2: return launch_smooth_xyz<2>(ctx, a, in, out, tmp, d_max_bits);
+            case 3: return launch_smooth_xyz<3>(ctx, a, in, out, tmp, d_max_bits);
+            case 4: return launch_smooth_xyz<4>(ctx, a, in, out, tmp, d_max_bits);
+            case 5: return launch_smooth_xyz<5>(ctx, a, in, out, tmp, d_max_bits);
+            case 6: return launch_smooth_xyz<6>(ctx, a, in, out, tmp, d_max_bits);
+            case 7: return launch_smooth_xyz<7>(ctx, a, in, out, tmp, d_max_bits);
+            case 8: return launch_smooth_xyz<8>(ctx, a, in, out, tmp, d_max_bits);
+            case 9: return launch_smooth_xyz<9>(ctx, a, in, out, tmp, d_max_bits);
+            case 10: return launch_smooth_xyz<10>(ctx, a, in, out, tmp, d_max_bits);
+            case 11: return launch_smooth_xyz<11>(ctx, a, in, out, tmp, d_max_bits);
+            case 12: return launch_smooth_xyz<12>(ctx, a, in, out, tmp, d_max_bits);
             default: break;
         }
     }
+    FW_CHECK(in != out, "smooth field: the general path needs a separate output");
     dim3 grid((a.g.nx + STX - 1) / STX, (a.g.ny + STY - 1) / STY, 1);
     long long tiles = (long long)grid.x * grid.y;
     int want = (int)std::max<long long>(1, (4LL * ctx->num_sms + tiles - 1) / tiles);
@@ -616,14 +611,16 @@ extern "C" {
 int fw_smooth_field(fw_ctx* ctx, fw_field* field, double variance) {
     FW_CHECK(ctx && field, "null argument");
     if (!(variance > 0.0)) return 0;  // returned unchanged (faces not zeroed)
-    fw_field* tmp;
+    fw_field *tmp = nullptr, *res = nullptr;
     FW_TRY(new_field(ctx, field->grid, &tmp));
-    int rc = launch_smooth(ctx, field, tmp, variance, nullptr);
+    int rc = new_field(ctx, field->grid, &res);
+    // the result lands in `res` (tmp holds the xy pass), then takes the field's place
+    if (!rc) rc = launch_smooth(ctx, field, res, variance, nullptr, tmp);
     if (!rc) {
-        // the result takes the field's place
-        std::swap(field->d, tmp->d);
+        std::swap(field->d, res->d);
         rc = sync(ctx);
     }
+    fw_field_free(res);
     fw_field_free(tmp);
     return rc;
 }

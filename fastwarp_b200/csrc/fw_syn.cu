@@ -190,6 +190,9 @@ struct Level {
     fw_field *sF = nullptr, *sM = nullptr;      // smoothed updates
     fw_field* T = nullptr;                      // total-field smoothing
     fw_field* R = nullptr;                      // inversion residual of the last measurement
+    float4* G4 = nullptr;                       // interleaved copy of the field being inverted
+    size_t g4_bytes = 0;
+    fw_ctx* ctx = nullptr;                      // owner of the work buffers
     const fw_image* fmask = nullptr;            // recipe masks on their own grids (or none)
     const fw_image* mmask = nullptr;
     fw_image* valid = nullptr;                  // the masks resolved on the level grid
@@ -205,6 +208,8 @@ void free_level_work(Level& L) {
     fw_field* fs[] = {L.dF, L.dM, L.accF, L.accM, L.sF, L.sM, L.T, L.R};
     for (auto* f : fs) fw_field_free(f);
     L.dF = L.dM = L.accF = L.accM = L.sF = L.sM = L.T = L.R = nullptr;
+    if (L.G4) dev_free(L.ctx, L.G4, L.g4_bytes);
+    L.G4 = nullptr;
 }
 
 int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
@@ -215,9 +220,12 @@ int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
         FW_TRY(new_image(ctx, L.grid, &b));
         L.mmid.push_back(b);
     }
+    L.ctx = ctx;
     FW_TRY(new_field(ctx, L.grid, &L.dF));
     FW_TRY(new_field(ctx, L.grid, &L.dM));
     FW_TRY(new_field(ctx, L.grid, &L.R));
+    L.g4_bytes = sizeof(float4) * (size_t)L.grid.count();
+    FW_TRY(dev_alloc(ctx, L.g4_bytes, (void**)&L.G4));
     if (L.channels > 1) {
         FW_TRY(new_field(ctx, L.grid, &L.accF));
         FW_TRY(new_field(ctx, L.grid, &L.accM));
@@ -266,12 +274,13 @@ int add_while(cudaStream_t s, unsigned int default_value, unsigned int flags,
 
 // One inversion: in graph mode a WHILE node around the body kernel; in direct mode a host loop.
 int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inverse,
-                   fw_field* res, InvState* st) {
+                   fw_field* res, InvState* st, const float4* field4, float4* inverse4_out) {
     if (!graph) {
-        FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, 0, 0));
+        FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, 0, 0, field4));
         InvState h;
         for (int body = 0; body < kSynInvert.max_iterations; ++body) {
-            FW_TRY(enqueue_inversion_body(ctx, field, inverse, res, st, 0, 0));
+            FW_TRY(enqueue_inversion_body(ctx, field, inverse, res, st, 0, 0, field4,
+                                          inverse4_out));
             FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, st, sizeof(InvState), cudaMemcpyDeviceToHost,
                                     ctx->stream));
             FW_TRY(sync(ctx));
@@ -288,7 +297,7 @@ int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inv
     FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
     cudaGraphConditionalHandle h;
     FW_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, h, 1));
+    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, h, 1, field4));
     FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
     cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
     p.conditional.handle = h;
@@ -304,7 +313,7 @@ int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inv
     FW_CUDA(cudaStreamBeginCaptureToGraph(ctx->aux, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
     ctx->stream = ctx->aux;
-    int rc = enqueue_inversion_body(ctx, field, inverse, res, st, h, 1);
+    int rc = enqueue_inversion_body(ctx, field, inverse, res, st, h, 1, field4, inverse4_out);
     ctx->stream = main;
     cudaGraph_t out;
     cudaError_t e = cudaStreamEndCapture(ctx->aux, &out);
@@ -365,8 +374,8 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
     }
     // smooth_field(update variance) with the max norm fused; without smoothing, the max alone
     if (r->update_field_variance > 0.0) {
-        FW_TRY(launch_smooth(ctx, gF, L.sF, r->update_field_variance, d.max_bits));
-        FW_TRY(launch_smooth(ctx, gM, L.sM, r->update_field_variance, d.max_bits + 1));
+        FW_TRY(launch_smooth(ctx, gF, L.sF, r->update_field_variance, d.max_bits, L.R));
+        FW_TRY(launch_smooth(ctx, gM, L.sM, r->update_field_variance, d.max_bits + 1, L.R));
         gF = L.sF;
         gM = L.sM;
     } else {
@@ -382,16 +391,21 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
         InvState* st;
     } sides[2] = {{gF, L.F, L.Fi, d.max_bits, d.inv}, {gM, L.M, L.Mi, d.max_bits + 1, d.inv + 2}};
     for (auto& s : sides) {
-        // compose in place: every voxel reads its own field value and the update elsewhere
-        FW_TRY(launch_compose(ctx, s.u, s.field, s.field, s.max, r->gradient_step));
-        if (r->total_field_variance > 0.0) {
-            FW_TRY(launch_smooth(ctx, s.field, L.T, r->total_field_variance, nullptr));
+        // compose in place: every voxel reads its own field value and the update elsewhere; the
+        // interleaved copy of the result is what the first inversion gathers from
+        const bool total = r->total_field_variance > 0.0;
+        FW_TRY(launch_compose(ctx, s.u, s.field, s.field, s.max, r->gradient_step,
+                              total ? nullptr : L.G4));
+        if (total) {
+            FW_TRY(launch_smooth(ctx, s.field, L.T, r->total_field_variance, nullptr, L.R));
             FW_CUDA(cudaMemcpyAsync(s.field->d, L.T->d, s.field->bytes, cudaMemcpyDeviceToDevice,
                                     ctx->stream));
+            FW_TRY(launch_pack4(ctx, s.field, L.G4));
         }
-        // inverse = invert(field), then field = invert(inverse)
-        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, L.R, s.st));
-        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, L.R, s.st + 1));
+        // inverse = invert(field), whose last body leaves the interleaved inverse in G4 for the
+        // second: field = invert(inverse)
+        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, L.R, s.st, L.G4, L.G4));
+        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, L.R, s.st + 1, L.G4, nullptr));
     }
     return 0;
 }
@@ -644,7 +658,7 @@ int check_status(int status) {
 // Kernels per iteration outside the inversion bodies (for the launch counter).
 int kernels_per_iteration(const fw_syn_recipe* r, int mask_warps) {
     int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) + 2 /*smooth or max*/ +
-            2 /*compose*/ + (r->total_field_variance > 0.0 ? 2 : 0) + 4 * 2 /*inv init+measure*/ +
+            2 /*compose*/ + (r->total_field_variance > 0.0 ? 4 : 0) + 4 * 2 /*inv init+measure*/ +
             1 /*record*/ + mask_warps;
     return k;
 }

@@ -153,6 +153,12 @@ int fw_ctx_create(int device, fw_ctx** out);
 /* Destroys the context and its stream. Free every image, field and MI level made on it first:
  * their free functions use the context's stream. */
 void fw_ctx_destroy(fw_ctx* ctx);
+/* Backend::release_idle_buffers (backend.rs:48-50): a context keeps the device buffers it frees
+ * for the next allocation of the same size (so repeated registrations of one shape allocate
+ * nothing after the first); this returns them and the pool's unused memory to the device. */
+int fw_ctx_release_idle_buffers(fw_ctx* ctx);
+/* Bytes held by that cache. */
+int fw_ctx_cached_bytes(const fw_ctx* ctx, uint64_t* out);
 /* The context's cudaStream_t, for callers that interleave their own device work. */
 void* fw_ctx_stream(fw_ctx* ctx);
 int fw_ctx_synchronize(fw_ctx* ctx);

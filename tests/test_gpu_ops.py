@@ -330,3 +330,22 @@ def test_errors_carry_the_reference_messages(backend):
     with pytest.raises(N.FastwarpError, match="radius"):
         im = backend.upload_image(g1, np.zeros((8, 8, 8), np.float32))
         backend.cc_value_derivative_pair(im, im, 9)
+
+
+def test_freed_buffers_are_reused_and_released_on_request(backend):
+    """A context keeps the buffers it frees for the next allocation of that size (one shape
+    allocates nothing after its first registration); release_idle_buffers (backend.rs:48-50)
+    hands them back."""
+    case = CASES["selftest"]
+    g = fgrid(case)
+    backend.release_idle_buffers()
+    assert backend.cached_bytes() == 0
+    a = backend.zero_field(g)
+    a.free()
+    held = backend.cached_bytes()
+    assert held > 0
+    b = backend.zero_field(g)  # the same size: taken from the cache
+    assert backend.cached_bytes() == 0
+    b.free()
+    backend.release_idle_buffers()
+    assert backend.cached_bytes() == 0
