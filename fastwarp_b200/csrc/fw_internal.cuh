@@ -442,13 +442,17 @@ int launch_cc_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, i
 // Gaussian smoothing of `in` into `out` (out may be in) with the max |u/sp| of the result fused
 // into d_max_bits (may be null); `tmp`, a third field on the grid, holds the xy pass (null: the
 // general single-kernel path, out != in).
+// `out4` (optional): the result also interleaved (x, y, z per voxel) for a gather that follows;
+// `out` may then be null (the fixed-radius path writes only the interleaved copy).
 int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double variance,
-                  unsigned int* d_max_bits, fw_field* tmp);
+                  unsigned int* d_max_bits, fw_field* tmp, float4* out4 = nullptr);
 int launch_max_norm(fw_ctx* ctx, const fw_field* f, unsigned int* d_max_bits);
 // out = warping + step/max * disp(x + warping) (step 1 without max bits); `out4` (optional)
 // also receives the result interleaved (x, y, z, 0) for the gathers of an inversion.
+// `disp4` (optional): an interleaved copy of disp to gather from (disp may then be null).
 int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, fw_field* out,
-                   const unsigned int* d_scale_max_bits, double step, float4* out4 = nullptr);
+                   const unsigned int* d_scale_max_bits, double step, float4* out4 = nullptr,
+                   const float4* disp4 = nullptr);
 // The interleaved copy of a field.
 int launch_pack4(fw_ctx* ctx, const fw_field* f, float4* out4);
 int launch_scale_by_max(fw_ctx* ctx, fw_field* f, const unsigned int* d_max_bits, double step);

@@ -192,6 +192,8 @@ struct Level {
     fw_field* R = nullptr;                      // inversion residual of the last measurement
     float4* G4 = nullptr;                       // interleaved copy of the field being inverted
     size_t g4_bytes = 0;
+    float4* U4 = nullptr;                       // the smoothed update, interleaved
+    bool keep_updates = false;                  // also keep sF / sM (the single-step API)
     fw_ctx* ctx = nullptr;                      // owner of the work buffers
     const fw_image* fmask = nullptr;            // recipe masks on their own grids (or none)
     const fw_image* mmask = nullptr;
@@ -209,7 +211,8 @@ void free_level_work(Level& L) {
     for (auto* f : fs) fw_field_free(f);
     L.dF = L.dM = L.accF = L.accM = L.sF = L.sM = L.T = L.R = nullptr;
     if (L.G4) dev_free(L.ctx, L.G4, L.g4_bytes);
-    L.G4 = nullptr;
+    if (L.U4) dev_free(L.ctx, L.U4, L.g4_bytes);
+    L.G4 = L.U4 = nullptr;
 }
 
 int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
@@ -231,8 +234,11 @@ int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
         FW_TRY(new_field(ctx, L.grid, &L.accM));
     }
     if (r->update_field_variance > 0.0) {
-        FW_TRY(new_field(ctx, L.grid, &L.sF));
-        FW_TRY(new_field(ctx, L.grid, &L.sM));
+        FW_TRY(dev_alloc(ctx, L.g4_bytes, (void**)&L.U4));
+        if (L.keep_updates) {
+            FW_TRY(new_field(ctx, L.grid, &L.sF));
+            FW_TRY(new_field(ctx, L.grid, &L.sM));
+        }
     }
     if (r->total_field_variance > 0.0) FW_TRY(new_field(ctx, L.grid, &L.T));
     if (L.fmask || L.mmask) FW_TRY(new_image(ctx, L.grid, &L.valid));
@@ -372,30 +378,34 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
         gF = L.accF;
         gM = L.accM;
     }
-    // smooth_field(update variance) with the max norm fused; without smoothing, the max alone
-    if (r->update_field_variance > 0.0) {
-        FW_TRY(launch_smooth(ctx, gF, L.sF, r->update_field_variance, d.max_bits, L.R));
-        FW_TRY(launch_smooth(ctx, gM, L.sM, r->update_field_variance, d.max_bits + 1, L.R));
-        gF = L.sF;
-        gM = L.sM;
-    } else {
-        FW_TRY(launch_max_norm(ctx, gF, d.max_bits));
-        FW_TRY(launch_max_norm(ctx, gM, d.max_bits + 1));
-    }
-    // update_total_field for both sides (syn.rs:422-445)
+    // update_total_field for both sides (syn.rs:422-445), one side after the other: smooth the
+    // update (variance in voxels^2) with its max |u/sp| fused, written interleaved for the gather
+    // of the composition; F <- F + (step / max) u(x + F) in place (its interleaved copy is what
+    // the first inversion gathers); optional total-field smoothing; the inversion pair. The two
+    // sides only share scratch (R, U4, G4), so running them in turn gives the reference's fields.
     struct Side {
-        fw_field* u;
+        fw_field* g;       // raw update (CC derivative or channel combination)
+        fw_field* keep;    // where the smoothed update is also kept (single-step API) or null
         fw_field* field;
         fw_field* inverse;
-        const unsigned int* max;
+        unsigned int* max;
         InvState* st;
-    } sides[2] = {{gF, L.F, L.Fi, d.max_bits, d.inv}, {gM, L.M, L.Mi, d.max_bits + 1, d.inv + 2}};
+    } sides[2] = {{gF, L.sF, L.F, L.Fi, d.max_bits, d.inv},
+                  {gM, L.sM, L.M, L.Mi, d.max_bits + 1, d.inv + 2}};
     for (auto& s : sides) {
-        // compose in place: every voxel reads its own field value and the update elsewhere; the
-        // interleaved copy of the result is what the first inversion gathers from
+        const fw_field* u = s.g;
+        const float4* u4 = nullptr;
+        if (r->update_field_variance > 0.0) {
+            FW_TRY(launch_smooth(ctx, s.g, s.keep, r->update_field_variance, s.max, L.R, L.U4));
+            u = s.keep;
+            u4 = L.U4;
+        } else {
+            FW_TRY(launch_max_norm(ctx, s.g, s.max));
+        }
+        // compose in place: every voxel reads its own field value and the update elsewhere
         const bool total = r->total_field_variance > 0.0;
-        FW_TRY(launch_compose(ctx, s.u, s.field, s.field, s.max, r->gradient_step,
-                              total ? nullptr : L.G4));
+        FW_TRY(launch_compose(ctx, u, s.field, s.field, s.max, r->gradient_step,
+                              total ? nullptr : L.G4, u4));
         if (total) {
             FW_TRY(launch_smooth(ctx, s.field, L.T, r->total_field_variance, nullptr, L.R));
             FW_CUDA(cudaMemcpyAsync(s.field->d, L.T->d, s.field->bytes, cudaMemcpyDeviceToDevice,
@@ -911,6 +921,7 @@ int fw_syn_step_masked(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image*
     L.channels = recipe->channels;
     L.fmask = fixed_mask;
     L.mmask = moving_mask;
+    L.keep_updates = true;  // the scaled updates are outputs of this call
     L.grid = g;
     L.F = f2m;
     L.Fi = f2m_inv;
