@@ -356,10 +356,9 @@ struct FieldArgs {
 // `w` and `out` may be the same buffer (the SyN loop composes in place: a voxel reads only its
 // own value of `w`), so neither is declared __restrict__.
 __global__ void __launch_bounds__(256) k_compose(FieldArgs a, const float* __restrict__ u,
-                                                 const float4* __restrict__ u4, const float* w,
-                                                 float* out,
+                                                 const float* w, float* out,
                                                  const unsigned int* __restrict__ max_bits,
-                                                 double step, float4* __restrict__ out4) {
+                                                 double step) {
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= a.g.n) return;
     float s = 1.0f;
@@ -376,24 +375,11 @@ __global__ void __launch_bounds__(256) k_compose(FieldArgs a, const float* __res
         c[r] = (r == 0 ? i : (r == 1 ? j : k)) +
                (a.g.inv[r * 3] * wx + a.g.inv[r * 3 + 1] * wy + a.g.inv[r * 3 + 2] * wz);
     float d[3] = {0.0f, 0.0f, 0.0f};
-    if (inside_index(c[0], c[1], c[2], a.g.nx, a.g.ny, a.g.nz)) {
-        if (u4)
-            vec_at_index4(u4, a.g.nx, a.g.ny, a.g.nz, c[0], c[1], c[2], d);
-        else
-            vec_at_index(u, a.ps, a.g.nx, a.g.ny, a.g.nz, c[0], c[1], c[2], d);
-    }
-    const float ox = fmaf(s, d[0], wx), oy = fmaf(s, d[1], wy), oz = fmaf(s, d[2], wz);
-    out[l] = ox;
-    out[l + a.ps] = oy;
-    out[l + 2 * a.ps] = oz;
-    if (out4) out4[l] = make_float4(ox, oy, oz, 0.0f);
-}
-
-__global__ void __launch_bounds__(256) k_pack4(FieldArgs a, const float* __restrict__ f,
-                                               float4* __restrict__ out4) {
-    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= a.g.n) return;
-    out4[l] = make_float4(f[l], f[l + a.ps], f[l + 2 * a.ps], 0.0f);
+    if (inside_index(c[0], c[1], c[2], a.g.nx, a.g.ny, a.g.nz))
+        vec_at_index(u, a.ps, a.g.nx, a.g.ny, a.g.nz, c[0], c[1], c[2], d);
+    out[l] = fmaf(s, d[0], wx);
+    out[l + a.ps] = fmaf(s, d[1], wy);
+    out[l + 2 * a.ps] = fmaf(s, d[2], wz);
 }
 
 // field_ops.rs:580-605: onto another grid, scalar linear interpolation per component, zero
@@ -560,20 +546,11 @@ int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const f
 }
 
 int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, fw_field* out,
-                   const unsigned int* d_scale_max_bits, double step, float4* out4,
-                   const float4* disp4) {
-    FW_CHECK(disp || disp4, "compose: no displacement");
+                   const unsigned int* d_scale_max_bits, double step) {
     FieldArgs a{dev_grid(warping->grid), warping->ps};
-    k_compose<<<blocks_for(a.g.n), 256, 0, ctx->stream>>>(a, disp ? disp->d : nullptr, disp4,
-                                                          warping->d, out->d, d_scale_max_bits,
-                                                          step, out4);
+    k_compose<<<blocks_for(a.g.n), 256, 0, ctx->stream>>>(a, disp->d, warping->d, out->d,
+                                                          d_scale_max_bits, step);
     return check_launch(ctx, "k_compose");
-}
-
-int launch_pack4(fw_ctx* ctx, const fw_field* f, float4* out4) {
-    FieldArgs a{dev_grid(f->grid), f->ps};
-    k_pack4<<<blocks_for(a.g.n), 256, 0, ctx->stream>>>(a, f->d, out4);
-    return check_launch(ctx, "k_pack4");
 }
 
 int launch_max_norm(fw_ctx* ctx, const fw_field* f, unsigned int* d_max_bits) {

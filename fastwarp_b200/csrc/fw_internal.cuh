@@ -209,40 +209,6 @@ __device__ __forceinline__ void vec_at_index(const float* __restrict__ f, long l
     }
 }
 
-// The same from an interleaved copy of the field (x, y, z, unused per voxel): one 16-byte load
-// per corner instead of three, with the arithmetic of vec_at_index in the same order (bitwise the
-// same result).
-__device__ __forceinline__ void vec_at_index4(const float4* __restrict__ f, int nx, int ny,
-                                              int nz, double cx, double cy, double cz,
-                                              float out[3]) {
-    double fx = floor(cx), fy = floor(cy), fz = floor(cz);
-    float dx = (float)(cx - fx), dy = (float)(cy - fy), dz = (float)(cz - fz);
-    int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
-    int xa = min(max(x0, 0), nx - 1), xb = min(max(x0 + 1, 0), nx - 1);
-    int ya = min(max(y0, 0), ny - 1), yb = min(max(y0 + 1, 0), ny - 1);
-    int za = min(max(z0, 0), nz - 1), zb = min(max(z0 + 1, 0), nz - 1);
-    const long long sy = nx, sz = (long long)nx * ny;
-    const long long idx[8] = {xa + sy * ya + sz * za, xb + sy * ya + sz * za,
-                              xa + sy * yb + sz * za, xb + sy * yb + sz * za,
-                              xa + sy * ya + sz * zb, xb + sy * ya + sz * zb,
-                              xa + sy * yb + sz * zb, xb + sy * yb + sz * zb};
-    float w[2][3] = {{1.0f - dx, 1.0f - dy, 1.0f - dz}, {dx, dy, dz}};
-    float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const float o = w[q & 1][0] * w[(q >> 1) & 1][1] * w[q >> 2][2];
-        if (o != 0.0f) {
-            const float4 v = __ldg(f + idx[q]);
-            acc0 += o * v.x;
-            acc1 += o * v.y;
-            acc2 += o * v.z;
-        }
-    }
-    out[0] = acc0;
-    out[1] = acc1;
-    out[2] = acc2;
-}
-
 // Grid::index_to_point then another grid's Grid::point_to_index (grid.rs:131-156) in the
 // reference's float64 operation order with no fused multiply-adds, so points on a buffer edge
 // (-0.5 or n - 0.5) fall on the same side as in the reference.
@@ -395,15 +361,11 @@ struct InvState {
 
 // The inversion loop (fw_invert.cu). `res` (a field on the inverse's grid) keeps the residual
 // of the last measurement for the body that follows.
-// `field4` (optional): an interleaved copy of `field` to gather from; `inverse4_out` (optional):
-// where the last body writes the interleaved copy of the final inverse.
 int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
                              fw_field* res, const fw_invert_params& prm, InvState* st,
-                             cudaGraphConditionalHandle handle, int use_handle,
-                             const float4* field4 = nullptr);
+                             cudaGraphConditionalHandle handle, int use_handle);
 int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
-                           InvState* st, cudaGraphConditionalHandle handle, int use_handle,
-                           const float4* field4 = nullptr, float4* inverse4_out = nullptr);
+                           InvState* st, cudaGraphConditionalHandle handle, int use_handle);
 int enqueue_inversion_rearm(fw_ctx* ctx, InvState* st, int max_iterations);
 int read_back(fw_ctx* ctx, const double* d, int k, double* out);
 // The SyN stage on device images (fw_syn.cu); masks may be null.
@@ -442,19 +404,12 @@ int launch_cc_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, i
 // Gaussian smoothing of `in` into `out` (out may be in) with the max |u/sp| of the result fused
 // into d_max_bits (may be null); `tmp`, a third field on the grid, holds the xy pass (null: the
 // general single-kernel path, out != in).
-// `out4` (optional): the result also interleaved (x, y, z per voxel) for a gather that follows;
-// `out` may then be null (the fixed-radius path writes only the interleaved copy).
 int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double variance,
-                  unsigned int* d_max_bits, fw_field* tmp, float4* out4 = nullptr);
+                  unsigned int* d_max_bits, fw_field* tmp);
 int launch_max_norm(fw_ctx* ctx, const fw_field* f, unsigned int* d_max_bits);
-// out = warping + step/max * disp(x + warping) (step 1 without max bits); `out4` (optional)
-// also receives the result interleaved (x, y, z, 0) for the gathers of an inversion.
-// `disp4` (optional): an interleaved copy of disp to gather from (disp may then be null).
+// out = warping + step/max * disp(x + warping) (step 1 without max bits).
 int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, fw_field* out,
-                   const unsigned int* d_scale_max_bits, double step, float4* out4 = nullptr,
-                   const float4* disp4 = nullptr);
-// The interleaved copy of a field.
-int launch_pack4(fw_ctx* ctx, const fw_field* f, float4* out4);
+                   const unsigned int* d_scale_max_bits, double step);
 int launch_scale_by_max(fw_ctx* ctx, fw_field* f, const unsigned int* d_max_bits, double step);
 int invert_field(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
                  const fw_invert_params& prm, fw_invert_stats* stats);

@@ -24,8 +24,6 @@ struct InvArgs {
     DevGrid g;
     long long ps_f, ps_psi;
     float isx, isy, isz;
-    const float4* f4;  // interleaved copy of the field to gather from (or null: its planes)
-    float4* psi4;      // where the last body writes the interleaved final inverse (or null)
 };
 
 __device__ __forceinline__ void residual(const InvArgs& a, const float* __restrict__ f,
@@ -35,12 +33,8 @@ __device__ __forceinline__ void residual(const InvArgs& a, const float* __restri
     double c1 = j + (a.g.inv[3] * px + a.g.inv[4] * py + a.g.inv[5] * pz);
     double c2 = k + (a.g.inv[6] * px + a.g.inv[7] * py + a.g.inv[8] * pz);
     float d[3] = {0.0f, 0.0f, 0.0f};
-    if (inside_index(c0, c1, c2, a.g.nx, a.g.ny, a.g.nz)) {
-        if (a.f4)
-            vec_at_index4(a.f4, a.g.nx, a.g.ny, a.g.nz, c0, c1, c2, d);
-        else
-            vec_at_index(f, a.ps_f, a.g.nx, a.g.ny, a.g.nz, c0, c1, c2, d);
-    }
+    if (inside_index(c0, c1, c2, a.g.nx, a.g.ny, a.g.nz))
+        vec_at_index(f, a.ps_f, a.g.nx, a.g.ny, a.g.nz, c0, c1, c2, d);
     e[0] = px + d[0];
     e[1] = py + d[1];
     e[2] = pz + d[2];
@@ -210,9 +204,6 @@ __global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __rest
             psi[l] = px[v];
             psi[l + a.ps_psi] = py[v];
             psi[l + 2 * a.ps_psi] = pz[v];
-            // the last body: no gather follows in this sweep, so the interleaved copy may be
-            // written over the one this loop gathered from
-            if (!next && a.psi4) a.psi4[l] = make_float4(px[v], py[v], pz[v], 0.0f);
         }
         if (next) {
 #pragma unroll
@@ -289,12 +280,10 @@ static unsigned int inv_blocks(fw_ctx* ctx, long long n) {
 // (each returns at once after the loop has ended). Used by graph capture with bodies = 0.
 int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
                              fw_field* res, const fw_invert_params& prm, InvState* st,
-                             cudaGraphConditionalHandle handle, int use_handle,
-                             const float4* field4) {
+                             cudaGraphConditionalHandle handle, int use_handle) {
     FW_CHECK(res->grid.same(inverse->grid) && res->ps == inverse->ps,
              "invert: the residual buffer does not match the inverse");
     InvArgs a = inv_args(field, inverse);
-    a.f4 = field4;
     unsigned int blocks = inv_blocks(ctx, a.g.n);
     FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 2 * (size_t)blocks + 16));
     k_inv_init<<<1, 1, 0, ctx->stream>>>(st, prm);
@@ -306,11 +295,8 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
 }
 
 int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
-                           InvState* st, cudaGraphConditionalHandle handle, int use_handle,
-                           const float4* field4, float4* inverse4_out) {
+                           InvState* st, cudaGraphConditionalHandle handle, int use_handle) {
     InvArgs a = inv_args(field, inverse);
-    a.f4 = field4;
-    a.psi4 = inverse4_out;
     unsigned int blocks = inv_blocks(ctx, a.g.n);
     k_inv_body<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
                                                 ctx->d_scratch + SLOT_PARTIALS,

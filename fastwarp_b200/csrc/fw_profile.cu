@@ -47,13 +47,6 @@ int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, 
     if (!rc) rc = fw_field_zero(ctx, &cg, &s);
     if (!rc) rc = fw_field_zero(ctx, &cg, &w);
     if (!rc) rc = fw_field_zero(ctx, &cg, &e);
-    // the interleaved copy the SyN inversions gather from, and a second one of the same size
-    // for the interleaved outputs of compose and of the last inversion body
-    float4 *g4 = nullptr, *g4_out = nullptr, *u4 = nullptr;
-    const size_t g4_bytes = sizeof(float4) * (size_t)g.count();
-    if (!rc) rc = dev_alloc(ctx, g4_bytes, (void**)&g4);
-    if (!rc) rc = dev_alloc(ctx, g4_bytes, (void**)&g4_out);
-    if (!rc) rc = dev_alloc(ctx, g4_bytes, (void**)&u4);
     if (!rc) rc = new_image(ctx, g, &out);
     if (!rc) rc = ensure_scratch(ctx, SLOT_PARTIALS + (size_t)(1 << 20));
     Events ev;
@@ -64,8 +57,6 @@ int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, 
     // a smooth nonzero field for the gathers: the CC derivative of the pair, smoothed
     if (!rc) rc = launch_cc_pair_impl(ctx, fixed, moving, radius, a, b, ctx->d_scratch + SLOT_CC_VALUE, 0);
     if (!rc) rc = launch_smooth(ctx, a, u, variance, bits, e);
-    if (!rc) rc = launch_pack4(ctx, u, g4);
-    if (!rc) rc = launch_pack4(ctx, u, u4);
     if (!rc) rc = sync(ctx);
     // kinds 0-6 as documented; kind 7 is the re-arm kernel alone, subtracted from kind 5
     double t_rearm = 0.0;
@@ -75,26 +66,23 @@ int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, 
                 case 0: return launch_warp(ctx, moving, u, nullptr, nullptr, out->d, false, nullptr);
                 case 1: return launch_cc_pair_impl(ctx, fixed, moving, radius, a, b,
                                                    ctx->d_scratch + SLOT_CC_VALUE, 0);
-                // as the SyN loop runs them: the smoothed update written interleaved only, and
-                // the composition gathering it and writing the interleaved field too
-                case 2: return launch_smooth(ctx, a, nullptr, variance, bits, e, g4_out);
-                case 3: return launch_compose(ctx, nullptr, w, w, bits, 0.1, g4_out, u4);
+                case 2: return launch_smooth(ctx, a, s, variance, bits, e);
+                case 3: return launch_compose(ctx, u, w, w, bits, 0.1);
                 case 4: {
                     fw_invert_params p = {20, 0.0, 0.0, 1};
-                    return enqueue_inversion_prefix(ctx, u, w, e, p, st, 0, 0, g4);
+                    return enqueue_inversion_prefix(ctx, u, w, e, p, st, 0, 0);
                 }
-                case 5: {  // the last body of a loop: re-armed for exactly one more body; it
-                           // writes the interleaved inverse (to a spare: u's copy stays intact)
+                case 5: {  // the last body of a loop: re-armed for exactly one more body
                     FW_TRY(enqueue_inversion_rearm(ctx, st, 1));
-                    return enqueue_inversion_body(ctx, u, w, e, st, 0, 0, g4, g4_out);
+                    return enqueue_inversion_body(ctx, u, w, e, st, 0, 0);
                 }
-                case 6: return enqueue_inversion_body(ctx, u, w, e, st, 0, 0, g4);
+                case 6: return enqueue_inversion_body(ctx, u, w, e, st, 0, 0);
                 default: return enqueue_inversion_rearm(ctx, st, 1);
             }
         };
         if (kind == 5 || kind == 6) {  // a measured loop state; for 6 every body measures again
             fw_invert_params p = {kind == 5 ? 1 : (1 << 30), -1.0, -1.0, 1};
-            rc = enqueue_inversion_prefix(ctx, u, w, e, p, st, 0, 0, g4);
+            rc = enqueue_inversion_prefix(ctx, u, w, e, p, st, 0, 0);
             if (rc) break;
         }
         rc = launch();  // warm-up
@@ -113,15 +101,12 @@ int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, 
     // algorithmic bytes: float32 voxels and field components
     bytes[0] = n * (12.0 + 4.0 + 4.0);         // field, source gather (one value), output
     bytes[1] = n * (8.0 + 24.0);               // two images in, two fields out
-    bytes[2] = n * (12.0 + 16.0);              // field in, interleaved field out
-    bytes[3] = n * (16.0 + 12.0 + 12.0 + 16.0);  // update gather, field in, field out + copy
-    bytes[4] = n * (12.0 + 16.0 + 12.0);       // psi, interleaved field gather, residual out
-    bytes[5] = n * (12.0 + 12.0 + 12.0 + 16.0);  // psi and residual in, psi out + copy
-    bytes[6] = n * (12.0 * 4 + 16.0);          // + interleaved field gather and residual out
+    bytes[2] = n * (12.0 + 12.0);              // field in, field out
+    bytes[3] = n * (12.0 + 12.0 + 12.0);       // update gather, field in, field out
+    bytes[4] = n * (12.0 + 12.0 + 12.0);       // psi, field gather, residual out
+    bytes[5] = n * (12.0 + 12.0 + 12.0);       // psi and residual in, psi out
+    bytes[6] = n * (12.0 * 5);                 // + field gather and residual out
     fw_field_free(e);
-    if (g4) dev_free(ctx, g4, g4_bytes);
-    if (g4_out) dev_free(ctx, g4_out, g4_bytes);
-    if (u4) dev_free(ctx, u4, g4_bytes);
     fw_field_free(u);
     fw_field_free(a);
     fw_field_free(b);

@@ -63,12 +63,10 @@ int estimate(const fw_syn_request* q, uint64_t* out) {
     if (q->fixed == nullptr) b += 0;
     else b += 4 * C * (nf + nm);                       // uploaded inputs
     if (smooth) b += 4 * C * (nf + nm) + 24 * std::max(nf, nm);  // smoothed copies + Deriche temp
-    int fields = 4 + 2 + 1 /* inversion residual */ + (C > 1 ? 2 : 0) +
-                 (r->total_field_variance > 0 ? 1 : 0) + 2 /* outputs */;
+    int fields = 4 + 2 + 1 /* inversion residual */ + (r->update_field_variance > 0 ? 2 : 0) +
+                 (C > 1 ? 2 : 0) + (r->total_field_variance > 0 ? 1 : 0) + 2 /* outputs */;
     b += 12 * ps * (uint64_t)fields;
     b += 4 * (uint64_t)n * 2 * C;                      // warped images
-    b += 16 * (uint64_t)n;                             // interleaved copy for the inversions
-    if (r->update_field_variance > 0) b += 16 * (uint64_t)n;  // interleaved smoothed update
     b += 12 * psp * 4;                                 // state of the previous level at a transition
     b += 2u << 20;                                     // records and scalars
     *out = b;

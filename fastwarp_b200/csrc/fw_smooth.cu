@@ -275,12 +275,10 @@ __global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* 
 
 // blockIdx.x: z segment (fastest, so neighbouring segments share their halo rows in L2),
 // blockIdx.y: 32 columns in x, blockIdx.z: 8 rows in y.
-// `out` (SoA planes) and `out4` (interleaved x, y, z per voxel, for a gather that follows) may
-// each be null, not both.
 template <int R>
 __global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __restrict__ tmp,
                                                   long long ps_tmp, const float* in,
-                                                  float* out, float4* __restrict__ out4,
+                                                  float* out,
                                                   unsigned int* __restrict__ max_bits) {
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
     const int x = blockIdx.y * 32 + (threadIdx.x & 31), y = blockIdx.z * 8 + (threadIdx.x >> 5);
@@ -317,8 +315,7 @@ __global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __r
                 if (face) o = 0.0f;
                 else if (a.w2 != 0.0f) o = v * a.w1 + in[l + c * a.ps_in] * a.w2;
                 else o = v;
-                if (out) out[l + c * a.ps_out] = o;
-                if (out4) reinterpret_cast<float*>(out4 + l)[c] = o;
+                out[l + c * a.ps_out] = o;
                 const float p = o * isp[c];
                 nsq[q] = fmaf(p, p, nsq[q]);
             }
@@ -339,13 +336,12 @@ __global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __r
 
 template <int R>
 int launch_smooth_xyz(fw_ctx* ctx, const SmoothArgs& a, const fw_field* in, fw_field* out,
-                      fw_field* tmp, unsigned int* d_max_bits, float4* out4) {
+                      fw_field* tmp, unsigned int* d_max_bits) {
     dim3 g1((a.g.nx + XY_T - 1) / XY_T, (a.g.ny + XY_T - 1) / XY_T, a.g.nz);
     k_smooth_xy<R><<<g1, XY_NT, 0, ctx->stream>>>(a, in->d, tmp->d, tmp->ps);
     FW_TRY(check_launch(ctx, "k_smooth_xy"));
     dim3 g2((a.g.nz + Z_SEG - 1) / Z_SEG, (a.g.nx + 31) / 32, (a.g.ny + 7) / 8);
-    k_smooth_z<R><<<g2, 256, 0, ctx->stream>>>(a, tmp->d, tmp->ps, in->d, out ? out->d : nullptr,
-                                               out4, d_max_bits);
+    k_smooth_z<R><<<g2, 256, 0, ctx->stream>>>(a, tmp->d, tmp->ps, in->d, out->d, d_max_bits);
     return check_launch(ctx, "k_smooth_z");
 }
 
@@ -505,13 +501,12 @@ __global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b
 }  // namespace
 
 int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double variance,
-                  unsigned int* d_max_bits, fw_field* tmp, float4* out4) {
-    FW_CHECK(out || (out4 && tmp), "smooth field: no output");
+                  unsigned int* d_max_bits, fw_field* tmp) {
     SmoothArgs a;
     std::memset(&a, 0, sizeof(a));
     a.g = dev_grid(in->grid);
     a.ps_in = in->ps;
-    a.ps_out = out ? out->ps : in->ps;
+    a.ps_out = out->ps;
     int r[3];
     for (int ax = 0; ax < 3; ++ax) {
         std::vector<double> k = gaussian_taps(variance, 0.001, in->grid.n[ax]);
@@ -535,26 +530,22 @@ int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double varianc
         FW_CHECK(tmp->grid.same(in->grid) && tmp != in && tmp != out,
                  "smooth field: the temporary field must be a third field on the same grid");
         switch (r[0]) {
-            case 1: return launch_smooth_xyz<1>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 2: return launch_smooth_xyz<2>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 3: return launch_smooth_xyz<3>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 4: return launch_smooth_xyz<4>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 5: return launch_smooth_xyz<5>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 6: return launch_smooth_xyz<6>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 7: return launch_smooth_xyz<7>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 8: return launch_smooth_xyz<8>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 9: return launch_smooth_xyz<9>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 10: return launch_smooth_xyz<10>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 11: return launch_smooth_xyz<11>(ctx, a, in, out, tmp, d_max_bits, out4);
-            case 12: return launch_smooth_xyz<12>(ctx, a, in, out, tmp, d_max_bits, out4);
+            case 1: return launch_smooth_xyz<1>(ctx, a, in, out, tmp, d_max_bits);
+            case 2: return launch_smooth_xyz<2>(ctx, a, in, out, tmp, d_max_bits);
+            case 3: return launch_smooth_xyz<3>(ctx, a, in, out, tmp, d_max_bits);
+            case 4: return launch_smooth_xyz<4>(ctx, a, in, out, tmp, d_max_bits);
+            case 5: return launch_smooth_xyz<5>(ctx, a, in, out, tmp, d_max_bits);
+            case 6: return launch_smooth_xyz<6>(ctx, a, in, out, tmp, d_max_bits);
+            case 7: return launch_smooth_xyz<7>(ctx, a, in, out, tmp, d_max_bits);
+            case 8: return launch_smooth_xyz<8>(ctx, a, in, out, tmp, d_max_bits);
+            case 9: return launch_smooth_xyz<9>(ctx, a, in, out, tmp, d_max_bits);
+            case 10: return launch_smooth_xyz<10>(ctx, a, in, out, tmp, d_max_bits);
+            case 11: return launch_smooth_xyz<11>(ctx, a, in, out, tmp, d_max_bits);
+            case 12: return launch_smooth_xyz<12>(ctx, a, in, out, tmp, d_max_bits);
             default: break;
         }
     }
-    // the general path: one kernel into `out` (or into `tmp` when only the interleaved copy is
-    // wanted), then the interleaved copy
-    fw_field* dst = out ? out : tmp;
-    FW_CHECK(in != dst, "smooth field: the general path needs a separate output");
-    a.ps_out = dst->ps;
+    FW_CHECK(in != out, "smooth field: the general path needs a separate output");
     dim3 grid((a.g.nx + STX - 1) / STX, (a.g.ny + STY - 1) / STY, 1);
     long long tiles = (long long)grid.x * grid.y;
     int want = (int)std::max<long long>(1, (4LL * ctx->num_sms + tiles - 1) / tiles);
@@ -565,9 +556,8 @@ int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double varianc
     const int HX = STX + 2 * a.rx, HY = STY + 2 * a.ry, W = 2 * a.rz + 1;
     size_t bytes = sizeof(float) * (3 * HY * HX + 3 * HY * STX + W * 3 * SNT);
     FW_CUDA(cudaFuncSetAttribute(k_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    k_smooth<<<grid, SNT, bytes, ctx->stream>>>(a, in->d, dst->d, d_max_bits);
-    FW_TRY(check_launch(ctx, "k_smooth"));
-    return out4 ? launch_pack4(ctx, dst, out4) : 0;
+    k_smooth<<<grid, SNT, bytes, ctx->stream>>>(a, in->d, out->d, d_max_bits);
+    return check_launch(ctx, "k_smooth");
 }
 
 int launch_smooth_recursive(fw_ctx* ctx, const fw_image* img, const double sigma_mm[3],

@@ -190,11 +190,6 @@ struct Level {
     fw_field *sF = nullptr, *sM = nullptr;      // smoothed updates
     fw_field* T = nullptr;                      // total-field smoothing
     fw_field* R = nullptr;                      // inversion residual of the last measurement
-    float4* G4 = nullptr;                       // interleaved copy of the field being inverted
-    size_t g4_bytes = 0;
-    float4* U4 = nullptr;                       // the smoothed update, interleaved
-    bool keep_updates = false;                  // also keep sF / sM (the single-step API)
-    fw_ctx* ctx = nullptr;                      // owner of the work buffers
     const fw_image* fmask = nullptr;            // recipe masks on their own grids (or none)
     const fw_image* mmask = nullptr;
     fw_image* valid = nullptr;                  // the masks resolved on the level grid
@@ -210,9 +205,6 @@ void free_level_work(Level& L) {
     fw_field* fs[] = {L.dF, L.dM, L.accF, L.accM, L.sF, L.sM, L.T, L.R};
     for (auto* f : fs) fw_field_free(f);
     L.dF = L.dM = L.accF = L.accM = L.sF = L.sM = L.T = L.R = nullptr;
-    if (L.G4) dev_free(L.ctx, L.G4, L.g4_bytes);
-    if (L.U4) dev_free(L.ctx, L.U4, L.g4_bytes);
-    L.G4 = L.U4 = nullptr;
 }
 
 int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
@@ -223,22 +215,16 @@ int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
         FW_TRY(new_image(ctx, L.grid, &b));
         L.mmid.push_back(b);
     }
-    L.ctx = ctx;
     FW_TRY(new_field(ctx, L.grid, &L.dF));
     FW_TRY(new_field(ctx, L.grid, &L.dM));
     FW_TRY(new_field(ctx, L.grid, &L.R));
-    L.g4_bytes = sizeof(float4) * (size_t)L.grid.count();
-    FW_TRY(dev_alloc(ctx, L.g4_bytes, (void**)&L.G4));
     if (L.channels > 1) {
         FW_TRY(new_field(ctx, L.grid, &L.accF));
         FW_TRY(new_field(ctx, L.grid, &L.accM));
     }
     if (r->update_field_variance > 0.0) {
-        FW_TRY(dev_alloc(ctx, L.g4_bytes, (void**)&L.U4));
-        if (L.keep_updates) {
-            FW_TRY(new_field(ctx, L.grid, &L.sF));
-            FW_TRY(new_field(ctx, L.grid, &L.sM));
-        }
+        FW_TRY(new_field(ctx, L.grid, &L.sF));
+        FW_TRY(new_field(ctx, L.grid, &L.sM));
     }
     if (r->total_field_variance > 0.0) FW_TRY(new_field(ctx, L.grid, &L.T));
     if (L.fmask || L.mmask) FW_TRY(new_image(ctx, L.grid, &L.valid));
@@ -280,13 +266,12 @@ int add_while(cudaStream_t s, unsigned int default_value, unsigned int flags,
 
 // One inversion: in graph mode a WHILE node around the body kernel; in direct mode a host loop.
 int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inverse,
-                   fw_field* res, InvState* st, const float4* field4, float4* inverse4_out) {
+                   fw_field* res, InvState* st) {
     if (!graph) {
-        FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, 0, 0, field4));
+        FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, 0, 0));
         InvState h;
         for (int body = 0; body < kSynInvert.max_iterations; ++body) {
-            FW_TRY(enqueue_inversion_body(ctx, field, inverse, res, st, 0, 0, field4,
-                                          inverse4_out));
+            FW_TRY(enqueue_inversion_body(ctx, field, inverse, res, st, 0, 0));
             FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, st, sizeof(InvState), cudaMemcpyDeviceToHost,
                                     ctx->stream));
             FW_TRY(sync(ctx));
@@ -303,7 +288,7 @@ int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inv
     FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
     cudaGraphConditionalHandle h;
     FW_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, h, 1, field4));
+    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, h, 1));
     FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
     cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
     p.conditional.handle = h;
@@ -319,7 +304,7 @@ int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inv
     FW_CUDA(cudaStreamBeginCaptureToGraph(ctx->aux, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
     ctx->stream = ctx->aux;
-    int rc = enqueue_inversion_body(ctx, field, inverse, res, st, h, 1, field4, inverse4_out);
+    int rc = enqueue_inversion_body(ctx, field, inverse, res, st, h, 1);
     ctx->stream = main;
     cudaGraph_t out;
     cudaError_t e = cudaStreamEndCapture(ctx->aux, &out);
@@ -379,13 +364,12 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
         gM = L.accM;
     }
     // update_total_field for both sides (syn.rs:422-445), one side after the other: smooth the
-    // update (variance in voxels^2) with its max |u/sp| fused, written interleaved for the gather
-    // of the composition; F <- F + (step / max) u(x + F) in place (its interleaved copy is what
-    // the first inversion gathers); optional total-field smoothing; the inversion pair. The two
-    // sides only share scratch (R, U4, G4), so running them in turn gives the reference's fields.
+    // update (variance in voxels^2) with its max |u/sp| fused; F <- F + (step / max) u(x + F) in
+    // place; optional total-field smoothing; the inversion pair. The sides only share scratch
+    // (the residual field R), so running them in turn gives the reference's fields.
     struct Side {
-        fw_field* g;       // raw update (CC derivative or channel combination)
-        fw_field* keep;    // where the smoothed update is also kept (single-step API) or null
+        fw_field* g;  // raw update (CC derivative or channel combination)
+        fw_field* s;  // smoothed update
         fw_field* field;
         fw_field* inverse;
         unsigned int* max;
@@ -394,28 +378,22 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
                   {gM, L.sM, L.M, L.Mi, d.max_bits + 1, d.inv + 2}};
     for (auto& s : sides) {
         const fw_field* u = s.g;
-        const float4* u4 = nullptr;
         if (r->update_field_variance > 0.0) {
-            FW_TRY(launch_smooth(ctx, s.g, s.keep, r->update_field_variance, s.max, L.R, L.U4));
-            u = s.keep;
-            u4 = L.U4;
+            FW_TRY(launch_smooth(ctx, s.g, s.s, r->update_field_variance, s.max, L.R));
+            u = s.s;
         } else {
             FW_TRY(launch_max_norm(ctx, s.g, s.max));
         }
         // compose in place: every voxel reads its own field value and the update elsewhere
-        const bool total = r->total_field_variance > 0.0;
-        FW_TRY(launch_compose(ctx, u, s.field, s.field, s.max, r->gradient_step,
-                              total ? nullptr : L.G4, u4));
-        if (total) {
+        FW_TRY(launch_compose(ctx, u, s.field, s.field, s.max, r->gradient_step));
+        if (r->total_field_variance > 0.0) {
             FW_TRY(launch_smooth(ctx, s.field, L.T, r->total_field_variance, nullptr, L.R));
             FW_CUDA(cudaMemcpyAsync(s.field->d, L.T->d, s.field->bytes, cudaMemcpyDeviceToDevice,
                                     ctx->stream));
-            FW_TRY(launch_pack4(ctx, s.field, L.G4));
         }
-        // inverse = invert(field), whose last body leaves the interleaved inverse in G4 for the
-        // second: field = invert(inverse)
-        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, L.R, s.st, L.G4, L.G4));
-        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, L.R, s.st + 1, L.G4, nullptr));
+        // inverse = invert(field), then field = invert(inverse)
+        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, L.R, s.st));
+        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, L.R, s.st + 1));
     }
     return 0;
 }
@@ -668,7 +646,7 @@ int check_status(int status) {
 // Kernels per iteration outside the inversion bodies (for the launch counter).
 int kernels_per_iteration(const fw_syn_recipe* r, int mask_warps) {
     int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) + 2 /*smooth or max*/ +
-            2 /*compose*/ + (r->total_field_variance > 0.0 ? 4 : 0) + 4 * 2 /*inv init+measure*/ +
+            2 /*compose*/ + (r->total_field_variance > 0.0 ? 2 : 0) + 4 * 2 /*inv init+measure*/ +
             1 /*record*/ + mask_warps;
     return k;
 }
@@ -921,7 +899,6 @@ int fw_syn_step_masked(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image*
     L.channels = recipe->channels;
     L.fmask = fixed_mask;
     L.mmask = moving_mask;
-    L.keep_updates = true;  // the scaled updates are outputs of this call
     L.grid = g;
     L.F = f2m;
     L.Fi = f2m_inv;
