@@ -66,7 +66,8 @@ class SynRecipe(C.Structure):
                 ("shrink_factors", C.c_uint32 * MAX_LEVELS),
                 ("smoothing_sigmas", C.c_double * MAX_LEVELS), ("sigma_units_mm", C.c_int32),
                 ("convergence_threshold", C.c_double), ("convergence_window", C.c_int32),
-                ("channels", C.c_int32), ("channel_weights", C.c_double * MAX_CHANNELS)]
+                ("channels", C.c_int32), ("channel_weights", C.c_double * MAX_CHANNELS),
+                ("channel_metrics", C.c_int32 * MAX_CHANNELS), ("mi_bins", C.c_int32)]
 
 
 class SynIteration(C.Structure):
@@ -118,6 +119,8 @@ def lib():
         L.fw_field_free.restype = None
         L.fw_mi_level_free.restype = None
         L.fw_ctx_reset_stats.restype = None
+        L.fw_abi_struct_size.restype = C.c_size_t
+        L.fw_abi_struct_size.argtypes = [C.c_char_p]
         _lib = L
     return _lib
 

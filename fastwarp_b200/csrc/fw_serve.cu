@@ -386,3 +386,21 @@ void fw_server_destroy(fw_server* s) {
 }
 
 }  // extern "C"
+
+extern "C" size_t fw_abi_struct_size(const char* name) {
+    if (!name) return 0;
+    const std::string n(name);
+    if (n == "fw_grid") return sizeof(fw_grid);
+    if (n == "fw_affine") return sizeof(fw_affine);
+    if (n == "fw_invert_params") return sizeof(fw_invert_params);
+    if (n == "fw_invert_stats") return sizeof(fw_invert_stats);
+    if (n == "fw_mi_binning") return sizeof(fw_mi_binning);
+    if (n == "fw_linear_transform") return sizeof(fw_linear_transform);
+    if (n == "fw_syn_recipe") return sizeof(fw_syn_recipe);
+    if (n == "fw_syn_iteration") return sizeof(fw_syn_iteration);
+    if (n == "fw_stats") return sizeof(fw_stats);
+    if (n == "fw_syn_request") return sizeof(fw_syn_request);
+    if (n == "fw_syn_result") return sizeof(fw_syn_result);
+    if (n == "fw_server_stats") return sizeof(fw_server_stats);
+    return 0;
+}

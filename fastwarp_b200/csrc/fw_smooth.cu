@@ -215,51 +215,60 @@ __global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* 
     constexpr int HX = XY_T + 2 * R, HY = XY_T + 2 * R;
     constexpr int HXP = (HX + 3) & ~3;       // rows start on 16 bytes
     constexpr int NV = (4 + 2 * R + 3) / 4;  // float4 loads per x window of four outputs
-    __shared__ __align__(16) float tile[HY * HXP + 4 * NV];
-    __shared__ __align__(16) float xs[HY * XY_T];
+    constexpr int TILE = HY * HXP;
+    // the three components' tiles at once (dynamic: [3][TILE] + pad, then [3][HY][32] x sums):
+    // all their loads in flight together, two barriers per block
+    extern __shared__ __align__(16) float smem_xy[];
+    float* tile = smem_xy;
+    float* xs = smem_xy + 3 * TILE + 4 * NV;
     const int nx = a.g.nx, ny = a.g.ny;
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
     const int x0 = blockIdx.x * XY_T, y0 = blockIdx.y * XY_T;
     const long long zoff = (long long)blockIdx.z * nx * ny;
     const int x = x0 + tx;
+    for (int s = tid; s < HY * HX; s += XY_NT) {
+        const int hy = s / HX, hx = s - hy * HX;
+        const int gx = min(max(x0 - R + hx, 0), nx - 1);  // edge replication
+        const int gy = min(max(y0 - R + hy, 0), ny - 1);
+        const float* src = in + zoff + (long long)gy * nx + gx;
+        const float v0 = __ldg(src), v1 = __ldg(src + a.ps_in), v2 = __ldg(src + 2 * a.ps_in);
+        tile[hy * HXP + hx] = v0;
+        tile[TILE + hy * HXP + hx] = v1;
+        tile[2 * TILE + hy * HXP + hx] = v2;
+    }
+    __syncthreads();
+    // x pass: (component, halo row, group of four output columns)
+    for (int s = tid; s < 3 * HY * (XY_T / 4); s += XY_NT) {
+        const int c = s / (HY * (XY_T / 4)), rr = s - c * (HY * (XY_T / 4));
+        const int hy = rr >> 3, g4 = rr & 7;
+        const float4* row = reinterpret_cast<const float4*>(tile + c * TILE + hy * HXP) + g4;
+        float win[4 * NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const float4 q = row[v];
+            win[4 * v] = q.x;
+            win[4 * v + 1] = q.y;
+            win[4 * v + 2] = q.z;
+            win[4 * v + 3] = q.w;
+        }
+        float4 o = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+        for (int t = 0; t <= 2 * R; ++t) {
+            const float w = a.tx_[t];
+            o.x = fmaf(w, win[t], o.x);
+            o.y = fmaf(w, win[t + 1], o.y);
+            o.z = fmaf(w, win[t + 2], o.z);
+            o.w = fmaf(w, win[t + 3], o.w);
+        }
+        reinterpret_cast<float4*>(xs + (c * HY + hy) * XY_T)[g4] = o;
+    }
+    __syncthreads();
+    // y pass: four consecutive output rows of the thread's column, per component
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float* src = in + c * a.ps_in + zoff;
-        for (int s = tid; s < HY * HX; s += XY_NT) {
-            const int hy = s / HX, hx = s - hy * HX;
-            const int gx = min(max(x0 - R + hx, 0), nx - 1);  // edge replication
-            const int gy = min(max(y0 - R + hy, 0), ny - 1);
-            tile[hy * HXP + hx] = __ldg(src + (long long)gy * nx + gx);
-        }
-        __syncthreads();
-        // x pass: (halo row, group of four output columns)
-        for (int s = tid; s < HY * (XY_T / 4); s += XY_NT) {
-            const int hy = s >> 3, g4 = s & 7;
-            const float4* row = reinterpret_cast<const float4*>(tile + hy * HXP) + g4;
-            float win[4 * NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                const float4 q = row[v];
-                win[4 * v] = q.x;
-                win[4 * v + 1] = q.y;
-                win[4 * v + 2] = q.z;
-                win[4 * v + 3] = q.w;
-            }
-            float4 o = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-#pragma unroll
-            for (int t = 0; t <= 2 * R; ++t) {
-                const float w = a.tx_[t];
-                o.x = fmaf(w, win[t], o.x);
-                o.y = fmaf(w, win[t + 1], o.y);
-                o.z = fmaf(w, win[t + 2], o.z);
-                o.w = fmaf(w, win[t + 3], o.w);
-            }
-            reinterpret_cast<float4*>(xs + hy * XY_T)[g4] = o;
-        }
-        __syncthreads();
-        // y pass: four consecutive output rows of the thread's column
         float col[4 + 2 * R];
 #pragma unroll
-        for (int t = 0; t < 4 + 2 * R; ++t) col[t] = xs[(ty * 4 + t) * XY_T + tx];
+        for (int t = 0; t < 4 + 2 * R; ++t) col[t] = xs[(c * HY + ty * 4 + t) * XY_T + tx];
         float* dst = tmp + c * ps_tmp + zoff;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -269,7 +278,6 @@ __global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* 
             const int y = y0 + ty * 4 + q;
             if (x < nx && y < ny) dst[(long long)y * nx + x] = acc;
         }
-        __syncthreads();  // the next component overwrites tile and xs
     }
 }
 
@@ -337,8 +345,12 @@ __global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __r
 template <int R>
 int launch_smooth_xyz(fw_ctx* ctx, const SmoothArgs& a, const fw_field* in, fw_field* out,
                       fw_field* tmp, unsigned int* d_max_bits) {
+    constexpr int HY = XY_T + 2 * R, HXP = (XY_T + 2 * R + 3) & ~3, NV = (4 + 2 * R + 3) / 4;
+    constexpr size_t bytes = sizeof(float) * (3 * HY * HXP + 4 * NV + 3 * HY * XY_T);
+    FW_CUDA(cudaFuncSetAttribute(k_smooth_xy<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)bytes));
     dim3 g1((a.g.nx + XY_T - 1) / XY_T, (a.g.ny + XY_T - 1) / XY_T, a.g.nz);
-    k_smooth_xy<R><<<g1, XY_NT, 0, ctx->stream>>>(a, in->d, tmp->d, tmp->ps);
+    k_smooth_xy<R><<<g1, XY_NT, bytes, ctx->stream>>>(a, in->d, tmp->d, tmp->ps);
     FW_TRY(check_launch(ctx, "k_smooth_xy"));
     dim3 g2((a.g.nz + Z_SEG - 1) / Z_SEG, (a.g.nx + 31) / 32, (a.g.ny + 7) / 8);
     k_smooth_z<R><<<g2, 256, 0, ctx->stream>>>(a, tmp->d, tmp->ps, in->d, out->d, d_max_bits);

@@ -26,6 +26,9 @@ class SynRecipe:
     convergence_threshold: float = 1e-6
     convergence_window: int = 10
     channel_weights: List[float] = field(default_factory=lambda: [1.0])
+    # SynMetric per channel (recipe.rs channel_metrics): "cc" or "mattes"; empty = all CC
+    channel_metrics: List[str] = field(default_factory=list)
+    mi_bins: int = 32
 
     @staticmethod
     def cohort() -> "SynRecipe":
@@ -59,6 +62,15 @@ class SynRecipe:
         r.channels = len(self.channel_weights)
         for k, w in enumerate(self.channel_weights):
             r.channel_weights[k] = float(w)
+        metrics = self.channel_metrics or ["cc"] * r.channels
+        if len(metrics) != r.channels:
+            raise N.FastwarpError(N.FW_ERR_INVALID, "syn recipe: channel metrics must have one "
+                                  "entry per channel weight")
+        for k, m in enumerate(metrics):
+            if m not in ("cc", "mattes"):
+                raise N.FastwarpError(N.FW_ERR_INVALID, f"syn recipe: unknown metric {m!r}")
+            r.channel_metrics[k] = 0 if m == "cc" else 1
+        r.mi_bins = int(self.mi_bins)
         return r
 
 

@@ -100,7 +100,10 @@ typedef struct fw_linear_transform {
     double center[3];
 } fw_linear_transform;
 
-/* SynRecipe, recipe.rs:52-100 (CC channels; masks are passed beside it as images). */
+/* SynRecipe, recipe.rs:52-100 (masks are passed beside it as images). channel_metrics (SynMetric):
+ * FW_METRIC_CC (neighbourhood CC of cc_radius) or FW_METRIC_MATTES (dense Mattes MI of mi_bins). */
+#define FW_METRIC_CC 0
+#define FW_METRIC_MATTES 1
 #define FW_MAX_LEVELS 8
 #define FW_MAX_CHANNELS 4
 typedef struct fw_syn_recipe {
@@ -117,6 +120,8 @@ typedef struct fw_syn_recipe {
     int32_t convergence_window;
     int32_t channels;
     double channel_weights[FW_MAX_CHANNELS];
+    int32_t channel_metrics[FW_MAX_CHANNELS];
+    int32_t mi_bins;
 } fw_syn_recipe;
 
 /* SynIteration, syn.rs:96-113. */

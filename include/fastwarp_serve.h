@@ -82,6 +82,11 @@ int fw_server_estimate(const fw_syn_request* req, uint64_t* bytes);
 /* Waits for every queued and running request, then stops the slots. */
 void fw_server_destroy(fw_server* s);
 
+/* No counterpart in the reference: sizeof of a struct of these headers by name ("fw_grid",
+ * "fw_syn_recipe", "fw_syn_request", ...; 0 for an unknown name), for bindings to check their
+ * mirrored layouts against the library's. */
+size_t fw_abi_struct_size(const char* name);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,7 +63,8 @@ class SynRecipe(C.Structure):
                 ("shrink_factors", C.c_uint32 * MAX_LEVELS),
                 ("smoothing_sigmas", C.c_double * MAX_LEVELS), ("sigma_units_mm", C.c_int32),
                 ("convergence_threshold", C.c_double), ("convergence_window", C.c_int32),
-                ("channels", C.c_int32), ("channel_weights", C.c_double * MAX_CHANNELS)]
+                ("channels", C.c_int32), ("channel_weights", C.c_double * MAX_CHANNELS),
+                ("channel_metrics", C.c_int32 * MAX_CHANNELS), ("mi_bins", C.c_int32)]
 
 
 class SynIteration(C.Structure):
@@ -370,7 +371,8 @@ def convergence_value(values, window, total):
 def syn_recipe(gradient_step=0.1, update_variance=3.0, total_variance=0.0, cc_radius=4,
                iterations=(100, 70, 50, 20), shrink=(8, 4, 2, 1), sigmas=(3, 2, 1, 0),
                sigma_units_mm=False, convergence_threshold=1e-6, convergence_window=10,
-               weights=(1.0,)):
+               weights=(1.0,), metrics=None, mi_bins=32):
+    """metrics: one per channel, "cc" or "mattes" (SynMetric; all CC by default)."""
     r = SynRecipe()
     r.gradient_step = gradient_step
     r.update_field_variance = update_variance
@@ -387,6 +389,9 @@ def syn_recipe(gradient_step=0.1, update_variance=3.0, total_variance=0.0, cc_ra
     r.channels = len(weights)
     for k, w in enumerate(weights):
         r.channel_weights[k] = float(w)
+    for k, m in enumerate(metrics or ["cc"] * len(weights)):
+        r.channel_metrics[k] = {"cc": 0, "mattes": 1}[m]
+    r.mi_bins = int(mi_bins)
     return r
 
 

@@ -1627,27 +1627,53 @@ int syn_iteration(const fwo_syn_recipe* r, const Grid& lg, const Grid& fg,
     double totF = 0.0, totM = 0.0;
     std::vector<double> valsF, valsM;
     fwo_grid lgc = to_c(lg), fgc = to_c(fg), mgc = to_c(mg);
-    std::vector<double> valid;
+    // syn.rs:496-580: each given mask resolved on the level grid (the fixed one through F^-1, the
+    // moving one through affine(M^-1)); CC takes the voxels inside both, Mattes each on its own
+    std::vector<double> valid, fvalid, mvalid;
     const bool has_fm = masks && masks->fixed, has_mm = masks && masks->moving;
-    if (has_fm || has_mm) {
-        valid.resize(n);
-        if (has_fm && fwo_warp_mask(masks->fixed_grid, masks->fixed, &lgc, f2m_inv, nullptr,
-                                    nullptr, nullptr, nullptr, valid.data()))
-            return -1;
-        if (has_mm && fwo_warp_mask(masks->moving_grid, masks->moving, &lgc, m2m_inv, nullptr,
-                                    nullptr, initial, has_fm ? valid.data() : nullptr,
-                                    valid.data()))
+    if (has_fm) {
+        fvalid.resize(n);
+        if (fwo_warp_mask(masks->fixed_grid, masks->fixed, &lgc, f2m_inv, nullptr, nullptr,
+                          nullptr, nullptr, fvalid.data()))
             return -1;
     }
+    if (has_mm) {
+        mvalid.resize(n);
+        if (fwo_warp_mask(masks->moving_grid, masks->moving, &lgc, m2m_inv, nullptr, nullptr,
+                          initial, nullptr, mvalid.data()))
+            return -1;
+    }
+    if (has_fm || has_mm) {
+        valid.resize(n);
+        for (int64_t l = 0; l < n; ++l)
+            valid[l] = (has_fm ? fvalid[l] : 1.0) * (has_mm ? mvalid[l] : 1.0);
+    }
+    std::vector<double> zero;
     for (int c = 0; c < channels; ++c) {
         if (fwo_warp(&fgc, fixed_s[c], &lgc, f2m_inv, nullptr, nullptr, nullptr, fmid.data()))
             return -1;
         if (fwo_warp(&mgc, moving_s[c], &lgc, m2m_inv, nullptr, nullptr, initial, mmid.data()))
             return -1;
         double vals[2];
-        if (fwo_cc_pair(&lgc, fmid.data(), mmid.data(), valid.empty() ? nullptr : valid.data(),
-                        r->cc_radius, vals, dF.data(), dM.data()))
+        if (r->channel_metrics[c] == 1) {
+            // cpu/mod.rs:352-381 (mi_pair): evaluate_dense (fixed, moving) then (moving, fixed)
+            if (zero.empty()) zero.assign(3 * n, 0.0);
+            const fwo_grid* fmg = has_fm ? &lgc : nullptr;
+            const fwo_grid* mmg = has_mm ? &lgc : nullptr;
+            const double* fm = has_fm ? fvalid.data() : nullptr;
+            const double* mm = has_mm ? mvalid.data() : nullptr;
+            int64_t nv = 0;
+            if (fwo_mi_dense(&lgc, fmid.data(), &lgc, mmid.data(), zero.data(), fmg, fm, mmg, mm,
+                             r->mi_bins, &vals[0], &nv, dF.data()))
+                return -1;
+            if (fwo_mi_dense(&lgc, mmid.data(), &lgc, fmid.data(), zero.data(), mmg, mm, fmg, fm,
+                             r->mi_bins, &vals[1], &nv, dM.data()))
+                return -1;
+        } else if (fwo_cc_pair(&lgc, fmid.data(), mmid.data(),
+                               valid.empty() ? nullptr : valid.data(), r->cc_radius, vals,
+                               dF.data(), dM.data())) {
             return -1;
+        }
         valsF.push_back(vals[0]);
         valsM.push_back(vals[1]);
         if (channels == 1) {

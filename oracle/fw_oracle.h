@@ -74,8 +74,8 @@ typedef struct fwo_linear_transform {
     double center[3];
 } fwo_linear_transform;
 
-/* SyN recipe, crates/fastwarp-reg/src/recipe.rs:52-100 (Mattes channels are not part of this
- * restatement; masks are passed beside it as fwo_syn_masks). */
+/* SyN recipe, crates/fastwarp-reg/src/recipe.rs:52-100 (masks are passed beside it as
+ * fwo_syn_masks). channel_metrics: 0 = CC[radius], 1 = dense Mattes MI[mi_bins] (SynMetric). */
 #define FWO_MAX_LEVELS 8
 #define FWO_MAX_CHANNELS 4
 typedef struct fwo_syn_recipe {
@@ -92,6 +92,8 @@ typedef struct fwo_syn_recipe {
     int32_t convergence_window;
     int32_t channels;
     double channel_weights[FWO_MAX_CHANNELS];
+    int32_t channel_metrics[FWO_MAX_CHANNELS];
+    int32_t mi_bins;
 } fwo_syn_recipe;
 
 /* One SyN iteration record, crates/fastwarp-reg/src/syn.rs:96-113. */

@@ -50,3 +50,19 @@ def test_the_backend_name_and_error_reporting_work_without_a_device():
     bad = N.Grid()
     assert lib.fw_shrink_grid(C.byref(bad), (C.c_uint32 * 3)(2, 2, 2), C.byref(g)) == N.FW_ERR_INVALID
     assert b"zero size" in lib.fw_last_error()
+
+
+def test_every_mirrored_struct_has_the_library_layout_size():
+    import ctypes as C
+
+    from fastwarp_b200 import _native as N
+    from fastwarp_b200 import serve as S
+    pairs = {"fw_grid": N.Grid, "fw_affine": N.Affine, "fw_invert_params": N.InvertParams,
+             "fw_invert_stats": N.InvertStats, "fw_mi_binning": N.MiBinning,
+             "fw_linear_transform": N.LinearTransform, "fw_syn_recipe": N.SynRecipe,
+             "fw_syn_iteration": N.SynIteration, "fw_stats": N.Stats,
+             "fw_syn_request": S.SynRequest, "fw_syn_result": S.SynResultC,
+             "fw_server_stats": S.ServerStats}
+    for name, cls in pairs.items():
+        assert N.lib().fw_abi_struct_size(name.encode()) == C.sizeof(cls), name
+    assert N.lib().fw_abi_struct_size(b"no such struct") == 0

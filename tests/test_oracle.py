@@ -564,3 +564,30 @@ def test_an_all_zero_mask_is_refused():
                      shrink=(1,), sigmas=(0.0,), convergence_threshold=-1.0)
     with pytest.raises(RuntimeError, match="fixed mask has no voxel inside"):
         O.syn_run(r, g, [f], g, [m], masks=dict(fixed_grid=g, fixed=np.zeros((n, n, n))))
+
+
+def test_a_mattes_channel_syn_loop_reduces_its_energy():
+    """SynMetric::Mattes channels (syn.rs:301-335): the dense MI pair drives the loop."""
+    n = 24
+    g = cube(n)
+    f, m, _ = _cavity_pair(n)
+    r = O.syn_recipe(gradient_step=0.1, update_variance=3.0, cc_radius=2, iterations=(12,),
+                     shrink=(1,), sigmas=(0.0,), convergence_threshold=-1.0,
+                     metrics=["mattes"], mi_bins=32)
+    warp, inv, recs, _ = O.syn_run(r, g, [f], g, [m])
+    assert len(recs) == 12
+    assert recs[-1].energy < recs[0].energy - 0.1  # -MI: lower is better
+    assert np.isfinite(warp).all() and np.abs(warp).max() > 0.1
+
+
+def test_a_cc_and_a_mattes_channel_combine():
+    n = 20
+    g = cube(n)
+    f, m, _ = _cavity_pair(n)
+    r = O.syn_recipe(gradient_step=0.25, update_variance=3.0, cc_radius=2, iterations=(4,),
+                     shrink=(1,), sigmas=(0.0,), convergence_threshold=-1.0,
+                     weights=(0.5, 0.5), metrics=["cc", "mattes"], mi_bins=16)
+    warp, inv, recs, _ = O.syn_run(r, g, [f, 1.0 - f], g, [m, 1.0 - m])
+    # the energy is the first channel's (CC) value; the weighted energy mixes in the MI value
+    assert recs[0].energy != recs[0].energy_weighted
+    assert np.isfinite(warp).all()
