@@ -202,9 +202,12 @@ int new_field(fw_ctx* ctx, const HostGrid& g, fw_field** out) {
     return 0;
 }
 
+// Waits for the context's stream on a blocking-sync event: the waiting thread sleeps instead of
+// spinning, so the slots of a server do not take host cores from one another while they wait.
 int sync(fw_ctx* ctx) {
     ctx->stats.host_syncs++;
-    FW_CUDA(cudaStreamSynchronize(ctx->stream));
+    FW_CUDA(cudaEventRecord(ctx->done, ctx->stream));
+    FW_CUDA(cudaEventSynchronize(ctx->done));
     return 0;
 }
 
@@ -553,6 +556,18 @@ int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, f
     return check_launch(ctx, "k_compose");
 }
 
+__global__ void k_image_product(const float* __restrict__ a, const float* __restrict__ b,
+                                float* __restrict__ out, long long n) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < n) out[l] = a[l] * b[l];
+}
+
+int launch_image_product(fw_ctx* ctx, const fw_image* a, const fw_image* b, fw_image* out) {
+    long long n = out->grid.count();
+    k_image_product<<<blocks_for(n), 256, 0, ctx->stream>>>(a->d, b->d, out->d, n);
+    return check_launch(ctx, "k_image_product");
+}
+
 int launch_max_norm(fw_ctx* ctx, const fw_field* f, unsigned int* d_max_bits) {
     FieldArgs a{dev_grid(f->grid), f->ps};
     k_max_norm<<<blocks_for(a.g.n), 256, 0, ctx->stream>>>(a, f->d, d_max_bits);
@@ -625,6 +640,8 @@ int fw_ctx_create(int device, fw_ctx** out) {
     ctx->num_sms = prop.multiProcessorCount;
     e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&ctx->done, cudaEventBlockingSync | cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete ctx;
         return cuda_fail(e, "cudaStreamCreate");
@@ -676,6 +693,7 @@ void fw_ctx_destroy(fw_ctx* ctx) {
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->done) cudaEventDestroy(ctx->done);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->aux) cudaStreamDestroy(ctx->aux);
     // the pool's blocks go back to the device; a buffer still outstanding keeps them until freed

@@ -93,6 +93,7 @@ struct fw_ctx {
     const volatile int32_t* cancel = nullptr;
     bool capturing = false;          // a graph capture is in progress on `stream`
     cudaStream_t aux = nullptr;      // second stream for capturing conditional bodies
+    cudaEvent_t done = nullptr;      // blocking-sync event the host waits on
     cudaMemPool_t pool = nullptr;    // the context's own stream-ordered memory pool
     // freed buffers kept by size for the next allocation of that size (stream order makes the
     // reuse safe: every user of a buffer runs on `stream`); guarded for frees from other threads
@@ -368,6 +369,25 @@ int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse
                            InvState* st, cudaGraphConditionalHandle handle, int use_handle);
 int enqueue_inversion_rearm(fw_ctx* ctx, InvState* st, int max_iterations);
 int read_back(fw_ctx* ctx, const double* d, int k, double* out);
+}  // namespace fw
+
+// Device scratch of one dense Mattes MI pair (fw_mi.cu).
+struct fw_dense_mi;
+
+namespace fw {
+
+// The dense Mattes MI pair (Backend::mi_value_derivative_pair[_masked]) as a stream-ordered
+// sequence of kernels without host read-back (capturable in a graph): the two derivative fields,
+// and at `publish` on the device [value (fixed, moving), |d_fixed|^2, |d_moving|^2, 0,
+// value (moving, fixed), status] (status as dense_mi_status reads it).
+int dense_mi_create(fw_ctx* ctx, int bins, long long n, fw_dense_mi** out);
+void dense_mi_free(fw_dense_mi* d);
+int enqueue_dense_mi_pair(fw_ctx* ctx, const fw_image* f, const fw_image* m, const fw_image* fm,
+                          const fw_image* mm, fw_field* d_fixed, fw_field* d_moving,
+                          fw_dense_mi* sc, double* publish);
+// The error of a published status (0: none); `masked`: the pair had a mask.
+int dense_mi_status(int status, bool masked);
+
 // The SyN stage on device images (fw_syn.cu); masks may be null.
 int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
                    const fw_image* const* moving, const fw_image* fixed_mask,
@@ -407,6 +427,8 @@ int launch_cc_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, i
 int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double variance,
                   unsigned int* d_max_bits, fw_field* tmp);
 int launch_max_norm(fw_ctx* ctx, const fw_field* f, unsigned int* d_max_bits);
+// out = a * b voxelwise (three images on one grid; out may be a or b).
+int launch_image_product(fw_ctx* ctx, const fw_image* a, const fw_image* b, fw_image* out);
 // out = warping + step/max * disp(x + warping) (step 1 without max bits).
 int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, fw_field* out,
                    const unsigned int* d_scale_max_bits, double step);

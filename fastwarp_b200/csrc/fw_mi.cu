@@ -863,139 +863,170 @@ std::string empty_range_message(const char* role, bool masked) {
     return std::string("the ") + role + " image has no finite voxel";
 }
 
+// [vF, |dF|^2, |dM|^2, 0, vM, status]: the scalars of one pair where the SyN driver reads them.
+// status: 0 ok, 1 / 2 no finite fixed / moving voxel (inside its mask), 3 / 4 fixed / moving
+// image constant, 5 no voxel contributes, 6 joint PDF zero.
+__global__ void k_dense_publish(const DenseState* __restrict__ st, const double* __restrict__ out,
+                                const double* __restrict__ norms, double* __restrict__ pub) {
+    int status = st->status;
+    for (int dir = 0; dir < 2 && status == 0; ++dir) {
+        if (out[4 * dir + 2] == 1.0) status = 5;
+        else if (out[4 * dir + 2] == 2.0) status = 6;
+    }
+    pub[0] = out[0];
+    pub[1] = norms[0];
+    pub[2] = norms[1];
+    pub[3] = 0.0;
+    pub[4] = out[4];
+    pub[5] = (double)status;
+}
+
+}  // namespace
+}  // namespace fw
+
 // Device scratch of one dense pair: [state | out 2x4 | norms 2 | hist | ratio | partials].
-struct DenseScratch {
+struct fw_dense_mi {
     fw_ctx* ctx = nullptr;
     void* base = nullptr;
     size_t bytes = 0;
-    DenseState* st = nullptr;
+    int bins = 0;
+    unsigned int blocks = 0;
+    fw::DenseState* st = nullptr;
     double* out = nullptr;
     double* norms = nullptr;
     unsigned long long* hist = nullptr;
     double* ratio = nullptr;
     double* partials = nullptr;
     unsigned int* counter = nullptr;
-    ~DenseScratch() {
-        if (base) dev_free(ctx, base, bytes);
-    }
-    static constexpr size_t head = 512;  // state + out + norms, read back in one copy
-    int init(fw_ctx* c, int bins, unsigned int blocks) {
-        ctx = c;
-        const size_t cells = (size_t)bins * bins + bins;
-        const size_t o_hist = head, o_ratio = o_hist + 16 * cells,
-                     o_part = o_ratio + 16 * (size_t)bins * bins,
-                     o_cnt = o_part + 16 * (size_t)blocks;
-        bytes = o_cnt + 256;
-        FW_TRY(dev_alloc(ctx, bytes, &base));
-        char* b = static_cast<char*>(base);
-        st = reinterpret_cast<DenseState*>(b);
-        out = reinterpret_cast<double*>(b + 256);
-        norms = reinterpret_cast<double*>(b + 256 + 64);
-        hist = reinterpret_cast<unsigned long long*>(b + o_hist);
-        ratio = reinterpret_cast<double*>(b + o_ratio);
-        partials = reinterpret_cast<double*>(b + o_part);
-        counter = reinterpret_cast<unsigned int*>(b + o_cnt);
-        FW_CUDA(cudaMemsetAsync(base, 0, bytes, ctx->stream));
-        return 0;
-    }
 };
 
-static_assert(sizeof(DenseState) <= 256, "dense state slot");
+namespace fw {
+
+int dense_mi_create(fw_ctx* ctx, int bins, long long n, fw_dense_mi** out) {
+    if (bins <= 4) return fail(FW_ERR_INVALID, "mattes: at least five histogram bins are required");
+    if (bins > MAX_BINS) return fail(FW_ERR_INVALID, "mattes: bins must be in 5..=32");
+    fw_dense_mi* d = new fw_dense_mi();
+    d->ctx = ctx;
+    d->bins = bins;
+    d->blocks = (unsigned int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 2LL * ctx->num_sms));
+    const size_t cells = (size_t)bins * bins + bins;
+    const size_t o_hist = 512, o_ratio = o_hist + 16 * cells,
+                 o_part = o_ratio + 16 * (size_t)bins * bins, o_cnt = o_part + 16 * (size_t)d->blocks;
+    d->bytes = o_cnt + 256;
+    int rc = dev_alloc(ctx, d->bytes, &d->base);
+    if (rc) {
+        delete d;
+        return rc;
+    }
+    char* b = static_cast<char*>(d->base);
+    d->st = reinterpret_cast<DenseState*>(b);
+    d->out = reinterpret_cast<double*>(b + 256);
+    d->norms = reinterpret_cast<double*>(b + 256 + 64);
+    d->hist = reinterpret_cast<unsigned long long*>(b + o_hist);
+    d->ratio = reinterpret_cast<double*>(b + o_ratio);
+    d->partials = reinterpret_cast<double*>(b + o_part);
+    d->counter = reinterpret_cast<unsigned int*>(b + o_cnt);
+    cudaError_t e = cudaMemsetAsync(d->base, 0, d->bytes, ctx->stream);
+    if (e != cudaSuccess) {
+        dense_mi_free(d);
+        return cuda_fail(e, "dense MI scratch");
+    }
+    *out = d;
+    return 0;
+}
+
+void dense_mi_free(fw_dense_mi* d) {
+    if (!d) return;
+    if (d->base) dev_free(d->ctx, d->base, d->bytes);
+    delete d;
+}
+
+int enqueue_dense_mi_pair(fw_ctx* ctx, const fw_image* f, const fw_image* m, const fw_image* fm,
+                          const fw_image* mm, fw_field* d_fixed, fw_field* d_moving,
+                          fw_dense_mi* sc, double* publish) {
+    if (!f->grid.same(m->grid)) return fail(FW_ERR_INVALID, "mattes: the images are not on one grid");
+    if ((fm && !fm->grid.same(f->grid)) || (mm && !mm->grid.same(f->grid)))
+        return fail(FW_ERR_INVALID, "mattes: a mask is not on the grid of the images");
+    const HostGrid& g = f->grid;
+    const long long n = g.count();
+    const int bins = sc->bins;
+    const unsigned int blocks = sc->blocks;
+    const float* fmp = fm ? fm->d : nullptr;
+    const float* mmp = mm ? mm->d : nullptr;
+    k_dense_init<<<1, 1, 0, ctx->stream>>>(sc->st);
+    FW_TRY(check_launch(ctx, "k_dense_init"));
+    FW_CUDA(cudaMemsetAsync(sc->hist, 0, 16 * ((size_t)bins * bins + bins), ctx->stream));
+    k_dense_range<<<blocks, 256, 0, ctx->stream>>>(f->d, m->d, fmp, mmp, n, sc->st);
+    FW_TRY(check_launch(ctx, "k_dense_range"));
+    k_dense_setup<<<1, 1, 0, ctx->stream>>>(sc->st, bins);
+    FW_TRY(check_launch(ctx, "k_dense_setup"));
+    const size_t sh = 2 * sizeof(unsigned long long) * ((size_t)bins * bins + bins);
+    k_dense_hist<<<blocks, MI_THREADS, sh, ctx->stream>>>(f->d, m->d, fmp, mmp, n, bins, sc->st,
+                                                          sc->hist);
+    FW_TRY(check_launch(ctx, "k_dense_hist"));
+    k_mi_finish<<<2, 1024, 0, ctx->stream>>>(sc->hist, bins, 0.0, sc->st->mbin, sc->ratio,
+                                             sc->out, 1);
+    FW_TRY(check_launch(ctx, "k_mi_finish"));
+    DenseArgs da;
+    std::memset(&da, 0, sizeof(da));
+    da.g = dev_grid(g);
+    da.ps = d_fixed->ps;
+    da.bins = bins;
+    da.identity = 1;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            if (g.dir[r * 3 + c] != (r == c ? 1.0 : 0.0)) da.identity = 0;
+    for (int d = 0; d < 3; ++d) da.isp[d] = 1.0 / g.sp[d];
+    k_dense_deriv<<<blocks, MI_THREADS, 0, ctx->stream>>>(da, f->d, m->d, fmp, mmp, sc->st,
+                                                          sc->ratio, d_fixed->d, d_moving->d,
+                                                          sc->partials, sc->counter, sc->norms);
+    FW_TRY(check_launch(ctx, "k_dense_deriv"));
+    k_dense_publish<<<1, 1, 0, ctx->stream>>>(sc->st, sc->out, sc->norms, publish);
+    return check_launch(ctx, "k_dense_publish");
+}
+
+int dense_mi_status(int status, bool masked) {
+    switch (status) {
+        case 0: return 0;
+        case 1: return fail(FW_ERR_INVALID, "mattes: " + empty_range_message("fixed", masked));
+        case 2: return fail(FW_ERR_INVALID, "mattes: " + empty_range_message("moving", masked));
+        case 3: return fail(FW_ERR_INVALID, "mattes: the fixed image is constant");
+        case 4: return fail(FW_ERR_INVALID, "mattes: the moving image is constant");
+        case 5:
+            return fail(FW_ERR_INVALID, masked ? std::string("mattes: ") + FW_NO_VOXEL_IN_MASKS
+                                               : std::string("mattes: all samples map outside the moving image buffer"));
+        default: return fail(FW_ERR_INVALID, "mattes: joint PDF summed to zero");
+    }
+}
+
+namespace {
 
 int dense_pair(fw_ctx* ctx, const fw_image* f, const fw_image* m, const fw_image* fm,
                const fw_image* mm, int bins, double values[2], fw_field** d_fixed,
                fw_field** d_moving, double norms[2]) {
     FW_CHECK(ctx && f && m && values && d_fixed && d_moving, "null argument");
     if (!f->grid.same(m->grid)) return fail(FW_ERR_INVALID, "mattes: the images are not on one grid");
-    if ((fm && !fm->grid.same(f->grid)) || (mm && !mm->grid.same(f->grid)))
-        return fail(FW_ERR_INVALID, "mattes: a mask is not on the grid of the images");
-    if (bins <= 4) return fail(FW_ERR_INVALID, "mattes: at least five histogram bins are required");
-    if (bins > MAX_BINS) return fail(FW_ERR_INVALID, "mattes: bins must be in 5..=32");
-    const HostGrid& g = f->grid;
-    const long long n = g.count();
+    fw_dense_mi* sc = nullptr;
+    FW_TRY(dense_mi_create(ctx, bins, f->grid.count(), &sc));
     fw_field *a = nullptr, *b = nullptr;
-    FW_TRY(new_field(ctx, g, &a));
-    int rc = new_field(ctx, g, &b);
-    const unsigned int blocks =
-        (unsigned int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 2LL * ctx->num_sms));
-    DenseScratch sc;
-    if (!rc) rc = sc.init(ctx, bins, blocks);
-    const float* fmp = fm ? fm->d : nullptr;
-    const float* mmp = mm ? mm->d : nullptr;
-    if (!rc) {
-        k_dense_init<<<1, 1, 0, ctx->stream>>>(sc.st);
-        rc = check_launch(ctx, "k_dense_init");
-    }
-    if (!rc) {
-        k_dense_range<<<blocks, 256, 0, ctx->stream>>>(f->d, m->d, fmp, mmp, n, sc.st);
-        rc = check_launch(ctx, "k_dense_range");
-    }
-    if (!rc) {
-        k_dense_setup<<<1, 1, 0, ctx->stream>>>(sc.st, bins);
-        rc = check_launch(ctx, "k_dense_setup");
-    }
-    if (!rc) {
-        const size_t sh = 2 * sizeof(unsigned long long) * ((size_t)bins * bins + bins);
-        k_dense_hist<<<blocks, MI_THREADS, sh, ctx->stream>>>(f->d, m->d, fmp, mmp, n, bins, sc.st,
-                                                              sc.hist);
-        rc = check_launch(ctx, "k_dense_hist");
-    }
-    if (!rc) {
-        k_mi_finish<<<2, 1024, 0, ctx->stream>>>(sc.hist, bins, 0.0, sc.st->mbin, sc.ratio, sc.out,
-                                                 1);
-        rc = check_launch(ctx, "k_mi_finish");
-    }
-    if (!rc) {
-        DenseArgs da;
-        std::memset(&da, 0, sizeof(da));
-        da.g = dev_grid(g);
-        da.ps = a->ps;
-        da.bins = bins;
-        da.identity = 1;
-        for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c)
-                if (g.dir[r * 3 + c] != (r == c ? 1.0 : 0.0)) da.identity = 0;
-        for (int d = 0; d < 3; ++d) da.isp[d] = 1.0 / g.sp[d];
-        k_dense_deriv<<<blocks, MI_THREADS, 0, ctx->stream>>>(da, f->d, m->d, fmp, mmp, sc.st,
-                                                              sc.ratio, a->d, b->d, sc.partials,
-                                                              sc.counter, sc.norms);
-        rc = check_launch(ctx, "k_dense_deriv");
-    }
-    double headd[DenseScratch::head / sizeof(double)];  // copied bitwise, doubles or not
-    if (!rc) rc = read_back(ctx, static_cast<const double*>(sc.base), DenseScratch::head / 8, headd);
-    const unsigned char* head = reinterpret_cast<const unsigned char*>(headd);
-    if (!rc) {
-        DenseState st;
-        std::memcpy(&st, head, sizeof(st));
-        const double* out = reinterpret_cast<const double*>(head + 256);
-        const double* nr = reinterpret_cast<const double*>(head + 256 + 64);
-        switch (st.status) {
-            case 1: rc = fail(FW_ERR_INVALID, "mattes: " + empty_range_message("fixed", fm != nullptr)); break;
-            case 2: rc = fail(FW_ERR_INVALID, "mattes: " + empty_range_message("moving", mm != nullptr)); break;
-            case 3: rc = fail(FW_ERR_INVALID, "mattes: the fixed image is constant"); break;
-            case 4: rc = fail(FW_ERR_INVALID, "mattes: the moving image is constant"); break;
-            default: break;
-        }
-        for (int dir = 0; dir < 2 && !rc; ++dir) {
-            if (out[4 * dir + 2] == 1.0)
-                rc = fail(FW_ERR_INVALID, (fm || mm) ? std::string("mattes: ") + FW_NO_VOXEL_IN_MASKS
-                                                     : std::string("mattes: all samples map outside the moving image buffer"));
-            else if (out[4 * dir + 2] == 2.0)
-                rc = fail(FW_ERR_INVALID, "mattes: joint PDF summed to zero");
-        }
-        if (!rc) {
-            values[0] = out[0];
-            values[1] = out[4];
-            if (norms) {
-                norms[0] = std::sqrt(nr[0]);
-                norms[1] = std::sqrt(nr[1]);
-            }
-        }
-    }
+    int rc = new_field(ctx, f->grid, &a);
+    if (!rc) rc = new_field(ctx, f->grid, &b);
+    double* pub = ctx->d_scratch + SLOT_MI;
+    if (!rc) rc = enqueue_dense_mi_pair(ctx, f, m, fm, mm, a, b, sc, pub);
+    double h[6] = {0, 0, 0, 0, 0, 0};
+    if (!rc) rc = read_back(ctx, pub, 6, h);
+    if (!rc) rc = dense_mi_status((int)h[5], fm || mm);
+    dense_mi_free(sc);
     if (rc) {
         fw_field_free(a);
         fw_field_free(b);
         return rc;
+    }
+    values[0] = h[0];
+    values[1] = h[4];
+    if (norms) {
+        norms[0] = std::sqrt(h[1]);
+        norms[1] = std::sqrt(h[2]);
     }
     *d_fixed = a;
     *d_moving = b;

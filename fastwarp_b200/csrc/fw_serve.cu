@@ -157,7 +157,7 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
     fw_field_free(w);
     fw_field_free(iw);
     cudaEventRecord(e1, ctx->stream);
-    cudaStreamSynchronize(ctx->stream);
+    if (sync(ctx) && !rc) rc = FW_ERR_CUDA;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->epoch_set) {

@@ -38,7 +38,7 @@ struct SynDev {
     int limit;       // iteration limit of this level
     int converged;
     int status;      // 0 ok, 1 gradient not finite, 2 field not finite, 3 cancelled,
-                     // 4 no voxel inside the masks
+                     // 4 no voxel inside the masks (CC), 10 + k a Mattes pair's status k
     int level;
     int window;
     int count;       // values in the window
@@ -50,6 +50,7 @@ struct SynDev {
     int channels;
     int masked;      // the CC pairs take the masks' valid voxels
     double wnorm[FW_MAX_CHANNELS];
+    int metric[FW_MAX_CHANNELS];  // FW_METRIC_CC or FW_METRIC_MATTES
 };
 
 // convergence.rs:91-126, the closed form of the two-control-point fit.
@@ -95,21 +96,40 @@ __global__ void k_syn_level_init(SynDev* s, int level, int limit) {
     s->total = 0.0;
 }
 
-// cc: [channel][value, |dF|^2, |dM|^2, valid voxels]; max_bits: [F side, M side]; inv: 4 loop
-// states.
+// Per-channel scalars, CC_STRIDE doubles a channel: [value (fixed, moving), |dF|^2, |dM|^2,
+// valid voxels (masked CC), value (moving, fixed) (Mattes), status (Mattes)].
+constexpr int CC_STRIDE = 8;
+
+// cc: the per-channel scalars; max_bits: [F side, M side]; inv: 4 loop states.
 __global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
                              const unsigned int* __restrict__ max_bits,
                              const InvState* __restrict__ inv, fw_syn_iteration* trace,
                              int trace_cap, const volatile int* cancel,
                              cudaGraphConditionalHandle handle, int use_handle) {
-    double vF = cc[0], vM = cc[0];  // the CC value is symmetric in its two images
-    double weighted = 0.0;
-    for (int c = 0; c < s->channels; ++c) weighted += cc[4 * c] * s->wnorm[c];
-    if (s->channels == 1) weighted = vF;
+    // the CC value is symmetric in its two images; Mattes gives one value per direction
+    auto value_m = [&](int c) {
+        return s->metric[c] == FW_METRIC_MATTES ? cc[CC_STRIDE * c + 4] : cc[CC_STRIDE * c];
+    };
+    double vF = cc[0], vM = value_m(0);
+    double wF = 0.0, wM = 0.0;
+    for (int c = 0; c < s->channels; ++c) {
+        wF += cc[CC_STRIDE * c] * s->wnorm[c];
+        wM += value_m(c) * s->wnorm[c];
+    }
+    if (s->channels == 1) {
+        wF = vF;
+        wM = vM;
+    }
     for (int c = 0; c < s->channels && s->channels > 1; ++c)
-        if (!isfinite(cc[4 * c + 1]) || !isfinite(cc[4 * c + 2])) s->status = 1;
-    for (int c = 0; c < s->channels && s->masked; ++c)
-        if (cc[4 * c + 3] == 0.0) s->status = 4;
+        if (!isfinite(cc[CC_STRIDE * c + 1]) || !isfinite(cc[CC_STRIDE * c + 2])) s->status = 1;
+    for (int c = 0; c < s->channels; ++c) {
+        if (s->metric[c] == FW_METRIC_MATTES) {
+            const int k = (int)cc[CC_STRIDE * c + 5];
+            if (k != 0) s->status = 10 + k;
+        } else if (s->masked && cc[CC_STRIDE * c + 3] == 0.0) {
+            s->status = 4;
+        }
+    }
     float mF = __uint_as_float(max_bits[0]), mM = __uint_as_float(max_bits[1]);
     if (!isfinite(mF) || !isfinite(mM)) s->status = 1;
     for (int q = 0; q < 4; ++q)
@@ -131,7 +151,7 @@ __global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
         fw_syn_iteration r;
         r.level = s->level;
         r.energy = energy;
-        r.energy_weighted = 0.5 * (weighted + weighted);
+        r.energy_weighted = 0.5 * (wF + wM);
         r.convergence_value = cv;
         r.fixed_update_scale = mF > 0.0f ? s->step / (double)mF : s->step;
         r.moving_update_scale = mM > 0.0f ? s->step / (double)mM : s->step;
@@ -170,7 +190,7 @@ __global__ void k_scale_norms(float4* __restrict__ acc, long long n4, const doub
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= n4) return;
     double tot = 0.0;
-    for (int c = 0; c < channels; ++c) tot += sqrt(cc[4 * c + which]);
+    for (int c = 0; c < channels; ++c) tot += sqrt(cc[CC_STRIDE * c + which]);
     float s = (float)(tot / channels);
     float4 v = acc[l];
     v.x *= s;
@@ -192,7 +212,10 @@ struct Level {
     fw_field* R = nullptr;                      // inversion residual of the last measurement
     const fw_image* fmask = nullptr;            // recipe masks on their own grids (or none)
     const fw_image* mmask = nullptr;
-    fw_image* valid = nullptr;                  // the masks resolved on the level grid
+    fw_image* fvalid = nullptr;                 // each given mask resolved on the level grid
+    fw_image* mvalid = nullptr;
+    fw_image* valid = nullptr;                  // inside both (the CC pairs' voxels)
+    fw_dense_mi* mi = nullptr;                  // scratch of the Mattes pairs
 };
 
 void free_level_work(Level& L) {
@@ -201,7 +224,11 @@ void free_level_work(Level& L) {
     L.fmid.clear();
     L.mmid.clear();
     fw_image_free(L.valid);
-    L.valid = nullptr;
+    fw_image_free(L.fvalid);
+    fw_image_free(L.mvalid);
+    L.valid = L.fvalid = L.mvalid = nullptr;
+    dense_mi_free(L.mi);
+    L.mi = nullptr;
     fw_field* fs[] = {L.dF, L.dM, L.accF, L.accM, L.sF, L.sM, L.T, L.R};
     for (auto* f : fs) fw_field_free(f);
     L.dF = L.dM = L.accF = L.accM = L.sF = L.sM = L.T = L.R = nullptr;
@@ -227,14 +254,19 @@ int alloc_level_work(fw_ctx* ctx, const fw_syn_recipe* r, Level& L) {
         FW_TRY(new_field(ctx, L.grid, &L.sM));
     }
     if (r->total_field_variance > 0.0) FW_TRY(new_field(ctx, L.grid, &L.T));
-    if (L.fmask || L.mmask) FW_TRY(new_image(ctx, L.grid, &L.valid));
+    if (L.fmask) FW_TRY(new_image(ctx, L.grid, &L.fvalid));
+    if (L.mmask) FW_TRY(new_image(ctx, L.grid, &L.mvalid));
+    if (L.fmask && L.mmask) FW_TRY(new_image(ctx, L.grid, &L.valid));
+    bool mattes = false;
+    for (int c = 0; c < L.channels; ++c) mattes = mattes || r->channel_metrics[c] == FW_METRIC_MATTES;
+    if (mattes) FW_TRY(dense_mi_create(ctx, r->mi_bins, L.grid.count(), &L.mi));
     return 0;
 }
 
 // Device scalars of a run.
 struct RunDev {
     SynDev* syn;
-    double* cc;              // [channels][4]
+    double* cc;              // [channels][CC_STRIDE]
     unsigned int* max_bits;  // [2]
     InvState* inv;           // [4]
     fw_syn_iteration* trace;
@@ -329,27 +361,36 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
     double wsum = 0.0;
     for (int c = 0; c < C; ++c) wsum += r->channel_weights[c];
     const long long n4 = 3 * L.dF->ps / 4;
-    // syn.rs:555-580: the voxels of the level grid inside both masks (nearest voxel, half up):
-    // the fixed mask through F^-1, times the moving mask through affine(M^-1)
+    // syn.rs:496-580: each given mask resolved on the level grid (nearest voxel, half up), the
+    // fixed one through F^-1 and the moving one through affine(M^-1); CC takes the voxels inside
+    // both, a Mattes pair each mask on its own
     if (L.fmask)
-        FW_TRY(launch_warp(ctx, L.fmask, L.Fi, nullptr, nullptr, L.valid->d, true, nullptr));
+        FW_TRY(launch_warp(ctx, L.fmask, L.Fi, nullptr, nullptr, L.fvalid->d, true, nullptr));
     if (L.mmask)
-        FW_TRY(launch_warp(ctx, L.mmask, L.Mi, nullptr, initial, L.valid->d, true,
-                           L.fmask ? L.valid->d : nullptr));
+        FW_TRY(launch_warp(ctx, L.mmask, L.Mi, nullptr, initial, L.mvalid->d, true, nullptr));
+    const fw_image* valid = L.fvalid ? L.fvalid : L.mvalid;
+    if (L.fvalid && L.mvalid) {
+        FW_TRY(launch_image_product(ctx, L.fvalid, L.mvalid, L.valid));
+        valid = L.valid;
+    }
     for (int c = 0; c < C; ++c) {
         FW_TRY(launch_warp(ctx, fs[c], L.Fi, nullptr, nullptr, L.fmid[c]->d, false, nullptr));
         FW_TRY(launch_warp(ctx, ms[c], L.Mi, nullptr, initial, L.mmid[c]->d, false, nullptr));
-        FW_TRY(launch_cc_pair_impl(ctx, L.fmid[c], L.mmid[c], r->cc_radius, L.dF, L.dM,
-                                   d.cc + 4 * c, C > 1 ? 1 : 0, L.valid));
+        if (r->channel_metrics[c] == FW_METRIC_MATTES)
+            FW_TRY(enqueue_dense_mi_pair(ctx, L.fmid[c], L.mmid[c], L.fvalid, L.mvalid, L.dF,
+                                         L.dM, L.mi, d.cc + CC_STRIDE * c));
+        else
+            FW_TRY(launch_cc_pair_impl(ctx, L.fmid[c], L.mmid[c], r->cc_radius, L.dF, L.dM,
+                                       d.cc + CC_STRIDE * c, C > 1 ? 1 : 0, valid));
         if (C > 1) {
             double wn = r->channel_weights[c] / wsum;
             k_axpy_norm<<<blocks256(n4), 256, 0, ctx->stream>>>((float4*)L.accF->d,
                                                                 (const float4*)L.dF->d, n4,
-                                                                d.cc + 4 * c + 1, wn);
+                                                                d.cc + CC_STRIDE * c + 1, wn);
             FW_TRY(check_launch(ctx, "k_axpy_norm"));
             k_axpy_norm<<<blocks256(n4), 256, 0, ctx->stream>>>((float4*)L.accM->d,
                                                                 (const float4*)L.dM->d, n4,
-                                                                d.cc + 4 * c + 2, wn);
+                                                                d.cc + CC_STRIDE * c + 2, wn);
             FW_TRY(check_launch(ctx, "k_axpy_norm"));
         }
     }
@@ -417,6 +458,15 @@ int syn_validate(const fw_syn_recipe* r) {
              "syn recipe: convergence window must be in 1..=64");
     FW_CHECK(std::isfinite(r->update_field_variance) && std::isfinite(r->total_field_variance),
              "syn recipe: variances must be finite");
+    bool mattes = false;
+    for (int c = 0; c < r->channels; ++c) {
+        FW_CHECK(r->channel_metrics[c] == FW_METRIC_CC || r->channel_metrics[c] == FW_METRIC_MATTES,
+                 "syn recipe: unknown channel metric");
+        mattes = mattes || r->channel_metrics[c] == FW_METRIC_MATTES;
+    }
+    // recipe.rs:233-238
+    FW_CHECK(!mattes || r->mi_bins >= 5, "syn recipe: MI needs at least five histogram bins");
+    FW_CHECK(!mattes || r->mi_bins <= 32, "syn recipe: MI bins must be in 5..=32 on this engine");
     return 0;
 }
 
@@ -514,6 +564,7 @@ int upload_syn_dev(fw_ctx* ctx, const fw_syn_recipe* r, SynDev* d, bool masked) 
     SynDev h;
     std::memset(&h, 0, sizeof(h));
     h.masked = masked ? 1 : 0;
+    for (int c = 0; c < r->channels; ++c) h.metric[c] = r->channel_metrics[c];
     h.window = r->convergence_window;
     h.threshold = r->convergence_threshold;
     h.step = r->gradient_step;
@@ -632,7 +683,8 @@ int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
     return rc2;
 }
 
-int check_status(int status) {
+int check_status(int status, bool masked) {
+    if (status > 10) return dense_mi_status(status - 10, masked);
     switch (status) {
         case 0: return 0;
         case 1: return fail(FW_ERR_NOT_FINITE, "syn: the metric gradient is not finite");
@@ -645,9 +697,12 @@ int check_status(int status) {
 
 // Kernels per iteration outside the inversion bodies (for the launch counter).
 int kernels_per_iteration(const fw_syn_recipe* r, int mask_warps) {
-    int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) + 2 /*smooth or max*/ +
-            2 /*compose*/ + (r->total_field_variance > 0.0 ? 2 : 0) + 4 * 2 /*inv init+measure*/ +
-            1 /*record*/ + mask_warps;
+    int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) +
+            4 /*two-pass smoothing or max*/ + 2 /*compose*/ +
+            (r->total_field_variance > 0.0 ? 4 : 0) + 4 * 2 /*inv init+measure*/ + 1 /*record*/ +
+            mask_warps + (mask_warps == 2 ? 1 : 0) /*product*/;
+    for (int c = 0; c < r->channels; ++c)
+        if (r->channel_metrics[c] == FW_METRIC_MATTES) k += 6;  // 7 dense MI kernels, not 1 CC
     return k;
 }
 
@@ -813,7 +868,7 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
             ctx->stats.kernel_launches +=
                 (uint64_t)ran * kernels_per_iteration(r, (fixed_mask ? 1 : 0) + (moving_mask ? 1 : 0)) + 1;
             done += ran;
-            rc = check_status(h.status);
+            rc = check_status(h.status, fixed_mask || moving_mask);
         }
     }
     free_level_work(L);
@@ -936,7 +991,7 @@ int fw_syn_step_masked(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image*
     if (!rc) {
         SynDev h;
         FW_CUDA(cudaMemcpy(&h, rs.d.syn, sizeof(h), cudaMemcpyDeviceToHost));
-        rc = check_status(h.status);
+        rc = check_status(h.status, fixed_mask || moving_mask);
     }
     L.F = L.Fi = L.M = L.Mi = nullptr;  // owned by the caller
     free_level_work(L);

@@ -243,16 +243,21 @@ def run_syn_ops(backend: CudaBackend, recipe: SynRecipe, fixed_grid: N.Grid, fix
             sides = []
             for side in range(2):
                 sides.append({"values": [], "grad": None, "mag": 0.0})
+            metrics = recipe.channel_metrics or ["cc"] * C_
             for c in range(C_):
+                # syn.rs:350-398: the channel's metric pair, with norms for several channels
+                if metrics[c] == "mattes":
+                    pair, norms = b.mi_value_derivative_pair_with_norms(fmid[c], mmid[c],
+                                                                        recipe.mi_bins)
+                else:
+                    pair, norms = b.cc_value_derivative_pair_with_norms(fmid[c], mmid[c],
+                                                                        recipe.cc_radius)
+                (vf, df), (vm, dm) = pair
                 if C_ == 1:
-                    (vf, df), (vm, dm) = b.cc_value_derivative_pair(fmid[c], mmid[c],
-                                                                    recipe.cc_radius)
                     sides[0]["values"].append(vf)
                     sides[1]["values"].append(vm)
                     sides[0]["grad"], sides[1]["grad"] = df, dm
                 else:
-                    ((vf, df), (vm, dm)), norms = b.cc_value_derivative_pair_with_norms(
-                        fmid[c], mmid[c], recipe.cc_radius)
                     for side, (v, d, nrm) in enumerate([(vf, df, norms[0]), (vm, dm, norms[1])]):
                         s = sides[side]
                         s["values"].append(v)

@@ -32,7 +32,8 @@ def oracle_recipe(r: SynRecipe):
     return O.syn_recipe(r.gradient_step, r.update_field_variance, r.total_field_variance,
                         r.cc_radius, r.iterations, r.shrink_factors, r.smoothing_sigmas,
                         r.sigma_units_mm, r.convergence_threshold, r.convergence_window,
-                        r.channel_weights)
+                        r.channel_weights, metrics=r.channel_metrics or None,
+                        mi_bins=r.mi_bins)
 
 
 def ogrid(g):
@@ -245,3 +246,84 @@ def test_an_all_zero_mask_is_refused(backend):
     r = config1(2)
     with pytest.raises(N.FastwarpError, match="moving mask has no voxel inside"):
         run_syn(backend, r, g, [fixed], g, [moving], moving_mask=(g, np.zeros((24, 24, 24))))
+
+
+# ---- Mattes channels (SynMetric::Mattes, syn.rs:301-335): the dense MI pair drives the side ----
+# updates. Bars: one step matches to 1e-5 relative on the energy and 5e-4 of the largest update
+# component (the MI derivative tolerance, parity.rs:45-48); a run to 0.05 mm RMS and 1e-4
+# relative final energy.
+
+def mattes(iterations=1, **kw):
+    base = dict(gradient_step=0.1, update_field_variance=3.0, cc_radius=2,
+                iterations=[iterations], shrink_factors=[1], smoothing_sigmas=[0.0],
+                convergence_threshold=-1.0, channel_metrics=["mattes"], mi_bins=32)
+    base.update(kw)
+    return SynRecipe(**base)
+
+
+def test_one_mattes_syn_step_matches(backend, pair):
+    g, fixed, moving = pair
+    r = mattes()
+    og = ogrid(g)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    state = {k: backend.zero_field(g) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    rec, fu, mu = syn_step(backend, r, [fi], [mi], None, state)
+    ostate = {k: np.zeros((64, 64, 64, 3)) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    orec, ofu, omu = O.syn_step(oracle_recipe(r), og, og, [fixed], og, [moving], None, ostate)
+    assert abs(rec["energy"] - orec.energy) <= 1e-5 * abs(orec.energy)
+    assert abs(rec["energy_weighted"] - orec.energy_weighted) <= 1e-5 * abs(orec.energy_weighted)
+    assert np.abs(fu - ofu).max() <= 5e-4 * np.abs(ofu).max()
+    assert np.abs(mu - omu).max() <= 5e-4 * np.abs(omu).max()
+
+
+def test_mattes_registration_matches_the_oracle(backend):
+    g, fixed, moving = blob_pair(40, seed=61)
+    r = mattes(iterations=5, shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0])
+    r.iterations = [5, 4]
+    og = ogrid(g)
+    res = run_syn(backend, r, g, [fixed], g, [moving])
+    ow, oinv, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed], og, [moving])
+    assert len(res.iterations) == len(orecs) == 9
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    assert rms <= 0.05, rms
+    assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
+
+
+def test_a_cc_and_a_mattes_channel_with_masks_match_the_oracle(backend):
+    g, fixed, moving = blob_pair(40, seed=62)
+    r = mattes(iterations=4, channel_weights=[0.5, 0.5], channel_metrics=["cc", "mattes"])
+    fm, mgrid, mm = masks_for(40)
+    f2, m2 = 1.0 - fixed, 1.0 - moving
+    og = ogrid(g)
+    res = run_syn(backend, r, g, [fixed, f2], g, [moving, m2], fixed_mask=(g, fm),
+                  moving_mask=(mgrid, mm))
+    ow, _, orecs, _ = O.syn_run(oracle_recipe(r), og, [fixed, f2], og, [moving, m2],
+                                masks=dict(fixed_grid=og, fixed=fm, moving_grid=ogrid(mgrid),
+                                           moving=mm))
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    assert rms <= 0.05, rms
+    for a, b in zip(res.iterations, orecs):
+        assert abs(a["energy"] - b.energy) <= 1e-4 * abs(b.energy)
+        assert abs(a["energy_weighted"] - b.energy_weighted) <= 1e-4 * abs(b.energy_weighted)
+
+
+def test_mattes_recipe_errors(backend):
+    from fastwarp_b200 import _native as N
+    g, fixed, moving = blob_pair(16, seed=63)
+    with pytest.raises(N.FastwarpError, match="at least five histogram bins"):
+        run_syn(backend, mattes(mi_bins=4), g, [fixed], g, [moving])
+    flat = np.full_like(fixed, 0.5)
+    with pytest.raises(N.FastwarpError, match="the fixed image is constant"):
+        run_syn(backend, mattes(), g, [flat], g, [moving])
+
+
+def test_the_op_by_op_loop_with_a_mattes_channel_matches_the_graph_driver(backend):
+    from fastwarp_b200.syn import run_syn_ops
+    g, fixed, moving = blob_pair(32, seed=64)
+    r = mattes(iterations=3, channel_weights=[0.6, 0.4], channel_metrics=["mattes", "cc"])
+    f2, m2 = 1.0 - fixed, 1.0 - moving
+    res = run_syn(backend, r, g, [fixed, f2], g, [moving, m2])
+    w, iw, recs = run_syn_ops(backend, r, g, [fixed, f2], g, [moving, m2])
+    assert len(recs) == len(res.iterations) == 3
+    assert np.sqrt(((w - res.warp) ** 2).sum(-1).mean()) <= 1e-3
+    assert abs(recs[-1]["energy"] - res.iterations[-1]["energy"]) <= 1e-5 * abs(recs[-1]["energy"])
