@@ -844,31 +844,73 @@ int fw_field_upload(fw_ctx* ctx, const fw_grid* grid, const double* aos, fw_fiel
     return 0;
 }
 
-static int download_soa(fw_ctx* ctx, const fw_field* field, std::vector<float>& soa) {
-    soa.resize((size_t)(3 * field->ps));
-    FW_CUDA(cudaMemcpyAsync(soa.data(), field->d, field->bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    ctx->stats.bytes_downloaded += field->bytes;
-    return sync(ctx);
+}  // extern "C"
+
+namespace fw {
+namespace {
+
+// SoA planes -> AoS (x, y, z per voxel) of float or double, on the device.
+template <typename T>
+__global__ void k_soa_to_aos(const float* __restrict__ f, long long ps, long long n,
+                             T* __restrict__ out) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n) return;
+    out[3 * l] = (T)f[l];
+    out[3 * l + 1] = (T)f[l + ps];
+    out[3 * l + 2] = (T)f[l + 2 * ps];
 }
+
+template <typename T>
+int enqueue_field_aos(fw_ctx* ctx, const fw_field* field, T* host) {
+    const long long n = field->grid.count();
+    const size_t bytes = sizeof(T) * 3 * (size_t)n;
+    void* tmp = nullptr;
+    FW_TRY(dev_alloc(ctx, bytes, &tmp));
+    k_soa_to_aos<T><<<blocks_for(n), 256, 0, ctx->stream>>>(field->d, field->ps, n,
+                                                            static_cast<T*>(tmp));
+    int rc = check_launch(ctx, "k_soa_to_aos");
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "field download");
+    }
+    ctx->stats.bytes_downloaded += bytes;
+    dev_free(ctx, tmp, bytes);  // reused only by later work on this stream
+    return rc;
+}
+
+}  // namespace
+
+int enqueue_field_download_f32(fw_ctx* ctx, const fw_field* field, float* host) {
+    return enqueue_field_aos<float>(ctx, field, host);
+}
+
+int enqueue_image_upload_f32(fw_ctx* ctx, const HostGrid& g, const float* host, fw_image** out) {
+    fw_image* im;
+    FW_TRY(new_image(ctx, g, &im));
+    cudaError_t e = cudaMemcpyAsync(im->d, host, im->bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+        fw_image_free(im);
+        return cuda_fail(e, "image upload");
+    }
+    ctx->stats.bytes_uploaded += im->bytes;
+    *out = im;
+    return 0;
+}
+
+}  // namespace fw
+
+extern "C" {
 
 int fw_field_download(fw_ctx* ctx, const fw_field* field, double* aos) {
     FW_CHECK(ctx && field && aos, "null argument");
-    std::vector<float> soa;
-    FW_TRY(download_soa(ctx, field, soa));
-    int64_t n = field->grid.count();
-    for (int64_t l = 0; l < n; ++l)
-        for (int c = 0; c < 3; ++c) aos[3 * l + c] = soa[c * field->ps + l];
-    return 0;
+    FW_TRY(enqueue_field_aos<double>(ctx, field, aos));
+    return sync(ctx);
 }
 
 int fw_field_download_f32(fw_ctx* ctx, const fw_field* field, float* aos) {
     FW_CHECK(ctx && field && aos, "null argument");
-    std::vector<float> soa;
-    FW_TRY(download_soa(ctx, field, soa));
-    int64_t n = field->grid.count();
-    for (int64_t l = 0; l < n; ++l)
-        for (int c = 0; c < 3; ++c) aos[3 * l + c] = soa[c * field->ps + l];
-    return 0;
+    FW_TRY(enqueue_field_aos<float>(ctx, field, aos));
+    return sync(ctx);
 }
 
 int fw_field_grid(const fw_field* field, fw_grid* out) {

@@ -388,6 +388,12 @@ int enqueue_dense_mi_pair(fw_ctx* ctx, const fw_image* f, const fw_image* m, con
 // The error of a published status (0: none); `masked`: the pair had a mask.
 int dense_mi_status(int status, bool masked);
 
+// Stream-ordered host copies without a wait (the host buffer must stay valid, and for a
+// download unread, until the caller synchronises): a field as AoS float32 (converted on the
+// device) and an image from float32 host data.
+int enqueue_field_download_f32(fw_ctx* ctx, const fw_field* field, float* host);
+int enqueue_image_upload_f32(fw_ctx* ctx, const HostGrid& g, const float* host, fw_image** out);
+
 // The SyN stage on device images (fw_syn.cu); masks may be null.
 int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
                    const fw_image* const* moving, const fw_image* fixed_mask,

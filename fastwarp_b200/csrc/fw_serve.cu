@@ -15,6 +15,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <thread>
 #include <vector>
 
@@ -25,10 +26,46 @@ using Clock = std::chrono::steady_clock;
 
 namespace {
 
+// Pinned host buffers kept by size for reuse (cudaHostAlloc is slow and synchronises the
+// device): the staging of host inputs and the host results, so both copies run as DMA at full
+// link speed without a bounce through pageable memory. Process-wide: results outlive servers.
+struct PinnedPool {
+    std::mutex mu;
+    std::unordered_multimap<size_t, void*> free;
+    void* get(size_t bytes) {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            auto it = free.find(bytes);
+            if (it != free.end()) {
+                void* p = it->second;
+                free.erase(it);
+                return p;
+            }
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return p;
+    }
+    void put(void* p, size_t bytes) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lock(mu);
+        free.emplace(bytes, p);
+    }
+};
+
+PinnedPool& pinned() {
+    static PinnedPool* pool = new PinnedPool();  // kept to process exit (results may outlive it)
+    return *pool;
+}
+
 struct Job {
     uint64_t ticket = 0;
     fw_syn_request req{};
-    std::vector<std::vector<float>> fixed_host, moving_host;
+    std::vector<float*> fixed_host, moving_host;  // pinned staging of host inputs
+    size_t fixed_bytes = 0, moving_bytes = 0;
     std::vector<const fw_image*> fixed_dev, moving_dev;
     uint64_t bytes = 0;
     Clock::time_point submitted;
@@ -115,17 +152,18 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
             mi[c] = j->moving_dev[c];
         }
     } else {
+        HostGrid fg, mg;
+        rc = make_grid(&q.fixed_grid, fg);
+        if (!rc) rc = make_grid(&q.moving_grid, mg);
         for (int c = 0; c < C && !rc; ++c) {
             fw_image *a = nullptr, *b = nullptr;
-            rc = fw_image_upload_f32(ctx, &q.fixed_grid, j->fixed_host[c].data(), &a);
+            rc = enqueue_image_upload_f32(ctx, fg, j->fixed_host[c], &a);
             if (!rc) up.push_back(a);
-            if (!rc) rc = fw_image_upload_f32(ctx, &q.moving_grid, j->moving_host[c].data(), &b);
+            if (!rc) rc = enqueue_image_upload_f32(ctx, mg, j->moving_host[c], &b);
             if (!rc) up.push_back(b);
             fi[c] = a;
             mi[c] = b;
         }
-        j->fixed_host.clear();
-        j->moving_host.clear();
     }
     int64_t cap = 0;
     for (int l = 0; l < q.recipe.levels; ++l) cap += q.recipe.iterations[l];
@@ -146,18 +184,24 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
             res.inverse_dev = iw;
             w = iw = nullptr;
         } else {
-            size_t n3 = 3 * (size_t)w->grid.count();
-            res.warp = static_cast<float*>(std::malloc(n3 * sizeof(float)));
-            res.inverse_warp = static_cast<float*>(std::malloc(n3 * sizeof(float)));
+            // AoS float32 made on the device and copied straight into pinned result buffers
+            size_t bytes = 3 * sizeof(float) * (size_t)w->grid.count();
+            res.warp = static_cast<float*>(pinned().get(bytes));
+            res.inverse_warp = static_cast<float*>(pinned().get(bytes));
             if (!res.warp || !res.inverse_warp) rc = fail(FW_ERR_MEMORY, "serve: host allocation failed");
-            if (!rc) rc = fw_field_download_f32(ctx, w, res.warp);
-            if (!rc) rc = fw_field_download_f32(ctx, iw, res.inverse_warp);
+            if (!rc) rc = enqueue_field_download_f32(ctx, w, res.warp);
+            if (!rc) rc = enqueue_field_download_f32(ctx, iw, res.inverse_warp);
         }
     }
     fw_field_free(w);
     fw_field_free(iw);
     cudaEventRecord(e1, ctx->stream);
     if (sync(ctx) && !rc) rc = FW_ERR_CUDA;
+    // the uploads have completed: the staging goes back to the pool
+    for (auto* p : j->fixed_host) pinned().put(p, j->fixed_bytes);
+    for (auto* p : j->moving_host) pinned().put(p, j->moving_bytes);
+    j->fixed_host.clear();
+    j->moving_host.clear();
     {
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->epoch_set) {
@@ -173,9 +217,7 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
     res.status = rc;
     if (rc) {
         std::strncpy(res.error, fw_last_error(), sizeof(res.error) - 1);
-        std::free(res.warp);
-        std::free(res.inverse_warp);
-        res.warp = res.inverse_warp = nullptr;
+        fw_server_result_free(&res);
         fw_field_free(res.warp_dev);
         fw_field_free(res.inverse_dev);
         res.warp_dev = res.inverse_dev = nullptr;
@@ -287,9 +329,21 @@ int fw_server_submit(fw_server* s, const fw_syn_request* req, uint64_t* ticket) 
         return rc;
     }
     if (host) {
+        j->fixed_bytes = sizeof(float) * (size_t)fg.count();
+        j->moving_bytes = sizeof(float) * (size_t)mg.count();
         for (int c = 0; c < C; ++c) {
-            j->fixed_host.emplace_back(req->fixed[c], req->fixed[c] + fg.count());
-            j->moving_host.emplace_back(req->moving[c], req->moving[c] + mg.count());
+            float* a = static_cast<float*>(pinned().get(j->fixed_bytes));
+            float* b = static_cast<float*>(pinned().get(j->moving_bytes));
+            if (a) j->fixed_host.push_back(a);
+            if (b) j->moving_host.push_back(b);
+            if (!a || !b) {
+                for (auto* p : j->fixed_host) pinned().put(p, j->fixed_bytes);
+                for (auto* p : j->moving_host) pinned().put(p, j->moving_bytes);
+                delete j;
+                return fail(FW_ERR_MEMORY, "serve: pinned host staging allocation failed");
+            }
+            std::memcpy(a, req->fixed[c], j->fixed_bytes);
+            std::memcpy(b, req->moving[c], j->moving_bytes);
         }
     } else {
         for (int c = 0; c < C; ++c) {
@@ -332,8 +386,10 @@ int fw_server_wait(fw_server* s, uint64_t ticket, double timeout_s, fw_syn_resul
 
 void fw_server_result_free(fw_syn_result* r) {
     if (!r) return;
-    std::free(r->warp);
-    std::free(r->inverse_warp);
+    const size_t bytes =
+        3 * sizeof(float) * (size_t)(r->grid.size[0] * r->grid.size[1] * r->grid.size[2]);
+    pinned().put(r->warp, bytes);
+    pinned().put(r->inverse_warp, bytes);
     r->warp = r->inverse_warp = nullptr;
 }
 

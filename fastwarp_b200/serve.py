@@ -23,6 +23,25 @@ class SynRequest(C.Structure):
                 ("keep_on_device", C.c_int32), ("tag", C.c_uint64)]
 
 
+class _ResultBuffers:
+    """Owns the host buffers of one server result (fw_server_result_free when collected)."""
+
+    def __init__(self, result):
+        self.result = result
+
+    def array(self, address, shape):
+        n = int(np.prod(shape))
+        buf = (C.c_float * n).from_address(address)
+        buf._owner = self  # numpy's view keeps `buf`, `buf` keeps the owner
+        return np.ctypeslib.as_array(buf).reshape(shape)
+
+    def __del__(self):
+        try:
+            lib().fw_server_result_free(C.byref(self.result))
+        except Exception:
+            pass
+
+
 class SynResultC(C.Structure):
     _fields_ = [("tag", C.c_uint64), ("status", C.c_int32), ("error", C.c_char * 256),
                 ("grid", N.Grid), ("warp", C.c_void_p), ("inverse_warp", C.c_void_p),
@@ -113,14 +132,16 @@ class Server:
                "device_bytes": r.device_bytes, "queued_s": r.queued_s, "run_s": r.run_s,
                "latency_s": r.queued_s + r.run_s, "device_start_ms": r.device_start_ms,
                "device_end_ms": r.device_end_ms, "grid": r.grid}
-        if r.status == 0 and r.warp:
-            shape = grid_shape(r.grid) + (3,)
-            n = int(np.prod(shape))
-            out["warp"] = np.ctypeslib.as_array((C.c_float * n).from_address(r.warp)).reshape(shape).copy()
-            out["inverse_warp"] = np.ctypeslib.as_array(
-                (C.c_float * n).from_address(r.inverse_warp)).reshape(shape).copy()
         out["warp_dev"], out["inverse_dev"] = r.warp_dev, r.inverse_dev
-        lib().fw_server_result_free(C.byref(r))
+        if r.status == 0 and r.warp:
+            # the arrays view the result's pinned buffers; they go back to the library's pool
+            # when the last array referring to them is gone
+            shape = grid_shape(r.grid) + (3,)
+            owner = _ResultBuffers(r)
+            out["warp"] = owner.array(r.warp, shape)
+            out["inverse_warp"] = owner.array(r.inverse_warp, shape)
+        else:
+            lib().fw_server_result_free(C.byref(r))
         return out
 
     @staticmethod
