@@ -310,42 +310,37 @@ __global__ void __launch_bounds__(256) k_warp(WarpArgs a, const float* __restric
 // The plain warp (no earlier field, linear interpolation) -- the SyN loop's two per-iteration
 // warps -- with VPT voxels per thread, 256 apart, so their independent gathers are in flight
 // together.
-template <int VPT>
-__global__ void __launch_bounds__(256) k_warp_v(WarpArgs a, const float* __restrict__ u,
+// The plain warp (no earlier field, linear interpolation) -- the SyN loop's per-iteration warps --
+// over 32 x 8 column tiles marching along z, the next slice's displacement loaded while the
+// current one gathers.
+__global__ void __launch_bounds__(256) k_warp_t(WarpArgs a, int zchunk,
+                                                const float* __restrict__ u,
                                                 const float* __restrict__ src,
                                                 float* __restrict__ out) {
-    const long long base = (long long)blockIdx.x * (256 * VPT) + threadIdx.x;
-    float ux[VPT], uy[VPT], uz[VPT];
-#pragma unroll
-    for (int v = 0; v < VPT; ++v) {
-        long long l = base + v * 256;
-        ux[v] = uy[v] = uz[v] = 0.0f;
-        if (l < a.g.n) {
-            ux[v] = u[l];
-            uy[v] = u[l + a.fps];
-            uz[v] = u[l + 2 * a.fps];
+    int x, y, z0, z1;
+    if (!column_of(a.g.nx, a.g.ny, a.g.nz, zchunk, x, y, z0, z1)) return;
+    const long long sxy = (long long)a.g.nx * a.g.ny;
+    long long l = (long long)z0 * sxy + (long long)y * a.g.nx + x;
+    float ux = u[l], uy = u[l + a.fps], uz = u[l + 2 * a.fps];
+    for (int k = z0; k < z1; ++k, l += sxy) {
+        float nx_ = 0.0f, ny_ = 0.0f, nz_ = 0.0f;
+        if (k + 1 < z1) {
+            nx_ = u[l + sxy];
+            ny_ = u[l + sxy + a.fps];
+            nz_ = u[l + sxy + 2 * a.fps];
         }
-    }
-    float val[VPT];
-#pragma unroll
-    for (int v = 0; v < VPT; ++v) {
-        long long l = base + v * 256;
-        val[v] = 0.0f;
-        if (l >= a.g.n) continue;
-        int i, j, k;
-        voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
         double c[3];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
-            c[r] = a.q[r * 3] * i + a.q[r * 3 + 1] * j + a.q[r * 3 + 2] * k + a.q0[r] +
-                   (a.r[r * 3] * ux[v] + a.r[r * 3 + 1] * uy[v] + a.r[r * 3 + 2] * uz[v]);
+            c[r] = a.q[r * 3] * x + a.q[r * 3 + 1] * y + a.q[r * 3 + 2] * k + a.q0[r] +
+                   (a.r[r * 3] * ux + a.r[r * 3 + 1] * uy + a.r[r * 3 + 2] * uz);
+        float v = 0.0f;
         if (inside_index(c[0], c[1], c[2], a.s.nx, a.s.ny, a.s.nz))
-            val[v] = lin_at_index(src, a.s.nx, a.s.ny, a.s.nz, c[0], c[1], c[2]);
-    }
-#pragma unroll
-    for (int v = 0; v < VPT; ++v) {
-        long long l = base + v * 256;
-        if (l < a.g.n) out[l] = val[v];
+            v = lin_at_index(src, a.s.nx, a.s.ny, a.s.nz, c[0], c[1], c[2]);
+        out[l] = v;
+        ux = nx_;
+        uy = ny_;
+        uz = nz_;
     }
 }
 
@@ -358,31 +353,45 @@ struct FieldArgs {
 // s = step / max |u/sp| (step when the max is 0) or 1 without a max.
 // `w` and `out` may be the same buffer (the SyN loop composes in place: a voxel reads only its
 // own value of `w`), so neither is declared __restrict__.
-__global__ void __launch_bounds__(256) k_compose(FieldArgs a, const float* __restrict__ u,
-                                                 const float* w, float* out,
+__global__ void __launch_bounds__(256) k_compose(FieldArgs a, int zchunk,
+                                                 const float* __restrict__ u, const float* w,
+                                                 float* out,
                                                  const unsigned int* __restrict__ max_bits,
                                                  double step) {
-    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= a.g.n) return;
+    int i, j, z0, z1;
+    if (!column_of(a.g.nx, a.g.ny, a.g.nz, zchunk, i, j, z0, z1)) return;
     float s = 1.0f;
     if (max_bits) {
         float mx = __uint_as_float(*max_bits);
         s = mx > 0.0f ? (float)(step / (double)mx) : (float)step;
     }
-    int i, j, k;
-    voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
+    const long long sxy = (long long)a.g.nx * a.g.ny;
+    long long l = (long long)z0 * sxy + (long long)j * a.g.nx + i;
     float wx = w[l], wy = w[l + a.ps], wz = w[l + 2 * a.ps];
-    double c[3];
+    for (int k = z0; k < z1; ++k, l += sxy) {
+        // the next slice's own field values, in flight during this slice's gather (each voxel
+        // reads only its own w, so the composition may run in place)
+        float qx = 0.0f, qy = 0.0f, qz = 0.0f;
+        if (k + 1 < z1) {
+            qx = w[l + sxy];
+            qy = w[l + sxy + a.ps];
+            qz = w[l + sxy + 2 * a.ps];
+        }
+        double c[3];
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
-        c[r] = (r == 0 ? i : (r == 1 ? j : k)) +
-               (a.g.inv[r * 3] * wx + a.g.inv[r * 3 + 1] * wy + a.g.inv[r * 3 + 2] * wz);
-    float d[3] = {0.0f, 0.0f, 0.0f};
-    if (inside_index(c[0], c[1], c[2], a.g.nx, a.g.ny, a.g.nz))
-        vec_at_index(u, a.ps, a.g.nx, a.g.ny, a.g.nz, c[0], c[1], c[2], d);
-    out[l] = fmaf(s, d[0], wx);
-    out[l + a.ps] = fmaf(s, d[1], wy);
-    out[l + 2 * a.ps] = fmaf(s, d[2], wz);
+        for (int r = 0; r < 3; ++r)
+            c[r] = (r == 0 ? i : (r == 1 ? j : k)) +
+                   (a.g.inv[r * 3] * wx + a.g.inv[r * 3 + 1] * wy + a.g.inv[r * 3 + 2] * wz);
+        float d[3] = {0.0f, 0.0f, 0.0f};
+        if (inside_index(c[0], c[1], c[2], a.g.nx, a.g.ny, a.g.nz))
+            vec_at_index(u, a.ps, a.g.nx, a.g.ny, a.g.nz, c[0], c[1], c[2], d);
+        out[l] = fmaf(s, d[0], wx);
+        out[l + a.ps] = fmaf(s, d[1], wy);
+        out[l + 2 * a.ps] = fmaf(s, d[2], wz);
+        wx = qx;
+        wy = qy;
+        wz = qz;
+    }
 }
 
 // field_ops.rs:580-605: onto another grid, scalar linear interpolation per component, zero
@@ -540,8 +549,10 @@ int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const f
     }
     long long n = a.g.n;
     if (!pre && !mask) {
-        k_warp_v<4><<<blocks_for(n, 1024), 256, 0, ctx->stream>>>(a, field->d, src->d, out);
-        return check_launch(ctx, "k_warp_v");
+        int zchunk = 1;
+        const dim3 grid = column_grid(a.g.nx, a.g.ny, a.g.nz, ctx->num_sms, &zchunk);
+        k_warp_t<<<grid, 256, 0, ctx->stream>>>(a, zchunk, field->d, src->d, out);
+        return check_launch(ctx, "k_warp_t");
     }
     k_warp<<<blocks_for(n), 256, 0, ctx->stream>>>(a, field->d, pre ? pre->d : nullptr, src->d,
                                                    product, out);
@@ -551,8 +562,10 @@ int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const f
 int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, fw_field* out,
                    const unsigned int* d_scale_max_bits, double step) {
     FieldArgs a{dev_grid(warping->grid), warping->ps};
-    k_compose<<<blocks_for(a.g.n), 256, 0, ctx->stream>>>(a, disp->d, warping->d, out->d,
-                                                          d_scale_max_bits, step);
+    int zchunk = 1;
+    const dim3 grid = column_grid(a.g.nx, a.g.ny, a.g.nz, ctx->num_sms, &zchunk);
+    k_compose<<<grid, 256, 0, ctx->stream>>>(a, zchunk, disp->d, warping->d, out->d,
+                                             d_scale_max_bits, step);
     return check_launch(ctx, "k_compose");
 }
 

@@ -318,6 +318,28 @@ __device__ __forceinline__ void central_difference_voxel(const float* __restrict
     }
 }
 
+// Thread mapping of the gather sweeps (warp, compose, inversion): a block of 256 threads is a
+// 32 x 8 tile of (x, y) columns and each thread marches along z through `zchunk` slices, so the
+// trilinear gathers of neighbouring columns and consecutive slices meet in L1.
+inline dim3 column_grid(int nx, int ny, int nz, int num_sms, int* zchunk) {
+    dim3 g((unsigned int)((nx + 31) / 32), (unsigned int)((ny + 7) / 8), 1);
+    const long long tiles = (long long)g.x * g.y;
+    const long long want = (6LL * num_sms + tiles - 1) / tiles;
+    *zchunk = (int)((nz + (want > 1 ? want : 1) - 1) / (want > 1 ? want : 1));
+    if (*zchunk < 1) *zchunk = 1;
+    g.z = (unsigned int)((nz + *zchunk - 1) / *zchunk);
+    return g;
+}
+
+__device__ __forceinline__ bool column_of(int nx, int ny, int nz, int zchunk, int& x, int& y,
+                                          int& z0, int& z1) {
+    x = blockIdx.x * 32 + (threadIdx.x & 31);
+    y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    z0 = blockIdx.z * zchunk;
+    z1 = min(z0 + zchunk, nz);
+    return x < nx && y < ny && z0 < z1;
+}
+
 __device__ __forceinline__ void voxel_ijk(long long l, int nx, int ny, int& i, int& j, int& k) {
     long long q = l / nx;
     i = (int)(l - q * nx);

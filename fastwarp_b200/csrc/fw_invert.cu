@@ -24,7 +24,28 @@ struct InvArgs {
     DevGrid g;
     long long ps_f, ps_psi;
     float isx, isy, isz;
+    int zchunk;  // slices a thread marches through
 };
+
+// Thread mapping of the sweeps: a block is a 32 x 8 tile of (x, y) columns and each thread marches
+// along z through `zchunk` slices. The trilinear gathers of neighbouring columns and of
+// consecutive slices fall on the same rows of the field, so they meet in L1 instead of each
+// crossing from L2 (the gathers' bound); the next slice's own values are loaded while the current
+// slice gathers.
+struct Column {
+    int x, y, z0, z1;
+    bool own;
+};
+
+__device__ __forceinline__ Column column_of(const InvArgs& a) {
+    Column c;
+    c.x = blockIdx.x * 32 + (threadIdx.x & 31);
+    c.y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    c.z0 = blockIdx.z * a.zchunk;
+    c.z1 = min(c.z0 + a.zchunk, a.g.nz);
+    c.own = c.x < a.g.nx && c.y < a.g.ny;
+    return c;
+}
 
 __device__ __forceinline__ void residual(const InvArgs& a, const float* __restrict__ f,
                                          long long l, int i, int j, int k, float px, float py,
@@ -51,6 +72,8 @@ __device__ void reduce_and_finish(double sum, float mx, double* __restrict__ par
     sum = warp_sum_d(sum);
     mx = warp_max_f(mx);
     const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
     if ((threadIdx.x & 31) == 0) {
         rs[w] = sum;
         rm[w] = mx;
@@ -63,17 +86,17 @@ __device__ void reduce_and_finish(double sum, float mx, double* __restrict__ par
             s += rs[q];
             m = __int_as_float(max(__float_as_int(m), __float_as_int(rm[q])));
         }
-        partials[2 * blockIdx.x] = s;
-        partials[2 * blockIdx.x + 1] = (double)m;
+        partials[2 * bid] = s;
+        partials[2 * bid + 1] = (double)m;
     }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == nblocks - 1;
     __syncthreads();
     if (!last) return;
     if (threadIdx.x < 32) {
         double s = 0.0, m = 0.0;
-        for (unsigned int b = threadIdx.x; b < gridDim.x; b += 32) {
+        for (unsigned int b = threadIdx.x; b < nblocks; b += 32) {
             s += __ldcg(partials + 2 * b);
             double mb = __ldcg(partials + 2 * b + 1);
             m = (mb > m || mb != mb) ? mb : m;
@@ -103,25 +126,30 @@ __global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __r
                                                      int use_handle) {
     double sum = 0.0;
     float mx = 0.0f;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    // two voxels a step, `stride` apart: their gathers are in flight together
-    for (long long l0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; l0 < a.g.n;
-         l0 += 2 * stride) {
-#pragma unroll
-        for (int v = 0; v < 2; ++v) {
-            long long l = l0 + v * stride;
-            if (l >= a.g.n) continue;
-            int i, j, k;
-            voxel_ijk(l, a.g.nx, a.g.ny, i, j, k);
+    const Column col = column_of(a);
+    if (col.own && col.z0 < col.z1) {
+        const long long sxy = (long long)a.g.nx * a.g.ny;
+        long long l = (long long)col.z0 * sxy + (long long)col.y * a.g.nx + col.x;
+        float px = psi[l], py = psi[l + a.ps_psi], pz = psi[l + 2 * a.ps_psi];
+        for (int z = col.z0; z < col.z1; ++z, l += sxy) {
+            float qx = 0.0f, qy = 0.0f, qz = 0.0f;
+            if (z + 1 < col.z1) {  // the next slice's psi, in flight during this gather
+                qx = psi[l + sxy];
+                qy = psi[l + sxy + a.ps_psi];
+                qz = psi[l + sxy + 2 * a.ps_psi];
+            }
             float e[3];
-            residual(a, f, l, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
+            residual(a, f, l, col.x, col.y, z, px, py, pz, e);
             res[l] = e[0];
             res[l + a.ps_psi] = e[1];
             res[l + 2 * a.ps_psi] = e[2];
-            float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
-            float nrm = nan_canon(sqrtf(x * x + y * y + z * z));
+            float x = e[0] * a.isx, y = e[1] * a.isy, zz = e[2] * a.isz;
+            float nrm = nan_canon(sqrtf(x * x + y * y + zz * zz));
             sum += (double)nrm;
             mx = __int_as_float(max(__float_as_int(mx), __float_as_int(nrm)));
+            px = qx;
+            py = qy;
+            pz = qz;
         }
     }
     const double count = (double)a.g.n;
@@ -271,9 +299,22 @@ static InvArgs inv_args(const fw_field* field, const fw_field* inverse) {
     return a;
 }
 
+// The body streams psi and the residual (a flat grid-stride sweep, two voxels a step); only when
+// the loop goes on does it gather, and the measurement -- a gather of every voxel -- runs over
+// 32 x 8 column tiles marching along z (z chunks so that the grid fills the GPU a few blocks
+// deep per SM).
 static unsigned int inv_blocks(fw_ctx* ctx, long long n) {
     long long b = (n + 255) / 256;
     return (unsigned int)std::max<long long>(1, std::min<long long>(b, 8LL * ctx->num_sms));
+}
+
+static dim3 inv_grid(fw_ctx* ctx, InvArgs& a) {
+    dim3 g((a.g.nx + 31) / 32, (a.g.ny + 7) / 8, 1);
+    const long long tiles = (long long)g.x * g.y;
+    const long long want = std::max<long long>(1, (6LL * ctx->num_sms + tiles - 1) / tiles);
+    a.zchunk = (int)std::max<long long>(1, (a.g.nz + want - 1) / want);
+    g.z = (unsigned int)((a.g.nz + a.zchunk - 1) / a.zchunk);
+    return g;
 }
 
 // Launches the whole inversion on the stream: init, first measurement and `bodies` body kernels
@@ -284,8 +325,11 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
     FW_CHECK(res->grid.same(inverse->grid) && res->ps == inverse->ps,
              "invert: the residual buffer does not match the inverse");
     InvArgs a = inv_args(field, inverse);
-    unsigned int blocks = inv_blocks(ctx, a.g.n);
-    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 2 * (size_t)blocks + 16));
+    const dim3 blocks = inv_grid(ctx, a);
+    // block partials of the measurement's tiles and of the bodies' flat grid
+    const size_t parts = std::max<size_t>((size_t)blocks.x * blocks.y * blocks.z,
+                                          inv_blocks(ctx, a.g.n));
+    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 2 * parts + 16));
     k_inv_init<<<1, 1, 0, ctx->stream>>>(st, prm);
     FW_TRY(check_launch(ctx, "k_inv_init"));
     k_inv_measure<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
@@ -297,7 +341,7 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
 int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
                            InvState* st, cudaGraphConditionalHandle handle, int use_handle) {
     InvArgs a = inv_args(field, inverse);
-    unsigned int blocks = inv_blocks(ctx, a.g.n);
+    const unsigned int blocks = inv_blocks(ctx, a.g.n);
     k_inv_body<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
                                                 ctx->d_scratch + SLOT_PARTIALS,
                                                 ctx->d_counter + 2, st, handle, use_handle);
