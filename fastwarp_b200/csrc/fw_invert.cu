@@ -27,26 +27,6 @@ struct InvArgs {
     int zchunk;  // slices a thread marches through
 };
 
-// Thread mapping of the sweeps: a block is a 32 x 8 tile of (x, y) columns and each thread marches
-// along z through `zchunk` slices. The trilinear gathers of neighbouring columns and of
-// consecutive slices fall on the same rows of the field, so they meet in L1 instead of each
-// crossing from L2 (the gathers' bound); the next slice's own values are loaded while the current
-// slice gathers.
-struct Column {
-    int x, y, z0, z1;
-    bool own;
-};
-
-__device__ __forceinline__ Column column_of(const InvArgs& a) {
-    Column c;
-    c.x = blockIdx.x * 32 + (threadIdx.x & 31);
-    c.y = blockIdx.y * 8 + (threadIdx.x >> 5);
-    c.z0 = blockIdx.z * a.zchunk;
-    c.z1 = min(c.z0 + a.zchunk, a.g.nz);
-    c.own = c.x < a.g.nx && c.y < a.g.ny;
-    return c;
-}
-
 __device__ __forceinline__ void residual(const InvArgs& a, const float* __restrict__ f,
                                          long long l, int i, int j, int k, float px, float py,
                                          float pz, float e[3]) {
@@ -126,8 +106,10 @@ __global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __r
                                                      int use_handle) {
     double sum = 0.0;
     float mx = 0.0f;
-    const Column col = column_of(a);
-    if (col.own && col.z0 < col.z1) {
+    struct {
+        int x, y, z0, z1;
+    } col;
+    if (column_of(a.g.nx, a.g.ny, a.g.nz, a.zchunk, col.x, col.y, col.z0, col.z1)) {
         const long long sxy = (long long)a.g.nx * a.g.ny;
         long long l = (long long)col.z0 * sxy + (long long)col.y * a.g.nx + col.x;
         float px = psi[l], py = psi[l + a.ps_psi], pz = psi[l + 2 * a.ps_psi];
@@ -309,12 +291,7 @@ static unsigned int inv_blocks(fw_ctx* ctx, long long n) {
 }
 
 static dim3 inv_grid(fw_ctx* ctx, InvArgs& a) {
-    dim3 g((a.g.nx + 31) / 32, (a.g.ny + 7) / 8, 1);
-    const long long tiles = (long long)g.x * g.y;
-    const long long want = std::max<long long>(1, (6LL * ctx->num_sms + tiles - 1) / tiles);
-    a.zchunk = (int)std::max<long long>(1, (a.g.nz + want - 1) / want);
-    g.z = (unsigned int)((a.g.nz + a.zchunk - 1) / a.zchunk);
-    return g;
+    return column_grid(a.g.nx, a.g.ny, a.g.nz, ctx->num_sms, &a.zchunk);
 }
 
 // Launches the whole inversion on the stream: init, first measurement and `bodies` body kernels

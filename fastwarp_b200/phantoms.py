@@ -106,12 +106,13 @@ def head_phantom(shape_xyz=(193, 229, 193), seed: int = BASE_SEED + 2):
     return img.astype(np.float32)
 
 
-def head_pair(shape_xyz=(193, 229, 193), seed: int = BASE_SEED + 2):
-    """Config 2: (grid, fixed, moving_grid, moving, initial affine)."""
+def head_pair(shape_xyz=(193, 229, 193), seed: int = BASE_SEED + 2, spacing: float = 1.0):
+    """Config 2: (grid, fixed, moving_grid, moving, initial affine). With spacing 0.5 and twice
+    the shape, config 3: the same head geometry sampled finer, with fresh noise per voxel."""
     rng = np.random.default_rng(seed + 1000)
     fixed = head_phantom(shape_xyz, seed)
     nx, ny, nz = shape_xyz
-    grid = make_grid(shape_xyz)
+    grid = make_grid(shape_xyz, (spacing,) * 3)
     centre = np.array([(nx - 1) / 2.0, (ny - 1) / 2.0, (nz - 1) / 2.0])
     rot = _rot(*np.deg2rad(rng.uniform(-10.0, 10.0, size=3)))
     trans = rng.uniform(-15.0, 15.0, size=3)
@@ -135,5 +136,6 @@ def head_pair(shape_xyz=(193, 229, 193), seed: int = BASE_SEED + 2):
     uz = _warp(u[0], coords)
     moving = _warp(fixed.astype(np.float64), np.stack([qz + uz, qy + uy, qx + ux]))
     moving = np.clip(moving, 0.0, None).astype(np.float32)
-    initial = make_affine(lin, offset)
+    # index-space map -> physical: isotropic spacing scales the offset only
+    initial = make_affine(lin, offset * spacing)
     return grid, fixed, grid, moving, initial
