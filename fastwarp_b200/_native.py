@@ -59,6 +59,28 @@ class LinearTransform(C.Structure):
                 ("parameters", C.c_double * 12), ("center", C.c_double * 3)]
 
 
+class CgSettings(C.Structure):
+    _fields_ = [("max_step_mm", C.c_double), ("lower_limit", C.c_double),
+                ("upper_limit", C.c_double), ("epsilon", C.c_double),
+                ("max_line_search_iterations", C.c_int32), ("iterations", C.c_int32),
+                ("convergence_threshold", C.c_double), ("convergence_window", C.c_int32),
+                ("small_parameter_variation", C.c_double)]
+
+
+class CgTrace(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32),
+                ("converged_value", C.c_double), ("best_value", C.c_double),
+                ("initial_learning_rate", C.c_double), ("final_learning_rate", C.c_double),
+                ("line_search_evaluations", C.c_uint64), ("scales", C.c_double * 12),
+                ("nvalues", C.c_int64)]
+
+
+METRIC_VALUE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform),
+                              C.POINTER(C.c_double))
+METRIC_VALUE_DERIVATIVE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double))
+
+
 class SynRecipe(C.Structure):
     _fields_ = [("gradient_step", C.c_double), ("update_field_variance", C.c_double),
                 ("total_field_variance", C.c_double), ("cc_radius", C.c_int32),

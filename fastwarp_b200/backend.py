@@ -464,3 +464,81 @@ class CudaLinearEngine:
                                         _ptr(fb), C.c_int64(p.shape[0]), C.byref(binning),
                                         C.byref(h)))
         return MiLevel(self.backend, h)
+
+
+# ---- the linear-stage optimiser (optimizer.rs:60-435) --------------------------------------------
+
+def cg_settings_ants(max_step_mm=0.1, iterations=100, threshold=1e-6, window=10) -> N.CgSettings:
+    """CgSettings::ants (optimizer.rs:94-106)."""
+    s = N.CgSettings()
+    lib().fw_cg_settings_ants(C.c_double(max_step_mm), C.c_int32(iterations),
+                              C.c_double(threshold), C.c_int32(window), C.byref(s))
+    return s
+
+
+def grid_corners(grid: N.Grid) -> np.ndarray:
+    """corner_points (optimizer.rs:142-166): (8, 3) physical corner points."""
+    out = (C.c_double * 24)()
+    check(lib().fw_grid_corners(C.byref(grid), out))
+    return np.array(out[:]).reshape(8, 3)
+
+
+def _trace(tr: N.CgTrace, values, n_params) -> dict:
+    return {"iterations": tr.iterations, "converged": bool(tr.converged),
+            "converged_value": None if np.isnan(tr.converged_value) else tr.converged_value,
+            "best_value": tr.best_value, "initial_learning_rate": tr.initial_learning_rate,
+            "final_learning_rate": tr.final_learning_rate,
+            "line_search_evaluations": tr.line_search_evaluations,
+            "scales": list(tr.scales[:n_params]), "values": list(values[:min(tr.nvalues, len(values))])}
+
+
+def optimize_level(value, value_and_derivative, corners, transform: N.LinearTransform,
+                   settings: N.CgSettings, cap: int = 100000):
+    """optimise_level (optimizer.rs:311-435) over a Python metric: `value(t) -> float` and
+    `value_and_derivative(t) -> (float, derivative)`. Returns (best transform, trace)."""
+    nparams = 6 if transform.kind == 0 else 12
+    err = []
+
+    def v_cb(user, t, out):
+        try:
+            out[0] = float(value(t.contents))
+            return 0
+        except Exception as e:  # reported through the optimiser's error
+            err.append(e)
+            return -1
+
+    def vd_cb(user, t, out, d):
+        try:
+            val, der = value_and_derivative(t.contents)
+            out[0] = float(val)
+            for i in range(nparams):
+                d[i] = float(der[i])
+            return 0
+        except Exception as e:
+            err.append(e)
+            return -1
+
+    c = (C.c_double * 24)(*np.asarray(corners, np.float64).ravel())
+    t = N.LinearTransform.from_buffer_copy(transform)
+    tr = N.CgTrace()
+    vals = (C.c_double * cap)()
+    f1, f2 = N.METRIC_VALUE_FN(v_cb), N.METRIC_VALUE_DERIVATIVE_FN(vd_cb)
+    rc = lib().fw_cg_optimize_level(C.byref(settings), c, C.byref(t), f1, f2, None,
+                                    C.byref(tr), vals, C.c_int64(cap), None)
+    if err:
+        raise err[0]
+    check(rc)
+    return t, _trace(tr, vals, nparams)
+
+
+def mi_level_optimize(level, corners, transform: N.LinearTransform, settings: N.CgSettings,
+                      cap: int = 100000):
+    """The optimiser on a device MI level (fw_mi_level_optimize)."""
+    nparams = 6 if transform.kind == 0 else 12
+    c = (C.c_double * 24)(*np.asarray(corners, np.float64).ravel())
+    t = N.LinearTransform.from_buffer_copy(transform)
+    tr = N.CgTrace()
+    vals = (C.c_double * cap)()
+    check(lib().fw_mi_level_optimize(level.handle, C.byref(settings), c, C.byref(t), C.byref(tr),
+                                     vals, C.c_int64(cap)))
+    return t, _trace(tr, vals, nparams)

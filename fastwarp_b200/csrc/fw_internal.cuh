@@ -416,6 +416,9 @@ int dense_mi_status(int status, bool masked);
 int enqueue_field_download_f32(fw_ctx* ctx, const fw_field* field, float* host);
 int enqueue_image_upload_f32(fw_ctx* ctx, const HostGrid& g, const float* host, fw_image** out);
 
+// transform/param.rs:421-446: outer(optimised(p)) as one affine map y = M p + off (fw_mi.cu).
+void linear_transform_map(const fw_linear_transform* t, double M[9], double off[3]);
+
 // The SyN stage on device images (fw_syn.cu); masks may be null.
 int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
                    const fw_image* const* moving, const fw_image* fixed_mask,

@@ -852,6 +852,12 @@ void fw_mi_level_free(fw_mi_level* L) {
 
 }  // extern "C"
 
+namespace fw {
+void linear_transform_map(const fw_linear_transform* t, double M[9], double off[3]) {
+    linear_map(t, M, off);
+}
+}  // namespace fw
+
 // ---- dense Mattes MI pair: host side -----------------------------------------------------------
 
 namespace fw {

@@ -66,6 +66,8 @@ struct Job {
     fw_syn_request req{};
     std::vector<float*> fixed_host, moving_host;  // pinned staging of host inputs
     size_t fixed_bytes = 0, moving_bytes = 0;
+    float* mask_host[2] = {nullptr, nullptr};     // pinned staging of host masks
+    size_t mask_bytes[2] = {0, 0};
     std::vector<const fw_image*> fixed_dev, moving_dev;
     uint64_t bytes = 0;
     Clock::time_point submitted;
@@ -105,6 +107,14 @@ int estimate(const fw_syn_request* q, uint64_t* out) {
     b += 12 * ps * (uint64_t)fields;
     b += 4 * (uint64_t)n * 2 * C;                      // warped images
     b += 12 * psp * 4;                                 // state of the previous level at a transition
+    const fw_grid* mg_[2] = {&q->fixed_mask_grid, &q->moving_mask_grid};
+    const bool mask_[2] = {q->fixed_mask || q->fixed_mask_dev, q->moving_mask || q->moving_mask_dev};
+    for (int k = 0; k < 2; ++k) {
+        if (!mask_[k]) continue;
+        b += 4 * (uint64_t)n * 2;                      // resolved on the level grid (+ product)
+        if (k == 0 ? q->fixed_mask != nullptr : q->moving_mask != nullptr)
+            b += 4 * (uint64_t)(mg_[k]->size[0] * mg_[k]->size[1] * mg_[k]->size[2]);  // upload
+    }
     b += 2u << 20;                                     // records and scalars
     *out = b;
     return 0;
@@ -165,13 +175,27 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
             mi[c] = b;
         }
     }
+    // the recipe's masks: device images as given, host data uploaded from the pinned staging
+    const fw_image* masks[2] = {q.fixed_mask_dev, q.moving_mask_dev};
+    const fw_grid* mgrids[2] = {&q.fixed_mask_grid, &q.moving_mask_grid};
+    for (int k = 0; k < 2 && !rc; ++k) {
+        if (!j->mask_host[k]) continue;
+        HostGrid mgk;
+        rc = make_grid(mgrids[k], mgk);
+        fw_image* im = nullptr;
+        if (!rc) rc = enqueue_image_upload_f32(ctx, mgk, j->mask_host[k], &im);
+        if (!rc) {
+            up.push_back(im);
+            masks[k] = im;
+        }
+    }
     int64_t cap = 0;
     for (int l = 0; l < q.recipe.levels; ++l) cap += q.recipe.iterations[l];
     std::vector<fw_syn_iteration> recs((size_t)std::max<int64_t>(cap, 1));
     int64_t count = 0;
     fw_field *w = nullptr, *iw = nullptr;
     if (!rc)
-        rc = syn_run_device(ctx, &q.recipe, fi.data(), mi.data(), nullptr, nullptr,
+        rc = syn_run_device(ctx, &q.recipe, fi.data(), mi.data(), masks[0], masks[1],
                             q.has_initial ? &q.initial : nullptr,
                             &w, &iw, recs.data(), (int64_t)recs.size(), &count);
     for (auto* im : up) fw_image_free(im);
@@ -202,6 +226,10 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
     for (auto* p : j->moving_host) pinned().put(p, j->moving_bytes);
     j->fixed_host.clear();
     j->moving_host.clear();
+    for (int k = 0; k < 2; ++k) {
+        pinned().put(j->mask_host[k], j->mask_bytes[k]);
+        j->mask_host[k] = nullptr;
+    }
     {
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->epoch_set) {
@@ -312,6 +340,8 @@ int fw_server_submit(fw_server* s, const fw_syn_request* req, uint64_t* ticket) 
     bool host = req->fixed && req->moving;
     bool dev = req->fixed_dev && req->moving_dev;
     FW_CHECK(host != dev, "serve: give either host or device images");
+    FW_CHECK(!(req->fixed_mask && req->fixed_mask_dev) && !(req->moving_mask && req->moving_mask_dev),
+             "serve: give a mask either as host data or as a device image");
     uint64_t bytes = 0;
     FW_TRY(estimate(req, &bytes));
     if (bytes > s->budget)
@@ -351,8 +381,29 @@ int fw_server_submit(fw_server* s, const fw_syn_request* req, uint64_t* ticket) 
             j->moving_dev.push_back(req->moving_dev[c]);
         }
     }
+    const float* mask_src[2] = {req->fixed_mask, req->moving_mask};
+    const fw_grid* mask_grid[2] = {&req->fixed_mask_grid, &req->moving_mask_grid};
+    for (int k = 0; k < 2; ++k) {
+        if (!mask_src[k]) continue;
+        HostGrid mgk;
+        int mrc = make_grid(mask_grid[k], mgk);
+        if (!mrc) {
+            j->mask_bytes[k] = sizeof(float) * (size_t)mgk.count();
+            j->mask_host[k] = static_cast<float*>(pinned().get(j->mask_bytes[k]));
+            if (!j->mask_host[k]) mrc = fail(FW_ERR_MEMORY, "serve: pinned host staging allocation failed");
+        }
+        if (mrc) {
+            for (auto* p : j->fixed_host) pinned().put(p, j->fixed_bytes);
+            for (auto* p : j->moving_host) pinned().put(p, j->moving_bytes);
+            for (int q = 0; q < 2; ++q) pinned().put(j->mask_host[q], j->mask_bytes[q]);
+            delete j;
+            return mrc;
+        }
+        std::memcpy(j->mask_host[k], mask_src[k], j->mask_bytes[k]);
+    }
     j->req.fixed = j->req.moving = nullptr;
     j->req.fixed_dev = j->req.moving_dev = nullptr;
+    j->req.fixed_mask = j->req.moving_mask = nullptr;
     j->submitted = Clock::now();
     {
         std::lock_guard<std::mutex> lock(s->mu);

@@ -20,7 +20,10 @@ class SynRequest(C.Structure):
     _fields_ = [("recipe", N.SynRecipe), ("fixed_grid", N.Grid), ("moving_grid", N.Grid),
                 ("fixed", C.c_void_p), ("moving", C.c_void_p), ("fixed_dev", C.c_void_p),
                 ("moving_dev", C.c_void_p), ("initial", N.Affine), ("has_initial", C.c_int32),
-                ("keep_on_device", C.c_int32), ("tag", C.c_uint64)]
+                ("keep_on_device", C.c_int32), ("tag", C.c_uint64),
+                ("fixed_mask_grid", N.Grid), ("moving_mask_grid", N.Grid),
+                ("fixed_mask", C.c_void_p), ("moving_mask", C.c_void_p),
+                ("fixed_mask_dev", C.c_void_p), ("moving_mask_dev", C.c_void_p)]
 
 
 class _ResultBuffers:
@@ -77,7 +80,7 @@ class Server:
         self.close()
 
     def _request(self, recipe: SynRecipe, fixed_grid, fixed, moving_grid, moving, initial, tag,
-                 keep_on_device):
+                 keep_on_device, fixed_mask=None, moving_mask=None):
         q = SynRequest()
         q.recipe = recipe.to_c()
         q.fixed_grid = fixed_grid
@@ -102,6 +105,20 @@ class Server:
             q.has_initial = 1
         q.keep_on_device = int(bool(keep_on_device))
         q.tag = int(tag)
+        # masks: a device Image, or (grid, host array) copied at submit
+        for name, m in (("fixed", fixed_mask), ("moving", moving_mask)):
+            if m is None:
+                continue
+            if isinstance(m, Image):
+                setattr(q, name + "_mask_grid", m.grid)
+                setattr(q, name + "_mask_dev", m.handle.value)
+                keep.append(m)
+            else:
+                grid, data = m
+                arr = np.ascontiguousarray(data, np.float32)
+                setattr(q, name + "_mask_grid", grid)
+                setattr(q, name + "_mask", arr.ctypes.data)
+                keep.append(arr)
         return q, keep
 
     def estimate(self, recipe, fixed_grid, fixed, moving_grid, moving, initial=None) -> int:
@@ -111,15 +128,15 @@ class Server:
         return int(b.value)
 
     def submit(self, recipe: SynRecipe, fixed_grid, fixed, moving_grid, moving, initial=None,
-               tag=0, keep_on_device=False) -> int:
+               tag=0, keep_on_device=False, fixed_mask=None, moving_mask=None) -> int:
         """Queues one SyN registration; `fixed`/`moving` are lists (one per channel) of host
-        float arrays or of device `Image`s. Returns the ticket."""
+        float arrays or of device `Image`s; masks are a device `Image` or (grid, host array).
+        Returns the ticket."""
         q, keep = self._request(recipe, fixed_grid, fixed, moving_grid, moving, initial, tag,
-                                keep_on_device)
+                                keep_on_device, fixed_mask, moving_mask)
         t = C.c_uint64()
         check(lib().fw_server_submit(self.handle, C.byref(q), C.byref(t)))
-        if isinstance(fixed[0], Image):
-            self._keep[int(t.value)] = keep  # device images must outlive the request
+        self._keep[int(t.value)] = keep  # device images must outlive the request
         return int(t.value)
 
     def wait(self, ticket: int, timeout: float = -1.0) -> dict:

@@ -410,6 +410,63 @@ int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_gr
                const fw_affine* initial, float* warp, float* inverse_warp,
                fw_syn_iteration* records, int64_t cap, int64_t* count);
 
+/* ---- linear-stage optimiser (optimizer.rs:60-435) ---------------------------------------- */
+
+/* CgSettings, optimizer.rs:67-106 (fw_cg_settings_ants: the antsRegistration settings). */
+typedef struct fw_cg_settings {
+    double max_step_mm;            /* MaximumStepSizeInPhysicalUnits, the first learning rate */
+    double lower_limit, upper_limit;  /* the line search's bracket, times the learning rate */
+    double epsilon;                /* relative width at which the line search stops */
+    int32_t max_line_search_iterations;
+    int32_t iterations;            /* iterations of the level */
+    double convergence_threshold;
+    int32_t convergence_window;
+    double small_parameter_variation;  /* of the scale estimator */
+} fw_cg_settings;
+
+/* CgTrace, optimizer.rs:108-140. */
+typedef struct fw_cg_trace {
+    int32_t iterations;            /* steps taken */
+    int32_t converged;             /* the monitor ended the level before its limit */
+    double converged_value;        /* the value the monitor stopped on (NaN if none) */
+    double best_value;
+    double initial_learning_rate;
+    double final_learning_rate;
+    uint64_t line_search_evaluations;
+    double scales[12];             /* parameter scales of the level */
+    int64_t nvalues;               /* values written (all of them, even past `cap`) */
+} fw_cg_trace;
+
+/* The metric the optimiser drives (trait LinearMetric, optimizer.rs:56-65): return 0, or a
+ * non-zero status with the message in fw_last_error(). `derivative` has 6 (Euler) or 12
+ * (affine) entries in ITK's sign: the direction that decreases the value. */
+typedef int (*fw_metric_value_fn)(void* user, const fw_linear_transform* t, double* value);
+typedef int (*fw_metric_value_derivative_fn)(void* user, const fw_linear_transform* t,
+                                             double* value, double* derivative);
+
+void fw_cg_settings_ants(double max_step_mm, int32_t iterations, double threshold,
+                         int32_t window, fw_cg_settings* out);
+/* corner_points (optimizer.rs:142-166): the 8 corner points (x, y, z mm) of a grid. */
+int fw_grid_corners(const fw_grid* grid, double corners[24]);
+/* estimate_scales / estimate_step_scale (optimizer.rs:185-231). */
+int fw_linear_estimate_scales(const double corners[24], const fw_linear_transform* t,
+                              double small_variation, double* scales);
+int fw_linear_estimate_step_scale(const double corners[24], const fw_linear_transform* t,
+                                  const double* step, double small_variation, double* out);
+/* optimise_level (optimizer.rs:311-435): ITK's conjugate-gradient optimiser with a golden-
+ * section line search over `transform`'s parameters from its current values; on return it holds
+ * the best transform. `values` (may be NULL) receives the value of every iteration that stepped,
+ * up to `cap`. `cancel` (may be NULL) is polled before every iteration. */
+int fw_cg_optimize_level(const fw_cg_settings* settings, const double corners[24],
+                         fw_linear_transform* transform, fw_metric_value_fn value,
+                         fw_metric_value_derivative_fn value_derivative, void* user,
+                         fw_cg_trace* trace, double* values, int64_t cap,
+                         const volatile int32_t* cancel);
+/* The same on a device MI level (fw_mi_level_value / _value_and_derivative). */
+int fw_mi_level_optimize(fw_mi_level* level, const fw_cg_settings* settings,
+                         const double corners[24], fw_linear_transform* transform,
+                         fw_cg_trace* trace, double* values, int64_t cap);
+
 /* ---- profiling (crates/fastwarp-gpu/src/profiler.rs:8-60: per-op device timestamps) ----- */
 
 /* Times `reps` launches of each kernel of one SyN iteration on the grid of `fixed` with CUDA

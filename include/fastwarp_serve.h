@@ -35,6 +35,15 @@ typedef struct fw_syn_request {
     int32_t has_initial;
     int32_t keep_on_device;  /* 1: the fields stay on the device (warp_dev / inverse_dev) */
     uint64_t tag;
+    /* The recipe's masks (recipe.rs fixed_mask / moving_mask), each on its own grid: host float32
+     * data (copied at submit) or a device image (kept valid until the result is taken); both
+     * NULL when the mask is not given. */
+    fw_grid fixed_mask_grid;
+    fw_grid moving_mask_grid;
+    const float* fixed_mask;
+    const float* moving_mask;
+    const fw_image* fixed_mask_dev;
+    const fw_image* moving_mask_dev;
 } fw_syn_request;
 
 typedef struct fw_syn_result {

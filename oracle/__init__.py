@@ -482,3 +482,80 @@ def mi_dense(fgrid, fixed, mgrid, moving, field, bins, fmask_grid=None, fmask=No
                               None if mmask_grid is None else C.byref(mmask_grid), _p(mmask),
                               C.c_int32(bins), C.byref(value), C.byref(nv), _p(deriv)))
     return value.value, nv.value, deriv
+
+
+# ---- the linear-stage optimiser (optimizer.rs:60-435) -------------------------------------------
+
+class CgSettings(C.Structure):
+    _fields_ = [("max_step_mm", C.c_double), ("lower_limit", C.c_double),
+                ("upper_limit", C.c_double), ("epsilon", C.c_double),
+                ("max_line_search_iterations", C.c_int32), ("iterations", C.c_int32),
+                ("convergence_threshold", C.c_double), ("convergence_window", C.c_int32),
+                ("small_parameter_variation", C.c_double)]
+
+
+class CgTrace(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32),
+                ("converged_value", C.c_double), ("best_value", C.c_double),
+                ("initial_learning_rate", C.c_double), ("final_learning_rate", C.c_double),
+                ("line_search_evaluations", C.c_uint64), ("scales", C.c_double * 12),
+                ("nvalues", C.c_int64)]
+
+
+_VALUE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform), C.POINTER(C.c_double))
+_VD_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform), C.POINTER(C.c_double),
+                     C.POINTER(C.c_double))
+
+
+def cg_settings_ants(max_step_mm=0.1, iterations=100, threshold=1e-6, window=10):
+    """CgSettings::ants (optimizer.rs:94-106)."""
+    s = CgSettings()
+    s.max_step_mm, s.lower_limit, s.upper_limit, s.epsilon = max_step_mm, 0.0, 2.0, 0.2
+    s.max_line_search_iterations, s.iterations = 20, iterations
+    s.convergence_threshold, s.convergence_window = threshold, window
+    s.small_parameter_variation = 0.01
+    return s
+
+
+def estimate_scales(corners, t, small=0.01):
+    n = 6 if t.kind == 0 else 12
+    out = (C.c_double * 12)()
+    c = (C.c_double * 24)(*np.asarray(corners, np.float64).ravel())
+    _check(lib().fwo_estimate_scales(c, C.byref(t), C.c_double(small), out))
+    return list(out[:n])
+
+
+def estimate_step_scale(corners, t, step, small=0.01):
+    c = (C.c_double * 24)(*np.asarray(corners, np.float64).ravel())
+    s = (C.c_double * 12)(*list(step))
+    lib().fwo_estimate_step_scale.restype = C.c_double
+    return lib().fwo_estimate_step_scale(c, C.byref(t), s, C.c_double(small))
+
+
+def cg_optimize_level(value, value_and_derivative, corners, t, settings, cap=100000):
+    """optimise_level over Python callables; returns (best transform, trace dict)."""
+    n = 6 if t.kind == 0 else 12
+
+    def v_cb(user, tt, out):
+        out[0] = float(value(tt.contents))
+        return 0
+
+    def vd_cb(user, tt, out, d):
+        v, der = value_and_derivative(tt.contents)
+        out[0] = float(v)
+        for i in range(n):
+            d[i] = float(der[i])
+        return 0
+
+    c = (C.c_double * 24)(*np.asarray(corners, np.float64).ravel())
+    tt = LinearTransform.from_buffer_copy(t)
+    tr = CgTrace()
+    vals = (C.c_double * cap)()
+    f1, f2 = _VALUE_FN(v_cb), _VD_FN(vd_cb)
+    _check(lib().fwo_cg_optimize_level(C.byref(settings), c, C.byref(tt), f1, f2, None,
+                                       C.byref(tr), vals, C.c_int64(cap)))
+    return tt, {"iterations": tr.iterations, "converged": bool(tr.converged),
+                "best_value": tr.best_value, "initial_learning_rate": tr.initial_learning_rate,
+                "final_learning_rate": tr.final_learning_rate,
+                "line_search_evaluations": tr.line_search_evaluations,
+                "scales": list(tr.scales[:n]), "values": list(vals[:min(tr.nvalues, cap)])}

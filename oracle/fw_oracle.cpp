@@ -1882,3 +1882,183 @@ int fwo_syn_run_masked(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
 }
 
 }  // extern "C"
+
+// ---- the linear-stage optimiser, crates/fastwarp-reg/src/optimizer.rs:142-435 -------------------
+
+namespace {
+
+int opt_nparams(const fwo_linear_transform& t) { return t.kind == 0 ? 6 : 12; }
+
+void opt_apply(const fwo_linear_transform& t, const double* p, double* out) {
+    fwo_affine a;
+    linear_map(&t, &a);
+    for (int r = 0; r < 3; ++r)
+        out[r] = a.matrix[r * 3] * p[0] + a.matrix[r * 3 + 1] * p[1] + a.matrix[r * 3 + 2] * p[2] +
+                 a.offset[r];
+}
+
+// optimizer.rs:168-183: the largest corner displacement caused by adding `delta`.
+double opt_shift(const double* corners, const fwo_linear_transform& t, const double* delta) {
+    fwo_linear_transform m = t;
+    for (int i = 0; i < opt_nparams(t); ++i) m.parameters[i] += delta[i];
+    double best = 0.0;
+    for (int c = 0; c < 8; ++c) {
+        double a[3], b[3];
+        opt_apply(m, corners + 3 * c, a);
+        opt_apply(t, corners + 3 * c, b);
+        double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+        best = std::max(best, std::sqrt(dx * dx + dy * dy + dz * dz));
+    }
+    return best;
+}
+
+}  // namespace
+
+extern "C" {
+
+// optimizer.rs:185-216
+int fwo_estimate_scales(const double* corners, const fwo_linear_transform* t, double small,
+                        double* scales) {
+    const int n = opt_nparams(*t);
+    double lo = DBL_MAX;
+    for (int i = 0; i < n; ++i) {
+        double d[12] = {0};
+        d[i] = small;
+        scales[i] = opt_shift(corners, *t, d);
+        if (scales[i] > DBL_EPSILON && scales[i] < lo) lo = scales[i];
+    }
+    if (lo == DBL_MAX) {
+        for (int i = 0; i < n; ++i) scales[i] = 1.0;
+        return 0;
+    }
+    for (int i = 0; i < n; ++i) {
+        scales[i] = scales[i] <= DBL_EPSILON ? lo * lo : scales[i] * scales[i];
+        scales[i] *= 1.0 / (small * small);
+    }
+    return 0;
+}
+
+// optimizer.rs:218-231
+double fwo_estimate_step_scale(const double* corners, const fwo_linear_transform* t,
+                               const double* step, double small) {
+    const int n = opt_nparams(*t);
+    double mx = 0.0;
+    for (int i = 0; i < n; ++i) mx = std::max(mx, std::fabs(step[i]));
+    if (mx <= DBL_EPSILON) return 0.0;
+    const double f = small / mx;
+    double s[12];
+    for (int i = 0; i < n; ++i) s[i] = step[i] * f;
+    return opt_shift(corners, *t, s) / f;
+}
+
+// optimizer.rs:236-309 (golden-section search) and :311-435 (the conjugate-gradient loop).
+int fwo_cg_optimize_level(const fwo_cg_settings* st, const double* corners,
+                          fwo_linear_transform* t, fwo_metric_value_fn value,
+                          fwo_metric_value_derivative_fn value_derivative, void* user,
+                          fwo_cg_trace* trace, double* values, int64_t cap) {
+    const int n = opt_nparams(*t);
+    const double resphi = 2.0 - 1.618034;
+    double scales[12];
+    fwo_estimate_scales(corners, t, st->small_parameter_variation, scales);
+    fwo_linear_transform cur = *t, best = *t;
+    double conj[12] = {0}, last[12] = {0}, g[12];
+    double lr = st->max_step_mm;
+    std::vector<double> window;
+    double total = 0.0;
+    double best_value = DBL_MAX;
+    *trace = fwo_cg_trace{};
+    trace->converged_value = std::numeric_limits<double>::quiet_NaN();
+    for (int i = 0; i < n; ++i) trace->scales[i] = scales[i];
+    trace->initial_learning_rate = lr;
+    int it = 0;
+    while (it < st->iterations) {
+        double v;
+        if (value_derivative(user, &cur, &v, g)) return fail("the metric failed");
+        window.push_back(v);
+        if ((int)window.size() > st->convergence_window) window.erase(window.begin());
+        total += std::fabs(v);
+        const double cv = fwo_convergence_value(window.data(), (int64_t)window.size(),
+                                                st->convergence_window, total);
+        if (cv <= st->convergence_threshold) {
+            trace->converged = 1;
+            trace->converged_value = v;
+            break;
+        }
+        if (values && trace->nvalues < cap) values[trace->nvalues] = v;
+        trace->nvalues++;
+        for (int i = 0; i < n; ++i) g[i] *= 1.0 / scales[i];
+        if (it == 0) {
+            const double ss = fwo_estimate_step_scale(corners, &cur, g, st->small_parameter_variation);
+            lr = ss <= DBL_EPSILON ? 1.0 : st->max_step_mm / ss;
+            trace->initial_learning_rate = lr;
+        }
+        double gamma = 0.0, den = 0.0;
+        for (int i = 0; i < n; ++i) den += last[i] * last[i];
+        if (den > DBL_EPSILON) {
+            double num = 0.0;
+            for (int i = 0; i < n; ++i) num += (g[i] - last[i]) * g[i];
+            gamma = num / den;
+        }
+        if (!(gamma >= 0.0 && gamma <= 5.0)) gamma = 0.0;
+        for (int i = 0; i < n; ++i) {
+            last[i] = g[i];
+            conj[i] = g[i] + conj[i] * gamma;
+        }
+        // golden-section search over [lower, 1, upper] * lr
+        double a = lr * st->lower_limit, b = lr, c = lr * st->upper_limit;
+        double mb = DBL_MAX;
+        int lsi = 0;
+        auto at = [&](double step, double* out) {
+            trace->line_search_evaluations++;
+            fwo_linear_transform q = cur;
+            for (int i = 0; i < n; ++i) q.parameters[i] = cur.parameters[i] + step * conj[i];
+            return value(user, &q, out);
+        };
+        for (;;) {
+            if (lsi > st->max_line_search_iterations) {
+                lr = (c + a) / 2.0;
+                break;
+            }
+            ++lsi;
+            const double x = c - b > b - a ? b + resphi * (c - b) : b - resphi * (b - a);
+            if (std::fabs(c - a) < st->epsilon * (std::fabs(b) + std::fabs(x))) {
+                lr = (c + a) / 2.0;
+                break;
+            }
+            double mx;
+            if (at(x, &mx)) return fail("the metric failed");
+            if (mb == DBL_MAX && at(b, &mb)) return fail("the metric failed");
+            if (mx < mb) {
+                if (c - b > b - a) {
+                    a = b;
+                    b = x;
+                } else {
+                    c = b;
+                    b = x;
+                }
+                mb = mx;
+            } else if (c - b > b - a) {
+                c = x;
+            } else if (mx == DBL_MAX) {
+                c = b;
+                b = x;
+                mb = mx;
+            } else {
+                a = x;
+            }
+        }
+        for (int i = 0; i < n; ++i) cur.parameters[i] += lr * conj[i];
+        if (v < best_value) {
+            best_value = v;
+            best = cur;
+        }
+        ++it;
+    }
+    trace->iterations = it;
+    trace->best_value = best_value;
+    trace->final_learning_rate = lr;
+    *t = best;
+    return 0;
+}
+
+}  // extern "C"

@@ -175,6 +175,38 @@ int fwo_mi_dense(const fwo_grid* fgrid, const double* fixed, const fwo_grid* mgr
                  const double* fmask, const fwo_grid* mmask_grid, const double* mmask,
                  int32_t bins, double* value, int64_t* num_valid, double* derivative);
 
+/* the linear-stage optimiser, crates/fastwarp-reg/src/optimizer.rs:60-435 */
+typedef struct fwo_cg_settings {
+    double max_step_mm, lower_limit, upper_limit, epsilon;
+    int32_t max_line_search_iterations;
+    int32_t iterations;
+    double convergence_threshold;
+    int32_t convergence_window;
+    double small_parameter_variation;
+} fwo_cg_settings;
+typedef struct fwo_cg_trace {
+    int32_t iterations;
+    int32_t converged;
+    double converged_value;
+    double best_value;
+    double initial_learning_rate;
+    double final_learning_rate;
+    uint64_t line_search_evaluations;
+    double scales[12];
+    int64_t nvalues;
+} fwo_cg_trace;
+typedef int (*fwo_metric_value_fn)(void* user, const fwo_linear_transform* t, double* value);
+typedef int (*fwo_metric_value_derivative_fn)(void* user, const fwo_linear_transform* t,
+                                              double* value, double* derivative);
+int fwo_estimate_scales(const double* corners, const fwo_linear_transform* t, double small,
+                        double* scales);
+double fwo_estimate_step_scale(const double* corners, const fwo_linear_transform* t,
+                               const double* step, double small);
+int fwo_cg_optimize_level(const fwo_cg_settings* st, const double* corners,
+                          fwo_linear_transform* t, fwo_metric_value_fn value,
+                          fwo_metric_value_derivative_fn value_derivative, void* user,
+                          fwo_cg_trace* trace, double* values, int64_t cap);
+
 /* convergence, crates/fastwarp-reg/src/convergence.rs */
 double fwo_convergence_value(const double* values, int64_t n, int32_t window,
                              double total_energy);

@@ -176,3 +176,45 @@ def test_dense_mi_errors_carry_the_reference_messages(backend):
     with pytest.raises(FastwarpError, match="no voxel of the registration level lies inside"):
         backend.mi_value_derivative_pair_masked(fi, mi, backend.upload_image(g, half),
                                                 backend.upload_image(g, other), 32)
+
+
+# ---- the linear-stage optimiser on the device MI level (optimizer.rs:311-435) ---------------
+def test_level_optimiser_matches_the_callback_path_and_follows_the_oracle(backend):
+    """fw_mi_level_optimize against (a) the same optimiser driven through Python callbacks over
+    the same device level (bit-identical: the evaluations are deterministic) and (b) the oracle's
+    optimiser over the f64 oracle MI: the MI values agree to 1e-5 relative, so the trajectories
+    stay together over a short level; the final transforms agree to 0.02 mm at the corners."""
+    from fastwarp_b200.backend import cg_settings_ants, grid_corners, mi_level_optimize, \
+        optimize_level
+    og, g, f, m, kept, fbin, b = setup(size=(32, 30, 28), spacing=(1.0, 1.0, 1.0),
+                                       origin=(0, 0, 0), direction=np.eye(3), seed=5)
+    level = CudaLinearEngine(backend).prepare_level(g, m, kept, fbin, b)
+    center = (15.5, 14.5, 13.5)
+    start = [0.02, -0.01, 0.015, 0.6, -0.4, 0.3]
+    corners = grid_corners(g)
+    settings = cg_settings_ants(0.1, 12, -1.0, 10)
+    t, trace = mi_level_optimize(level, corners, linear_transform("euler", start, center=center),
+                                 settings)
+    assert trace["iterations"] == 12 and trace["line_search_evaluations"] > 0
+    assert trace["values"][-1] < trace["values"][0]
+    t2, trace2 = optimize_level(level.value, level.value_and_derivative, corners,
+                                linear_transform("euler", start, center=center), settings)
+    assert trace2["values"] == trace["values"]
+    assert list(t2.parameters[:6]) == list(t.parameters[:6])
+
+    def ov(tt):
+        return O.mi_evaluate(b, og, m, kept, fbin, tt, False)[0]
+
+    def ovd(tt):
+        v, d, _, _ = O.mi_evaluate(b, og, m, kept, fbin, tt)
+        return v, d
+    ot, otrace = O.cg_optimize_level(ov, ovd, corners,
+                                     O.linear_transform("euler", start, center=center),
+                                     O.cg_settings_ants(0.1, 12, -1.0, 10))
+    assert otrace["iterations"] == 12
+    assert abs(trace["values"][0] - otrace["values"][0]) <= 1e-5 * abs(otrace["values"][0])
+    assert abs(trace["best_value"] - otrace["best_value"]) <= 1e-4 * abs(otrace["best_value"])
+    ma, oa = O.linear_map(O.linear_transform("euler", list(t.parameters[:6]), center=center))
+    mb, ob = O.linear_map(ot)
+    shift = max(np.linalg.norm((ma - mb) @ c + oa - ob) for c in corners)
+    assert shift < 0.02, shift

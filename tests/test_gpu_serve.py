@@ -83,3 +83,41 @@ def test_device_resident_images_and_fields(pairs):
             assert dev["warp_dev"] and dev["device_end_ms"] > dev["device_start_ms"] >= 0.0
             assert dev["final_energy"] == host["final_energy"]
             Server.free_device_fields(dev)
+
+
+def test_a_mixed_stream_of_masked_mattes_and_two_channel_requests(pairs, backend):
+    """Ragged shapes and request kinds in flight together (masks, a Mattes channel, two
+    channels): every served result equals the same registration run directly."""
+    from fastwarp_b200 import run_syn
+    from fastwarp_b200.backend import make_grid
+    (g1, f1, m1), (g2, f2, m2), (g3, f3, m3) = pairs
+    base = small_recipe()
+    masked = (g1, np.where(np.indices(f1.shape)[0] > 4, 1.0, 0.0))
+    mattes = SynRecipe(gradient_step=0.1, update_field_variance=3.0, cc_radius=2, iterations=[4, 3],
+                       shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0],
+                       convergence_threshold=-1.0, channel_metrics=["mattes"], mi_bins=24)
+    two = SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2, iterations=[3],
+                    shrink_factors=[1], smoothing_sigmas=[0.0], convergence_threshold=-1.0,
+                    channel_weights=[0.5, 0.5])
+    mg = make_grid((30, 30, 30), (1.4, 1.4, 1.4), (-1.0, -2.0, 0.5))
+    mmask = np.ones((30, 30, 30))
+    mmask[20:] = 0.0
+    jobs = [
+        dict(recipe=base, g=g1, f=[f1], m=[m1], fixed_mask=masked),
+        dict(recipe=mattes, g=g2, f=[f2], m=[m2]),
+        dict(recipe=two, g=g3, f=[f3, 1 - f3], m=[m3, 1 - m3], moving_mask=(mg, mmask)),
+        dict(recipe=base, g=g2, f=[f2], m=[m2], moving_mask=(mg, mmask)),
+    ]
+    direct = []
+    for j in jobs:
+        direct.append(run_syn(backend, j["recipe"], j["g"], j["f"], j["g"], j["m"],
+                              fixed_mask=j.get("fixed_mask"), moving_mask=j.get("moving_mask")))
+    with Server(0, slots=3) as s:
+        ts = [s.submit(j["recipe"], j["g"], j["f"], j["g"], j["m"],
+                       fixed_mask=j.get("fixed_mask"), moving_mask=j.get("moving_mask"))
+              for j in jobs]
+        served = [s.wait(t) for t in ts]
+    for d, r in zip(direct, served):
+        assert r["status"] == 0, r["error"]
+        assert np.array_equal(r["warp"], d.warp)
+        assert np.array_equal(r["inverse_warp"], d.inverse_warp)
