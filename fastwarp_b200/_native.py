@@ -81,6 +81,13 @@ METRIC_VALUE_DERIVATIVE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTr
                                          C.POINTER(C.c_double), C.POINTER(C.c_double))
 
 
+class TransformElem(C.Structure):
+    """fw_transform_elem (include/fastwarp_transform_io.h)."""
+    _fields_ = [("kind", C.c_int32), ("matrix", C.c_double * 9),
+                ("translation", C.c_double * 3), ("center", C.c_double * 3), ("grid", Grid),
+                ("field", C.c_void_p)]
+
+
 class SynRecipe(C.Structure):
     _fields_ = [("gradient_step", C.c_double), ("update_field_variance", C.c_double),
                 ("total_field_variance", C.c_double), ("cc_radius", C.c_int32),
@@ -143,6 +150,8 @@ def lib():
         L.fw_ctx_reset_stats.restype = None
         L.fw_abi_struct_size.restype = C.c_size_t
         L.fw_abi_struct_size.argtypes = [C.c_char_p]
+        L.fw_lookup3.restype = C.c_uint32
+        L.fw_lookup3.argtypes = [C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
 

@@ -6,12 +6,14 @@
 // coefficient * grad(moving) by ITK's half-spacing central difference (interp.rs:96-120).
 //
 // Kernel design (sm_100a): one CTA owns a TX x TY column tile and marches along z over a chunk
-// of slices. Each input slice (with an r-voxel halo in x and y) is staged in shared memory; the
-// x and y box passes run in shared memory and the z window is a running sum over a ring of the
-// per-slice xy sums. Sums are float64: products of float32 voxels are exact in float64, so the
-// centred second moments (sum f^2 - (sum f)^2 / n) keep their precision in flat bright regions
-// where float32 cancels. The window planes never touch HBM: the kernel reads the two images once
-// (plus halo re-reads that hit L2) and writes the two derivative fields.
+// of slices. The z window comes first, as running sums in registers over the tile's halo columns
+// (entering slice added, leaving slice subtracted); the x and y box passes then run in shared
+// memory on those sums. Sums are float64: products of float32 voxels are exact in float64, so
+// the centred second moments (sum f^2 - (sum f)^2 / n) keep their precision in flat bright
+// regions where float32 cancels. The window planes never touch HBM: the kernel reads the two
+// images (the leaving slice and the halo a second time, from L2) and writes the two derivative
+// fields. Shared memory holds only the z sums of one slice and the x sums, so several CTAs share
+// an SM and hide each other's float64 and load latency.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -34,33 +36,48 @@ struct CcArgs {
     double isp[3];      // 1 / spacing (the central difference's denominator)
 };
 
-// Shared-memory layout (dynamic): input ring [D][HY][HX] float2 (f, m); with a mask, its flags
-// [D][HY][HX] bytes; x sums [5][HY][TX] double (+ [HY][TX] int counts); xy-sum ring
-// [2R+1][5][TX*TY] double (+ [2R+1][TX*TY] int counts); block-reduction space.
+// Shared-memory layout (dynamic): the z-window sums of every halo column, double-buffered by
+// slice, [ZB][5][HY*HX] double (+ [ZB][HY*HX] int counts with a mask); x sums [5][HY][TX] double
+// (+ [HY][TX] int counts); the raw voxels of the tile with a one-voxel halo for the last D
+// slices, [D][TY+2][TX+2] float2 (f, m), for the centre values and the central differences;
+// block-reduction space.
 template <int R, int TY, bool MK>
 struct Layout {
     static constexpr int HX = TX + 2 * R;
     static constexpr int HY = TY + 2 * R;
-    static constexpr int D = R + 2;        // input slices kept: k-R-1 .. k
-    static constexpr int W = 2 * R + 1;    // z window
+    static constexpr int HC = HX * HY;           // halo columns of the tile
     static constexpr int NT = TX * TY;
+    static constexpr int CPT = (HC + NT - 1) / NT;  // halo columns per thread
     static constexpr int NP = MK ? 4 : 3;  // block partials: cc, |dF|^2, |dM|^2 (+ valid voxels)
-    static constexpr size_t in_bytes = sizeof(float2) * D * HY * HX;
-    static constexpr size_t vin_bytes = MK ? (size_t)(D * HY * HX + 15) / 16 * 16 : 0;
+    static constexpr int RX = TX + 2, RY = TY + 2, RXY = RX * RY;
+    // raw slices kept: the output at step k reads slices k-R-1 .. k-R+1, and slice k is written
+    // before step k's first barrier, while slow threads may still read step k-1's outputs
+    static constexpr int D = R + 3;
+    static constexpr size_t zs1 = sizeof(double) * 5 * HC + (MK ? sizeof(int) * HC : 0);
     static constexpr size_t xs_bytes = sizeof(double) * 5 * HY * TX;
     static constexpr size_t xc_bytes = MK ? sizeof(int) * HY * TX : 0;
-    static constexpr size_t ring_bytes = sizeof(double) * W * 5 * NT;
-    static constexpr size_t rc_bytes = MK ? sizeof(int) * W * NT : 0;
-    static constexpr size_t bytes =
-        in_bytes + vin_bytes + xs_bytes + xc_bytes + ring_bytes + rc_bytes + 64 * sizeof(double);
+    static constexpr size_t raw_bytes = sizeof(float2) * D * RXY;
+    // two z-sum buffers (one barrier less per slice) when two CTAs still share an SM
+    static constexpr int ZB = (2 * zs1 + xs_bytes + xc_bytes + raw_bytes) <= 110 * 1024 ? 2 : 1;
+    static constexpr size_t bytes = ZB * zs1 + xs_bytes + xc_bytes + raw_bytes + 64 * sizeof(double);
 };
 
 // MK: masked (cpu/mod.rs:134-163 -> evaluate_masked with Some(valid)): a voxel counts only where
 // `vimg` is not zero; invalid voxels add nothing to any window sum, the count is the number of
 // valid voxels in the window, their outputs are zero and the value is the mean over the valid
 // voxels (result[3] receives their number; zero means no voxel in the masks).
+//
+// Pass order z, x, y. Each thread keeps the z-window sums of up to CPT halo columns in registers
+// and moves them one slice per step: the entering slice is added and the leaving slice (read
+// again, from L2) subtracted. Products of float32 voxels are exact in float64, so the running
+// sums carry no drift beyond float64 rounding. The z sums go to shared memory, the x pass makes
+// row sums of them and each thread's y pass finishes its own voxel's six window sums.
+#ifndef FW_CC_MIN_BLOCKS
+#define FW_CC_MIN_BLOCKS 2
+#endif
+
 template <int R, int TY, bool MK>
-__global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __restrict__ fimg,
+__global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a, const float* __restrict__ fimg,
                                                      const float* __restrict__ mimg,
                                                      const float* __restrict__ vimg,
                                                      float* __restrict__ d_fixed,
@@ -70,14 +87,11 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
                                                      double* __restrict__ result, int want_norms) {
     using L = Layout<R, TY, MK>;
     extern __shared__ __align__(16) unsigned char smem[];
-    float2* in = reinterpret_cast<float2*>(smem);
-    unsigned char* vin = smem + L::in_bytes;
-    double* xs = reinterpret_cast<double*>(smem + L::in_bytes + L::vin_bytes);
-    int* xc = reinterpret_cast<int*>(smem + L::in_bytes + L::vin_bytes + L::xs_bytes);
-    double* ring = reinterpret_cast<double*>(smem + L::in_bytes + L::vin_bytes + L::xs_bytes +
-                                             L::xc_bytes);
-    int* rcn = reinterpret_cast<int*>(ring + L::W * 5 * L::NT);
-    double* red = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(rcn) + L::rc_bytes);
+    double* xs = reinterpret_cast<double*>(smem + L::ZB * L::zs1);
+    int* xc = reinterpret_cast<int*>(smem + L::ZB * L::zs1 + L::xs_bytes);
+    float2* raw = reinterpret_cast<float2*>(smem + L::ZB * L::zs1 + L::xs_bytes + L::xc_bytes);
+    double* red = reinterpret_cast<double*>(smem + L::ZB * L::zs1 + L::xs_bytes + L::xc_bytes +
+                                            L::raw_bytes);
 
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
     const int tid = threadIdx.x;
@@ -89,165 +103,152 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
     const bool own = x < nx && y < ny;
     const long long sxy = (long long)nx * ny;
 
-    for (int s = tid; s < L::W * 5 * L::NT; s += L::NT) ring[s] = 0.0;
-    if constexpr (MK)
-        for (int s = tid; s < L::W * L::NT; s += L::NT) rcn[s] = 0;
-    double S[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    int Sc = 0;  // valid voxels in the window (masked)
     double acc_cc = 0.0, acc_nf = 0.0, acc_nm = 0.0, acc_nv = 0.0;
-
     // analytic voxel counts of the clamped window along x and y
     const int cxn = own ? (min(x + R, nx - 1) - max(x - R, 0) + 1) : 0;
     const int cyn = own ? (min(y + R, ny - 1) - max(y - R, 0) + 1) : 0;
 
-    const int kbeg = max(z0 - R, 0);
-    const int kend = min(z1 + R, nz);  // slices that exist and are needed (exclusive)
-    // slice-invariant prefetch slots: offset inside a slice (-1 outside the image in x or y)
-    constexpr int PERC = (L::HY * L::HX + L::NT - 1) / L::NT;
-    int src_off[PERC];
+    // the thread's halo columns: offset inside a slice, -1 outside the image (sums stay zero)
+    // and, for columns within one voxel of the tile, their slot in a raw slice (-1 otherwise)
+    int coff[L::CPT], ridx[L::CPT];
+    double Z[L::CPT][5];
+    int Zc[L::CPT];
 #pragma unroll
-    for (int q = 0; q < PERC; ++q) {
-        int s = tid + q * L::NT;
-        src_off[q] = -1;
-        if (s < L::HY * L::HX) {
-            int hy = s / L::HX, hx = s - hy * L::HX;
-            int gx = x0 - R + hx, gy = y0 - R + hy;
-            if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) src_off[q] = gy * nx + gx;
+    for (int j = 0; j < L::CPT; ++j) {
+        const int s = tid + j * L::NT;
+        coff[j] = -1;
+        ridx[j] = -1;
+        if (s < L::HC) {
+            const int hy = s / L::HX, hx = s - hy * L::HX;
+            const int gx = x0 - R + hx, gy = y0 - R + hy;
+            if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) coff[j] = gy * nx + gx;
+            const int rx = hx - (R - 1), ry = hy - (R - 1);
+            if (rx >= 0 && rx < L::RX && ry >= 0 && ry < L::RY) ridx[j] = ry * L::RX + rx;
         }
-    }
-    float2 pre[PERC];
-    unsigned char prev[PERC];
-    auto fetch = [&](int k) {
-        const long long zoff = (long long)k * sxy;
 #pragma unroll
-        for (int q = 0; q < PERC; ++q) {
-            pre[q] = src_off[q] >= 0 ? make_float2(__ldg(fimg + zoff + src_off[q]),
-                                                   __ldg(mimg + zoff + src_off[q]))
-                                     : make_float2(0.0f, 0.0f);
-            if constexpr (MK)
-                prev[q] = src_off[q] >= 0 ? (__ldg(vimg + zoff + src_off[q]) != 0.0f) : 0;
+        for (int q = 0; q < 5; ++q) Z[j][q] = 0.0;
+        Zc[j] = 0;
+    }
+    // entering slice k and leaving slice k - 2R - 1 of the next step, in flight during a step
+    float2 pin[L::CPT], pout[L::CPT];
+    bool vin[L::CPT], vout[L::CPT];
+    const int kb = max(z0 - R, 0);
+    auto fetch = [&](int k) {
+        const bool add = k < nz, sub = k - 2 * R - 1 >= kb;
+        const long long zi = (long long)k * sxy, zo = (long long)(k - 2 * R - 1) * sxy;
+#pragma unroll
+        for (int j = 0; j < L::CPT; ++j) {
+            const bool c = coff[j] >= 0;
+            pin[j] = c && add ? make_float2(__ldg(fimg + zi + coff[j]), __ldg(mimg + zi + coff[j]))
+                              : make_float2(0.0f, 0.0f);
+            pout[j] = c && sub ? make_float2(__ldg(fimg + zo + coff[j]), __ldg(mimg + zo + coff[j]))
+                               : make_float2(0.0f, 0.0f);
+            if constexpr (MK) {  // pin stays raw: the central differences read it
+                vin[j] = c && add && __ldg(vimg + zi + coff[j]) != 0.0f;
+                vout[j] = c && sub && __ldg(vimg + zo + coff[j]) != 0.0f;
+                if (!vout[j]) pout[j] = make_float2(0.0f, 0.0f);
+            }
         }
     };
-    if (kbeg < kend) fetch(kbeg);
-    for (int k = kbeg; k < z1 + R; ++k) {
-        __syncthreads();  // previous slice's readers are done with the slot and the x sums
-        double P[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        int Pc = 0;
-        const bool have = k < kend;
-        if (have) {
-            float2* slot = in + (k % L::D) * (L::HY * L::HX);
-            unsigned char* vslot = vin + (k % L::D) * (L::HY * L::HX);
+    fetch(kb);
+    int buf = 0;
+    for (int k = kb; k < z1 + R; ++k) {
+        // z step: add slice k (if it exists), drop slice k - 2R - 1 (if it was added)
+        float2* rslot = raw + (k % L::D) * L::RXY;
 #pragma unroll
-            for (int q = 0; q < PERC; ++q) {
-                int s = tid + q * L::NT;
-                if (s < L::HY * L::HX) {
-                    slot[s] = pre[q];
-                    if constexpr (MK) vslot[s] = prev[q];
-                }
+        for (int j = 0; j < L::CPT; ++j) {
+            if (ridx[j] >= 0 && k < nz) rslot[ridx[j]] = pin[j];
+            float2 a = pin[j];
+            if constexpr (MK)
+                if (!vin[j]) a = make_float2(0.0f, 0.0f);  // a masked-out voxel adds nothing
+            const double f = a.x, m = a.y, g = pout[j].x, n = pout[j].y;
+            Z[j][0] += f - g;
+            Z[j][1] += m - n;
+            Z[j][2] += f * f - g * g;
+            Z[j][3] += m * m - n * n;
+            Z[j][4] += f * m - g * n;
+            if constexpr (MK) Zc[j] += (int)vin[j] - (int)vout[j];
+        }
+        if (k + 1 < z1 + R) fetch(k + 1);
+        const int z = k - R;
+        if (z < z0) continue;  // the window is still filling (uniform across the CTA)
+
+        double* zs = reinterpret_cast<double*>(smem + buf * L::zs1);
+        int* zc = reinterpret_cast<int*>(zs + 5 * L::HC);
+        buf ^= (L::ZB - 1);
+        if constexpr (L::ZB == 1) __syncthreads();  // the previous x pass is done with zs
+#pragma unroll
+        for (int j = 0; j < L::CPT; ++j) {
+            const int s = tid + j * L::NT;
+            if (s < L::HC) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) zs[q * L::HC + s] = Z[j][q];
+                if constexpr (MK) zc[s] = Zc[j];
             }
-            __syncthreads();
-            if (k + 1 < kend) fetch(k + 1);  // in flight while this slice is summed
-            // x pass: each item makes the sums of two adjacent columns from one window of
-            // 2r + 2 voxels (the 2r in the middle are shared)
-            for (int s = tid; s < L::HY * (TX / 2); s += L::NT) {
-                int hy = s / (TX / 2), cp = s - hy * (TX / 2);
-                const float2* row = slot + hy * L::HX + 2 * cp;
-                const unsigned char* vrow = vslot + hy * L::HX + 2 * cp;
-                // a masked-out voxel enters every sum as zero
-                auto val = [&](int t) {
-                    float2 v = row[t];
-                    if constexpr (MK)
-                        if (!vrow[t]) v = make_float2(0.0f, 0.0f);
-                    return v;
-                };
-                if constexpr (MK) {
-                    int cn = 0;
-#pragma unroll
-                    for (int t = 1; t <= 2 * R; ++t) cn += vrow[t];
-                    xc[hy * TX + 2 * cp] = cn + vrow[0];
-                    xc[hy * TX + 2 * cp + 1] = cn + vrow[2 * R + 1];
-                }
-                // two interleaved partial sums per plane: half-length add chains
-                double c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0;
-                double e0 = 0, e1 = 0, e2 = 0, e3 = 0, e4 = 0;
-#pragma unroll
-                for (int t = 1; t <= 2 * R; t += 2) {
-                    float2 v = val(t), w = val(t + 1);
-                    double f = v.x, m = v.y, g = w.x, n = w.y;
-                    c0 += f;
-                    c1 += m;
-                    c2 += f * f;
-                    c3 += m * m;
-                    c4 += f * m;
-                    e0 += g;
-                    e1 += n;
-                    e2 += g * g;
-                    e3 += n * n;
-                    e4 += g * n;
-                }
-                c0 += e0;
-                c1 += e1;
-                c2 += e2;
-                c3 += e3;
-                c4 += e4;
-                float2 va = val(0), vb = val(2 * R + 1);
-                double fa = va.x, ma = va.y, fb = vb.x, mb = vb.y;
-                double* o = xs + hy * TX + 2 * cp;
-                *reinterpret_cast<double2*>(o + 0 * L::HY * TX) = make_double2(c0 + fa, c0 + fb);
-                *reinterpret_cast<double2*>(o + 1 * L::HY * TX) = make_double2(c1 + ma, c1 + mb);
-                *reinterpret_cast<double2*>(o + 2 * L::HY * TX) = make_double2(c2 + fa * fa, c2 + fb * fb);
-                *reinterpret_cast<double2*>(o + 3 * L::HY * TX) = make_double2(c3 + ma * ma, c3 + mb * mb);
-                *reinterpret_cast<double2*>(o + 4 * L::HY * TX) = make_double2(c4 + fa * ma, c4 + fb * mb);
-            }
-            __syncthreads();
-            // y pass for the thread's own column
+        }
+        __syncthreads();  // z sums visible; the previous y pass is done with the x sums
+        // x pass: each item makes the sums of two adjacent columns from one window of 2r + 2
+        // halo columns (the 2r in the middle are shared)
+        for (int s = tid; s < L::HY * (TX / 2); s += L::NT) {
+            const int hy = s / (TX / 2), cp = s - hy * (TX / 2);
+            const int base = hy * L::HX + 2 * cp;
+            double* o = xs + hy * TX + 2 * cp;
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                double s = 0.0, s2 = 0.0;  // two partial sums: half-length add chains
+                const double* row = zs + q * L::HC + base;
+                double c = 0.0, e = 0.0;  // two partial sums: half-length add chains
 #pragma unroll
-                for (int t = 0; t < 2 * R; t += 2) {
-                    s += xs[(q * L::HY + ty + t) * TX + tx];
-                    s2 += xs[(q * L::HY + ty + t + 1) * TX + tx];
+                for (int t = 1; t <= 2 * R; t += 2) {
+                    c += row[t];
+                    e += row[t + 1];
                 }
-                P[q] = s + s2 + xs[(q * L::HY + ty + 2 * R) * TX + tx];
+                c += e;
+                *reinterpret_cast<double2*>(o + q * L::HY * TX) =
+                    make_double2(c + row[0], c + row[2 * R + 1]);
             }
             if constexpr (MK) {
+                const int* crow = zc + base;
+                int cn = 0;
 #pragma unroll
-                for (int t = 0; t <= 2 * R; ++t) Pc += xc[(ty + t) * TX + tx];
+                for (int t = 1; t <= 2 * R; ++t) cn += crow[t];
+                xc[hy * TX + 2 * cp] = cn + crow[0];
+                xc[hy * TX + 2 * cp + 1] = cn + crow[2 * R + 1];
             }
         }
-        // z window: running sum over the ring of xy sums (entering k, leaving k - 2R - 1)
-        double* rs = ring + (k % L::W) * 5 * L::NT + tid;
+        __syncthreads();
+        if (!own) continue;
+        // y pass for the thread's own column
+        double S[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            double old = rs[q * L::NT];
-            S[q] += P[q] - old;
-            rs[q * L::NT] = P[q];
+            double s = 0.0, s2 = 0.0;
+#pragma unroll
+            for (int t = 0; t < 2 * R; t += 2) {
+                s += xs[(q * L::HY + ty + t) * TX + tx];
+                s2 += xs[(q * L::HY + ty + t + 1) * TX + tx];
+            }
+            S[q] = s + s2 + xs[(q * L::HY + ty + 2 * R) * TX + tx];
         }
-        if constexpr (MK) {
-            int* rc = rcn + (k % L::W) * L::NT + tid;
-            Sc += Pc - *rc;
-            *rc = Pc;
-        }
-        const int z = k - R;
-        if (z < z0 || z >= z1 || !own) continue;
 
         // ---- output voxel (x, y, z) ----
         const long long l = (long long)z * sxy + (long long)y * nx + x;
         double cnt;
         if constexpr (MK) {
-            if (!vin[(z % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R)]) {
+            if (__ldg(vimg + l) == 0.0f) {
                 d_fixed[l] = d_fixed[l + a.ps] = d_fixed[l + 2 * a.ps] = 0.0f;
                 d_moving[l] = d_moving[l + a.ps] = d_moving[l + 2 * a.ps] = 0.0f;
                 continue;
             }
+            int Sc = 0;
+#pragma unroll
+            for (int t = 0; t <= 2 * R; ++t) Sc += xc[(ty + t) * TX + tx];
             cnt = (double)Sc;  // >= 1: the centre is valid
             acc_nv += 1.0;
         } else {
             const int czn = min(z + R, nz - 1) - max(z - R, 0) + 1;
             cnt = (double)(cxn * cyn * czn);
         }
-        const float2* cs = in + (z % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R);
+        const float2* cs = raw + (z % L::D) * L::RXY + (ty + 1) * L::RX + (tx + 1);
         const float fv = cs[0].x, mv = cs[0].y;
         // metric/cc.rs:267-302 (same expression order)
         const double sum_f = S[0], sum_m = S[1], sum_f2 = S[2], sum_m2 = S[3], sum_fm = S[4];
@@ -273,6 +274,8 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
         // gradients of moving (for the first direction) and of fixed (for the second)
         float gm[3], gf[3];
         if (a.identity_dir) {
+            // interp.rs:96-120 on an identity-direction grid: the probes at +-half a spacing lerp
+            // halfway toward the neighbours along the axis, read from the raw slices
             const int nn[3] = {nx, ny, nz};
             const int pos[3] = {x, y, z};
 #pragma unroll
@@ -282,28 +285,25 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
                 if (!axis_probe_inside(a.g, x, y, z, d, -1.0, nn[d]) ||
                     !axis_probe_inside(a.g, x, y, z, d, +1.0, nn[d]))
                     continue;
-                // neighbours along d inside the staged tile / ring
-                float2 lo, hi;
-                const float2* c0 = cs;
-                if (d == 0) {
-                    lo = c0[-1];
-                    hi = c0[1];
-                } else if (d == 1) {
-                    lo = c0[-L::HX];
-                    hi = c0[L::HX];
-                } else {
-                    lo = (z > 0) ? in[((z - 1) % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R)]
-                                 : cs[0];
-                    hi = (z < nz - 1) ? in[((z + 1) % L::D) * (L::HY * L::HX) + (ty + R) * L::HX + (tx + R)]
-                                      : cs[0];
-                }
                 const int p = pos[d];
-                // upper probe at p + 0.5: lerp to p + 1 unless p is the last voxel
-                float m2 = p < nn[d] - 1 ? fmaf(hi.y - mv, 0.5f, mv) : mv;
-                float f2 = p < nn[d] - 1 ? fmaf(hi.x - fv, 0.5f, fv) : fv;
-                // lower probe at p - 0.5: base p - 1 with weight 0.5, or the first voxel itself
-                float m1 = p > 0 ? fmaf(mv - lo.y, 0.5f, lo.y) : mv;
-                float f1 = p > 0 ? fmaf(fv - lo.x, 0.5f, lo.x) : fv;
+                float2 lo = cs[0], hi = cs[0];
+                if (d == 0) {
+                    if (p > 0) lo = cs[-1];
+                    if (p < nn[d] - 1) hi = cs[1];
+                } else if (d == 1) {
+                    if (p > 0) lo = cs[-L::RX];
+                    if (p < nn[d] - 1) hi = cs[L::RX];
+                } else {
+                    const int o = (ty + 1) * L::RX + (tx + 1);
+                    if (p > 0) lo = raw[((z - 1) % L::D) * L::RXY + o];
+                    if (p < nn[d] - 1) hi = raw[((z + 1) % L::D) * L::RXY + o];
+                }
+                // upper probe at p + 0.5: lerp to p + 1 unless p is the last voxel; lower probe
+                // at p - 0.5: base p - 1 with weight 0.5, or the first voxel itself
+                const float m2 = p < nn[d] - 1 ? fmaf(hi.y - mv, 0.5f, mv) : mv;
+                const float f2 = p < nn[d] - 1 ? fmaf(hi.x - fv, 0.5f, fv) : fv;
+                const float m1 = p > 0 ? fmaf(mv - lo.y, 0.5f, lo.y) : mv;
+                const float f1 = p > 0 ? fmaf(fv - lo.x, 0.5f, lo.x) : fv;
                 gm[d] = (float)((double)(m2 - m1) * a.isp[d]);
                 gf[d] = (float)((double)(f2 - f1) * a.isp[d]);
             }
@@ -370,23 +370,49 @@ __global__ void __launch_bounds__(TX * TY) k_cc_pair(CcArgs a, const float* __re
     }
 }
 
+// Grid of a launch: TX x TY column tiles times z chunks. The chunk count is the one with the
+// least estimated time: whole waves of resident CTAs, each chunk paying 2R filling steps (about
+// half an output step each).
+template <int R, int TY, bool MK>
+int plan_launch(CcArgs& a, int num_sms, dim3* grid) {
+    using L = Layout<R, TY, MK>;
+    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY, MK>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes));
+    static const int occ = [] {
+        int o = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_cc_pair<R, TY, MK>, L::NT,
+                                                          L::bytes) != cudaSuccess || o < 1)
+            o = 1;
+        return o;
+    }();
+    dim3 g((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, 1);
+    const long long tiles = (long long)g.x * g.y;
+    const long long slots = (long long)occ * num_sms;
+    int best = 1;
+    double best_t = 0.0;
+    for (int c = 1; c <= a.g.nz; ++c) {
+        const long long waves = (tiles * c + slots - 1) / slots;
+        const double t = (double)waves * ((a.g.nz + c - 1) / c + 0.5 * R);
+        if (c == 1 || t < best_t) {
+            best = c;
+            best_t = t;
+        }
+    }
+    a.zchunk = (a.g.nz + best - 1) / best;
+    g.z = (a.g.nz + a.zchunk - 1) / a.zchunk;
+    *grid = g;
+    return 0;
+}
+
 template <int R, int TY, bool MK>
 int launch_r(fw_ctx* ctx, const CcArgs& a0, const float* f, const float* m, const float* v,
              float* df, float* dm, double* d_result, int want_norms) {
     using L = Layout<R, TY, MK>;
     CcArgs a = a0;
-    dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, 1);
-    // z chunks: enough CTAs to fill the GPU a few times over, chunks no thinner than 4R slices
-    long long tiles = (long long)grid.x * grid.y;
-    int want = (int)std::max<long long>(1, (4LL * ctx->num_sms + tiles - 1) / tiles);
-    int chunk = (a.g.nz + want - 1) / want;
-    chunk = std::max(chunk, std::min(a.g.nz, 4 * R + 4));
-    a.zchunk = chunk;
-    grid.z = (a.g.nz + chunk - 1) / chunk;
+    dim3 grid;
+    FW_TRY((plan_launch<R, TY, MK>(a, ctx->num_sms, &grid)));
     unsigned int nblocks = grid.x * grid.y * grid.z;
     FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)L::NP * nblocks + 16));
-    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY, MK>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes));
     k_cc_pair<R, TY, MK><<<grid, L::NT, L::bytes, ctx->stream>>>(
         a, f, m, v, df, dm, ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 1, d_result,
         want_norms);
@@ -402,9 +428,9 @@ int launch_radius(fw_ctx* ctx, const CcArgs& a, int radius, const float* f, cons
         case 3: return launch_r<3, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
         case 4: return launch_r<4, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
         case 5: return launch_r<5, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 6: return launch_r<6, 4, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 7: return launch_r<7, 4, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 8: return launch_r<8, 4, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 6: return launch_r<6, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 7: return launch_r<7, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        case 8: return launch_r<8, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
         default:
             return fail(FW_ERR_INVALID, "cc metric: radius must be in 1..=8 (BOX_RADIUS_MAX)");
     }
@@ -571,13 +597,8 @@ int noalloc_launch(const CcArgs& a0, int num_sms, const float* f, const float* m
                    float* dm, double* result, NoAllocScratch* s, cudaStream_t stream) {
     using L = Layout<R, TY, false>;
     CcArgs a = a0;
-    dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, 1);
-    long long tiles = (long long)grid.x * grid.y;
-    int want = (int)std::max<long long>(1, (4LL * num_sms + tiles - 1) / tiles);
-    int chunk = (a.g.nz + want - 1) / want;
-    chunk = std::max(chunk, std::min(a.g.nz, 4 * R + 4));
-    a.zchunk = chunk;
-    grid.z = (a.g.nz + chunk - 1) / chunk;
+    dim3 grid;
+    FW_TRY((plan_launch<R, TY, false>(a, num_sms, &grid)));
     long long nblocks = (long long)grid.x * grid.y * grid.z;
     if (nblocks > FW_NOALLOC_MAX_BLOCKS)
         return fail(FW_ERR_INVALID,
@@ -586,8 +607,6 @@ int noalloc_launch(const CcArgs& a0, int num_sms, const float* f, const float* m
                         " the static scratch holds (use fw_cc_value_derivative_pair)");
     // the last-block counter must start at zero whatever the previous call left
     FW_CUDA(cudaMemsetAsync(s->counter, 0, sizeof(unsigned int), stream));
-    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes));
     k_cc_pair<R, TY, false><<<grid, L::NT, L::bytes, stream>>>(a, f, m, nullptr, df, dm,
                                                                 s->partials, s->counter, result, 1);
     cudaError_t e = cudaGetLastError();
@@ -629,9 +648,9 @@ extern "C" int fw_cc_value_derivative_pair_noalloc(const fw_grid* grid, const fl
         case 3: return noalloc_launch<3, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
         case 4: return noalloc_launch<4, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
         case 5: return noalloc_launch<5, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
-        case 6: return noalloc_launch<6, 4>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
-        case 7: return noalloc_launch<7, 4>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
-        case 8: return noalloc_launch<8, 4>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 6: return noalloc_launch<6, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 7: return noalloc_launch<7, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
+        case 8: return noalloc_launch<8, 8>(a, num_sms, fixed, moving, d_fixed, d_moving, result, s, st);
         default:
             return fail(FW_ERR_INVALID, "cc metric: radius must be in 1..=8 (BOX_RADIUS_MAX)");
     }

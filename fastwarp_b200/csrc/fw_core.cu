@@ -83,7 +83,9 @@ int make_grid(const fw_grid* g, HostGrid& out) {
         out.sp[a] = g->spacing[a];
         out.org[a] = g->origin[a];
     }
-    FW_CHECK(out.n[0] * out.n[1] * out.n[2] < (int64_t(1) << 40), "voxel count overflows");
+    // voxel offsets inside a plane are 32-bit in the kernels
+    FW_CHECK(out.n[0] * out.n[1] * out.n[2] < (int64_t(1) << 31),
+             "grid too large: 2^31 voxels or more");
     for (int k = 0; k < 9; ++k) {
         FW_CHECK(std::isfinite(g->direction[k]), "origin and direction must be finite");
         out.dir[k] = g->direction[k];

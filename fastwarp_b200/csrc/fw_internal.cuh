@@ -148,6 +148,7 @@ __device__ __forceinline__ void lin_axis(double c, int n, int& b, float& w) {
 }
 
 // interp.rs:43-85: LinearInterpolateImageFunction::EvaluateAtContinuousIndex (no bounds check).
+// Voxel offsets are 32-bit (grids hold fewer than 2^31 voxels).
 __device__ __forceinline__ float lin_at_index(const float* __restrict__ img, int nx, int ny,
                                               int nz, double cx, double cy, double cz) {
     int bx, by, bz;
@@ -155,19 +156,19 @@ __device__ __forceinline__ float lin_at_index(const float* __restrict__ img, int
     lin_axis(cx, nx, bx, wx);
     lin_axis(cy, ny, by, wy);
     lin_axis(cz, nz, bz, wz);
-    const long long sy = nx, sz = (long long)nx * ny;
-    const float* p = img + bx + sy * by + sz * bz;
-    int ox = wx > 0.0f ? 1 : 0;
-    long long oy = wy > 0.0f ? sy : 0;
-    long long oz = wz > 0.0f ? sz : 0;
-    float v000 = __ldg(p), v100 = __ldg(p + ox);
-    float v010 = __ldg(p + oy), v110 = __ldg(p + oy + ox);
+    const unsigned int sy = (unsigned int)nx, sz = (unsigned int)nx * (unsigned int)ny;
+    const unsigned int b = (unsigned int)bx + sy * (unsigned int)by + sz * (unsigned int)bz;
+    const unsigned int ox = wx > 0.0f ? 1u : 0u;
+    const unsigned int oy = wy > 0.0f ? sy : 0u;
+    const unsigned int oz = wz > 0.0f ? sz : 0u;
+    float v000 = __ldg(img + b), v100 = __ldg(img + (b + ox));
+    float v010 = __ldg(img + (b + oy)), v110 = __ldg(img + (b + oy + ox));
     float x0 = fmaf(v100 - v000, wx, v000);
     float x1 = fmaf(v110 - v010, wx, v010);
     float y0 = fmaf(x1 - x0, wy, x0);
     if (wz > 0.0f) {
-        float v001 = __ldg(p + oz), v101 = __ldg(p + oz + ox);
-        float v011 = __ldg(p + oz + oy), v111 = __ldg(p + oz + oy + ox);
+        float v001 = __ldg(img + (b + oz)), v101 = __ldg(img + (b + oz + ox));
+        float v011 = __ldg(img + (b + oz + oy)), v111 = __ldg(img + (b + oz + oy + ox));
         float x2 = fmaf(v101 - v001, wx, v001);
         float x3 = fmaf(v111 - v011, wx, v011);
         float y1 = fmaf(x3 - x2, wy, x2);
@@ -177,7 +178,10 @@ __device__ __forceinline__ float lin_at_index(const float* __restrict__ img, int
 }
 
 // field_ops.rs:143-172: VectorLinearInterpolateImageFunction (neighbours clamped, weights 1-d, d)
-// of a SoA field at a continuous index.
+// of a SoA field at a continuous index. The eight corner weights are formed once for the three
+// planes; voxel offsets are 32-bit (grids hold fewer than 2^31 voxels). A corner of weight zero
+// adds nothing, as in the reference, by a select rather than a branch, so that all 24 loads can
+// be in flight at once (every corner address is inside the buffer: the indices are clamped).
 __device__ __forceinline__ void vec_at_index(const float* __restrict__ f, long long ps, int nx,
                                              int ny, int nz, double cx, double cy, double cz,
                                              float out[3]) {
@@ -187,25 +191,25 @@ __device__ __forceinline__ void vec_at_index(const float* __restrict__ f, long l
     int xa = min(max(x0, 0), nx - 1), xb = min(max(x0 + 1, 0), nx - 1);
     int ya = min(max(y0, 0), ny - 1), yb = min(max(y0 + 1, 0), ny - 1);
     int za = min(max(z0, 0), nz - 1), zb = min(max(z0 + 1, 0), nz - 1);
-    const long long sy = nx, sz = (long long)nx * ny;
-    long long i000 = xa + sy * ya + sz * za, i100 = xb + sy * ya + sz * za;
-    long long i010 = xa + sy * yb + sz * za, i110 = xb + sy * yb + sz * za;
-    long long i001 = xa + sy * ya + sz * zb, i101 = xb + sy * ya + sz * zb;
-    long long i011 = xa + sy * yb + sz * zb, i111 = xb + sy * yb + sz * zb;
-    float w[2][3] = {{1.0f - dx, 1.0f - dy, 1.0f - dz}, {dx, dy, dz}};
+    const unsigned int sy = (unsigned int)nx, sz = (unsigned int)nx * (unsigned int)ny;
+    const unsigned int b = (unsigned int)xa + sy * (unsigned int)ya + sz * (unsigned int)za;
+    const unsigned int ox = (unsigned int)(xb - xa), oy = sy * (unsigned int)(yb - ya),
+                       oz = sz * (unsigned int)(zb - za);
+    const unsigned int off[8] = {b, b + ox, b + oy, b + oy + ox,
+                                 b + oz, b + oz + ox, b + oz + oy, b + oz + oy + ox};
+    const float w0[3] = {1.0f - dx, 1.0f - dy, 1.0f - dz}, w1[3] = {dx, dy, dz};
+    const float o[8] = {w0[0] * w0[1] * w0[2], w1[0] * w0[1] * w0[2], w0[0] * w1[1] * w0[2],
+                        w1[0] * w1[1] * w0[2], w0[0] * w0[1] * w1[2], w1[0] * w0[1] * w1[2],
+                        w0[0] * w1[1] * w1[2], w1[0] * w1[1] * w1[2]};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const float* p = f + c * ps;
         float acc = 0.0f;
-        float o;
-        o = w[0][0] * w[0][1] * w[0][2]; if (o != 0.0f) acc += o * __ldg(p + i000);
-        o = w[1][0] * w[0][1] * w[0][2]; if (o != 0.0f) acc += o * __ldg(p + i100);
-        o = w[0][0] * w[1][1] * w[0][2]; if (o != 0.0f) acc += o * __ldg(p + i010);
-        o = w[1][0] * w[1][1] * w[0][2]; if (o != 0.0f) acc += o * __ldg(p + i110);
-        o = w[0][0] * w[0][1] * w[1][2]; if (o != 0.0f) acc += o * __ldg(p + i001);
-        o = w[1][0] * w[0][1] * w[1][2]; if (o != 0.0f) acc += o * __ldg(p + i101);
-        o = w[0][0] * w[1][1] * w[1][2]; if (o != 0.0f) acc += o * __ldg(p + i011);
-        o = w[1][0] * w[1][1] * w[1][2]; if (o != 0.0f) acc += o * __ldg(p + i111);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float v = __ldg(p + off[q]);
+            acc = o[q] != 0.0f ? fmaf(o[q], v, acc) : acc;
+        }
         out[c] = acc;
     }
 }
@@ -340,11 +344,14 @@ __device__ __forceinline__ bool column_of(int nx, int ny, int nz, int zchunk, in
     return x < nx && y < ny && z0 < z1;
 }
 
+// 32-bit division: grids hold fewer than 2^31 voxels.
 __device__ __forceinline__ void voxel_ijk(long long l, int nx, int ny, int& i, int& j, int& k) {
-    long long q = l / nx;
-    i = (int)(l - q * nx);
-    k = (int)(q / ny);
-    j = (int)(q - (long long)k * ny);
+    const unsigned int u = (unsigned int)l;
+    const unsigned int q = u / (unsigned int)nx;
+    i = (int)(u - q * (unsigned int)nx);
+    const unsigned int kk = q / (unsigned int)ny;
+    k = (int)kk;
+    j = (int)(q - kk * (unsigned int)ny);
 }
 
 // non-negative float max via integer compare; NaN (canonical, positive) wins.

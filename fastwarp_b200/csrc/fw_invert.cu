@@ -6,8 +6,9 @@
 //
 // Device design: the error at voxel x depends only on psi(x) and the read-only field f, so one
 // sweep can apply body k's update to psi(x) and at once measure body k+1's error at the same
-// voxel. Each body is therefore ONE sweep (read psi, gather f, write psi, gather f again for the
-// next measurement) plus a fixed-order reduction done by the last block to finish. The loop
+// voxel. Each body is therefore ONE sweep (read psi and the kept residual, write psi, gather f
+// for the next measurement only when there is a next body) plus a fixed-order reduction done by
+// the last block to finish; it is launched as a pair of kernels of which one works. The loop
 // state (errors of the last measurement, body index, whether the next body runs) lives in device
 // memory and is updated by that last block, so the loop needs no host read-back: the SyN driver
 // runs it inside a CUDA graph WHILE node whose condition the last block sets.
@@ -96,7 +97,7 @@ __device__ void reduce_and_finish(double sum, float mx, double* __restrict__ par
 
 // First measurement (body 0's error) of psi against f; the residual e = psi + f(x + psi) of
 // every voxel is kept in `res` for the body that follows.
-__global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __restrict__ f,
+__global__ void __launch_bounds__(256, 4) k_inv_measure(InvArgs a, const float* __restrict__ f,
                                                      const float* __restrict__ psi,
                                                      float* __restrict__ res,
                                                      double* __restrict__ partials,
@@ -148,26 +149,32 @@ __global__ void __launch_bounds__(256) k_inv_measure(InvArgs a, const float* __r
 // One body: the update with eps (0.75 on body 0, else 0.5) and limit eps * max of the last
 // measurement, from the residual that measurement kept in `res`; faces to zero; then -- when
 // the next body will run -- its measurement, whose residual replaces the voxel's in `res`.
-// Without a next body the sweep is elementwise (no gather).
-__global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __restrict__ f,
-                                                  float* __restrict__ psi,
-                                                  float* __restrict__ res,
-                                                  double* __restrict__ partials,
-                                                  unsigned int* __restrict__ counter,
-                                                  InvState* __restrict__ st,
-                                                  cudaGraphConditionalHandle handle,
-                                                  int use_handle) {
+// Two kernels share the work, launched in this order every body: GATHER = false runs the body
+// when the loop stops after it (an elementwise sweep, no gather), GATHER = true when the loop
+// goes on (update and next measurement in one sweep). Each decides from the loop state, which
+// only the kernel that runs changes (in its last block), so exactly one of them works; kept
+// apart, the elementwise sweep keeps the gather's register footprint out of its occupancy.
+template <bool GATHER>
+__global__ void __launch_bounds__(256, 4) k_inv_body(InvArgs a, const float* __restrict__ f,
+                                                     float* __restrict__ psi,
+                                                     float* __restrict__ res,
+                                                     double* __restrict__ partials,
+                                                     unsigned int* __restrict__ counter,
+                                                     InvState* __restrict__ st,
+                                                     cudaGraphConditionalHandle handle,
+                                                     int use_handle) {
     const int go = st->go;
-    if (!go) {  // uniform: the state only changes in the last block of this grid
+    if (!go) {  // uniform: the state only changes in the last block of the grid that works
         // keep a WHILE loop from spinning should its condition ever disagree with the state
         if (use_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
         return;
     }
     const int kb = st->k;
     const double mean = st->mean, mxe = st->max;
+    const bool next = (kb + 1 < st->max_iterations) && mxe > st->max_tol && mean > st->mean_tol;
+    if (next != GATHER) return;  // the other kernel of the pair runs this body
     const float eps = kb == 0 ? 0.75f : 0.5f;
     const float limit = eps * (float)mxe;
-    const bool next = (kb + 1 < st->max_iterations) && mxe > st->max_tol && mean > st->mean_tol;
     const bool enforce = st->enforce != 0;
     double sum = 0.0;
     float mx = 0.0f;
@@ -215,7 +222,7 @@ __global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __rest
             psi[l + a.ps_psi] = py[v];
             psi[l + 2 * a.ps_psi] = pz[v];
         }
-        if (next) {
+        if constexpr (GATHER) {
 #pragma unroll
             for (int v = 0; v < 2; ++v) {
                 if (!ok[v]) continue;
@@ -235,13 +242,13 @@ __global__ void __launch_bounds__(256) k_inv_body(InvArgs a, const float* __rest
     const double count = (double)a.g.n;
     reduce_and_finish(sum, mx, partials, counter, [&](double s, double m) {
         st->executed = kb + 1;
-        if (next) {
+        if (GATHER) {
             st->mean = s / count;
             st->max = m;
             st->k = kb + 1;
         }
-        st->go = next ? 1 : 0;
-        if (use_handle) cudaGraphSetConditional(handle, next ? 1u : 0u);
+        st->go = GATHER ? 1 : 0;
+        if (use_handle) cudaGraphSetConditional(handle, GATHER ? 1u : 0u);
     });
 }
 
@@ -319,9 +326,13 @@ int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse
                            InvState* st, cudaGraphConditionalHandle handle, int use_handle) {
     InvArgs a = inv_args(field, inverse);
     const unsigned int blocks = inv_blocks(ctx, a.g.n);
-    k_inv_body<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
-                                                ctx->d_scratch + SLOT_PARTIALS,
-                                                ctx->d_counter + 2, st, handle, use_handle);
+    k_inv_body<false><<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
+                                                       ctx->d_scratch + SLOT_PARTIALS,
+                                                       ctx->d_counter + 2, st, handle, use_handle);
+    FW_TRY(check_launch(ctx, "k_inv_body"));
+    k_inv_body<true><<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
+                                                      ctx->d_scratch + SLOT_PARTIALS,
+                                                      ctx->d_counter + 2, st, handle, use_handle);
     return check_launch(ctx, "k_inv_body");
 }
 

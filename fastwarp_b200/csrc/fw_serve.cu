@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/fastwarp_serve.h"
+#include "../../include/fastwarp_transform_io.h"
 #include "fw_internal.cuh"
 
 using Clock = std::chrono::steady_clock;
@@ -509,5 +510,8 @@ extern "C" size_t fw_abi_struct_size(const char* name) {
     if (n == "fw_syn_request") return sizeof(fw_syn_request);
     if (n == "fw_syn_result") return sizeof(fw_syn_result);
     if (n == "fw_server_stats") return sizeof(fw_server_stats);
+    if (n == "fw_cg_settings") return sizeof(fw_cg_settings);
+    if (n == "fw_cg_trace") return sizeof(fw_cg_trace);
+    if (n == "fw_transform_elem") return sizeof(fw_transform_elem);
     return 0;
 }

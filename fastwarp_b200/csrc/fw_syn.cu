@@ -860,10 +860,11 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
                 int k = (int)std::min<int64_t>(ran, cap - done);
                 FW_CUDA(cudaMemcpy(records + done, rs.d.trace + done, sizeof(fw_syn_iteration) * k,
                                    cudaMemcpyDeviceToHost));
-                // inversion bodies ran inside the graph: count them as launches
+                // inversion bodies ran inside the graph (two kernels each): count the launches
                 for (int q = 0; q < k; ++q)
                     for (int s = 0; s < 4; ++s)
-                        ctx->stats.kernel_launches += records[done + q].inversions[s].iterations;
+                        ctx->stats.kernel_launches +=
+                            2 * (uint64_t)records[done + q].inversions[s].iterations;
             }
             ctx->stats.kernel_launches +=
                 (uint64_t)ran * kernels_per_iteration(r, (fixed_mask ? 1 : 0) + (moving_mask ? 1 : 0)) + 1;
