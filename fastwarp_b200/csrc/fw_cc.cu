@@ -37,8 +37,8 @@ struct CcArgs {
 };
 
 // Shared-memory layout (dynamic): the z-window sums of every halo column, double-buffered by
-// slice, [ZB][5][HY*HX] double (+ [ZB][HY*HX] int counts with a mask); x sums [5][HY][TX] double
-// (+ [HY][TX] int counts); the raw voxels of the tile with a one-voxel halo for the last D
+// slice, [ZB][5][HY*HX] double (+ [ZB][HY*HX] int counts with a mask); y sums [5][TY][HX] double
+// (+ [TY][HX] int counts); the raw voxels of the tile with a one-voxel halo for the last D
 // slices, [D][TY+2][TX+2] float2 (f, m), for the centre values and the central differences;
 // block-reduction space.
 template <int R, int TY, bool MK>
@@ -48,14 +48,15 @@ struct Layout {
     static constexpr int HC = HX * HY;           // halo columns of the tile
     static constexpr int NT = TX * TY;
     static constexpr int CPT = (HC + NT - 1) / NT;  // halo columns per thread
+    static_assert(TY % 2 == 0, "the y pass makes output rows in pairs");
     static constexpr int NP = MK ? 4 : 3;  // block partials: cc, |dF|^2, |dM|^2 (+ valid voxels)
     static constexpr int RX = TX + 2, RY = TY + 2, RXY = RX * RY;
     // raw slices kept: the output at step k reads slices k-R-1 .. k-R+1, and slice k is written
     // before step k's first barrier, while slow threads may still read step k-1's outputs
     static constexpr int D = R + 3;
     static constexpr size_t zs1 = sizeof(double) * 5 * HC + (MK ? sizeof(int) * HC : 0);
-    static constexpr size_t xs_bytes = sizeof(double) * 5 * HY * TX;
-    static constexpr size_t xc_bytes = MK ? sizeof(int) * HY * TX : 0;
+    static constexpr size_t xs_bytes = sizeof(double) * 5 * TY * HX;  // y sums [5][TY][HX]
+    static constexpr size_t xc_bytes = MK ? sizeof(int) * TY * HX : 0;
     static constexpr size_t raw_bytes = sizeof(float2) * D * RXY;
     // two z-sum buffers (one barrier less per slice) when two CTAs still share an SM
     static constexpr int ZB = (2 * zs1 + xs_bytes + xc_bytes + raw_bytes) <= 110 * 1024 ? 2 : 1;
@@ -67,11 +68,14 @@ struct Layout {
 // valid voxels in the window, their outputs are zero and the value is the mean over the valid
 // voxels (result[3] receives their number; zero means no voxel in the masks).
 //
-// Pass order z, x, y. Each thread keeps the z-window sums of up to CPT halo columns in registers
+// Pass order z, y, x. Each thread keeps the z-window sums of up to CPT halo columns in registers
 // and moves them one slice per step: the entering slice is added and the leaving slice (read
 // again, from L2) subtracted. Products of float32 voxels are exact in float64, so the running
-// sums carry no drift beyond float64 rounding. The z sums go to shared memory, the x pass makes
-// row sums of them and each thread's y pass finishes its own voxel's six window sums.
+// sums carry no drift beyond float64 rounding. The z sums go to shared memory, the y pass makes
+// column sums of them two output rows at a time, and each thread's x pass finishes its own
+// voxel's window sums. The kernel is bound by shared-memory bandwidth, which this order spends
+// least on: the shared-tap pairs sit in the pass over the wider (halo) extent, and both passes
+// read along consecutive banks.
 #ifndef FW_CC_MIN_BLOCKS
 #define FW_CC_MIN_BLOCKS 2
 #endif
@@ -186,48 +190,50 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
                 if constexpr (MK) zc[s] = Zc[j];
             }
         }
-        __syncthreads();  // z sums visible; the previous y pass is done with the x sums
-        // x pass: each item makes the sums of two adjacent columns from one window of 2r + 2
-        // halo columns (the 2r in the middle are shared)
-        for (int s = tid; s < L::HY * (TX / 2); s += L::NT) {
-            const int hy = s / (TX / 2), cp = s - hy * (TX / 2);
-            const int base = hy * L::HX + 2 * cp;
-            double* o = xs + hy * TX + 2 * cp;
+        __syncthreads();  // z sums visible; the previous x pass is done with the y sums
+        // y pass: each item makes the sums of two adjacent output rows of one halo column from
+        // one window of 2r + 2 rows (the 2r in the middle are shared); a warp's items are
+        // consecutive columns, so its loads fall on distinct banks
+        for (int s = tid; s < L::HX * (TY / 2); s += L::NT) {
+            const int rp = s / L::HX, hx = s - rp * L::HX;
+            const int base = 2 * rp * L::HX + hx;
+            double* o = xs + 2 * rp * L::HX + hx;
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                const double* row = zs + q * L::HC + base;
+                const double* col = zs + q * L::HC + base;
                 double c = 0.0, e = 0.0;  // two partial sums: half-length add chains
 #pragma unroll
                 for (int t = 1; t <= 2 * R; t += 2) {
-                    c += row[t];
-                    e += row[t + 1];
+                    c += col[t * L::HX];
+                    e += col[(t + 1) * L::HX];
                 }
                 c += e;
-                *reinterpret_cast<double2*>(o + q * L::HY * TX) =
-                    make_double2(c + row[0], c + row[2 * R + 1]);
+                o[q * TY * L::HX] = c + col[0];
+                o[q * TY * L::HX + L::HX] = c + col[(2 * R + 1) * L::HX];
             }
             if constexpr (MK) {
-                const int* crow = zc + base;
+                const int* ccol = zc + base;
                 int cn = 0;
 #pragma unroll
-                for (int t = 1; t <= 2 * R; ++t) cn += crow[t];
-                xc[hy * TX + 2 * cp] = cn + crow[0];
-                xc[hy * TX + 2 * cp + 1] = cn + crow[2 * R + 1];
+                for (int t = 1; t <= 2 * R; ++t) cn += ccol[t * L::HX];
+                xc[2 * rp * L::HX + hx] = cn + ccol[0];
+                xc[(2 * rp + 1) * L::HX + hx] = cn + ccol[(2 * R + 1) * L::HX];
             }
         }
         __syncthreads();
         if (!own) continue;
-        // y pass for the thread's own column
+        // x pass for the thread's own voxel (a warp reads one row: consecutive banks)
         double S[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
+            const double* row = xs + (q * TY + ty) * L::HX + tx;
             double s = 0.0, s2 = 0.0;
 #pragma unroll
             for (int t = 0; t < 2 * R; t += 2) {
-                s += xs[(q * L::HY + ty + t) * TX + tx];
-                s2 += xs[(q * L::HY + ty + t + 1) * TX + tx];
+                s += row[t];
+                s2 += row[t + 1];
             }
-            S[q] = s + s2 + xs[(q * L::HY + ty + 2 * R) * TX + tx];
+            S[q] = s + s2 + row[2 * R];
         }
 
         // ---- output voxel (x, y, z) ----
@@ -241,7 +247,7 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
             }
             int Sc = 0;
 #pragma unroll
-            for (int t = 0; t <= 2 * R; ++t) Sc += xc[(ty + t) * TX + tx];
+            for (int t = 0; t <= 2 * R; ++t) Sc += xc[ty * L::HX + tx + t];
             cnt = (double)Sc;  // >= 1: the centre is valid
             acc_nv += 1.0;
         } else {

@@ -324,7 +324,9 @@ __global__ void __launch_bounds__(256) k_warp_t(WarpArgs a, int zchunk,
     const long long sxy = (long long)a.g.nx * a.g.ny;
     long long l = (long long)z0 * sxy + (long long)y * a.g.nx + x;
     float ux = u[l], uy = u[l + a.fps], uz = u[l + 2 * a.fps];
-    for (int k = z0; k < z1; ++k, l += sxy) {
+    const double xd = (double)x, yd = (double)y;  // converted once (the conversions are slow)
+    double kd = (double)z0;
+    for (int k = z0; k < z1; ++k, l += sxy, kd += 1.0) {
         float nx_ = 0.0f, ny_ = 0.0f, nz_ = 0.0f;
         if (k + 1 < z1) {
             nx_ = u[l + sxy];
@@ -334,7 +336,7 @@ __global__ void __launch_bounds__(256) k_warp_t(WarpArgs a, int zchunk,
         double c[3];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
-            c[r] = a.q[r * 3] * x + a.q[r * 3 + 1] * y + a.q[r * 3 + 2] * k + a.q0[r] +
+            c[r] = a.q[r * 3] * xd + a.q[r * 3 + 1] * yd + a.q[r * 3 + 2] * kd + a.q0[r] +
                    (a.r[r * 3] * ux + a.r[r * 3 + 1] * uy + a.r[r * 3 + 2] * uz);
         float v = 0.0f;
         if (inside_index(c[0], c[1], c[2], a.s.nx, a.s.ny, a.s.nz))

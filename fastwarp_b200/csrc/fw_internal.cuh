@@ -139,12 +139,22 @@ __device__ __forceinline__ bool inside_index(double cx, double cy, double cz, in
 
 // One axis of ITK's scalar linear interpolation: base clamped into the buffer, no weight when
 // the distance is not positive or the upper neighbour is past the last voxel.
+// The three cases keep the f64 subtraction of the clamped base exact without converting the base
+// back to f64 (one conversion fewer per axis).
 __device__ __forceinline__ void lin_axis(double c, int n, int& b, float& w) {
-    double fl = floor(c);
-    long long bb = fl < 0.0 ? 0 : (long long)fmin(fl, (double)(n - 1));
-    double d = c - (double)bb;
-    b = (int)bb;
-    w = (d <= 0.0 || bb + 1 > n - 1) ? 0.0f : (float)d;
+    const double fl = floor(c);
+    double d;
+    if (fl < 0.0) {  // clamped to the first voxel
+        b = 0;
+        d = c;
+    } else if (!(fl <= (double)(n - 1))) {  // clamped to the last (NaN too)
+        b = n - 1;
+        d = c - (double)(n - 1);
+    } else {
+        b = (int)fl;
+        d = c - fl;
+    }
+    w = (d <= 0.0 || b + 1 > n - 1) ? 0.0f : (float)d;
 }
 
 // interp.rs:43-85: LinearInterpolateImageFunction::EvaluateAtContinuousIndex (no bounds check).
