@@ -6,14 +6,14 @@
 // coefficient * grad(moving) by ITK's half-spacing central difference (interp.rs:96-120).
 //
 // Kernel design (sm_100a): one CTA owns a TX x TY column tile and marches along z over a chunk
-// of slices. The z window comes first, as running sums in registers over the tile's halo columns
-// (entering slice added, leaving slice subtracted); the x and y box passes then run in shared
-// memory on those sums. Sums are float64: products of float32 voxels are exact in float64, so
-// the centred second moments (sum f^2 - (sum f)^2 / n) keep their precision in flat bright
-// regions where float32 cancels. The window planes never touch HBM: the kernel reads the two
-// images (the leaving slice and the halo a second time, from L2) and writes the two derivative
-// fields. Shared memory holds only the z sums of one slice and the x sums, so several CTAs share
-// an SM and hide each other's float64 and load latency.
+// of slices. The z window comes first, as running sums over the tile's halo columns kept in
+// shared memory (entering slice added, leaving slice subtracted); the y and x box passes then run
+// on those sums. Sums are float64: products of float32 voxels are exact in float64, so the
+// centred second moments (sum f^2 - (sum f)^2 / n) keep their precision in flat bright regions
+// where float32 cancels. The window planes never touch HBM: the kernel reads the two images (the
+// leaving slice and the halo a second time, from L2) and writes the two derivative fields. Shared
+// memory holds the z sums, the y sums and a few raw slices (58 KB at r = 4), and 80 registers a
+// thread let three CTAs share an SM and hide each other's float64 and load latency.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -36,8 +36,8 @@ struct CcArgs {
     double isp[3];      // 1 / spacing (the central difference's denominator)
 };
 
-// Shared-memory layout (dynamic): the z-window sums of every halo column, double-buffered by
-// slice, [ZB][5][HY*HX] double (+ [ZB][HY*HX] int counts with a mask); y sums [5][TY][HX] double
+// Shared-memory layout (dynamic): the z-window sums of every halo column, [5][HY*HX] double
+// (+ [HY*HX] int counts with a mask); y sums [5][TY][HX] double
 // (+ [TY][HX] int counts); the raw voxels of the tile with a one-voxel halo for the last D
 // slices, [D][TY+2][TX+2] float2 (f, m), for the centre values and the central differences;
 // block-reduction space.
@@ -58,9 +58,7 @@ struct Layout {
     static constexpr size_t xs_bytes = sizeof(double) * 5 * TY * HX;  // y sums [5][TY][HX]
     static constexpr size_t xc_bytes = MK ? sizeof(int) * TY * HX : 0;
     static constexpr size_t raw_bytes = sizeof(float2) * D * RXY;
-    // two z-sum buffers (one barrier less per slice) when two CTAs still share an SM
-    static constexpr int ZB = (2 * zs1 + xs_bytes + xc_bytes + raw_bytes) <= 110 * 1024 ? 2 : 1;
-    static constexpr size_t bytes = ZB * zs1 + xs_bytes + xc_bytes + raw_bytes + 64 * sizeof(double);
+    static constexpr size_t bytes = zs1 + xs_bytes + xc_bytes + raw_bytes + 64 * sizeof(double);
 };
 
 // MK: masked (cpu/mod.rs:134-163 -> evaluate_masked with Some(valid)): a voxel counts only where
@@ -68,16 +66,17 @@ struct Layout {
 // valid voxels in the window, their outputs are zero and the value is the mean over the valid
 // voxels (result[3] receives their number; zero means no voxel in the masks).
 //
-// Pass order z, y, x. Each thread keeps the z-window sums of up to CPT halo columns in registers
-// and moves them one slice per step: the entering slice is added and the leaving slice (read
-// again, from L2) subtracted. Products of float32 voxels are exact in float64, so the running
-// sums carry no drift beyond float64 rounding. The z sums go to shared memory, the y pass makes
-// column sums of them two output rows at a time, and each thread's x pass finishes its own
+// Pass order z, y, x. Each thread owns up to CPT halo columns and moves their z-window sums (in
+// shared memory, where the y pass reads them) one slice per step: the entering slice is added
+// and the leaving slice (read again, from L2) subtracted -- before the step's first barrier, which
+// the previous step's y pass has passed. Products of float32 voxels are exact in float64, so the
+// running sums carry no drift beyond float64 rounding. The y pass makes column sums of them two
+// output rows at a time, and each thread's x pass finishes its own
 // voxel's window sums. The kernel is bound by shared-memory bandwidth, which this order spends
 // least on: the shared-tap pairs sit in the pass over the wider (halo) extent, and both passes
 // read along consecutive banks.
 #ifndef FW_CC_MIN_BLOCKS
-#define FW_CC_MIN_BLOCKS 2
+#define FW_CC_MIN_BLOCKS 3
 #endif
 
 template <int R, int TY, bool MK>
@@ -91,10 +90,10 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
                                                      double* __restrict__ result, int want_norms) {
     using L = Layout<R, TY, MK>;
     extern __shared__ __align__(16) unsigned char smem[];
-    double* xs = reinterpret_cast<double*>(smem + L::ZB * L::zs1);
-    int* xc = reinterpret_cast<int*>(smem + L::ZB * L::zs1 + L::xs_bytes);
-    float2* raw = reinterpret_cast<float2*>(smem + L::ZB * L::zs1 + L::xs_bytes + L::xc_bytes);
-    double* red = reinterpret_cast<double*>(smem + L::ZB * L::zs1 + L::xs_bytes + L::xc_bytes +
+    double* xs = reinterpret_cast<double*>(smem + L::zs1);
+    int* xc = reinterpret_cast<int*>(smem + L::zs1 + L::xs_bytes);
+    float2* raw = reinterpret_cast<float2*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes);
+    double* red = reinterpret_cast<double*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes +
                                             L::raw_bytes);
 
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
@@ -115,8 +114,8 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
     // the thread's halo columns: offset inside a slice, -1 outside the image (sums stay zero)
     // and, for columns within one voxel of the tile, their slot in a raw slice (-1 otherwise)
     int coff[L::CPT], ridx[L::CPT];
-    double Z[L::CPT][5];
-    int Zc[L::CPT];
+    double* zs = reinterpret_cast<double*>(smem);
+    int* zc = reinterpret_cast<int*>(zs + 5 * L::HC);
 #pragma unroll
     for (int j = 0; j < L::CPT; ++j) {
         const int s = tid + j * L::NT;
@@ -129,9 +128,11 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
             const int rx = hx - (R - 1), ry = hy - (R - 1);
             if (rx >= 0 && rx < L::RX && ry >= 0 && ry < L::RY) ridx[j] = ry * L::RX + rx;
         }
+        if (s < L::HC) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Z[j][q] = 0.0;
-        Zc[j] = 0;
+            for (int q = 0; q < 5; ++q) zs[q * L::HC + s] = 0.0;
+            if constexpr (MK) zc[s] = 0;
+        }
     }
     // entering slice k and leaving slice k - 2R - 1 of the next step, in flight during a step
     float2 pin[L::CPT], pout[L::CPT];
@@ -155,7 +156,6 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
         }
     };
     fetch(kb);
-    int buf = 0;
     for (int k = kb; k < z1 + R; ++k) {
         // z step: add slice k (if it exists), drop slice k - 2R - 1 (if it was added)
         float2* rslot = raw + (k % L::D) * L::RXY;
@@ -166,30 +166,21 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
             if constexpr (MK)
                 if (!vin[j]) a = make_float2(0.0f, 0.0f);  // a masked-out voxel adds nothing
             const double f = a.x, m = a.y, g = pout[j].x, n = pout[j].y;
-            Z[j][0] += f - g;
-            Z[j][1] += m - n;
-            Z[j][2] += f * f - g * g;
-            Z[j][3] += m * m - n * n;
-            Z[j][4] += f * m - g * n;
-            if constexpr (MK) Zc[j] += (int)vin[j] - (int)vout[j];
+            const int s = tid + j * L::NT;
+            if (s < L::HC) {
+                double* zq = zs + s;
+                zq[0] += f - g;
+                zq[L::HC] += m - n;
+                zq[2 * L::HC] += f * f - g * g;
+                zq[3 * L::HC] += m * m - n * n;
+                zq[4 * L::HC] += f * m - g * n;
+                if constexpr (MK) zc[s] += (int)vin[j] - (int)vout[j];
+            }
         }
         if (k + 1 < z1 + R) fetch(k + 1);
         const int z = k - R;
         if (z < z0) continue;  // the window is still filling (uniform across the CTA)
 
-        double* zs = reinterpret_cast<double*>(smem + buf * L::zs1);
-        int* zc = reinterpret_cast<int*>(zs + 5 * L::HC);
-        buf ^= (L::ZB - 1);
-        if constexpr (L::ZB == 1) __syncthreads();  // the previous x pass is done with zs
-#pragma unroll
-        for (int j = 0; j < L::CPT; ++j) {
-            const int s = tid + j * L::NT;
-            if (s < L::HC) {
-#pragma unroll
-                for (int q = 0; q < 5; ++q) zs[q * L::HC + s] = Z[j][q];
-                if constexpr (MK) zc[s] = Zc[j];
-            }
-        }
         __syncthreads();  // z sums visible; the previous x pass is done with the y sums
         // y pass: each item makes the sums of two adjacent output rows of one halo column from
         // one window of 2r + 2 rows (the 2r in the middle are shared); a warp's items are
