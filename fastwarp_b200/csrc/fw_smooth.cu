@@ -226,15 +226,31 @@ __global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* 
     const int x0 = blockIdx.x * XY_T, y0 = blockIdx.y * XY_T;
     const long long zoff = (long long)blockIdx.z * nx * ny;
     const int x = x0 + tx;
-    for (int s = tid; s < HY * HX; s += XY_NT) {
-        const int hy = s / HX, hx = s - hy * HX;
-        const int gx = min(max(x0 - R + hx, 0), nx - 1);  // edge replication
-        const int gy = min(max(y0 - R + hy, 0), ny - 1);
-        const float* src = in + zoff + (long long)gy * nx + gx;
-        const float v0 = __ldg(src), v1 = __ldg(src + a.ps_in), v2 = __ldg(src + 2 * a.ps_in);
-        tile[hy * HXP + hx] = v0;
-        tile[TILE + hy * HXP + hx] = v1;
-        tile[2 * TILE + hy * HXP + hx] = v2;
+    static_assert(HX <= 64, "a lane loads two halo columns");
+    {
+        // halo rows by warps: lane l loads halo columns l and l + 32 (edge replication)
+        const int warp = tid >> 5;
+        const int gxa = min(max(x0 - R + tx, 0), nx - 1);
+        const int gxb = min(max(x0 - R + tx + 32, 0), nx - 1);
+        const bool second = tx + 32 < HX;
+        const float* plane = in + zoff;
+        for (int hy = warp; hy < HY; hy += XY_NT / 32) {
+            const int gy = min(max(y0 - R + hy, 0), ny - 1);
+            const float* rowp = plane + (long long)gy * nx;
+            const float v0 = __ldg(rowp + gxa), v1 = __ldg(rowp + gxa + a.ps_in),
+                        v2 = __ldg(rowp + gxa + 2 * a.ps_in);
+            float* t = tile + hy * HXP + tx;
+            t[0] = v0;
+            t[TILE] = v1;
+            t[2 * TILE] = v2;
+            if (second) {
+                const float w0 = __ldg(rowp + gxb), w1 = __ldg(rowp + gxb + a.ps_in),
+                            w2 = __ldg(rowp + gxb + 2 * a.ps_in);
+                t[32] = w0;
+                t[TILE + 32] = w1;
+                t[2 * TILE + 32] = w2;
+            }
+        }
     }
     __syncthreads();
     // x pass: (component, halo row, group of four output columns)
