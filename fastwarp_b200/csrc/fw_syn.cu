@@ -34,6 +34,7 @@ namespace {
 constexpr int MAX_WINDOW = 64;
 
 struct SynDev {
+    int done;        // iterations recorded over all levels (the trace's write position)
     int it;          // iterations done in this level
     int limit;       // iteration limit of this level
     int converged;
@@ -85,15 +86,18 @@ __device__ double convergence_value(const SynDev& s) {
     return phi[0] - phi[1];
 }
 
-__global__ void k_syn_level_init(SynDev* s, int level, int limit) {
+// A level whose run is enqueued behind a failed one (the status is kept from level to level)
+// runs no iteration: the host reads the status once, after the last level.
+__global__ void k_syn_level_init(SynDev* s, int level, int limit,
+                                 cudaGraphConditionalHandle handle, int use_handle) {
     s->it = 0;
-    s->limit = limit;
+    s->limit = s->status == 0 ? limit : 0;
     s->converged = 0;
-    s->status = 0;
     s->level = level;
     s->count = 0;
     s->head = 0;
     s->total = 0.0;
+    if (use_handle) cudaGraphSetConditional(handle, s->limit > 0 ? 1u : 0u);
 }
 
 // Per-channel scalars, CC_STRIDE doubles a channel: [value (fixed, moving), |dF|^2, |dM|^2,
@@ -146,8 +150,8 @@ __global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
     s->total += fabs(energy);
     double cv = convergence_value(*s);
     if (cv < s->threshold) s->converged = 1;
-    int it = s->it;
-    if (it < trace_cap) {
+    int it = s->it, rec = s->done;
+    if (rec < trace_cap) {
         fw_syn_iteration r;
         r.level = s->level;
         r.energy = energy;
@@ -160,9 +164,10 @@ __global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
             r.inversions[q].mean_error_norm = inv[q].executed ? inv[q].mean : 0.0;
             r.inversions[q].max_error_norm = inv[q].executed ? inv[q].max : 0.0;
         }
-        trace[it] = r;
+        trace[rec] = r;
     }
     s->it = it + 1;
+    s->done = rec + 1;
     if (cancel && *cancel) s->status = 3;
     int more = (s->it < s->limit) && !s->converged && s->status == 0;
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
@@ -275,18 +280,16 @@ struct RunDev {
 
 const fw_invert_params kSynInvert = {20, 0.001, 0.1, 1};
 
-// Adds a WHILE node at the capture position of `s` and returns its body graph.
-int add_while(cudaStream_t s, unsigned int default_value, unsigned int flags,
-              cudaGraphConditionalHandle* handle, cudaGraph_t* body) {
+// Adds a WHILE node on an existing handle at the capture position of `s`.
+int add_while_node(cudaStream_t s, cudaGraphConditionalHandle handle, cudaGraph_t* body) {
     cudaStreamCaptureStatus status;
     cudaGraph_t g;
     const cudaGraphNode_t* deps;
     size_t ndeps;
     FW_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, &g, &deps, &ndeps));
     FW_CHECK(status == cudaStreamCaptureStatusActive, "graph capture is not active");
-    FW_CUDA(cudaGraphConditionalHandleCreate(handle, g, default_value, flags));
     cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
-    p.conditional.handle = *handle;
+    p.conditional.handle = handle;
     p.conditional.type = cudaGraphCondTypeWhile;
     p.conditional.size = 1;
     cudaGraphNode_t node;
@@ -613,7 +616,7 @@ int run_level_direct(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
                      const std::vector<const fw_image*>& fs, const std::vector<const fw_image*>& ms,
                      const fw_affine* initial, const RunDev& d, int level, int limit,
                      fw_syn_iteration* trace_dev_base) {
-    k_syn_level_init<<<1, 1, 0, ctx->stream>>>(d.syn, level, limit);
+    k_syn_level_init<<<1, 1, 0, ctx->stream>>>(d.syn, level, limit, 0, 0);
     FW_TRY(check_launch(ctx, "k_syn_level_init"));
     for (int it = 0; it < limit; ++it) {
         if (ctx->cancel && *ctx->cancel) return fail(FW_ERR_CANCELLED, "registration cancelled");
@@ -637,16 +640,20 @@ int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
                     fw_syn_iteration* trace_dev_base) {
     GraphGuard G;
     const double t0 = tracing() ? now_ms() : 0.0;
+    const uint64_t launches0 = ctx->stats.kernel_launches;  // captured kernels are not launches
     FW_CUDA(cudaGraphCreate(&G.g, 0));
+    // the iteration loop's condition: set by the level init (no iteration after a failed level)
+    // and then by the record kernel at the end of every iteration
+    cudaGraphConditionalHandle h_it = 0;
+    FW_CUDA(cudaGraphConditionalHandleCreate(&h_it, G.g, 0, 0));
     FW_CUDA(cudaStreamBeginCaptureToGraph(ctx->stream, G.g, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
     ctx->capturing = true;
     int rc = 0;
-    cudaGraphConditionalHandle h_it = 0;
     cudaGraph_t body = nullptr;
-    k_syn_level_init<<<1, 1, 0, ctx->stream>>>(d.syn, level, limit);
+    k_syn_level_init<<<1, 1, 0, ctx->stream>>>(d.syn, level, limit, h_it, 1);
     rc = check_launch(ctx, "k_syn_level_init");
-    if (!rc) rc = add_while(ctx->stream, limit > 0 ? 1u : 0u, cudaGraphCondAssignDefault, &h_it, &body);
+    if (!rc) rc = add_while_node(ctx->stream, h_it, &body);
     cudaGraph_t top;
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &top);
     if (!rc && e != cudaSuccess) rc = cuda_fail(e, "level graph capture");
@@ -667,6 +674,7 @@ int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
         }
     }
     ctx->capturing = false;
+    ctx->stats.kernel_launches = launches0;
     if (rc) {
         cudaGetLastError();
         return rc;
@@ -674,13 +682,15 @@ int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
     const double t1 = tracing() ? now_ms() : 0.0;
     FW_CUDA(cudaGraphInstantiate(&G.e, G.g, 0));
     const double t2 = tracing() ? now_ms() : 0.0;
+    // launched without a wait: the next level's pyramid, fields and graph are enqueued behind it
+    // while it runs (the executable graph is released when it completes)
     FW_CUDA(cudaGraphLaunch(G.e, ctx->stream));
     ctx->stats.graph_launches++;
-    int rc2 = sync(ctx);
     if (tracing())
-        std::fprintf(stderr, "[fastwarp] level %d (%lld voxels): capture %.2f ms, instantiate %.2f ms, "
-                     "run %.2f ms\n", level, (long long)L.grid.count(), t1 - t0, t2 - t1, now_ms() - t2);
-    return rc2;
+        std::fprintf(stderr, "[fastwarp] level %d (%lld voxels): capture %.2f ms, instantiate %.2f ms "
+                     "(host, overlapping the device)\n", level, (long long)L.grid.count(), t1 - t0,
+                     t2 - t1);
+    return 0;
 }
 
 int check_status(int status, bool masked) {
@@ -779,11 +789,14 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
     };
     int rc = 0;
     int done = 0;
+    const bool graphs = use_graphs();
+    int graph_levels = 0;
     for (int level = 0; level < r->levels && !rc; ++level) {
         if (ctx->cancel && *ctx->cancel) {
             rc = fail(FW_ERR_CANCELLED, "registration cancelled");
             break;
         }
+        const double t_level = tracing() ? now_ms() : 0.0;
         HostGrid lg;
         rc = level_grid(r, fg, level, lg);
         if (rc) break;
@@ -839,39 +852,62 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
         L.grid = lg;
         prev = lg;
         have_prev = true;
+        const double t_fields = tracing() ? now_ms() : 0.0;
         free_level_work(L);
         rc = alloc_level_work(ctx, r, L);
         if (rc) break;
+        if (tracing())
+            std::fprintf(stderr, "[fastwarp] level %d: pyramid and state fields %.2f ms, work buffers "
+                         "%.2f ms (host)\n", level, t_fields - t_level, now_ms() - t_fields);
         int limit = (int)r->iterations[level];
         if (limit > 0) {
-            if (use_graphs())
-                rc = run_level_graph(ctx, r, L, fs, ms, initial, rs.d, level, limit, rs.d.trace + done);
-            else
-                rc = run_level_direct(ctx, r, L, fs, ms, initial, rs.d, level, limit, rs.d.trace + done);
+            if (graphs) {
+                // enqueued behind the previous level without waiting for it
+                rc = run_level_graph(ctx, r, L, fs, ms, initial, rs.d, level, limit, rs.d.trace);
+                if (rc) break;
+                ++graph_levels;
+                continue;
+            }
+            rc = run_level_direct(ctx, r, L, fs, ms, initial, rs.d, level, limit, rs.d.trace);
             if (rc) break;
-            // the level's records and the device status
+            // the level's status, read after every level (the host drives the loop)
             SynDev h;
             FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, rs.d.syn, sizeof(SynDev), cudaMemcpyDeviceToHost, ctx->stream));
             rc = sync(ctx);
             if (rc) break;
             std::memcpy(&h, ctx->h_pinned, sizeof(h));
-            int ran = h.it;
-            if (records && done < cap) {
-                int k = (int)std::min<int64_t>(ran, cap - done);
-                FW_CUDA(cudaMemcpy(records + done, rs.d.trace + done, sizeof(fw_syn_iteration) * k,
-                                   cudaMemcpyDeviceToHost));
-                // inversion bodies ran inside the graph (two kernels each): count the launches
-                for (int q = 0; q < k; ++q)
-                    for (int s = 0; s < 4; ++s)
-                        ctx->stats.kernel_launches +=
-                            2 * (uint64_t)records[done + q].inversions[s].iterations;
-            }
-            ctx->stats.kernel_launches +=
-                (uint64_t)ran * kernels_per_iteration(r, (fixed_mask ? 1 : 0) + (moving_mask ? 1 : 0)) + 1;
-            done += ran;
             rc = check_status(h.status, fixed_mask || moving_mask);
         }
     }
+    // the records of every level and the final status: one read-back after the last level
+    if (!rc) {
+        SynDev h;
+        FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, rs.d.syn, sizeof(SynDev), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        rc = sync(ctx);
+        if (!rc) {
+            std::memcpy(&h, ctx->h_pinned, sizeof(h));
+            done = std::min(h.done, std::max(total_iters, 1));
+            std::vector<fw_syn_iteration> all((size_t)std::max(done, 1));
+            if (done > 0)
+                FW_CUDA(cudaMemcpy(all.data(), rs.d.trace, sizeof(fw_syn_iteration) * done,
+                                   cudaMemcpyDeviceToHost));
+            // the kernels the level graphs ran (direct launches are counted as they are made):
+            // every iteration's kernels, two per inversion body, one level init per level
+            for (int q = 0; q < done && graphs; ++q) {
+                for (int s = 0; s < 4; ++s)
+                    ctx->stats.kernel_launches += 2 * (uint64_t)all[q].inversions[s].iterations;
+                ctx->stats.kernel_launches +=
+                    kernels_per_iteration(r, (fixed_mask ? 1 : 0) + (moving_mask ? 1 : 0));
+            }
+            if (graphs) ctx->stats.kernel_launches += (uint64_t)graph_levels;
+            if (records && cap > 0)
+                std::memcpy(records, all.data(),
+                            sizeof(fw_syn_iteration) * (size_t)std::min<int64_t>(done, cap));
+            rc = check_status(h.status, fixed_mask || moving_mask);
+        }
+    }
+    const double t_end = tracing() ? now_ms() : 0.0;
     free_level_work(L);
     free_owned();
     if (!rc) {
@@ -893,8 +929,8 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
     free_state();
     if (count) *count = done;
     if (tracing())
-        std::fprintf(stderr, "[fastwarp] registration: %d iterations, %.2f ms on the host\n", done,
-                     now_ms() - t_start);
+        std::fprintf(stderr, "[fastwarp] registration: %d iterations, %.2f ms on the host "
+                     "(final composition %.2f ms)\n", done, now_ms() - t_start, now_ms() - t_end);
     return rc;
 }
 
@@ -966,7 +1002,7 @@ int fw_syn_step_masked(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image*
     if (!rc) rc = upload_syn_dev(ctx, recipe, rs.d.syn, fixed_mask || moving_mask);
     std::vector<const fw_image*> fs(fixed, fixed + L.channels), ms(moving, moving + L.channels);
     if (!rc) {
-        k_syn_level_init<<<1, 1, 0, ctx->stream>>>(rs.d.syn, 0, 1);
+        k_syn_level_init<<<1, 1, 0, ctx->stream>>>(rs.d.syn, 0, 1, 0, 0);
         rc = check_launch(ctx, "k_syn_level_init");
     }
     if (!rc) rc = enqueue_iteration(ctx, false, recipe, L, fs, ms, initial, rs.d);
