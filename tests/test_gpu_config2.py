@@ -1,0 +1,97 @@
+"""Config 2 at full size and the shape of config 4, against the f64 oracle.
+
+Config 2 is the benchmark's own workload: the 193 x 229 x 193 head phantom at 1 mm with its
+initial affine (the rigid + affine part of the phantom's map), CC r = 4. One SyN step of the
+finest level is checked at full size from a deformed state (three GPU steps from zero, downloaded
+and handed to both engines): 1e-5 relative on the CC energy, 1e-4 voxel on both update fields
+(the oracle takes a few seconds for one step at 8.5 M voxels on the host cores).
+
+Config 4 registers subjects of their own grids to one template with two channels (T1-like, and
+T2-like with inverted contrast). Its shape in miniature: two channels, a moving grid whose size,
+spacing and origin all differ from the fixed grid's, a two-level pyramid; the full registration
+matches the oracle to 0.05 mm RMS and 1e-4 relative final energy.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from fastwarp_b200 import SynRecipe, make_grid, run_syn, syn_step
+from fastwarp_b200.phantoms import blob_pair, head_pair
+
+pytestmark = pytest.mark.gpu
+
+
+def ogrid(g):
+    return O.make_grid(tuple(g.size), tuple(g.spacing), tuple(g.origin),
+                       np.array(g.direction[:]).reshape(3, 3))
+
+
+def oaffine(a):
+    return O.make_affine(np.array(a.matrix[:]).reshape(3, 3), tuple(a.offset[:]))
+
+
+def test_one_full_size_config2_step_matches_the_oracle(backend):
+    g, fixed, mg, moving, initial = head_pair()
+    r = SynRecipe(gradient_step=0.1, update_field_variance=3.0, total_field_variance=0.0,
+                  cc_radius=4, iterations=[1], shrink_factors=[1], smoothing_sigmas=[0.0],
+                  convergence_threshold=-1.0)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(mg, moving)
+    state = {k: backend.zero_field(g) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    for _ in range(3):
+        syn_step(backend, r, [fi], [mi], initial, state, want_updates=False)
+    ostate = {k: backend.download_field(v).astype(np.float64) for k, v in state.items()}
+    assert max(np.abs(v).max() for v in ostate.values()) > 0.1  # a deformed state
+    rec, fu, mu = syn_step(backend, r, [fi], [mi], initial, state)
+    orec, ofu, omu = O.syn_step(
+        O.syn_recipe(0.1, 3.0, 0.0, 4, (1,), (1,), (0.0,), False, -1.0, 10, (1.0,)),
+        ogrid(g), ogrid(g), [fixed.astype(np.float64)], ogrid(mg), [moving.astype(np.float64)],
+        oaffine(initial), ostate)
+    assert abs(rec["energy"] - orec.energy) <= 1e-5 * abs(orec.energy), (rec["energy"], orec.energy)
+    assert np.abs(fu - ofu).max() <= 1e-4
+    assert np.abs(mu - omu).max() <= 1e-4
+
+
+def resample(img, grid_from, grid_to):
+    """Trilinear samples of `img` (on grid_from, identity direction) at grid_to's voxel centres."""
+    nx, ny, nz = grid_to.size
+    sp, org = np.array(grid_to.spacing[:]), np.array(grid_to.origin[:])
+    spf, orgf = np.array(grid_from.spacing[:]), np.array(grid_from.origin[:])
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    c = [(org[a] + sp[a] * v - orgf[a]) / spf[a] for a, v in enumerate((x, y, z))]
+    src = img.astype(np.float64)
+    n = src.shape[::-1]
+    i0 = [np.clip(np.floor(cc).astype(int), 0, n[a] - 1) for a, cc in enumerate(c)]
+    i1 = [np.clip(i + 1, 0, n[a] - 1) for a, i in enumerate(i0)]
+    w = [np.clip(cc - i, 0.0, 1.0) for cc, i in zip(c, i0)]
+    out = np.zeros(z.shape)
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                ix = i1[0] if dx else i0[0]
+                iy = i1[1] if dy else i0[1]
+                iz = i1[2] if dz else i0[2]
+                wt = (w[0] if dx else 1 - w[0]) * (w[1] if dy else 1 - w[1]) * \
+                     (w[2] if dz else 1 - w[2])
+                out += wt * src[iz, iy, ix]
+    return out.astype(np.float32)
+
+
+def test_two_channels_on_their_own_moving_grid_match_the_oracle(backend):
+    g, fixed, moving = blob_pair(40, seed=404)
+    mg = make_grid((36, 44, 38), (1.1, 0.9, 1.05), (-1.5, 1.0, -0.5))
+    m1 = resample(moving, g, mg)
+    f2, m2 = (1.0 - fixed).astype(np.float32), (1.0 - m1).astype(np.float32)  # T2-like
+    r = SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2, iterations=[6, 5],
+                  shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0], convergence_threshold=-1.0,
+                  channel_weights=[0.5, 0.5])
+    res = run_syn(backend, r, g, [fixed, f2], mg, [m1, m2])
+    orec = O.syn_recipe(0.25, 3.0, 0.0, 2, (6, 5), (2, 1), (1.0, 0.0), False, -1.0, 10,
+                        (0.5, 0.5))
+    ow, oinv, orecs, _ = O.syn_run(orec, ogrid(g), [fixed, f2], ogrid(mg), [m1, m2])
+    assert len(res.iterations) == len(orecs) == 11
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    rms_inv = np.sqrt(((res.inverse_warp.astype(np.float64) - oinv) ** 2).sum(-1).mean())
+    assert rms <= 0.05 and rms_inv <= 0.05, (rms, rms_inv)
+    assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
+    last = [it["energy"] for it in res.iterations if it["level"] == 1]
+    assert last[-1] < last[0]  # the energy falls within a level (levels are not comparable)
