@@ -97,12 +97,14 @@ __device__ void reduce_and_finish(double sum, float mx, double* __restrict__ par
 
 // First measurement (body 0's error) of psi against f; the residual e = psi + f(x + psi) of
 // every voxel is kept in `res` for the body that follows.
+// Its last block also writes the loop's settings into the state (no separate init launch).
 __global__ void __launch_bounds__(256, 4) k_inv_measure(InvArgs a, const float* __restrict__ f,
                                                      const float* __restrict__ psi,
                                                      float* __restrict__ res,
                                                      double* __restrict__ partials,
                                                      unsigned int* __restrict__ counter,
                                                      InvState* __restrict__ st,
+                                                     fw_invert_params prm,
                                                      cudaGraphConditionalHandle handle,
                                                      int use_handle) {
     double sum = 0.0;
@@ -137,11 +139,15 @@ __global__ void __launch_bounds__(256, 4) k_inv_measure(InvArgs a, const float* 
     }
     const double count = (double)a.g.n;
     reduce_and_finish(sum, mx, partials, counter, [&](double s, double m) {
+        st->max_iterations = prm.max_iterations;
+        st->mean_tol = prm.mean_error_tolerance;
+        st->max_tol = prm.max_error_tolerance;
+        st->enforce = prm.enforce_boundary_condition;
         st->mean = s / count;
         st->max = m;
         st->executed = 0;
         st->k = 0;
-        st->go = st->max_iterations > 0 ? 1 : 0;
+        st->go = prm.max_iterations > 0 ? 1 : 0;
         if (use_handle) cudaGraphSetConditional(handle, st->go ? 1u : 0u);
     });
 }
@@ -252,18 +258,6 @@ __global__ void __launch_bounds__(256, 4) k_inv_body(InvArgs a, const float* __r
     });
 }
 
-__global__ void k_inv_init(InvState* st, fw_invert_params p) {
-    st->mean = DBL_MAX;
-    st->max = DBL_MAX;
-    st->executed = 0;
-    st->k = 0;
-    st->go = 0;
-    st->max_iterations = p.max_iterations;
-    st->mean_tol = p.mean_error_tolerance;
-    st->max_tol = p.max_error_tolerance;
-    st->enforce = p.enforce_boundary_condition;
-}
-
 // Re-arms a finished loop for one more body from its last measurement (kernel timing).
 __global__ void k_inv_rearm(InvState* st, int max_iterations) {
     st->go = 1;
@@ -314,11 +308,9 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
     const size_t parts = std::max<size_t>((size_t)blocks.x * blocks.y * blocks.z,
                                           inv_blocks(ctx, a.g.n));
     FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 2 * parts + 16));
-    k_inv_init<<<1, 1, 0, ctx->stream>>>(st, prm);
-    FW_TRY(check_launch(ctx, "k_inv_init"));
     k_inv_measure<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
                                                    ctx->d_scratch + SLOT_PARTIALS,
-                                                   ctx->d_counter + 2, st, handle, use_handle);
+                                                   ctx->d_counter + 2, st, prm, handle, use_handle);
     return check_launch(ctx, "k_inv_measure");
 }
 

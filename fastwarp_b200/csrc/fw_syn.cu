@@ -709,7 +709,7 @@ int check_status(int status, bool masked) {
 int kernels_per_iteration(const fw_syn_recipe* r, int mask_warps) {
     int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) +
             4 /*two-pass smoothing or max*/ + 2 /*compose*/ +
-            (r->total_field_variance > 0.0 ? 4 : 0) + 4 * 2 /*inv init+measure*/ + 1 /*record*/ +
+            (r->total_field_variance > 0.0 ? 4 : 0) + 4 /*inversion measures*/ + 1 /*record*/ +
             mask_warps + (mask_warps == 2 ? 1 : 0) /*product*/;
     for (int c = 0; c < r->channels; ++c)
         if (r->channel_metrics[c] == FW_METRIC_MATTES) k += 6;  // 7 dense MI kernels, not 1 CC
