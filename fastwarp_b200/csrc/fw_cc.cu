@@ -553,10 +553,10 @@ int fw_cc_value_derivative(fw_ctx* ctx, const fw_image* fixed, const fw_image* m
 
 // ---- allocation-free variant of the CC pair ---------------------------------------------------
 //
-// For callers that cannot allocate device memory: code that records its work inside a CUDA
-// stream capture (allocating there breaks the capture), hosts that hand every byte of the GPU to
+// For callers that cannot allocate device memory: hosts that hand every byte of the GPU to
 // their own pool allocator (a deep-learning framework's caching allocator, a serving process
-// with a fixed HBM budget) and real-time pipelines that plan all memory before they start. The
+// with a fixed HBM budget), plug-ins that get only the buffers such a host gives them, and
+// real-time pipelines that plan all memory before they start. The
 // caller passes the images, the two derivative fields and a 3-double result on the device; the
 // kernel's only scratch -- the block partials and the last-block counter -- lives in the
 // file-scope array below, which every GPU that loads this library holds until the process exits.

@@ -282,9 +282,10 @@ int fw_mi_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* f
                                                   fw_field** d_moving, double norms[2]);
 
 /* No counterpart in the reference. The CC pair above for callers that cannot allocate device
- * memory: code recording into a CUDA stream capture (an allocation there breaks the capture),
- * hosts whose own pool allocator owns the GPU's memory (a framework's caching allocator, a server
- * under a fixed HBM budget) and real-time pipelines that plan all memory up front. This call
+ * memory: hosts whose own pool allocator owns the GPU's memory (a framework's caching allocator
+ * that must see every byte, a server under a fixed HBM budget), plug-ins that run inside such a
+ * host and get only the buffers it hands them, and real-time pipelines that plan all memory up
+ * front and may not allocate once running. This call
  * allocates nothing and needs no context: `fixed` and `moving` are float32 device images on
  * `grid`, `d_fixed` / `d_moving` receive the two derivative fields as three float32 planes of
  * `plane_stride` (>= voxel count) floats, and `result` (device, 3 doubles) receives the value,

@@ -1,9 +1,9 @@
 """The allocation-free CC pair entry point against the ordinary one, through the C ABI.
 
-fw_cc_value_derivative_pair_noalloc serves callers that cannot allocate device memory (work
-recorded inside a CUDA stream capture, hosts whose own pool allocator owns the GPU, real-time
-pipelines with pre-planned memory): they pass every input and output, and the kernel's scratch is
-a static array inside the library. This file runs after every other test (pytest collects it
+fw_cc_value_derivative_pair_noalloc serves callers that cannot allocate device memory (hosts
+whose own pool allocator owns the GPU, plug-ins handed only their buffers, real-time pipelines
+with pre-planned memory): they pass every input and output, and the kernel's scratch is a static
+array inside the library. This file runs after every other test (pytest collects it
 last) and also passes alone in a fresh process.
 """
 import ctypes as C
