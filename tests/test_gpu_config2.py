@@ -4,7 +4,9 @@ Config 2 is the benchmark's own workload: the 193 x 229 x 193 head phantom at 1 
 initial affine (the rigid + affine part of the phantom's map), CC r = 4. One SyN step of the
 finest level is checked at full size from a deformed state (three GPU steps from zero, downloaded
 and handed to both engines): 1e-5 relative on the CC energy, 1e-4 voxel on both update fields
-(the oracle takes a few seconds for one step at 8.5 M voxels on the host cores).
+(the oracle takes a few seconds for one step at 8.5 M voxels on the host cores). The whole
+registration (all 140 iterations of the three levels) is checked too: 0.05 mm RMS on both fields
+and 1e-4 relative final energy (about a minute and a half of oracle time).
 
 Config 4 registers subjects of their own grids to one template with two channels (T1-like, and
 T2-like with inverted contrast). Its shape in miniature: two channels, a moving grid whose size,
@@ -95,3 +97,24 @@ def test_two_channels_on_their_own_moving_grid_match_the_oracle(backend):
     assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
     last = [it["energy"] for it in res.iterations if it["level"] == 1]
     assert last[-1] < last[0]  # the energy falls within a level (levels are not comparable)
+
+
+def test_the_full_config2_registration_matches_the_oracle(backend):
+    """The benchmark's registration end to end -- 4/2/1 shrink, sigma 2/1/0, 70/50/20 iterations,
+    CC r = 4, step 0.1 -- with every iteration run (threshold -1: the window monitor would stop
+    both engines where their last energies happen to cross it) against the oracle's, which takes
+    a couple of minutes on the host cores: 0.05 mm RMS on both fields, 1e-4 relative final CC."""
+    g, fixed, mg, moving, initial = head_pair()
+    r = SynRecipe(gradient_step=0.1, update_field_variance=3.0, total_field_variance=0.0,
+                  cc_radius=4, iterations=[70, 50, 20], shrink_factors=[4, 2, 1],
+                  smoothing_sigmas=[2.0, 1.0, 0.0], convergence_threshold=-1.0,
+                  convergence_window=10)
+    res = run_syn(backend, r, g, [fixed], mg, [moving], initial)
+    orec = O.syn_recipe(0.1, 3.0, 0.0, 4, (70, 50, 20), (4, 2, 1), (2.0, 1.0, 0.0), False, -1.0,
+                        10, (1.0,))
+    ow, oinv, orecs, _ = O.syn_run(orec, ogrid(g), [fixed], ogrid(mg), [moving], oaffine(initial))
+    assert len(res.iterations) == len(orecs) == 140
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    rms_inv = np.sqrt(((res.inverse_warp.astype(np.float64) - oinv) ** 2).sum(-1).mean())
+    assert rms <= 0.05 and rms_inv <= 0.05, (rms, rms_inv)
+    assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
