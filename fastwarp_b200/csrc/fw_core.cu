@@ -309,9 +309,6 @@ __global__ void __launch_bounds__(256) k_warp(WarpArgs a, const float* __restric
     out[l] = v;
 }
 
-// The plain warp (no earlier field, linear interpolation) -- the SyN loop's two per-iteration
-// warps -- with VPT voxels per thread, 256 apart, so their independent gathers are in flight
-// together.
 // The plain warp (no earlier field, linear interpolation) -- the SyN loop's per-iteration warps --
 // over 32 x 8 column tiles marching along z, the next slice's displacement loaded while the
 // current one gathers.
