@@ -347,6 +347,42 @@ class CudaBackend:
         check(lib().fw_smooth_recursive(self.ctx, image.handle, s, C.byref(h)))
         return Image(self, h)
 
+    # -- image preparation (register.rs:82-249, preprocess.rs:45-215)
+    def resample_isotropic(self, image: Image, mm: float) -> Image:
+        """resample_isotropic: the image on the isotropic `mm` grid (a copy if already there)."""
+        h = C.c_void_p()
+        check(lib().fw_resample_isotropic(self.ctx, image.handle, C.c_double(mm), C.byref(h)))
+        return Image(self, h)
+
+    def quantile_window(self, image: Image, lower: float, upper: float):
+        """quantile_window: (lo, hi) of the finite voxels' 256-bin histogram, float32 values."""
+        w = (C.c_double * 2)()
+        check(lib().fw_quantile_window(self.ctx, image.handle, C.c_float(lower), C.c_float(upper),
+                                       w))
+        return w[0], w[1]
+
+    def preprocess(self, image: Image, lower: float, upper: float, out_min: float = 0.0,
+                   out_max: float = 1.0) -> Image:
+        """preprocess_volume: the quantile window mapped onto [out_min, out_max]."""
+        h = C.c_void_p()
+        check(lib().fw_preprocess(self.ctx, image.handle, C.c_float(lower), C.c_float(upper),
+                                  C.c_double(out_min), C.c_double(out_max), C.byref(h), None))
+        return Image(self, h)
+
+    def prepare_channels(self, fixed, moving, iso_mm=None, winsorize=(0.005, 0.995)):
+        """prepare_channels_with: (channels as [(fixed, moving)], fixed_raw, moving_raw).
+        `iso_mm` None keeps the images' grids; `winsorize` None is the plain (0, 1) rescale."""
+        k = len(fixed)
+        arr = C.c_void_p * max(k, 1)
+        outs = [arr() for _ in range(4)]
+        mm = C.byref(C.c_double(iso_mm)) if iso_mm is not None else None
+        w = (C.c_float * 2)(*winsorize) if winsorize is not None else None
+        check(lib().fw_prepare_channels(
+            self.ctx, C.c_int32(k if k == len(moving) else 0),
+            arr(*[i.handle for i in fixed]), arr(*[i.handle for i in moving]), mm, w, *outs))
+        fo, mo, fr, mr = ([Image(self, C.c_void_p(o[c])) for c in range(k)] for o in outs)
+        return list(zip(fo, mo)), fr, mr
+
 
 def shrink_factors(factor: int, spacing):
     out = (C.c_uint32 * 3)()

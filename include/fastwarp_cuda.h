@@ -343,6 +343,32 @@ int fw_shrink_grid(const fw_grid* grid, const uint32_t factors[3], fw_grid* out)
 int fw_smooth_recursive(fw_ctx* ctx, const fw_image* img, const double sigma_mm[3],
                         fw_image** out);
 
+/* ---- image preparation (register.rs:82-249, preprocess.rs:45-215) ----------------------- */
+
+/* resample_isotropic (register.rs:112-146): a new image on the isotropic `mm` grid (same origin
+ * and direction, floor((n - 1) * spacing / mm + 1e-9) + 1 voxels per axis); output voxel i
+ * samples source index min(i * mm / spacing, n - 1) trilinearly. A copy when every axis already
+ * has `mm` spacing (within 1e-6 mm). */
+int fw_resample_isotropic(fw_ctx* ctx, const fw_image* img, double mm, fw_image** out);
+/* quantile_window (preprocess.rs:168-173): the (lower, upper) quantiles of a 256-bin histogram
+ * of the finite voxels, each rounded to float32. Fails for an image without finite voxels. */
+int fw_quantile_window(fw_ctx* ctx, const fw_image* img, float lower, float upper,
+                       double window[2]);
+/* preprocess_volume (preprocess.rs:180-223): a new image, the quantile window mapped linearly
+ * onto [out_min, out_max], values outside it clamped, NaN passed through. `window` (nullable)
+ * receives the window. Fails for no finite voxels and for a degenerate window (hi <= lo). */
+int fw_preprocess(fw_ctx* ctx, const fw_image* img, float lower, float upper, double out_min,
+                  double out_max, fw_image** out, double window[2]);
+/* prepare_channels_with (register.rs:201-249): rejects images with non-finite voxels, resamples
+ * every channel onto the isotropic grid (`iso_mm` NULL: copies as they are), and preprocesses
+ * each onto [0, 1] with the quantile window `winsorize` = {lower, upper} (NULL: (0, 1), the plain
+ * rescale). fixed_out / moving_out receive `channels` new images each; fixed_raw / moving_raw
+ * (nullable) the resampled images before preprocessing. */
+int fw_prepare_channels(fw_ctx* ctx, int32_t channels, const fw_image* const* fixed,
+                        const fw_image* const* moving, const double* iso_mm,
+                        const float* winsorize, fw_image** fixed_out, fw_image** moving_out,
+                        fw_image** fixed_raw, fw_image** moving_raw);
+
 /* ---- Mattes MI of the linear stages (linear.rs:288-320, optimizer.rs:60-65) ------------- */
 
 /* LinearEngine::prepare_level (linear.rs:303-308): the moving level image and the prepared

@@ -270,6 +270,40 @@ def shrink_grid(grid, factors):
     return out
 
 
+def quantile_window(values, lower, upper):
+    """preprocess.rs:168-173: (lo, hi), each rounded to float32."""
+    v = _f64(np.ravel(values))
+    out = (C.c_double * 2)()
+    _check(lib().fwo_quantile_window(_p(v), C.c_int64(v.size), C.c_float(lower),
+                                     C.c_float(upper), out))
+    return out[0], out[1]
+
+
+def preprocess(values, lower, upper, out_min=0.0, out_max=1.0):
+    """preprocess.rs:180-209: the quantile window mapped onto [out_min, out_max]."""
+    v = _f64(values)
+    out = np.empty_like(v)
+    _check(lib().fwo_preprocess(_p(v), C.c_int64(v.size), C.c_float(lower), C.c_float(upper),
+                                C.c_double(out_min), C.c_double(out_max), _p(out)))
+    return out
+
+
+def isotropic_grid(grid, mm):
+    """register.rs:112-129: the grid resample_isotropic produces."""
+    out = Grid()
+    _check(lib().fwo_isotropic_grid(C.byref(grid), C.c_double(mm), C.byref(out)))
+    return out
+
+
+def resample_isotropic(grid, img, mm):
+    """register.rs:112-146: (grid, image) resampled onto the isotropic mm grid."""
+    og = isotropic_grid(grid, mm)
+    img = _f64(img)
+    out = np.empty(grid_shape(og))
+    _check(lib().fwo_resample_isotropic(C.byref(grid), _p(img), C.c_double(mm), _p(out)))
+    return og, out
+
+
 def point_to_index(grid, p):
     out = (C.c_double * 3)()
     _check(lib().fwo_point_to_index(C.byref(grid), (C.c_double * 3)(*p), out))

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <limits>
@@ -2058,6 +2059,233 @@ int fwo_cg_optimize_level(const fwo_cg_settings* st, const double* corners,
     trace->best_value = best_value;
     trace->final_learning_rate = lr;
     *t = best;
+    return 0;
+}
+
+}  // extern "C"
+
+// ---- image preparation: isotropic resampling and intensity preprocessing --------------------
+
+namespace {
+
+constexpr int PRE_BINS = 256;         // preprocess.rs:36
+constexpr double PRE_MARGIN = 10.0;   // preprocess.rs:37 (marginal scale)
+
+// The 256-bin histogram of the finite values (preprocess.rs:46-102): bin edges from float32
+// interval arithmetic, the last bin widened by a tenth of a bin, counts per bin.
+struct PreHistogram {
+    double mn[PRE_BINS], mx[PRE_BINS], freq[PRE_BINS];
+
+    bool build(const double* v, int64_t n) {
+        double lo = DBL_MAX, hi = -DBL_MAX;
+        int64_t finite = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            if (!std::isfinite(v[i])) continue;
+            ++finite;
+            lo = std::min(lo, v[i]);
+            hi = std::max(hi, v[i]);
+        }
+        if (finite == 0) return fail("preprocess: image has no finite values") == 0;
+        const double margin = ((hi - lo) / PRE_BINS) / PRE_MARGIN;
+        const double upper = hi + margin;
+        const float interval = ((float)upper - (float)lo) / (float)PRE_BINS;
+        for (int j = 0; j < PRE_BINS - 1; ++j) {
+            mn[j] = lo + (double)((float)j * interval);
+            mx[j] = lo + (double)((float)(j + 1) * interval);
+        }
+        mn[PRE_BINS - 1] = lo + (double)((float)(PRE_BINS - 1) * interval);
+        mx[PRE_BINS - 1] = upper;
+        std::vector<int64_t> counts(PRE_BINS, 0);
+#pragma omp parallel
+        {
+            std::vector<int64_t> local(PRE_BINS, 0);
+#pragma omp for schedule(static) nowait
+            for (int64_t i = 0; i < n; ++i)
+                if (std::isfinite(v[i])) ++local[index_of(v[i])];
+#pragma omp critical
+            for (int j = 0; j < PRE_BINS; ++j) counts[j] += local[j];
+        }
+        for (int j = 0; j < PRE_BINS; ++j) freq[j] = (double)counts[j];
+        return true;
+    }
+
+    // preprocess.rs:104-113: the bin whose lower edge is the last one <= v.
+    int index_of(double v) const {
+        if (v < mn[0]) return 0;
+        if (v >= mx[PRE_BINS - 1]) return PRE_BINS - 1;
+        int lo = 0, hi = PRE_BINS;  // first j with mn[j] > v
+        while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            if (mn[mid] <= v) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo > 0 ? lo - 1 : 0;
+    }
+
+    // preprocess.rs:115-161 (ITK Histogram::Quantile): walk the cumulative frequency from the
+    // nearer end and interpolate linearly inside the bin that crosses p.
+    double quantile(double p) const {
+        double total = 0.0;
+        for (int j = 0; j < PRE_BINS; ++j) total += freq[j];
+        double cumulated = 0.0, p_prev = 0.0, f_n = 0.0;
+        if (p < 0.5) {
+            int n = 0;
+            double p_n = 0.0;
+            do {
+                f_n = freq[n];
+                cumulated += f_n;
+                p_prev = p_n;
+                p_n = cumulated / total;
+                ++n;
+            } while (n < PRE_BINS && p_n < p);
+            const double proportion = f_n / total;
+            const double lo = mn[n - 1], width = mx[n - 1] - lo;
+            return lo + ((p - p_prev) / proportion) * width;
+        }
+        int n = PRE_BINS - 1, m = 0;
+        double p_n = 1.0;
+        do {
+            f_n = freq[n];
+            cumulated += f_n;
+            p_prev = p_n;
+            p_n = 1.0 - cumulated / total;
+            --n;
+            ++m;
+        } while (m < PRE_BINS && p_n > p);
+        const double proportion = f_n / total;
+        const int bin = n + 1;
+        const double top = mx[bin], width = top - mn[bin];
+        return top - ((p_prev - p) / proportion) * width;
+    }
+};
+
+// preprocess.rs:168-173: both quantiles, each rounded to float32.
+bool quantile_window(const double* v, int64_t n, float lower, float upper, double out[2]) {
+    PreHistogram* h = new PreHistogram;
+    const bool ok = h->build(v, n);
+    if (ok) {
+        out[0] = (double)(float)h->quantile((double)lower);
+        out[1] = (double)(float)h->quantile((double)upper);
+    }
+    delete h;
+    return ok;
+}
+
+// register.rs:112-146: the isotropic grid (same origin and direction, mm spacing) and the
+// source index every output index samples along each axis.
+void isotropic_axes(const Grid& g, double mm, int64_t out_n[3], double ratio[3], double last[3]) {
+    for (int a = 0; a < 3; ++a) {
+        last[a] = (double)(g.n[a] - 1);
+        ratio[a] = mm / g.sp[a];
+        const int64_t t = (int64_t)std::floor(last[a] * g.sp[a] / mm + 1e-9) + 1;
+        out_n[a] = std::max<int64_t>(t, 1);
+    }
+}
+
+bool same_spacing(const Grid& g, double mm) {
+    for (int a = 0; a < 3; ++a)
+        if (!(std::fabs(g.sp[a] - mm) < 1e-6)) return false;
+    return true;
+}
+
+// register.rs:82-108: trilinear sample at a continuous index, corners outside skipped.
+double sample_linear_clamped(const double* data, const int64_t size[3], const double c[3]) {
+    const double lo[3] = {std::floor(c[0]), std::floor(c[1]), std::floor(c[2])};
+    const double fr[3] = {c[0] - lo[0], c[1] - lo[1], c[2] - lo[2]};
+    double acc = 0.0;
+    for (int corner = 0; corner < 8; ++corner) {
+        int64_t idx[3];
+        double w = 1.0;
+        bool inside = true;
+        for (int a = 0; a < 3; ++a) {
+            const int bit = (corner >> a) & 1;
+            const int64_t i = (int64_t)lo[a] + bit;
+            if (i < 0 || i >= size[a]) {
+                inside = false;
+                break;
+            }
+            idx[a] = i;
+            w *= bit ? fr[a] : 1.0 - fr[a];
+        }
+        if (w == 0.0 || !inside) continue;
+        acc += w * data[idx[0] + size[0] * (idx[1] + size[1] * idx[2])];
+    }
+    return acc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fwo_quantile_window(const double* values, int64_t n, float lower, float upper,
+                        double out[2]) {
+    if (!values || !out || n < 0) return fail("null argument");
+    return quantile_window(values, n, lower, upper, out) ? 0 : -1;
+}
+
+int fwo_preprocess(const double* values, int64_t n, float lower, float upper, double out_min,
+                   double out_max, double* out) {
+    if (!values || !out || n < 0) return fail("null argument");
+    double w[2];
+    if (!quantile_window(values, n, lower, upper, w)) return -1;
+    const double lo = w[0], hi = w[1];
+    if (!(hi > lo)) {
+        char msg[160];
+        std::snprintf(msg, sizeof(msg), "preprocess: degenerate intensity window [%.17g, %.17g]",
+                      lo, hi);
+        return fail(msg);
+    }
+    const double scale = (out_max - out_min) / (hi - lo);
+    const double shift = out_min - lo * scale;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const double x = values[i];
+        out[i] = x < lo ? out_min : x > hi ? out_max : x * scale + shift;
+    }
+    return 0;
+}
+
+int fwo_isotropic_grid(const fwo_grid* grid, double mm, fwo_grid* out) {
+    Grid g;
+    if (!make_grid(grid, g)) return -1;
+    if (!(std::isfinite(mm) && mm > 0.0)) return fail("isotropic spacing must be positive");
+    if (same_spacing(g, mm)) {
+        *out = *grid;
+        return 0;
+    }
+    int64_t n[3];
+    double ratio[3], last[3];
+    isotropic_axes(g, mm, n, ratio, last);
+    fwo_grid o = *grid;
+    for (int a = 0; a < 3; ++a) {
+        o.size[a] = n[a];
+        o.spacing[a] = mm;
+    }
+    *out = o;
+    return 0;
+}
+
+int fwo_resample_isotropic(const fwo_grid* grid, const double* img, double mm, double* out) {
+    Grid g;
+    if (!make_grid(grid, g)) return -1;
+    if (!img || !out) return fail("null argument");
+    if (!(std::isfinite(mm) && mm > 0.0)) return fail("isotropic spacing must be positive");
+    if (same_spacing(g, mm)) {
+        std::memcpy(out, img, sizeof(double) * g.count());
+        return 0;
+    }
+    int64_t n[3];
+    double ratio[3], last[3];
+    isotropic_axes(g, mm, n, ratio, last);
+    const int64_t count = n[0] * n[1] * n[2];
+#pragma omp parallel for schedule(static)
+    for (int64_t l = 0; l < count; ++l) {
+        const int64_t i = l % n[0], j = (l / n[0]) % n[1], k = l / (n[0] * n[1]);
+        const double c[3] = {std::min((double)i * ratio[0], last[0]),
+                             std::min((double)j * ratio[1], last[1]),
+                             std::min((double)k * ratio[2], last[2])};
+        out[l] = (double)(float)sample_linear_clamped(img, g.n, c);
+    }
     return 0;
 }
 

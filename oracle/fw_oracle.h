@@ -245,6 +245,22 @@ int fwo_syn_run_masked(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
                        const fwo_syn_masks* masks, double* warp, double* inverse_warp,
                        fwo_syn_iteration* records, int64_t cap, int64_t* count);
 
+/* Image preparation (crates/fastwarp-reg/src/preprocess.rs, register.rs). */
+/* quantile_window (preprocess.rs:168-173): the window of a 256-bin histogram of the finite
+ * values, each bound rounded to float32. Fails for an image without finite values. */
+int fwo_quantile_window(const double* values, int64_t n, float lower, float upper,
+                        double out[2]);
+/* preprocess_values (preprocess.rs:180-209): the window mapped onto [out_min, out_max], values
+ * outside clamped, NaN passed through; fails for a degenerate window (hi <= lo). */
+int fwo_preprocess(const double* values, int64_t n, float lower, float upper, double out_min,
+                   double out_max, double* out);
+/* resample_isotropic's grid rule (register.rs:112-129): same origin and direction, mm spacing,
+ * floor((n - 1) * spacing / mm + 1e-9) + 1 voxels; the grid itself when every axis has mm. */
+int fwo_isotropic_grid(const fwo_grid* grid, double mm, fwo_grid* out);
+/* resample_isotropic (register.rs:112-146): trilinear at index min(i * mm / spacing, n - 1),
+ * rounded to float32; `out` holds fwo_isotropic_grid's voxel count. */
+int fwo_resample_isotropic(const fwo_grid* grid, const double* img, double mm, double* out);
+
 #ifdef __cplusplus
 }
 #endif

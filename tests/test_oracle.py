@@ -591,3 +591,150 @@ def test_a_cc_and_a_mattes_channel_combine():
     # the energy is the first channel's (CC) value; the weighted energy mixes in the MI value
     assert recs[0].energy != recs[0].energy_weighted
     assert np.isfinite(warp).all()
+
+
+# ---- preprocess.rs:235-323 (intensity preprocessing) -----------------------------------------
+
+def values_ramp(n):
+    return np.arange(n, dtype=np.float64)
+
+
+def test_preprocess_without_winsorizing_maps_min_to_zero_and_max_just_below_one():
+    out = O.preprocess(values_ramp(1000), 0.0, 1.0, 0.0, 1.0)
+    assert out[0] == 0.0
+    assert abs(out[999] - 999.0 / (999.0 + 999.0 / 2560.0)) < 1e-6
+    assert np.all(np.diff(out) > 0)
+
+
+def test_preprocess_winsorizing_clamps_the_tails_and_is_affine_inside():
+    v = values_ramp(1000)
+    v[3], v[997] = -5000.0, 9000.0
+    out = O.preprocess(v, 0.005, 0.995, 0.0, 1.0)
+    assert out[3] == 0.0 and out[997] == 1.0
+    lo, hi = O.quantile_window(v, 0.005, 0.995)
+    assert -5000.0 < lo < 100.0 and 500.0 < hi < 9000.0
+    assert abs(out[500] - (500.0 - lo) / (hi - lo)) < 1e-12
+
+
+def test_quantile_interpolates_inside_the_bin_like_itk():
+    lo, hi = O.quantile_window(values_ramp(2560), 0.25, 0.75)
+    assert abs(lo - 640.0) < 5.0 and abs(hi - 1920.0) < 5.0
+
+
+def test_preprocess_output_range_and_degenerate_inputs():
+    out = O.preprocess(values_ramp(100), 0.0, 1.0, -1.0, 3.0)
+    assert out[0] == -1.0 and 2.99 < out[99] < 3.0
+    for bad in (np.full(10, 2.0), np.zeros(0), np.array([np.nan, np.inf])):
+        with pytest.raises(O.OracleError):
+            O.preprocess(bad, 0.0, 1.0, 0.0, 1.0)
+    mixed = O.preprocess(np.array([1.0, 3.0, np.nan]), 0.0, 1.0, 0.0, 1.0)
+    assert mixed[0] == 0.0 and 0.99 < mixed[1] < 1.0 and np.isnan(mixed[2])
+
+
+def test_preprocess_is_invariant_to_affine_intensity_changes():
+    v = ((np.arange(500) * 37) % 101).astype(np.float64)
+    a = O.preprocess(v, 0.005, 0.995)
+    b = O.preprocess(3.0 * v + 40.0, 0.005, 0.995)
+    assert np.abs(a - b).max() < 1e-5
+
+
+def test_the_unwinsorized_window_reaches_past_the_maximum():
+    v = np.append(np.arange(101, dtype=np.float64), 9000.0)
+    lo, hi = O.quantile_window(v, 0.0, 1.0)
+    assert lo == 0.0 and hi > 9000.0
+    assert O.preprocess(v, 0.005, 0.995)[101] == 1.0
+    assert O.preprocess(v, 0.0, 1.0)[101] < 1.0
+
+
+def _window_by_loops(values, lower, upper):
+    """Small-case restatement of preprocess.rs:46-173 in plain Python loops (float32 steps in
+    numpy float32), the independent check of the oracle's histogram and quantile walk."""
+    f32 = np.float32
+    fin = [float(x) for x in values if math.isfinite(x)]
+    lo, hi = min(fin), max(fin)
+    upper_edge = hi + ((hi - lo) / 256.0) / 10.0
+    interval = f32(f32(f32(upper_edge) - f32(lo)) / f32(256.0))
+    mn = [lo + float(f32(f32(j) * interval)) for j in range(256)]
+    mx = [lo + float(f32(f32(j + 1) * interval)) for j in range(255)] + [upper_edge]
+    freq = [0.0] * 256
+    for x in fin:
+        if x < mn[0]:
+            b = 0
+        elif x >= mx[255]:
+            b = 255
+        else:
+            b = max(sum(1 for m in mn if m <= x) - 1, 0)
+        freq[b] += 1.0
+    total = sum(freq)
+
+    def quantile(p):
+        cum, p_prev = 0.0, 0.0
+        if p < 0.5:
+            n, p_n = 0, 0.0
+            while True:
+                f_n = freq[n]
+                cum += f_n
+                p_prev, p_n = p_n, cum / total
+                n += 1
+                if not (n < 256 and p_n < p):
+                    break
+            return mn[n - 1] + ((p - p_prev) / (f_n / total)) * (mx[n - 1] - mn[n - 1])
+        n, m, p_n = 255, 0, 1.0
+        while True:
+            f_n = freq[n]
+            cum += f_n
+            p_prev, p_n = p_n, 1.0 - cum / total
+            n -= 1
+            m += 1
+            if not (m < 256 and p_n > p):
+                break
+        b = n + 1
+        return mx[b] - ((p_prev - p) / (f_n / total)) * (mx[b] - mn[b])
+
+    return (float(f32(quantile(float(f32(lower))))), float(f32(quantile(float(f32(upper))))))
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_the_quantile_window_matches_a_loop_restatement_bit_for_bit(seed):
+    rng = np.random.default_rng(seed)
+    v = rng.gamma(2.0, 50.0, 3000).astype(np.float32).astype(np.float64)
+    v[rng.integers(0, 3000, 20)] = np.nan
+    for lower, upper in ((0.0, 1.0), (0.005, 0.995), (0.25, 0.75), (0.6, 0.9)):
+        assert O.quantile_window(v, lower, upper) == _window_by_loops(v, lower, upper)
+
+
+# ---- register.rs:432-470 (isotropic resampling) ----------------------------------------------
+
+def iso_blob_volume(n, spacing, shift):
+    """register.rs:432-445: a Gaussian blob plus a hashed noise term."""
+    g = O.make_grid((n, n, n), (spacing,) * 3)
+    c = (n - 1) * spacing / 2.0
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    lin = (i + n * (j + n * k)).astype(np.uint64)
+    r2 = (i * spacing - c - shift) ** 2 + (j * spacing - c) ** 2 + (k * spacing - c) ** 2
+    noise = ((lin * np.uint64(2654435761)) % np.uint64(1000)).astype(np.float64) / 20000.0
+    return g, np.exp(-r2 / (2.0 * (0.25 * n * spacing) ** 2)) + noise
+
+
+def test_isotropic_resample_follows_the_pipeline_grid_rule():
+    g, v = iso_blob_volume(21, 0.5, 0.0)
+    rg, r = O.resample_isotropic(g, v, 1.0)
+    assert tuple(rg.size) == (11, 11, 11) and tuple(rg.spacing) == (1.0, 1.0, 1.0)
+    assert tuple(rg.origin) == tuple(g.origin)
+    assert abs(r[5, 4, 3] - v[10, 8, 6]) < 1e-6
+    sg, same = O.resample_isotropic(rg, r, 1.0)
+    assert tuple(sg.size) == tuple(rg.size) and np.array_equal(same, r)
+
+
+def test_isotropic_resample_interpolates_between_source_voxels():
+    g = O.make_grid((4, 1, 1), (1.5, 1.0, 1.0))
+    rg, r = O.resample_isotropic(g, np.array([0.0, 3.0, 6.0, 9.0]).reshape(1, 1, 4), 1.0)
+    assert tuple(rg.size) == (5, 1, 1)
+    assert np.abs(r.ravel() - [0.0, 2.0, 4.0, 6.0, 8.0]).max() < 1e-6
+
+
+def test_isotropic_resample_rejects_a_non_positive_spacing():
+    g, v = iso_blob_volume(5, 2.0, 0.0)
+    for mm in (0.0, -1.0, math.nan):
+        with pytest.raises(O.OracleError):
+            O.resample_isotropic(g, v, mm)
