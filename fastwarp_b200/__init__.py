@@ -12,11 +12,12 @@ from ._native import FastwarpError, build, lib
 from .backend import (CudaBackend, CudaLinearEngine, Field, Image, MiLevel, binning_from_ranges,
                       grid_shape, linear_transform, make_affine, make_grid, shrink_factors,
                       shrink_grid)
-from .syn import SynRecipe, SynResult, level_grid, run_syn, run_syn_device, syn_step
+from .syn import (SynRecipe, SynResult, level_grid, run_syn, run_syn_device, run_syn_from,
+                  syn_step)
 
 __all__ = [
     "FastwarpError", "build", "lib", "CudaBackend", "CudaLinearEngine", "Field", "Image",
     "MiLevel", "binning_from_ranges", "grid_shape", "linear_transform", "make_affine",
     "make_grid", "shrink_factors", "shrink_grid", "SynRecipe", "SynResult", "level_grid",
-    "run_syn", "run_syn_device", "syn_step",
+    "run_syn", "run_syn_device", "run_syn_from", "syn_step",
 ]

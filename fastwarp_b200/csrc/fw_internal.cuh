@@ -439,12 +439,13 @@ int enqueue_image_upload_f32(fw_ctx* ctx, const HostGrid& g, const float* host, 
 // transform/param.rs:421-446: outer(optimised(p)) as one affine map y = M p + off (fw_mi.cu).
 void linear_transform_map(const fw_linear_transform* t, double M[9], double off[3]);
 
-// The SyN stage on device images (fw_syn.cu); masks may be null.
+// The SyN stage on device images (fw_syn.cu); masks may be null; prior / prior_inverse are the
+// earlier SyN stages' collapsed fields (both null for a first stage).
 int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
                    const fw_image* const* moving, const fw_image* fixed_mask,
-                   const fw_image* moving_mask, const fw_affine* initial, fw_field** warp,
-                   fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
-                   int64_t* count);
+                   const fw_image* moving_mask, const fw_affine* initial, const fw_field* prior,
+                   const fw_field* prior_inverse, fw_field** warp, fw_field** inverse_warp,
+                   fw_syn_iteration* records, int64_t cap, int64_t* count);
 
 // d_result: [value, sum |d_fixed|^2, sum |d_moving|^2] and, with `valid` (the masked metric:
 // voxels where it is not zero), the number of valid voxels at d_result[3].

@@ -197,7 +197,7 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
     fw_field *w = nullptr, *iw = nullptr;
     if (!rc)
         rc = syn_run_device(ctx, &q.recipe, fi.data(), mi.data(), masks[0], masks[1],
-                            q.has_initial ? &q.initial : nullptr,
+                            q.has_initial ? &q.initial : nullptr, nullptr, nullptr,
                             &w, &iw, recs.data(), (int64_t)recs.size(), &count);
     for (auto* im : up) fw_image_free(im);
     if (!rc) {

@@ -221,6 +221,7 @@ struct Level {
     fw_image* mvalid = nullptr;
     fw_image* valid = nullptr;                  // inside both (the CC pairs' voxels)
     fw_dense_mi* mi = nullptr;                  // scratch of the Mattes pairs
+    const fw_field* prior = nullptr;            // earlier SyN stages' collapsed field (or none)
 };
 
 void free_level_work(Level& L) {
@@ -370,7 +371,7 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
     if (L.fmask)
         FW_TRY(launch_warp(ctx, L.fmask, L.Fi, nullptr, nullptr, L.fvalid->d, true, nullptr));
     if (L.mmask)
-        FW_TRY(launch_warp(ctx, L.mmask, L.Mi, nullptr, initial, L.mvalid->d, true, nullptr));
+        FW_TRY(launch_warp(ctx, L.mmask, L.Mi, L.prior, initial, L.mvalid->d, true, nullptr));
     const fw_image* valid = L.fvalid ? L.fvalid : L.mvalid;
     if (L.fvalid && L.mvalid) {
         FW_TRY(launch_image_product(ctx, L.fvalid, L.mvalid, L.valid));
@@ -378,7 +379,7 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
     }
     for (int c = 0; c < C; ++c) {
         FW_TRY(launch_warp(ctx, fs[c], L.Fi, nullptr, nullptr, L.fmid[c]->d, false, nullptr));
-        FW_TRY(launch_warp(ctx, ms[c], L.Mi, nullptr, initial, L.mmid[c]->d, false, nullptr));
+        FW_TRY(launch_warp(ctx, ms[c], L.Mi, L.prior, initial, L.mmid[c]->d, false, nullptr));
         if (r->channel_metrics[c] == FW_METRIC_MATTES)
             FW_TRY(enqueue_dense_mi_pair(ctx, L.fmid[c], L.mmid[c], L.fvalid, L.mvalid, L.dF,
                                          L.dM, L.mi, d.cc + CC_STRIDE * c));
@@ -753,9 +754,9 @@ int check_masks(fw_ctx* ctx, const fw_image* fmask, const fw_image* mmask) {
 
 int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
                    const fw_image* const* moving, const fw_image* fixed_mask,
-                   const fw_image* moving_mask, const fw_affine* initial, fw_field** warp,
-                   fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
-                   int64_t* count) {
+                   const fw_image* moving_mask, const fw_affine* initial, const fw_field* prior,
+                   const fw_field* prior_inverse, fw_field** warp, fw_field** inverse_warp,
+                   fw_syn_iteration* records, int64_t cap, int64_t* count) {
     FW_TRY(syn_validate(r));
     const double t_start = tracing() ? now_ms() : 0.0;
     FW_TRY(check_masks(ctx, fixed_mask, moving_mask));
@@ -764,6 +765,16 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
     const HostGrid fg = fixed[0]->grid;
     for (int c = 1; c < C; ++c)
         if (!fixed[c]->grid.same(fg)) return fail(FW_ERR_INVALID, "syn: fixed images of the channels differ in grid");
+    // syn.rs:803-817: the earlier stages' fields lie on the grid of this stage's last level
+    FW_CHECK(!prior == !prior_inverse, "syn: the prior needs both the warp and its inverse");
+    if (prior) {
+        HostGrid last;
+        FW_TRY(level_grid(r, fg, r->levels - 1, last));
+        if (!prior->grid.same(last) || !prior_inverse->grid.same(last))
+            return fail(FW_ERR_INVALID,
+                        "syn: the field of the earlier SyN stages is not on the grid of this "
+                        "stage's last level: every SyN stage must end with the same shrink factor");
+    }
     int total_iters = 0;
     for (int l = 0; l < r->levels; ++l) total_iters += (int)r->iterations[l];
     // scratch for every reduction of the biggest level, before any capture
@@ -775,6 +786,7 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
     L.channels = C;
     L.fmask = fixed_mask;
     L.mmask = moving_mask;
+    L.prior = prior;
     HostGrid prev;
     bool have_prev = false;
     std::vector<fw_image*> owned;
@@ -917,6 +929,20 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
         if (!rc) rc = new_field(ctx, L.grid, &iw);
         if (!rc) rc = launch_compose(ctx, L.Mi, L.F, w, nullptr, 1.0);
         if (!rc) rc = launch_compose(ctx, L.Fi, L.M, iw, nullptr, 1.0);
+        if (!rc && prior) {
+            // syn.rs:761-774 (collapse): total = W + P(x + W) in place; the inverse needs a
+            // new field, total^-1 = Pinv + Winv(x + Pinv)
+            fw_field* tiw = nullptr;
+            rc = launch_compose(ctx, prior, w, w, nullptr, 1.0);
+            if (!rc) rc = new_field(ctx, L.grid, &tiw);
+            if (!rc) rc = launch_compose(ctx, iw, prior_inverse, tiw, nullptr, 1.0);
+            if (!rc) {
+                fw_field_free(iw);
+                iw = tiw;
+            } else {
+                fw_field_free(tiw);
+            }
+        }
         if (!rc) rc = sync(ctx);
         if (rc) {
             fw_field_free(w);
@@ -1040,8 +1066,8 @@ int fw_syn_run_device(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* 
                       fw_field** warp, fw_field** inverse_warp, fw_syn_iteration* records,
                       int64_t cap, int64_t* count) {
     FW_CHECK(ctx && recipe && fixed && moving && warp && inverse_warp, "null argument");
-    return syn_run_device(ctx, recipe, fixed, moving, nullptr, nullptr, initial, warp,
-                          inverse_warp, records, cap, count);
+    return syn_run_device(ctx, recipe, fixed, moving, nullptr, nullptr, initial, nullptr, nullptr,
+                          warp, inverse_warp, records, cap, count);
 }
 
 int fw_syn_run_device_masked(fw_ctx* ctx, const fw_syn_recipe* recipe,
@@ -1050,8 +1076,20 @@ int fw_syn_run_device_masked(fw_ctx* ctx, const fw_syn_recipe* recipe,
                              const fw_affine* initial, fw_field** warp, fw_field** inverse_warp,
                              fw_syn_iteration* records, int64_t cap, int64_t* count) {
     FW_CHECK(ctx && recipe && fixed && moving && warp && inverse_warp, "null argument");
-    return syn_run_device(ctx, recipe, fixed, moving, fixed_mask, moving_mask, initial, warp,
-                          inverse_warp, records, cap, count);
+    return syn_run_device(ctx, recipe, fixed, moving, fixed_mask, moving_mask, initial, nullptr,
+                          nullptr, warp, inverse_warp, records, cap, count);
+}
+
+int fw_syn_run_device_from(fw_ctx* ctx, const fw_syn_recipe* recipe,
+                           const fw_image* const* fixed, const fw_image* const* moving,
+                           const fw_image* fixed_mask, const fw_image* moving_mask,
+                           const fw_affine* initial, const fw_field* prior,
+                           const fw_field* prior_inverse, fw_field** warp,
+                           fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
+                           int64_t* count) {
+    FW_CHECK(ctx && recipe && fixed && moving && warp && inverse_warp, "null argument");
+    return syn_run_device(ctx, recipe, fixed, moving, fixed_mask, moving_mask, initial, prior,
+                          prior_inverse, warp, inverse_warp, records, cap, count);
 }
 
 int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_grid,
@@ -1071,8 +1109,8 @@ int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_gr
     fw_field *w = nullptr, *iw = nullptr;
     if (!rc) {
         std::vector<const fw_image*> cf(fi.begin(), fi.end()), cm(mi.begin(), mi.end());
-        rc = syn_run_device(ctx, recipe, cf.data(), cm.data(), nullptr, nullptr, initial, &w, &iw,
-                            records, cap, count);
+        rc = syn_run_device(ctx, recipe, cf.data(), cm.data(), nullptr, nullptr, initial, nullptr,
+                            nullptr, &w, &iw, records, cap, count);
     }
     if (!rc) rc = fw_field_download_f32(ctx, w, warp);
     if (!rc) rc = fw_field_download_f32(ctx, iw, inverse_warp);

@@ -143,8 +143,11 @@ def run_syn(backend: CudaBackend, recipe: SynRecipe, fixed_grid: N.Grid, fixed: 
 
 def run_syn_device(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
                    moving: List[Image], initial: N.Affine | None = None,
-                   fixed_mask: Image | None = None, moving_mask: Image | None = None):
-    """The same on device-resident images; returns (warp Field, inverse Field, records)."""
+                   fixed_mask: Image | None = None, moving_mask: Image | None = None,
+                   prior: tuple | None = None):
+    """The same on device-resident images; returns (warp Field, inverse Field, records).
+    `prior` = (warp Field, inverse Field) of earlier SyN stages makes this run_syn_from
+    (syn.rs:620-660): a later stage, collapsed with the prior."""
     r = recipe.to_c()
     fp = (C.c_void_p * len(fixed))(*[im.handle.value for im in fixed])
     mp = (C.c_void_p * len(moving))(*[im.handle.value for im in moving])
@@ -152,13 +155,36 @@ def run_syn_device(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
     recs = (N.SynIteration * cap)()
     count = C.c_int64()
     w, iw = C.c_void_p(), C.c_void_p()
-    check(lib().fw_syn_run_device_masked(backend.ctx, C.byref(r), fp, mp,
-                                         None if fixed_mask is None else fixed_mask.handle,
-                                         None if moving_mask is None else moving_mask.handle,
-                                         None if initial is None else C.byref(initial),
-                                         C.byref(w), C.byref(iw), recs, C.c_int64(cap),
-                                         C.byref(count)))
+    fm = None if fixed_mask is None else fixed_mask.handle
+    mm = None if moving_mask is None else moving_mask.handle
+    init = None if initial is None else C.byref(initial)
+    if prior is None:
+        check(lib().fw_syn_run_device_masked(backend.ctx, C.byref(r), fp, mp, fm, mm, init,
+                                             C.byref(w), C.byref(iw), recs, C.c_int64(cap),
+                                             C.byref(count)))
+    else:
+        check(lib().fw_syn_run_device_from(backend.ctx, C.byref(r), fp, mp, fm, mm, init,
+                                           prior[0].handle, prior[1].handle, C.byref(w),
+                                           C.byref(iw), recs, C.c_int64(cap), C.byref(count)))
     return Field(backend, w), Field(backend, iw), _records(recs, min(count.value, cap))
+
+
+def run_syn_from(backend: CudaBackend, recipe: SynRecipe, fixed_grid: N.Grid, fixed: list,
+                 moving_grid: N.Grid, moving: list, initial: N.Affine | None,
+                 prior_warp, prior_inverse_warp, fixed_mask=None,
+                 moving_mask=None) -> SynResult:
+    """run_syn_from (syn.rs:620-660) from host images: a later SyN stage whose moving side goes
+    through the earlier stages' collapsed fields (AoS arrays on the grid of this stage's last
+    level, as SynResult.warp / inverse_warp hold them); the result is collapsed with them."""
+    last = level_grid(recipe, fixed_grid, recipe.to_c().levels - 1)
+    fi = [backend.upload_image(fixed_grid, a) for a in fixed]
+    mi = [backend.upload_image(moving_grid, a) for a in moving]
+    fm = None if fixed_mask is None else backend.upload_image(*fixed_mask)
+    mm = None if moving_mask is None else backend.upload_image(*moving_mask)
+    prior = (backend.upload_field(last, prior_warp), backend.upload_field(last, prior_inverse_warp))
+    w, iw, recs = run_syn_device(backend, recipe, fi, mi, initial, fm, mm, prior)
+    return SynResult(backend.download_field(w).astype(np.float32),
+                     backend.download_field(iw).astype(np.float32), last, recs)
 
 
 class WindowConvergenceMonitor:

@@ -430,6 +430,19 @@ int fw_syn_run_device_masked(fw_ctx* ctx, const fw_syn_recipe* recipe,
                              const fw_affine* initial, fw_field** warp, fw_field** inverse_warp,
                              fw_syn_iteration* records, int64_t cap, int64_t* count);
 
+/* run_syn_from (syn.rs:620-660, 803-820, 971-977): a later SyN stage. `prior` / `prior_inverse`
+ * are the earlier SyN stages' collapsed fields (PriorWarp), on the grid of this stage's last
+ * level; the moving images and mask are sampled at affine(prior(M^-1(x))) every iteration, and
+ * the result is collapsed with the prior: warp = W + P(x + W), inverse = Pinv + Winv(x + Pinv).
+ * Masks may be NULL; both prior fields NULL is a first stage (fw_syn_run_device_masked). */
+int fw_syn_run_device_from(fw_ctx* ctx, const fw_syn_recipe* recipe,
+                           const fw_image* const* fixed, const fw_image* const* moving,
+                           const fw_image* fixed_mask, const fw_image* moving_mask,
+                           const fw_affine* initial, const fw_field* prior,
+                           const fw_field* prior_inverse, fw_field** warp,
+                           fw_field** inverse_warp, fw_syn_iteration* records, int64_t cap,
+                           int64_t* count);
+
 /* run_syn from host float32 images: uploads, runs, and writes the two fields as AoS float32
  * (DisplacementField) on the grid of the last level (fw_syn_level_grid). */
 int fw_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_grid* fixed_grid,

@@ -484,8 +484,9 @@ def syn_step(recipe, level_grid, fixed_grid, fixed_smooth, moving_grid, moving_s
 
 
 def syn_run(recipe, fixed_grid, fixed, moving_grid, moving, initial=None, cap=100000,
-            masks=None):
-    """Whole SyN stage; fixed/moving are lists (one image per channel)."""
+            masks=None, prior=None):
+    """Whole SyN stage; fixed/moving are lists (one image per channel). `prior` = None or
+    (grid, warp, inverse_warp): the earlier SyN stages' collapsed fields (run_syn_from)."""
     fs = [_f64(a) for a in fixed]
     ms = [_f64(a) for a in moving]
     last = syn_level_grid(recipe, fixed_grid, recipe.levels - 1)
@@ -494,11 +495,15 @@ def syn_run(recipe, fixed_grid, fixed, moving_grid, moving, initial=None, cap=10
     recs = (SynIteration * cap)()
     count = C.c_int64()
     cm, _keep = _masks(masks)
-    _check(lib().fwo_syn_run_masked(C.byref(recipe), C.byref(fixed_grid), _ptrs(fs),
-                                    C.byref(moving_grid), _ptrs(ms),
-                                    None if initial is None else C.byref(initial),
-                                    None if cm is None else C.byref(cm), _p(warp_out),
-                                    _p(inv_out), recs, C.c_int64(cap), C.byref(count)))
+    pg, pw, pi = (None, None, None) if prior is None else (prior[0], _f64(prior[1]),
+                                                           _f64(prior[2]))
+    _check(lib().fwo_syn_run_from(C.byref(recipe), C.byref(fixed_grid), _ptrs(fs),
+                                  C.byref(moving_grid), _ptrs(ms),
+                                  None if initial is None else C.byref(initial),
+                                  None if cm is None else C.byref(cm),
+                                  None if pg is None else C.byref(pg), _p(pw), _p(pi),
+                                  _p(warp_out), _p(inv_out), recs, C.c_int64(cap),
+                                  C.byref(count)))
     return warp_out, inv_out, [recs[i] for i in range(min(count.value, cap))], last
 
 

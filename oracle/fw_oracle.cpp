@@ -1617,7 +1617,8 @@ int syn_iteration(const fwo_syn_recipe* r, const Grid& lg, const Grid& fg,
                   const double* const* fixed_s, const Grid& mg, const double* const* moving_s,
                   const fwo_affine* initial, const fwo_syn_masks* masks, double* f2m,
                   double* f2m_inv, double* m2m, double* m2m_inv, double* fixed_update_out,
-                  double* moving_update_out, fwo_syn_iteration* rec) {
+                  double* moving_update_out, fwo_syn_iteration* rec,
+                  const fwo_grid* prior_grid = nullptr, const double* prior = nullptr) {
     int64_t n = lg.count();
     int channels = r->channels;
     double wsum = 0.0;
@@ -1640,7 +1641,7 @@ int syn_iteration(const fwo_syn_recipe* r, const Grid& lg, const Grid& fg,
     }
     if (has_mm) {
         mvalid.resize(n);
-        if (fwo_warp_mask(masks->moving_grid, masks->moving, &lgc, m2m_inv, nullptr, nullptr,
+        if (fwo_warp_mask(masks->moving_grid, masks->moving, &lgc, m2m_inv, prior_grid, prior,
                           initial, nullptr, mvalid.data()))
             return -1;
     }
@@ -1653,7 +1654,7 @@ int syn_iteration(const fwo_syn_recipe* r, const Grid& lg, const Grid& fg,
     for (int c = 0; c < channels; ++c) {
         if (fwo_warp(&fgc, fixed_s[c], &lgc, f2m_inv, nullptr, nullptr, nullptr, fmid.data()))
             return -1;
-        if (fwo_warp(&mgc, moving_s[c], &lgc, m2m_inv, nullptr, nullptr, initial, mmid.data()))
+        if (fwo_warp(&mgc, moving_s[c], &lgc, m2m_inv, prior_grid, prior, initial, mmid.data()))
             return -1;
         double vals[2];
         if (r->channel_metrics[c] == 1) {
@@ -1791,10 +1792,37 @@ int fwo_syn_run_masked(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
                        const double* const* moving, const fwo_affine* initial,
                        const fwo_syn_masks* masks, double* warp, double* inverse_warp,
                        fwo_syn_iteration* records, int64_t cap, int64_t* count) {
+    return fwo_syn_run_from(r, fixed_grid, fixed, moving_grid, moving, initial, masks, nullptr,
+                            nullptr, nullptr, warp, inverse_warp, records, cap, count);
+}
+
+// syn.rs:620-660, 776-986 -- syn_fields from a SynStart: after earlier SyN stages their collapsed
+// field (on the grid of this stage's last level) enters every moving-side warp, and the result is
+// collapsed with it (syn.rs:761-774, 971-977).
+int fwo_syn_run_from(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
+                     const double* const* fixed, const fwo_grid* moving_grid,
+                     const double* const* moving, const fwo_affine* initial,
+                     const fwo_syn_masks* masks, const fwo_grid* prior_grid, const double* prior,
+                     const double* prior_inverse, double* warp, double* inverse_warp,
+                     fwo_syn_iteration* records, int64_t cap, int64_t* count) {
     Grid fg, mg;
     if (!make_grid(fixed_grid, fg) || !make_grid(moving_grid, mg)) return -1;
     if (r->levels <= 0 || r->levels > FWO_MAX_LEVELS) return fail("bad level count");
     if (r->channels <= 0 || r->channels > FWO_MAX_CHANNELS) return fail("bad channel count");
+    if (!prior != !prior_inverse) return fail("syn: the prior needs both the warp and its inverse");
+    if (prior) {
+        uint32_t factors[3];
+        shrink_factors(r->shrink_factors[r->levels - 1], fg.sp, factors);
+        Grid last, pg;
+        if (!shrink_grid(fg, factors, last) || !make_grid(prior_grid, pg)) return -1;
+        bool same = true;
+        for (int a = 0; a < 3; ++a)
+            same = same && pg.n[a] == last.n[a] && pg.sp[a] == last.sp[a] && pg.org[a] == last.org[a];
+        for (int k = 0; k < 9; ++k) same = same && pg.dir[k] == last.dir[k];
+        if (!same)
+            return fail("syn: the field of the earlier SyN stages is not on the grid of this "
+                        "stage's last level: every SyN stage must end with the same shrink factor");
+    }
     // recipe.rs:239-246: a given mask must have a voxel inside
     if (masks) {
         const fwo_grid* mgs[2] = {masks->fixed_grid, masks->moving_grid};
@@ -1865,7 +1893,8 @@ int fwo_syn_run_masked(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
             ++current;
             fwo_syn_iteration rec{};
             if (syn_iteration(r, lg, fg, fptr.data(), mg, mptr.data(), initial, masks, f2m.data(),
-                              f2m_inv.data(), m2m.data(), m2m_inv.data(), nullptr, nullptr, &rec))
+                              f2m_inv.data(), m2m.data(), m2m_inv.data(), nullptr, nullptr, &rec,
+                              prior_grid, prior))
                 return -1;
             monitor.add(rec.energy);
             rec.convergence_value = monitor.value();
@@ -1878,6 +1907,13 @@ int fwo_syn_run_masked(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
     // syn.rs:969-970
     compose(prev, m2m_inv.data(), f2m.data(), warp);
     compose(prev, f2m_inv.data(), m2m.data(), inverse_warp);
+    if (prior) {
+        // syn.rs:761-774 (collapse): total = compose(P, W), total^-1 = compose(Winv, Pinv)
+        const int64_t n3 = 3 * prev.count();
+        std::vector<double> later(warp, warp + n3), later_inv(inverse_warp, inverse_warp + n3);
+        compose(prev, prior, later.data(), warp);
+        compose(prev, later_inv.data(), prior_inverse, inverse_warp);
+    }
     if (count) *count = nrec;
     return 0;
 }

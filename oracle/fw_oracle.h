@@ -245,6 +245,16 @@ int fwo_syn_run_masked(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
                        const fwo_syn_masks* masks, double* warp, double* inverse_warp,
                        fwo_syn_iteration* records, int64_t cap, int64_t* count);
 
+/* run_syn_from, syn.rs:620-660, 761-774, 803-820, 971-977: a later SyN stage whose moving side
+ * goes through the earlier stages' collapsed field (prior, AoS on prior_grid = the grid of this
+ * stage's last level; NULL for a first stage), collapsed with it at the end. masks may be NULL. */
+int fwo_syn_run_from(const fwo_syn_recipe* r, const fwo_grid* fixed_grid,
+                     const double* const* fixed, const fwo_grid* moving_grid,
+                     const double* const* moving, const fwo_affine* initial,
+                     const fwo_syn_masks* masks, const fwo_grid* prior_grid, const double* prior,
+                     const double* prior_inverse, double* warp, double* inverse_warp,
+                     fwo_syn_iteration* records, int64_t cap, int64_t* count);
+
 /* Image preparation (crates/fastwarp-reg/src/preprocess.rs, register.rs). */
 /* quantile_window (preprocess.rs:168-173): the window of a 256-bin histogram of the finite
  * values, each bound rounded to float32. Fails for an image without finite values. */

@@ -738,3 +738,27 @@ def test_isotropic_resample_rejects_a_non_positive_spacing():
     for mm in (0.0, -1.0, math.nan):
         with pytest.raises(O.OracleError):
             O.resample_isotropic(g, v, mm)
+
+
+# ---- run_syn_from: a later SyN stage through the earlier stages' field (syn.rs:620-660, 761-986)
+
+def test_a_zero_prior_leaves_the_syn_run_unchanged_and_a_real_prior_starts_closer():
+    n = 20
+    g = cube(n)
+    f, m, _ = _cavity_pair(n)
+    r = O.syn_recipe(gradient_step=0.25, update_variance=3.0, cc_radius=2, iterations=(4, 3),
+                     shrink=(2, 1), sigmas=(1.0, 0.0), convergence_threshold=-1.0)
+    w0, i0, r0, last = O.syn_run(r, g, [f], g, [m])
+    zero = np.zeros(O.grid_shape(last) + (3,))
+    w1, i1, r1, _ = O.syn_run(r, g, [f], g, [m], prior=(last, zero, zero))
+    assert np.abs(w1 - w0).max() < 1e-9 and np.abs(i1 - i0).max() < 1e-9
+    assert max(abs(a.energy - b.energy) for a, b in zip(r0, r1)) < 1e-12
+    # the second stage from the first one's fields: it starts better aligned, and its result is
+    # the collapse of its own fields with the prior
+    w2, i2, r2, _ = O.syn_run(r, g, [f], g, [m], prior=(last, w0, i0))
+    assert r2[0].energy < r0[0].energy
+    assert np.abs(w2 - w0).max() > 1e-3
+    with pytest.raises(O.OracleError, match="not on the grid of this stage's last level"):
+        coarse = O.syn_level_grid(r, g, 0)
+        z = np.zeros(O.grid_shape(coarse) + (3,))
+        O.syn_run(r, g, [f], g, [m], prior=(coarse, z, z))
