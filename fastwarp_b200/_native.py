@@ -75,6 +75,20 @@ class CgTrace(C.Structure):
                 ("nvalues", C.c_int64)]
 
 
+class LinearRecipe(C.Structure):
+    _fields_ = [("levels", C.c_int32), ("iterations", C.c_uint32 * 8),
+                ("shrink_factors", C.c_uint32 * 8), ("smoothing_sigmas", C.c_double * 8),
+                ("sigma_units_mm", C.c_int32), ("gradient_step", C.c_double),
+                ("convergence_threshold", C.c_double), ("convergence_window", C.c_int32),
+                ("bins", C.c_int32), ("sampling_percentage", C.c_float), ("seed", C.c_uint32)]
+
+
+class LinearLevelTrace(C.Structure):
+    _fields_ = [("level", C.c_int32), ("shrink_factors", C.c_uint32 * 3),
+                ("grid_size", C.c_int64 * 3), ("samples", C.c_int64), ("skipped", C.c_int32),
+                ("cg", CgTrace), ("parameters", C.c_double * 12)]
+
+
 METRIC_VALUE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform),
                               C.POINTER(C.c_double))
 METRIC_VALUE_DERIVATIVE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform),

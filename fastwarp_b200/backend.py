@@ -504,6 +504,38 @@ class CudaLinearEngine:
 
 # ---- the linear-stage optimiser (optimizer.rs:60-435) --------------------------------------------
 
+def linear_recipe(iterations=(1000, 500, 250, 100), shrink_factors=(8, 4, 2, 1),
+                  smoothing_sigmas=(3.0, 2.0, 1.0, 0.0), sigma_units_mm=False, gradient_step=0.1,
+                  convergence_threshold=1e-6, convergence_window=10, bins=32,
+                  sampling_percentage=0.25, seed=1) -> N.LinearRecipe:
+    """LinearRecipe (linear.rs:75-128); the defaults are antsRegistration's cohort stage with the
+    `MI[...,32,Regular,0.25]` metric and --random-seed 1."""
+    r = N.LinearRecipe()
+    r.levels = len(iterations)
+    for i, (it, sf, sg) in enumerate(zip(iterations, shrink_factors, smoothing_sigmas)):
+        r.iterations[i], r.shrink_factors[i], r.smoothing_sigmas[i] = int(it), int(sf), float(sg)
+    r.sigma_units_mm = int(bool(sigma_units_mm))
+    r.gradient_step, r.convergence_threshold = float(gradient_step), float(convergence_threshold)
+    r.convergence_window, r.bins = int(convergence_window), int(bins)
+    r.sampling_percentage, r.seed = float(sampling_percentage), int(seed)
+    return r
+
+
+def run_linear_stage(backend: "CudaBackend", recipe: N.LinearRecipe, fixed: Image,
+                     moving: Image, start: N.LinearTransform):
+    """run_linear_stage (linear.rs:512-597) on the device: (transform, [level trace dicts])."""
+    t = N.LinearTransform.from_buffer_copy(start)
+    traces = (N.LinearLevelTrace * recipe.levels)()
+    check(lib().fw_linear_stage_run(backend.ctx, C.byref(recipe), fixed.handle, moving.handle,
+                                    C.byref(t), traces))
+    n = 6 if t.kind == 0 else 12
+    out = [dict(level=tr.level, shrink_factors=tuple(tr.shrink_factors),
+                grid_size=tuple(tr.grid_size), samples=tr.samples, skipped=bool(tr.skipped),
+                iterations=tr.cg.iterations, best_value=tr.cg.best_value,
+                parameters=list(tr.parameters[:n])) for tr in traces]
+    return t, out
+
+
 def cg_settings_ants(max_step_mm=0.1, iterations=100, threshold=1e-6, window=10) -> N.CgSettings:
     """CgSettings::ants (optimizer.rs:94-106)."""
     s = N.CgSettings()

@@ -513,5 +513,7 @@ extern "C" size_t fw_abi_struct_size(const char* name) {
     if (n == "fw_cg_settings") return sizeof(fw_cg_settings);
     if (n == "fw_cg_trace") return sizeof(fw_cg_trace);
     if (n == "fw_transform_elem") return sizeof(fw_transform_elem);
+    if (n == "fw_linear_recipe") return sizeof(fw_linear_recipe);
+    if (n == "fw_linear_level_trace") return sizeof(fw_linear_level_trace);
     return 0;
 }

@@ -507,6 +507,46 @@ int fw_mi_level_optimize(fw_mi_level* level, const fw_cg_settings* settings,
                          const double corners[24], fw_linear_transform* transform,
                          fw_cg_trace* trace, double* values, int64_t cap);
 
+/* ---- one linear stage (linear.rs:512-597, 873-1068) -------------------------------------- */
+
+/* LinearRecipe (linear.rs:75-128) without a fixed mask; the transform kind is the start
+ * transform's (Euler3D: rigid, affine: affine). */
+typedef struct fw_linear_recipe {
+    int32_t levels;
+    uint32_t iterations[FW_MAX_LEVELS];
+    uint32_t shrink_factors[FW_MAX_LEVELS];
+    double smoothing_sigmas[FW_MAX_LEVELS];
+    int32_t sigma_units_mm;          /* 0: sigmas in voxels (the cohort recipe), 1: in mm */
+    double gradient_step;            /* Rigid[step] / Affine[step]: maximum step in mm */
+    double convergence_threshold;
+    int32_t convergence_window;
+    int32_t bins;                    /* MI[...] histogram bins */
+    float sampling_percentage;       /* MI[...] regular sampling percentage, (0, 1] */
+    uint32_t seed;                   /* --random-seed: the first level's generator seed */
+} fw_linear_recipe;
+
+/* LinearLevelTrace (linear.rs:420-470). */
+typedef struct fw_linear_level_trace {
+    int32_t level;
+    uint32_t shrink_factors[3];
+    int64_t grid_size[3];
+    int64_t samples;                 /* prepared samples (0 when skipped) */
+    int32_t skipped;                 /* 1: Mattes MI undefined on the level's samples */
+    fw_cg_trace cg;
+    double parameters[12];           /* the optimised parameters after the level */
+} fw_linear_level_trace;
+
+/* run_linear_stage (linear.rs:512-597): per level, the fixed grid shrunk by the level's factors,
+ * both images smoothed at full resolution on the device, one regular sample set from the next
+ * seed, the samples prepared (nearest-voxel fixed range, whole-image moving range, trilinear
+ * fixed bins), and the conjugate-gradient optimiser over the device MI level. A level whose
+ * samples leave MI undefined is skipped; every level skipped is an error. `transform` holds the
+ * start (with the earlier transforms as its outer part) and receives the result; `traces`
+ * (nullable) receives recipe->levels entries. */
+int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* recipe, const fw_image* fixed,
+                        const fw_image* moving, fw_linear_transform* transform,
+                        fw_linear_level_trace* traces);
+
 /* ---- profiling (crates/fastwarp-gpu/src/profiler.rs:8-60: per-op device timestamps) ----- */
 
 /* Times `reps` launches of each kernel of one SyN iteration on the grid of `fixed` with CUDA

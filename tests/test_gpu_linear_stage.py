@@ -1,0 +1,98 @@
+"""One linear stage (run_linear_stage, linear.rs:512-597) on the device against the oracle's
+pieces composed the same way: per level the shrunk virtual grid, Deriche smoothing, regular
+sampling with the stage's seed sequence, sample preparation and the conjugate-gradient optimiser
+over Mattes MI.
+
+The device smooths into float32 images and evaluates MI in float32 with f64 reductions, the oracle
+in f64, so the bars are those of the level-optimiser test: each level's best MI value to 1e-4
+relative, the prepared sample counts to 0.5 %, the final transforms to 0.05 mm at the level grid's
+corners.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from fastwarp_b200 import FastwarpError, linear_transform
+from fastwarp_b200.backend import grid_corners, linear_recipe, run_linear_stage
+from fastwarp_b200.phantoms import blob_pair
+
+pytestmark = pytest.mark.gpu
+
+
+def ogrid(g):
+    return O.make_grid(tuple(g.size), tuple(g.spacing), tuple(g.origin),
+                       np.array(g.direction[:]).reshape(3, 3))
+
+
+def oracle_stage(g, fixed, moving, kind, start, center, iterations, shrink, sigmas, step=0.1,
+                 pct=0.25, bins=32, seed=1):
+    """run_linear_stage restated over the oracle's pieces (sigmas in voxels)."""
+    og = ogrid(g)
+    fixed, moving = fixed.astype(np.float64), moving.astype(np.float64)
+    t = O.linear_transform(kind, start, center=center)
+    out = []
+    for level, (its, sf, sg) in enumerate(zip(iterations, shrink, sigmas)):
+        f = O.shrink_factors(sf, tuple(g.spacing))
+        lg = O.shrink_grid(og, f)
+        if sg > 0:
+            s = tuple(sg * x for x in g.spacing)
+            fs, ms = O.smooth_recursive(og, fixed, s), O.smooth_recursive(og, moving, s)
+        else:
+            fs, ms = fixed, moving
+        pts = O.sample_points_regular(lg, pct, seed + level)
+        kept, fbin, b = O.prepare_samples(og, fs, og, ms, pts, bins)
+
+        def ov(tt):
+            return O.mi_evaluate(b, og, ms, kept, fbin, tt, False)[0]
+
+        def ovd(tt):
+            v, d, _, _ = O.mi_evaluate(b, og, ms, kept, fbin, tt)
+            return v, d
+        corners = grid_corners(lg)
+        t, trace = O.cg_optimize_level(ov, ovd, corners, t,
+                                       O.cg_settings_ants(step, its, 1e-6, 10))
+        out.append(dict(samples=len(fbin), values=trace["values"], corners=corners))
+    return t, out
+
+
+def corner_shift(t_dev, t_orc, corners):
+    ma, oa = O.linear_map(O.linear_transform("euler" if t_dev.kind == 0 else "affine",
+                                             list(t_dev.parameters[:6 if t_dev.kind == 0 else 12]),
+                                             center=tuple(t_dev.center)))
+    mb, ob = O.linear_map(t_orc)
+    return max(np.linalg.norm((ma - mb) @ c + oa - ob) for c in corners)
+
+
+@pytest.mark.parametrize("kind", ["euler", "affine"])
+def test_a_linear_stage_matches_the_oracle(backend, kind):
+    g, fixed, moving = blob_pair(48, seed=77)
+    center = tuple((s - 1) * sp / 2.0 for s, sp in zip(g.size, g.spacing))
+    start = [0.0] * 6 if kind == "euler" else list(np.eye(3).ravel()) + [0.0] * 3
+    its, shrink, sigmas = (12, 8), (2, 1), (1.0, 0.0)
+    r = linear_recipe(iterations=its, shrink_factors=shrink, smoothing_sigmas=sigmas)
+    t, levels = run_linear_stage(backend, r, backend.upload_image(g, fixed),
+                                 backend.upload_image(g, moving),
+                                 linear_transform(kind, start, center=center))
+    ot, olevels = oracle_stage(g, fixed, moving, kind, start, center, its, shrink, sigmas)
+    assert [lv["skipped"] for lv in levels] == [False, False]
+    for lv, ol in zip(levels, olevels):
+        assert abs(lv["samples"] - ol["samples"]) <= 0.005 * ol["samples"]
+        best = min(ol["values"])
+        assert abs(lv["best_value"] - best) <= 1e-4 * abs(best), (lv["best_value"], best)
+    assert levels[0]["iterations"] > 0 and levels[1]["iterations"] > 0
+    shift = corner_shift(t, ot, olevels[-1]["corners"])
+    print(f"{kind}: corner shift {shift:.2e} mm, best MI {levels[-1]['best_value']:.6f} "
+          f"(oracle {min(olevels[-1]['values']):.6f}), samples {levels[-1]['samples']}")
+    assert shift < 0.05, shift
+    # the stage moved the transform
+    assert max(abs(p - s) for p, s in zip(levels[-1]["parameters"], start)) > 1e-4
+
+
+def test_a_stage_whose_levels_all_see_one_fixed_value_is_refused(backend):
+    g, _, moving = blob_pair(24, seed=3)
+    flat = np.full(tuple(g.size)[::-1], 0.5, np.float32)
+    r = linear_recipe(iterations=(5,), shrink_factors=(1,), smoothing_sigmas=(0.0,))
+    with pytest.raises(FastwarpError, match="every level of the rigid stage has too few usable"):
+        run_linear_stage(backend, r, backend.upload_image(g, flat),
+                         backend.upload_image(g, moving),
+                         linear_transform("euler", [0.0] * 6, center=(11.5, 11.5, 11.5)))
