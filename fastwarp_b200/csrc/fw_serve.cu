@@ -75,7 +75,30 @@ struct Job {
     fw_syn_result result{};
     bool done = false;
     bool taken = false;
+    bool linear = false;           // a linear-stage request (lreq / lres)
+    fw_linear_request lreq{};
+    fw_linear_result lres{};
+    int status() const { return linear ? lres.status : result.status; }
 };
+
+// Device memory of one linear stage: the uploaded inputs, the smoothed copies with the Deriche
+// temporaries, the device MI level (16-byte samples, at most one per fixed voxel) and scratch.
+int estimate_linear(const fw_linear_request* q, uint64_t* out) {
+    using namespace fw;
+    HostGrid fg, mg;
+    FW_TRY(make_grid(&q->fixed_grid, fg));
+    FW_TRY(make_grid(&q->moving_grid, mg));
+    const fw_linear_recipe* r = &q->recipe;
+    FW_CHECK(r->levels >= 1 && r->levels <= FW_MAX_LEVELS, "serve: recipe has no levels");
+    const uint64_t nf = (uint64_t)fg.count(), nm = (uint64_t)mg.count();
+    uint64_t b = 0;
+    if (q->fixed) b += 4 * (nf + nm);
+    b += 4 * (nf + nm) + 24 * std::max(nf, nm);
+    b += 16 * nf + 4 * nm;
+    b += 4u << 20;
+    *out = b;
+    return 0;
+}
 
 int estimate(const fw_syn_request* q, uint64_t* out) {
     using namespace fw;
@@ -253,6 +276,43 @@ void run_job(fw_server* s, fw_ctx* ctx, Job* j) {
     }
 }
 
+void run_linear_job(fw_ctx* ctx, Job* j) {
+    using namespace fw;
+    fw_linear_result& res = j->lres;
+    const fw_linear_request& q = j->lreq;
+    res.tag = q.tag;
+    res.device_bytes = j->bytes;
+    res.nlevels = q.recipe.levels;
+    res.transform = q.start;
+    std::vector<fw_image*> up;
+    const fw_image *fi = nullptr, *mi = nullptr;
+    int rc = 0;
+    if (!j->fixed_dev.empty()) {
+        fi = j->fixed_dev[0];
+        mi = j->moving_dev[0];
+    } else {
+        HostGrid fg, mg;
+        rc = make_grid(&q.fixed_grid, fg);
+        if (!rc) rc = make_grid(&q.moving_grid, mg);
+        fw_image *a = nullptr, *b = nullptr;
+        if (!rc) rc = enqueue_image_upload_f32(ctx, fg, j->fixed_host[0], &a);
+        if (!rc) up.push_back(a);
+        if (!rc) rc = enqueue_image_upload_f32(ctx, mg, j->moving_host[0], &b);
+        if (!rc) up.push_back(b);
+        fi = a;
+        mi = b;
+    }
+    if (!rc) rc = fw_linear_stage_run(ctx, &q.recipe, fi, mi, &res.transform, res.levels);
+    for (auto* im : up) fw_image_free(im);
+    if (sync(ctx) && !rc) rc = FW_ERR_CUDA;
+    for (auto* p : j->fixed_host) pinned().put(p, j->fixed_bytes);
+    for (auto* p : j->moving_host) pinned().put(p, j->moving_bytes);
+    j->fixed_host.clear();
+    j->moving_host.clear();
+    res.status = rc;
+    if (rc) std::strncpy(res.error, fw_last_error(), sizeof(res.error) - 1);
+}
+
 void worker(fw_server* s, int slot) {
     cudaSetDevice(s->device);
     fw_ctx* ctx = s->ctxs[slot];
@@ -277,14 +337,17 @@ void worker(fw_server* s, int slot) {
             s->active++;
         }
         auto t0 = Clock::now();
-        j->result.queued_s = std::chrono::duration<double>(t0 - j->submitted).count();
-        run_job(s, ctx, j);
-        j->result.run_s = std::chrono::duration<double>(Clock::now() - t0).count();
+        const double queued = std::chrono::duration<double>(t0 - j->submitted).count();
+        if (j->linear) run_linear_job(ctx, j);
+        else run_job(s, ctx, j);
+        const double ran = std::chrono::duration<double>(Clock::now() - t0).count();
+        (j->linear ? j->lres.queued_s : j->result.queued_s) = queued;
+        (j->linear ? j->lres.run_s : j->result.run_s) = ran;
         {
             std::lock_guard<std::mutex> lock(s->mu);
             s->reserved -= j->bytes;
             s->active--;
-            if (j->result.status) s->failed++;
+            if (j->status()) s->failed++;
             else s->completed++;
             j->done = true;
         }
@@ -424,6 +487,7 @@ int fw_server_wait(fw_server* s, uint64_t ticket, double timeout_s, fw_syn_resul
     auto it = s->jobs.find(ticket);
     if (it == s->jobs.end()) return fail(FW_ERR_INVALID, "serve: unknown or already taken ticket");
     Job* j = it->second;
+    if (j->linear) return fail(FW_ERR_INVALID, "serve: the ticket is a linear-stage request");
     auto ready = [&] { return j->done; };
     if (timeout_s < 0) {
         s->cv_done.wait(lock, ready);
@@ -431,6 +495,83 @@ int fw_server_wait(fw_server* s, uint64_t ticket, double timeout_s, fw_syn_resul
         return fail(FW_ERR_TIMEOUT, "serve: the request is not done yet");
     }
     *out = j->result;
+    s->jobs.erase(it);
+    delete j;
+    return 0;
+}
+
+int fw_server_estimate_linear(const fw_linear_request* req, uint64_t* bytes) {
+    FW_CHECK(req && bytes, "null argument");
+    return estimate_linear(req, bytes);
+}
+
+int fw_server_submit_linear(fw_server* s, const fw_linear_request* req, uint64_t* ticket) {
+    FW_CHECK(s && req && ticket, "null argument");
+    const bool host = req->fixed && req->moving;
+    const bool dev = req->fixed_dev && req->moving_dev;
+    FW_CHECK(host != dev, "serve: give either host or device images");
+    uint64_t bytes = 0;
+    FW_TRY(estimate_linear(req, &bytes));
+    if (bytes > s->budget)
+        return fail(FW_ERR_MEMORY, "serve: the request needs " + std::to_string(bytes) +
+                                       " bytes of device memory, more than the budget of " +
+                                       std::to_string(s->budget));
+    HostGrid fg, mg;
+    FW_TRY(make_grid(&req->fixed_grid, fg));
+    FW_TRY(make_grid(&req->moving_grid, mg));
+    Job* j = new Job();
+    j->linear = true;
+    j->lreq = *req;
+    j->bytes = bytes;
+    if (host) {
+        j->fixed_bytes = sizeof(float) * (size_t)fg.count();
+        j->moving_bytes = sizeof(float) * (size_t)mg.count();
+        float* a = static_cast<float*>(pinned().get(j->fixed_bytes));
+        float* b = static_cast<float*>(pinned().get(j->moving_bytes));
+        if (!a || !b) {
+            pinned().put(a, j->fixed_bytes);
+            pinned().put(b, j->moving_bytes);
+            delete j;
+            return fail(FW_ERR_MEMORY, "serve: pinned host staging allocation failed");
+        }
+        std::memcpy(a, req->fixed, j->fixed_bytes);
+        std::memcpy(b, req->moving, j->moving_bytes);
+        j->fixed_host.push_back(a);
+        j->moving_host.push_back(b);
+    } else {
+        j->fixed_dev.push_back(req->fixed_dev);
+        j->moving_dev.push_back(req->moving_dev);
+    }
+    j->lreq.fixed = j->lreq.moving = nullptr;
+    j->lreq.fixed_dev = j->lreq.moving_dev = nullptr;
+    j->submitted = Clock::now();
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        j->ticket = s->next_ticket++;
+        s->jobs[j->ticket] = j;
+        s->queue.push_back(j);
+        s->submitted++;
+    }
+    s->cv_work.notify_all();
+    *ticket = j->ticket;
+    return 0;
+}
+
+int fw_server_wait_linear(fw_server* s, uint64_t ticket, double timeout_s,
+                          fw_linear_result* out) {
+    FW_CHECK(s && out, "null argument");
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return fail(FW_ERR_INVALID, "serve: unknown or already taken ticket");
+    Job* j = it->second;
+    if (!j->linear) return fail(FW_ERR_INVALID, "serve: the ticket is a SyN request");
+    auto ready = [&] { return j->done; };
+    if (timeout_s < 0) {
+        s->cv_done.wait(lock, ready);
+    } else if (!s->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), ready)) {
+        return fail(FW_ERR_TIMEOUT, "serve: the request is not done yet");
+    }
+    *out = j->lres;
     s->jobs.erase(it);
     delete j;
     return 0;
@@ -515,5 +656,7 @@ extern "C" size_t fw_abi_struct_size(const char* name) {
     if (n == "fw_transform_elem") return sizeof(fw_transform_elem);
     if (n == "fw_linear_recipe") return sizeof(fw_linear_recipe);
     if (n == "fw_linear_level_trace") return sizeof(fw_linear_level_trace);
+    if (n == "fw_linear_request") return sizeof(fw_linear_request);
+    if (n == "fw_linear_result") return sizeof(fw_linear_result);
     return 0;
 }

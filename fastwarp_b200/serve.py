@@ -60,6 +60,19 @@ class ServerStats(C.Structure):
         "peak_reserved_bytes", "budget_bytes", "kernel_launches", "graph_launches")]
 
 
+class LinearRequest(C.Structure):
+    _fields_ = [("recipe", N.LinearRecipe), ("fixed_grid", N.Grid), ("moving_grid", N.Grid),
+                ("fixed", C.c_void_p), ("moving", C.c_void_p), ("fixed_dev", C.c_void_p),
+                ("moving_dev", C.c_void_p), ("start", N.LinearTransform), ("tag", C.c_uint64)]
+
+
+class LinearResultC(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("status", C.c_int32), ("error", C.c_char * 256),
+                ("transform", N.LinearTransform), ("nlevels", C.c_int32),
+                ("levels", N.LinearLevelTrace * 8), ("device_bytes", C.c_uint64),
+                ("queued_s", C.c_double), ("run_s", C.c_double)]
+
+
 class Server:
     def __init__(self, device: int = 0, budget_bytes: int = 0, slots: int = 4):
         h = C.c_void_p()
@@ -160,6 +173,39 @@ class Server:
         else:
             lib().fw_server_result_free(C.byref(r))
         return out
+
+    def submit_linear(self, recipe: N.LinearRecipe, fixed_grid, fixed, moving_grid, moving,
+                      start: N.LinearTransform, tag=0) -> int:
+        """Queues one linear stage (run_linear_stage); `fixed`/`moving` are host float arrays
+        (copied at submit) or device `Image`s. Returns the ticket."""
+        q = LinearRequest()
+        q.recipe, q.fixed_grid, q.moving_grid, q.start, q.tag = (recipe, fixed_grid, moving_grid,
+                                                                 start, int(tag))
+        if isinstance(fixed, Image):
+            q.fixed_dev, q.moving_dev = fixed.handle.value, moving.handle.value
+            keep = [fixed, moving]
+        else:
+            fa = np.ascontiguousarray(fixed, np.float32)
+            ma = np.ascontiguousarray(moving, np.float32)
+            q.fixed, q.moving = fa.ctypes.data, ma.ctypes.data
+            keep = [fa, ma]
+        t = C.c_uint64()
+        check(lib().fw_server_submit_linear(self.handle, C.byref(q), C.byref(t)))
+        self._keep[int(t.value)] = keep
+        return int(t.value)
+
+    def wait_linear(self, ticket: int, timeout: float = -1.0) -> dict:
+        r = LinearResultC()
+        check(lib().fw_server_wait_linear(self.handle, C.c_uint64(ticket), C.c_double(timeout),
+                                          C.byref(r)))
+        self._keep.pop(ticket, None)
+        n = 6 if r.transform.kind == 0 else 12
+        return {"tag": r.tag, "status": r.status, "error": r.error.decode(errors="replace"),
+                "transform": r.transform, "parameters": list(r.transform.parameters[:n]),
+                "levels": [dict(samples=lv.samples, skipped=bool(lv.skipped),
+                                iterations=lv.cg.iterations, best_value=lv.cg.best_value)
+                           for lv in r.levels[:r.nlevels]],
+                "device_bytes": r.device_bytes, "queued_s": r.queued_s, "run_s": r.run_s}
 
     @staticmethod
     def free_device_fields(result: dict):

@@ -64,6 +64,34 @@ typedef struct fw_syn_result {
     double device_end_ms;
 } fw_syn_result;
 
+/* One linear-stage request (run_linear_stage, linear.rs:512-597; the reference's affine-only
+ * registrations): host float32 images (copied at submit) or device images made on any context of
+ * the same device (kept alive until the result is taken). `start` is the start transform, with
+ * the earlier transforms as its outer part. */
+typedef struct fw_linear_request {
+    fw_linear_recipe recipe;
+    fw_grid fixed_grid;
+    fw_grid moving_grid;
+    const float* fixed;                /* host, or NULL */
+    const float* moving;
+    const fw_image* fixed_dev;         /* device, or NULL */
+    const fw_image* moving_dev;
+    fw_linear_transform start;
+    uint64_t tag;
+} fw_linear_request;
+
+typedef struct fw_linear_result {
+    uint64_t tag;
+    int32_t status;                    /* FW_OK or an FW_ERR_* code */
+    char error[256];
+    fw_linear_transform transform;     /* the optimised transform */
+    int32_t nlevels;
+    fw_linear_level_trace levels[FW_MAX_LEVELS];
+    uint64_t device_bytes;             /* the admission estimate of this request */
+    double queued_s;                   /* submit -> start (host clock) */
+    double run_s;                      /* start -> done (host clock) */
+} fw_linear_result;
+
 typedef struct fw_server_stats {
     uint64_t submitted, completed, failed;
     uint64_t active, queued;
@@ -88,6 +116,11 @@ int fw_server_mark(fw_server* s);
 int fw_server_stats_get(fw_server* s, fw_server_stats* out);
 /* The device-memory estimate the server admits a request by. */
 int fw_server_estimate(const fw_syn_request* req, uint64_t* bytes);
+/* Linear-stage requests share the slots, the queue and the HBM budget with SyN requests; a
+ * ticket is waited for with the function of its kind (the other one fails). */
+int fw_server_submit_linear(fw_server* s, const fw_linear_request* req, uint64_t* ticket);
+int fw_server_wait_linear(fw_server* s, uint64_t ticket, double timeout_s, fw_linear_result* out);
+int fw_server_estimate_linear(const fw_linear_request* req, uint64_t* bytes);
 /* Waits for every queued and running request, then stops the slots. */
 void fw_server_destroy(fw_server* s);
 
