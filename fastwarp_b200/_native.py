@@ -89,6 +89,14 @@ class LinearLevelTrace(C.Structure):
                 ("cg", CgTrace), ("parameters", C.c_double * 12)]
 
 
+class LinearChainResult(C.Structure):
+    _fields_ = [("initial_matrix", C.c_double * 9), ("initial_translation", C.c_double * 3),
+                ("initial_center", C.c_double * 3), ("rigid", LinearTransform),
+                ("affine", LinearTransform), ("rigid_levels", LinearLevelTrace * 8),
+                ("affine_levels", LinearLevelTrace * 8), ("total_matrix", C.c_double * 9),
+                ("total_translation", C.c_double * 3), ("total_center", C.c_double * 3)]
+
+
 METRIC_VALUE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform),
                               C.POINTER(C.c_double))
 METRIC_VALUE_DERIVATIVE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform),

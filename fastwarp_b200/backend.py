@@ -536,6 +536,25 @@ def run_linear_stage(backend: "CudaBackend", recipe: N.LinearRecipe, fixed: Imag
     return t, out
 
 
+def run_linear_chain(backend: "CudaBackend", rigid: N.LinearRecipe, affine: N.LinearRecipe,
+                     fixed_raw: Image, moving_raw: Image, fixed: Image, moving: Image) -> dict:
+    """run_linear_chain (linear.rs:1105-1212) on the device: the centre-of-mass initial
+    transform, the rigid and the affine stage, and the collapsed total, each affine transform
+    as (matrix, translation, centre) with y = M (x - c) + c + t."""
+    r = N.LinearChainResult()
+    check(lib().fw_linear_chain_run(backend.ctx, C.byref(rigid), C.byref(affine),
+                                    fixed_raw.handle, moving_raw.handle, fixed.handle,
+                                    moving.handle, C.byref(r)))
+
+    def m3(a):
+        return np.array(a[:]).reshape(3, 3)
+    return {"initial": (m3(r.initial_matrix), np.array(r.initial_translation[:]),
+                        np.array(r.initial_center[:])),
+            "rigid": list(r.rigid.parameters[:6]), "affine": list(r.affine.parameters[:12]),
+            "total": (m3(r.total_matrix), np.array(r.total_translation[:]),
+                      np.array(r.total_center[:]))}
+
+
 def cg_settings_ants(max_step_mm=0.1, iterations=100, threshold=1e-6, window=10) -> N.CgSettings:
     """CgSettings::ants (optimizer.rs:94-106)."""
     s = N.CgSettings()

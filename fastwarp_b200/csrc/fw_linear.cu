@@ -165,6 +165,39 @@ int download(fw_ctx* ctx, const fw_image* img, std::vector<double>& out) {
     return 0;
 }
 
+// init.rs:50-74 (centre_of_gravity): the intensity-weighted mean of the voxel centres, summed in
+// raster order.
+int centre_of_gravity(fw_ctx* ctx, const fw_image* img, double out[3]) {
+    std::vector<double> h;
+    FW_TRY(download(ctx, img, h));
+    const HostGrid& g = img->grid;
+    double mass = 0.0, cg[3] = {0.0, 0.0, 0.0};
+    size_t lin = 0;
+    for (int64_t k = 0; k < g.n[2]; ++k)
+        for (int64_t j = 0; j < g.n[1]; ++j)
+            for (int64_t i = 0; i < g.n[0]; ++i, ++lin) {
+                const double v = h[lin];
+                const double c[3] = {(double)i, (double)j, (double)k};
+                double p[3];
+                index_to_point(g, c, p);
+                mass += v;
+                for (int a = 0; a < 3; ++a) cg[a] += p[a] * v;
+            }
+    if (mass == 0.0) return fail(FW_ERR_INVALID, "total mass of the image is zero");
+    for (int a = 0; a < 3; ++a) out[a] = cg[a] / mass;
+    return 0;
+}
+
+// The optimised part of a stage's transform alone (ParametricTransform::to_affine) as a matrix
+// and an offset.
+void stage_map(const fw_linear_transform* t, double M[9], double off[3]) {
+    fw_linear_transform inner = *t;
+    const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    std::memcpy(inner.outer_matrix, eye, sizeof(eye));
+    for (int a = 0; a < 3; ++a) inner.outer_translation[a] = inner.outer_center[a] = 0.0;
+    linear_transform_map(&inner, M, off);
+}
+
 }  // namespace
 }  // namespace fw
 
@@ -325,6 +358,68 @@ int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* r, const fw_image* 
                         " stage has too few usable samples for Mattes mutual information (" + why +
                         "); use smaller shrink factors, a larger sampling percentage, a larger "
                         "fixed mask, or a finer registration grid (iso_mm)");
+    return 0;
+}
+
+// run_linear_chain_cached_async (linear.rs:1148-1212): the centre-of-mass initial transform
+// of the raw images (init.rs:76-86), the rigid stage from it, the affine stage from the rigid
+// result, and their collapse recentred on the affine stage's centre (with_center, :1071-1076).
+int fw_linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid, const fw_linear_recipe* affine,
+                        const fw_image* fixed_raw, const fw_image* moving_raw,
+                        const fw_image* fixed, const fw_image* moving,
+                        fw_linear_chain_result* out) {
+    FW_CHECK(ctx && rigid && affine && fixed_raw && moving_raw && fixed && moving && out,
+             "null argument");
+    std::memset(out, 0, sizeof(*out));
+    double fc[3], mc[3];
+    FW_TRY(centre_of_gravity(ctx, fixed_raw, fc));
+    FW_TRY(centre_of_gravity(ctx, moving_raw, mc));
+    const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    std::memcpy(out->initial_matrix, eye, sizeof(eye));
+    for (int a = 0; a < 3; ++a) {
+        out->initial_translation[a] = mc[a] - fc[a];
+        out->initial_center[a] = fc[a];
+    }
+    // the rigid stage: Euler3D at zero about the initial centre, the initial transform outside
+    fw_linear_transform& tr = out->rigid;
+    std::memcpy(tr.outer_matrix, eye, sizeof(eye));
+    for (int a = 0; a < 3; ++a) {
+        tr.outer_translation[a] = out->initial_translation[a];
+        tr.outer_center[a] = fc[a];
+        tr.center[a] = fc[a];
+    }
+    tr.kind = 0;
+    FW_TRY(fw_linear_stage_run(ctx, rigid, fixed, moving, &tr, out->rigid_levels));
+    // after_rigid = initial o rigid as a matrix and an offset (the initial transform's matrix is
+    // the identity, so its offset is its translation)
+    double Mr[9], offr[3];
+    stage_map(&tr, Mr, offr);
+    double off_after[3];
+    for (int a = 0; a < 3; ++a) off_after[a] = offr[a] + out->initial_translation[a];
+    // the affine stage: identity about the rigid centre, after_rigid outside (centre zero)
+    fw_linear_transform& ta = out->affine;
+    std::memcpy(ta.outer_matrix, Mr, sizeof(Mr));
+    for (int a = 0; a < 3; ++a) {
+        ta.outer_translation[a] = off_after[a];
+        ta.outer_center[a] = 0.0;
+        ta.center[a] = tr.center[a];
+    }
+    ta.kind = 1;
+    for (int k = 0; k < 12; ++k) ta.parameters[k] = k < 9 ? eye[k] : 0.0;
+    FW_TRY(fw_linear_stage_run(ctx, affine, fixed, moving, &ta, out->affine_levels));
+    // collapsed = after_rigid o affine, recentred on the affine centre
+    double Ma[9], offa[3], M[9], off[3], mo[3];
+    stage_map(&ta, Ma, offa);
+    mat3_mul(Mr, Ma, M);
+    mat3_vec(Mr, offa, mo);
+    for (int a = 0; a < 3; ++a) off[a] = mo[a] + off_after[a];
+    double mcen[3];
+    mat3_vec(M, ta.center, mcen);
+    std::memcpy(out->total_matrix, M, sizeof(M));
+    for (int a = 0; a < 3; ++a) {
+        out->total_center[a] = ta.center[a];
+        out->total_translation[a] = off[a] - ta.center[a] + mcen[a];
+    }
     return 0;
 }
 

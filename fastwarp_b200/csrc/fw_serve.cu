@@ -657,6 +657,7 @@ extern "C" size_t fw_abi_struct_size(const char* name) {
     if (n == "fw_linear_recipe") return sizeof(fw_linear_recipe);
     if (n == "fw_linear_level_trace") return sizeof(fw_linear_level_trace);
     if (n == "fw_linear_request") return sizeof(fw_linear_request);
+    if (n == "fw_linear_chain_result") return sizeof(fw_linear_chain_result);
     if (n == "fw_linear_result") return sizeof(fw_linear_result);
     return 0;
 }

@@ -547,6 +547,27 @@ int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* recipe, const fw_im
                         const fw_image* moving, fw_linear_transform* transform,
                         fw_linear_level_trace* traces);
 
+/* LinearChainResult (linear.rs:1078-1101): the centre-of-mass initial transform, both stages
+ * (each optimised transform with its outer part, and its level traces) and the collapsed
+ * initial(rigid(affine(x))) with the affine stage's centre (what 0GenericAffine.mat holds). An
+ * affine transform here is y = matrix (x - center) + center + translation. */
+typedef struct fw_linear_chain_result {
+    double initial_matrix[9], initial_translation[3], initial_center[3];
+    fw_linear_transform rigid;
+    fw_linear_transform affine;
+    fw_linear_level_trace rigid_levels[FW_MAX_LEVELS];
+    fw_linear_level_trace affine_levels[FW_MAX_LEVELS];
+    double total_matrix[9], total_translation[3], total_center[3];
+} fw_linear_chain_result;
+
+/* run_linear_chain (linear.rs:1105-1212): the initial transform from the centres of mass of the
+ * raw (resampled, un-preprocessed) images, then the rigid stage and the affine stage on the
+ * preprocessed images (`rigid` and `affine` recipes, fw_linear_stage_run each). */
+int fw_linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid, const fw_linear_recipe* affine,
+                        const fw_image* fixed_raw, const fw_image* moving_raw,
+                        const fw_image* fixed, const fw_image* moving,
+                        fw_linear_chain_result* out);
+
 /* ---- profiling (crates/fastwarp-gpu/src/profiler.rs:8-60: per-op device timestamps) ----- */
 
 /* Times `reps` launches of each kernel of one SyN iteration on the grid of `fixed` with CUDA

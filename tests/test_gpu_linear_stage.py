@@ -1,4 +1,5 @@
-"""One linear stage (run_linear_stage, linear.rs:512-597) on the device against the oracle's
+"""One linear stage (run_linear_stage, linear.rs:512-597) and the rigid + affine chain
+(run_linear_chain, linear.rs:1105-1212) on the device against the oracle's
 pieces composed the same way: per level the shrunk virtual grid, Deriche smoothing, regular
 sampling with the stage's seed sequence, sample preparation and the conjugate-gradient optimiser
 over Mattes MI.
@@ -13,7 +14,8 @@ import pytest
 
 import oracle as O
 from fastwarp_b200 import FastwarpError, linear_transform
-from fastwarp_b200.backend import grid_corners, linear_recipe, run_linear_stage
+from fastwarp_b200.backend import (grid_corners, linear_recipe, run_linear_chain,
+                                   run_linear_stage)
 from fastwarp_b200.phantoms import blob_pair
 
 pytestmark = pytest.mark.gpu
@@ -25,11 +27,13 @@ def ogrid(g):
 
 
 def oracle_stage(g, fixed, moving, kind, start, center, iterations, shrink, sigmas, step=0.1,
-                 pct=0.25, bins=32, seed=1):
-    """run_linear_stage restated over the oracle's pieces (sigmas in voxels)."""
+                 pct=0.25, bins=32, seed=1, outer=(np.eye(3), (0, 0, 0), (0, 0, 0))):
+    """run_linear_stage restated over the oracle's pieces (sigmas in voxels); `outer` is the
+    earlier transforms as (matrix, translation, centre)."""
     og = ogrid(g)
     fixed, moving = fixed.astype(np.float64), moving.astype(np.float64)
-    t = O.linear_transform(kind, start, center=center)
+    t = O.linear_transform(kind, start, center=center, outer_matrix=outer[0],
+                           outer_translation=outer[1], outer_center=outer[2])
     out = []
     for level, (its, sf, sg) in enumerate(zip(iterations, shrink, sigmas)):
         f = O.shrink_factors(sf, tuple(g.spacing))
@@ -96,3 +100,44 @@ def test_a_stage_whose_levels_all_see_one_fixed_value_is_refused(backend):
         run_linear_stage(backend, r, backend.upload_image(g, flat),
                          backend.upload_image(g, moving),
                          linear_transform("euler", [0.0] * 6, center=(11.5, 11.5, 11.5)))
+
+
+def inner_map(t):
+    """The optimised part of a stage's transform alone, as (matrix, offset)."""
+    n = 6 if t.kind == 0 else 12
+    return O.linear_map(O.linear_transform("euler" if t.kind == 0 else "affine",
+                                           list(t.parameters[:n]), center=tuple(t.center)))
+
+
+def test_the_linear_chain_matches_the_oracle(backend):
+    """Centre-of-mass start, rigid stage, affine stage from the rigid result, collapsed total."""
+    g, fixed, moving = blob_pair(40, seed=29)
+    its, shrink, sigmas = (10, 6), (2, 1), (1.0, 0.0)
+    r = linear_recipe(iterations=its, shrink_factors=shrink, smoothing_sigmas=sigmas)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    out = run_linear_chain(backend, r, r, fi, mi, fi, mi)
+    nz, ny, nx = fixed.shape
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    pts = [g.origin[a] + g.spacing[a] * v for a, v in enumerate((x, y, z))]
+
+    def cog(v):
+        v = v.astype(np.float64)
+        return np.array([(p * v).sum() for p in pts]) / v.sum()
+    fc, mc = cog(fixed), cog(moving)
+    assert np.abs(out["initial"][2] - fc).max() < 1e-9
+    assert np.abs(out["initial"][1] - (mc - fc)).max() < 1e-9
+    rt, _ = oracle_stage(g, fixed, moving, "euler", [0.0] * 6, tuple(fc), its, shrink, sigmas,
+                         outer=(np.eye(3), tuple(mc - fc), tuple(fc)))
+    mr, offr = inner_map(rt)
+    off_after = offr + (mc - fc)
+    at, _ = oracle_stage(g, fixed, moving, "affine", list(np.eye(3).ravel()) + [0.0] * 3,
+                         tuple(fc), its, shrink, sigmas, outer=(mr, tuple(off_after), (0, 0, 0)))
+    ma, offa = inner_map(at)
+    total_m, total_off = mr @ ma, mr @ offa + off_after
+    dm, dt, dc = out["total"]
+    shift = max(np.linalg.norm((dm @ (c - dc) + dc + dt) - (total_m @ c + total_off))
+                for c in grid_corners(g))
+    print(f"chain: corner shift {shift:.2e} mm")
+    assert shift < 0.05, shift
+    assert np.abs(dc - fc).max() < 1e-9  # the total keeps the affine stage's centre
+    assert max(abs(v) for v in out["rigid"]) > 1e-4  # the rigid stage moved
