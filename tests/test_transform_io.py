@@ -123,6 +123,44 @@ def test_mat_file_is_193_bytes_per_affine_and_equals_the_oracle():
     assert T.format_mat([a, a]) == m + m
 
 
+def decode_ants_mat(raw):
+    """An independent decode of a MATLAB v4 file ANTs wrote for one affine transform: the
+    AffineTransform_double_3_3 variable (9 matrix values row by row, then 3 translation values)
+    and the `fixed` variable (the centre), each a header of five little-endian u32s, the
+    variable's name with its NUL, then float64 data (samples.rs:34-67 reads the same offsets)."""
+    out = {}
+    at = 0
+    while at < len(raw):
+        mopt, mrows, ncols, imagf, namelen = struct.unpack("<5I", raw[at:at + 20])
+        assert mopt == 0 and ncols == 1 and imagf == 0
+        name = raw[at + 20:at + 20 + namelen - 1].decode()
+        data_at = at + 20 + namelen
+        out[name] = np.frombuffer(raw[data_at:data_at + 8 * mrows], "<f8")
+        at = data_at + 8 * mrows
+    return out
+
+
+@pytest.mark.parametrize("name", ["ms0.mat", "ms20.mat"])
+def test_mat_writer_reproduces_the_ants_fixtures_byte_for_byte(name):
+    """The reference's ANTs-written .mat fixtures (crates/fastwarp-reg/tests/data/ms0.mat and
+    ms20.mat, copied by tests/golden/make_mat_golden.py): all 193 bytes come back from the
+    decoded matrix, translation and centre (tests/samples.rs:34-67)."""
+    raw = open(os.path.join(HERE, "golden", "ants_" + name), "rb").read()
+    assert len(raw) == 193
+    v = decode_ants_mat(raw)
+    assert set(v) == {"AffineTransform_double_3_3", "fixed"}
+    p, c = v["AffineTransform_double_3_3"], v["fixed"]
+    assert abs(np.linalg.det(p[:9].reshape(3, 3)) - 1.0) < 1e-6  # an ANTs rigid result
+    out = T.format_mat([T.affine(p[:9].reshape(3, 3), p[9:], c)])
+    assert out == raw
+    assert O.format_mat([O.affine(p[:9].reshape(3, 3), p[9:], c)]) == raw
+    if name == "ms0.mat":  # samples.rs:70-81
+        assert p[0] == 0.9998442385050702 and p[1] == 0.01355877025201078
+        assert p[8] == 0.9998821761749128
+        assert list(p[9:]) == [-2.675791891854692, -290.9203827342067, 148.534870757413]
+        assert list(c) == [-5.927373278, -3.158446675, -46.74841833]
+
+
 def test_fields_in_a_mat_file_and_empty_chains_are_refused():
     g, d, _ = sample_field()
     with pytest.raises(FastwarpError, match="in a .mat file"):
