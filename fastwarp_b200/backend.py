@@ -157,6 +157,12 @@ class CudaBackend:
     def reset_stats(self):
         lib().fw_ctx_reset_stats(self.ctx)
 
+    def request_cancel(self, on: bool = True) -> None:
+        """fw_ctx_request_cancel: the context's own cancel flag, which the SyN level graph reads
+        once per iteration (a run stops after the iteration in flight and fails with
+        FW_ERR_CANCELLED). It stays set until cleared with on=False."""
+        check(lib().fw_ctx_request_cancel(self.ctx, C.c_int32(1 if on else 0)))
+
     def synchronize(self):
         check(lib().fw_ctx_synchronize(self.ctx))
 
@@ -464,6 +470,13 @@ class MiLevel:
         n = 6 if t.kind == 0 else 12
         return v.value, np.array(d[:n])
 
+    def time_passes(self, t: N.LinearTransform, reps: int = 20):
+        """fw_mi_level_time: mean ms and algorithmic bytes per launch of the histogram pass,
+        ComputeResults and the gradient pass (CUDA events on the context's stream)."""
+        ms, by = (C.c_double * 3)(), (C.c_double * 3)()
+        check(lib().fw_mi_level_time(self.handle, C.byref(t), C.c_int32(reps), ms, by))
+        return {k: (ms[i], by[i]) for i, k in enumerate(("hist", "finish", "deriv"))}
+
     def num_valid(self) -> int:
         v = C.c_int64()
         check(lib().fw_mi_level_num_valid(self.handle, C.byref(v)))
@@ -501,6 +514,19 @@ class CudaLinearEngine:
                                         C.byref(h)))
         return MiLevel(self.backend, h)
 
+    def prepare_level_regular(self, level_grid: N.Grid, fixed: Image, moving: Image,
+                              percentage: float = 0.25, seed: int = 1, bins: int = 32,
+                              fixed_mask: Image | None = None) -> MiLevel:
+        """The level a linear stage prepares from device images at the level's smoothing:
+        regular samples of `level_grid`, binning and fixed bins on the host, then the device
+        level (fw_mi_level_prepare_regular)."""
+        h = C.c_void_p()
+        check(lib().fw_mi_level_prepare_regular(
+            self.backend.ctx, C.byref(level_grid), fixed.handle, moving.handle,
+            fixed_mask.handle if fixed_mask is not None else None, C.c_float(percentage),
+            C.c_uint32(seed), C.c_int32(bins), C.byref(h)))
+        return MiLevel(self.backend, h)
+
 
 # ---- the linear-stage optimiser (optimizer.rs:60-435) --------------------------------------------
 
@@ -522,12 +548,16 @@ def linear_recipe(iterations=(1000, 500, 250, 100), shrink_factors=(8, 4, 2, 1),
 
 
 def run_linear_stage(backend: "CudaBackend", recipe: N.LinearRecipe, fixed: Image,
-                     moving: Image, start: N.LinearTransform):
-    """run_linear_stage (linear.rs:512-597) on the device: (transform, [level trace dicts])."""
+                     moving: Image, start: N.LinearTransform, fixed_mask: Image | None = None):
+    """run_linear_stage (linear.rs:512-597) on the device: (transform, [level trace dicts]).
+    `fixed_mask` (an image on its own grid, non-zero inside) keeps only the sample points inside
+    it (LinearRecipe::mask, linear.rs:940-945)."""
     t = N.LinearTransform.from_buffer_copy(start)
     traces = (N.LinearLevelTrace * recipe.levels)()
-    check(lib().fw_linear_stage_run(backend.ctx, C.byref(recipe), fixed.handle, moving.handle,
-                                    C.byref(t), traces))
+    check(lib().fw_linear_stage_run_masked(backend.ctx, C.byref(recipe), fixed.handle,
+                                           moving.handle,
+                                           fixed_mask.handle if fixed_mask is not None else None,
+                                           C.byref(t), traces))
     n = 6 if t.kind == 0 else 12
     out = [dict(level=tr.level, shrink_factors=tuple(tr.shrink_factors),
                 grid_size=tuple(tr.grid_size), samples=tr.samples, skipped=bool(tr.skipped),
@@ -537,20 +567,26 @@ def run_linear_stage(backend: "CudaBackend", recipe: N.LinearRecipe, fixed: Imag
 
 
 def run_linear_chain(backend: "CudaBackend", rigid: N.LinearRecipe, affine: N.LinearRecipe,
-                     fixed_raw: Image, moving_raw: Image, fixed: Image, moving: Image) -> dict:
+                     fixed_raw: Image, moving_raw: Image, fixed: Image, moving: Image,
+                     fixed_mask: Image | None = None) -> dict:
     """run_linear_chain (linear.rs:1105-1212) on the device: the centre-of-mass initial
     transform, the rigid and the affine stage, and the collapsed total, each affine transform
-    as (matrix, translation, centre) with y = M (x - c) + c + t."""
+    as (matrix, translation, centre) with y = M (x - c) + c + t. `fixed_mask` restricts both
+    stages' samples."""
     r = N.LinearChainResult()
-    check(lib().fw_linear_chain_run(backend.ctx, C.byref(rigid), C.byref(affine),
-                                    fixed_raw.handle, moving_raw.handle, fixed.handle,
-                                    moving.handle, C.byref(r)))
+    check(lib().fw_linear_chain_run_masked(backend.ctx, C.byref(rigid), C.byref(affine),
+                                           fixed_raw.handle, moving_raw.handle, fixed.handle,
+                                           moving.handle,
+                                           fixed_mask.handle if fixed_mask is not None else None,
+                                           C.byref(r)))
 
     def m3(a):
         return np.array(a[:]).reshape(3, 3)
     return {"initial": (m3(r.initial_matrix), np.array(r.initial_translation[:]),
                         np.array(r.initial_center[:])),
             "rigid": list(r.rigid.parameters[:6]), "affine": list(r.affine.parameters[:12]),
+            "rigid_samples": [r.rigid_levels[k].samples for k in range(rigid.levels)],
+            "affine_samples": [r.affine_levels[k].samples for k in range(affine.levels)],
             "total": (m3(r.total_matrix), np.array(r.total_translation[:]),
                       np.array(r.total_center[:]))}
 

@@ -686,6 +686,19 @@ int fw_ctx_create(int device, fw_ctx** out) {
         fw_ctx_destroy(ctx);
         return fail(FW_ERR_MEMORY, "context scratch allocation failed");
     }
+    // the cancel flag the device can read: one int of mapped pinned host memory
+    void* flag = nullptr;
+    void* flag_dev = nullptr;
+    if (cudaHostAlloc(&flag, 64, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess ||
+        cudaHostGetDevicePointer(&flag_dev, flag, 0) != cudaSuccess) {
+        cudaGetLastError();
+        if (flag) cudaFreeHost(flag);
+        fw_ctx_destroy(ctx);
+        return fail(FW_ERR_MEMORY, "context cancel flag allocation failed");
+    }
+    ctx->cancel_mapped = static_cast<volatile int32_t*>(flag);
+    *ctx->cancel_mapped = 0;
+    ctx->cancel_mapped_dev = static_cast<const volatile int32_t*>(flag_dev);
     int rc = ensure_scratch(ctx, 1 << 16);
     if (rc) {
         fw_ctx_destroy(ctx);
@@ -707,6 +720,7 @@ void fw_ctx_destroy(fw_ctx* ctx) {
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->cancel_mapped) cudaFreeHost(const_cast<int32_t*>(ctx->cancel_mapped));
     if (ctx->done) cudaEventDestroy(ctx->done);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->aux) cudaStreamDestroy(ctx->aux);
@@ -751,6 +765,12 @@ void fw_ctx_reset_stats(fw_ctx* ctx) {
 int fw_ctx_set_cancel_flag(fw_ctx* ctx, const volatile int32_t* flag) {
     FW_CHECK(ctx, "null context");
     ctx->cancel = flag;
+    return 0;
+}
+
+int fw_ctx_request_cancel(fw_ctx* ctx, int32_t on) {
+    FW_CHECK(ctx && ctx->cancel_mapped, "null context");
+    *ctx->cancel_mapped = on ? 1 : 0;
     return 0;
 }
 

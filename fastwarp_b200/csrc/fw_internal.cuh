@@ -90,7 +90,11 @@ struct fw_ctx {
     double* h_pinned = nullptr;      // pinned host scalars for read-backs
     fw_stats stats{};
     std::atomic<uint64_t> live_bytes{0};
-    const volatile int32_t* cancel = nullptr;
+    const volatile int32_t* cancel = nullptr;  // the caller's flag (fw_ctx_set_cancel_flag)
+    // the context's own flag (fw_ctx_request_cancel) in mapped pinned host memory: the host view
+    // and the device view, which the level graph's record kernel reads once per iteration
+    volatile int32_t* cancel_mapped = nullptr;
+    const volatile int32_t* cancel_mapped_dev = nullptr;
     bool capturing = false;          // a graph capture is in progress on `stream`
     cudaStream_t aux = nullptr;      // second stream for capturing conditional bodies
     cudaEvent_t done = nullptr;      // blocking-sync event the host waits on
@@ -118,6 +122,11 @@ struct fw_field {
 };
 
 namespace fw {
+
+// Whether a cancel has been asked for, through the caller's flag or the context's own.
+inline bool cancel_requested(const fw_ctx* ctx) {
+    return (ctx->cancel && *ctx->cancel) || (ctx->cancel_mapped && *ctx->cancel_mapped);
+}
 
 // stream-ordered allocation from the device's memory pool (kept cached: the buffer pool)
 int dev_alloc(fw_ctx* ctx, size_t bytes, void** out);
@@ -438,6 +447,8 @@ int enqueue_image_upload_f32(fw_ctx* ctx, const HostGrid& g, const float* host, 
 
 // transform/param.rs:421-446: outer(optimised(p)) as one affine map y = M p + off (fw_mi.cu).
 void linear_transform_map(const fw_linear_transform* t, double M[9], double off[3]);
+// The context a device MI level evaluates on (fw_mi.cu).
+const fw_ctx* mi_level_context(const fw_mi_level* level);
 
 // The SyN stage on device images (fw_syn.cu); masks may be null; prior / prior_inverse are the
 // earlier SyN stages' collapsed fields (both null for a first stage).

@@ -7,11 +7,13 @@
 // MI undefined is skipped (linear.rs:474-492), the samples are prepared (fixed range from the
 // nearest voxels, moving range from the whole image, fixed bins from trilinear values;
 // linear.rs:251-280, metric/mi.rs:121-317) and the conjugate-gradient optimiser runs on the
-// device level (fw_mi_level_optimize). Sampling and sample preparation are host work, as in the
+// device level (fw_mi_level_optimize). With a fixed mask only the sample points inside it are
+// kept (linear.rs:940-945). Sampling and sample preparation are host work, as in the
 // reference (they run once per level over the level's samples); every metric evaluation is on
 // the device.
 #include "fw_internal.cuh"
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -201,14 +203,124 @@ void stage_map(const fw_linear_transform* t, double M[9], double off[3]) {
 }  // namespace
 }  // namespace fw
 
-using namespace fw;
+namespace fw {
+namespace {
 
-extern "C" {
+// mask.rs:76-110 (MaskVolume::is_inside): the nearest voxel of the mask (rounding half up) must be
+// inside its buffer and not zero; the mask is evaluated in physical space on its own grid.
+struct HostMask {
+    HostGrid grid;
+    std::vector<float> data;
+    bool inside(const double p[3]) const {
+        double c[3];
+        point_to_index(grid, p, c);
+        int64_t q[3];
+        for (int a = 0; a < 3; ++a) {
+            const double r = std::floor(c[a] + 0.5);
+            if (!(r >= 0.0 && r < (double)grid.n[a])) return false;
+            q[a] = (int64_t)r;
+        }
+        return data[(size_t)(q[0] + grid.n[0] * (q[1] + grid.n[1] * q[2]))] != 0.0f;
+    }
+};
 
-int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* r, const fw_image* fixed,
-                        const fw_image* moving, fw_linear_transform* transform,
-                        fw_linear_level_trace* traces) {
-    FW_CHECK(ctx && r && fixed && moving && transform, "null argument");
+int load_mask(fw_ctx* ctx, const fw_image* mask, HostMask& out) {
+    out.grid = mask->grid;
+    out.data.resize((size_t)mask->grid.count());
+    FW_TRY(fw_image_download(ctx, mask, out.data.data()));
+    for (float v : out.data)
+        if (v != 0.0f) return 0;
+    return fail(FW_ERR_INVALID, "linear recipe: the fixed mask has no voxel inside (every voxel is zero)");
+}
+
+// One level's Mattes MI samples (linear.rs:474-492, 251-280, 940-945): the regular sample set
+// of the level grid `lg` from `seed` (only the points inside the fixed mask, when one is given);
+// `skip` with the reference's reason when MI is undefined on them; otherwise the binning (fixed
+// range at the samples' nearest voxels, moving range over the whole image, MiBinning::new,
+// metric/mi.rs:229-262) and the kept points with their trilinear fixed bins.
+int level_samples(const HostGrid& lg, const HostGrid& fg, const std::vector<double>& fh,
+                  const std::vector<double>& mh, const HostMask* mask, float percentage,
+                  uint32_t seed, int bins, std::vector<double>& kept, std::vector<uint32_t>& fbin,
+                  fw_mi_binning& b, bool& skip, std::string& why) {
+    skip = false;
+    kept.clear();
+    fbin.clear();
+    std::vector<double> raw = regular_samples(lg, percentage, seed);
+    if (mask) {
+        // linear.rs:940-945 / sampling.rs:225-228: with a fixed mask only the jittered points
+        // inside it are kept (every point still takes its six draws)
+        size_t w = 0;
+        for (size_t i = 0; i < raw.size() / 3; ++i) {
+            if (!mask->inside(&raw[3 * i])) continue;
+            for (int a = 0; a < 3; ++a) raw[3 * w + a] = raw[3 * i + a];
+            ++w;
+        }
+        raw.resize(3 * w);
+    }
+    const int64_t candidates = (int64_t)(raw.size() / 3);
+    double lo = 0, hi = 0;
+    int64_t seen = 0;
+    char msg[256];
+    if (!fixed_sample_range(fg, fh, raw, lo, hi, seen)) {
+        std::snprintf(msg, sizeof(msg), "no sample point lands on the fixed image inside the fixed "
+                      "mask, if one is given (%lld candidate points on the level grid)",
+                      (long long)candidates);
+        skip = true;
+    } else if (hi - lo <= DBL_EPSILON) {
+        std::snprintf(msg, sizeof(msg), "the fixed image takes a single value at its %lld sample "
+                      "point(s) (%lld candidate points)", (long long)seen, (long long)candidates);
+        skip = true;
+    }
+    if (skip) {
+        why = msg;
+        return 0;
+    }
+    bool mhave = false;
+    double mlo = 0, mhi = 0;
+    for (double v : mh) {
+        if (!std::isfinite(v)) continue;
+        if (!mhave) {
+            mlo = mhi = v;
+            mhave = true;
+        } else {
+            mlo = std::min(mlo, v);
+            mhi = std::max(mhi, v);
+        }
+    }
+    if (!mhave) return fail(FW_ERR_INVALID, "the moving image has no finite voxel");
+    if (mhi - mlo <= DBL_EPSILON) return fail(FW_ERR_INVALID, "the moving image is constant");
+    const double span = (double)(bins - 4);
+    b.bins = bins;
+    b.fixed_min = lo;
+    b.fixed_max = hi;
+    b.moving_min = mlo;
+    b.moving_max = mhi;
+    b.fixed_bin_size = (hi - lo) / span;
+    b.moving_bin_size = (mhi - mlo) / span;
+    b.fixed_normalized_min = lo / b.fixed_bin_size - 2.0;
+    b.moving_normalized_min = mlo / b.moving_bin_size - 2.0;
+    // prepare_samples (linear.rs:251-280): points whose trilinear fixed value exists, with its
+    // box-window bin
+    for (int64_t i = 0; i < candidates; ++i) {
+        double v;
+        if (!linear_at_point(fg, fh, &raw[(size_t)(3 * i)], v) || !std::isfinite(v)) continue;
+        kept.insert(kept.end(), &raw[(size_t)(3 * i)], &raw[(size_t)(3 * i)] + 3);
+        const double term = v / b.fixed_bin_size - b.fixed_normalized_min;
+        const int64_t idx = std::isnan(term) ? 0 : (int64_t)term;
+        fbin.push_back((uint32_t)std::min<int64_t>(std::max<int64_t>(idx, 2), bins - 3));
+    }
+    if (kept.empty()) {
+        std::snprintf(msg, sizeof(msg), "no sample point lies inside the fixed image (%lld "
+                      "candidate points)", (long long)candidates);
+        why = msg;
+        skip = true;
+    }
+    return 0;
+}
+
+int linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* r, const fw_image* fixed,
+                     const fw_image* moving, const HostMask* mask, fw_linear_transform* transform,
+                     fw_linear_level_trace* traces) {
     FW_CHECK(r->levels >= 1 && r->levels <= FW_MAX_LEVELS, "linear recipe: 1 to 8 levels");
     FW_CHECK(r->bins > 4, "at least five histogram bins are required");
     FW_CHECK(r->sampling_percentage > 0.0f && r->sampling_percentage <= 1.0f,
@@ -219,7 +331,7 @@ int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* r, const fw_image* 
     int skipped = 0;
     std::string why;
     for (int level = 0; level < r->levels; ++level) {
-        if (ctx->cancel && *ctx->cancel) return fail(FW_ERR_CANCELLED, "registration cancelled");
+        if (cancel_requested(ctx)) return fail(FW_ERR_CANCELLED, "registration cancelled");
         uint32_t f[3];
         FW_TRY(fw_shrink_factors(r->shrink_factors[level], fg.sp, f));
         const fw_grid fgc = to_c(fg);
@@ -252,78 +364,17 @@ int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* r, const fw_image* 
         if (!rc) rc = download(ctx, fl, fh);
         if (!rc) rc = download(ctx, ml, mh);
         // sampling and the level's usable samples
-        std::vector<double> raw, kept;
+        std::vector<double> kept;
         std::vector<uint32_t> fbin;
         fw_mi_binning b{};
         bool skip = false;
-        if (!rc) {
-            raw = regular_samples(lg, r->sampling_percentage, seed++);
-            const int64_t candidates = (int64_t)(raw.size() / 3);
-            double lo = 0, hi = 0;
-            int64_t seen = 0;
-            char msg[256];
-            if (!fixed_sample_range(fg, fh, raw, lo, hi, seen)) {
-                std::snprintf(msg, sizeof(msg), "no sample point lands on the fixed image inside "
-                              "the fixed mask, if one is given (%lld candidate points on the "
-                              "level grid)", (long long)candidates);
-                skip = true;
-            } else if (hi - lo <= DBL_EPSILON) {
-                std::snprintf(msg, sizeof(msg), "the fixed image takes a single value at its %lld "
-                              "sample point(s) (%lld candidate points)", (long long)seen,
-                              (long long)candidates);
-                skip = true;
-            }
-            if (!skip) {
-                // MiBinning::new (metric/mi.rs:229-262): fixed range over the samples, moving
-                // range over the whole image
-                bool mhave = false;
-                double mlo = 0, mhi = 0;
-                for (double v : mh) {
-                    if (!std::isfinite(v)) continue;
-                    if (!mhave) {
-                        mlo = mhi = v;
-                        mhave = true;
-                    } else {
-                        mlo = std::min(mlo, v);
-                        mhi = std::max(mhi, v);
-                    }
-                }
-                if (!mhave) rc = fail(FW_ERR_INVALID, "the moving image has no finite voxel");
-                else if (mhi - mlo <= DBL_EPSILON)
-                    rc = fail(FW_ERR_INVALID, "the moving image is constant");
-                if (!rc) {
-                    const double span = (double)(r->bins - 4);
-                    b.bins = r->bins;
-                    b.fixed_min = lo;
-                    b.fixed_max = hi;
-                    b.moving_min = mlo;
-                    b.moving_max = mhi;
-                    b.fixed_bin_size = (hi - lo) / span;
-                    b.moving_bin_size = (mhi - mlo) / span;
-                    b.fixed_normalized_min = lo / b.fixed_bin_size - 2.0;
-                    b.moving_normalized_min = mlo / b.moving_bin_size - 2.0;
-                    // prepare_samples (linear.rs:251-280): points whose trilinear fixed value
-                    // exists, with its box-window bin
-                    for (int64_t i = 0; i < candidates; ++i) {
-                        double v;
-                        if (!linear_at_point(fg, fh, &raw[(size_t)(3 * i)], v) || !std::isfinite(v))
-                            continue;
-                        kept.insert(kept.end(), &raw[(size_t)(3 * i)], &raw[(size_t)(3 * i)] + 3);
-                        const double term = v / b.fixed_bin_size - b.fixed_normalized_min;
-                        const int64_t idx = std::isnan(term) ? 0 : (int64_t)term;
-                        fbin.push_back((uint32_t)std::min<int64_t>(std::max<int64_t>(idx, 2),
-                                                                   r->bins - 3));
-                    }
-                    if (kept.empty()) {
-                        std::snprintf(msg, sizeof(msg), "no sample point lies inside the fixed "
-                                      "image (%lld candidate points)", (long long)candidates);
-                        skip = true;
-                    }
-                }
-            }
-            if (skip) why += std::string(why.empty() ? "" : "; ") + "level " +
-                             std::to_string(level + 1) + ": " + msg;
-        }
+        std::string msg;
+        if (!rc)
+            rc = level_samples(lg, fg, fh, mh, mask, r->sampling_percentage, seed++, r->bins, kept,
+                               fbin, b, skip, msg);
+        if (!rc && skip)
+            why += std::string(why.empty() ? "" : "; ") + "level " + std::to_string(level + 1) +
+                   ": " + msg;
         if (!rc && !skip) {
             fw_mi_level* lvl = nullptr;
             rc = fw_mi_level_prepare_image(ctx, ml, kept.data(), fbin.data(),
@@ -361,16 +412,71 @@ int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* r, const fw_image* 
     return 0;
 }
 
+}  // namespace
+}  // namespace fw
+
+using namespace fw;
+
+extern "C" {
+
+int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* r, const fw_image* fixed,
+                        const fw_image* moving, fw_linear_transform* transform,
+                        fw_linear_level_trace* traces) {
+    FW_CHECK(ctx && r && fixed && moving && transform, "null argument");
+    return linear_stage_run(ctx, r, fixed, moving, nullptr, transform, traces);
+}
+
+int fw_mi_level_prepare_regular(fw_ctx* ctx, const fw_grid* level_grid, const fw_image* fixed,
+                                const fw_image* moving, const fw_image* fixed_mask,
+                                float percentage, uint32_t seed, int32_t bins,
+                                fw_mi_level** out) {
+    FW_CHECK(ctx && level_grid && fixed && moving && out, "null argument");
+    FW_CHECK(bins > 4 && bins <= 32, "mattes: bins must be in 5..=32");
+    FW_CHECK(percentage > 0.0f && percentage <= 1.0f,
+             "linear recipe: the sampling percentage must lie in (0, 1]");
+    HostGrid lg;
+    FW_TRY(make_grid(level_grid, lg));
+    HostMask m;
+    if (fixed_mask) FW_TRY(load_mask(ctx, fixed_mask, m));
+    std::vector<double> fh, mh, kept;
+    FW_TRY(download(ctx, fixed, fh));
+    FW_TRY(download(ctx, moving, mh));
+    std::vector<uint32_t> fbin;
+    fw_mi_binning b{};
+    bool skip = false;
+    std::string why;
+    FW_TRY(level_samples(lg, fixed->grid, fh, mh, fixed_mask ? &m : nullptr, percentage, seed,
+                         bins, kept, fbin, b, skip, why));
+    if (skip) return fail(FW_ERR_INVALID, "mattes: " + why);
+    return fw_mi_level_prepare_image(ctx, moving, kept.data(), fbin.data(), (int64_t)fbin.size(),
+                                     &b, out);
+}
+
+int fw_linear_stage_run_masked(fw_ctx* ctx, const fw_linear_recipe* r, const fw_image* fixed,
+                               const fw_image* moving, const fw_image* fixed_mask,
+                               fw_linear_transform* transform, fw_linear_level_trace* traces) {
+    FW_CHECK(ctx && r && fixed && moving && transform, "null argument");
+    if (!fixed_mask) return linear_stage_run(ctx, r, fixed, moving, nullptr, transform, traces);
+    HostMask m;
+    FW_TRY(load_mask(ctx, fixed_mask, m));
+    return linear_stage_run(ctx, r, fixed, moving, &m, transform, traces);
+}
+
 // run_linear_chain_cached_async (linear.rs:1148-1212): the centre-of-mass initial transform
 // of the raw images (init.rs:76-86), the rigid stage from it, the affine stage from the rigid
 // result, and their collapse recentred on the affine stage's centre (with_center, :1071-1076).
-int fw_linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid, const fw_linear_recipe* affine,
-                        const fw_image* fixed_raw, const fw_image* moving_raw,
-                        const fw_image* fixed, const fw_image* moving,
-                        fw_linear_chain_result* out) {
+// The fixed mask (nullable) restricts both stages' samples (LinearRecipe::mask of each stage).
+static int linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid,
+                            const fw_linear_recipe* affine, const fw_image* fixed_raw,
+                            const fw_image* moving_raw, const fw_image* fixed,
+                            const fw_image* moving, const fw_image* fixed_mask,
+                            fw_linear_chain_result* out) {
     FW_CHECK(ctx && rigid && affine && fixed_raw && moving_raw && fixed && moving && out,
              "null argument");
     std::memset(out, 0, sizeof(*out));
+    HostMask mask;
+    if (fixed_mask) FW_TRY(load_mask(ctx, fixed_mask, mask));
+    const HostMask* mp = fixed_mask ? &mask : nullptr;
     double fc[3], mc[3];
     FW_TRY(centre_of_gravity(ctx, fixed_raw, fc));
     FW_TRY(centre_of_gravity(ctx, moving_raw, mc));
@@ -389,7 +495,7 @@ int fw_linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid, const fw_lin
         tr.center[a] = fc[a];
     }
     tr.kind = 0;
-    FW_TRY(fw_linear_stage_run(ctx, rigid, fixed, moving, &tr, out->rigid_levels));
+    FW_TRY(linear_stage_run(ctx, rigid, fixed, moving, mp, &tr, out->rigid_levels));
     // after_rigid = initial o rigid as a matrix and an offset (the initial transform's matrix is
     // the identity, so its offset is its translation)
     double Mr[9], offr[3];
@@ -406,7 +512,7 @@ int fw_linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid, const fw_lin
     }
     ta.kind = 1;
     for (int k = 0; k < 12; ++k) ta.parameters[k] = k < 9 ? eye[k] : 0.0;
-    FW_TRY(fw_linear_stage_run(ctx, affine, fixed, moving, &ta, out->affine_levels));
+    FW_TRY(linear_stage_run(ctx, affine, fixed, moving, mp, &ta, out->affine_levels));
     // collapsed = after_rigid o affine, recentred on the affine centre
     double Ma[9], offa[3], M[9], off[3], mo[3];
     stage_map(&ta, Ma, offa);
@@ -421,6 +527,22 @@ int fw_linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid, const fw_lin
         out->total_translation[a] = off[a] - ta.center[a] + mcen[a];
     }
     return 0;
+}
+
+int fw_linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid, const fw_linear_recipe* affine,
+                        const fw_image* fixed_raw, const fw_image* moving_raw,
+                        const fw_image* fixed, const fw_image* moving,
+                        fw_linear_chain_result* out) {
+    return linear_chain_run(ctx, rigid, affine, fixed_raw, moving_raw, fixed, moving, nullptr, out);
+}
+
+int fw_linear_chain_run_masked(fw_ctx* ctx, const fw_linear_recipe* rigid,
+                               const fw_linear_recipe* affine, const fw_image* fixed_raw,
+                               const fw_image* moving_raw, const fw_image* fixed,
+                               const fw_image* moving, const fw_image* fixed_mask,
+                               fw_linear_chain_result* out) {
+    return linear_chain_run(ctx, rigid, affine, fixed_raw, moving_raw, fixed, moving, fixed_mask,
+                            out);
 }
 
 }  // extern "C"

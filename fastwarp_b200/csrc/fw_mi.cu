@@ -17,6 +17,7 @@
 //    reference's sum_cell dpdf[cell] * ratio[cell], reordered.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstring>
 #include <vector>
@@ -829,6 +830,64 @@ int fw_mi_level_value_and_derivative(fw_mi_level* L, const fw_linear_transform* 
     return 0;
 }
 
+int fw_mi_level_time(fw_mi_level* L, const fw_linear_transform* t, int32_t reps, double ms[3],
+                     double bytes[3]) {
+    FW_CHECK(L && t && ms && bytes && reps > 0, "null argument");
+    fw_ctx* ctx = L->ctx;
+    // one evaluation first: the maps in scratch, the ratio table and the status
+    double v = 0.0, d[12];
+    FW_TRY(fw_mi_level_value_and_derivative(L, t, &v, d));
+    const int bins = L->binning.bins;
+    const int cells = bins * bins + bins;
+    const MiMap* d_maps = reinterpret_cast<const MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+        if (a) cudaEventDestroy(a);
+        return fail(FW_ERR_CUDA, "event creation failed");
+    }
+    int rc = 0;
+    for (int kind = 0; kind < 3 && !rc; ++kind) {
+        auto launch = [&]() -> int {
+            if (kind == 0) {
+                FW_CUDA(cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells,
+                                        ctx->stream));
+                k_mi_hist<<<dim3(L->blocks, 1), MI_THREADS, sizeof(unsigned long long) * cells,
+                            ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d, L->d_hist);
+                return check_launch(ctx, "k_mi_hist");
+            }
+            if (kind == 1) {
+                k_mi_finish<<<1, 1024, 0, ctx->stream>>>(L->d_hist, bins, L->binning.moving_bin_size,
+                                                         nullptr, L->d_ratio, L->d_out, 1);
+                return check_launch(ctx, "k_mi_finish");
+            }
+            k_mi_deriv<<<L->blocks, MI_THREADS, 0, ctx->stream>>>(d_maps, L->d_rec, L->n,
+                                                                  L->moving->d, L->d_ratio,
+                                                                  L->d_part, L->d_counter,
+                                                                  L->d_mom);
+            return check_launch(ctx, "k_mi_deriv");
+        };
+        rc = launch();  // warm-up
+        if (rc) break;
+        cudaEventRecord(a, ctx->stream);
+        for (int r = 0; r < reps && !rc; ++r) rc = launch();
+        cudaEventRecord(b, ctx->stream);
+        if (!rc) rc = sync(ctx);
+        float tm = 0.0f;
+        if (!rc) cudaEventElapsedTime(&tm, a, b);
+        ms[kind] = (double)tm / reps;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    // algorithmic bytes per pass: the 16-byte sample records plus the moving image's gathers,
+    // at most the whole image and at most one 8-corner gather per sample (32 bytes)
+    const double S = (double)L->n, Nm = (double)L->moving->grid.count();
+    const double pass = 16.0 * S + std::min(4.0 * Nm, 32.0 * S);
+    bytes[0] = pass + 8.0 * cells;
+    bytes[1] = 16.0 * cells;
+    bytes[2] = pass + 8.0 * bins * bins;
+    return rc;
+}
+
 int fw_mi_level_num_valid(const fw_mi_level* L, int64_t* out) {
     FW_CHECK(L && out, "null argument");
     *out = L->last_valid;
@@ -856,6 +915,8 @@ namespace fw {
 void linear_transform_map(const fw_linear_transform* t, double M[9], double off[3]) {
     linear_map(t, M, off);
 }
+
+const fw_ctx* mi_level_context(const fw_mi_level* level) { return level ? level->ctx : nullptr; }
 }  // namespace fw
 
 // ---- dense Mattes MI pair: host side -----------------------------------------------------------

@@ -196,7 +196,7 @@ double inner(const double* a, const double* b, int n) {
 // optimizer.rs:311-435
 int optimise_level(const Metric& metric, const double* corners, fw_linear_transform* t,
                    const fw_cg_settings& s, fw_cg_trace* trace, double* values, int64_t cap,
-                   const volatile int32_t* cancel) {
+                   const volatile int32_t* cancel, const fw_ctx* ctx = nullptr) {
     const int n = num_params(*t);
     double scales[12];
     estimate_scales(corners, *t, s.small_parameter_variation, scales);
@@ -211,7 +211,8 @@ int optimise_level(const Metric& metric, const double* corners, fw_linear_transf
     trace->initial_learning_rate = learning_rate;
     int iteration = 0;
     while (iteration < s.iterations) {
-        if (cancel && *cancel) return fail(FW_ERR_CANCELLED, "registration cancelled");
+        if ((cancel && *cancel) || (ctx && cancel_requested(ctx)))
+            return fail(FW_ERR_CANCELLED, "registration cancelled");
         double value;
         if (metric.value_derivative(metric.user, &current, &value, gradient) != 0)
             return fail(FW_ERR_INVALID, std::string("linear metric: ") + fw_last_error());
@@ -338,7 +339,9 @@ int fw_mi_level_optimize(fw_mi_level* level, const fw_cg_settings* settings,
     FW_CHECK(level && settings && corners && transform && trace, "null argument");
     FW_CHECK(transform->kind == 0 || transform->kind == 1, "linear transform: unknown kind");
     const Metric m{mi_value, mi_value_derivative, level};
-    return optimise_level(m, corners, transform, *settings, trace, values, cap, nullptr);
+    // the level's context: its cancel flags are polled before every iteration
+    return optimise_level(m, corners, transform, *settings, trace, values, cap, nullptr,
+                          mi_level_context(level));
 }
 
 }  // extern "C"

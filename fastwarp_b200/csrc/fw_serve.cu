@@ -76,6 +76,7 @@ struct Job {
     bool done = false;
     bool taken = false;
     bool linear = false;           // a linear-stage request (lreq / lres)
+    int slot = -1;                 // the slot running it (-1 while queued)
     fw_linear_request lreq{};
     fw_linear_result lres{};
     int status() const { return linear ? lres.status : result.status; }
@@ -332,6 +333,7 @@ void worker(fw_server* s, int slot) {
                 s->cv_work.wait(lock);
             }
             if (!j) return;
+            j->slot = slot;
             s->reserved += j->bytes;
             s->peak = std::max(s->peak, s->reserved);
             s->active++;
@@ -350,6 +352,8 @@ void worker(fw_server* s, int slot) {
             if (j->status()) s->failed++;
             else s->completed++;
             j->done = true;
+            // a cancel that came for this request ends with it: the slot's next request runs
+            fw_ctx_request_cancel(ctx, 0);
         }
         s->cv_done.notify_all();
         s->cv_work.notify_all();
@@ -497,6 +501,50 @@ int fw_server_wait(fw_server* s, uint64_t ticket, double timeout_s, fw_syn_resul
     *out = j->result;
     s->jobs.erase(it);
     delete j;
+    return 0;
+}
+
+int fw_server_cancel(fw_server* s, uint64_t ticket) {
+    FW_CHECK(s, "null server");
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        auto it = s->jobs.find(ticket);
+        if (it == s->jobs.end()) return fail(FW_ERR_INVALID, "serve: unknown or already taken ticket");
+        Job* j = it->second;
+        if (j->done) return 0;  // finished already: its result stands
+        if (j->slot >= 0) {
+            // running: the slot's context flag stops its level graph after the iteration in
+            // flight; the slot clears the flag when the request ends
+            return fw_ctx_request_cancel(s->ctxs[j->slot], 1);
+        }
+        // queued: it ends here without running
+        for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
+            if (*q == j) {
+                s->queue.erase(q);
+                break;
+            }
+        for (auto* p : j->fixed_host) pinned().put(p, j->fixed_bytes);
+        for (auto* p : j->moving_host) pinned().put(p, j->moving_bytes);
+        j->fixed_host.clear();
+        j->moving_host.clear();
+        for (int k = 0; k < 2; ++k) {
+            pinned().put(j->mask_host[k], j->mask_bytes[k]);
+            j->mask_host[k] = nullptr;
+        }
+        const char* why = "registration cancelled";
+        if (j->linear) {
+            j->lres.tag = j->lreq.tag;
+            j->lres.status = FW_ERR_CANCELLED;
+            std::strncpy(j->lres.error, why, sizeof(j->lres.error) - 1);
+        } else {
+            j->result.tag = j->req.tag;
+            j->result.status = FW_ERR_CANCELLED;
+            std::strncpy(j->result.error, why, sizeof(j->result.error) - 1);
+        }
+        j->done = true;
+        s->failed++;
+    }
+    s->cv_done.notify_all();
     return 0;
 }
 

@@ -620,10 +620,10 @@ int run_level_direct(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
     k_syn_level_init<<<1, 1, 0, ctx->stream>>>(d.syn, level, limit, 0, 0);
     FW_TRY(check_launch(ctx, "k_syn_level_init"));
     for (int it = 0; it < limit; ++it) {
-        if (ctx->cancel && *ctx->cancel) return fail(FW_ERR_CANCELLED, "registration cancelled");
+        if (cancel_requested(ctx)) return fail(FW_ERR_CANCELLED, "registration cancelled");
         FW_TRY(enqueue_iteration(ctx, false, r, L, fs, ms, initial, d));
         k_syn_record<<<1, 1, 0, ctx->stream>>>(d.syn, d.cc, d.max_bits, d.inv, trace_dev_base,
-                                              d.trace_cap, nullptr, 0, 0);
+                                              d.trace_cap, ctx->cancel_mapped_dev, 0, 0);
         FW_TRY(check_launch(ctx, "k_syn_record"));
         FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, d.syn, sizeof(SynDev), cudaMemcpyDeviceToHost,
                                 ctx->stream));
@@ -665,8 +665,11 @@ int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
         if (!rc) {
             rc = enqueue_iteration(ctx, true, r, L, fs, ms, initial, d);
             if (!rc) {
+                // the context's cancel flag is read once per iteration: a cancel stops the
+                // level graph after the iteration in flight
                 k_syn_record<<<1, 1, 0, ctx->stream>>>(d.syn, d.cc, d.max_bits, d.inv,
-                                                      trace_dev_base, d.trace_cap, nullptr, h_it, 1);
+                                                      trace_dev_base, d.trace_cap,
+                                                      ctx->cancel_mapped_dev, h_it, 1);
                 rc = check_launch(ctx, "k_syn_record");
             }
             cudaGraph_t b2;
@@ -804,7 +807,7 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
     const bool graphs = use_graphs();
     int graph_levels = 0;
     for (int level = 0; level < r->levels && !rc; ++level) {
-        if (ctx->cancel && *ctx->cancel) {
+        if (cancel_requested(ctx)) {
             rc = fail(FW_ERR_CANCELLED, "registration cancelled");
             break;
         }

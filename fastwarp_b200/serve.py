@@ -214,6 +214,11 @@ class Server:
                 lib().fw_field_free(C.c_void_p(result[k]))
                 result[k] = None
 
+    def cancel(self, ticket: int) -> None:
+        """fw_server_cancel: a queued request ends without running, a running one after the
+        iteration in flight; its result then fails with FW_ERR_CANCELLED."""
+        check(lib().fw_server_cancel(self.handle, C.c_uint64(ticket)))
+
     def mark(self):
         check(lib().fw_server_mark(self.handle))
 

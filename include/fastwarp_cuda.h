@@ -294,7 +294,10 @@ int fw_mi_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* f
  * Its scratch is a static device array compiled into the library (block partials for at most
  * FW_NOALLOC_MAX_BLOCKS thread blocks, about 196 KB, held on every GPU that loads the library
  * until the process exits); a grid that needs more blocks is rejected with FW_ERR_INVALID. The
- * first call on a device looks the array's address up, so make it before any stream capture.
+ * first call on a device looks the array's address up, so make it before any stream capture;
+ * the address is kept for the life of the process, so do not use this call on a device after
+ * cudaDeviceReset (or after the device's primary context was destroyed and the library's module
+ * reloaded): the kept address would then name freed memory.
  * All calls share the array: calls whose kernels overlap on the GPU race and must be ordered
  * on one stream (or otherwise serialised) by the caller. */
 #define FW_NOALLOC_MAX_BLOCKS 8192
@@ -381,6 +384,16 @@ int fw_mi_level_prepare_image(fw_ctx* ctx, const fw_image* moving, const double*
                               const uint32_t* fixed_bin, int64_t n,
                               const fw_mi_binning* binning, fw_mi_level** out);
 /* LinearMetric::value (optimizer.rs:61): -MI. */
+/* The level a linear stage prepares (linear.rs:474-492, 251-280, 940-945; sampling.rs:196-238)
+ * from device images already at the level's smoothing: the regular sample set of `level_grid`
+ * from `seed` (only the points inside `fixed_mask`, which may be NULL), the binning (fixed range at
+ * the samples' nearest voxels, moving range over the whole moving image) and the kept points with
+ * their trilinear fixed bins, then as fw_mi_level_prepare_image. Fails with the reference's
+ * reason when Mattes MI is undefined on the samples. */
+int fw_mi_level_prepare_regular(fw_ctx* ctx, const fw_grid* level_grid, const fw_image* fixed,
+                                const fw_image* moving, const fw_image* fixed_mask,
+                                float percentage, uint32_t seed, int32_t bins,
+                                fw_mi_level** out);
 int fw_mi_level_value(fw_mi_level* level, const fw_linear_transform* t, double* value);
 /* LinearMetric::value_and_derivative (optimizer.rs:62-64): -MI and +dMI/dtheta (6 or 12). */
 int fw_mi_level_value_and_derivative(fw_mi_level* level, const fw_linear_transform* t,
@@ -390,6 +403,14 @@ int fw_mi_level_values(fw_mi_level* level, const fw_linear_transform* ts, int32_
                        double* values);
 /* Samples that contributed to the last evaluation. */
 int fw_mi_level_num_valid(const fw_mi_level* level, int64_t* out);
+/* Profiling (crates/fastwarp-gpu/src/profiler.rs:8-60, per-op device timestamps): after one
+ * evaluation at `t`, times `reps` back-to-back launches of each pass of the level with CUDA events
+ * on the context's stream and writes the mean milliseconds per launch and the algorithmic bytes
+ * per launch of [0] the joint histogram (clear + k_mi_hist), [1] ComputeResults (k_mi_finish),
+ * [2] the gradient moments (k_mi_deriv). A pass's bytes are the 16-byte sample records and the
+ * moving image's gathers, min(4 Nm, 32 S) for S samples on Nm moving voxels. */
+int fw_mi_level_time(fw_mi_level* level, const fw_linear_transform* t, int32_t reps,
+                     double ms[3], double bytes[3]);
 void fw_mi_level_free(fw_mi_level* level);
 
 /* ---- SyN stage (syn.rs:776-986) --------------------------------------------------------- */
@@ -509,8 +530,8 @@ int fw_mi_level_optimize(fw_mi_level* level, const fw_cg_settings* settings,
 
 /* ---- one linear stage (linear.rs:512-597, 873-1068) -------------------------------------- */
 
-/* LinearRecipe (linear.rs:75-128) without a fixed mask; the transform kind is the start
- * transform's (Euler3D: rigid, affine: affine). */
+/* LinearRecipe (linear.rs:75-128); its fixed mask is an argument of the _masked entry points.
+ * The transform kind is the start transform's (Euler3D: rigid, affine: affine). */
 typedef struct fw_linear_recipe {
     int32_t levels;
     uint32_t iterations[FW_MAX_LEVELS];
@@ -546,6 +567,16 @@ typedef struct fw_linear_level_trace {
 int fw_linear_stage_run(fw_ctx* ctx, const fw_linear_recipe* recipe, const fw_image* fixed,
                         const fw_image* moving, fw_linear_transform* transform,
                         fw_linear_level_trace* traces);
+/* The same with a fixed-image mask (LinearRecipe::mask, linear.rs:98-100, 130-134: `--masks
+ * [fixed,NULL]`): `fixed_mask` is an image on its own grid whose non-zero voxels are inside
+ * (MaskVolume::is_inside, mask.rs:76-78: the nearest voxel, rounding half up, inside the buffer
+ * and not zero); only the jittered sample points inside it are kept (linear.rs:940-945,
+ * sampling.rs:225-228), and a level left without a point is skipped with the reference's "no
+ * sample point lands on the fixed image inside the fixed mask" reason (linear.rs:474-482). A mask
+ * with no voxel inside is refused. NULL runs the unmasked stage. */
+int fw_linear_stage_run_masked(fw_ctx* ctx, const fw_linear_recipe* recipe, const fw_image* fixed,
+                               const fw_image* moving, const fw_image* fixed_mask,
+                               fw_linear_transform* transform, fw_linear_level_trace* traces);
 
 /* LinearChainResult (linear.rs:1078-1101): the centre-of-mass initial transform, both stages
  * (each optimised transform with its outer part, and its level traces) and the collapsed
@@ -562,11 +593,21 @@ typedef struct fw_linear_chain_result {
 
 /* run_linear_chain (linear.rs:1105-1212): the initial transform from the centres of mass of the
  * raw (resampled, un-preprocessed) images, then the rigid stage and the affine stage on the
- * preprocessed images (`rigid` and `affine` recipes, fw_linear_stage_run each). */
+ * preprocessed images (`rigid` and `affine` recipes, fw_linear_stage_run each). The centres of
+ * mass are summed in float64 over the images' float32 device values (init.rs:50-74 sums the f64
+ * volume): a caller holding float64 raw data that float32 cannot represent exactly gets the
+ * centre of its float32 rounding. */
 int fw_linear_chain_run(fw_ctx* ctx, const fw_linear_recipe* rigid, const fw_linear_recipe* affine,
                         const fw_image* fixed_raw, const fw_image* moving_raw,
                         const fw_image* fixed, const fw_image* moving,
                         fw_linear_chain_result* out);
+/* The chain with a fixed-image mask restricting both stages' samples (as
+ * fw_linear_stage_run_masked). */
+int fw_linear_chain_run_masked(fw_ctx* ctx, const fw_linear_recipe* rigid,
+                               const fw_linear_recipe* affine, const fw_image* fixed_raw,
+                               const fw_image* moving_raw, const fw_image* fixed,
+                               const fw_image* moving, const fw_image* fixed_mask,
+                               fw_linear_chain_result* out);
 
 /* ---- profiling (crates/fastwarp-gpu/src/profiler.rs:8-60: per-op device timestamps) ----- */
 
@@ -579,8 +620,17 @@ int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, 
                     double variance, int32_t reps, double ms[7], double bytes[7]);
 
 /* Sets a flag polled before every level and iteration (SynOptions::cancel, syn.rs:80-85);
- * a run that sees it set fails with FW_ERR_CANCELLED. Pass NULL to clear. */
+ * a run that sees it set fails with FW_ERR_CANCELLED. The flag is caller memory the device
+ * cannot read, so inside a SyN level graph it is seen only at the next level; pass NULL to
+ * clear. */
 int fw_ctx_set_cancel_flag(fw_ctx* ctx, const volatile int32_t* flag);
+
+/* Sets (on != 0) or clears the context's own cancel flag, which lives in mapped pinned host
+ * memory: the host polls it before every level and linear-optimiser iteration, and the SyN level
+ * graph's record kernel reads it once per iteration, so a run stops after the iteration in
+ * flight and fails with FW_ERR_CANCELLED (SynOptions::cancel, syn.rs:80-85). It stays set until
+ * cleared: a later run on the context fails at once. Safe to call from any thread. */
+int fw_ctx_request_cancel(fw_ctx* ctx, int32_t on);
 
 #ifdef __cplusplus
 }

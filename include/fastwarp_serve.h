@@ -22,7 +22,9 @@ typedef struct fw_server fw_server;
 
 /* One SyN-stage request (run_syn, syn.rs:555-564). Images are either host float32 volumes
  * (copied at submit, so the caller may free them at once) or device images made on any context
- * of the same device (used in place; they must stay alive until the request completes). */
+ * of the same device (used in place; they must stay alive until the request completes, and
+ * their contents must be complete when submitted: the slot reads them on its own stream without
+ * waiting for the caller's, so a caller that filled them asynchronously synchronises first). */
 typedef struct fw_syn_request {
     fw_syn_recipe recipe;
     fw_grid fixed_grid;
@@ -66,8 +68,8 @@ typedef struct fw_syn_result {
 
 /* One linear-stage request (run_linear_stage, linear.rs:512-597; the reference's affine-only
  * registrations): host float32 images (copied at submit) or device images made on any context of
- * the same device (kept alive until the result is taken). `start` is the start transform, with
- * the earlier transforms as its outer part. */
+ * the same device (kept alive until the result is taken, and complete when submitted, as for a
+ * SyN request). `start` is the start transform, with the earlier transforms as its outer part. */
 typedef struct fw_linear_request {
     fw_linear_recipe recipe;
     fw_grid fixed_grid;
@@ -121,6 +123,12 @@ int fw_server_estimate(const fw_syn_request* req, uint64_t* bytes);
 int fw_server_submit_linear(fw_server* s, const fw_linear_request* req, uint64_t* ticket);
 int fw_server_wait_linear(fw_server* s, uint64_t ticket, double timeout_s, fw_linear_result* out);
 int fw_server_estimate_linear(const fw_linear_request* req, uint64_t* bytes);
+/* Cancels a request of either kind (SynOptions::cancel, syn.rs:80-85): a queued one ends at once
+ * without running; a running one stops after the SyN iteration (or linear-optimiser iteration)
+ * in flight, through its slot context's cancel flag, which the level graph reads once per
+ * iteration. Either way its result carries FW_ERR_CANCELLED; the other requests run on untouched.
+ * A request that has finished keeps its result. The ticket is still waited for as usual. */
+int fw_server_cancel(fw_server* s, uint64_t ticket);
 /* Waits for every queued and running request, then stops the slots. */
 void fw_server_destroy(fw_server* s);
 

@@ -329,6 +329,24 @@ def sample_points_regular(grid, percentage, seed):
     return out
 
 
+def mask_inside(mask_grid, mask, points):
+    """MaskVolume::is_inside (mask.rs:76-110) for every point (rows of `points`, LPS mm): the
+    nearest voxel of the mask on its own grid, rounding half up, inside the buffer and not zero.
+    Test infrastructure, in numpy: the grid map is grid.rs:131-156 (point_to_index)."""
+    pts = np.asarray(points, np.float64).reshape(-1, 3)
+    d = np.array(mask_grid.direction[:]).reshape(3, 3)
+    sp = np.array(mask_grid.spacing[:])
+    org = np.array(mask_grid.origin[:])
+    inv = np.linalg.inv(d * sp[None, :])
+    c = (pts - org) @ inv.T
+    r = np.floor(c + 0.5)
+    size = np.array(mask_grid.size[:])
+    ok = np.all((r >= 0) & (r < size), axis=1)
+    q = np.where(ok[:, None], r, 0).astype(np.int64)
+    m = np.asarray(mask).reshape(size[2], size[1], size[0])
+    return ok & (m[q[:, 2], q[:, 1], q[:, 0]] != 0)
+
+
 def bspline3(u):
     return lib().fwo_bspline3(u)
 

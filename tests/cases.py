@@ -69,3 +69,51 @@ def interior(shape, margin=1):
     m = np.zeros(shape, bool)
     m[margin:shape[0] - margin, margin:shape[1] - margin, margin:shape[2] - margin] = True
     return m
+
+
+def grid_matrices(case):
+    """(origin, index->offset matrix D diag(spacing), its inverse) of a case's grid."""
+    d = np.asarray(case["direction"], float)
+    ds = d * np.asarray(case["spacing"], float)[None, :]
+    return np.asarray(case["origin"], float), ds, np.linalg.inv(ds)
+
+
+def voxel_points(case):
+    """Physical points of every voxel, shape (nz, ny, nx, 3) (grid.rs:131-140)."""
+    org, ds, _ = grid_matrices(case)
+    nx, ny, nz = case["size"]
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    return org + np.stack([x, y, z], -1).astype(np.float64) @ ds.T
+
+
+def continuous_index(case, points):
+    """Continuous indices of physical points on a case's grid (grid.rs:146-156)."""
+    org, _, inv = grid_matrices(case)
+    return (np.asarray(points, float) - org) @ inv.T
+
+
+def edge_distance(case, c):
+    """Distance, in voxels, of continuous indices from the nearest buffer face (-0.5 or n - 0.5
+    on any axis, where ITK's IsInsideBuffer flips)."""
+    n = np.asarray(case["size"], float)
+    return np.minimum(np.abs(c + 0.5), np.abs(c - (n - 0.5))).min(-1)
+
+
+def vector_at(case, f, c):
+    """ITK's vector linear interpolation (neighbours clamped) of an AoS field at continuous
+    indices c (field_ops.rs:143-172); zero outside the buffer."""
+    n = np.asarray(case["size"])
+    inside = np.all((c >= -0.5) & (c < n - 0.5), -1)
+    fl = np.floor(c)
+    t = c - fl
+    b0 = fl.astype(np.int64)
+    out = np.zeros(c.shape[:-1] + (3,))
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                q = [np.clip(b0[..., a] + o, 0, n[a] - 1) for a, o in enumerate((dx, dy, dz))]
+                w = np.ones(c.shape[:-1])
+                for a, o in enumerate((dx, dy, dz)):
+                    w = w * (t[..., a] if o else 1.0 - t[..., a])
+                out += w[..., None] * f[q[2], q[1], q[0]]
+    return np.where(inside[..., None], out, 0.0)

@@ -100,10 +100,10 @@ def test_two_channels_on_their_own_moving_grid_match_the_oracle(backend):
 
 
 def test_the_full_config2_registration_matches_the_oracle(backend):
-    """The benchmark's registration end to end -- 4/2/1 shrink, sigma 2/1/0, 70/50/20 iterations,
-    CC r = 4, step 0.1 -- with every iteration run (threshold -1: the window monitor would stop
-    both engines where their last energies happen to cross it) against the oracle's, which takes
-    a couple of minutes on the host cores: 0.05 mm RMS on both fields, 1e-4 relative final CC."""
+    """The benchmark's exact registration end to end (bench.py's recipe) -- 4/2/1 shrink, sigma
+    2/1/0, 70/50/20 iterations all run (threshold -1), CC r = 4, step 0.1 -- against the oracle's,
+    which takes about a minute and a half on the host cores: 0.05 mm RMS on both fields, 1e-4
+    relative final CC."""
     g, fixed, mg, moving, initial = head_pair()
     r = SynRecipe(gradient_step=0.1, update_field_variance=3.0, total_field_variance=0.0,
                   cc_radius=4, iterations=[70, 50, 20], shrink_factors=[4, 2, 1],
@@ -116,5 +116,31 @@ def test_the_full_config2_registration_matches_the_oracle(backend):
     assert len(res.iterations) == len(orecs) == 140
     rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
     rms_inv = np.sqrt(((res.inverse_warp.astype(np.float64) - oinv) ** 2).sum(-1).mean())
+    assert rms <= 0.05 and rms_inv <= 0.05, (rms, rms_inv)
+    assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)
+
+
+def test_the_converging_config2_registration_stops_where_the_oracle_does(backend):
+    """The cohort's convergence rule at full size (window monitor, 1e-6 over 10 iterations,
+    convergence.rs:47-126): the device monitor stops every level at the iteration the oracle's
+    does, and the fields and the final CC agree as in the full run (0.05 mm RMS, 1e-4)."""
+    g, fixed, mg, moving, initial = head_pair()
+    r = SynRecipe(gradient_step=0.1, update_field_variance=3.0, total_field_variance=0.0,
+                  cc_radius=4, iterations=[70, 50, 20], shrink_factors=[4, 2, 1],
+                  smoothing_sigmas=[2.0, 1.0, 0.0], convergence_threshold=1e-6,
+                  convergence_window=10)
+    res = run_syn(backend, r, g, [fixed], mg, [moving], initial)
+    orec = O.syn_recipe(0.1, 3.0, 0.0, 4, (70, 50, 20), (4, 2, 1), (2.0, 1.0, 0.0), False, 1e-6,
+                        10, (1.0,))
+    ow, oinv, orecs, _ = O.syn_run(orec, ogrid(g), [fixed], ogrid(mg), [moving], oaffine(initial))
+    counts = [sum(1 for it in res.iterations if it["level"] == lv) for lv in range(3)]
+    ocounts = [sum(1 for it in orecs if it.level == lv) for lv in range(3)]
+    rms = np.sqrt(((res.warp.astype(np.float64) - ow) ** 2).sum(-1).mean())
+    rms_inv = np.sqrt(((res.inverse_warp.astype(np.float64) - oinv) ** 2).sum(-1).mean())
+    print(f"iterations per level {counts} (oracle {ocounts}); field RMS {rms:.2e} / "
+          f"{rms_inv:.2e} mm; final CC {res.iterations[-1]['energy']:.8f} "
+          f"(oracle {orecs[-1].energy:.8f})")
+    assert counts == ocounts
+    assert sum(counts) < 140  # the monitor did stop a level early
     assert rms <= 0.05 and rms_inv <= 0.05, (rms, rms_inv)
     assert abs(res.iterations[-1]["energy"] - orecs[-1].energy) <= 1e-4 * abs(orecs[-1].energy)

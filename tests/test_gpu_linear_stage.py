@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from fastwarp_b200 import FastwarpError, linear_transform
+from fastwarp_b200 import FastwarpError, linear_transform, make_grid
 from fastwarp_b200.backend import (grid_corners, linear_recipe, run_linear_chain,
                                    run_linear_stage)
 from fastwarp_b200.phantoms import blob_pair
@@ -27,9 +27,11 @@ def ogrid(g):
 
 
 def oracle_stage(g, fixed, moving, kind, start, center, iterations, shrink, sigmas, step=0.1,
-                 pct=0.25, bins=32, seed=1, outer=(np.eye(3), (0, 0, 0), (0, 0, 0))):
+                 pct=0.25, bins=32, seed=1, outer=(np.eye(3), (0, 0, 0), (0, 0, 0)), mask=None):
     """run_linear_stage restated over the oracle's pieces (sigmas in voxels); `outer` is the
-    earlier transforms as (matrix, translation, centre)."""
+    earlier transforms as (matrix, translation, centre); `mask` (grid, values) keeps only the
+    sample points inside it (linear.rs:940-945). A level left without a sample point reports
+    samples 0 and no values."""
     og = ogrid(g)
     fixed, moving = fixed.astype(np.float64), moving.astype(np.float64)
     t = O.linear_transform(kind, start, center=center, outer_matrix=outer[0],
@@ -44,6 +46,11 @@ def oracle_stage(g, fixed, moving, kind, start, center, iterations, shrink, sigm
         else:
             fs, ms = fixed, moving
         pts = O.sample_points_regular(lg, pct, seed + level)
+        if mask is not None:
+            pts = pts[O.mask_inside(mask[0], mask[1], pts)]
+            if len(pts) == 0:
+                out.append(dict(samples=0, values=[], corners=grid_corners(lg)))
+                continue
         kept, fbin, b = O.prepare_samples(og, fs, og, ms, pts, bins)
 
         def ov(tt):
@@ -141,3 +148,96 @@ def test_the_linear_chain_matches_the_oracle(backend):
     assert shift < 0.05, shift
     assert np.abs(dc - fc).max() < 1e-9  # the total keeps the affine stage's centre
     assert max(abs(v) for v in out["rigid"]) > 1e-4  # the rigid stage moved
+
+
+def half_mask(g):
+    """linear.rs:1546-1576: the voxels of the upper half along x."""
+    nx, ny, nz = g.size
+    m = np.zeros((nz, ny, nx), np.float32)
+    m[:, :, nx // 2:] = 1.0
+    return m
+
+
+@pytest.mark.parametrize("kind", ["euler", "affine"])
+def test_a_masked_linear_stage_matches_the_oracle(backend, kind):
+    """The fixed mask (LinearRecipe::mask): only the jittered sample points whose nearest mask
+    voxel is inside are kept (linear.rs:940-945); the sample set shrinks (linear.rs:1546-1576)
+    and the stage follows the oracle's on the kept points. The mask has its own grid, coarser
+    and shifted against the fixed image's, as ANTs attaches it in physical space."""
+    g, fixed, moving = blob_pair(48, seed=77)
+    mg = make_grid((24, 24, 24), spacing=tuple(2.0 * s for s in g.spacing),
+                   origin=tuple(o + 0.3 for o in g.origin))
+    mask = half_mask(mg)
+    mask[:, :4, :] = 0.0  # and a slab off the bottom rows
+    center = tuple((s - 1) * sp / 2.0 for s, sp in zip(g.size, g.spacing))
+    start = [0.0] * 6 if kind == "euler" else list(np.eye(3).ravel()) + [0.0] * 3
+    its, shrink, sigmas = (12, 8), (2, 1), (1.0, 0.0)
+    r = linear_recipe(iterations=its, shrink_factors=shrink, smoothing_sigmas=sigmas)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    _, base = run_linear_stage(backend, r, fi, mi, linear_transform(kind, start, center=center))
+    t, levels = run_linear_stage(backend, r, fi, mi, linear_transform(kind, start, center=center),
+                                 fixed_mask=backend.upload_image(mg, mask))
+    omg = ogrid(mg)
+    ot, olevels = oracle_stage(g, fixed, moving, kind, start, center, its, shrink, sigmas,
+                               mask=(omg, mask))
+    for lv, bl, ol in zip(levels, base, olevels):
+        assert 0 < lv["samples"] < 0.6 * bl["samples"]
+        assert abs(lv["samples"] - ol["samples"]) <= 0.005 * ol["samples"]
+        best = min(ol["values"])
+        assert abs(lv["best_value"] - best) <= 1e-4 * abs(best), (lv["best_value"], best)
+    shift = corner_shift(t, ot, olevels[-1]["corners"])
+    print(f"masked {kind}: corner shift {shift:.2e} mm, samples {[lv['samples'] for lv in levels]}"
+          f" of {[b['samples'] for b in base]}")
+    assert shift < 0.05, shift
+
+
+def plane_mask_missed_by_coarse_level(g, shrink, seed=1):
+    """After linear.rs:1578-1596: a one-voxel plane x = const of the fixed grid that none of the
+    coarse level's jittered sample points (the stage's first seed) rounds to."""
+    og = ogrid(g)
+    pts = O.sample_points_regular(O.shrink_grid(og, O.shrink_factors(shrink, tuple(g.spacing))),
+                                  0.25, seed)
+    hit = {int(np.floor(O.point_to_index(og, p)[0] + 0.5)) for p in pts}
+    plane = next(x for x in range(2, g.size[0] - 2) if x not in hit)
+    m = np.zeros(tuple(g.size)[::-1], np.float32)
+    m[:, :, plane] = 1.0
+    return m
+
+
+def test_a_level_without_masked_samples_is_skipped_and_a_stage_of_only_such_levels_fails(backend):
+    """linear.rs:1598-1640: the coarse level keeps no sample point inside a thin plane mask and is
+    skipped (samples 0, no iteration, the start unchanged); the fine level runs. A stage whose
+    only level is skipped fails with the reference's reason."""
+    g, fixed, moving = blob_pair(30, seed=5)
+    mask = plane_mask_missed_by_coarse_level(g, 6)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    m = backend.upload_image(g, mask)
+    start = linear_transform("euler", [0.0] * 6, center=(14.5, 14.5, 14.5))
+    r = linear_recipe(iterations=(5, 5), shrink_factors=(6, 1), smoothing_sigmas=(0.0, 0.0))
+    t, levels = run_linear_stage(backend, r, fi, mi, start, fixed_mask=m)
+    opts = O.sample_points_regular(O.shrink_grid(ogrid(g), O.shrink_factors(6, (1.0,) * 3)),
+                                   0.25, 1)
+    assert not O.mask_inside(ogrid(g), mask, opts).any()
+    assert levels[0]["skipped"] and levels[0]["samples"] == 0 and levels[0]["iterations"] == 0
+    assert levels[0]["parameters"] == [0.0] * 6
+    assert not levels[1]["skipped"] and levels[1]["samples"] > 0
+    coarse = linear_recipe(iterations=(5,), shrink_factors=(6,), smoothing_sigmas=(0.0,))
+    with pytest.raises(FastwarpError, match="no sample point lands on the fixed image inside the "
+                                            "fixed mask"):
+        run_linear_stage(backend, coarse, fi, mi, start, fixed_mask=m)
+    with pytest.raises(FastwarpError, match="fixed mask has no voxel inside"):
+        run_linear_stage(backend, coarse, fi, mi, start,
+                         fixed_mask=backend.upload_image(g, np.zeros_like(mask)))
+
+
+def test_the_masked_linear_chain_keeps_its_samples_inside_the_mask(backend):
+    """The chain passes the fixed mask to both stages."""
+    g, fixed, moving = blob_pair(40, seed=29)
+    r = linear_recipe(iterations=(6, 4), shrink_factors=(2, 1), smoothing_sigmas=(1.0, 0.0))
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    m = backend.upload_image(g, half_mask(g))
+    full = run_linear_chain(backend, r, r, fi, mi, fi, mi)
+    masked = run_linear_chain(backend, r, r, fi, mi, fi, mi, fixed_mask=m)
+    for key in ("rigid_samples", "affine_samples"):
+        for a, b in zip(masked[key], full[key]):
+            assert 0 < a < 0.6 * b

@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 import oracle as O
-from cases import CASES, field, grid_of, image
+from cases import (CASES, continuous_index, edge_distance, field, grid_of, image,
+                   vector_at, voxel_points)
 from fastwarp_b200 import _native as N
 from fastwarp_b200.backend import make_affine, make_grid
 
@@ -31,6 +32,16 @@ def worst(a, b):
     return float(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64)).max())
 
 
+def assert_only_edge_flips(diff, edge, tol):
+    """Every voxel off by more than `tol` samples within one voxel of a buffer face (where the
+    f32 field and the two engines' index arithmetic can put a point on either side of ITK's
+    inside test); they are rare; every other voxel meets `tol`."""
+    bad = diff > tol
+    assert np.mean(bad) < 2e-3, np.mean(bad)
+    assert edge[bad].max(initial=0.0) < 1.0, edge[bad].max()
+    assert diff[edge >= 1.0].max(initial=0.0) <= tol, diff[edge >= 1.0].max()
+
+
 @pytest.mark.parametrize("name", NAMES)
 def test_warp_through_field_matches(backend, name):
     case = CASES[name]
@@ -47,9 +58,9 @@ def test_warp_through_field_matches(backend, name):
     out = backend.warp_through_field(src, f, affine=make_affine(A, off)).download()
     want = O.warp(og, img, og, fld, affine=O.make_affine(A, off))
     diff = np.abs(out - want)
-    # validity flips at the buffer edge aside (points within float32 rounding of -0.5 / n-0.5)
-    assert np.mean(diff > 1e-5) < 1e-3
-    assert np.median(diff) < 1e-6
+    # the sampled source index of every voxel: c = S^-1 (A (x + u) + off - origin)
+    c = continuous_index(case, (voxel_points(case) + fld) @ A.T + off)
+    assert_only_edge_flips(diff, edge_distance(case, c), 1e-5 * max(1.0, np.abs(want).max()))
 
 
 @pytest.mark.parametrize("name", ["selftest", "awkward_oblique"])
@@ -67,7 +78,13 @@ def test_warp_with_an_earlier_field_and_masks_matches(backend, name):
     aff = (np.eye(3) * 1.01, np.array([0.2, -0.1, 0.05]))
     out = backend.warp_through_field(src, f, pre=p, affine=make_affine(*aff)).download()
     want = O.warp(og, img, og, fld, opg, pre, O.make_affine(*aff))
-    assert np.mean(np.abs(out - want) > 1e-5) < 2e-3
+    # two places where a sample can flip: the earlier field's buffer at q = x + u(x), and the
+    # source's at c = S^-1 (A (q + pre(q)) + off - origin)
+    q = voxel_points(case) + fld
+    cq = continuous_index(pre_case, q)
+    c = continuous_index(case, (q + vector_at(pre_case, pre, cq)) @ aff[0].T + aff[1])
+    near = np.minimum(edge_distance(pre_case, cq), edge_distance(case, c))
+    assert_only_edge_flips(np.abs(out - want), near, 1e-5 * max(1.0, np.abs(want).max()))
     mask_img = (img > np.median(img)).astype(np.float64)
     m = backend.upload_image(g, mask_img.astype(np.float32))
     got = backend.warp_mask_through_field(m, f, pre=p, affine=make_affine(*aff)).download()
@@ -250,9 +267,10 @@ def test_compose_matches(backend, name):
     u, w = field(case), field(case, amp=2.5, seed_offset=9)
     out = backend.compose(backend.upload_field(g, u), backend.upload_field(g, w))
     want = O.compose(og, u, w)
-    diff = np.abs(backend.download_field(out) - want)
-    assert np.mean(diff > 1e-5) < 2e-3  # buffer-edge validity flips aside
-    assert np.median(diff) < 1e-6
+    diff = np.abs(backend.download_field(out) - want).max(-1)
+    # the gathered index of every voxel: x + w(x) on the same grid
+    c = continuous_index(case, voxel_points(case) + w)
+    assert_only_edge_flips(diff, edge_distance(case, c), 1e-5 * max(1.0, np.abs(want).max()))
 
 
 @pytest.mark.parametrize("name", NAMES)

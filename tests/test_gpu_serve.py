@@ -1,9 +1,12 @@
 """The continuous-batching server: each result is the same alone and in a mix, admission follows
 the HBM budget, and requests that cannot fit are refused before any work."""
+import time
+
 import numpy as np
 import pytest
 
 from fastwarp_b200 import CudaBackend, FastwarpError, SynRecipe
+from fastwarp_b200._native import FW_ERR_CANCELLED
 from fastwarp_b200.phantoms import blob_pair
 from fastwarp_b200.serve import Server
 
@@ -121,3 +124,79 @@ def test_a_mixed_stream_of_masked_mattes_and_two_channel_requests(pairs, backend
         assert r["status"] == 0, r["error"]
         assert np.array_equal(r["warp"], d.warp)
         assert np.array_equal(r["inverse_warp"], d.inverse_warp)
+
+
+def long_recipe(iterations=20000):
+    """One level of many iterations at 96^3 (several seconds), to be cancelled while it runs."""
+    return SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2,
+                     iterations=[iterations], shrink_factors=[1], smoothing_sigmas=[0.0],
+                     convergence_threshold=-1.0)
+
+
+def test_a_cancel_stops_a_running_request_inside_its_level_graph(pairs):
+    """A host-injected cancel (SynOptions::cancel, syn.rs:80-85) of a running request in a
+    3-slot server: the record kernel of its level graph reads the slot's flag once per iteration,
+    so the request ends FW_ERR_CANCELLED long before its 20000 iterations; the two requests
+    running beside it are bit-identical to the same requests served alone, and the slot serves
+    the next request normally (the flag is cleared with the cancelled request)."""
+    r = small_recipe()
+    (g1, f1, m1), (g2, f2, m2), _ = pairs
+    g, f, m = blob_pair(96, seed=7)
+    with Server(0, slots=1) as s:
+        alone = [s.wait(s.submit(r, g1, [f1], g1, [m1])), s.wait(s.submit(r, g2, [f2], g2, [m2]))]
+    with Server(0, slots=3) as s:
+        tl = s.submit(long_recipe(), g, [f], g, [m])
+        t1 = s.submit(r, g1, [f1], g1, [m1])
+        t2 = s.submit(r, g2, [f2], g2, [m2])
+        time.sleep(0.4)
+        t0 = time.perf_counter()
+        s.cancel(tl)
+        cancelled = s.wait(tl)
+        waited = time.perf_counter() - t0
+        others = [s.wait(t1), s.wait(t2)]
+        after = s.wait(s.submit(r, g1, [f1], g1, [m1]))
+        st = s.stats()
+    assert cancelled["status"] == FW_ERR_CANCELLED and "cancelled" in cancelled["error"]
+    # 20000 iterations would take seconds; the cancel lands within an iteration or two
+    assert waited < 0.5, waited
+    assert cancelled["run_s"] < 2.0, cancelled["run_s"]
+    for got, want in zip(others + [after], alone + [alone[0]]):
+        assert got["status"] == 0, got["error"]
+        assert np.array_equal(got["warp"], want["warp"])
+        assert np.array_equal(got["inverse_warp"], want["inverse_warp"])
+        assert got["final_energy"] == want["final_energy"]
+    assert st["failed"] == 1 and st["completed"] == 3
+
+
+def test_a_cancelled_queued_request_never_runs(pairs):
+    r = small_recipe()
+    g1, f1, m1 = pairs[0]
+    g, f, m = blob_pair(96, seed=7)
+    with Server(0, slots=1) as s:
+        tl = s.submit(long_recipe(), g, [f], g, [m])
+        tq = s.submit(r, g1, [f1], g1, [m1])
+        s.cancel(tq)
+        q = s.wait(tq, timeout=5.0)
+        s.cancel(tl)
+        lres = s.wait(tl)
+        nxt = s.wait(s.submit(r, g1, [f1], g1, [m1]))
+        with pytest.raises(FastwarpError, match="unknown or already taken"):
+            s.cancel(tq)
+    assert q["status"] == FW_ERR_CANCELLED and q["run_s"] == 0.0
+    assert lres["status"] == FW_ERR_CANCELLED
+    assert nxt["status"] == 0 and nxt["iterations"] == 10
+
+
+def test_the_context_cancel_flag_fails_a_run_until_cleared(pairs, backend):
+    from fastwarp_b200 import run_syn
+    g, f, m = pairs[2]
+    r = small_recipe()
+    backend.request_cancel(True)
+    try:
+        with pytest.raises(FastwarpError, match="cancelled") as e:
+            run_syn(backend, r, g, [f], g, [m])
+        assert e.value.code == FW_ERR_CANCELLED
+    finally:
+        backend.request_cancel(False)
+    res = run_syn(backend, r, g, [f], g, [m])
+    assert len(res.iterations) == 10
