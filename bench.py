@@ -71,6 +71,7 @@ def parse():
                    help="time the kernels of one finest-level iteration only (profiling target)")
     p.add_argument("--reps", type=int, default=20)
     p.add_argument("--no-mi", action="store_true", help="skip the sampled Mattes MI leg")
+    p.add_argument("--no-batch", action="store_true", help="skip the batching-form leg")
     p.add_argument("--full-cpu", action="store_true",
                    help="with --impl reference: time one whole oracle registration")
     return p.parse_args()
@@ -381,6 +382,9 @@ def run_ours(args, rank, world, local):
                       "h2d_bytes_per_step": int((fixed.nbytes + moving.nbytes) * conc),
                       "d2h_bytes_per_step": int(2 * 12 * shape3 * conc),
                       "timing": "wall clock, first submit to last result (host copies included)"}
+    if not args.no_batch:
+        log("batching form (config 4)")
+        out["batched"] = batch_leg(b, rank)
     if not args.no_mi:
         log("sampled Mattes MI leg and linear chain")
         out["mattes_mi"] = mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world)
@@ -577,6 +581,98 @@ def mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world):
                            "recipe": "CoM + rigid + affine, MI 32 bins 25 % regular, shrink "
                                      "4/2/1, sigma 2/1/0 vox, 500/250/100 iterations, 1e-6/10"}
     return out
+
+
+def batch_leg(b, rank, n_subjects=48):
+    """Config 4: `n_subjects` two-channel subjects (T1-like and inverted-contrast T2-like), grid
+    dims drawn per axis from 160-240 at 1 mm, each with its own random affine and smooth
+    displacement, registered to the 193 x 229 x 193 template: SyN CC r4, shrink 4/2/1, sigma
+    2/1/0, 70/50/20 iterations all run, equal channel weights. Batched (fw_batch_syn_run: one
+    persistent launch per sub-step over all subjects, each level one graph, autotuned tiles)
+    against the same subjects one at a time through the single-registration path and served
+    through 4 slots; two subjects' batched fields are compared with their runs alone."""
+    import numpy as np
+
+    from fastwarp_b200 import SynRecipe, run_syn_batch, run_syn_device
+    from fastwarp_b200.phantoms import BASE_SEED, batch_subjects
+    from fastwarp_b200.serve import Server
+    g, fixed, subjects = batch_subjects(b, n_subjects, seed=BASE_SEED + 4 + rank)
+    r = SynRecipe(gradient_step=0.1, update_field_variance=3.0, total_field_variance=0.0,
+                  cc_radius=4, iterations=list(ITERATIONS), shrink_factors=list(SHRINK),
+                  smoothing_sigmas=list(SIGMAS), convergence_threshold=-1.0,
+                  convergence_window=10, channel_weights=[0.5, 0.5])
+
+    def release(res):
+        for x in res.subjects:
+            if x is not None:
+                x.warp.free()
+                x.inverse_warp.free()
+
+    t0 = time.perf_counter()
+    first = run_syn_batch(b, r, fixed, subjects, download=False)  # tunes each level's shapes
+    t_first = time.perf_counter() - t0
+    release(first)
+    t0 = time.perf_counter()
+    res = run_syn_batch(b, r, fixed, subjects, download=False)
+    t_batch = time.perf_counter() - t0
+    dev_batch = sum(res.level_ms) / 1000.0
+    ok = sum(1 for st in res.statuses if st == 0)
+    # two subjects against their runs alone (0.05 mm RMS, 1e-4 final CC is the bar)
+    checks = []
+    for k in (0, n_subjects - 1):
+        moving, initial = subjects[k]
+        w, iw, recs = run_syn_device(b, r, fixed, moving, initial)
+        got = res.subjects[k]
+        a, a0 = b.download_field(got.warp), b.download_field(w)
+        ia, ia0 = b.download_field(got.inverse_warp), b.download_field(iw)
+        checks.append({"subject": k,
+                       "rms_mm": float(np.sqrt(((a - a0) ** 2).sum(-1).mean())),
+                       "rms_inverse_mm": float(np.sqrt(((ia - ia0) ** 2).sum(-1).mean())),
+                       "max_abs_mm": float(max(np.abs(a - a0).max(), np.abs(ia - ia0).max())),
+                       "final_cc": got.iterations[-1]["energy"],
+                       "final_cc_alone": recs[-1]["energy"]})
+        w.free()
+        iw.free()
+    release(res)
+    # the same subjects one at a time (single-registration graphs), on a sample of 8
+    ns = min(8, n_subjects)
+    b.synchronize()
+    t0 = time.perf_counter()
+    for moving, initial in subjects[:ns]:
+        w, iw, _ = run_syn_device(b, r, fixed, moving, initial)
+        w.free()
+        iw.free()
+    b.synchronize()
+    t_seq = (time.perf_counter() - t0) / ns
+    # and served through 4 slots (continuous batching of independent registrations)
+    with Server(b.device, slots=4) as srv:
+        def served():
+            ts = [srv.submit(r, g, fixed, moving[0].grid, moving, initial, keep_on_device=True)
+                  for moving, initial in subjects]
+            for t in ts:
+                o = srv.wait(t)
+                Server.free_device_fields(o)
+        served()
+        t0 = time.perf_counter()
+        served()
+        t_srv = time.perf_counter() - t0
+    sizes = [tuple(m[0].grid.size) for m, _ in subjects]
+    return {"workload": f"{n_subjects} two-channel subjects, dims U(160-240) per axis, to the "
+                        "193x229x193 template; CC r4 shrink 4/2/1 sigma 2/1/0 70/50/20 (all run)",
+            "value": round(n_subjects / t_batch * 3600.0, 1), "unit": "registrations/hour",
+            "seconds": round(t_batch, 3), "device_seconds": round(dev_batch, 3),
+            "first_run_seconds_with_tuning": round(t_first, 3),
+            "subjects_ok": ok,
+            "sequential_value": round(3600.0 / t_seq, 1),
+            "sequential_seconds_per_subject": round(t_seq, 4),
+            "served_4_slots_value": round(n_subjects / t_srv * 3600.0, 1),
+            "batched_over_sequential": round(t_seq * n_subjects / t_batch, 3),
+            "batched_over_served": round(t_srv / t_batch, 3),
+            "level_ms": [round(x, 2) for x in res.level_ms],
+            "tuning": res.tuning, "device_bytes": res.device_bytes,
+            "moving_dims_min": [min(x[a] for x in sizes) for a in range(3)],
+            "moving_dims_max": [max(x[a] for x in sizes) for a in range(3)],
+            "vs_alone": checks}
 
 
 def mi_cpu_baseline(g, fixed, mg, moving, initial):

@@ -127,6 +127,28 @@ class SynIteration(C.Structure):
                 ("moving_update_scale", C.c_double), ("inversions", InvertStats * 4)]
 
 
+class BatchSubject(C.Structure):
+    """fw_batch_subject (include/fastwarp_cuda.h)."""
+    _fields_ = [("moving", C.c_void_p * MAX_CHANNELS), ("initial", Affine),
+                ("has_initial", C.c_int32)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("level", C.c_int32), ("grid_size", C.c_int64 * 3),
+                ("warp_zchunk", C.c_int32), ("warp_blocks_per_sm", C.c_int32),
+                ("compose_zchunk", C.c_int32), ("compose_blocks_per_sm", C.c_int32),
+                ("cc_zchunk", C.c_int32), ("cc_blocks_per_sm", C.c_int32),
+                ("measure_zchunk", C.c_int32), ("measure_blocks_per_sm", C.c_int32),
+                ("body_blocks_per_sm", C.c_int32), ("smooth_blocks_per_sm", C.c_int32),
+                ("from_cache", C.c_int32), ("tune_ms", C.c_double)]
+
+
+class BatchReport(C.Structure):
+    _fields_ = [("subjects", C.c_int32), ("levels", C.c_int32),
+                ("tuning", BatchTuning * MAX_LEVELS), ("level_ms", C.c_double * MAX_LEVELS),
+                ("device_bytes", C.c_uint64)]
+
+
 class Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_uint64), ("graph_launches", C.c_uint64),
                 ("host_syncs", C.c_uint64), ("bytes_uploaded", C.c_uint64),

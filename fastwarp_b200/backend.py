@@ -447,9 +447,11 @@ def binning_from_ranges(bins, fixed_range, moving_range) -> N.MiBinning:
 class MiLevel:
     """LinearMetric of one prepared level (GpuMiLevel's role): -MI and its gradient."""
 
-    def __init__(self, backend: CudaBackend, handle):
+    def __init__(self, backend: CudaBackend, handle, keep=()):
         self.backend = backend
         self.handle = handle
+        # device images the level reads in place (they must outlive it)
+        self._keep = tuple(keep)
         backend._live.add(self)
 
     def value(self, t: N.LinearTransform) -> float:
@@ -525,7 +527,7 @@ class CudaLinearEngine:
             self.backend.ctx, C.byref(level_grid), fixed.handle, moving.handle,
             fixed_mask.handle if fixed_mask is not None else None, C.c_float(percentage),
             C.c_uint32(seed), C.c_int32(bins), C.byref(h)))
-        return MiLevel(self.backend, h)
+        return MiLevel(self.backend, h, keep=(moving,))
 
 
 # ---- the linear-stage optimiser (optimizer.rs:60-435) --------------------------------------------

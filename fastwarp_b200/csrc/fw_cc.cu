@@ -79,28 +79,25 @@ struct Layout {
 #define FW_CC_MIN_BLOCKS 3
 #endif
 
+// One tile (bx, by, bz) of the CC pair: writes the tile's derivative voxels and leaves the
+// thread's sums [cc, |dF|^2, |dM|^2, valid voxels] in acc_out.
 template <int R, int TY, bool MK>
-__global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a, const float* __restrict__ fimg,
-                                                     const float* __restrict__ mimg,
-                                                     const float* __restrict__ vimg,
-                                                     float* __restrict__ d_fixed,
-                                                     float* __restrict__ d_moving,
-                                                     double* __restrict__ partials,
-                                                     unsigned int* __restrict__ counter,
-                                                     double* __restrict__ result, int want_norms) {
+__device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
+                                        unsigned char* smem, const float* __restrict__ fimg,
+                                        const float* __restrict__ mimg,
+                                        const float* __restrict__ vimg,
+                                        float* __restrict__ d_fixed, float* __restrict__ d_moving,
+                                        int want_norms, double acc_out[4]) {
     using L = Layout<R, TY, MK>;
-    extern __shared__ __align__(16) unsigned char smem[];
     double* xs = reinterpret_cast<double*>(smem + L::zs1);
     int* xc = reinterpret_cast<int*>(smem + L::zs1 + L::xs_bytes);
     float2* raw = reinterpret_cast<float2*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes);
-    double* red = reinterpret_cast<double*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes +
-                                            L::raw_bytes);
 
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int z0 = blockIdx.z * a.zchunk;
+    const int x0 = bx * TX, y0 = by * TY;
+    const int z0 = bz * a.zchunk;
     const int z1 = min(z0 + a.zchunk, nz);
     const int x = x0 + tx, y = y0 + ty;
     const bool own = x < nx && y < ny;
@@ -323,31 +320,47 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
         }
     }
 
-    // block partials, then the fixed-order last-block reduction
-    constexpr int NP = L::NP;
-    double acc[4] = {acc_cc, acc_nf, acc_nm, acc_nv};
+    acc_out[0] = acc_cc;
+    acc_out[1] = acc_nf;
+    acc_out[2] = acc_nm;
+    acc_out[3] = acc_nv;
+}
+
+// The block's sums of acc (NP of them) into dst[0 .. NP) (warp sums, then warps in order).
+template <int NP, int NT>
+__device__ __forceinline__ void cc_block_partials(double acc[4], double* red, double* dst) {
+    const int tid = threadIdx.x;
 #pragma unroll
     for (int q = 0; q < NP; ++q) acc[q] = warp_sum_d(acc[q]);
     __syncthreads();
-    const int warps = L::NT / 32;
     if ((tid & 31) == 0) {
 #pragma unroll
         for (int q = 0; q < NP; ++q) red[(tid >> 5) * NP + q] = acc[q];
     }
     __syncthreads();
-    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     if (tid < NP) {
         double s = 0.0;
-        for (int w = 0; w < warps; ++w) s += red[w * NP + tid];
-        partials[(size_t)bid * NP + tid] = s;
+        for (int w = 0; w < NT / 32; ++w) s += red[w * NP + tid];
+        dst[tid] = s;
     }
+}
+
+// Whether this block is the last of `total` to add its partials (fixed-order reduction).
+__device__ __forceinline__ bool cc_last(unsigned int* counter, unsigned int total) {
+    __shared__ bool last;
     __threadfence();
     __syncthreads();
-    __shared__ bool last;
-    if (tid == 0) last = atomicAdd(counter, 1u) == nblocks - 1;
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == total - 1;
     __syncthreads();
-    if (!last) return;
+    return last;
+}
+
+// The last block's reduction of `nblocks` partials, in block order (lane-strided, then a warp
+// sum): [value, |dF|^2, |dM|^2 (, valid voxels)] into result; the counter is reset.
+template <int NP, bool MK>
+__device__ __forceinline__ void cc_finish(const double* partials, unsigned int nblocks,
+                                          long long n, double* result, unsigned int* counter) {
+    const int tid = threadIdx.x;
     if (tid < 32) {
         double tot[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
@@ -358,12 +371,71 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
         }
         if (tid == 0) {
             // the mean over the valid voxels (all voxels without a mask); no valid voxel: NaN
-            result[0] = -tot[0] / (MK ? tot[3] : (double)a.g.n);
+            result[0] = -tot[0] / (MK ? tot[3] : (double)n);
             result[1] = tot[1];
             result[2] = tot[2];
             if constexpr (MK) result[3] = tot[3];
             *counter = 0;
         }
+    }
+}
+
+template <int R, int TY, bool MK>
+__global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a, const float* __restrict__ fimg,
+                                                     const float* __restrict__ mimg,
+                                                     const float* __restrict__ vimg,
+                                                     float* __restrict__ d_fixed,
+                                                     float* __restrict__ d_moving,
+                                                     double* __restrict__ partials,
+                                                     unsigned int* __restrict__ counter,
+                                                     double* __restrict__ result, int want_norms) {
+    using L = Layout<R, TY, MK>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* red = reinterpret_cast<double*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes +
+                                            L::raw_bytes);
+    double acc[4];
+    cc_tile<R, TY, MK>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, fimg, mimg, vimg, d_fixed,
+                       d_moving, want_norms, acc);
+    // block partials, then the fixed-order last-block reduction
+    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    cc_block_partials<L::NP, L::NT>(acc, red, partials + (size_t)bid * L::NP);
+    if (!cc_last(counter, nblocks)) return;
+    cc_finish<L::NP, MK>(partials, nblocks, a.g.n, result, counter);
+}
+
+// The CC pair of every active subject of a batch (unmasked): subject b's images at
+// fimg / mimg + b * img_stride, its derivative fields at d_fixed / d_moving + b * field_stride,
+// its tile partials at partials + b * part_stride, its last-tile counter at counter[b] and its
+// [value, |dF|^2, |dM|^2] at result + b * result_stride. Tiles are summed in the single
+// kernel's block order, so a subject's value does not depend on the batch.
+template <int R, int TY>
+__global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair_batch(
+    CcArgs a, BatchList Lb, const float* __restrict__ fimg, const float* __restrict__ mimg,
+    long long img_stride, float* __restrict__ d_fixed, float* __restrict__ d_moving,
+    long long field_stride, double* __restrict__ partials, long long part_stride,
+    unsigned int* __restrict__ counter, double* __restrict__ result, int result_stride,
+    int want_norms) {
+    using L = Layout<R, TY, false>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* red = reinterpret_cast<double*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes +
+                                            L::raw_bytes);
+    const int work = *Lb.count * Lb.tiles;
+    const int gx = (a.g.nx + TX - 1) / TX, gy = (a.g.ny + TY - 1) / TY;
+    for (int w = blockIdx.x; w < work; w += gridDim.x) {
+        const int b = Lb.active[w / Lb.tiles], t = w % Lb.tiles;
+        int bx, by, bz;
+        tile_coords(t, gx, gy, bx, by, bz);
+        double acc[4];
+        cc_tile<R, TY, false>(a, bx, by, bz, smem, fimg + b * img_stride, mimg + b * img_stride,
+                              nullptr, d_fixed + b * field_stride, d_moving + b * field_stride,
+                              want_norms, acc);
+        double* pb = partials + b * part_stride;
+        cc_block_partials<L::NP, L::NT>(acc, red, pb + (size_t)t * L::NP);
+        if (cc_last(counter + b, (unsigned int)Lb.tiles))
+            cc_finish<L::NP, false>(pb, (unsigned int)Lb.tiles, a.g.n,
+                                    result + (size_t)b * result_stride, counter + b);
+        __syncthreads();  // the next tile rewrites the shared sums
     }
 }
 
@@ -427,23 +499,103 @@ int launch_radius(fw_ctx* ctx, const CcArgs& a, int radius, const float* f, cons
     }
 }
 
+template <int R>
+int launch_cc_batch_r(fw_ctx* ctx, const CcArgs& a, const BatchList& L, int blocks,
+                      const float* f, const float* m, long long img_stride, float* df, float* dm,
+                      long long field_stride, double* partials, long long part_stride,
+                      unsigned int* counter, double* result, int result_stride, int want_norms) {
+    using Lay = Layout<R, 8, false>;
+    FW_CUDA(cudaFuncSetAttribute(k_cc_pair_batch<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Lay::bytes));
+    k_cc_pair_batch<R, 8><<<blocks, Lay::NT, Lay::bytes, ctx->stream>>>(
+        a, L, f, m, img_stride, df, dm, field_stride, partials, part_stride, counter, result,
+        result_stride, want_norms);
+    return check_launch(ctx, "k_cc_pair_batch");
+}
+
+template <int R>
+int cc_batch_occupancy() {
+    using Lay = Layout<R, 8, false>;
+    cudaFuncSetAttribute(k_cc_pair_batch<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Lay::bytes);
+    int o = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_cc_pair_batch<R, 8>, Lay::NT,
+                                                      Lay::bytes) != cudaSuccess || o < 1) {
+        cudaGetLastError();
+        o = 1;
+    }
+    return o;
+}
+
+CcArgs cc_args(const HostGrid& g, long long ps) {
+    CcArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = dev_grid(g);
+    a.ps = ps;
+    for (int d = 0; d < 3; ++d) a.isp[d] = 1.0 / g.sp[d];
+    a.identity_dir = 1;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            if (g.dir[r * 3 + c] != (r == c ? 1.0 : 0.0)) a.identity_dir = 0;
+    return a;
+}
+
 }  // namespace
+
+int cc_batch_tiles(const HostGrid& g, int zchunk) {
+    const long long gx = (g.n[0] + TX - 1) / TX, gy = (g.n[1] + 7) / 8;
+    const long long gz = (g.n[2] + zchunk - 1) / zchunk;
+    return (int)(gx * gy * gz);
+}
+
+int cc_batch_blocks_per_sm(int radius) {
+    switch (radius) {
+        case 1: return cc_batch_occupancy<1>();
+        case 2: return cc_batch_occupancy<2>();
+        case 3: return cc_batch_occupancy<3>();
+        case 4: return cc_batch_occupancy<4>();
+        case 5: return cc_batch_occupancy<5>();
+        case 6: return cc_batch_occupancy<6>();
+        case 7: return cc_batch_occupancy<7>();
+        case 8: return cc_batch_occupancy<8>();
+        default: return 1;
+    }
+}
+
+int launch_cc_pair_batch(fw_ctx* ctx, const HostGrid& g, long long ps, int radius, int zchunk,
+                         const BatchList& L, int blocks, const float* fimg, const float* mimg,
+                         long long img_stride, float* d_fixed, float* d_moving,
+                         long long field_stride, double* partials, long long part_stride,
+                         unsigned int* counter, double* result, int result_stride,
+                         int want_norms) {
+    CcArgs a = cc_args(g, ps);
+    a.zchunk = zchunk;
+#define FW_CC_BATCH(RR)                                                                          \
+    case RR:                                                                                    \
+        return launch_cc_batch_r<RR>(ctx, a, L, blocks, fimg, mimg, img_stride, d_fixed,         \
+                                     d_moving, field_stride, partials, part_stride, counter,     \
+                                     result, result_stride, want_norms);
+    switch (radius) {
+        FW_CC_BATCH(1)
+        FW_CC_BATCH(2)
+        FW_CC_BATCH(3)
+        FW_CC_BATCH(4)
+        FW_CC_BATCH(5)
+        FW_CC_BATCH(6)
+        FW_CC_BATCH(7)
+        FW_CC_BATCH(8)
+        default:
+            return fail(FW_ERR_INVALID, "cc metric: radius must be in 1..=8 (BOX_RADIUS_MAX)");
+    }
+#undef FW_CC_BATCH
+}
 
 // d_result receives [value, sum |d_fixed|^2, sum |d_moving|^2] and, with `valid`, the number of
 // valid voxels in d_result[3].
 int launch_cc_pair_impl(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
                         fw_field* d_fixed, fw_field* d_moving, double* d_result, int want_norms,
                         const fw_image* valid) {
-    CcArgs a;
-    std::memset(&a, 0, sizeof(a));
-    a.g = dev_grid(fixed->grid);
-    a.ps = d_fixed->ps;
-    const HostGrid& g = fixed->grid;
-    for (int d = 0; d < 3; ++d) a.isp[d] = 1.0 / g.sp[d];
-    a.identity_dir = 1;
-    for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c)
-            if (g.dir[r * 3 + c] != (r == c ? 1.0 : 0.0)) a.identity_dir = 0;
+    CcArgs a = cc_args(fixed->grid, d_fixed->ps);
     if (valid)
         return launch_radius<true>(ctx, a, radius, fixed->d, moving->d, valid->d, d_fixed->d,
                                    d_moving->d, d_result, want_norms);

@@ -311,13 +311,11 @@ __global__ void __launch_bounds__(256) k_warp(WarpArgs a, const float* __restric
 
 // The plain warp (no earlier field, linear interpolation) -- the SyN loop's per-iteration warps --
 // over 32 x 8 column tiles marching along z, the next slice's displacement loaded while the
-// current one gathers.
-__global__ void __launch_bounds__(256) k_warp_t(WarpArgs a, int zchunk,
-                                                const float* __restrict__ u,
-                                                const float* __restrict__ src,
-                                                float* __restrict__ out) {
-    int x, y, z0, z1;
-    if (!column_of(a.g.nx, a.g.ny, a.g.nz, zchunk, x, y, z0, z1)) return;
+// current one gathers. One column [z0, z1) of the thread.
+__device__ __forceinline__ void warp_column(const WarpArgs& a, int x, int y, int z0, int z1,
+                                            const float* __restrict__ u,
+                                            const float* __restrict__ src,
+                                            float* __restrict__ out) {
     const long long sxy = (long long)a.g.nx * a.g.ny;
     long long l = (long long)z0 * sxy + (long long)y * a.g.nx + x;
     float ux = u[l], uy = u[l + a.fps], uz = u[l + 2 * a.fps];
@@ -345,6 +343,38 @@ __global__ void __launch_bounds__(256) k_warp_t(WarpArgs a, int zchunk,
     }
 }
 
+__global__ void __launch_bounds__(256) k_warp_t(WarpArgs a, int zchunk,
+                                                const float* __restrict__ u,
+                                                const float* __restrict__ src,
+                                                float* __restrict__ out) {
+    int x, y, z0, z1;
+    if (!column_of(a.g.nx, a.g.ny, a.g.nz, zchunk, x, y, z0, z1)) return;
+    warp_column(a, x, y, z0, z1, u, src, out);
+}
+
+// The same warp for every active subject of a batch: subject b gathers from srcs[b] through
+// args[b] (per_subject) or from srcs[0] through args[0] (the shared template), with its field at
+// u + b * u_stride and its output at out + b * out_stride.
+__global__ void __launch_bounds__(256) k_warp_t_batch(const WarpArgs* __restrict__ args,
+                                                      const float* const* __restrict__ srcs,
+                                                      int per_subject, int zchunk, BatchList L,
+                                                      const float* __restrict__ u,
+                                                      long long u_stride,
+                                                      float* __restrict__ out,
+                                                      long long out_stride) {
+    const int work = *L.count * L.tiles;
+    const int gx = (args[0].g.nx + 31) / 32, gy = (args[0].g.ny + 7) / 8;
+    for (int w = blockIdx.x; w < work; w += gridDim.x) {
+        const int b = L.active[w / L.tiles];
+        const int q = per_subject ? b : 0;
+        const WarpArgs& a = args[q];
+        int bx, by, bz, x, y, z0, z1;
+        tile_coords(w % L.tiles, gx, gy, bx, by, bz);
+        if (!column_of_tile(a.g.nx, a.g.ny, a.g.nz, zchunk, bx, by, bz, x, y, z0, z1)) continue;
+        warp_column(a, x, y, z0, z1, u + b * u_stride, srcs[q], out + b * out_stride);
+    }
+}
+
 struct FieldArgs {
     DevGrid g;
     long long ps;
@@ -353,14 +383,12 @@ struct FieldArgs {
 // field_ops.rs:251-272 with the scale of syn.rs:285-298 fused: out(x) = w(x) + s * u(x + w(x)),
 // s = step / max |u/sp| (step when the max is 0) or 1 without a max.
 // `w` and `out` may be the same buffer (the SyN loop composes in place: a voxel reads only its
-// own value of `w`), so neither is declared __restrict__.
-__global__ void __launch_bounds__(256) k_compose(FieldArgs a, int zchunk,
-                                                 const float* __restrict__ u, const float* w,
-                                                 float* out,
-                                                 const unsigned int* __restrict__ max_bits,
-                                                 double step) {
-    int i, j, z0, z1;
-    if (!column_of(a.g.nx, a.g.ny, a.g.nz, zchunk, i, j, z0, z1)) return;
+// own value of `w`), so neither is declared __restrict__. One column [z0, z1) of the thread.
+__device__ __forceinline__ void compose_column(const FieldArgs& a, int i, int j, int z0, int z1,
+                                               const float* __restrict__ u, const float* w,
+                                               float* out,
+                                               const unsigned int* __restrict__ max_bits,
+                                               double step) {
     float s = 1.0f;
     if (max_bits) {
         float mx = __uint_as_float(*max_bits);
@@ -392,6 +420,35 @@ __global__ void __launch_bounds__(256) k_compose(FieldArgs a, int zchunk,
         wx = qx;
         wy = qy;
         wz = qz;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_compose(FieldArgs a, int zchunk,
+                                                 const float* __restrict__ u, const float* w,
+                                                 float* out,
+                                                 const unsigned int* __restrict__ max_bits,
+                                                 double step) {
+    int i, j, z0, z1;
+    if (!column_of(a.g.nx, a.g.ny, a.g.nz, zchunk, i, j, z0, z1)) return;
+    compose_column(a, i, j, z0, z1, u, w, out, max_bits, step);
+}
+
+// In place for every active subject of a batch: field + b * stride composed with the update
+// u + b * stride, scaled by step / its max at max_bits[b * max_stride].
+__global__ void __launch_bounds__(256) k_compose_batch(FieldArgs a, int zchunk, BatchList L,
+                                                       const float* __restrict__ u, float* field,
+                                                       long long stride,
+                                                       const unsigned int* __restrict__ max_bits,
+                                                       int max_stride, double step) {
+    const int work = *L.count * L.tiles;
+    const int gx = (a.g.nx + 31) / 32, gy = (a.g.ny + 7) / 8;
+    for (int w = blockIdx.x; w < work; w += gridDim.x) {
+        const int b = L.active[w / L.tiles];
+        int bx, by, bz, i, j, z0, z1;
+        tile_coords(w % L.tiles, gx, gy, bx, by, bz);
+        if (!column_of_tile(a.g.nx, a.g.ny, a.g.nz, zchunk, bx, by, bz, i, j, z0, z1)) continue;
+        float* f = field + b * stride;
+        compose_column(a, i, j, z0, z1, u + b * stride, f, f, max_bits + b * max_stride, step);
     }
 }
 
@@ -516,14 +573,14 @@ static inline unsigned int blocks_for(long long n, int t = 256) {
     return (unsigned int)((n + t - 1) / t);
 }
 
-int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const fw_field* pre,
-                const fw_affine* affine, float* out, bool mask, const float* product) {
-    WarpArgs a;
+// The arguments of a warp of a source on `sg` through a field on `fg` (plane stride fps) and an
+// optional affine, without an earlier field: the index map c = Q idx + R u + q0.
+static void plain_warp_args(const HostGrid& sg, const HostGrid& fg, long long fps,
+                            const fw_affine* affine, WarpArgs& a) {
     std::memset(&a, 0, sizeof(a));
-    a.g = dev_grid(field->grid);
-    a.s = dev_grid(src->grid);
-    a.fps = field->ps;
-    a.mask = mask ? 1 : 0;
+    a.g = dev_grid(fg);
+    a.s = dev_grid(sg);
+    a.fps = fps;
     double am[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, ao[3] = {0, 0, 0};
     if (affine) {
         std::memcpy(am, affine->matrix, sizeof(am));
@@ -531,22 +588,54 @@ int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const f
     }
     std::memcpy(a.am, am, sizeof(am));
     std::memcpy(a.ao, ao, sizeof(ao));
+    // c = S^-1 (A (org + DS idx + u) + ao - s_org) = Q idx + R u + q0
+    double ra[9];
+    mat3_mul(sg.inv, am, ra);
+    mat3_mul(ra, fg.ds, a.q);
+    std::memcpy(a.r, ra, sizeof(ra));
+    double ag[3];
+    mat3_vec(am, fg.org, ag);
+    double t[3] = {ag[0] + ao[0] - sg.org[0], ag[1] + ao[1] - sg.org[1], ag[2] + ao[2] - sg.org[2]};
+    mat3_vec(sg.inv, t, a.q0);
+}
+
+size_t warp_args_size() { return sizeof(WarpArgs); }
+
+void fill_warp_args(const HostGrid& src_grid, const HostGrid& field_grid, long long fps,
+                    const fw_affine* affine, void* out) {
+    plain_warp_args(src_grid, field_grid, fps, affine, *static_cast<WarpArgs*>(out));
+}
+
+int launch_warp_batch(fw_ctx* ctx, const void* d_args, const float* const* d_srcs,
+                      int per_subject, const HostGrid& g, int zchunk, const BatchList& L,
+                      int blocks, const float* u, long long u_stride, float* out,
+                      long long out_stride) {
+    (void)g;
+    k_warp_t_batch<<<blocks, 256, 0, ctx->stream>>>(static_cast<const WarpArgs*>(d_args), d_srcs,
+                                                   per_subject, zchunk, L, u, u_stride, out,
+                                                   out_stride);
+    return check_launch(ctx, "k_warp_t_batch");
+}
+
+int launch_compose_batch(fw_ctx* ctx, const HostGrid& g, long long ps, int zchunk,
+                         const BatchList& L, int blocks, const float* u, float* field,
+                         long long stride, const unsigned int* max_bits, int max_stride,
+                         double step) {
+    FieldArgs a{dev_grid(g), ps};
+    k_compose_batch<<<blocks, 256, 0, ctx->stream>>>(a, zchunk, L, u, field, stride, max_bits,
+                                                    max_stride, step);
+    return check_launch(ctx, "k_compose_batch");
+}
+
+int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const fw_field* pre,
+                const fw_affine* affine, float* out, bool mask, const float* product) {
+    WarpArgs a;
+    plain_warp_args(src->grid, field->grid, field->ps, affine, a);
+    a.mask = mask ? 1 : 0;
     if (pre) {
         a.has_pre = 1;
         a.p = dev_grid(pre->grid);
         a.pps = pre->ps;
-    } else {
-        // c = S^-1 (A (org + DS idx + u) + ao - s_org) = Q idx + R u + q0
-        const HostGrid& g = field->grid;
-        const HostGrid& s = src->grid;
-        double ra[9];
-        mat3_mul(s.inv, am, ra);
-        mat3_mul(ra, g.ds, a.q);
-        std::memcpy(a.r, ra, sizeof(ra));
-        double ag[3];
-        mat3_vec(am, g.org, ag);
-        double t[3] = {ag[0] + ao[0] - s.org[0], ag[1] + ao[1] - s.org[1], ag[2] + ao[2] - s.org[2]};
-        mat3_vec(s.inv, t, a.q0);
     }
     long long n = a.g.n;
     if (!pre && !mask) {

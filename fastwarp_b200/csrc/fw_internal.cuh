@@ -357,13 +357,42 @@ inline dim3 column_grid(int nx, int ny, int nz, int num_sms, int* zchunk) {
     return g;
 }
 
-__device__ __forceinline__ bool column_of(int nx, int ny, int nz, int zchunk, int& x, int& y,
-                                          int& z0, int& z1) {
-    x = blockIdx.x * 32 + (threadIdx.x & 31);
-    y = blockIdx.y * 8 + (threadIdx.x >> 5);
-    z0 = blockIdx.z * zchunk;
+// The thread's column of tile (bx, by, bz): x, y and the slices [z0, z1).
+__device__ __forceinline__ bool column_of_tile(int nx, int ny, int nz, int zchunk, int bx, int by,
+                                               int bz, int& x, int& y, int& z0, int& z1) {
+    x = bx * 32 + (threadIdx.x & 31);
+    y = by * 8 + (threadIdx.x >> 5);
+    z0 = bz * zchunk;
     z1 = min(z0 + zchunk, nz);
     return x < nx && y < ny && z0 < z1;
+}
+
+__device__ __forceinline__ bool column_of(int nx, int ny, int nz, int zchunk, int& x, int& y,
+                                          int& z0, int& z1) {
+    return column_of_tile(nx, ny, nz, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, x, y, z0, z1);
+}
+
+// ---- batched launches: many subjects of one level grid in one launch ---------------------
+//
+// The subjects of a batch share the template's level grid, so every per-subject buffer of a kind
+// is one allocation with a fixed stride per subject. A batched kernel walks a work list: item w
+// is tile (w mod tiles) of subject active[w / tiles]; blocks stride over the items
+// (persistently: a grid of a few blocks per SM). The active list and its length live on the
+// device and change between iterations (a subject that converged or failed drops out), so a
+// captured graph's launches stay valid while the ragged list shrinks.
+struct BatchList {
+    const int* active;  // subject indices, in slot order
+    const int* count;   // number of active subjects
+    int tiles;          // work items per subject
+};
+
+// Tile t of a (gx, gy, *) grid as block coordinates (the single-subject kernels' blockIdx order,
+// so a tile's partial sums land at the same index in both).
+__device__ __forceinline__ void tile_coords(int t, int gx, int gy, int& bx, int& by, int& bz) {
+    bx = t % gx;
+    const int r = t / gx;
+    by = r % gy;
+    bz = r / gy;
 }
 
 // 32-bit division: grids hold fewer than 2^31 voxels.
@@ -419,6 +448,34 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
 int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
                            InvState* st, cudaGraphConditionalHandle handle, int use_handle);
 int enqueue_inversion_rearm(fw_ctx* ctx, InvState* st, int max_iterations);
+// Adds a WHILE node on `handle` at the capture position of stream `s`; `body` receives the graph
+// the loop runs (fw_syn.cu).
+int add_while_node(cudaStream_t s, cudaGraphConditionalHandle handle, cudaGraph_t* body);
+
+// Batched Gaussian smoothing of update fields (fw_smooth.cu; the same taps on the three axes,
+// radius <= 12): in / out / tmp + b * stride, the max |u/sp| of subject b into
+// max_bits[b * max_stride]; `blocks_xy` / `blocks_z` persistent blocks for the two passes.
+int launch_smooth_batch(fw_ctx* ctx, const HostGrid& g, long long ps, double variance,
+                        const int* active, const int* count, int blocks_xy, int blocks_z,
+                        const float* in, float* out, float* tmp, long long stride,
+                        unsigned int* max_bits, int max_stride);
+
+// Batched inversions (fw_invert.cu): measurement tiles per subject for z chunks of `zchunk`,
+// virtual blocks per subject of a body sweep, the measurement, a body (the pair of kernels) and
+// the kernel that sets the inner loop's condition. Partials: 2 doubles per tile or virtual block.
+int inv_measure_tiles(const HostGrid& g, int zchunk);
+int inv_body_vblocks(fw_ctx* ctx, long long n);
+int launch_inv_measure_batch(fw_ctx* ctx, const HostGrid& g, long long ps, int zchunk,
+                             const BatchList& L, int blocks, const float* f, const float* psi,
+                             float* res, long long stride, double* partials,
+                             long long part_stride, unsigned int* counter, InvState* st,
+                             int st_stride, const fw_invert_params& prm);
+int launch_inv_body_batch(fw_ctx* ctx, const HostGrid& g, long long ps, const BatchList& L,
+                          int blocks, const float* f, float* psi, float* res, long long stride,
+                          double* partials, long long part_stride, unsigned int* counter,
+                          InvState* st, int st_stride);
+int launch_inv_any(fw_ctx* ctx, const InvState* st, int st_stride, const BatchList& L,
+                   cudaGraphConditionalHandle handle);
 int read_back(fw_ctx* ctx, const double* d, int k, double* out);
 }  // namespace fw
 
@@ -449,6 +506,15 @@ int enqueue_image_upload_f32(fw_ctx* ctx, const HostGrid& g, const float* host, 
 void linear_transform_map(const fw_linear_transform* t, double M[9], double off[3]);
 // The context a device MI level evaluates on (fw_mi.cu).
 const fw_ctx* mi_level_context(const fw_mi_level* level);
+
+// The SyN recipe's validation (fw_syn.cu): 0 or FW_ERR_INVALID with the reference's message.
+int syn_recipe_check(const fw_syn_recipe* r);
+
+// The batching form (fw_batch.cu): fw_batch_syn_run after the argument checks.
+int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed, int nsub,
+                  const fw_batch_subject* subj, fw_field** warps, fw_field** inverses,
+                  fw_syn_iteration* records, int64_t cap, int64_t* counts, int32_t* statuses,
+                  fw_batch_report* report);
 
 // The SyN stage on device images (fw_syn.cu); masks may be null; prior / prior_inverse are the
 // earlier SyN stages' collapsed fields (both null for a first stage).
@@ -482,6 +548,34 @@ enum Slot : int {
 
 int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const fw_field* pre,
                 const fw_affine* affine, float* out, bool mask, const float* product);
+
+// ---- batched kernels (fw_core.cu, fw_cc.cu, fw_smooth.cu, fw_invert.cu) ---------------------
+// Every one runs the single-subject kernel's tile body over a BatchList with `blocks` blocks;
+// per-subject buffers are base + b * stride.
+
+// The warp arguments (an opaque device struct of warp_args_size() bytes) of a source on
+// `src_grid` through a field on `field_grid` and an optional affine.
+size_t warp_args_size();
+void fill_warp_args(const HostGrid& src_grid, const HostGrid& field_grid, long long fps,
+                    const fw_affine* affine, void* out);
+int launch_warp_batch(fw_ctx* ctx, const void* d_args, const float* const* d_srcs,
+                      int per_subject, const HostGrid& g, int zchunk, const BatchList& L,
+                      int blocks, const float* u, long long u_stride, float* out,
+                      long long out_stride);
+int launch_compose_batch(fw_ctx* ctx, const HostGrid& g, long long ps, int zchunk,
+                         const BatchList& L, int blocks, const float* u, float* field,
+                         long long stride, const unsigned int* max_bits, int max_stride,
+                         double step);
+// The CC pair of a batch (unmasked): tiles per subject for z chunks of `zchunk` slices, resident
+// blocks per SM, and the launch (partials: 3 doubles per tile and subject).
+int cc_batch_tiles(const HostGrid& g, int zchunk);
+int cc_batch_blocks_per_sm(int radius);
+int launch_cc_pair_batch(fw_ctx* ctx, const HostGrid& g, long long ps, int radius, int zchunk,
+                         const BatchList& L, int blocks, const float* fimg, const float* mimg,
+                         long long img_stride, float* d_fixed, float* d_moving,
+                         long long field_stride, double* partials, long long part_stride,
+                         unsigned int* counter, double* result, int result_stride,
+                         int want_norms);
 int launch_cc_pair(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int radius,
                    fw_field* d_fixed, fw_field* d_moving, double* d_value, double* d_norms);
 // Gaussian smoothing of `in` into `out` (out may be in) with the max |u/sp| of the result fused

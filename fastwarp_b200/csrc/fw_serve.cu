@@ -707,5 +707,8 @@ extern "C" size_t fw_abi_struct_size(const char* name) {
     if (n == "fw_linear_request") return sizeof(fw_linear_request);
     if (n == "fw_linear_chain_result") return sizeof(fw_linear_chain_result);
     if (n == "fw_linear_result") return sizeof(fw_linear_result);
+    if (n == "fw_batch_subject") return sizeof(fw_batch_subject);
+    if (n == "fw_batch_tuning") return sizeof(fw_batch_tuning);
+    if (n == "fw_batch_report") return sizeof(fw_batch_report);
     return 0;
 }

@@ -209,22 +209,23 @@ constexpr int XY_T = 32;     // output tile edge of the xy pass
 constexpr int XY_NT = 256;   // threads: 32 columns x 8 rows, 4 output rows each
 constexpr int Z_SEG = 16;    // z outputs per thread of the z pass
 
+// One 32 x 32 tile (bx, by) of slice z of the xy pass.
 template <int R>
-__global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* __restrict__ in,
-                                                     float* __restrict__ tmp, long long ps_tmp) {
+__device__ __forceinline__ void smooth_xy_tile(const SmoothArgs& a, int bx, int by, int z,
+                                               float* smem_xy, const float* __restrict__ in,
+                                               float* __restrict__ tmp, long long ps_tmp) {
     constexpr int HX = XY_T + 2 * R, HY = XY_T + 2 * R;
     constexpr int HXP = (HX + 3) & ~3;       // rows start on 16 bytes
     constexpr int NV = (4 + 2 * R + 3) / 4;  // float4 loads per x window of four outputs
     constexpr int TILE = HY * HXP;
     // the three components' tiles at once (dynamic: [3][TILE] + pad, then [3][HY][32] x sums):
     // all their loads in flight together, two barriers per block
-    extern __shared__ __align__(16) float smem_xy[];
     float* tile = smem_xy;
     float* xs = smem_xy + 3 * TILE + 4 * NV;
     const int nx = a.g.nx, ny = a.g.ny;
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
-    const int x0 = blockIdx.x * XY_T, y0 = blockIdx.y * XY_T;
-    const long long zoff = (long long)blockIdx.z * nx * ny;
+    const int x0 = bx * XY_T, y0 = by * XY_T;
+    const long long zoff = (long long)z * nx * ny;
     const int x = x0 + tx;
     static_assert(HX <= 64, "a lane loads two halo columns");
     {
@@ -297,16 +298,42 @@ __global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* 
     }
 }
 
-// blockIdx.x: z segment (fastest, so neighbouring segments share their halo rows in L2),
-// blockIdx.y: 32 columns in x, blockIdx.z: 8 rows in y.
 template <int R>
-__global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __restrict__ tmp,
-                                                  long long ps_tmp, const float* in,
-                                                  float* out,
-                                                  unsigned int* __restrict__ max_bits) {
+__global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* __restrict__ in,
+                                                     float* __restrict__ tmp, long long ps_tmp) {
+    extern __shared__ __align__(16) float smem_xy[];
+    smooth_xy_tile<R>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_xy, in, tmp, ps_tmp);
+}
+
+// The xy pass of every active subject of a batch: input at in + b * stride (or at the subject's
+// multichannel accumulator), output into tmp + b * stride; tiles (x, y, slice) in the single
+// kernel's block order.
+template <int R>
+__global__ void __launch_bounds__(XY_NT) k_smooth_xy_batch(SmoothArgs a, BatchList L,
+                                                           const float* __restrict__ in,
+                                                           float* __restrict__ tmp,
+                                                           long long stride) {
+    extern __shared__ __align__(16) float smem_xy[];
+    const int work = *L.count * L.tiles;
+    const int gx = (a.g.nx + XY_T - 1) / XY_T, gy = (a.g.ny + XY_T - 1) / XY_T;
+    for (int w = blockIdx.x; w < work; w += gridDim.x) {
+        const int b = L.active[w / L.tiles];
+        int bx, by, bz;
+        tile_coords(w % L.tiles, gx, gy, bx, by, bz);
+        smooth_xy_tile<R>(a, bx, by, bz, smem_xy, in + b * stride, tmp + b * stride, a.ps_out);
+        __syncthreads();  // the next tile reloads the shared tile
+    }
+}
+
+// The thread's column of tile (z segment zb, 32 columns xb, 8 rows yb) of the z pass; returns the
+// largest |u/sp| it wrote (when max_bits is wanted).
+template <int R>
+__device__ __forceinline__ float smooth_z_tile(const SmoothArgs& a, int zb, int xb, int yb,
+                                               const float* __restrict__ tmp, long long ps_tmp,
+                                               const float* in, float* out, bool want_max) {
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
-    const int x = blockIdx.y * 32 + (threadIdx.x & 31), y = blockIdx.z * 8 + (threadIdx.x >> 5);
-    const int zs = blockIdx.x * Z_SEG;
+    const int x = xb * 32 + (threadIdx.x & 31), y = yb * 8 + (threadIdx.x >> 5);
+    const int zs = zb * Z_SEG;
     const long long sxy = (long long)nx * ny;
     float vmax = 0.0f;
     if (x < nx && y < ny) {
@@ -344,7 +371,7 @@ __global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __r
                 nsq[q] = fmaf(p, p, nsq[q]);
             }
         }
-        if (max_bits) {
+        if (want_max) {
 #pragma unroll
             for (int q = 0; q < Z_SEG; ++q)
                 if (zs + q < nz)
@@ -352,9 +379,44 @@ __global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __r
                                               __float_as_int(nan_canon(sqrtf(nsq[q])))));
         }
     }
+    return vmax;
+}
+
+// blockIdx.x: z segment (fastest, so neighbouring segments share their halo rows in L2),
+// blockIdx.y: 32 columns in x, blockIdx.z: 8 rows in y.
+template <int R>
+__global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __restrict__ tmp,
+                                                  long long ps_tmp, const float* in,
+                                                  float* out,
+                                                  unsigned int* __restrict__ max_bits) {
+    float vmax = smooth_z_tile<R>(a, blockIdx.x, blockIdx.y, blockIdx.z, tmp, ps_tmp, in, out,
+                                  max_bits != nullptr);
     if (max_bits) {
         vmax = warp_max_f(vmax);
         if ((threadIdx.x & 31) == 0 && vmax > 0.0f) atomicMax(max_bits, __float_as_uint(vmax));
+    }
+}
+
+// The z pass of every active subject of a batch: tmp / in / out at + b * stride, the max of
+// subject b into max_bits[b * max_stride].
+template <int R>
+__global__ void __launch_bounds__(256) k_smooth_z_batch(SmoothArgs a, BatchList L,
+                                                        const float* __restrict__ tmp,
+                                                        const float* in, float* out,
+                                                        long long stride,
+                                                        unsigned int* __restrict__ max_bits,
+                                                        int max_stride) {
+    const int work = *L.count * L.tiles;
+    const int gz = (a.g.nz + Z_SEG - 1) / Z_SEG, gx = (a.g.nx + 31) / 32;
+    for (int w = blockIdx.x; w < work; w += gridDim.x) {
+        const int b = L.active[w / L.tiles];
+        int zb, xb, yb;
+        tile_coords(w % L.tiles, gz, gx, zb, xb, yb);
+        float vmax = smooth_z_tile<R>(a, zb, xb, yb, tmp + b * stride, a.ps_out, in + b * stride,
+                                      out + b * stride, true);
+        vmax = warp_max_f(vmax);
+        if ((threadIdx.x & 31) == 0 && vmax > 0.0f)
+            atomicMax(max_bits + b * max_stride, __float_as_uint(vmax));
     }
 }
 
@@ -371,6 +433,25 @@ int launch_smooth_xyz(fw_ctx* ctx, const SmoothArgs& a, const fw_field* in, fw_f
     dim3 g2((a.g.nz + Z_SEG - 1) / Z_SEG, (a.g.nx + 31) / 32, (a.g.ny + 7) / 8);
     k_smooth_z<R><<<g2, 256, 0, ctx->stream>>>(a, tmp->d, tmp->ps, in->d, out->d, d_max_bits);
     return check_launch(ctx, "k_smooth_z");
+}
+
+template <int R>
+int launch_smooth_batch_r(fw_ctx* ctx, const SmoothArgs& a, const int* active, const int* count,
+                          int blocks_xy, int blocks_z, const float* in, float* out, float* tmp,
+                          long long stride, unsigned int* max_bits, int max_stride) {
+    constexpr int HY = XY_T + 2 * R, HXP = (XY_T + 2 * R + 3) & ~3, NV = (4 + 2 * R + 3) / 4;
+    constexpr size_t bytes = sizeof(float) * (3 * HY * HXP + 4 * NV + 3 * HY * XY_T);
+    FW_CUDA(cudaFuncSetAttribute(k_smooth_xy_batch<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)bytes));
+    const int gx = (a.g.nx + XY_T - 1) / XY_T, gy = (a.g.ny + XY_T - 1) / XY_T;
+    BatchList Lxy{active, count, gx * gy * a.g.nz};
+    k_smooth_xy_batch<R><<<blocks_xy, XY_NT, bytes, ctx->stream>>>(a, Lxy, in, tmp, stride);
+    FW_TRY(check_launch(ctx, "k_smooth_xy_batch"));
+    const int gz = (a.g.nz + Z_SEG - 1) / Z_SEG, gxc = (a.g.nx + 31) / 32, gyc = (a.g.ny + 7) / 8;
+    BatchList Lz{active, count, gz * gxc * gyc};
+    k_smooth_z_batch<R><<<blocks_z, 256, 0, ctx->stream>>>(a, Lz, tmp, in, out, stride, max_bits,
+                                                          max_stride);
+    return check_launch(ctx, "k_smooth_z_batch");
 }
 
 // ---- Deriche recursive Gaussian (pyramid.rs:186-300, 418-427) --------------------------------
@@ -586,6 +667,55 @@ int launch_smooth(fw_ctx* ctx, const fw_field* in, fw_field* out, double varianc
     FW_CUDA(cudaFuncSetAttribute(k_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     k_smooth<<<grid, SNT, bytes, ctx->stream>>>(a, in->d, out->d, d_max_bits);
     return check_launch(ctx, "k_smooth");
+}
+
+int launch_smooth_batch(fw_ctx* ctx, const HostGrid& g, long long ps, double variance,
+                        const int* active, const int* count, int blocks_xy, int blocks_z,
+                        const float* in, float* out, float* tmp, long long stride,
+                        unsigned int* max_bits, int max_stride) {
+    SmoothArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = dev_grid(g);
+    a.ps_in = a.ps_out = ps;
+    int r[3];
+    for (int ax = 0; ax < 3; ++ax) {
+        std::vector<double> k = gaussian_taps(variance, 0.001, g.n[ax]);
+        r[ax] = (int)k.size() / 2;
+        if (r[ax] > 12)
+            return fail(FW_ERR_INVALID, "batched SyN: the update field's Gaussian radius exceeds 12");
+        float* dst = ax == 0 ? a.tx_ : (ax == 1 ? a.ty_ : a.tz_);
+        for (size_t t = 0; t < k.size(); ++t) dst[t] = (float)k[t];
+    }
+    bool same = r[0] == r[1] && r[1] == r[2];
+    for (int t = 0; same && t <= 2 * r[0]; ++t)
+        same = a.tx_[t] == a.ty_[t] && a.ty_[t] == a.tz_[t];
+    if (!same)
+        return fail(FW_ERR_INVALID,
+                    "batched SyN: the update field's Gaussian differs between axes on this grid");
+    a.rx = a.ry = a.rz = r[0];
+    double w1 = variance < 0.5 ? 1.0 - variance / 0.5 : 1.0;
+    a.w1 = (float)w1;
+    a.w2 = (float)(1.0 - w1);
+#define FW_SMOOTH_BATCH(RR) \
+    case RR:                \
+        return launch_smooth_batch_r<RR>(ctx, a, active, count, blocks_xy, blocks_z, in, out, tmp, stride, max_bits, max_stride);
+    switch (r[0]) {
+        FW_SMOOTH_BATCH(1)
+        FW_SMOOTH_BATCH(2)
+        FW_SMOOTH_BATCH(3)
+        FW_SMOOTH_BATCH(4)
+        FW_SMOOTH_BATCH(5)
+        FW_SMOOTH_BATCH(6)
+        FW_SMOOTH_BATCH(7)
+        FW_SMOOTH_BATCH(8)
+        FW_SMOOTH_BATCH(9)
+        FW_SMOOTH_BATCH(10)
+        FW_SMOOTH_BATCH(11)
+        FW_SMOOTH_BATCH(12)
+        default:
+            return fail(FW_ERR_INVALID, "batched SyN: the update field's Gaussian radius is zero");
+    }
+#undef FW_SMOOTH_BATCH
 }
 
 int launch_smooth_recursive(fw_ctx* ctx, const fw_image* img, const double sigma_mm[3],

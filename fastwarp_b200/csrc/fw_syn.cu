@@ -26,150 +26,26 @@
 #include <vector>
 
 #include "fw_internal.cuh"
+#include "fw_syn_state.cuh"
 
 namespace fw {
 
 namespace {
 
-constexpr int MAX_WINDOW = 64;
-
-struct SynDev {
-    int done;        // iterations recorded over all levels (the trace's write position)
-    int it;          // iterations done in this level
-    int limit;       // iteration limit of this level
-    int converged;
-    int status;      // 0 ok, 1 gradient not finite, 2 field not finite, 3 cancelled,
-                     // 4 no voxel inside the masks (CC), 10 + k a Mattes pair's status k
-    int level;
-    int window;
-    int count;       // values in the window
-    int head;
-    double total;    // running sum of |energy| of every value added
-    double values[MAX_WINDOW];
-    double threshold;
-    double step;
-    int channels;
-    int masked;      // the CC pairs take the masks' valid voxels
-    double wnorm[FW_MAX_CHANNELS];
-    int metric[FW_MAX_CHANNELS];  // FW_METRIC_CC or FW_METRIC_MATTES
-};
-
-// convergence.rs:91-126, the closed form of the two-control-point fit.
-__device__ double convergence_value(const SynDev& s) {
-    if (s.count < s.window) return DBL_MAX;
-    if (s.window < 2) return 0.0;
-    const double spline_eps = 1e-3, domain_spacing = 0.1, domain_size = 11.0;
-    double r = 1.0 / ((domain_size - 1.0) * domain_spacing);
-    double epsilon = r * domain_spacing * spline_eps;
-    double delta[2] = {0, 0}, omega[2] = {0, 0};
-    for (int k = 0; k < s.count; ++k) {
-        double e = s.values[(s.head + k) % s.window];
-        double p = ((double)k / (double)(s.window - 1)) * r;
-        if (fabs(p - 1.0) <= epsilon) p = 1.0 - epsilon;
-        if (p < 0.0 && fabs(p) <= epsilon) p = 0.0;
-        double t = p - floor(p);
-        double w[2] = {1.0 - t, t};
-        double w2 = w[0] * w[0] + w[1] * w[1];
-        double v = e / s.total;
-        for (int j = 0; j < 2; ++j) {
-            omega[j] += w[j] * w[j];
-            delta[j] += v * (w[j] * w[j] * w[j] / w2);
-        }
-    }
-    double phi[2] = {0, 0};
-    for (int j = 0; j < 2; ++j) {
-        if (fabs(omega[j]) > DBL_EPSILON) {
-            double q = delta[j] / omega[j];
-            phi[j] = isfinite(q) ? q : 0.0;
-        }
-    }
-    return phi[0] - phi[1];
-}
-
 // A level whose run is enqueued behind a failed one (the status is kept from level to level)
 // runs no iteration: the host reads the status once, after the last level.
 __global__ void k_syn_level_init(SynDev* s, int level, int limit,
                                  cudaGraphConditionalHandle handle, int use_handle) {
-    s->it = 0;
-    s->limit = s->status == 0 ? limit : 0;
-    s->converged = 0;
-    s->level = level;
-    s->count = 0;
-    s->head = 0;
-    s->total = 0.0;
-    if (use_handle) cudaGraphSetConditional(handle, s->limit > 0 ? 1u : 0u);
+    const int run = syn_level_begin(s, level, limit);
+    if (use_handle) cudaGraphSetConditional(handle, run ? 1u : 0u);
 }
 
-// Per-channel scalars, CC_STRIDE doubles a channel: [value (fixed, moving), |dF|^2, |dM|^2,
-// valid voxels (masked CC), value (moving, fixed) (Mattes), status (Mattes)].
-constexpr int CC_STRIDE = 8;
-
-// cc: the per-channel scalars; max_bits: [F side, M side]; inv: 4 loop states.
 __global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
                              const unsigned int* __restrict__ max_bits,
                              const InvState* __restrict__ inv, fw_syn_iteration* trace,
                              int trace_cap, const volatile int* cancel,
                              cudaGraphConditionalHandle handle, int use_handle) {
-    // the CC value is symmetric in its two images; Mattes gives one value per direction
-    auto value_m = [&](int c) {
-        return s->metric[c] == FW_METRIC_MATTES ? cc[CC_STRIDE * c + 4] : cc[CC_STRIDE * c];
-    };
-    double vF = cc[0], vM = value_m(0);
-    double wF = 0.0, wM = 0.0;
-    for (int c = 0; c < s->channels; ++c) {
-        wF += cc[CC_STRIDE * c] * s->wnorm[c];
-        wM += value_m(c) * s->wnorm[c];
-    }
-    if (s->channels == 1) {
-        wF = vF;
-        wM = vM;
-    }
-    for (int c = 0; c < s->channels && s->channels > 1; ++c)
-        if (!isfinite(cc[CC_STRIDE * c + 1]) || !isfinite(cc[CC_STRIDE * c + 2])) s->status = 1;
-    for (int c = 0; c < s->channels; ++c) {
-        if (s->metric[c] == FW_METRIC_MATTES) {
-            const int k = (int)cc[CC_STRIDE * c + 5];
-            if (k != 0) s->status = 10 + k;
-        } else if (s->masked && cc[CC_STRIDE * c + 3] == 0.0) {
-            s->status = 4;
-        }
-    }
-    float mF = __uint_as_float(max_bits[0]), mM = __uint_as_float(max_bits[1]);
-    if (!isfinite(mF) || !isfinite(mM)) s->status = 1;
-    for (int q = 0; q < 4; ++q)
-        if (!isfinite(inv[q].mean) || !isfinite(inv[q].max)) s->status = s->status ? s->status : 2;
-    double energy = 0.5 * (vF + vM);
-    // WindowConvergenceMonitor::add_energy_value
-    if (s->count < s->window) {
-        s->values[(s->head + s->count) % s->window] = energy;
-        s->count++;
-    } else {
-        s->values[s->head] = energy;
-        s->head = (s->head + 1) % s->window;
-    }
-    s->total += fabs(energy);
-    double cv = convergence_value(*s);
-    if (cv < s->threshold) s->converged = 1;
-    int it = s->it, rec = s->done;
-    if (rec < trace_cap) {
-        fw_syn_iteration r;
-        r.level = s->level;
-        r.energy = energy;
-        r.energy_weighted = 0.5 * (wF + wM);
-        r.convergence_value = cv;
-        r.fixed_update_scale = mF > 0.0f ? s->step / (double)mF : s->step;
-        r.moving_update_scale = mM > 0.0f ? s->step / (double)mM : s->step;
-        for (int q = 0; q < 4; ++q) {
-            r.inversions[q].iterations = inv[q].executed;
-            r.inversions[q].mean_error_norm = inv[q].executed ? inv[q].mean : 0.0;
-            r.inversions[q].max_error_norm = inv[q].executed ? inv[q].max : 0.0;
-        }
-        trace[rec] = r;
-    }
-    s->it = it + 1;
-    s->done = rec + 1;
-    if (cancel && *cancel) s->status = 3;
-    int more = (s->it < s->limit) && !s->converged && s->status == 0;
+    const int more = syn_record_step(s, cc, max_bits, inv, trace, trace_cap, cancel);
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
@@ -281,6 +157,8 @@ struct RunDev {
 
 const fw_invert_params kSynInvert = {20, 0.001, 0.1, 1};
 
+}  // namespace
+
 // Adds a WHILE node on an existing handle at the capture position of `s`.
 int add_while_node(cudaStream_t s, cudaGraphConditionalHandle handle, cudaGraph_t* body) {
     cudaStreamCaptureStatus status;
@@ -299,6 +177,8 @@ int add_while_node(cudaStream_t s, cudaGraphConditionalHandle handle, cudaGraph_
     FW_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
     return 0;
 }
+
+namespace {
 
 // One inversion: in graph mode a WHILE node around the body kernel; in direct mode a host loop.
 int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inverse,
@@ -754,6 +634,8 @@ int check_masks(fw_ctx* ctx, const fw_image* fmask, const fw_image* mmask) {
 }
 
 }  // namespace
+
+int syn_recipe_check(const fw_syn_recipe* r) { return syn_validate(r); }
 
 int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fixed,
                    const fw_image* const* moving, const fw_image* fixed_mask,

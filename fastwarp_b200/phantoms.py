@@ -139,3 +139,54 @@ def head_pair(shape_xyz=(193, 229, 193), seed: int = BASE_SEED + 2, spacing: flo
     # index-space map -> physical: isotropic spacing scales the offset only
     initial = make_affine(lin, offset * spacing)
     return grid, fixed, grid, moving, initial
+
+
+def t2_like(t1):
+    """The T2w-like channel of config 4: inverted tissue contrast inside the head (1 - value where
+    the T1-like value exceeds the background), background unchanged."""
+    head = t1 > 0.1
+    return np.where(head, 1.0 - t1, t1).astype(np.float32)
+
+
+def batch_subjects(backend, n, template_shape=(193, 229, 193), dims=(160, 240),
+                   seed: int = BASE_SEED + 4):
+    """Config 4 on the device: the template's two channels (the head phantom as the T1-like one
+    and its inverted-contrast T2-like copy) and `n` subjects, each on its own 1 mm grid with dims
+    drawn uniformly per axis from `dims`, made from the template by an independent random rigid
+    (<= 10 deg, <= 15 mm) and affine (scale 0.9-1.1, shear <= 0.05) map and a smooth displacement
+    (<= 6 mm), warped on the device (subject(x) = template(A(x + u(x))) for every channel).
+    Returns (template grid, [t1, t2] device images, [([s1, s2] device images, initial affine)]):
+    the initial affine maps template points to subject points (the linear part of A, inverted),
+    as a converged linear stage would."""
+    rng = np.random.default_rng(seed)
+    t1 = head_phantom(template_shape, seed)
+    g = make_grid(template_shape)
+    imgs = [backend.upload_image(g, t1), backend.upload_image(g, t2_like(t1))]
+    ct = (np.array(template_shape, float) - 1.0) / 2.0
+    subjects = []
+    for _ in range(n):
+        d = np.array([int(rng.integers(dims[0], dims[1] + 1)) for _ in range(3)])
+        cs = (d - 1.0) / 2.0
+        origin = ct - cs + rng.uniform(-5.0, 5.0, size=3)
+        sg = make_grid(tuple(int(x) for x in d), (1.0, 1.0, 1.0), tuple(origin))
+        rot = _rot(*np.deg2rad(rng.uniform(-10.0, 10.0, size=3)))
+        scale = np.diag(rng.uniform(0.9, 1.1, size=3))
+        shear = np.eye(3)
+        shear[0, 1], shear[0, 2], shear[1, 2] = rng.uniform(-0.05, 0.05, size=3)
+        lin = rot @ scale @ shear
+        centre_s = origin + cs
+        # subject points to template points: p_t = lin (p_s - centre_s) + ct + t
+        off = ct + rng.uniform(-15.0, 15.0, size=3) - lin @ centre_s
+        # a smooth displacement on the subject grid: components on a grid 4x coarser, upsampled
+        cd = tuple(int(x) for x in np.maximum(4, np.ceil(d / 4.0)))
+        comps = [_gaussian(rng.standard_normal(cd[::-1]), 3.0) for _ in range(3)]
+        u = np.stack(comps, -1)
+        u *= 6.0 / np.sqrt((u ** 2).sum(-1)).max()
+        cg = make_grid(cd, (4.0, 4.0, 4.0), tuple(origin + 1.5))
+        field = backend.resample_field(backend.upload_field(cg, u), sg)
+        A = make_affine(lin, off)
+        moving = [backend.warp_through_field(im, field, affine=A) for im in imgs]
+        inv = np.linalg.inv(lin)
+        initial = make_affine(inv, -inv @ off)
+        subjects.append((moving, initial))
+    return g, imgs, subjects

@@ -352,3 +352,63 @@ def syn_step(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image], moving
                             None if mu is None else mu.ctypes.data_as(C.c_void_p),
                             C.byref(rec)))
     return _records([rec], 1)[0], fu, mu
+
+
+@dataclass
+class BatchResult:
+    """The batching form's outcome: per subject its SynResult (None when it failed) and status,
+    and the autotuner's per-level choices with each level's device time."""
+    subjects: list
+    statuses: list
+    tuning: list
+    level_ms: list
+    device_bytes: int
+
+
+def run_syn_batch(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
+                  subjects: list, download: bool = True) -> BatchResult:
+    """fw_batch_syn_run: every subject registered to the one template `fixed` (device images, one
+    per channel) in lockstep; `subjects` is a list of (moving: [Image per channel], initial
+    affine or None). Each subject's fields are downloaded (AoS float32) unless download is False,
+    when the SynResult holds the device Fields instead."""
+    r = recipe.to_c()
+    B = len(subjects)
+    subj = (N.BatchSubject * B)()
+    for b, (moving, initial) in enumerate(subjects):
+        for c, im in enumerate(moving):
+            subj[b].moving[c] = im.handle
+        if initial is not None:
+            subj[b].initial = initial
+            subj[b].has_initial = 1
+    fp = (C.c_void_p * len(fixed))(*[im.handle for im in fixed])
+    warps = (C.c_void_p * B)()
+    invs = (C.c_void_p * B)()
+    cap = max(1, sum(recipe.iterations))
+    recs = (N.SynIteration * (cap * B))()
+    counts = (C.c_int64 * B)()
+    statuses = (C.c_int32 * B)()
+    rep = N.BatchReport()
+    check(lib().fw_batch_syn_run(backend.ctx, C.byref(r), fp, C.c_int32(B), subj, warps, invs,
+                                 recs, C.c_int64(cap), counts, statuses, C.byref(rep)))
+    last = level_grid(recipe, fixed[0].grid, r.levels - 1)
+    out = []
+    for b in range(B):
+        if statuses[b] != 0:
+            out.append(None)
+            continue
+        w, iw = Field(backend, C.c_void_p(warps[b])), Field(backend, C.c_void_p(invs[b]))
+        its = _records(recs[b * cap:(b + 1) * cap], counts[b])
+        if download:
+            out.append(SynResult(backend.download_field(w).astype(np.float32),
+                                 backend.download_field(iw).astype(np.float32), last, its))
+            w.free()
+            iw.free()
+        else:
+            out.append(SynResult(w, iw, last, its))
+    tuning = []
+    for lv in range(r.levels):
+        t = rep.tuning[lv]
+        tuning.append({k: (list(getattr(t, k)) if k == "grid_size" else getattr(t, k))
+                       for k, _ in N.BatchTuning._fields_})
+    return BatchResult(out, list(statuses), tuning, list(rep.level_ms[:r.levels]),
+                       int(rep.device_bytes))

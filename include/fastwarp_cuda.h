@@ -379,21 +379,22 @@ int fw_prepare_channels(fw_ctx* ctx, int32_t channels, const fw_image* const* fi
 int fw_mi_level_prepare(fw_ctx* ctx, const fw_grid* moving_grid, const double* moving,
                         const double* points, const uint32_t* fixed_bin, int64_t n,
                         const fw_mi_binning* binning, fw_mi_level** out);
-/* The same with the moving image already on the device (no upload). */
+/* The same with the moving image already on the device (no upload): the level reads it in
+ * place, so it must outlive the level. */
 int fw_mi_level_prepare_image(fw_ctx* ctx, const fw_image* moving, const double* points,
                               const uint32_t* fixed_bin, int64_t n,
                               const fw_mi_binning* binning, fw_mi_level** out);
-/* LinearMetric::value (optimizer.rs:61): -MI. */
 /* The level a linear stage prepares (linear.rs:474-492, 251-280, 940-945; sampling.rs:196-238)
  * from device images already at the level's smoothing: the regular sample set of `level_grid`
  * from `seed` (only the points inside `fixed_mask`, which may be NULL), the binning (fixed range at
  * the samples' nearest voxels, moving range over the whole moving image) and the kept points with
- * their trilinear fixed bins, then as fw_mi_level_prepare_image. Fails with the reference's
- * reason when Mattes MI is undefined on the samples. */
+ * their trilinear fixed bins, then as fw_mi_level_prepare_image (`moving` must outlive the
+ * level). Fails with the reference's reason when Mattes MI is undefined on the samples. */
 int fw_mi_level_prepare_regular(fw_ctx* ctx, const fw_grid* level_grid, const fw_image* fixed,
                                 const fw_image* moving, const fw_image* fixed_mask,
                                 float percentage, uint32_t seed, int32_t bins,
                                 fw_mi_level** out);
+/* LinearMetric::value (optimizer.rs:61): -MI. */
 int fw_mi_level_value(fw_mi_level* level, const fw_linear_transform* t, double* value);
 /* LinearMetric::value_and_derivative (optimizer.rs:62-64): -MI and +dMI/dtheta (6 or 12). */
 int fw_mi_level_value_and_derivative(fw_mi_level* level, const fw_linear_transform* t,
@@ -608,6 +609,57 @@ int fw_linear_chain_run_masked(fw_ctx* ctx, const fw_linear_recipe* rigid,
                                const fw_image* moving_raw, const fw_image* fixed,
                                const fw_image* moving, const fw_image* fixed_mask,
                                fw_linear_chain_result* out);
+
+/* ---- the batching form: many subjects to one template in one run ------------------------- */
+
+/* One subject of a batch: its moving channels (device images on the subject's own grid, one grid
+ * for all its channels) and its initial affine (the linear stages' result). */
+typedef struct fw_batch_subject {
+    const fw_image* moving[FW_MAX_CHANNELS];
+    fw_affine initial;
+    int32_t has_initial;
+} fw_batch_subject;
+
+/* The autotuner's choice for one level: z slices per tile of each tiled kernel family and the
+ * persistent grid of each (blocks per SM), the time spent tuning, and whether it came from the
+ * process-wide cache of earlier batches of the same shape. */
+typedef struct fw_batch_tuning {
+    int32_t level;
+    int64_t grid_size[3];
+    int32_t warp_zchunk, warp_blocks_per_sm;
+    int32_t compose_zchunk, compose_blocks_per_sm;
+    int32_t cc_zchunk, cc_blocks_per_sm;
+    int32_t measure_zchunk, measure_blocks_per_sm;
+    int32_t body_blocks_per_sm;
+    int32_t smooth_blocks_per_sm;
+    int32_t from_cache;
+    double tune_ms;
+} fw_batch_tuning;
+
+typedef struct fw_batch_report {
+    int32_t subjects;
+    int32_t levels;
+    fw_batch_tuning tuning[FW_MAX_LEVELS];
+    double level_ms[FW_MAX_LEVELS]; /* device time of each level's graph (CUDA events) */
+    uint64_t device_bytes;          /* device memory the batch held at its largest level */
+} fw_batch_report;
+
+/* No counterpart in the reference, whose nearest path registers several moving images to one
+ * fixed image as independent runs (register_atlases, crates/fastwarp-cli/src/engine.rs:1016-1072).
+ * The SyN stage (as fw_syn_run_device, syn.rs:776-986) of `subjects` subjects against ONE
+ * template (`fixed`, recipe->channels device images), in lockstep: every sub-step of an
+ * iteration is one persistent launch over a device-side work list of (subject, tile) items, each
+ * level one CUDA graph, the list shrinking as subjects converge; tile shapes and persistent grids
+ * come from an autotuner (`report->tuning`). Each subject's result equals its own
+ * fw_syn_run_device result up to last-bit rounding of the tiled reductions. CC channels only, the
+ * update field smoothed (variance > 0), no total-field smoothing, no masks; 1..=256 subjects.
+ * Outputs per subject b: warps[b] / inverse_warps[b] (NULL when the subject failed),
+ * records[b * cap ...] and counts[b] (nullable), statuses[b] (nullable: FW_OK or the subject's
+ * FW_ERR_*). The call fails only for invalid arguments or a device error. */
+int fw_batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* const* fixed,
+                     int32_t subjects, const fw_batch_subject* subject, fw_field** warps,
+                     fw_field** inverse_warps, fw_syn_iteration* records, int64_t cap,
+                     int64_t* counts, int32_t* statuses, fw_batch_report* report);
 
 /* ---- profiling (crates/fastwarp-gpu/src/profiler.rs:8-60: per-op device timestamps) ----- */
 

@@ -66,7 +66,8 @@ def test_every_mirrored_struct_has_the_library_layout_size():
              "fw_cg_trace": N.CgTrace, "fw_transform_elem": N.TransformElem,
              "fw_linear_recipe": N.LinearRecipe, "fw_linear_level_trace": N.LinearLevelTrace,
              "fw_linear_request": S.LinearRequest, "fw_linear_result": S.LinearResultC,
-             "fw_linear_chain_result": N.LinearChainResult}
+             "fw_linear_chain_result": N.LinearChainResult, "fw_batch_subject": N.BatchSubject,
+             "fw_batch_tuning": N.BatchTuning, "fw_batch_report": N.BatchReport}
     for name, cls in pairs.items():
         assert N.lib().fw_abi_struct_size(name.encode()) == C.sizeof(cls), name
     assert N.lib().fw_abi_struct_size(b"no such struct") == 0

@@ -109,8 +109,8 @@ def test_sampled_mi_at_the_config2_finest_level_matches_the_oracle(backend):
         assert abs(v - wv) <= 1e-5 * abs(wv)
         assert np.linalg.norm(d - wd) <= 5e-4 * np.linalg.norm(wd)
         assert level.num_valid() == wn
-    own = CudaLinearEngine(backend).prepare_level_regular(
-        g, backend.upload_image(g, fixed), backend.upload_image(mg, moving), 0.25, 1, 32)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(mg, moving)
+    own = CudaLinearEngine(backend).prepare_level_regular(g, fi, mi, 0.25, 1, 32)
     t0 = linear_transform(**cases[0])
     assert abs(own.value(t0) - level.value(t0)) <= 1e-12 * abs(level.value(t0))
     assert own.num_valid() == level.num_valid()
