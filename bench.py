@@ -72,6 +72,11 @@ def parse():
     p.add_argument("--reps", type=int, default=20)
     p.add_argument("--no-mi", action="store_true", help="skip the sampled Mattes MI leg")
     p.add_argument("--no-batch", action="store_true", help="skip the batching-form leg")
+    p.add_argument("--only", choices=["batch", "mi", "stream"], default=None,
+                   help="run one leg alone (profiling target): the batching form or the sampled "
+                        "Mattes MI with the linear chain")
+    p.add_argument("--subjects", type=int, default=48, help="subjects of the batching leg")
+    p.add_argument("--no-chain", action="store_true", help="MI leg without the linear chain")
     p.add_argument("--full-cpu", action="store_true",
                    help="with --impl reference: time one whole oracle registration")
     return p.parse_args()
@@ -104,6 +109,23 @@ def run_kernels_only(args, local):
         t = time_kernels(b, b.upload_image(g, fixed), b.upload_image(g, moving), args.reps)
     return {"kernels": {k: {"ms": round(v[0], 4), "gbs": round(v[1] / (v[0] / 1000) / 1e9, 1)}
                         for k, v in t.items()}, "shape": shape}
+
+
+def run_one_leg(args, rank, world, local):
+    from fastwarp_b200 import CudaBackend
+    b = CudaBackend(local)
+    if args.only == "batch":
+        out = {"batched": batch_leg(b, rank, args.subjects)}
+    elif args.only == "stream":
+        out = {"stream": stream_leg(b, rank)}
+    else:
+        from fastwarp_b200.phantoms import head_pair
+        g, fixed, mg, moving, initial = head_pair(SHAPE, seed=20_260_910 + 2 + rank)
+        fi, mi = b.upload_image(g, fixed), b.upload_image(mg, moving)
+        out = {"mattes_mi": mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world,
+                                   chain=not args.no_chain)}
+    b.close()
+    return out
 
 
 def recipe():
@@ -384,7 +406,7 @@ def run_ours(args, rank, world, local):
                       "timing": "wall clock, first submit to last result (host copies included)"}
     if not args.no_batch:
         log("batching form (config 4)")
-        out["batched"] = batch_leg(b, rank)
+        out["batched"] = batch_leg(b, rank, args.subjects)
     if not args.no_mi:
         log("sampled Mattes MI leg and linear chain")
         out["mattes_mi"] = mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world)
@@ -517,7 +539,7 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------------------------
 # the affine stage's sampled Mattes MI at the finest level, and the linear chain
 
-def mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world):
+def mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world, chain=True):
     """Times the sampled Mattes MI of config 2's finest level (25 % regular sampling, 32 bins)
     and the whole linear chain. Per pass: CUDA events on the engine stream, algorithmic bytes
     16 S + min(4 Nm, 32 S); through the host API: wall clock per evaluation (one read-back)."""
@@ -557,6 +579,8 @@ def mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world):
         level.value_and_derivative(tr)
     out["value_and_derivative_call_ms"] = round((time.perf_counter() - t0) / n * 1000, 4)
     level.free()
+    if not chain:
+        return out
     # the whole linear chain at the config-2 shape
     rigid = linear_recipe(iterations=(500, 250, 100), shrink_factors=(4, 2, 1),
                           smoothing_sigmas=(2.0, 1.0, 0.0))
@@ -567,17 +591,13 @@ def mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world):
     t0 = time.perf_counter()
     chain = run_linear_chain(b, rigid, affine, fi, mi, fi, mi)
     t_chain = time.perf_counter() - t0
-    dm, dt, dc = chain["total"]
-    corners = [np.array([g.origin[0] + i * (g.size[0] - 1) * g.spacing[0],
-                         g.origin[1] + j * (g.size[1] - 1) * g.spacing[1],
-                         g.origin[2] + k * (g.size[2] - 1) * g.spacing[2]])
-               for i in (0, 1) for j in (0, 1) for k in (0, 1)]
-    err = max(np.linalg.norm((dm @ (c - dc) + dc + dt) - (M @ c + np.array(initial.offset[:])))
-              for c in corners)
     out["linear_chain"] = {"seconds": round(t_chain, 3),
                            "rigid_samples": chain["rigid_samples"],
                            "affine_samples": chain["affine_samples"],
-                           "corner_error_vs_phantom_mm": round(float(err), 3),
+                           "rigid_iterations": chain["rigid_iterations"],
+                           "affine_iterations": chain["affine_iterations"],
+                           "rigid_best_mi": [round(v, 6) for v in chain["rigid_best"]],
+                           "affine_best_mi": [round(v, 6) for v in chain["affine_best"]],
                            "recipe": "CoM + rigid + affine, MI 32 bins 25 % regular, shrink "
                                      "4/2/1, sigma 2/1/0 vox, 500/250/100 iterations, 1e-6/10"}
     return out
@@ -675,6 +695,134 @@ def batch_leg(b, rank, n_subjects=48):
             "vs_alone": checks}
 
 
+class MemorySampler:
+    """Polls the device's used memory (cudaMemGetInfo through the library) every 50 ms."""
+
+    def __init__(self, device):
+        self.device = device
+        self.peak = 0
+        self.stop = threading.Event()
+        self.thread = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        import ctypes as C
+
+        from fastwarp_b200 import _native as N
+        free, total = C.c_uint64(), C.c_uint64()
+        while not self.stop.is_set():
+            if N.lib().fw_device_memory(self.device, C.byref(free), C.byref(total)) == 0:
+                self.peak = max(self.peak, total.value - free.value)
+            self.stop.wait(0.05)
+
+    def __enter__(self):
+        self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        self.thread.join()
+
+
+def stream_leg(b, rank, rates=(20, 100, 400), n=40, compress=360.0, slots=4, budget=170e9):
+    """Config 5: an open-loop request stream, Poisson arrivals at each nominal rate (requests per
+    hour), time-compressed by `compress` (one wall second stands for `compress` seconds), 70 %
+    single-channel SyN / 20 % affine-only Mattes MI fits / 10 % two-channel SyN, grid dims drawn
+    per axis from 160-240 at 1 mm, every request a seeded phantom pair kept on the device.
+    Admission by a 170 GB HBM budget. Each stream runs through the server with `slots` slots and
+    through one slot (sequential execution of the same stream, the same arrival times);
+    reported per rate: throughput, p50/p95/p99 latency (submit to result, wall seconds) and
+    peak HBM (admission estimates and measured device use)."""
+    import numpy as np
+
+    from fastwarp_b200 import SynRecipe, linear_transform
+    from fastwarp_b200.backend import linear_recipe
+    from fastwarp_b200.phantoms import BASE_SEED, stream_requests
+    from fastwarp_b200.serve import Server
+    reqs = stream_requests(b, n, seed=BASE_SEED + 5 + rank)
+
+    def syn_recipe(channels):
+        return SynRecipe(gradient_step=0.1, update_field_variance=3.0, total_field_variance=0.0,
+                         cc_radius=4, iterations=list(ITERATIONS), shrink_factors=list(SHRINK),
+                         smoothing_sigmas=list(SIGMAS), convergence_threshold=-1.0,
+                         convergence_window=10, channel_weights=[1.0 / channels] * channels)
+    rs = {"syn": syn_recipe(1), "syn2": syn_recipe(2)}
+    lr = linear_recipe(iterations=(500, 250, 100), shrink_factors=(4, 2, 1),
+                       smoothing_sigmas=(2.0, 1.0, 0.0))
+
+    def submit(srv, q):
+        if q["kind"] == "affine":
+            g = q["grid"]
+            c = tuple(g.origin[a] + 0.5 * (g.size[a] - 1) * g.spacing[a] for a in range(3))
+            start = linear_transform("affine", list(np.eye(3).ravel()) + [0.0] * 3, center=c)
+            return srv.submit_linear(lr, g, q["fixed"][0], g, q["moving"][0], start)
+        return srv.submit(rs[q["kind"]], q["grid"], q["fixed"], q["grid"], q["moving"],
+                          q["initial"], keep_on_device=True)
+
+    def wait(srv, q, t):
+        if q["kind"] == "affine":
+            o = srv.wait_linear(t)
+        else:
+            o = srv.wait(t)
+            Server.free_device_fields(o)
+        if o["status"] != 0:
+            raise RuntimeError(o["error"])
+        return o["queued_s"] + o["run_s"]
+
+    def run(k, arrivals):
+        with Server(b.device, budget_bytes=int(budget), slots=k) as srv:
+            for q in [next(x for x in reqs if x["kind"] == kd) for kd in ("syn", "affine", "syn2")
+                      if any(x["kind"] == kd for x in reqs)]:
+                wait(srv, q, submit(srv, q))  # warm-up: each kind once
+            sub = [None] * n
+            tickets = [None] * n
+
+            def feeder():
+                t0 = time.perf_counter()
+                for i, q in enumerate(reqs):
+                    dt = arrivals[i] - (time.perf_counter() - t0)
+                    if dt > 0:
+                        time.sleep(dt)
+                    sub[i] = time.perf_counter()
+                    tickets[i] = submit(srv, q)
+            with MemorySampler(b.device) as mem:
+                th = threading.Thread(target=feeder)
+                th.start()
+                lat = []
+                for i, q in enumerate(reqs):
+                    while tickets[i] is None:
+                        time.sleep(0.001)
+                    lat.append(wait(srv, q, tickets[i]))
+                th.join()
+            st = srv.stats()
+        span = max(s + l for s, l in zip(sub, lat)) - min(sub)
+        lat_sorted = sorted(lat)
+
+        def pct(p):
+            return lat_sorted[min(n - 1, int(round(p / 100.0 * (n - 1))))]
+        return {"throughput_per_hour_wall": round(n / span * 3600.0, 1),
+                "throughput_per_hour_nominal": round(n / span * 3600.0 / compress, 2),
+                "p50_s": round(pct(50), 3), "p95_s": round(pct(95), 3), "p99_s": round(pct(99), 3),
+                "span_s": round(span, 2), "peak_reserved_bytes": st["peak_reserved_bytes"],
+                "peak_device_bytes": mem.peak}
+    out = {"workload": f"{n} requests per rate, 70/20/10 SyN / affine-only / two-channel SyN, "
+                       "dims U(160-240) per axis, SyN CC r4 4/2/1 70/50/20, affine MI 32 bins "
+                       "25 % 4/2/1 500/250/100",
+           "compress": compress, "budget_bytes": int(budget), "slots": slots,
+           "kinds": {kd: sum(1 for q in reqs if q["kind"] == kd) for kd in ("syn", "affine", "syn2")},
+           "rates": {}}
+    rng = np.random.default_rng(20_260_910 + 55)
+    for rate in rates:
+        gaps = rng.exponential(3600.0 / (rate * compress), size=n)
+        arrivals = np.concatenate([[0.0], np.cumsum(gaps)[:-1]])
+        served = run(slots, arrivals)
+        seq = run(1, arrivals)
+        out["rates"][str(rate)] = {"served": served, "sequential": seq,
+                                   "served_over_sequential_throughput": round(
+                                       served["throughput_per_hour_wall"] /
+                                       seq["throughput_per_hour_wall"], 3)}
+    return out
+
+
 def mi_cpu_baseline(g, fixed, mg, moving, initial):
     """The oracle's sampled Mattes MI value and derivative on the same finest-level samples
     (the reference's MattesMi::evaluate restated, all host cores)."""
@@ -713,7 +861,9 @@ def main():
             print(json.dumps(out), flush=True)
         return
     rank, world, local = dist_init(args)
-    if args.kernels_only:
+    if args.only:
+        out = run_one_leg(args, rank, world, local)
+    elif args.kernels_only:
         out = run_kernels_only(args, local)
     else:
         out = run_ours(args, rank, world, local)

@@ -589,6 +589,10 @@ def run_linear_chain(backend: "CudaBackend", rigid: N.LinearRecipe, affine: N.Li
             "rigid": list(r.rigid.parameters[:6]), "affine": list(r.affine.parameters[:12]),
             "rigid_samples": [r.rigid_levels[k].samples for k in range(rigid.levels)],
             "affine_samples": [r.affine_levels[k].samples for k in range(affine.levels)],
+            "rigid_best": [r.rigid_levels[k].cg.best_value for k in range(rigid.levels)],
+            "affine_best": [r.affine_levels[k].cg.best_value for k in range(affine.levels)],
+            "rigid_iterations": [r.rigid_levels[k].cg.iterations for k in range(rigid.levels)],
+            "affine_iterations": [r.affine_levels[k].cg.iterations for k in range(affine.levels)],
             "total": (m3(r.total_matrix), np.array(r.total_translation[:]),
                       np.array(r.total_center[:]))}
 

@@ -103,6 +103,16 @@ __device__ __forceinline__ bool sample_value(const MiMap& mp, const float* __res
     return true;
 }
 
+// Copies of the histogram per block: lane l adds into copy l mod MI_REP, so one warp instruction
+// puts at most 32 / MI_REP lanes on any cell (neighbouring samples see nearly the same
+// intensities and would otherwise all hit one cell); each copy is padded by one cell so a cell's
+// copies lie on different shared-memory banks. Integer sums: the merged histogram is exact.
+constexpr int MI_REP = 8;
+
+size_t mi_hist_smem(int bins) {
+    return sizeof(unsigned long long) * MI_REP * (size_t)(bins * bins + bins + 1);
+}
+
 // Joint histogram of transform blockIdx.y over a chunk of samples per block.
 __global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict__ maps,
                                                         const float4* __restrict__ rec,
@@ -112,9 +122,11 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict_
     const MiMap& mp = maps[blockIdx.y];
     const int bins = mp.bins;
     const int cells = bins * bins + bins;
-    extern __shared__ unsigned long long sh[];
-    for (int s = threadIdx.x; s < cells; s += blockDim.x) sh[s] = 0ULL;
+    const int cstride = cells + 1;
+    extern __shared__ unsigned long long sh_all[];
+    for (int s = threadIdx.x; s < MI_REP * cstride; s += blockDim.x) sh_all[s] = 0ULL;
     __syncthreads();
+    unsigned long long* sh = sh_all + (threadIdx.x & (MI_REP - 1)) * cstride;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         float4 r = __ldg(rec + i);
@@ -132,8 +144,12 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict_
     }
     __syncthreads();
     unsigned long long* out = hist + (size_t)blockIdx.y * cells;
-    for (int s = threadIdx.x; s < cells; s += blockDim.x)
-        if (sh[s]) atomicAdd(&out[s], sh[s]);
+    for (int s = threadIdx.x; s < cells; s += blockDim.x) {
+        unsigned long long v = 0ULL;
+#pragma unroll
+        for (int k = 0; k < MI_REP; ++k) v += sh_all[k * cstride + s];
+        if (v) atomicAdd(&out[s], v);
+    }
 }
 
 // ComputeResults (metric/mi.rs:702-768) for histogram blockIdx.x: one thread per cell.
@@ -413,6 +429,13 @@ __device__ __forceinline__ bool dense_voxel(const DenseState& st, int bins, floa
     return true;
 }
 
+// Copies of the pair's two histograms per block (lane l into copy l mod MI_REP_DENSE).
+constexpr int MI_REP_DENSE = 4;
+
+size_t dense_hist_smem(int bins) {
+    return sizeof(unsigned long long) * MI_REP_DENSE * (size_t)(2 * (bins * bins + bins) + 1);
+}
+
 // Both joint histograms: [direction][bins*bins joint + bins fixed marginal] in 2^-32 fixed point.
 __global__ void __launch_bounds__(MI_THREADS) k_dense_hist(const float* __restrict__ f,
                                                            const float* __restrict__ m,
@@ -421,10 +444,12 @@ __global__ void __launch_bounds__(MI_THREADS) k_dense_hist(const float* __restri
                                                            long long n, int bins,
                                                            const DenseState* __restrict__ st,
                                                            unsigned long long* __restrict__ hist) {
-    extern __shared__ unsigned long long sh[];
+    extern __shared__ unsigned long long sh_all[];
     const int nc = bins * bins, cells = nc + bins;
-    for (int s = threadIdx.x; s < 2 * cells; s += blockDim.x) sh[s] = 0ULL;
+    const int cstride = 2 * cells + 1;  // copies as in k_mi_hist, padded onto different banks
+    for (int s = threadIdx.x; s < MI_REP_DENSE * cstride; s += blockDim.x) sh_all[s] = 0ULL;
     __syncthreads();
+    unsigned long long* sh = sh_all + (threadIdx.x & (MI_REP_DENSE - 1)) * cstride;
     const DenseState S = *st;
     if (S.status == 0) {
         for (long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x; l < n;
@@ -447,8 +472,12 @@ __global__ void __launch_bounds__(MI_THREADS) k_dense_hist(const float* __restri
         }
     }
     __syncthreads();
-    for (int s = threadIdx.x; s < 2 * cells; s += blockDim.x)
-        if (sh[s]) atomicAdd(&hist[s], sh[s]);
+    for (int s = threadIdx.x; s < 2 * cells; s += blockDim.x) {
+        unsigned long long v = 0ULL;
+#pragma unroll
+        for (int k = 0; k < MI_REP_DENSE; ++k) v += sh_all[k * cstride + s];
+        if (v) atomicAdd(&hist[s], v);
+    }
 }
 
 struct DenseArgs {
@@ -650,6 +679,25 @@ MiMap make_map(const fw_mi_level* L, const fw_linear_transform* t) {
     return mp;
 }
 
+// The histogram kernel's shared memory can exceed the 48 KB default.
+int hist_launch_setup(fw_ctx* ctx, size_t smem) {
+    (void)ctx;
+    FW_CUDA(cudaFuncSetAttribute(k_mi_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return 0;
+}
+
+// One wave of resident histogram blocks (each merges its copies into the global histogram once).
+unsigned int hist_blocks(const fw_mi_level* L, size_t smem) {
+    int occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mi_hist, MI_THREADS, smem) != cudaSuccess ||
+        occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+    }
+    const long long want = (L->n + MI_THREADS - 1) / MI_THREADS;
+    return (unsigned int)std::max<long long>(1, std::min<long long>(want, (long long)occ * L->ctx->num_sms));
+}
+
 int hist_and_finish(fw_mi_level* L, const fw_linear_transform* ts, int count, bool want_ratio) {
     fw_ctx* ctx = L->ctx;
     const int bins = L->binning.bins;
@@ -662,8 +710,9 @@ int hist_and_finish(fw_mi_level* L, const fw_linear_transform* ts, int count, bo
     FW_CUDA(cudaMemcpyAsync(d_maps, maps.data(), sizeof(MiMap) * count, cudaMemcpyHostToDevice,
                             ctx->stream));
     FW_CUDA(cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells * count, ctx->stream));
-    size_t sh = sizeof(unsigned long long) * cells;
-    dim3 grid(L->blocks, count);
+    const size_t sh = mi_hist_smem(bins);
+    FW_TRY(hist_launch_setup(ctx, sh));
+    dim3 grid(hist_blocks(L, sh), count);
     k_mi_hist<<<grid, MI_THREADS, sh, ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d, L->d_hist);
     FW_TRY(check_launch(ctx, "k_mi_hist"));
     k_mi_finish<<<count, 1024, 0, ctx->stream>>>(L->d_hist, bins, L->binning.moving_bin_size,
@@ -851,8 +900,10 @@ int fw_mi_level_time(fw_mi_level* L, const fw_linear_transform* t, int32_t reps,
             if (kind == 0) {
                 FW_CUDA(cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells,
                                         ctx->stream));
-                k_mi_hist<<<dim3(L->blocks, 1), MI_THREADS, sizeof(unsigned long long) * cells,
-                            ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d, L->d_hist);
+                const size_t sh = mi_hist_smem(bins);
+                FW_TRY(hist_launch_setup(ctx, sh));
+                k_mi_hist<<<dim3(hist_blocks(L, sh), 1), MI_THREADS, sh, ctx->stream>>>(
+                    d_maps, L->d_rec, L->n, L->moving->d, L->d_hist);
                 return check_launch(ctx, "k_mi_hist");
             }
             if (kind == 1) {
@@ -1027,7 +1078,8 @@ int enqueue_dense_mi_pair(fw_ctx* ctx, const fw_image* f, const fw_image* m, con
     FW_TRY(check_launch(ctx, "k_dense_range"));
     k_dense_setup<<<1, 1, 0, ctx->stream>>>(sc->st, bins);
     FW_TRY(check_launch(ctx, "k_dense_setup"));
-    const size_t sh = 2 * sizeof(unsigned long long) * ((size_t)bins * bins + bins);
+    const size_t sh = dense_hist_smem(bins);
+    FW_CUDA(cudaFuncSetAttribute(k_dense_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
     k_dense_hist<<<blocks, MI_THREADS, sh, ctx->stream>>>(f->d, m->d, fmp, mmp, n, bins, sc->st,
                                                           sc->hist);
     FW_TRY(check_launch(ctx, "k_dense_hist"));

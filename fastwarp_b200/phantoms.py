@@ -190,3 +190,61 @@ def batch_subjects(backend, n, template_shape=(193, 229, 193), dims=(160, 240),
         initial = make_affine(inv, -inv @ off)
         subjects.append((moving, initial))
     return g, imgs, subjects
+
+
+def _random_linear(rng):
+    """Config 2's random linear part: rigid (<= 10 deg per axis) then affine (scale 0.9-1.1,
+    shear <= 0.05)."""
+    rot = _rot(*np.deg2rad(rng.uniform(-10.0, 10.0, size=3)))
+    scale = np.diag(rng.uniform(0.9, 1.1, size=3))
+    shear = np.eye(3)
+    shear[0, 1], shear[0, 2], shear[1, 2] = rng.uniform(-0.05, 0.05, size=3)
+    return rot @ scale @ shear
+
+
+def _device_field(backend, rng, grid, d, origin, max_mm=6.0):
+    """A smooth displacement (<= max_mm) on `grid`: components on a grid 4x coarser, upsampled."""
+    cd = tuple(int(x) for x in np.maximum(4, np.ceil(np.asarray(d) / 4.0)))
+    u = np.stack([_gaussian(rng.standard_normal(cd[::-1]), 3.0) for _ in range(3)], -1)
+    u *= max_mm / np.sqrt((u ** 2).sum(-1)).max()
+    cg = make_grid(cd, (4.0, 4.0, 4.0), tuple(np.asarray(origin) + 1.5))
+    return backend.resample_field(backend.upload_field(cg, u), grid)
+
+
+def stream_requests(backend, n, mix=(0.7, 0.2, 0.1), dims=(160, 240), template_shape=(193, 229, 193),
+                    seed: int = BASE_SEED + 5):
+    """Config 5's requests on the device: `n` seeded phantom pairs, each on its own 1 mm grid of
+    dims drawn uniformly per axis from `dims`; the kind is drawn from `mix` over ("syn" single
+    channel, "affine" an affine-only Mattes MI fit, "syn2" two channels). As in config 2 the fixed
+    image is the head phantom (placed on the request's grid with a shift of up to 5 mm) and the
+    moving image the fixed image under a random rigid + affine map and a smooth displacement
+    (<= 6 mm), on the same grid; the linear part is the SyN requests' initial transform. Returns
+    dicts: kind, grid, fixed / moving ([device image per channel]), initial (affine, fixed
+    points to moving points)."""
+    rng = np.random.default_rng(seed)
+    t1 = head_phantom(template_shape, seed)
+    tg = make_grid(template_shape)
+    tmpl = [backend.upload_image(tg, t1), backend.upload_image(tg, t2_like(t1))]
+    ct = (np.array(template_shape, float) - 1.0) / 2.0
+    kinds = ("syn", "affine", "syn2")
+    out = []
+    for _ in range(n):
+        kind = kinds[int(rng.choice(3, p=np.asarray(mix) / np.sum(mix)))]
+        d = np.array([int(rng.integers(dims[0], dims[1] + 1)) for _ in range(3)])
+        cs = (d - 1.0) / 2.0
+        origin = ct - cs
+        g = make_grid(tuple(int(x) for x in d), (1.0, 1.0, 1.0), tuple(origin))
+        zero = backend.zero_field(g)
+        shift = make_affine(np.eye(3), rng.uniform(-5.0, 5.0, size=3))
+        chans = 2 if kind == "syn2" else 1
+        fixed = [backend.warp_through_field(tmpl[c], zero, affine=shift) for c in range(chans)]
+        lin = _random_linear(rng)
+        centre = origin + cs
+        off = centre + rng.uniform(-15.0, 15.0, size=3) - lin @ centre
+        u = _device_field(backend, rng, g, d, origin)
+        # moving(y) = fixed(A(y + u(y))): A maps moving points to fixed points
+        moving = [backend.warp_through_field(f, u, affine=make_affine(lin, off)) for f in fixed]
+        inv = np.linalg.inv(lin)
+        out.append({"kind": kind, "grid": g, "fixed": fixed, "moving": moving,
+                    "initial": make_affine(inv, -inv @ off)})
+    return out

@@ -1,0 +1,177 @@
+"""Config 3 as a stated precision study: the float32 engine against the f64 oracle at 0.5 mm on
+the full 385 x 457 x 385 head phantom (67.7 M voxels).
+
+Every figure is written to a machine-readable record (FASTWARP_PRECISION_OUT, default
+precision_config3.json in the working directory) as well as checked:
+
+  - one SyN CC step from a deformed state: CC value relative error, both update fields' max and
+    RMS error in voxels (bars 1e-5 and 1e-4 voxel);
+  - one sampled Mattes MI value and gradient (25 % regular sampling, 32 bins, about 17 M samples)
+    at the phantom's own affine map: value and gradient relative errors (bars 1e-5, 5e-4);
+  - a short affine stage at shrink 2/1 (3 and 2 conjugate-gradient iterations): the optimised
+    affine matrix and translation against the oracle's (bar 0.05 mm at the grid corners);
+  - with FASTWARP_PRECISION_FULL=1 (about seven minutes of oracle time on the host cores): the
+    full three-level SyN registration (40/30/10 iterations, CC r4) against the oracle's, field
+    RMS in mm and relative final CC (bars 0.05 mm and 1e-4).
+
+Where the engine keeps float64: the CC window sums (products of float32 voxels are exact in
+float64, so sum f^2 - (sum f)^2 / n keeps full precision where the image is flat and bright), every
+volume reduction, the MI normalisation and entropy, and the index maps. The record states each
+error beside its bar.
+"""
+import json
+import os
+import time
+
+import numpy as np
+import pytest
+
+import oracle as O
+from fastwarp_b200 import (CudaLinearEngine, SynRecipe, linear_transform, make_grid,
+                           run_syn_device, syn_step)
+from fastwarp_b200.backend import grid_corners, linear_recipe, run_linear_stage
+
+pytestmark = pytest.mark.gpu
+
+RECORD = {}
+
+
+def record(key, value):
+    RECORD[key] = value
+    path = os.environ.get("FASTWARP_PRECISION_OUT", "precision_config3.json")
+    with open(path, "w") as fh:
+        json.dump({"config": "config 3: head phantom 385x457x385 at 0.5 mm, float32 engine vs "
+                             "the f64 oracle", **RECORD}, fh, indent=1, sort_keys=True)
+
+
+@pytest.fixture(scope="module")
+def pair():
+    from test_gpu_config3 import phantom_pair
+    return phantom_pair()
+
+
+def ogrid(g):
+    return O.make_grid(tuple(g.size), tuple(g.spacing), tuple(g.origin),
+                       np.array(g.direction[:]).reshape(3, 3))
+
+
+def oaffine(a):
+    return O.make_affine(np.array(a.matrix[:]).reshape(3, 3), tuple(a.offset[:]))
+
+
+def test_one_full_size_cc_step_error(backend, pair):
+    g, fixed, moving, initial = pair
+    sp = g.spacing[0]
+    r = SynRecipe(gradient_step=0.1, update_field_variance=3.0, cc_radius=4, iterations=[1],
+                  shrink_factors=[1], smoothing_sigmas=[0.0], convergence_threshold=-1.0)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    state = {k: backend.zero_field(g) for k in ("f2m", "f2m_inv", "m2m", "m2m_inv")}
+    for _ in range(3):
+        syn_step(backend, r, [fi], [mi], initial, state, want_updates=False)
+    ostate = {k: backend.download_field(v) for k, v in state.items()}
+    rec, fu, mu = syn_step(backend, r, [fi], [mi], initial, state)
+    t0 = time.perf_counter()
+    orec, ofu, omu = O.syn_step(
+        O.syn_recipe(0.1, 3.0, 0.0, 4, (1,), (1,), (0.0,), False, -1.0, 10, (1.0,)),
+        ogrid(g), ogrid(g), [fixed.astype(np.float64)], ogrid(g), [moving.astype(np.float64)],
+        oaffine(initial), ostate)
+    t_oracle = time.perf_counter() - t0
+    cc_rel = abs(rec["energy"] - orec.energy) / abs(orec.energy)
+    ef, em = np.sqrt(((fu - ofu) ** 2).sum(-1)) / sp, np.sqrt(((mu - omu) ** 2).sum(-1)) / sp
+    out = {"cc_value": rec["energy"], "cc_value_oracle": orec.energy, "cc_value_rel_error": cc_rel,
+           "fixed_update_max_error_voxels": float(ef.max()),
+           "fixed_update_rms_error_voxels": float(np.sqrt((ef ** 2).mean())),
+           "moving_update_max_error_voxels": float(em.max()),
+           "moving_update_rms_error_voxels": float(np.sqrt((em ** 2).mean())),
+           "update_max_voxels": float(max(np.abs(ofu).max(), np.abs(omu).max()) / sp),
+           "bars": {"cc_value_rel": 1e-5, "update_max_voxels": 1e-4},
+           "oracle_seconds": round(t_oracle, 1)}
+    record("syn_cc_step", out)
+    assert cc_rel <= 1e-5
+    assert ef.max() <= 1e-4 and em.max() <= 1e-4
+
+
+def test_one_full_size_mattes_gradient_error(backend, pair):
+    g, fixed, moving, initial = pair
+    og = ogrid(g)
+    f64, m64 = fixed.astype(np.float64), moving.astype(np.float64)
+    pts = O.sample_points_regular(og, 0.25, 1)
+    kept, fbin, b = O.prepare_samples(og, f64, og, m64, pts, 32)
+    level = CudaLinearEngine(backend).prepare_level(g, m64, kept, fbin, b)
+    center = tuple(0.5 * (g.size[a] - 1) * g.spacing[a] for a in range(3))
+    M = np.array(initial.matrix[:]).reshape(3, 3)
+    t = np.array(initial.offset[:]) - np.array(center) + M @ np.array(center)
+    kw = dict(kind="affine", parameters=list(M.ravel()) + list(t), center=center)
+    v, d = level.value_and_derivative(linear_transform(**kw))
+    wv, wd, wn, _ = O.mi_evaluate(b, og, m64, kept, fbin, O.linear_transform(**kw))
+    out = {"samples": int(len(fbin)), "valid": int(wn), "mi_value": v, "mi_value_oracle": wv,
+           "mi_value_rel_error": abs(v - wv) / abs(wv),
+           "gradient_rel_l2_error": float(np.linalg.norm(d - wd) / np.linalg.norm(wd)),
+           "gradient_max_abs_error": float(np.abs(d - wd).max()),
+           "bars": {"mi_value_rel": 1e-5, "gradient_rel_l2": 5e-4}}
+    record("mattes_mi_gradient", out)
+    assert level.num_valid() == wn
+    assert out["mi_value_rel_error"] <= 1e-5 and out["gradient_rel_l2_error"] <= 5e-4
+
+
+def test_a_short_full_size_affine_stage_matrix_error(backend, pair):
+    """Two levels (shrink 2 and 1, 3 and 2 iterations) of the affine stage from the identity: the
+    optimised matrix, translation and corner positions against the oracle's same stage."""
+    from test_gpu_linear_stage import oracle_stage
+    g, fixed, moving, initial = pair
+    center = tuple(0.5 * (g.size[a] - 1) * g.spacing[a] for a in range(3))
+    start = list(np.eye(3).ravel()) + [0.0] * 3
+    its, shrink, sigmas = (3, 2), (2, 1), (1.0, 0.0)
+    r = linear_recipe(iterations=its, shrink_factors=shrink, smoothing_sigmas=sigmas)
+    tr, levels = run_linear_stage(backend, r, backend.upload_image(g, fixed),
+                                  backend.upload_image(g, moving),
+                                  linear_transform("affine", start, center=center))
+    ot, olevels = oracle_stage(g, fixed, moving, "affine", start, center, its, shrink, sigmas)
+    Md = np.array(tr.parameters[:9]).reshape(3, 3)
+    Mo = np.array(ot.parameters[:9]).reshape(3, 3)
+    td, to = np.array(tr.parameters[9:12]), np.array(ot.parameters[9:12])
+    c = np.array(center)
+    shift = max(np.linalg.norm((Md - Mo) @ (p - c) + (td - to)) for p in grid_corners(g))
+    out = {"matrix_max_abs_error": float(np.abs(Md - Mo).max()),
+           "translation_max_abs_error_mm": float(np.abs(td - to).max()),
+           "corner_shift_mm": float(shift),
+           "best_mi": [lv["best_value"] for lv in levels],
+           "best_mi_oracle": [min(ol["values"]) for ol in olevels],
+           "bars": {"corner_shift_mm": 0.05}}
+    record("affine_stage", out)
+    assert shift < 0.05
+
+
+@pytest.mark.skipif(os.environ.get("FASTWARP_PRECISION_FULL") != "1",
+                    reason="the oracle's full 0.5 mm registration takes about seven minutes: "
+                           "set FASTWARP_PRECISION_FULL=1")
+def test_the_full_three_level_registration_error(backend, pair):
+    g, fixed, moving, initial = pair
+    r = SynRecipe(gradient_step=0.1, update_field_variance=3.0, total_field_variance=0.0,
+                  cc_radius=4, iterations=[40, 30, 10], shrink_factors=[4, 2, 1],
+                  smoothing_sigmas=[2.0, 1.0, 0.0], convergence_threshold=-1.0,
+                  convergence_window=10)
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    t0 = time.perf_counter()
+    w, iw, recs = run_syn_device(backend, r, [fi], [mi], initial)
+    backend.synchronize()
+    t_gpu = time.perf_counter() - t0
+    wd, iwd = backend.download_field(w), backend.download_field(iw)
+    orec = O.syn_recipe(0.1, 3.0, 0.0, 4, (40, 30, 10), (4, 2, 1), (2.0, 1.0, 0.0), False, -1.0,
+                        10, (1.0,))
+    t0 = time.perf_counter()
+    ow, oinv, orecs, _ = O.syn_run(orec, ogrid(g), [fixed], ogrid(g), [moving], oaffine(initial))
+    t_oracle = time.perf_counter() - t0
+    rms = float(np.sqrt(((wd - ow) ** 2).sum(-1).mean()))
+    rms_inv = float(np.sqrt(((iwd - oinv) ** 2).sum(-1).mean()))
+    e, e0 = recs[-1]["energy"], orecs[-1].energy
+    out = {"iterations": len(recs), "field_rms_mm": rms, "inverse_field_rms_mm": rms_inv,
+           "field_max_abs_mm": float(np.abs(wd - ow).max()),
+           "final_cc": e, "final_cc_oracle": e0, "final_cc_rel_error": abs(e - e0) / abs(e0),
+           "gpu_seconds": round(t_gpu, 3), "oracle_seconds": round(t_oracle, 1),
+           "oracle_cores": O.num_threads(),
+           "bars": {"field_rms_mm": 0.05, "final_cc_rel": 1e-4}}
+    record("full_registration", out)
+    assert len(recs) == len(orecs) == 80
+    assert rms <= 0.05 and rms_inv <= 0.05
+    assert out["final_cc_rel_error"] <= 1e-4

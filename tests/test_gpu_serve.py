@@ -200,3 +200,67 @@ def test_the_context_cancel_flag_fails_a_run_until_cleared(pairs, backend):
         backend.request_cancel(False)
     res = run_syn(backend, r, g, [f], g, [m])
     assert len(res.iterations) == 10
+
+
+def test_each_result_is_the_same_alone_and_in_an_open_loop_stream(backend):
+    """Config 5's form in miniature: requests of the three kinds (single-channel SyN, affine-only
+    Mattes MI fit, two-channel SyN) on their own grids, generated on the device, arrive by a
+    seeded Poisson process while earlier ones run, through a 3-slot server under an HBM budget.
+    Every SyN result is bit-identical, and every affine fit identical, to the same request served
+    alone."""
+    import threading
+
+    from fastwarp_b200 import linear_transform
+    from fastwarp_b200.backend import linear_recipe
+    from fastwarp_b200.phantoms import stream_requests
+    reqs = stream_requests(backend, 7, mix=(0.4, 0.3, 0.3), dims=(36, 48),
+                           template_shape=(44, 48, 40), seed=5151)
+    assert {q["kind"] for q in reqs} == {"syn", "affine", "syn2"}
+    syn = {"syn": small_recipe(),
+           "syn2": SynRecipe(gradient_step=0.25, update_field_variance=3.0, cc_radius=2,
+                             iterations=[4, 3], shrink_factors=[2, 1], smoothing_sigmas=[1.0, 0.0],
+                             convergence_threshold=-1.0, channel_weights=[0.5, 0.5])}
+    lr = linear_recipe(iterations=(8, 6), shrink_factors=(2, 1), smoothing_sigmas=(1.0, 0.0))
+
+    def submit(s, q):
+        if q["kind"] == "affine":
+            g = q["grid"]
+            c = tuple(g.origin[a] + 0.5 * (g.size[a] - 1) * g.spacing[a] for a in range(3))
+            start = linear_transform("affine", list(np.eye(3).ravel()) + [0.0] * 3, center=c)
+            return s.submit_linear(lr, g, q["fixed"][0], g, q["moving"][0], start)
+        return s.submit(syn[q["kind"]], q["grid"], q["fixed"], q["grid"], q["moving"],
+                        q["initial"])
+
+    def wait(s, q, t):
+        o = s.wait_linear(t) if q["kind"] == "affine" else s.wait(t)
+        assert o["status"] == 0, o["error"]
+        return o
+
+    with Server(0, slots=1) as s:
+        alone = [wait(s, q, submit(s, q)) for q in reqs]
+    rng = np.random.default_rng(77)
+    gaps = rng.exponential(0.02, size=len(reqs))
+    with Server(0, budget_bytes=40 << 30, slots=3) as s:
+        tickets = [None] * len(reqs)
+
+        def feeder():
+            for i, q in enumerate(reqs):
+                time.sleep(gaps[i])
+                tickets[i] = submit(s, q)
+        th = threading.Thread(target=feeder)
+        th.start()
+        streamed = []
+        for i, q in enumerate(reqs):
+            while tickets[i] is None:
+                time.sleep(0.001)
+            streamed.append(wait(s, q, tickets[i]))
+        th.join()
+        st = s.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    for q, a, b in zip(reqs, alone, streamed):
+        if q["kind"] == "affine":
+            assert a["parameters"] == b["parameters"]
+        else:
+            assert np.array_equal(a["warp"], b["warp"])
+            assert np.array_equal(a["inverse_warp"], b["inverse_warp"])
+            assert a["final_energy"] == b["final_energy"]
