@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <atomic>
 #include <cstring>
 
 #include "fw_internal.cuh"
@@ -79,9 +80,57 @@ struct Layout {
 #define FW_CC_MIN_BLOCKS 3
 #endif
 
+// The window sums' arithmetic. SumF64 (the default): float64, in which the products of float32
+// voxels are exact. SumC32: compensated float32, a (hi, lo) float pair per sum -- products split
+// exactly by an fma (TwoProduct), additions by Knuth's TwoSum with the rounding errors gathered
+// in lo and a Fast2Sum renormalisation; every operation is an explicitly rounded intrinsic, so
+// the compiler cannot fuse a product into a neighbouring addition. Both take 8 bytes a sum in
+// shared memory.
+struct SumF64 {
+    using T = double;
+    __device__ static __forceinline__ T zero() { return 0.0; }
+    __device__ static __forceinline__ T diff(float a, float b) { return (double)a - (double)b; }
+    __device__ static __forceinline__ T prod_diff(float a, float b, float c, float d) {
+        const double x = a, y = b, z = c, w = d;
+        return x * y - z * w;
+    }
+    __device__ static __forceinline__ T add(T a, T b) { return a + b; }
+    __device__ static __forceinline__ double value(T a) { return a; }
+};
+
+struct SumC32 {
+    using T = float2;  // x: hi, y: lo
+    __device__ static __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+        s = __fadd_rn(a, b);
+        const float bb = __fsub_rn(s, a);
+        e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+    }
+    __device__ static __forceinline__ T zero() { return make_float2(0.0f, 0.0f); }
+    __device__ static __forceinline__ T diff(float a, float b) {
+        float s, e;
+        two_sum(a, -b, s, e);
+        return make_float2(s, e);
+    }
+    __device__ static __forceinline__ T prod_diff(float a, float b, float c, float d) {
+        const float p = __fmul_rn(a, b), pe = __fmaf_rn(a, b, -p);
+        const float q = __fmul_rn(c, d), qe = __fmaf_rn(c, d, -q);
+        float s, e;
+        two_sum(p, -q, s, e);
+        return make_float2(s, __fadd_rn(e, __fsub_rn(pe, qe)));
+    }
+    __device__ static __forceinline__ T add(T a, T b) {
+        float s, e;
+        two_sum(a.x, b.x, s, e);
+        const float lo = __fadd_rn(e, __fadd_rn(a.y, b.y));
+        const float hi = __fadd_rn(s, lo);
+        return make_float2(hi, __fsub_rn(lo, __fsub_rn(hi, s)));
+    }
+    __device__ static __forceinline__ double value(T a) { return (double)a.x + (double)a.y; }
+};
+
 // One tile (bx, by, bz) of the CC pair: writes the tile's derivative voxels and leaves the
 // thread's sums [cc, |dF|^2, |dM|^2, valid voxels] in acc_out.
-template <int R, int TY, bool MK>
+template <int R, int TY, bool MK, class Acc = SumF64>
 __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
                                         unsigned char* smem, const float* __restrict__ fimg,
                                         const float* __restrict__ mimg,
@@ -89,7 +138,9 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
                                         float* __restrict__ d_fixed, float* __restrict__ d_moving,
                                         int want_norms, double acc_out[4]) {
     using L = Layout<R, TY, MK>;
-    double* xs = reinterpret_cast<double*>(smem + L::zs1);
+    using T = typename Acc::T;
+    static_assert(sizeof(T) == sizeof(double), "a window sum takes 8 bytes");
+    T* xs = reinterpret_cast<T*>(smem + L::zs1);
     int* xc = reinterpret_cast<int*>(smem + L::zs1 + L::xs_bytes);
     float2* raw = reinterpret_cast<float2*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes);
 
@@ -111,7 +162,7 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
     // the thread's halo columns: offset inside a slice, -1 outside the image (sums stay zero)
     // and, for columns within one voxel of the tile, their slot in a raw slice (-1 otherwise)
     int coff[L::CPT], ridx[L::CPT];
-    double* zs = reinterpret_cast<double*>(smem);
+    T* zs = reinterpret_cast<T*>(smem);
     int* zc = reinterpret_cast<int*>(zs + 5 * L::HC);
 #pragma unroll
     for (int j = 0; j < L::CPT; ++j) {
@@ -127,7 +178,7 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
         }
         if (s < L::HC) {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) zs[q * L::HC + s] = 0.0;
+            for (int q = 0; q < 5; ++q) zs[q * L::HC + s] = Acc::zero();
             if constexpr (MK) zc[s] = 0;
         }
     }
@@ -162,15 +213,15 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
             float2 a = pin[j];
             if constexpr (MK)
                 if (!vin[j]) a = make_float2(0.0f, 0.0f);  // a masked-out voxel adds nothing
-            const double f = a.x, m = a.y, g = pout[j].x, n = pout[j].y;
+            const float f = a.x, m = a.y, g = pout[j].x, n = pout[j].y;
             const int s = tid + j * L::NT;
             if (s < L::HC) {
-                double* zq = zs + s;
-                zq[0] += f - g;
-                zq[L::HC] += m - n;
-                zq[2 * L::HC] += f * f - g * g;
-                zq[3 * L::HC] += m * m - n * n;
-                zq[4 * L::HC] += f * m - g * n;
+                T* zq = zs + s;
+                zq[0] = Acc::add(zq[0], Acc::diff(f, g));
+                zq[L::HC] = Acc::add(zq[L::HC], Acc::diff(m, n));
+                zq[2 * L::HC] = Acc::add(zq[2 * L::HC], Acc::prod_diff(f, f, g, g));
+                zq[3 * L::HC] = Acc::add(zq[3 * L::HC], Acc::prod_diff(m, m, n, n));
+                zq[4 * L::HC] = Acc::add(zq[4 * L::HC], Acc::prod_diff(f, m, g, n));
                 if constexpr (MK) zc[s] += (int)vin[j] - (int)vout[j];
             }
         }
@@ -185,19 +236,19 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
         for (int s = tid; s < L::HX * (TY / 2); s += L::NT) {
             const int rp = s / L::HX, hx = s - rp * L::HX;
             const int base = 2 * rp * L::HX + hx;
-            double* o = xs + 2 * rp * L::HX + hx;
+            T* o = xs + 2 * rp * L::HX + hx;
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                const double* col = zs + q * L::HC + base;
-                double c = 0.0, e = 0.0;  // two partial sums: half-length add chains
+                const T* col = zs + q * L::HC + base;
+                T c = Acc::zero(), e = Acc::zero();  // two partial sums: half-length add chains
 #pragma unroll
                 for (int t = 1; t <= 2 * R; t += 2) {
-                    c += col[t * L::HX];
-                    e += col[(t + 1) * L::HX];
+                    c = Acc::add(c, col[t * L::HX]);
+                    e = Acc::add(e, col[(t + 1) * L::HX]);
                 }
-                c += e;
-                o[q * TY * L::HX] = c + col[0];
-                o[q * TY * L::HX + L::HX] = c + col[(2 * R + 1) * L::HX];
+                c = Acc::add(c, e);
+                o[q * TY * L::HX] = Acc::add(c, col[0]);
+                o[q * TY * L::HX + L::HX] = Acc::add(c, col[(2 * R + 1) * L::HX]);
             }
             if constexpr (MK) {
                 const int* ccol = zc + base;
@@ -214,14 +265,14 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
         double S[5];
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            const double* row = xs + (q * TY + ty) * L::HX + tx;
-            double s = 0.0, s2 = 0.0;
+            const T* row = xs + (q * TY + ty) * L::HX + tx;
+            T s = Acc::zero(), s2 = Acc::zero();
 #pragma unroll
             for (int t = 0; t < 2 * R; t += 2) {
-                s += row[t];
-                s2 += row[t + 1];
+                s = Acc::add(s, row[t]);
+                s2 = Acc::add(s2, row[t + 1]);
             }
-            S[q] = s + s2 + row[2 * R];
+            S[q] = Acc::value(Acc::add(Acc::add(s, s2), row[2 * R]));
         }
 
         // ---- output voxel (x, y, z) ----
@@ -380,7 +431,7 @@ __device__ __forceinline__ void cc_finish(const double* partials, unsigned int n
     }
 }
 
-template <int R, int TY, bool MK>
+template <int R, int TY, bool MK, class Acc = SumF64>
 __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a, const float* __restrict__ fimg,
                                                      const float* __restrict__ mimg,
                                                      const float* __restrict__ vimg,
@@ -394,8 +445,8 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
     double* red = reinterpret_cast<double*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes +
                                             L::raw_bytes);
     double acc[4];
-    cc_tile<R, TY, MK>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, fimg, mimg, vimg, d_fixed,
-                       d_moving, want_norms, acc);
+    cc_tile<R, TY, MK, Acc>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, fimg, mimg, vimg,
+                            d_fixed, d_moving, want_norms, acc);
     // block partials, then the fixed-order last-block reduction
     const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
     const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
@@ -443,14 +494,14 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair_batch(
 // CTAs (measured at the 193 x 229 x 193 finest level, r = 4: 8 chunks 0.398 ms, 5 chunks 0.401 ms,
 // 2 chunks -- less than one wave -- 0.426 ms), with chunks no thinner than 2R slices, the filling
 // steps every chunk pays before its first output.
-template <int R, int TY, bool MK>
+template <int R, int TY, bool MK, class Acc = SumF64>
 int plan_launch(CcArgs& a, int num_sms, dim3* grid) {
     using L = Layout<R, TY, MK>;
-    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY, MK>,
+    FW_CUDA(cudaFuncSetAttribute(k_cc_pair<R, TY, MK, Acc>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes));
     static const int occ = [] {
         int o = 1;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_cc_pair<R, TY, MK>, L::NT,
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_cc_pair<R, TY, MK, Acc>, L::NT,
                                                           L::bytes) != cudaSuccess || o < 1)
             o = 1;
         return o;
@@ -467,36 +518,47 @@ int plan_launch(CcArgs& a, int num_sms, dim3* grid) {
     return 0;
 }
 
-template <int R, int TY, bool MK>
+template <int R, int TY, bool MK, class Acc = SumF64>
 int launch_r(fw_ctx* ctx, const CcArgs& a0, const float* f, const float* m, const float* v,
              float* df, float* dm, double* d_result, int want_norms) {
     using L = Layout<R, TY, MK>;
     CcArgs a = a0;
     dim3 grid;
-    FW_TRY((plan_launch<R, TY, MK>(a, ctx->num_sms, &grid)));
+    FW_TRY((plan_launch<R, TY, MK, Acc>(a, ctx->num_sms, &grid)));
     unsigned int nblocks = grid.x * grid.y * grid.z;
     FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)L::NP * nblocks + 16));
-    k_cc_pair<R, TY, MK><<<grid, L::NT, L::bytes, ctx->stream>>>(
+    k_cc_pair<R, TY, MK, Acc><<<grid, L::NT, L::bytes, ctx->stream>>>(
         a, f, m, v, df, dm, ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 1, d_result,
         want_norms);
     return check_launch(ctx, "k_cc_pair");
 }
 
+// The window-sum arithmetic of the unmasked single-image CC pair (FW_CC_SUMS_*), process-wide.
+std::atomic<int> g_cc_sums{FW_CC_SUMS_F64};
+
 template <bool MK>
 int launch_radius(fw_ctx* ctx, const CcArgs& a, int radius, const float* f, const float* m,
                   const float* v, float* df, float* dm, double* d_result, int want_norms) {
+    const bool c32 = !MK && g_cc_sums.load() == FW_CC_SUMS_C32;
+#define FW_CC_RADIUS(RR)                                                                         \
+    case RR:                                                                                    \
+        if constexpr (!MK)                                                                      \
+            if (c32) return launch_r<RR, 8, false, SumC32>(ctx, a, f, m, v, df, dm, d_result,   \
+                                                          want_norms);                          \
+        return launch_r<RR, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
     switch (radius) {
-        case 1: return launch_r<1, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 2: return launch_r<2, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 3: return launch_r<3, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 4: return launch_r<4, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 5: return launch_r<5, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 6: return launch_r<6, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 7: return launch_r<7, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
-        case 8: return launch_r<8, 8, MK>(ctx, a, f, m, v, df, dm, d_result, want_norms);
+        FW_CC_RADIUS(1)
+        FW_CC_RADIUS(2)
+        FW_CC_RADIUS(3)
+        FW_CC_RADIUS(4)
+        FW_CC_RADIUS(5)
+        FW_CC_RADIUS(6)
+        FW_CC_RADIUS(7)
+        FW_CC_RADIUS(8)
         default:
             return fail(FW_ERR_INVALID, "cc metric: radius must be in 1..=8 (BOX_RADIUS_MAX)");
     }
+#undef FW_CC_RADIUS
 }
 
 template <int R>
@@ -681,6 +743,13 @@ int fw_cc_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* f
                                                   double norms[2]) {
     FW_CHECK(valid && norms, "null argument");
     return cc_pair_common(ctx, fixed, moving, valid, radius, values, d_fixed, d_moving, norms);
+}
+
+int fw_set_cc_window_sums(int32_t kind) {
+    FW_CHECK(kind == FW_CC_SUMS_F64 || kind == FW_CC_SUMS_C32,
+             "cc metric: unknown window-sum arithmetic");
+    g_cc_sums.store(kind);
+    return 0;
 }
 
 int fw_cc_value_derivative(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving,

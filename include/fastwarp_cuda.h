@@ -281,6 +281,17 @@ int fw_mi_value_derivative_pair_masked_with_norms(fw_ctx* ctx, const fw_image* f
                                                   double values[2], fw_field** d_fixed,
                                                   fw_field** d_moving, double norms[2]);
 
+/* No counterpart in the reference (its CPU engine sums in float64, its GPU engine in plain
+ * float32 after subtracting each image's intensity mode). The arithmetic of the CC window sums
+ * (sum f, sum m, sum f^2, sum m^2, sum fm over each voxel's box) of the unmasked CC pair, for the
+ * whole process: FW_CC_SUMS_F64 (the default: float64, in which products of float32 voxels are
+ * exact) or FW_CC_SUMS_C32 (compensated float32: a float hi/lo pair per sum, TwoSum additions and
+ * exact products by fma). The per-voxel CC and its derivative are float64 either way; the
+ * masked pair, the batched kernels and the allocation-free entry point always use float64. */
+#define FW_CC_SUMS_F64 0
+#define FW_CC_SUMS_C32 1
+int fw_set_cc_window_sums(int32_t kind);
+
 /* No counterpart in the reference. The CC pair above for callers that cannot allocate device
  * memory: hosts whose own pool allocator owns the GPU's memory (a framework's caching allocator
  * that must see every byte, a server under a fixed HBM budget), plug-ins that run inside such a

@@ -14,10 +14,11 @@ precision_config3.json in the working directory) as well as checked:
     full three-level SyN registration (40/30/10 iterations, CC r4) against the oracle's, field
     RMS in mm and relative final CC (bars 0.05 mm and 1e-4).
 
-Where the engine keeps float64: the CC window sums (products of float32 voxels are exact in
-float64, so sum f^2 - (sum f)^2 / n keeps full precision where the image is flat and bright), every
-volume reduction, the MI normalisation and entropy, and the index maps. The record states each
-error beside its bar.
+Where the engine keeps float64: the CC window sums by default (products of float32 voxels are
+exact in float64, so sum f^2 - (sum f)^2 / n keeps full precision where the image is flat and
+bright; the compensated-float32 sums the north star names are built too and compared here, error
+and time), every volume reduction, the MI normalisation and entropy, and the index maps. The
+record states each error beside its bar.
 """
 import json
 import os
@@ -89,6 +90,43 @@ def test_one_full_size_cc_step_error(backend, pair):
     record("syn_cc_step", out)
     assert cc_rel <= 1e-5
     assert ef.max() <= 1e-4 and em.max() <= 1e-4
+
+
+def test_compensated_float32_window_sums_against_float64(backend, pair):
+    """The CC pair of the full-size fixed and moving images (r = 4) with the window sums in float64
+    (the default) and in compensated float32 (FW_CC_SUMS_C32, the arithmetic the north star
+    names), each against the oracle's f64 evaluation, and each variant's kernel time at this size
+    (CUDA events, fw_time_kernels). The default is the variant that is at least as accurate and
+    not slower."""
+    import ctypes as C
+
+    from fastwarp_b200 import _native as N
+    g, fixed, moving, initial = pair
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    t0 = time.perf_counter()
+    (ov, od1), (_, od2) = O.cc_pair(ogrid(g), fixed.astype(np.float64), moving.astype(np.float64), 4)
+    t_oracle = time.perf_counter() - t0
+    out = {"oracle_value": ov, "oracle_seconds": round(t_oracle, 1)}
+    scale = max(np.abs(od1).max(), np.abs(od2).max())
+    try:
+        for name, kind in (("float64", 0), ("compensated_float32", 1)):
+            N.check(N.lib().fw_set_cc_window_sums(C.c_int32(kind)))
+            ((v, d1), (_, d2)), _ = backend.cc_value_derivative_pair_with_norms(fi, mi, 4)
+            e1 = np.abs(backend.download_field(d1) - od1).max()
+            e2 = np.abs(backend.download_field(d2) - od2).max()
+            ms, by = (C.c_double * 7)(), (C.c_double * 7)()
+            N.check(N.lib().fw_time_kernels(backend.ctx, fi.handle, mi.handle, C.c_int32(4),
+                                            C.c_double(3.0), C.c_int32(10), ms, by))
+            out[name] = {"value_rel_error": abs(v - ov) / abs(ov),
+                         "derivative_max_error": float(max(e1, e2)),
+                         "derivative_max_error_rel_to_largest": float(max(e1, e2) / scale),
+                         "cc_pair_ms": round(ms[1], 4)}
+    finally:
+        N.check(N.lib().fw_set_cc_window_sums(C.c_int32(0)))
+    record("cc_window_sums", out)
+    for name in ("float64", "compensated_float32"):
+        assert out[name]["value_rel_error"] <= 1e-5
+        assert out[name]["derivative_max_error_rel_to_largest"] <= 1e-4
 
 
 def test_one_full_size_mattes_gradient_error(backend, pair):
