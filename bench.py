@@ -701,17 +701,22 @@ class MemorySampler:
     def __init__(self, device):
         self.device = device
         self.peak = 0
+        self.start = self.used()
         self.stop = threading.Event()
         self.thread = threading.Thread(target=self.run, daemon=True)
 
-    def run(self):
+    def used(self):
         import ctypes as C
 
         from fastwarp_b200 import _native as N
         free, total = C.c_uint64(), C.c_uint64()
+        if N.lib().fw_device_memory(self.device, C.byref(free), C.byref(total)) != 0:
+            return 0
+        return total.value - free.value
+
+    def run(self):
         while not self.stop.is_set():
-            if N.lib().fw_device_memory(self.device, C.byref(free), C.byref(total)) == 0:
-                self.peak = max(self.peak, total.value - free.value)
+            self.peak = max(self.peak, self.used())
             self.stop.wait(0.05)
 
     def __enter__(self):
@@ -803,13 +808,14 @@ def stream_leg(b, rank, rates=(20, 100, 400), n=40, compress=360.0, slots=4, bud
                 "throughput_per_hour_nominal": round(n / span * 3600.0 / compress, 2),
                 "p50_s": round(pct(50), 3), "p95_s": round(pct(95), 3), "p99_s": round(pct(99), 3),
                 "span_s": round(span, 2), "peak_reserved_bytes": st["peak_reserved_bytes"],
-                "peak_device_bytes": mem.peak}
+                "peak_device_bytes_above_start": max(0, mem.peak - mem.start)}
     out = {"workload": f"{n} requests per rate, 70/20/10 SyN / affine-only / two-channel SyN, "
                        "dims U(160-240) per axis, SyN CC r4 4/2/1 70/50/20, affine MI 32 bins "
                        "25 % 4/2/1 500/250/100",
            "compress": compress, "budget_bytes": int(budget), "slots": slots,
            "kinds": {kd: sum(1 for q in reqs if q["kind"] == kd) for kd in ("syn", "affine", "syn2")},
            "rates": {}}
+    b.release_idle_buffers()  # the generation's temporaries leave the device
     rng = np.random.default_rng(20_260_910 + 55)
     for rate in rates:
         gaps = rng.exponential(3600.0 / (rate * compress), size=n)

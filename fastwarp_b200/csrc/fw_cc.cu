@@ -182,6 +182,14 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
             if constexpr (MK) zc[s] = 0;
         }
     }
+    // Non-zero voxels of each halo column's z window, fixed in the low byte, moving in the next
+    // (exact integers, never negative). The reference forms every window sum directly from the
+    // window's voxels (metric/cc.rs:137-157), so a window where an image is zero sums to exactly
+    // zero and its CC takes the degenerate value; a running sum keeps a float64 rounding residue
+    // of what entered and left, so the sums of an image are reset to zero whenever its count is.
+    int nzc[L::CPT];
+#pragma unroll
+    for (int j = 0; j < L::CPT; ++j) nzc[j] = 0;
     // entering slice k and leaving slice k - 2R - 1 of the next step, in flight during a step
     float2 pin[L::CPT], pout[L::CPT];
     bool vin[L::CPT], vout[L::CPT];
@@ -217,11 +225,15 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
             const int s = tid + j * L::NT;
             if (s < L::HC) {
                 T* zq = zs + s;
-                zq[0] = Acc::add(zq[0], Acc::diff(f, g));
-                zq[L::HC] = Acc::add(zq[L::HC], Acc::diff(m, n));
-                zq[2 * L::HC] = Acc::add(zq[2 * L::HC], Acc::prod_diff(f, f, g, g));
-                zq[3 * L::HC] = Acc::add(zq[3 * L::HC], Acc::prod_diff(m, m, n, n));
-                zq[4 * L::HC] = Acc::add(zq[4 * L::HC], Acc::prod_diff(f, m, g, n));
+                nzc[j] += ((int)(f != 0.0f) - (int)(g != 0.0f)) +
+                          256 * ((int)(m != 0.0f) - (int)(n != 0.0f));
+                const bool fz = (nzc[j] & 255) == 0, mz = (nzc[j] >> 8) == 0;
+                zq[0] = fz ? Acc::zero() : Acc::add(zq[0], Acc::diff(f, g));
+                zq[L::HC] = mz ? Acc::zero() : Acc::add(zq[L::HC], Acc::diff(m, n));
+                zq[2 * L::HC] = fz ? Acc::zero() : Acc::add(zq[2 * L::HC], Acc::prod_diff(f, f, g, g));
+                zq[3 * L::HC] = mz ? Acc::zero() : Acc::add(zq[3 * L::HC], Acc::prod_diff(m, m, n, n));
+                zq[4 * L::HC] = (fz || mz) ? Acc::zero()
+                                           : Acc::add(zq[4 * L::HC], Acc::prod_diff(f, m, g, n));
                 if constexpr (MK) zc[s] += (int)vin[j] - (int)vout[j];
             }
         }
@@ -406,28 +418,23 @@ __device__ __forceinline__ bool cc_last(unsigned int* counter, unsigned int tota
     return last;
 }
 
-// The last block's reduction of `nblocks` partials, in block order (lane-strided, then a warp
-// sum): [value, |dF|^2, |dM|^2 (, valid voxels)] into result; the counter is reset.
+// The last block's reduction of `nblocks` partials in a fixed order (every thread of the block,
+// block_sum_fixed): [value, |dF|^2, |dM|^2 (, valid voxels)] into result; the counter is reset.
+// `red` is the block's shared reduction space (NT / 32 doubles at least).
 template <int NP, bool MK>
 __device__ __forceinline__ void cc_finish(const double* partials, unsigned int nblocks,
-                                          long long n, double* result, unsigned int* counter) {
-    const int tid = threadIdx.x;
-    if (tid < 32) {
-        double tot[4] = {0.0, 0.0, 0.0, 0.0};
+                                          long long n, double* result, unsigned int* counter,
+                                          double* red) {
+    double tot[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-        for (int q = 0; q < NP; ++q) {
-            double s = 0.0;
-            for (unsigned int b = tid; b < nblocks; b += 32) s += __ldcg(partials + (size_t)b * NP + q);
-            tot[q] = warp_sum_d(s);
-        }
-        if (tid == 0) {
-            // the mean over the valid voxels (all voxels without a mask); no valid voxel: NaN
-            result[0] = -tot[0] / (MK ? tot[3] : (double)n);
-            result[1] = tot[1];
-            result[2] = tot[2];
-            if constexpr (MK) result[3] = tot[3];
-            *counter = 0;
-        }
+    for (int q = 0; q < NP; ++q) tot[q] = block_sum_fixed(partials + q, nblocks, NP, red);
+    if (threadIdx.x == 0) {
+        // the mean over the valid voxels (all voxels without a mask); no valid voxel: NaN
+        result[0] = -tot[0] / (MK ? tot[3] : (double)n);
+        result[1] = tot[1];
+        result[2] = tot[2];
+        if constexpr (MK) result[3] = tot[3];
+        *counter = 0;
     }
 }
 
@@ -452,7 +459,7 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
     const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     cc_block_partials<L::NP, L::NT>(acc, red, partials + (size_t)bid * L::NP);
     if (!cc_last(counter, nblocks)) return;
-    cc_finish<L::NP, MK>(partials, nblocks, a.g.n, result, counter);
+    cc_finish<L::NP, MK>(partials, nblocks, a.g.n, result, counter, red);
 }
 
 // The CC pair of every active subject of a batch (unmasked): subject b's images at
@@ -485,7 +492,7 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair_batch(
         cc_block_partials<L::NP, L::NT>(acc, red, pb + (size_t)t * L::NP);
         if (cc_last(counter + b, (unsigned int)Lb.tiles))
             cc_finish<L::NP, false>(pb, (unsigned int)Lb.tiles, a.g.n,
-                                    result + (size_t)b * result_stride, counter + b);
+                                    result + (size_t)b * result_stride, counter + b, red);
         __syncthreads();  // the next tile rewrites the shared sums
     }
 }

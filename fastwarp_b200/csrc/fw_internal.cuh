@@ -425,6 +425,62 @@ __device__ __forceinline__ float warp_max_f(float v) {
     return v;
 }
 
+// The last block's fixed-order sum of `count` partials values[k * stride] (k = 0 .. count - 1),
+// shared by every thread of the block (all must call it): thread t adds k = t, t + blockDim.x, ...
+// in that order with four loads in flight, the warps add by shuffles and thread 0 adds the warps in
+// order, so the result (valid in thread 0) does not depend on scheduling. `red` is shared scratch
+// of at least blockDim.x / 32 doubles, free on entry.
+__device__ __forceinline__ double block_sum_fixed(const double* values, unsigned int count,
+                                                  unsigned int stride, double* red) {
+    const unsigned int B = blockDim.x;
+    double s = 0.0;
+    unsigned int k = threadIdx.x;
+    for (; k + 3 * B < count; k += 4 * B) {
+        const double a0 = __ldcg(values + (size_t)k * stride);
+        const double a1 = __ldcg(values + (size_t)(k + B) * stride);
+        const double a2 = __ldcg(values + (size_t)(k + 2 * B) * stride);
+        const double a3 = __ldcg(values + (size_t)(k + 3 * B) * stride);
+        s += a0;
+        s += a1;
+        s += a2;
+        s += a3;
+    }
+    for (; k < count; k += B) s += __ldcg(values + (size_t)k * stride);
+    s = warp_sum_d(s);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (unsigned int w = 0; w < (B >> 5); ++w) t += red[w];
+    __syncthreads();  // red is free again for the caller
+    return t;
+}
+
+// The largest of `count` non-negative float64 partials values[k * stride] with NaN winning,
+// shared by every thread of the block; valid in thread 0.
+__device__ __forceinline__ double block_max_nan(const double* values, unsigned int count,
+                                                unsigned int stride, double* red) {
+    double m = 0.0;
+    for (unsigned int k = threadIdx.x; k < count; k += blockDim.x) {
+        const double v = __ldcg(values + (size_t)k * stride);
+        m = (v > m || v != v) ? v : m;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (t > m || t != t) ? t : m;
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (unsigned int w = 0; w < (blockDim.x >> 5); ++w) r = (red[w] > r || red[w] != red[w]) ? red[w] : r;
+    __syncthreads();
+    return r;
+}
+
 // ---- internal kernels launched by the SyN driver -------------------------------------------
 
 // Device loop state of one inversion (fw_invert.cu).

@@ -75,23 +75,13 @@ __device__ void reduce_and_finish(double sum, float mx, double* __restrict__ par
     if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == nblocks - 1;
     __syncthreads();
     if (!last) return;
-    if (threadIdx.x < 32) {
-        double s = 0.0, m = 0.0;
-        for (unsigned int b = threadIdx.x; b < nblocks; b += 32) {
-            s += __ldcg(partials + 2 * b);
-            double mb = __ldcg(partials + 2 * b + 1);
-            m = (mb > m || mb != mb) ? mb : m;
-        }
-        s = warp_sum_d(s);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            double t = __shfl_xor_sync(0xffffffffu, m, o);
-            m = (t > m || t != t) ? t : m;
-        }
-        if (threadIdx.x == 0) {
-            finish(s, m);
-            *counter = 0;
-        }
+    // the whole last block reduces the partials in a fixed order
+    __shared__ double red[32];
+    const double s = block_sum_fixed(partials, nblocks, 2, red);
+    const double m = block_max_nan(partials + 1, nblocks, 2, red);
+    if (threadIdx.x == 0) {
+        finish(s, m);
+        *counter = 0;
     }
 }
 

@@ -306,10 +306,11 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_deriv(const MiMap* __restrict
     if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
     __syncthreads();
     if (!last) return;
-    if (threadIdx.x < 12) {
-        double s = 0.0;
-        for (unsigned int b = 0; b < gridDim.x; ++b) s += __ldcg(partials + (size_t)b * 12 + threadIdx.x);
-        mom[threadIdx.x] = s;
+    // the whole last block sums the partials of each moment in a fixed order
+    __shared__ double fin[MI_THREADS / 32];
+    for (int q = 0; q < 12; ++q) {
+        const double s = block_sum_fixed(partials + q, gridDim.x, 12, fin);
+        if (threadIdx.x == 0) mom[q] = s;
     }
     if (threadIdx.x == 0) *counter = 0;
 }
@@ -555,10 +556,10 @@ __global__ void __launch_bounds__(MI_THREADS) k_dense_deriv(
     if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
     __syncthreads();
     if (!last) return;
-    if (threadIdx.x < 2) {
-        double s = 0.0;
-        for (unsigned int b = 0; b < gridDim.x; ++b) s += __ldcg(partials + (size_t)b * 2 + threadIdx.x);
-        result[threadIdx.x] = s;
+    __shared__ double fin[MI_THREADS / 32];
+    for (int q = 0; q < 2; ++q) {
+        const double s = block_sum_fixed(partials + q, gridDim.x, 2, fin);
+        if (threadIdx.x == 0) result[q] = s;
     }
     if (threadIdx.x == 0) *counter = 0;
 }

@@ -118,6 +118,38 @@ def test_cc_pair_matches_in_both_directions(backend, name):
     assert rel(norms[1], np.sqrt((e2 ** 2).sum())) <= 1e-5
 
 
+@pytest.mark.parametrize("name", ["awkward_aligned", "awkward_oblique", "cube_r1"])
+@pytest.mark.parametrize("sums", [0, 1])
+def test_cc_pair_with_exactly_zero_regions_matches_the_oracle(backend, name, sums):
+    """Images that are exactly zero over whole regions (a zero-padded or skull-stripped
+    background): the reference sums every window directly (metric/cc.rs:137-157), so a window
+    where an image is zero sums to exactly zero and takes the degenerate local CC of 1; the
+    engine's running z sums must do the same. Both window-sum arithmetics (float64, compensated
+    float32) are checked; the zero regions cover a third of the volume, so a wrong degenerate
+    rule moves the value by several per cent."""
+    import ctypes as C
+    case = CASES[name]
+    og, g = grid_of(case), fgrid(case)
+    fimg, mimg = image(case), image(case, seed_offset=5)
+    nz, ny, nx = fimg.shape
+    mimg[:, :, : nx // 3] = 0.0              # the moving image zero on a slab
+    fimg[: nz // 4] = 0.0                    # the fixed image zero on another
+    mimg[nz // 2:, ny // 2:, nx // 2:] = 0.0  # and both zero in a corner
+    fimg[nz // 2:, ny // 2:, nx // 2:] = 0.0
+    r = case["radius"]
+    fi = backend.upload_image(g, fimg.astype(np.float32))
+    mi = backend.upload_image(g, mimg.astype(np.float32))
+    N.check(N.lib().fw_set_cc_window_sums(C.c_int32(sums)))
+    try:
+        (v1, d1), (v2, d2) = backend.cc_value_derivative_pair(fi, mi, r)
+    finally:
+        N.check(N.lib().fw_set_cc_window_sums(C.c_int32(0)))
+    (w1, e1), (w2, e2) = O.cc_pair(og, fimg, mimg, r)
+    assert rel(v1, w1) <= 1e-5 and rel(v2, w2) <= 1e-5, (v1, w1)
+    assert worst(backend.download_field(d1), e1) <= 1e-4 * np.abs(e1).max()
+    assert worst(backend.download_field(d2), e2) <= 1e-4 * np.abs(e2).max()
+
+
 def test_cc_of_an_image_with_itself_is_minus_one(backend):
     case = CASES["awkward_aligned"]
     g = fgrid(case)
