@@ -598,6 +598,14 @@ def mi_leg(b, g, fixed, mg, moving, initial, fi, mi, rank, world, chain=True):
                            "affine_iterations": chain["affine_iterations"],
                            "rigid_best_mi": [round(v, 6) for v in chain["rigid_best"]],
                            "affine_best_mi": [round(v, 6) for v in chain["affine_best"]],
+                           "rigid_evaluations": chain["rigid_evaluations"],
+                           "affine_evaluations": chain["affine_evaluations"],
+                           "initial_ms": round(chain["initial_ms"], 2),
+                           "prepare_ms": [round(v, 2) for v in
+                                          chain["rigid_prepare_ms"] + chain["affine_prepare_ms"]],
+                           "optimize_ms": [round(v, 2) for v in
+                                           chain["rigid_optimize_ms"] + chain["affine_optimize_ms"]],
+                           "affine_samples_from_rigid": chain["affine_samples_cached"],
                            "recipe": "CoM + rigid + affine, MI 32 bins 25 % regular, shrink "
                                      "4/2/1, sigma 2/1/0 vox, 500/250/100 iterations, 1e-6/10"}
     return out

@@ -86,7 +86,9 @@ class LinearRecipe(C.Structure):
 class LinearLevelTrace(C.Structure):
     _fields_ = [("level", C.c_int32), ("shrink_factors", C.c_uint32 * 3),
                 ("grid_size", C.c_int64 * 3), ("samples", C.c_int64), ("skipped", C.c_int32),
-                ("cg", CgTrace), ("parameters", C.c_double * 12)]
+                ("cg", CgTrace), ("parameters", C.c_double * 12),
+                ("prepare_ms", C.c_double), ("optimize_ms", C.c_double),
+                ("samples_cached", C.c_int32)]
 
 
 class LinearChainResult(C.Structure):
@@ -94,7 +96,8 @@ class LinearChainResult(C.Structure):
                 ("initial_center", C.c_double * 3), ("rigid", LinearTransform),
                 ("affine", LinearTransform), ("rigid_levels", LinearLevelTrace * 8),
                 ("affine_levels", LinearLevelTrace * 8), ("total_matrix", C.c_double * 9),
-                ("total_translation", C.c_double * 3), ("total_center", C.c_double * 3)]
+                ("total_translation", C.c_double * 3), ("total_center", C.c_double * 3),
+                ("initial_ms", C.c_double)]
 
 
 METRIC_VALUE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(LinearTransform),
@@ -140,7 +143,8 @@ class BatchTuning(C.Structure):
                 ("cc_zchunk", C.c_int32), ("cc_blocks_per_sm", C.c_int32),
                 ("measure_zchunk", C.c_int32), ("measure_blocks_per_sm", C.c_int32),
                 ("body_blocks_per_sm", C.c_int32), ("smooth_blocks_per_sm", C.c_int32),
-                ("from_cache", C.c_int32), ("tune_ms", C.c_double)]
+                ("from_cache", C.c_int32), ("tune_ms", C.c_double),
+                ("kernel_ms", C.c_double * 6)]
 
 
 class BatchReport(C.Structure):

@@ -479,6 +479,18 @@ class MiLevel:
         check(lib().fw_mi_level_time(self.handle, C.byref(t), C.c_int32(reps), ms, by))
         return {k: (ms[i], by[i]) for i, k in enumerate(("hist", "finish", "deriv"))}
 
+    def samples(self):
+        """fw_mi_level_samples: (points (n, 3) mm, fixed bins (n,), binning) of the level."""
+        n = C.c_int64()
+        b = N.MiBinning()
+        check(lib().fw_mi_level_samples(self.handle, None, None, C.c_int64(0), C.byref(n),
+                                        C.byref(b)))
+        pts = np.empty((n.value, 3), np.float64)
+        fb = np.empty(n.value, np.uint32)
+        check(lib().fw_mi_level_samples(self.handle, _ptr(pts), _ptr(fb), C.c_int64(n.value),
+                                        C.byref(n), None))
+        return pts, fb, b
+
     def num_valid(self) -> int:
         v = C.c_int64()
         check(lib().fw_mi_level_num_valid(self.handle, C.byref(v)))
@@ -520,8 +532,8 @@ class CudaLinearEngine:
                               percentage: float = 0.25, seed: int = 1, bins: int = 32,
                               fixed_mask: Image | None = None) -> MiLevel:
         """The level a linear stage prepares from device images at the level's smoothing:
-        regular samples of `level_grid`, binning and fixed bins on the host, then the device
-        level (fw_mi_level_prepare_regular)."""
+        regular samples of `level_grid`, their binning and fixed bins, prepared on the device
+        (fw_mi_level_prepare_regular)."""
         h = C.c_void_p()
         check(lib().fw_mi_level_prepare_regular(
             self.backend.ctx, C.byref(level_grid), fixed.handle, moving.handle,
@@ -564,6 +576,8 @@ def run_linear_stage(backend: "CudaBackend", recipe: N.LinearRecipe, fixed: Imag
     out = [dict(level=tr.level, shrink_factors=tuple(tr.shrink_factors),
                 grid_size=tuple(tr.grid_size), samples=tr.samples, skipped=bool(tr.skipped),
                 iterations=tr.cg.iterations, best_value=tr.cg.best_value,
+                evaluations=tr.cg.line_search_evaluations, prepare_ms=tr.prepare_ms,
+                optimize_ms=tr.optimize_ms, samples_cached=bool(tr.samples_cached),
                 parameters=list(tr.parameters[:n])) for tr in traces]
     return t, out
 
@@ -593,8 +607,22 @@ def run_linear_chain(backend: "CudaBackend", rigid: N.LinearRecipe, affine: N.Li
             "affine_best": [r.affine_levels[k].cg.best_value for k in range(affine.levels)],
             "rigid_iterations": [r.rigid_levels[k].cg.iterations for k in range(rigid.levels)],
             "affine_iterations": [r.affine_levels[k].cg.iterations for k in range(affine.levels)],
+            "rigid_evaluations": [r.rigid_levels[k].cg.line_search_evaluations
+                                  for k in range(rigid.levels)],
+            "affine_evaluations": [r.affine_levels[k].cg.line_search_evaluations
+                                   for k in range(affine.levels)],
+            "rigid_prepare_ms": [r.rigid_levels[k].prepare_ms for k in range(rigid.levels)],
+            "affine_prepare_ms": [r.affine_levels[k].prepare_ms for k in range(affine.levels)],
+            "rigid_optimize_ms": [r.rigid_levels[k].optimize_ms for k in range(rigid.levels)],
+            "affine_optimize_ms": [r.affine_levels[k].optimize_ms for k in range(affine.levels)],
+            "affine_samples_cached": [bool(r.affine_levels[k].samples_cached)
+                                      for k in range(affine.levels)],
+            "initial_ms": r.initial_ms,
             "total": (m3(r.total_matrix), np.array(r.total_translation[:]),
-                      np.array(r.total_center[:]))}
+                      np.array(r.total_center[:])),
+            # each stage's whole transform (the earlier transforms as its outer part)
+            "rigid_transform": N.LinearTransform.from_buffer_copy(r.rigid),
+            "affine_transform": N.LinearTransform.from_buffer_copy(r.affine)}
 
 
 def cg_settings_ants(max_step_mm=0.1, iterations=100, threshold=1e-6, window=10) -> N.CgSettings:

@@ -154,6 +154,8 @@ struct Tuning {
     int body_bps = 4;
     int smooth_bps = 4;
     double tune_ms = 0.0;
+    // the timed best of each batched kernel (one launch over all subjects, ms)
+    double warp_ms = 0, cc_ms = 0, smooth_ms = 0, compose_ms = 0, measure_ms = 0, body_ms = 0;
     bool cached = false;
 };
 
@@ -489,6 +491,7 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
         }, &ms));
         if (ms < bestms) bestms = ms, best.warp_bps = bps;
     }
+    best.warp_ms = bestms;
     // the CC pair on the warped template and subject: z chunks per column (whole columns pay
     // the 2r filling steps once)
     {
@@ -510,6 +513,7 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
         if (ms < bestms) bestms = ms, best.cc_zc = zc == nz ? 0 : zc;
     }
     best.cc_bps = occ;
+    best.cc_ms = bestms;
     // the smoothing pair (into sF, with R as its temporary)
     bestms = DBL_MAX;
     for (int bps : {2, 4, 8}) {
@@ -520,6 +524,7 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
         }, &ms));
         if (ms < bestms) bestms = ms, best.smooth_bps = bps;
     }
+    best.smooth_ms = bestms;
     // the composition, in place on a cleared scratch field (dM) with sF as the update
     FW_CUDA(cudaMemsetAsync(L.dM.p, 0, L.dM.bytes, ctx->stream));
     bestms = DBL_MAX;
@@ -533,6 +538,7 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
             if (ms < bestms) bestms = ms, best.comp_zc = zc, best.comp_bps = bps;
         }
     }
+    best.compose_ms = bestms;
     // the inversion measurement of F^-1 against F (residual into R, loop states of slot 0)
     bestms = DBL_MAX;
     for (int zc : gz) {
@@ -547,6 +553,7 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
             if (ms < bestms) bestms = ms, best.meas_zc = zc, best.meas_bps = bps;
         }
     }
+    best.measure_ms = bestms;
     // a body with its next measurement, on a cleared scratch inverse (dM) that keeps iterating
     const fw_invert_params forever = {1 << 30, -1.0, -1.0, 1};
     FW_TRY(launch_inv_measure_batch(ctx, L.grid, L.ps, best.meas_zc,
@@ -564,6 +571,7 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
         }, &ms));
         if (ms < bestms) bestms = ms, best.body_bps = bps;
     }
+    best.body_ms = bestms;
     FW_CUDA(cudaMemsetAsync(run.sc.inv, 0, sizeof(InvState) * 4 * B, ctx->stream));
     FW_CUDA(cudaMemsetAsync(run.sc.mx, 0, sizeof(unsigned int) * 2 * B, ctx->stream));
     return sync(ctx);
@@ -864,6 +872,12 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
             o.smooth_blocks_per_sm = t.smooth_bps;
             o.from_cache = t.cached ? 1 : 0;
             o.tune_ms = t.tune_ms;
+            o.kernel_ms[0] = t.warp_ms;
+            o.kernel_ms[1] = t.cc_ms;
+            o.kernel_ms[2] = t.smooth_ms;
+            o.kernel_ms[3] = t.compose_ms;
+            o.kernel_ms[4] = t.measure_ms;
+            o.kernel_ms[5] = t.body_ms;
             report->level_ms[level] = ms;
         }
         // the smoothed sources of this level are not needed by the next one

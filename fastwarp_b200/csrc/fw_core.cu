@@ -3,11 +3,15 @@
 // (backend.rs:268-271), max and L2 norms (backend.rs:252-265).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstring>
 #include <string>
 
 #include "fw_internal.cuh"
+
+#include <chrono>
+#include <thread>
 
 namespace fw {
 
@@ -135,9 +139,33 @@ int dev_alloc(fw_ctx* ctx, size_t bytes, void** out) {
         std::lock_guard<std::mutex> lock(ctx->cache_mu);
         auto it = ctx->cache.find(sz);
         if (it != ctx->cache.end()) {
-            *out = it->second;
+            *out = it->second->p;
+            ctx->cache_lru.erase(it->second);
             ctx->cache.erase(it);
             ctx->cached_bytes -= sz;
+        } else if (!ctx->capturing) {
+            // Requests of many grid sizes (a served stream) would otherwise leave a buffer of
+            // every size they used in the cache. On a miss that would take the context past its
+            // largest working set (at least 1 GB), buffers idle in the cache for over a second go
+            // back to the pool, oldest first, which reuses their memory for any size; buffers
+            // freed more recently (the same shapes about to repeat) stay. Not during a capture,
+            // where a free would become a graph node.
+            const uint64_t cap = std::max<uint64_t>(ctx->stats.peak_device_bytes, (uint64_t)1 << 30);
+            const auto now = std::chrono::steady_clock::now();
+            while (!ctx->cache_lru.empty() &&
+                   ctx->live_bytes.load() + ctx->cached_bytes + sz > cap) {
+                const auto oldest = ctx->cache_lru.begin();
+                if (now - oldest->freed < std::chrono::seconds(1)) break;
+                auto range = ctx->cache.equal_range(oldest->size);
+                for (auto m = range.first; m != range.second; ++m)
+                    if (m->second == oldest) {
+                        ctx->cache.erase(m);
+                        break;
+                    }
+                cudaFreeAsync(oldest->p, ctx->stream);
+                ctx->cached_bytes -= oldest->size;
+                ctx->cache_lru.erase(oldest);
+            }
         }
     }
     if (!*out) {
@@ -160,7 +188,8 @@ void dev_free(fw_ctx* ctx, void* p, size_t bytes) {
     const size_t sz = cache_size(bytes);
     {
         std::lock_guard<std::mutex> lock(ctx->cache_mu);
-        ctx->cache.emplace(sz, p);
+        ctx->cache_lru.push_back(fw_ctx::CachedBuffer{sz, p, std::chrono::steady_clock::now()});
+        ctx->cache.emplace(sz, std::prev(ctx->cache_lru.end()));
         ctx->cached_bytes += sz;
     }
     ctx->live_bytes.fetch_sub(sz);
@@ -169,13 +198,15 @@ void dev_free(fw_ctx* ctx, void* p, size_t bytes) {
 
 // Returns the cached buffers to the pool and the pool's unused memory to the device.
 int trim_cache(fw_ctx* ctx) {
-    std::unordered_multimap<size_t, void*> drop;
+    drop_draws(ctx);
+    std::list<fw_ctx::CachedBuffer> drop;
     {
         std::lock_guard<std::mutex> lock(ctx->cache_mu);
-        drop.swap(ctx->cache);
+        drop.swap(ctx->cache_lru);
+        ctx->cache.clear();
         ctx->cached_bytes = 0;
     }
-    for (auto& kv : drop) cudaFreeAsync(kv.second, ctx->stream);
+    for (auto& c : drop) cudaFreeAsync(c.p, ctx->stream);
     FW_CUDA(cudaStreamSynchronize(ctx->stream));
     if (ctx->pool) FW_CUDA(cudaMemPoolTrimTo(ctx->pool, 0));
     return 0;
@@ -209,7 +240,40 @@ int new_field(fw_ctx* ctx, const HostGrid& g, fw_field** out) {
 int sync(fw_ctx* ctx) {
     ctx->stats.host_syncs++;
     FW_CUDA(cudaEventRecord(ctx->done, ctx->stream));
+    // A short wait is polled: a blocking wait sleeps until the device's interrupt wakes the
+    // thread, which adds tens to hundreds of microseconds to every small read-back (the linear
+    // optimiser makes thousands). The thread yields between queries, so that polling threads
+    // of other contexts (the server's slots) leave the driver to the launching ones. A wait
+    // longer than a millisecond then blocks and leaves the core free.
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t e = cudaEventQuery(ctx->done);
+        if (e == cudaSuccess) return 0;
+        if (e != cudaErrorNotReady) return cuda_fail(e, "cudaEventQuery");
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(1)) break;
+        std::this_thread::yield();
+    }
     FW_CUDA(cudaEventSynchronize(ctx->done));
+    return 0;
+}
+
+int host_stage(fw_ctx* ctx, size_t bytes, void** out) {
+    if (bytes > ctx->h_stage_bytes) {
+        if (ctx->h_stage) {
+            FW_TRY(sync(ctx));
+            cudaFreeHost(ctx->h_stage);
+            ctx->h_stage = nullptr;
+            ctx->h_stage_bytes = 0;
+        }
+        const size_t want = std::max<size_t>(bytes, (size_t)1 << 20);
+        if (cudaMallocHost(&ctx->h_stage, want) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->h_stage = nullptr;
+            return fail(FW_ERR_MEMORY, "pinned staging allocation failed");
+        }
+        ctx->h_stage_bytes = want;
+    }
+    *out = ctx->h_stage;
     return 0;
 }
 
@@ -800,15 +864,18 @@ int fw_ctx_create(int device, fw_ctx** out) {
 void fw_ctx_destroy(fw_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
+    drop_draws(ctx);
     if (ctx->stream) {
         cudaStreamSynchronize(ctx->stream);
-        for (auto& kv : ctx->cache) cudaFreeAsync(kv.second, ctx->stream);
+        for (auto& c : ctx->cache_lru) cudaFreeAsync(c.p, ctx->stream);
         cudaStreamSynchronize(ctx->stream);
     }
     ctx->cache.clear();
+    ctx->cache_lru.clear();
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     if (ctx->cancel_mapped) cudaFreeHost(const_cast<int32_t*>(ctx->cancel_mapped));
     if (ctx->done) cudaEventDestroy(ctx->done);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -12,6 +12,9 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <chrono>
+#include <future>
+#include <list>
 #include <unordered_map>
 #include <vector>
 
@@ -88,6 +91,8 @@ struct fw_ctx {
     size_t scratch_doubles = 0;
     unsigned int* d_counter = nullptr;  // last-block counters (zeroed after use)
     double* h_pinned = nullptr;      // pinned host scalars for read-backs
+    void* h_stage = nullptr;         // pinned host staging for larger uploads (grown on demand)
+    size_t h_stage_bytes = 0;
     fw_stats stats{};
     std::atomic<uint64_t> live_bytes{0};
     const volatile int32_t* cancel = nullptr;  // the caller's flag (fw_ctx_set_cancel_flag)
@@ -100,9 +105,28 @@ struct fw_ctx {
     cudaEvent_t done = nullptr;      // blocking-sync event the host waits on
     cudaMemPool_t pool = nullptr;    // the context's own stream-ordered memory pool
     // freed buffers kept by size for the next allocation of that size (stream order makes the
-    // reuse safe: every user of a buffer runs on `stream`); guarded for frees from other threads
+    // reuse safe: every user of a buffer runs on `stream`); guarded for frees from other threads.
+    // `cache_lru` holds them in the order they were freed, `cache` indexes it by size.
+    struct CachedBuffer {
+        size_t size;
+        void* p;
+        std::chrono::steady_clock::time_point freed;
+    };
     std::mutex cache_mu;
-    std::unordered_multimap<size_t, void*> cache;
+    std::list<CachedBuffer> cache_lru;
+    // the regular sampler's generator integers on the device, kept by (seed, picks) for the next
+    // registration of the same level grid (a few buffers, the least recently used out first);
+    // used by the context's own thread only
+    struct DrawBuffer {
+        uint32_t seed;
+        int64_t picks;
+        uint32_t* d;
+        size_t bytes;
+        uint64_t used;
+    };
+    std::vector<DrawBuffer> draws;
+    uint64_t draws_tick = 0;
+    std::unordered_multimap<size_t, std::list<CachedBuffer>::iterator> cache;
     uint64_t cached_bytes = 0;
 };
 
@@ -135,6 +159,9 @@ int new_image(fw_ctx* ctx, const HostGrid& g, fw_image** out);
 int new_field(fw_ctx* ctx, const HostGrid& g, fw_field** out);
 int sync(fw_ctx* ctx);
 int check_launch(fw_ctx* ctx, const char* what);
+// The context's pinned staging buffer, at least `bytes` long; the caller synchronises the
+// stream before it writes the buffer again.
+int host_stage(fw_ctx* ctx, size_t bytes, void** out);
 int ensure_scratch(fw_ctx* ctx, size_t doubles);
 
 // ---- device helpers: ITK interpolation rules (interp.rs:43-120, field_ops.rs:143-181) -----
@@ -562,6 +589,49 @@ int enqueue_image_upload_f32(fw_ctx* ctx, const HostGrid& g, const float* host, 
 void linear_transform_map(const fw_linear_transform* t, double M[9], double off[3]);
 // The context a device MI level evaluates on (fw_mi.cu).
 const fw_ctx* mi_level_context(const fw_mi_level* level);
+// A device MI level over sample records already on the device (fw_mi.cu): float32 offsets of
+// the points from `center` in xyz, the fixed bin's bits in w. The level takes the moving image
+// when own_moving and the records when own_rec (freed with the level, or here on failure).
+int mi_level_create(fw_ctx* ctx, fw_image* moving, bool own_moving, float4* d_rec, bool own_rec,
+                    int64_t n, const double center[3], const fw_mi_binning* binning,
+                    fw_mi_level** out);
+
+// A linear-stage level's prepared Mattes MI samples on the device (fw_samples.cu).
+struct LevelSamples {
+    float4* d_rec = nullptr;  // n records: float32 offsets from `center` in xyz, the fixed bin in w
+    int64_t n = 0;
+    double center[3] = {0.0, 0.0, 0.0};
+    fw_mi_binning binning{};
+    int64_t candidates = 0;   // sample points inside the fixed mask (every point without one)
+    bool skip = false;        // Mattes MI is undefined on the level's samples: `why`
+    std::string why;
+};
+// The regular sample set of level grid `lg` from `seed` (only the points inside `mask`, when
+// given, an image on its own grid), the fixed range at their nearest voxels of `fixed`, the
+// finite range of the whole `moving` image, the binning, and the records of the points whose
+// trilinear fixed value exists (linear.rs:251-280, 474-492, 940-945; sampling.rs:181-238).
+// Generator integers of levels generated ahead on host threads (one job per level).
+struct DrawPlan {
+    struct Job {
+        uint32_t seed;
+        int64_t picks;
+        std::future<std::vector<uint32_t>> draws;
+    };
+    std::vector<Job> jobs;
+};
+// Starts generating on a host thread the draws of level grid `lg` at `percentage` from `seed`,
+// unless the context holds them already.
+void plan_draws(fw_ctx* ctx, DrawPlan& plan, const HostGrid& lg, float percentage, uint32_t seed);
+// Returns the context's device copies of the draws to its buffer cache.
+void drop_draws(fw_ctx* ctx);
+int prepare_level_samples(fw_ctx* ctx, const HostGrid& lg, const fw_image* fixed,
+                          const fw_image* moving, const fw_image* mask, float percentage,
+                          uint32_t seed, int bins, LevelSamples& out, DrawPlan* plan = nullptr);
+void free_level_samples(fw_ctx* ctx, LevelSamples& s);
+// init.rs:50-74 (centre_of_gravity) over the image's float32 values, summed in float64.
+int centre_of_mass(fw_ctx* ctx, const fw_image* img, double out[3]);
+// Whether any voxel of the image is not zero.
+int mask_has_inside(fw_ctx* ctx, const fw_image* mask, bool* any);
 
 // The SyN recipe's validation (fw_syn.cu): 0 or FW_ERR_INVALID with the reference's message.
 int syn_recipe_check(const fw_syn_recipe* r);

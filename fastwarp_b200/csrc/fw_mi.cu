@@ -28,6 +28,7 @@ struct fw_mi_level {
     fw_ctx* ctx;
     fw_image* moving;
     bool own_moving;
+    bool own_rec;  // false: the records belong to the caller (a linear chain's sample cache)
     float4* d_rec;
     int64_t n;
     double center[3];
@@ -39,6 +40,8 @@ struct fw_mi_level {
     double* d_part;              // block partials
     unsigned int* d_counter;
     unsigned int blocks;
+    unsigned int hist_grid;  // resident histogram blocks (one wave)
+    size_t hist_smem;
     int64_t last_valid;
     size_t rec_bytes;
 };
@@ -711,10 +714,9 @@ int hist_and_finish(fw_mi_level* L, const fw_linear_transform* ts, int count, bo
     FW_CUDA(cudaMemcpyAsync(d_maps, maps.data(), sizeof(MiMap) * count, cudaMemcpyHostToDevice,
                             ctx->stream));
     FW_CUDA(cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells * count, ctx->stream));
-    const size_t sh = mi_hist_smem(bins);
-    FW_TRY(hist_launch_setup(ctx, sh));
-    dim3 grid(hist_blocks(L, sh), count);
-    k_mi_hist<<<grid, MI_THREADS, sh, ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d, L->d_hist);
+    dim3 grid(L->hist_grid, count);
+    k_mi_hist<<<grid, MI_THREADS, L->hist_smem, ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d,
+                                                              L->d_hist);
     FW_TRY(check_launch(ctx, "k_mi_hist"));
     k_mi_finish<<<count, 1024, 0, ctx->stream>>>(L->d_hist, bins, L->binning.moving_bin_size,
                                                  nullptr, L->d_ratio, L->d_out,
@@ -735,50 +737,46 @@ int check_status(fw_mi_level* L, const double* out) {
 
 using namespace fw;
 
-extern "C" {
-
-static int mi_prepare_common(fw_ctx* ctx, fw_image* moving, bool own, const double* points,
-                             const uint32_t* fixed_bin, int64_t n, const fw_mi_binning* binning,
-                             fw_mi_level** out) {
+// A level over sample records already on the device (float32 offsets from `center`, the fixed
+// bin in w). Takes the moving image when own_moving and the records when own_rec, also on failure.
+int fw::mi_level_create(fw_ctx* ctx, fw_image* moving, bool own_moving, float4* d_rec,
+                        bool own_rec, int64_t n, const double center[3],
+                        const fw_mi_binning* binning, fw_mi_level** out) {
+    auto drop = [&] {
+        if (own_rec && d_rec) dev_free(ctx, d_rec, sizeof(float4) * (size_t)std::max<int64_t>(n, 0));
+        if (own_moving) fw_image_free(moving);
+    };
     if (n <= 0) {
-        if (own) fw_image_free(moving);
+        drop();
         return fail(FW_ERR_INVALID, "mattes: no samples inside the fixed image");
     }
     if (binning->bins <= 4 || binning->bins > MAX_BINS) {
-        if (own) fw_image_free(moving);
+        drop();
         return fail(FW_ERR_INVALID, "mattes: bins must be in 5..=32");
     }
     fw_mi_level* L = new fw_mi_level();
     L->ctx = ctx;
     L->moving = moving;
-    L->own_moving = own;
+    L->own_moving = own_moving;
+    L->own_rec = own_rec;
+    L->d_rec = d_rec;
     L->n = n;
     L->binning = *binning;
-    // the cloud centre in float64; records hold float32 offsets from it
-    double c[3] = {0, 0, 0};
-    for (int64_t i = 0; i < n; ++i)
-        for (int a = 0; a < 3; ++a) c[a] += points[3 * i + a];
-    for (int a = 0; a < 3; ++a) L->center[a] = c[a] / (double)n;
-    std::vector<float4> rec((size_t)n);
-    for (int64_t i = 0; i < n; ++i) {
-        if (fixed_bin[i] >= (uint32_t)binning->bins) {
-            if (own) fw_image_free(moving);
-            delete L;
-            return fail(FW_ERR_INVALID, "mattes: a fixed bin is out of range");
-        }
-        rec[i].x = (float)(points[3 * i] - L->center[0]);
-        rec[i].y = (float)(points[3 * i + 1] - L->center[1]);
-        rec[i].z = (float)(points[3 * i + 2] - L->center[2]);
-        uint32_t b = fixed_bin[i];
-        std::memcpy(&rec[i].w, &b, 4);
-    }
+    for (int a = 0; a < 3; ++a) L->center[a] = center[a];
     L->rec_bytes = sizeof(float4) * (size_t)n;
     const int cells = binning->bins * binning->bins + binning->bins;
     const int max_t = 16;
+    // the gradient pass: one wave of resident blocks (a partial second wave would run its tail
+    // at a fraction of the occupancy)
+    int occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mi_deriv, MI_THREADS, 0) != cudaSuccess ||
+        occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+    }
     L->blocks = (unsigned int)std::max<long long>(
-        1, std::min<long long>((n + MI_THREADS - 1) / MI_THREADS, 4LL * ctx->num_sms));
-    int rc = dev_alloc(ctx, L->rec_bytes, (void**)&L->d_rec);
-    if (!rc) rc = dev_alloc(ctx, sizeof(unsigned long long) * cells * max_t, (void**)&L->d_hist);
+        1, std::min<long long>((n + MI_THREADS - 1) / MI_THREADS, (long long)occ * ctx->num_sms));
+    int rc = dev_alloc(ctx, sizeof(unsigned long long) * cells * max_t, (void**)&L->d_hist);
     if (!rc) rc = dev_alloc(ctx, sizeof(double) * binning->bins * binning->bins, (void**)&L->d_ratio);
     if (!rc) rc = dev_alloc(ctx, sizeof(double) * 4 * max_t, (void**)&L->d_out);
     if (!rc) rc = dev_alloc(ctx, sizeof(double) * 16, (void**)&L->d_mom);
@@ -786,18 +784,60 @@ static int mi_prepare_common(fw_ctx* ctx, fw_image* moving, bool own, const doub
     if (!rc) rc = dev_alloc(ctx, sizeof(unsigned int) * 4, (void**)&L->d_counter);
     if (!rc) {
         cudaError_t e = cudaMemsetAsync(L->d_counter, 0, sizeof(unsigned int) * 4, ctx->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(L->d_rec, rec.data(), L->rec_bytes, cudaMemcpyHostToDevice, ctx->stream);
-        if (e != cudaSuccess) rc = cuda_fail(e, "mi level upload");
-        ctx->stats.bytes_uploaded += L->rec_bytes;
+        if (e != cudaSuccess) rc = cuda_fail(e, "mi level setup");
     }
-    if (!rc) rc = sync(ctx);
+    if (!rc) {
+        L->hist_smem = mi_hist_smem(binning->bins);
+        rc = hist_launch_setup(ctx, L->hist_smem);
+        if (!rc) L->hist_grid = hist_blocks(L, L->hist_smem);
+    }
     if (rc) {
         fw_mi_level_free(L);
         return rc;
     }
     *out = L;
     return 0;
+}
+
+extern "C" {
+
+static int mi_prepare_common(fw_ctx* ctx, fw_image* moving, bool own, const double* points,
+                             const uint32_t* fixed_bin, int64_t n, const fw_mi_binning* binning,
+                             fw_mi_level** out) {
+    if (n <= 0 || binning->bins <= 4 || binning->bins > MAX_BINS)
+        return mi_level_create(ctx, moving, own, nullptr, false, n, nullptr, binning, out);
+    // the cloud centre in float64; records hold float32 offsets from it
+    double c[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) c[a] += points[3 * i + a];
+    for (int a = 0; a < 3; ++a) c[a] /= (double)n;
+    std::vector<float4> rec((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        if (fixed_bin[i] >= (uint32_t)binning->bins) {
+            if (own) fw_image_free(moving);
+            return fail(FW_ERR_INVALID, "mattes: a fixed bin is out of range");
+        }
+        rec[i].x = (float)(points[3 * i] - c[0]);
+        rec[i].y = (float)(points[3 * i + 1] - c[1]);
+        rec[i].z = (float)(points[3 * i + 2] - c[2]);
+        uint32_t b = fixed_bin[i];
+        std::memcpy(&rec[i].w, &b, 4);
+    }
+    const size_t bytes = sizeof(float4) * (size_t)n;
+    float4* d_rec = nullptr;
+    int rc = dev_alloc(ctx, bytes, (void**)&d_rec);
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(d_rec, rec.data(), bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "mi level upload");
+        ctx->stats.bytes_uploaded += bytes;
+    }
+    if (!rc) rc = sync(ctx);
+    if (rc) {
+        if (d_rec) dev_free(ctx, d_rec, bytes);
+        if (own) fw_image_free(moving);
+        return rc;
+    }
+    return mi_level_create(ctx, moving, own, d_rec, true, n, c, binning, out);
 }
 
 int fw_mi_level_prepare(fw_ctx* ctx, const fw_grid* moving_grid, const double* moving,
@@ -946,11 +986,33 @@ int fw_mi_level_num_valid(const fw_mi_level* L, int64_t* out) {
     return 0;
 }
 
+int fw_mi_level_samples(const fw_mi_level* L, double* points, uint32_t* fixed_bins, int64_t cap,
+                        int64_t* n, fw_mi_binning* binning) {
+    FW_CHECK(L && n, "null argument");
+    *n = L->n;
+    if (binning) *binning = L->binning;
+    if (cap < L->n || (!points && !fixed_bins)) return 0;
+    fw_ctx* ctx = L->ctx;
+    std::vector<float4> rec((size_t)L->n);
+    FW_CUDA(cudaMemcpyAsync(rec.data(), L->d_rec, L->rec_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    FW_TRY(sync(ctx));
+    ctx->stats.bytes_downloaded += L->rec_bytes;
+    for (int64_t i = 0; i < L->n; ++i) {
+        if (points) {
+            points[3 * i] = L->center[0] + (double)rec[i].x;
+            points[3 * i + 1] = L->center[1] + (double)rec[i].y;
+            points[3 * i + 2] = L->center[2] + (double)rec[i].z;
+        }
+        if (fixed_bins) std::memcpy(&fixed_bins[i], &rec[i].w, 4);
+    }
+    return 0;
+}
+
 void fw_mi_level_free(fw_mi_level* L) {
     if (!L) return;
     fw_ctx* ctx = L->ctx;
     const int cells = L->binning.bins * L->binning.bins + L->binning.bins;
-    dev_free(ctx, L->d_rec, L->rec_bytes);
+    if (L->own_rec) dev_free(ctx, L->d_rec, L->rec_bytes);
     dev_free(ctx, L->d_hist, sizeof(unsigned long long) * cells * 16);
     dev_free(ctx, L->d_ratio, sizeof(double) * L->binning.bins * L->binning.bins);
     dev_free(ctx, L->d_out, sizeof(double) * 4 * 16);

@@ -408,7 +408,7 @@ def run_syn_batch(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
     tuning = []
     for lv in range(r.levels):
         t = rep.tuning[lv]
-        tuning.append({k: (list(getattr(t, k)) if k == "grid_size" else getattr(t, k))
+        tuning.append({k: (list(getattr(t, k)) if k in ("grid_size", "kernel_ms") else getattr(t, k))
                        for k, _ in N.BatchTuning._fields_})
     return BatchResult(out, list(statuses), tuning, list(rep.level_ms[:r.levels]),
                        int(rep.device_bytes))

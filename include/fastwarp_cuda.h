@@ -399,12 +399,18 @@ int fw_mi_level_prepare_image(fw_ctx* ctx, const fw_image* moving, const double*
  * from device images already at the level's smoothing: the regular sample set of `level_grid`
  * from `seed` (only the points inside `fixed_mask`, which may be NULL), the binning (fixed range at
  * the samples' nearest voxels, moving range over the whole moving image) and the kept points with
- * their trilinear fixed bins, then as fw_mi_level_prepare_image (`moving` must outlive the
- * level). Fails with the reference's reason when Mattes MI is undefined on the samples. */
+ * their trilinear fixed bins, all on the device (the host draws only the generator's integers);
+ * `moving` must outlive the level. Fails with the reference's reason when Mattes MI is undefined
+ * on the samples. */
 int fw_mi_level_prepare_regular(fw_ctx* ctx, const fw_grid* level_grid, const fw_image* fixed,
                                 const fw_image* moving, const fw_image* fixed_mask,
                                 float percentage, uint32_t seed, int32_t bins,
                                 fw_mi_level** out);
+/* A level's samples, for inspection: the count in *n and, when cap >= *n, each sample's point
+ * (3 per sample, physical mm: the cloud centre plus the record's float32 offset) and fixed bin;
+ * `points`, `fixed_bins` and `binning` may be NULL. */
+int fw_mi_level_samples(const fw_mi_level* level, double* points, uint32_t* fixed_bins,
+                        int64_t cap, int64_t* n, fw_mi_binning* binning);
 /* LinearMetric::value (optimizer.rs:61): -MI. */
 int fw_mi_level_value(fw_mi_level* level, const fw_linear_transform* t, double* value);
 /* LinearMetric::value_and_derivative (optimizer.rs:62-64): -MI and +dMI/dtheta (6 or 12). */
@@ -567,6 +573,9 @@ typedef struct fw_linear_level_trace {
     int32_t skipped;                 /* 1: Mattes MI undefined on the level's samples */
     fw_cg_trace cg;
     double parameters[12];           /* the optimised parameters after the level */
+    double prepare_ms;               /* wall time: smoothing, sampling, sample preparation */
+    double optimize_ms;              /* wall time: the optimiser's metric evaluations */
+    int32_t samples_cached;          /* 1: the samples came from the chain's earlier stage */
 } fw_linear_level_trace;
 
 /* run_linear_stage (linear.rs:512-597): per level, the fixed grid shrunk by the level's factors,
@@ -601,6 +610,7 @@ typedef struct fw_linear_chain_result {
     fw_linear_level_trace rigid_levels[FW_MAX_LEVELS];
     fw_linear_level_trace affine_levels[FW_MAX_LEVELS];
     double total_matrix[9], total_translation[3], total_center[3];
+    double initial_ms;               /* wall time of the centre-of-mass initialiser */
 } fw_linear_chain_result;
 
 /* run_linear_chain (linear.rs:1105-1212): the initial transform from the centres of mass of the
@@ -645,6 +655,9 @@ typedef struct fw_batch_tuning {
     int32_t smooth_blocks_per_sm;
     int32_t from_cache;
     double tune_ms;
+    /* the tuned time of one launch over all subjects (ms; 0 when the shapes were not timed):
+     * moving-side warp, CC pair, smoothing pair, compose, inversion measure, inversion body */
+    double kernel_ms[6];
 } fw_batch_tuning;
 
 typedef struct fw_batch_report {

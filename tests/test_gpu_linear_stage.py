@@ -14,6 +14,7 @@ import pytest
 
 import oracle as O
 from fastwarp_b200 import FastwarpError, linear_transform, make_grid
+from fastwarp_b200 import _native as N
 from fastwarp_b200.backend import (grid_corners, linear_recipe, run_linear_chain,
                                    run_linear_stage)
 from fastwarp_b200.phantoms import blob_pair
@@ -116,13 +117,23 @@ def inner_map(t):
                                            list(t.parameters[:n]), center=tuple(t.center)))
 
 
-def test_the_linear_chain_matches_the_oracle(backend):
-    """Centre-of-mass start, rigid stage, affine stage from the rigid result, collapsed total."""
+def test_the_linear_chain_composes_its_stages_and_follows_the_oracle(backend):
+    """run_linear_chain (linear.rs:1148-1212): the centre-of-mass start, the rigid stage, the
+    affine stage from the rigid result, the collapsed total. Checked exactly: each of the chain's
+    stages is run_linear_stage from the chain's own start transform, bit for bit (the affine stage
+    takes the rigid stage's smoothed moving images and samples from the chain's cache, which equal
+    a fresh preparation); the initial transform is the centres of mass (1e-9 mm against numpy);
+    the total is the collapse of the three (1e-9 mm at the grid corners against the same
+    composition in numpy). Against the oracle's chain the total stays within 0.5 mm at the
+    corners: each stage alone is held to 0.05 mm by the stage tests, but two conjugate-gradient
+    runs of 10 + 6 iterations whose line searches compare MI values that agree to ~1e-7 can
+    branch differently at a near-tie, and the second stage starts from the first one's result."""
     g, fixed, moving = blob_pair(40, seed=29)
     its, shrink, sigmas = (10, 6), (2, 1), (1.0, 0.0)
     r = linear_recipe(iterations=its, shrink_factors=shrink, smoothing_sigmas=sigmas)
     fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
     out = run_linear_chain(backend, r, r, fi, mi, fi, mi)
+    assert out["affine_samples_cached"] == [True, True]
     nz, ny, nx = fixed.shape
     z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
     pts = [g.origin[a] + g.spacing[a] * v for a, v in enumerate((x, y, z))]
@@ -133,21 +144,37 @@ def test_the_linear_chain_matches_the_oracle(backend):
     fc, mc = cog(fixed), cog(moving)
     assert np.abs(out["initial"][2] - fc).max() < 1e-9
     assert np.abs(out["initial"][1] - (mc - fc)).max() < 1e-9
-    rt, _ = oracle_stage(g, fixed, moving, "euler", [0.0] * 6, tuple(fc), its, shrink, sigmas,
-                         outer=(np.eye(3), tuple(mc - fc), tuple(fc)))
-    mr, offr = inner_map(rt)
-    off_after = offr + (mc - fc)
-    at, _ = oracle_stage(g, fixed, moving, "affine", list(np.eye(3).ravel()) + [0.0] * 3,
-                         tuple(fc), its, shrink, sigmas, outer=(mr, tuple(off_after), (0, 0, 0)))
-    ma, offa = inner_map(at)
+    # each stage is the stage run alone from the chain's start transform
+    for key, n, start in (("rigid", 6, [0.0] * 6), ("affine", 12, list(np.eye(3).ravel()) + [0.0] * 3)):
+        t0 = N.LinearTransform.from_buffer_copy(out[key + "_transform"])
+        for k in range(12):
+            t0.parameters[k] = start[k] if k < n else 0.0
+        alone, _ = run_linear_stage(backend, r, fi, mi, t0)
+        assert list(alone.parameters[:n]) == out[key], key
+    # the collapse of the three
+    corners = grid_corners(g)
+    mr, offr = inner_map(out["rigid_transform"])
+    off_after = offr + out["initial"][1]
+    ma, offa = inner_map(out["affine_transform"])
     total_m, total_off = mr @ ma, mr @ offa + off_after
     dm, dt, dc = out["total"]
-    shift = max(np.linalg.norm((dm @ (c - dc) + dc + dt) - (total_m @ c + total_off))
-                for c in grid_corners(g))
-    print(f"chain: corner shift {shift:.2e} mm")
-    assert shift < 0.05, shift
-    assert np.abs(dc - fc).max() < 1e-9  # the total keeps the affine stage's centre
+    collapse = max(np.linalg.norm((dm @ (c - dc) + dc + dt) - (total_m @ c + total_off))
+                   for c in corners)
+    assert collapse < 1e-9, collapse
+    assert np.abs(dc - out["initial"][2]).max() == 0.0  # the total keeps the affine stage's centre
     assert max(abs(v) for v in out["rigid"]) > 1e-4  # the rigid stage moved
+    # the oracle's chain
+    rt, _ = oracle_stage(g, fixed, moving, "euler", [0.0] * 6, tuple(fc), its, shrink, sigmas,
+                         outer=(np.eye(3), tuple(mc - fc), tuple(fc)))
+    omr, ooffr = inner_map(rt)
+    ooff_after = ooffr + (mc - fc)
+    at, _ = oracle_stage(g, fixed, moving, "affine", list(np.eye(3).ravel()) + [0.0] * 3,
+                         tuple(fc), its, shrink, sigmas, outer=(omr, tuple(ooff_after), (0, 0, 0)))
+    oma, ooffa = inner_map(at)
+    om, ooff = omr @ oma, omr @ ooffa + ooff_after
+    shift = max(np.linalg.norm((dm @ (c - dc) + dc + dt) - (om @ c + ooff)) for c in corners)
+    print(f"chain: corner shift against the oracle's chain {shift:.2e} mm")
+    assert shift < 0.5, shift
 
 
 def half_mask(g):
@@ -241,3 +268,46 @@ def test_the_masked_linear_chain_keeps_its_samples_inside_the_mask(backend):
     for key in ("rigid_samples", "affine_samples"):
         for a, b in zip(masked[key], full[key]):
             assert 0 < a < 0.6 * b
+
+
+@pytest.mark.parametrize("masked", [False, True])
+def test_the_device_sample_preparation_matches_the_oracle(backend, masked):
+    """fw_mi_level_prepare_regular draws the regular sample set and prepares it on the device
+    (the jittered points, the fixed mask, the fixed range at the nearest voxels, the moving range
+    over the whole image, the trilinear fixed bins). Against the oracle's sampling and
+    preparation of the same float32 images on an oblique, anisotropic grid with a shrunk level
+    grid: the binning is equal to the last bit, the same points are kept in the same raster
+    order, each within the float32 rounding of its offset from the cloud centre, and every fixed
+    bin is equal. (The device's log and cos may differ from the host library's in the last bit;
+    that moves a point by ~1e-15 mm, and no point of this set lies that close to an edge.)"""
+    from fastwarp_b200.backend import CudaLinearEngine
+    rot = np.array([[0.98, -0.17, 0.1], [0.17, 0.985, 0.0], [-0.1, 0.02, 0.995]])
+    q, _ = np.linalg.qr(rot)
+    g = make_grid((44, 40, 36), (1.1, 0.9, 1.3), (-20.0, 7.5, -11.0), q)
+    _, fixed, moving = blob_pair(44, seed=303)
+    fixed, moving = fixed[:36, :40, :44].copy(), moving[:36, :40, :44].copy()
+    og = ogrid(g)
+    lg = O.shrink_grid(og, (2, 2, 1))
+    dlg = make_grid(tuple(lg.size), tuple(lg.spacing), tuple(lg.origin),
+                    np.array(lg.direction[:]).reshape(3, 3))
+    fi, mi = backend.upload_image(g, fixed), backend.upload_image(g, moving)
+    mask_img = None
+    pts = O.sample_points_regular(lg, 0.25, 7)
+    if masked:
+        mg = make_grid((20, 22, 18), (2.2, 1.9, 2.5), (-18.0, 8.0, -10.0), q)
+        mk = np.zeros((18, 22, 20), np.float32)
+        mk[2:15, 3:20, 4:17] = 1.0
+        mask_img = backend.upload_image(mg, mk)
+        pts = pts[O.mask_inside(ogrid(mg), mk, pts)]
+    kept, fbin, ob = O.prepare_samples(og, fixed, og, moving, pts, 32)
+    lvl = CudaLinearEngine(backend).prepare_level_regular(dlg, fi, mi, 0.25, 7, 32, mask_img)
+    dpts, dfb, db = lvl.samples()
+    for k in ("fixed_min", "fixed_max", "moving_min", "moving_max", "fixed_bin_size",
+              "moving_bin_size", "fixed_normalized_min", "moving_normalized_min"):
+        assert getattr(db, k) == getattr(ob, k), k
+    assert len(dfb) == len(fbin) > 1000
+    err = np.abs(dpts - kept).max()
+    print(f"samples {len(fbin)} of {len(pts)} candidates; largest point difference {err:.2e} mm")
+    assert err < 1e-5
+    assert np.array_equal(dfb, fbin)
+    lvl.free()
