@@ -42,6 +42,7 @@ struct fw_mi_level {
     unsigned int blocks;
     unsigned int hist_grid;  // resident histogram blocks (one wave)
     size_t hist_smem;
+    bool hist_clear;         // the histograms are zero (the next pass may add into them)
     int64_t last_valid;
     size_t rec_bytes;
 };
@@ -116,13 +117,10 @@ size_t mi_hist_smem(int bins) {
     return sizeof(unsigned long long) * MI_REP * (size_t)(bins * bins + bins + 1);
 }
 
-// Joint histogram of transform blockIdx.y over a chunk of samples per block.
-__global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict__ maps,
-                                                        const float4* __restrict__ rec,
-                                                        long long n,
-                                                        const float* __restrict__ img,
-                                                        unsigned long long* __restrict__ hist) {
-    const MiMap& mp = maps[blockIdx.y];
+// Joint histogram of one transform over a chunk of samples per block, added into `out`.
+__device__ __forceinline__ void mi_hist_body(const MiMap& mp, const float4* __restrict__ rec,
+                                             long long n, const float* __restrict__ img,
+                                             unsigned long long* __restrict__ out) {
     const int bins = mp.bins;
     const int cells = bins * bins + bins;
     const int cstride = cells + 1;
@@ -146,7 +144,6 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict_
         }
     }
     __syncthreads();
-    unsigned long long* out = hist + (size_t)blockIdx.y * cells;
     for (int s = threadIdx.x; s < cells; s += blockDim.x) {
         unsigned long long v = 0ULL;
 #pragma unroll
@@ -155,20 +152,54 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict_
     }
 }
 
+// Transform blockIdx.y of a batch (maps in device memory).
+__global__ void __launch_bounds__(MI_THREADS) k_mi_hist(const MiMap* __restrict__ maps,
+                                                        const float4* __restrict__ rec,
+                                                        long long n,
+                                                        const float* __restrict__ img,
+                                                        unsigned long long* __restrict__ hist) {
+    const MiMap& mp = maps[blockIdx.y];
+    mi_hist_body(mp, rec, n, img, hist + (size_t)blockIdx.y * (mp.bins * mp.bins + mp.bins));
+}
+
+// One transform, its map passed with the launch (no copy ahead of it).
+__global__ void __launch_bounds__(MI_THREADS) k_mi_hist1(const __grid_constant__ MiMap mp,
+                                                         const float4* __restrict__ rec,
+                                                         long long n,
+                                                         const float* __restrict__ img,
+                                                         unsigned long long* __restrict__ hist) {
+    mi_hist_body(mp, rec, n, img, hist);
+}
+
 // ComputeResults (metric/mi.rs:702-768) for histogram blockIdx.x: one thread per cell.
 // out[t*4 + 0] = -MI, [1] = valid samples, [2] = status (0 ok, 1 no valid sample, 2 zero PDF);
 // ratio[t * bins * bins + cell] with want_ratio. The moving bin size is `moving_bin_size`, or
-// mbin_dev[t] when that is given (bin sizes measured on the device).
-__global__ void __launch_bounds__(1024) k_mi_finish(const unsigned long long* __restrict__ hist,
-                                                    int bins, double moving_bin_size,
+// mbin_dev[t] when that is given (bin sizes measured on the device). With `clear` the histogram
+// is zeroed once read, ready for the next evaluation's pass.
+__device__ __forceinline__ void mi_finish_body(const unsigned long long* h, int bins,
+                                               double moving_bin_size, double* ratio, double* o,
+                                               int want_ratio);
+
+__global__ void __launch_bounds__(1024) k_mi_finish(unsigned long long* hist, int bins,
+                                                    double moving_bin_size,
                                                     const double* __restrict__ mbin_dev,
                                                     double* __restrict__ ratio_all,
-                                                    double* __restrict__ out, int want_ratio) {
+                                                    double* __restrict__ out, int want_ratio,
+                                                    int clear) {
     const int cells = bins * bins + bins;
-    const unsigned long long* h = hist + (size_t)blockIdx.x * cells;
-    double* o = out + 4 * blockIdx.x;
-    double* ratio = ratio_all + (size_t)blockIdx.x * bins * bins;
+    unsigned long long* h = hist + (size_t)blockIdx.x * cells;
     if (mbin_dev) moving_bin_size = mbin_dev[blockIdx.x];
+    mi_finish_body(h, bins, moving_bin_size, ratio_all + (size_t)blockIdx.x * bins * bins,
+                   out + 4 * blockIdx.x, want_ratio);
+    if (clear) {
+        __syncthreads();  // every read of the histogram is done
+        for (int s = threadIdx.x; s < cells; s += blockDim.x) h[s] = 0ULL;
+    }
+}
+
+__device__ __forceinline__ void mi_finish_body(const unsigned long long* h, int bins,
+                                               double moving_bin_size, double* ratio, double* o,
+                                               int want_ratio) {
     __shared__ unsigned long long s_int[1024];
     __shared__ double s_d[1024];
     __shared__ double fmarg[MAX_BINS], mmarg[MAX_BINS];
@@ -242,7 +273,7 @@ __global__ void __launch_bounds__(1024) k_mi_finish(const unsigned long long* __
 }
 
 // Derivative moments M[i][j] = sum_s w_s grad_i [r; 1]_j with a fixed-order last-block reduction.
-__global__ void __launch_bounds__(MI_THREADS) k_mi_deriv(const MiMap* __restrict__ maps,
+__global__ void __launch_bounds__(MI_THREADS, 3) k_mi_deriv(const __grid_constant__ MiMap mp,
                                                          const float4* __restrict__ rec,
                                                          long long n,
                                                          const float* __restrict__ img,
@@ -250,7 +281,6 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_deriv(const MiMap* __restrict
                                                          double* __restrict__ partials,
                                                          unsigned int* __restrict__ counter,
                                                          double* __restrict__ mom) {
-    const MiMap& mp = maps[0];
     const int bins = mp.bins;
     __shared__ double sratio[MAX_BINS * MAX_BINS];
     for (int s = threadIdx.x; s < bins * bins; s += blockDim.x) sratio[s] = ratio[s];
@@ -270,20 +300,24 @@ __global__ void __launch_bounds__(MI_THREADS) k_mi_deriv(const MiMap* __restrict
         for (int pm = -1; pm <= 2; ++pm)
             w += bspline3_derivative((double)(mbin + pm) - term) * sratio[fbin * bins + mbin + pm];
         if (w == 0.0) continue;
-        // interp.rs:96-120: half-spacing central difference along the physical axes
+        // interp.rs:96-120: half-spacing central difference along the physical axes. All six
+        // probes are interpolated unconditionally (lin_at_index clamps every corner into the
+        // buffer), so their 48 loads can be in flight together; an axis with a probe outside the
+        // buffer then contributes zero, as the reference's early exit does.
         double g[3];
+        float v1[3], v2[3];
+        bool ok[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            double c1x = c[0] - mp.h[d][0], c1y = c[1] - mp.h[d][1], c1z = c[2] - mp.h[d][2];
-            double c2x = c[0] + mp.h[d][0], c2y = c[1] + mp.h[d][1], c2z = c[2] + mp.h[d][2];
-            g[d] = 0.0;
-            if (!inside_index(c1x, c1y, c1z, mp.m.nx, mp.m.ny, mp.m.nz) ||
-                !inside_index(c2x, c2y, c2z, mp.m.nx, mp.m.ny, mp.m.nz))
-                continue;
-            float v1 = lin_at_index(img, mp.m.nx, mp.m.ny, mp.m.nz, c1x, c1y, c1z);
-            float v2 = lin_at_index(img, mp.m.nx, mp.m.ny, mp.m.nz, c2x, c2y, c2z);
-            g[d] = (double)(v2 - v1) / mp.m.sp[d];
+            const double c1x = c[0] - mp.h[d][0], c1y = c[1] - mp.h[d][1], c1z = c[2] - mp.h[d][2];
+            const double c2x = c[0] + mp.h[d][0], c2y = c[1] + mp.h[d][1], c2z = c[2] + mp.h[d][2];
+            ok[d] = inside_index(c1x, c1y, c1z, mp.m.nx, mp.m.ny, mp.m.nz) &&
+                    inside_index(c2x, c2y, c2z, mp.m.nx, mp.m.ny, mp.m.nz);
+            v1[d] = lin_at_index(img, mp.m.nx, mp.m.ny, mp.m.nz, c1x, c1y, c1z);
+            v2[d] = lin_at_index(img, mp.m.nx, mp.m.ny, mp.m.nz, c2x, c2y, c2z);
         }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d] = ok[d] ? (double)(v2[d] - v1[d]) / mp.m.sp[d] : 0.0;
         if (!(isfinite(g[0]) && isfinite(g[1]) && isfinite(g[2]))) g[0] = g[1] = g[2] = 0.0;
         const double p[4] = {(double)r.x, (double)r.y, (double)r.z, 1.0};
 #pragma unroll
@@ -687,6 +721,7 @@ MiMap make_map(const fw_mi_level* L, const fw_linear_transform* t) {
 int hist_launch_setup(fw_ctx* ctx, size_t smem) {
     (void)ctx;
     FW_CUDA(cudaFuncSetAttribute(k_mi_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FW_CUDA(cudaFuncSetAttribute(k_mi_hist1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     return 0;
 }
 
@@ -702,26 +737,45 @@ unsigned int hist_blocks(const fw_mi_level* L, size_t smem) {
     return (unsigned int)std::max<long long>(1, std::min<long long>(want, (long long)occ * L->ctx->num_sms));
 }
 
-int hist_and_finish(fw_mi_level* L, const fw_linear_transform* ts, int count, bool want_ratio) {
+// The histogram pass and ComputeResults of `count` transforms. One transform's map goes with
+// the launch; a batch's maps are copied ahead. The histograms are zero before the pass (cleared
+// by the previous ComputeResults, or here after an interrupted evaluation) and cleared again by
+// this one's. `map0` (nullable) receives the first transform's map.
+int hist_and_finish(fw_mi_level* L, const fw_linear_transform* ts, int count, bool want_ratio,
+                    MiMap* map0 = nullptr) {
     fw_ctx* ctx = L->ctx;
     const int bins = L->binning.bins;
     const int cells = bins * bins + bins;
-    std::vector<MiMap> maps(count);
-    for (int t = 0; t < count; ++t) maps[t] = make_map(L, &ts[t]);
-    MiMap* d_maps = reinterpret_cast<MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
-    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (sizeof(MiMap) * count + 7) / 8 + 16));
-    d_maps = reinterpret_cast<MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
-    FW_CUDA(cudaMemcpyAsync(d_maps, maps.data(), sizeof(MiMap) * count, cudaMemcpyHostToDevice,
-                            ctx->stream));
-    FW_CUDA(cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells * count, ctx->stream));
-    dim3 grid(L->hist_grid, count);
-    k_mi_hist<<<grid, MI_THREADS, L->hist_smem, ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d,
-                                                              L->d_hist);
-    FW_TRY(check_launch(ctx, "k_mi_hist"));
+    if (!L->hist_clear) {
+        FW_CUDA(cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells * 16, ctx->stream));
+        L->hist_clear = true;
+    }
+    L->hist_clear = false;
+    if (count == 1) {
+        const MiMap mp = make_map(L, &ts[0]);
+        if (map0) *map0 = mp;
+        k_mi_hist1<<<L->hist_grid, MI_THREADS, L->hist_smem, ctx->stream>>>(mp, L->d_rec, L->n,
+                                                                             L->moving->d, L->d_hist);
+        FW_TRY(check_launch(ctx, "k_mi_hist1"));
+    } else {
+        std::vector<MiMap> maps(count);
+        for (int t = 0; t < count; ++t) maps[t] = make_map(L, &ts[t]);
+        if (map0) *map0 = maps[0];
+        FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (sizeof(MiMap) * count + 7) / 8 + 16));
+        MiMap* d_maps = reinterpret_cast<MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
+        FW_CUDA(cudaMemcpyAsync(d_maps, maps.data(), sizeof(MiMap) * count, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        dim3 grid(L->hist_grid, count);
+        k_mi_hist<<<grid, MI_THREADS, L->hist_smem, ctx->stream>>>(d_maps, L->d_rec, L->n,
+                                                                  L->moving->d, L->d_hist);
+        FW_TRY(check_launch(ctx, "k_mi_hist"));
+    }
     k_mi_finish<<<count, 1024, 0, ctx->stream>>>(L->d_hist, bins, L->binning.moving_bin_size,
                                                  nullptr, L->d_ratio, L->d_out,
-                                                 want_ratio ? 1 : 0);
-    return check_launch(ctx, "k_mi_finish");
+                                                 want_ratio ? 1 : 0, 1);
+    FW_TRY(check_launch(ctx, "k_mi_finish"));
+    L->hist_clear = true;
+    return 0;
 }
 
 int check_status(fw_mi_level* L, const double* out) {
@@ -784,7 +838,10 @@ int fw::mi_level_create(fw_ctx* ctx, fw_image* moving, bool own_moving, float4* 
     if (!rc) rc = dev_alloc(ctx, sizeof(unsigned int) * 4, (void**)&L->d_counter);
     if (!rc) {
         cudaError_t e = cudaMemsetAsync(L->d_counter, 0, sizeof(unsigned int) * 4, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells * max_t, ctx->stream);
         if (e != cudaSuccess) rc = cuda_fail(e, "mi level setup");
+        L->hist_clear = true;
     }
     if (!rc) {
         L->hist_smem = mi_hist_smem(binning->bins);
@@ -885,9 +942,9 @@ int fw_mi_level_value_and_derivative(fw_mi_level* L, const fw_linear_transform* 
                                      double* value, double* derivative) {
     FW_CHECK(L && t && value && derivative, "null argument");
     fw_ctx* ctx = L->ctx;
-    FW_TRY(hist_and_finish(L, t, 1, true));
-    const MiMap* d_maps = reinterpret_cast<const MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
-    k_mi_deriv<<<L->blocks, MI_THREADS, 0, ctx->stream>>>(d_maps, L->d_rec, L->n, L->moving->d,
+    MiMap mp;
+    FW_TRY(hist_and_finish(L, t, 1, true, &mp));
+    k_mi_deriv<<<L->blocks, MI_THREADS, 0, ctx->stream>>>(mp, L->d_rec, L->n, L->moving->d,
                                                           L->d_ratio, L->d_part, L->d_counter,
                                                           L->d_mom);
     FW_TRY(check_launch(ctx, "k_mi_deriv"));
@@ -929,7 +986,7 @@ int fw_mi_level_time(fw_mi_level* L, const fw_linear_transform* t, int32_t reps,
     FW_TRY(fw_mi_level_value_and_derivative(L, t, &v, d));
     const int bins = L->binning.bins;
     const int cells = bins * bins + bins;
-    const MiMap* d_maps = reinterpret_cast<const MiMap*>(ctx->d_scratch + SLOT_PARTIALS);
+    const MiMap mp = make_map(L, t);
     cudaEvent_t a = nullptr, b = nullptr;
     if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
         if (a) cudaEventDestroy(a);
@@ -941,18 +998,16 @@ int fw_mi_level_time(fw_mi_level* L, const fw_linear_transform* t, int32_t reps,
             if (kind == 0) {
                 FW_CUDA(cudaMemsetAsync(L->d_hist, 0, sizeof(unsigned long long) * cells,
                                         ctx->stream));
-                const size_t sh = mi_hist_smem(bins);
-                FW_TRY(hist_launch_setup(ctx, sh));
-                k_mi_hist<<<dim3(hist_blocks(L, sh), 1), MI_THREADS, sh, ctx->stream>>>(
-                    d_maps, L->d_rec, L->n, L->moving->d, L->d_hist);
-                return check_launch(ctx, "k_mi_hist");
+                k_mi_hist1<<<L->hist_grid, MI_THREADS, L->hist_smem, ctx->stream>>>(
+                    mp, L->d_rec, L->n, L->moving->d, L->d_hist);
+                return check_launch(ctx, "k_mi_hist1");
             }
             if (kind == 1) {
                 k_mi_finish<<<1, 1024, 0, ctx->stream>>>(L->d_hist, bins, L->binning.moving_bin_size,
-                                                         nullptr, L->d_ratio, L->d_out, 1);
+                                                         nullptr, L->d_ratio, L->d_out, 1, 0);
                 return check_launch(ctx, "k_mi_finish");
             }
-            k_mi_deriv<<<L->blocks, MI_THREADS, 0, ctx->stream>>>(d_maps, L->d_rec, L->n,
+            k_mi_deriv<<<L->blocks, MI_THREADS, 0, ctx->stream>>>(mp, L->d_rec, L->n,
                                                                   L->moving->d, L->d_ratio,
                                                                   L->d_part, L->d_counter,
                                                                   L->d_mom);
@@ -970,6 +1025,7 @@ int fw_mi_level_time(fw_mi_level* L, const fw_linear_transform* t, int32_t reps,
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    L->hist_clear = false;  // the timed passes leave a histogram behind
     // algorithmic bytes per pass: the 16-byte sample records plus the moving image's gathers,
     // at most the whole image and at most one 8-corner gather per sample (32 bytes)
     const double S = (double)L->n, Nm = (double)L->moving->grid.count();
@@ -1147,7 +1203,7 @@ int enqueue_dense_mi_pair(fw_ctx* ctx, const fw_image* f, const fw_image* m, con
                                                           sc->hist);
     FW_TRY(check_launch(ctx, "k_dense_hist"));
     k_mi_finish<<<2, 1024, 0, ctx->stream>>>(sc->hist, bins, 0.0, sc->st->mbin, sc->ratio,
-                                             sc->out, 1);
+                                             sc->out, 1, 0);
     FW_TRY(check_launch(ctx, "k_mi_finish"));
     DenseArgs da;
     std::memset(&da, 0, sizeof(da));
