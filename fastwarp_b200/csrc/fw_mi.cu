@@ -180,6 +180,12 @@ __device__ __forceinline__ void mi_finish_body(const unsigned long long* h, int 
                                                double moving_bin_size, double* ratio, double* o,
                                                int want_ratio);
 
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __global__ void __launch_bounds__(1024) k_mi_finish(unsigned long long* hist, int bins,
                                                     double moving_bin_size,
                                                     const double* __restrict__ mbin_dev,
@@ -200,32 +206,34 @@ __global__ void __launch_bounds__(1024) k_mi_finish(unsigned long long* hist, in
 __device__ __forceinline__ void mi_finish_body(const unsigned long long* h, int bins,
                                                double moving_bin_size, double* ratio, double* o,
                                                int want_ratio) {
-    __shared__ unsigned long long s_int[1024];
-    __shared__ double s_d[1024];
+    __shared__ unsigned long long s_js[32], s_vs[32];
+    __shared__ double s_c[32];
     __shared__ double fmarg[MAX_BINS], mmarg[MAX_BINS];
     __shared__ double norm_s;
     __shared__ unsigned long long valid_s;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31, wp = t >> 5, nw = blockDim.x >> 5;
     const int nc = bins * bins;
-    // exact integer totals: the joint sum and the number of valid samples
+    // exact integer totals: the joint sum and the number of valid samples (warp shuffles, then
+    // the first warp over the warps' sums)
     unsigned long long js = 0, vs = 0;
     for (int s = t; s < nc; s += blockDim.x) js += h[s];
     for (int s = t; s < bins; s += blockDim.x) vs += h[nc + s];
-    s_int[t] = js;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (t < w) s_int[t] += s_int[t + w];
-        __syncthreads();
+    js = warp_sum_u64(js);
+    vs = warp_sum_u64(vs);
+    if (lane == 0) {
+        s_js[wp] = js;
+        s_vs[wp] = vs;
     }
-    if (t == 0) norm_s = (double)s_int[0] / FIXED;
     __syncthreads();
-    s_int[t] = vs;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (t < w) s_int[t] += s_int[t + w];
-        __syncthreads();
+    if (wp == 0) {
+        unsigned long long a = lane < nw ? s_js[lane] : 0ULL, b = lane < nw ? s_vs[lane] : 0ULL;
+        a = warp_sum_u64(a);
+        b = warp_sum_u64(b);
+        if (lane == 0) {
+            norm_s = (double)a / FIXED;
+            valid_s = b;
+        }
     }
-    if (t == 0) valid_s = s_int[0];
     __syncthreads();
     const double pdf_sum = norm_s;
     const unsigned long long num_valid = valid_s;
@@ -259,14 +267,15 @@ __device__ __forceinline__ void mi_finish_body(const unsigned long long* h, int 
         }
         if (want_ratio) ratio[t] = r;
     }
-    s_d[t] = contrib;
+    // the sum of the cells' terms in a fixed order: each warp's butterfly, then the first warp's
+    // over the warps in order
+    contrib = warp_sum_d(contrib);
+    if (lane == 0) s_c[wp] = contrib;
     __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (t < w) s_d[t] += s_d[t + w];
-        __syncthreads();
-    }
+    double total = 0.0;
+    if (wp == 0) total = warp_sum_d(lane < nw ? s_c[lane] : 0.0);
     if (t == 0) {
-        o[0] = -s_d[0];
+        o[0] = -total;
         o[1] = (double)num_valid;
         o[2] = 0.0;
     }
