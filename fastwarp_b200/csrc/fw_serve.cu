@@ -17,6 +17,7 @@
 #include <string>
 #include <unordered_map>
 #include <thread>
+#include <list>
 #include <vector>
 
 #include "../../include/fastwarp_serve.h"
@@ -30,18 +31,27 @@ namespace {
 // Pinned host buffers kept by size for reuse (cudaHostAlloc is slow and synchronises the
 // device): the staging of host inputs and the host results, so both copies run as DMA at full
 // link speed without a bounce through pageable memory. Process-wide: results outlive servers.
+// Requests of many grid sizes would leave a buffer of every size behind: past kMaxKept bytes the
+// buffers returned longest ago are released.
 struct PinnedPool {
+    static constexpr size_t kMaxKept = (size_t)8 << 30;
+    struct Kept {
+        size_t bytes;
+        void* p;
+    };
     std::mutex mu;
-    std::unordered_multimap<size_t, void*> free;
+    std::list<Kept> free;  // in the order they were returned
+    size_t kept = 0;
     void* get(size_t bytes) {
         {
             std::lock_guard<std::mutex> lock(mu);
-            auto it = free.find(bytes);
-            if (it != free.end()) {
-                void* p = it->second;
-                free.erase(it);
-                return p;
-            }
+            for (auto it = free.rbegin(); it != free.rend(); ++it)
+                if (it->bytes == bytes) {
+                    void* p = it->p;
+                    kept -= bytes;
+                    free.erase(std::next(it).base());
+                    return p;
+                }
         }
         void* p = nullptr;
         if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
@@ -52,8 +62,17 @@ struct PinnedPool {
     }
     void put(void* p, size_t bytes) {
         if (!p) return;
-        std::lock_guard<std::mutex> lock(mu);
-        free.emplace(bytes, p);
+        std::list<Kept> drop;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            free.push_back(Kept{bytes, p});
+            kept += bytes;
+            while (kept > kMaxKept && free.size() > 1) {
+                kept -= free.front().bytes;
+                drop.splice(drop.end(), free, free.begin());
+            }
+        }
+        for (auto& k : drop) cudaFreeHost(k.p);
     }
 };
 

@@ -85,7 +85,9 @@ def test_sampled_mi_at_the_config2_finest_level_matches_the_oracle(backend):
     the oracle on the same samples: value 1e-5 and derivative 5e-4 relative, valid-sample counts
     exact, for the phantom's own affine map and an Euler transform. The level the product
     prepares itself from device images (fw_mi_level_prepare_regular: sampling, binning and
-    fixed bins on the host) evaluates the same value on the same number of samples."""
+    fixed bins on the device) holds the oracle's prepared set -- the same 2.13 M points in the
+    same order, every fixed bin and the binning equal -- and evaluates the same value on the same
+    number of samples."""
     from fastwarp_b200.phantoms import head_pair
     g, fixed, mg, moving, initial = head_pair()
     og = O.make_grid(tuple(g.size), tuple(g.spacing), tuple(g.origin))
@@ -111,6 +113,13 @@ def test_sampled_mi_at_the_config2_finest_level_matches_the_oracle(backend):
         assert level.num_valid() == wn
     fi, mi = backend.upload_image(g, fixed), backend.upload_image(mg, moving)
     own = CudaLinearEngine(backend).prepare_level_regular(g, fi, mi, 0.25, 1, 32)
+    dpts, dfb, db = own.samples()
+    assert len(dfb) == len(fbin)
+    assert np.array_equal(dfb, fbin)
+    assert np.abs(dpts - kept).max() < 1e-4  # float32 offsets from the cloud centre
+    for k in ("fixed_min", "fixed_max", "moving_min", "moving_max", "fixed_bin_size",
+              "moving_bin_size", "fixed_normalized_min", "moving_normalized_min"):
+        assert getattr(db, k) == getattr(b, k), k
     t0 = linear_transform(**cases[0])
     assert abs(own.value(t0) - level.value(t0)) <= 1e-12 * abs(level.value(t0))
     assert own.num_valid() == level.num_valid()
