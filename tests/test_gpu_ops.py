@@ -399,3 +399,33 @@ def test_freed_buffers_are_reused_and_released_on_request(backend):
     b.free()
     backend.release_idle_buffers()
     assert backend.cached_bytes() == 0
+
+
+def test_buffers_of_sizes_no_longer_used_go_back_to_the_pool(backend):
+    """A stream of requests of many grid sizes must not leave a buffer of every size in a
+    context's cache: on a miss that would take the context past its largest working set (at
+    least 1 GB), buffers idle in the cache for over a second go back to the pool; buffers freed
+    more recently (the same shapes about to repeat) stay."""
+    import time
+
+    from fastwarp_b200.backend import CudaBackend
+
+    def nbytes(n):  # a field's cached size: three planes of a 64-voxel stride, 4 KB pages
+        ps = (n ** 3 + 63) // 64 * 64
+        return (3 * ps * 4 + 4095) // 4096 * 4096
+
+    with CudaBackend(backend.device) as b:  # a fresh context: its largest working set is its own
+        a = b.zero_field(make_grid((292, 292, 292)))  # ~0.3 GB
+        a.free()
+        assert b.cached_bytes() == nbytes(292)
+        time.sleep(1.2)
+        c = b.zero_field(make_grid((422, 422, 422)))  # ~0.9 GB: past 1 GB with the idle buffer
+        assert b.cached_bytes() == 0  # the idle buffer went back to the pool
+        c.free()
+        assert b.cached_bytes() == nbytes(422)
+        d = b.zero_field(make_grid((322, 322, 322)))  # ~0.4 GB, at once: the 0.9 GB one stays
+        assert b.cached_bytes() == nbytes(422)
+        d.free()
+        e = b.zero_field(make_grid((422, 422, 422)))  # the kept buffer serves the same shape
+        assert b.cached_bytes() == nbytes(322)
+        e.free()
