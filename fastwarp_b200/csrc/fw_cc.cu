@@ -38,10 +38,13 @@ struct CcArgs {
 };
 
 // Shared-memory layout (dynamic): the z-window sums of every halo column, [5][HY*HX] double
-// (+ [HY*HX] int counts with a mask); y sums [5][TY][HX] double
-// (+ [TY][HX] int counts); the raw voxels of the tile with a one-voxel halo for the last D
-// slices, [D][TY+2][TX+2] float2 (f, m), for the centre values and the central differences;
-// block-reduction space.
+// (+ [HY*HX] int counts with a mask); y sums [5][HX][TY+1] double, column-major with an odd
+// column stride (+ [TY][HX] int counts); the raw voxels of the tile with a one-voxel halo for the
+// last D slices, [D][TY+2][TX+2] float2 (f, m), for the centre values and the central
+// differences; the x sums of the tile's voxels [5][TX][TY+1] double; block-reduction space.
+// The odd strides keep every pass free of bank conflicts: the y pass stores consecutive columns,
+// the x pass reads eight rows of two column groups per half-warp, and each voxel's thread reads
+// its own row of a column.
 template <int R, int TY, bool MK>
 struct Layout {
     static constexpr int HX = TX + 2 * R;
@@ -56,10 +59,16 @@ struct Layout {
     // before step k's first barrier, while slow threads may still read step k-1's outputs
     static constexpr int D = R + 3;
     static constexpr size_t zs1 = sizeof(double) * 5 * HC + (MK ? sizeof(int) * HC : 0);
-    static constexpr size_t xs_bytes = sizeof(double) * 5 * TY * HX;  // y sums [5][TY][HX]
+    static constexpr int YS = TY + 1;                                  // odd: TY is even
+    static constexpr int XG = 8;                                       // x outputs per item
+    static_assert(TX % XG == 0, "whole x groups");
+    static constexpr size_t xs_bytes = sizeof(double) * 5 * HX * YS;  // y sums [5][HX][YS]
     static constexpr size_t xc_bytes = MK ? sizeof(int) * TY * HX : 0;
     static constexpr size_t raw_bytes = sizeof(float2) * D * RXY;
-    static constexpr size_t bytes = zs1 + xs_bytes + xc_bytes + raw_bytes + 64 * sizeof(double);
+    static constexpr size_t sx_bytes = sizeof(double) * 5 * TX * YS;  // x sums [5][TX][YS]
+    static constexpr size_t sx_off = zs1 + xs_bytes + xc_bytes + raw_bytes;
+    static constexpr size_t red_off = sx_off + sx_bytes;
+    static constexpr size_t bytes = red_off + 64 * sizeof(double);
 };
 
 // MK: masked (cpu/mod.rs:134-163 -> evaluate_masked with Some(valid)): a voxel counts only where
@@ -143,6 +152,7 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
     T* xs = reinterpret_cast<T*>(smem + L::zs1);
     int* xc = reinterpret_cast<int*>(smem + L::zs1 + L::xs_bytes);
     float2* raw = reinterpret_cast<float2*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes);
+    T* sx = reinterpret_cast<T*>(smem + L::sx_off);
 
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
     const int tid = threadIdx.x;
@@ -248,7 +258,7 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
         for (int s = tid; s < L::HX * (TY / 2); s += L::NT) {
             const int rp = s / L::HX, hx = s - rp * L::HX;
             const int base = 2 * rp * L::HX + hx;
-            T* o = xs + 2 * rp * L::HX + hx;
+            T* o = xs + hx * L::YS + 2 * rp;
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
                 const T* col = zs + q * L::HC + base;
@@ -259,8 +269,8 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
                     e = Acc::add(e, col[(t + 1) * L::HX]);
                 }
                 c = Acc::add(c, e);
-                o[q * TY * L::HX] = Acc::add(c, col[0]);
-                o[q * TY * L::HX + L::HX] = Acc::add(c, col[(2 * R + 1) * L::HX]);
+                o[q * L::HX * L::YS] = Acc::add(c, col[0]);
+                o[q * L::HX * L::YS + 1] = Acc::add(c, col[(2 * R + 1) * L::HX]);
             }
             if constexpr (MK) {
                 const int* ccol = zc + base;
@@ -272,20 +282,33 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
             }
         }
         __syncthreads();
+        // x pass: each item makes the sums of XG consecutive outputs of one row from one window
+        // of XG + 2r columns (each output's sum in the same order as alone: even taps, odd taps,
+        // the last); a half-warp's items are eight rows of two column groups
+        for (int s = tid; s < 5 * TY * (TX / L::XG); s += L::NT) {
+            const int q = s / (TY * (TX / L::XG)), rr = s - q * (TY * (TX / L::XG));
+            const int row = rr % TY, g = rr / TY;
+            const T* in = xs + (q * L::HX + g * L::XG) * L::YS + row;
+            T v[L::XG + 2 * R];
+#pragma unroll
+            for (int t = 0; t < L::XG + 2 * R; ++t) v[t] = in[t * L::YS];
+            T* out = sx + (q * TX + g * L::XG) * L::YS + row;
+#pragma unroll
+            for (int j = 0; j < L::XG; ++j) {
+                T e = Acc::zero(), o = Acc::zero();
+#pragma unroll
+                for (int t = 0; t < 2 * R; t += 2) {
+                    e = Acc::add(e, v[j + t]);
+                    o = Acc::add(o, v[j + t + 1]);
+                }
+                out[j * L::YS] = Acc::add(Acc::add(e, o), v[j + 2 * R]);
+            }
+        }
+        __syncthreads();
         if (!own) continue;
-        // x pass for the thread's own voxel (a warp reads one row: consecutive banks)
         double S[5];
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            const T* row = xs + (q * TY + ty) * L::HX + tx;
-            T s = Acc::zero(), s2 = Acc::zero();
-#pragma unroll
-            for (int t = 0; t < 2 * R; t += 2) {
-                s = Acc::add(s, row[t]);
-                s2 = Acc::add(s2, row[t + 1]);
-            }
-            S[q] = Acc::value(Acc::add(Acc::add(s, s2), row[2 * R]));
-        }
+        for (int q = 0; q < 5; ++q) S[q] = Acc::value(sx[(q * TX + tx) * L::YS + ty]);
 
         // ---- output voxel (x, y, z) ----
         const long long l = (long long)z * sxy + (long long)y * nx + x;
@@ -449,8 +472,7 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
                                                      double* __restrict__ result, int want_norms) {
     using L = Layout<R, TY, MK>;
     extern __shared__ __align__(16) unsigned char smem[];
-    double* red = reinterpret_cast<double*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes +
-                                            L::raw_bytes);
+    double* red = reinterpret_cast<double*>(smem + L::red_off);
     double acc[4];
     cc_tile<R, TY, MK, Acc>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem, fimg, mimg, vimg,
                             d_fixed, d_moving, want_norms, acc);
@@ -476,8 +498,7 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair_batch(
     int want_norms) {
     using L = Layout<R, TY, false>;
     extern __shared__ __align__(16) unsigned char smem[];
-    double* red = reinterpret_cast<double*>(smem + L::zs1 + L::xs_bytes + L::xc_bytes +
-                                            L::raw_bytes);
+    double* red = reinterpret_cast<double*>(smem + L::red_off);
     const int work = *Lb.count * Lb.tiles;
     const int gx = (a.g.nx + TX - 1) / TX, gy = (a.g.ny + TY - 1) / TY;
     for (int w = blockIdx.x; w < work; w += gridDim.x) {
