@@ -52,7 +52,6 @@ struct Layout {
     static constexpr int HC = HX * HY;           // halo columns of the tile
     static constexpr int NT = TX * TY;
     static constexpr int CPT = (HC + NT - 1) / NT;  // halo columns per thread
-    static_assert(TY % 2 == 0, "the y pass makes output rows in pairs");
     static constexpr int NP = MK ? 4 : 3;  // block partials: cc, |dF|^2, |dM|^2 (+ valid voxels)
     static constexpr int RX = TX + 2, RY = TY + 2, RXY = RX * RY;
     // raw slices kept: the output at step k reads slices k-R-1 .. k-R+1, and slice k is written
@@ -80,9 +79,9 @@ struct Layout {
 // shared memory, where the y pass reads them) one slice per step: the entering slice is added
 // and the leaving slice (read again, from L2) subtracted -- before the step's first barrier, which
 // the previous step's y pass has passed. Products of float32 voxels are exact in float64, so the
-// running sums carry no drift beyond float64 rounding. The y pass makes column sums of them two
-// output rows at a time, and each thread's x pass finishes its own
-// voxel's window sums. The kernel is bound by shared-memory bandwidth, which this order spends
+// running sums carry no drift beyond float64 rounding. The y pass makes column sums of them four
+// output rows at a time, the x pass eight outputs of a row at a time, and each thread then reads
+// its own voxel's window sums. The kernel is bound by shared-memory bandwidth, which this order spends
 // least on: the shared-tap pairs sit in the pass over the wider (halo) extent, and both passes
 // read along consecutive banks.
 #ifndef FW_CC_MIN_BLOCKS
@@ -252,33 +251,43 @@ __device__ __forceinline__ void cc_tile(const CcArgs& a, int bx, int by, int bz,
         if (z < z0) continue;  // the window is still filling (uniform across the CTA)
 
         __syncthreads();  // z sums visible; the previous x pass is done with the y sums
-        // y pass: each item makes the sums of two adjacent output rows of one halo column from
-        // one window of 2r + 2 rows (the 2r in the middle are shared); a warp's items are
-        // consecutive columns, so its loads fall on distinct banks
-        for (int s = tid; s < L::HX * (TY / 2); s += L::NT) {
-            const int rp = s / L::HX, hx = s - rp * L::HX;
-            const int base = 2 * rp * L::HX + hx;
-            T* o = xs + hx * L::YS + 2 * rp;
+        // y pass: each item makes four output rows of one halo column for one of the five window
+        // sums from one window of 2r + 4 rows, as two pairs of adjacent rows whose 2r middle rows are
+        // shared (each pair's sums in the same order as alone); a warp's items are consecutive
+        // columns, so its loads and stores fall on distinct banks
+        static_assert(TY % 4 == 0, "the y pass makes output rows in fours");
+        for (int s = tid; s < 5 * L::HX * (TY / 4); s += L::NT) {
+            const int q = s / (L::HX * (TY / 4)), rr = s - q * (L::HX * (TY / 4));
+            const int rq = rr / L::HX, hx = rr - rq * L::HX;
+            const T* col = zs + q * L::HC + 4 * rq * L::HX + hx;
+            T v[2 * R + 4];
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                const T* col = zs + q * L::HC + base;
+            for (int t = 0; t < 2 * R + 4; ++t) v[t] = col[t * L::HX];
+            T* o = xs + (q * L::HX + hx) * L::YS + 4 * rq;
+#pragma unroll
+            for (int p2 = 0; p2 < 4; p2 += 2) {
                 T c = Acc::zero(), e = Acc::zero();  // two partial sums: half-length add chains
 #pragma unroll
                 for (int t = 1; t <= 2 * R; t += 2) {
-                    c = Acc::add(c, col[t * L::HX]);
-                    e = Acc::add(e, col[(t + 1) * L::HX]);
+                    c = Acc::add(c, v[p2 + t]);
+                    e = Acc::add(e, v[p2 + t + 1]);
                 }
                 c = Acc::add(c, e);
-                o[q * L::HX * L::YS] = Acc::add(c, col[0]);
-                o[q * L::HX * L::YS + 1] = Acc::add(c, col[(2 * R + 1) * L::HX]);
+                o[p2] = Acc::add(c, v[p2]);
+                o[p2 + 1] = Acc::add(c, v[p2 + 2 * R + 1]);
             }
             if constexpr (MK) {
-                const int* ccol = zc + base;
-                int cn = 0;
+                if (q == 0) {
+                    const int* ccol = zc + 4 * rq * L::HX + hx;
 #pragma unroll
-                for (int t = 1; t <= 2 * R; ++t) cn += ccol[t * L::HX];
-                xc[2 * rp * L::HX + hx] = cn + ccol[0];
-                xc[(2 * rp + 1) * L::HX + hx] = cn + ccol[(2 * R + 1) * L::HX];
+                    for (int p2 = 0; p2 < 4; p2 += 2) {
+                        int cn = 0;
+#pragma unroll
+                        for (int t = 1; t <= 2 * R; ++t) cn += ccol[(p2 + t) * L::HX];
+                        xc[(4 * rq + p2) * L::HX + hx] = cn + ccol[p2 * L::HX];
+                        xc[(4 * rq + p2 + 1) * L::HX + hx] = cn + ccol[(p2 + 2 * R + 1) * L::HX];
+                    }
+                }
             }
         }
         __syncthreads();
