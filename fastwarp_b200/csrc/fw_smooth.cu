@@ -385,7 +385,7 @@ __device__ __forceinline__ float smooth_z_tile(const SmoothArgs& a, int zb, int 
 // blockIdx.x: z segment (fastest, so neighbouring segments share their halo rows in L2),
 // blockIdx.y: 32 columns in x, blockIdx.z: 8 rows in y.
 template <int R>
-__global__ void __launch_bounds__(256) k_smooth_z(SmoothArgs a, const float* __restrict__ tmp,
+__global__ void __launch_bounds__(256, R <= 6 ? 3 : 2) k_smooth_z(SmoothArgs a, const float* __restrict__ tmp,
                                                   long long ps_tmp, const float* in,
                                                   float* out,
                                                   unsigned int* __restrict__ max_bits) {
