@@ -697,6 +697,8 @@ def batch_leg(b, rank, n_subjects=48):
             "batched_over_sequential": round(t_seq * n_subjects / t_batch, 3),
             "batched_over_served": round(t_srv / t_batch, 3),
             "level_ms": [round(x, 2) for x in res.level_ms],
+            "prepare_ms": [round(x, 2) for x in res.prepare_ms],
+            "finish_ms": round(res.finish_ms, 2),
             "tuning": res.tuning, "device_bytes": res.device_bytes,
             "moving_dims_min": [min(x[a] for x in sizes) for a in range(3)],
             "moving_dims_max": [max(x[a] for x in sizes) for a in range(3)],

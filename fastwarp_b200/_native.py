@@ -150,7 +150,8 @@ class BatchTuning(C.Structure):
 class BatchReport(C.Structure):
     _fields_ = [("subjects", C.c_int32), ("levels", C.c_int32),
                 ("tuning", BatchTuning * MAX_LEVELS), ("level_ms", C.c_double * MAX_LEVELS),
-                ("device_bytes", C.c_uint64)]
+                ("device_bytes", C.c_uint64), ("prepare_ms", C.c_double * MAX_LEVELS),
+                ("finish_ms", C.c_double)]
 
 
 class Stats(C.Structure):

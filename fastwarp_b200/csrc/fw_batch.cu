@@ -525,8 +525,9 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
         if (ms < bestms) bestms = ms, best.smooth_bps = bps;
     }
     best.smooth_ms = bestms;
-    // the composition, in place on a cleared scratch field (dM) with sF as the update
-    FW_CUDA(cudaMemsetAsync(L.dM.p, 0, L.dM.bytes, ctx->stream));
+    // the composition, in place on a scratch copy (dM) of the level's field F with sF as the
+    // update: the gathers land where the iteration's will
+    FW_CUDA(cudaMemcpyAsync(L.dM.p, L.F.p, L.dM.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     bestms = DBL_MAX;
     for (int zc : gz) {
         for (int bps : {2, 4, 8}) {
@@ -554,7 +555,9 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
         }
     }
     best.measure_ms = bestms;
-    // a body with its next measurement, on a cleared scratch inverse (dM) that keeps iterating
+    // a body with its next measurement, on a scratch copy (dM) of the level's inverse that keeps
+    // iterating
+    FW_CUDA(cudaMemcpyAsync(L.dM.p, L.Fi.p, L.dM.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     const fw_invert_params forever = {1 << 30, -1.0, -1.0, 1};
     FW_TRY(launch_inv_measure_batch(ctx, L.grid, L.ps, best.meas_zc,
                                     run.sc.list(inv_measure_tiles(L.grid, best.meas_zc)),
@@ -819,6 +822,7 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
     std::unique_ptr<BatchLevel> prev, cur;
     for (int level = 0; level < r->levels; ++level) {
         if (cancel_requested(ctx)) return fail(FW_ERR_CANCELLED, "registration cancelled");
+        const auto t_level = std::chrono::steady_clock::now();
         HostGrid lg;
         FW_TRY(level_grid_of(r, fg, level, lg));
         cur.reset(new BatchLevel());
@@ -829,6 +833,11 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
         if (pps > run.part_stride) {
             run.part_stride = pps;
             FW_TRY(run.partials.alloc(ctx, sizeof(double) * (size_t)pps * B));
+        }
+        if (report) {
+            FW_TRY(sync(ctx));
+            report->prepare_ms[level] =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_level).count();
         }
         // the tile shapes and grids of this level: cached, tuned, or the defaults
         Tuning t;
@@ -889,6 +898,7 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
         prev = std::move(cur);
     }
     // every subject's status, records and final fields (syn.rs:969-970)
+    const auto t_finish = std::chrono::steady_clock::now();
     std::vector<SynDev> h((size_t)B);
     FW_CUDA(cudaMemcpyAsync(h.data(), run.sc.syn, sizeof(SynDev) * B, cudaMemcpyDeviceToHost,
                             ctx->stream));
@@ -926,7 +936,11 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
         inverses[b] = iw;
     }
     if (report) report->device_bytes = peak;
-    return sync(ctx);
+    FW_TRY(sync(ctx));
+    if (report)
+        report->finish_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_finish).count();
+    return 0;
 }
 
 }  // namespace fw

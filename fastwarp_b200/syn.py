@@ -363,6 +363,8 @@ class BatchResult:
     tuning: list
     level_ms: list
     device_bytes: int
+    prepare_ms: list = None
+    finish_ms: float = 0.0
 
 
 def run_syn_batch(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
@@ -411,4 +413,5 @@ def run_syn_batch(backend: CudaBackend, recipe: SynRecipe, fixed: List[Image],
         tuning.append({k: (list(getattr(t, k)) if k in ("grid_size", "kernel_ms") else getattr(t, k))
                        for k, _ in N.BatchTuning._fields_})
     return BatchResult(out, list(statuses), tuning, list(rep.level_ms[:r.levels]),
-                       int(rep.device_bytes))
+                       int(rep.device_bytes), list(rep.prepare_ms[:r.levels]),
+                       float(rep.finish_ms))

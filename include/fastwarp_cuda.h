@@ -666,6 +666,8 @@ typedef struct fw_batch_report {
     fw_batch_tuning tuning[FW_MAX_LEVELS];
     double level_ms[FW_MAX_LEVELS]; /* device time of each level's graph (CUDA events) */
     uint64_t device_bytes;          /* device memory the batch held at its largest level */
+    double prepare_ms[FW_MAX_LEVELS]; /* wall time of each level's buffers and smoothed sources */
+    double finish_ms;               /* wall time of the statuses, records and output fields */
 } fw_batch_report;
 
 /* No counterpart in the reference, whose nearest path registers several moving images to one
