@@ -145,12 +145,16 @@ int dev_alloc(fw_ctx* ctx, size_t bytes, void** out) {
             ctx->cached_bytes -= sz;
         } else if (!ctx->capturing) {
             // Requests of many grid sizes (a served stream) would otherwise leave a buffer of
-            // every size they used in the cache. On a miss that would take the context past its
-            // largest working set (at least 1 GB), buffers idle in the cache for over a second go
-            // back to the pool, oldest first, which reuses their memory for any size; buffers
-            // freed more recently (the same shapes about to repeat) stay. Not during a capture,
-            // where a free would become a graph node.
-            const uint64_t cap = std::max<uint64_t>(ctx->stats.peak_device_bytes, (uint64_t)1 << 30);
+            // every size they used in the cache. On a miss that would take the context past
+            // twice its largest working set (at least 1 GB), buffers idle in the cache for over a
+            // second go back to the pool, oldest first, which reuses their memory for any size;
+            // buffers freed more recently (the same shapes about to repeat) stay. Twice: a run
+            // whose levels have working sets of different sizes keeps them all for its next run
+            // (a pool that gave the coarse levels' memory to the finest level would have to grow
+            // for the coarse levels again). Not during a capture, where a free would become a
+            // graph node.
+            const uint64_t cap =
+                std::max<uint64_t>(2 * ctx->stats.peak_device_bytes, (uint64_t)1 << 30);
             const auto now = std::chrono::steady_clock::now();
             while (!ctx->cache_lru.empty() &&
                    ctx->live_bytes.load() + ctx->cached_bytes + sz > cap) {

@@ -403,9 +403,9 @@ def test_freed_buffers_are_reused_and_released_on_request(backend):
 
 def test_buffers_of_sizes_no_longer_used_go_back_to_the_pool(backend):
     """A stream of requests of many grid sizes must not leave a buffer of every size in a
-    context's cache: on a miss that would take the context past its largest working set (at
-    least 1 GB), buffers idle in the cache for over a second go back to the pool; buffers freed
-    more recently (the same shapes about to repeat) stay."""
+    context's cache: on a miss that would take the context past twice its largest working set
+    (at least 1 GB), buffers idle in the cache for over a second go back to the pool; buffers
+    freed more recently (the same shapes about to repeat) stay."""
     import time
 
     from fastwarp_b200.backend import CudaBackend
