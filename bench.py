@@ -92,8 +92,7 @@ def time_kernels(b, fimg, mimg, reps):
     by = (C.c_double * 7)()
     N.check(N.lib().fw_time_kernels(b.ctx, fimg.handle, mimg.handle, C.c_int32(4),
                                     C.c_double(3.0), C.c_int32(reps), ms, by))
-    names = ["warp", "cc_pair", "smooth", "compose", "inv_measure", "inv_body_last",
-             "inv_body_next"]
+    names = ["warp", "cc_pair", "smooth", "compose", "inv_body", "inv_bound", "inv_fix"]
     return {k: (ms[i], by[i]) for i, k in enumerate(names)}
 
 
@@ -365,10 +364,9 @@ def run_ours(args, rank, world, local):
     # per-kernel roofline at the finest level (CUDA events on the engine stream)
     log("kernel timing")
     t = time_kernels(b, fi, b.upload_image(g, fixed), 20)
-    # launches per iteration (ncu launch list of a registration: 4 inversions, each one
-    # measurement and one last body, plus 0.4 bodies per iteration that measure again)
-    per_iter = {"warp": 2, "cc_pair": 1, "smooth": 2, "compose": 2, "inv_measure": 4,
-                "inv_body_last": 4, "inv_body_next": 0.4}
+    # launches per iteration (ncu launch list of a registration: 4 inversions of 1.08 bodies on
+    # average, each body its bound, step and fix kernels; inv_body times all three)
+    per_iter = {"warp": 2, "cc_pair": 1, "smooth": 2, "compose": 2, "inv_body": 4.3}
     dom = max(per_iter, key=lambda k: t[k][0] * per_iter[k])
     ms, by = t[dom]
     peak, src = peaks()

@@ -150,12 +150,13 @@ struct Tuning {
     int warp_zc = 16, warp_bps = 4;
     int comp_zc = 16, comp_bps = 4;
     int cc_zc = 0, cc_bps = 3;  // cc_zc 0: the whole column
-    int meas_zc = 16, meas_bps = 4;
-    int body_bps = 4;
+    int step_zc = 1, step_bps = 3;  // inversion step: tiles per block (planned, not tuned)
+    int fix_bps = 2;                 // inversion fix kernel
     int smooth_bps = 4;
     double tune_ms = 0.0;
-    // the timed best of each batched kernel (one launch over all subjects, ms)
-    double warp_ms = 0, cc_ms = 0, smooth_ms = 0, compose_ms = 0, measure_ms = 0, body_ms = 0;
+    // the timed best of each batched kernel (one launch over all subjects, ms; body: the whole
+    // inversion body, bound + step + fix)
+    double warp_ms = 0, cc_ms = 0, smooth_ms = 0, compose_ms = 0, step_ms = 0, body_ms = 0;
     bool cached = false;
 };
 
@@ -291,15 +292,12 @@ std::vector<int> cc_zchunks(int nz, int radius) {
 }
 
 // Partials per subject: the most any batched reduction of the level needs under any candidate
-// (and the defaults): 3 doubles per CC tile, 2 per measurement tile or body virtual block.
-long long partials_per_subject(fw_ctx* ctx, const HostGrid& g, int radius) {
+// (and the defaults): 3 doubles per CC tile, 2 per inversion step block (at most one a tile).
+long long partials_per_subject(const HostGrid& g, int radius) {
     const int nz = (int)g.n[2];
     long long most = 3LL * cc_batch_tiles(g, nz);
     for (int zc : cc_zchunks(nz, radius)) most = std::max<long long>(most, 3LL * cc_batch_tiles(g, zc));
-    std::vector<int> zcs = gather_zchunks(nz);
-    zcs.push_back(std::min(Tuning().meas_zc, nz));
-    for (int zc : zcs) most = std::max<long long>(most, 2LL * inv_measure_tiles(g, zc));
-    most = std::max<long long>(most, 2LL * inv_body_vblocks(ctx, g.count()));
+    most = std::max<long long>(most, 2LL * inv_step_tiles(g));
     return (most + 31) / 32 * 32;
 }
 
@@ -309,16 +307,41 @@ struct Run {
     BatchScalars sc;
     Buf partials;
     long long part_stride = 0;
+    Buf defer;                  // [B][defer_stride] deferred step tiles of each subject
+    long long defer_stride = 0;
 };
 
-// The inversion `inverse = invert(field, init inverse)` of every active subject (slot q of the
-// four loop states): the measurement, then a WHILE node over the body pair.
-int enqueue_batch_invert(Run& run, BatchLevel& L, const Buf& field, const Buf& inverse, int q) {
-    fw_ctx* ctx = run.ctx;
+// Virtual blocks per subject of the batched fix kernel (its deferred tiles are few).
+constexpr int kFixItems = 8;
+
+// The work lists and grids of the level's batched inversion body.
+InvBatchBody body_plan(const Run& run, const BatchLevel& L) {
     const Tuning& t = run.plan.t;
     const int sms = run.plan.sms;
-    BatchList lm = run.sc.list(inv_measure_tiles(L.grid, t.meas_zc));
-    BatchList lb = run.sc.list(inv_body_vblocks(ctx, L.n));
+    InvBatchBody w;
+    w.zchunk = t.step_zc;
+    w.bound = run.sc.list(std::min(inv_bound_vblocks(L.grid), 4 * sms));
+    w.step = run.sc.list(inv_step_blocks(L.grid, t.step_zc));
+    w.fix = run.sc.list(kFixItems);
+    w.bound_blocks = 4 * sms;
+    w.step_blocks = t.step_bps * sms;
+    w.fix_blocks = t.fix_bps * sms;
+    return w;
+}
+
+int launch_batch_body(Run& run, BatchLevel& L, const InvBatchBody& w, const Buf& field,
+                      const Buf& inverse, int q, int which) {
+    return launch_inv_body_batch(run.ctx, L.grid, L.ps, w, field.f(), inverse.f(), L.R.f(), L.fs,
+                                 (double*)run.partials.p, run.part_stride, run.sc.counter,
+                                 run.sc.inv + q, 4, static_cast<unsigned int*>(run.defer.p),
+                                 run.defer_stride, which);
+}
+
+// The inversion `inverse = invert(field, init inverse)` of every active subject (slot q of the
+// four loop states): the loops' settings, then a WHILE node over the body (bound, step, fix).
+int enqueue_batch_invert(Run& run, BatchLevel& L, const Buf& field, const Buf& inverse, int q) {
+    fw_ctx* ctx = run.ctx;
+    const InvBatchBody w = body_plan(run, L);
     cudaStreamCaptureStatus status;
     cudaGraph_t g;
     const cudaGraphNode_t* deps;
@@ -326,21 +349,16 @@ int enqueue_batch_invert(Run& run, BatchLevel& L, const Buf& field, const Buf& i
     FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
     cudaGraphConditionalHandle h;
     FW_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    FW_TRY(launch_inv_measure_batch(ctx, L.grid, L.ps, t.meas_zc, lm, t.meas_bps * sms, field.f(),
-                                    inverse.f(), L.R.f(), L.fs, (double*)run.partials.p,
-                                    run.part_stride, run.sc.counter, run.sc.inv + q, 4,
-                                    kBatchInvert));
-    FW_TRY(launch_inv_any(ctx, run.sc.inv + q, 4, lb, h));
+    FW_TRY(launch_inv_init_batch(ctx, w.step, run.sc.inv + q, 4, kBatchInvert));
+    FW_TRY(launch_inv_any(ctx, run.sc.inv + q, 4, w.step, h));
     cudaGraph_t body;
     FW_TRY(add_while_node(ctx->stream, h, &body));
     cudaStream_t main = ctx->stream;
     FW_CUDA(cudaStreamBeginCaptureToGraph(ctx->aux, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
     ctx->stream = ctx->aux;
-    int rc = launch_inv_body_batch(ctx, L.grid, L.ps, lb, t.body_bps * sms, field.f(),
-                                   inverse.f(), L.R.f(), L.fs, (double*)run.partials.p,
-                                   run.part_stride, run.sc.counter, run.sc.inv + q, 4);
-    if (!rc) rc = launch_inv_any(ctx, run.sc.inv + q, 4, lb, h);
+    int rc = launch_batch_body(run, L, w, field, inverse, q, -1);
+    if (!rc) rc = launch_inv_any(ctx, run.sc.inv + q, 4, w.step, h);
     ctx->stream = main;
     cudaGraph_t out;
     cudaError_t e = cudaStreamEndCapture(ctx->aux, &out);
@@ -540,41 +558,33 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
         }
     }
     best.compose_ms = bestms;
-    // the inversion measurement of F^-1 against F (residual into R, loop states of slot 0)
-    bestms = DBL_MAX;
-    for (int zc : gz) {
-        for (int bps : {2, 4}) {
-            FW_TRY(time_launch(ctx, tm, reps, [&] {
-                return launch_inv_measure_batch(ctx, L.grid, L.ps, zc,
-                                                run.sc.list(inv_measure_tiles(L.grid, zc)),
-                                                bps * sms, L.F.f(), L.Fi.f(), L.R.f(), L.fs,
-                                                (double*)run.partials.p, run.part_stride,
-                                                run.sc.counter, run.sc.inv, 4, kBatchInvert);
-            }, &ms));
-            if (ms < bestms) bestms = ms, best.meas_zc = zc, best.meas_bps = bps;
-        }
-    }
-    best.measure_ms = bestms;
-    // a body with its next measurement, on a scratch copy (dM) of the level's inverse that keeps
-    // iterating
+    // the inversion step (with its bound) of F^-1 against F on a scratch copy (dM) of the level's
+    // inverse, loop states of slot 0 kept iterating; then the whole body with the best grid
     FW_CUDA(cudaMemcpyAsync(L.dM.p, L.Fi.p, L.dM.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     const fw_invert_params forever = {1 << 30, -1.0, -1.0, 1};
-    FW_TRY(launch_inv_measure_batch(ctx, L.grid, L.ps, best.meas_zc,
-                                    run.sc.list(inv_measure_tiles(L.grid, best.meas_zc)),
-                                    best.meas_bps * sms, L.F.f(), L.dM.f(), L.R.f(), L.fs,
-                                    (double*)run.partials.p, run.part_stride, run.sc.counter,
-                                    run.sc.inv, 4, forever));
+    best.step_zc = inv_step_zchunk(L.grid.n, sms);
+    run.plan.t.step_zc = best.step_zc;
+    FW_TRY(launch_inv_init_batch(ctx, run.sc.list(1), run.sc.inv, 4, forever));
     bestms = DBL_MAX;
-    for (int bps : {2, 4, 8}) {
+    for (int bps : {2, 3}) {
+        run.plan.t.step_bps = bps;
+        const InvBatchBody w = body_plan(run, L);
+        // every step after its own bound (which also clears the deferred lists)
         FW_TRY(time_launch(ctx, tm, reps, [&] {
-            return launch_inv_body_batch(ctx, L.grid, L.ps, run.sc.list(inv_body_vblocks(ctx, L.n)),
-                                         bps * sms, L.F.f(), L.dM.f(), L.R.f(), L.fs,
-                                         (double*)run.partials.p, run.part_stride,
-                                         run.sc.counter, run.sc.inv, 4);
+            FW_TRY(launch_batch_body(run, L, w, L.F, L.dM, 0, 0));
+            return launch_batch_body(run, L, w, L.F, L.dM, 0, 1);
         }, &ms));
-        if (ms < bestms) bestms = ms, best.body_bps = bps;
+        if (ms < bestms) bestms = ms, best.step_bps = bps;
     }
-    best.body_ms = bestms;
+    best.step_ms = bestms;
+    run.plan.t.step_bps = best.step_bps;
+    {
+        const InvBatchBody w = body_plan(run, L);
+        FW_TRY(time_launch(ctx, tm, reps, [&] {
+            return launch_batch_body(run, L, w, L.F, L.dM, 0, -1);
+        }, &ms));
+        best.body_ms = ms;
+    }
     FW_CUDA(cudaMemsetAsync(run.sc.inv, 0, sizeof(InvState) * 4 * B, ctx->stream));
     FW_CUDA(cudaMemsetAsync(run.sc.mx, 0, sizeof(unsigned int) * 2 * B, ctx->stream));
     return sync(ctx);
@@ -829,10 +839,15 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
         FW_TRY(setup_level(run, *cur, prev.get(), lg));
         prev.reset();  // the previous level's buffers go back to the cache
         FW_TRY(setup_sources(run, *cur, fixed, subj, fg, r->smoothing_sigmas[level]));
-        const long long pps = partials_per_subject(ctx, lg, r->cc_radius);
+        const long long pps = partials_per_subject(lg, r->cc_radius);
         if (pps > run.part_stride) {
             run.part_stride = pps;
             FW_TRY(run.partials.alloc(ctx, sizeof(double) * (size_t)pps * B));
+        }
+        const long long dps = (inv_step_tiles(lg) + 63) / 64 * 64;
+        if (dps > run.defer_stride) {
+            run.defer_stride = dps;
+            FW_TRY(run.defer.alloc(ctx, sizeof(unsigned int) * (size_t)dps * B));
         }
         if (report) {
             FW_TRY(sync(ctx));
@@ -860,6 +875,7 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
             std::lock_guard<std::mutex> lock(g_tune_mu);
             g_tune[key] = t;
         }
+        t.step_zc = inv_step_zchunk(lg.n, ctx->num_sms);  // as the single step plans it
         run.plan.t = t;
         peak = std::max<uint64_t>(peak, ctx->live_bytes.load() - live0);
         double ms = 0.0;
@@ -875,9 +891,9 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
             o.compose_blocks_per_sm = t.comp_bps;
             o.cc_zchunk = t.cc_zc > 0 ? t.cc_zc : (int)lg.n[2];
             o.cc_blocks_per_sm = t.cc_bps;
-            o.measure_zchunk = t.meas_zc;
-            o.measure_blocks_per_sm = t.meas_bps;
-            o.body_blocks_per_sm = t.body_bps;
+            o.measure_zchunk = t.step_zc;
+            o.measure_blocks_per_sm = t.step_bps;
+            o.body_blocks_per_sm = t.fix_bps;
             o.smooth_blocks_per_sm = t.smooth_bps;
             o.from_cache = t.cached ? 1 : 0;
             o.tune_ms = t.tune_ms;
@@ -885,7 +901,7 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
             o.kernel_ms[1] = t.cc_ms;
             o.kernel_ms[2] = t.smooth_ms;
             o.kernel_ms[3] = t.compose_ms;
-            o.kernel_ms[4] = t.measure_ms;
+            o.kernel_ms[4] = t.step_ms;
             o.kernel_ms[5] = t.body_ms;
             report->level_ms[level] = ms;
         }

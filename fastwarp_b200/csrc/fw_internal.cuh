@@ -520,6 +520,9 @@ struct InvState {
     int max_iterations;
     double mean_tol, max_tol;
     int enforce;
+    unsigned int lb;      // float bits: a lower bound on the running body's max error
+    unsigned int ndefer;  // tiles whose update the running body left to the fix kernel
+    float eps, limit;     // the last body's step and clamp (eps * max error)
     int pad;
 };
 
@@ -530,7 +533,13 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
                              cudaGraphConditionalHandle handle, int use_handle);
 int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
                            InvState* st, cudaGraphConditionalHandle handle, int use_handle);
-int enqueue_inversion_rearm(fw_ctx* ctx, InvState* st, int max_iterations);
+// One kernel of a body (0 bound, 1 step, 2 fix), for kernel timing.
+int enqueue_inversion_kernel(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
+                             InvState* st, int which);
+long long inv_step_tiles(const HostGrid& g);
+// Scratch doubles an inversion on grid g needs (block partials and the deferred-tile list).
+size_t inv_scratch_doubles(const HostGrid& g);
+long long inv_bound_voxels(const HostGrid& g);
 // Adds a WHILE node on `handle` at the capture position of stream `s`; `body` receives the graph
 // the loop runs (fw_syn.cu).
 int add_while_node(cudaStream_t s, cudaGraphConditionalHandle handle, cudaGraph_t* body);
@@ -543,20 +552,26 @@ int launch_smooth_batch(fw_ctx* ctx, const HostGrid& g, long long ps, double var
                         const float* in, float* out, float* tmp, long long stride,
                         unsigned int* max_bits, int max_stride);
 
-// Batched inversions (fw_invert.cu): measurement tiles per subject for z chunks of `zchunk`,
-// virtual blocks per subject of a body sweep, the measurement, a body (the pair of kernels) and
-// the kernel that sets the inner loop's condition. Partials: 2 doubles per tile or virtual block.
-int inv_measure_tiles(const HostGrid& g, int zchunk);
-int inv_body_vblocks(fw_ctx* ctx, long long n);
-int launch_inv_measure_batch(fw_ctx* ctx, const HostGrid& g, long long ps, int zchunk,
-                             const BatchList& L, int blocks, const float* f, const float* psi,
-                             float* res, long long stride, double* partials,
-                             long long part_stride, unsigned int* counter, InvState* st,
-                             int st_stride, const fw_invert_params& prm);
-int launch_inv_body_batch(fw_ctx* ctx, const HostGrid& g, long long ps, const BatchList& L,
-                          int blocks, const float* f, float* psi, float* res, long long stride,
+// The batched inversion body (fw_invert.cu): its three kernels' work lists and persistent grids.
+// Items per subject: the bound's lattice blocks, the step's blocks of `zchunk` step tiles (as the
+// single step plans them, inv_step_zchunk), the fix's virtual blocks over the deferred list.
+struct InvBatchBody {
+    int zchunk;
+    BatchList bound, step, fix;
+    int bound_blocks, step_blocks, fix_blocks;
+};
+int inv_step_zchunk(const int64_t n[3], int num_sms);
+int inv_step_blocks(const HostGrid& g, int zchunk);
+int inv_bound_vblocks(const HostGrid& g);
+int launch_inv_init_batch(fw_ctx* ctx, const BatchList& L, InvState* st, int st_stride,
+                          const fw_invert_params& prm);
+// which: -1 the whole body (bound, step, fix), else one kernel (0 bound, 1 step, 2 fix)
+int launch_inv_body_batch(fw_ctx* ctx, const HostGrid& g, long long ps, const InvBatchBody& w,
+                          const float* f, float* psi, float* res, long long stride,
                           double* partials, long long part_stride, unsigned int* counter,
-                          InvState* st, int st_stride);
+                          InvState* st, int st_stride, unsigned int* defer,
+                          long long defer_stride, int which);
+// The kernel that sets the inner loop's condition (any active subject runs another body).
 int launch_inv_any(fw_ctx* ctx, const InvState* st, int st_stride, const BatchList& L,
                    cudaGraphConditionalHandle handle);
 int read_back(fw_ctx* ctx, const double* d, int k, double* out);

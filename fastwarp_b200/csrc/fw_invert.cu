@@ -4,14 +4,25 @@
 // { e = psi + f(x + psi); measure mean and max of |e/sp|; psi += eps * clamp(-e) with
 // eps = 0.75 on the first body and 0.5 after; faces of psi to zero }.
 //
-// Device design: the error at voxel x depends only on psi(x) and the read-only field f, so one
-// sweep can apply body k's update to psi(x) and at once measure body k+1's error at the same
-// voxel. Each body is therefore ONE sweep (read psi and the kept residual, write psi, gather f
-// for the next measurement only when there is a next body) plus a fixed-order reduction done by
-// the last block to finish; it is launched as a pair of kernels of which one works. The loop
-// state (errors of the last measurement, body index, whether the next body runs) lives in device
-// memory and is updated by that last block, so the loop needs no host read-back: the SyN driver
-// runs it inside a CUDA graph WHILE node whose condition the last block sets.
+// Device design: the error at voxel x depends only on psi(x) and the read-only field f, so the
+// sweep that measures a body's error can apply the same body's update to psi(x) in place -- the
+// only thing it cannot know yet is the clamp, which needs the body's maximum error over the whole
+// volume. A body is therefore three kernels:
+//   k_inv_bound  the error on a sparse lattice of voxels (one in 64): its maximum is a lower
+//                bound L on the body's maximum error;
+//   k_inv_step   the measurement over 32 x 8 x 4 column tiles, each thread keeping its column's
+//                psi and error in registers. No voxel of a tile whose largest error is at most
+//                eps * L can be clamped (eps * L <= eps * max), so such a tile updates psi in
+//                place at once; any other tile writes its errors to the residual field and
+//                enters a short list. A fixed-order reduction (the last block) gives the mean
+//                and max and decides whether another body runs;
+//   k_inv_fix    the listed tiles' updates, now with the clamp eps * max.
+// The update of every voxel is the same arithmetic on either path, so the result does not depend
+// on which tiles were deferred. The loop state lives in device memory, so the loop needs no host
+// read-back: the SyN driver runs it inside a CUDA graph WHILE node whose condition the step's last
+// block sets. The batched kernels (many subjects, one launch) run the same body in two kernels:
+// a measurement that keeps the residual, then the update (with the next measurement when the
+// loop goes on).
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -31,15 +42,49 @@ struct InvArgs {
 __device__ __forceinline__ void residual(const InvArgs& a, const float* __restrict__ f,
                                          long long l, int i, int j, int k, float px, float py,
                                          float pz, float e[3]) {
-    double c0 = i + (a.g.inv[0] * px + a.g.inv[1] * py + a.g.inv[2] * pz);
-    double c1 = j + (a.g.inv[3] * px + a.g.inv[4] * py + a.g.inv[5] * pz);
-    double c2 = k + (a.g.inv[6] * px + a.g.inv[7] * py + a.g.inv[8] * pz);
+    // explicitly rounded (no contraction), in the reference's order: every kernel that measures
+    // a voxel maps it to the same continuous index
+    auto map = [&](int r, int base) {
+        const double* m = a.g.inv + 3 * r;
+        return __dadd_rn((double)base, __dadd_rn(__dadd_rn(__dmul_rn(m[0], (double)px),
+                                                           __dmul_rn(m[1], (double)py)),
+                                                 __dmul_rn(m[2], (double)pz)));
+    };
+    const double c0 = map(0, i), c1 = map(1, j), c2 = map(2, k);
     float d[3] = {0.0f, 0.0f, 0.0f};
     if (inside_index(c0, c1, c2, a.g.nx, a.g.ny, a.g.nz))
         vec_at_index(f, a.ps_f, a.g.nx, a.g.ny, a.g.nz, c0, c1, c2, d);
     e[0] = px + d[0];
     e[1] = py + d[1];
     e[2] = pz + d[2];
+}
+
+// |e / sp| of one voxel's error (every kernel that measures a voxel uses this one expression).
+// In a SyN run's first iteration the largest error equals the gradient step up to rounding, so
+// with a step of 0.1 (the inversion's max-error tolerance) this float's last bit decides whether
+// a second body runs; the expression is the one validated against the oracle.
+__device__ __forceinline__ float err_norm(const InvArgs& a, const float e[3]) {
+    const float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
+    return sqrtf(x * x + y * y + z * z);
+}
+
+// psi + eps * clamp(-e) at one voxel (field_ops.rs:368-383), faces to zero with `enforce`.
+__device__ __forceinline__ void update_voxel(const InvArgs& a, int i, int j, int k, float nrm,
+                                             const float e[3], float eps, float limit,
+                                             bool enforce, float p[3]) {
+    float ux = -e[0], uy = -e[1], uz = -e[2];
+    if (nrm > limit) {
+        const float fct = limit / nrm;
+        ux *= fct;
+        uy *= fct;
+        uz *= fct;
+    }
+    p[0] = p[0] + ux * eps;
+    p[1] = p[1] + uy * eps;
+    p[2] = p[2] + uz * eps;
+    const bool face = i == 0 || j == 0 || k == 0 || i == a.g.nx - 1 || j == a.g.ny - 1 ||
+                      k == a.g.nz - 1;
+    if (enforce && face) p[0] = p[1] = p[2] = 0.0f;
 }
 
 // Block sums (f64) and maxima -> partials; the last block reduces them in block order and
@@ -85,269 +130,362 @@ __device__ void reduce_and_finish(double sum, float mx, double* __restrict__ par
     }
 }
 
-// The measurement of tile (bx, by, bz): the thread's column of e = psi + f(x + psi) kept in
-// `res`, its sum and max of |e/sp| added to sum / mx.
-__device__ __forceinline__ void measure_tile(const InvArgs& a, int bx, int by, int bz,
-                                             const float* __restrict__ f,
-                                             const float* __restrict__ psi,
-                                             float* __restrict__ res, double& sum, float& mx) {
-    struct {
-        int x, y, z0, z1;
-    } col;
-    if (!column_of_tile(a.g.nx, a.g.ny, a.g.nz, a.zchunk, bx, by, bz, col.x, col.y, col.z0,
-                        col.z1))
-        return;
-    const long long sxy = (long long)a.g.nx * a.g.ny;
-    long long l = (long long)col.z0 * sxy + (long long)col.y * a.g.nx + col.x;
-    float px = psi[l], py = psi[l + a.ps_psi], pz = psi[l + 2 * a.ps_psi];
-    for (int z = col.z0; z < col.z1; ++z, l += sxy) {
-        float qx = 0.0f, qy = 0.0f, qz = 0.0f;
-        if (z + 1 < col.z1) {  // the next slice's psi, in flight during this gather
-            qx = psi[l + sxy];
-            qy = psi[l + sxy + a.ps_psi];
-            qz = psi[l + sxy + 2 * a.ps_psi];
-        }
+// ---- one inversion body: bound, step, fix --------------------------------------------------
+
+#ifndef FW_STEP_Z
+#define FW_STEP_Z 4
+#endif
+#ifndef FW_STEP_MIN_BLOCKS
+#define FW_STEP_MIN_BLOCKS 3
+#endif
+#ifndef FW_STEP_MAX_TILES
+#define FW_STEP_MAX_TILES 4
+#endif
+constexpr int kStepZ = FW_STEP_Z;  // slices of a step tile (a thread's column stays in registers)
+// eps * L is lowered by this factor before tiles are compared with it: the bound and the step
+// measure a voxel with the same code, so L is one of the step's errors; the factor guards against
+// the compiler contracting the norm's products differently in the two kernels (a last-bit change)
+constexpr float kSafeMargin = 0.999f;
+
+// The loop's settings before its first body (field_ops.rs:325-338: errors start at +inf, so the
+// first body runs whenever max_iterations > 0).
+__device__ __forceinline__ void init_state(InvState* __restrict__ st, const fw_invert_params& prm) {
+    st->max_iterations = prm.max_iterations;
+    st->mean_tol = prm.mean_error_tolerance;
+    st->max_tol = prm.max_error_tolerance;
+    st->enforce = prm.enforce_boundary_condition;
+    st->mean = 0.0;
+    st->max = 0.0;
+    st->executed = 0;
+    st->k = 0;
+    st->go = prm.max_iterations > 0 ? 1 : 0;
+    st->lb = 0u;
+    st->ndefer = 0u;
+    st->eps = 0.0f;
+    st->limit = 0.0f;
+}
+
+__global__ void k_inv_init(InvState* __restrict__ st, fw_invert_params prm,
+                           cudaGraphConditionalHandle handle, int use_handle) {
+    init_state(st, prm);
+    if (use_handle) cudaGraphSetConditional(handle, st->go ? 1u : 0u);
+}
+
+// The lattice of the bound: voxels 1, 5, 9, ... along each axis (0 on an axis of one voxel).
+struct Lattice {
+    int ox, oy, oz, mx, my, mz;
+    __host__ __device__ long long count() const { return (long long)mx * my * mz; }
+};
+
+static Lattice lattice_of(const DevGrid& g) {
+    Lattice t;
+    t.ox = g.nx > 1 ? 1 : 0;
+    t.oy = g.ny > 1 ? 1 : 0;
+    t.oz = g.nz > 1 ? 1 : 0;
+    t.mx = (g.nx - t.ox + 3) / 4;
+    t.my = (g.ny - t.oy + 3) / 4;
+    t.mz = (g.nz - t.oz + 3) / 4;
+    return t;
+}
+
+// The running body's error on the lattice points vb, vb + nvb, ... (256 a block step) of one
+// inverse; the block's largest (as float bits, NaN above everything) goes into st->lb, the lower
+// bound L the step compares tiles with.
+__device__ __forceinline__ void bound_block(const InvArgs& a, const Lattice& t,
+                                            const float* __restrict__ f,
+                                            const float* __restrict__ psi,
+                                            InvState* __restrict__ st, unsigned int vb,
+                                            unsigned int nvb) {
+    __shared__ float wm[8];
+    float best = 0.0f;
+    const long long m = t.count();
+    for (long long s = (long long)vb * blockDim.x + threadIdx.x; s < m;
+         s += (long long)nvb * blockDim.x) {
+        const long long q = s / t.mx;
+        const int i = t.ox + 4 * (int)(s - q * t.mx);
+        const int j = t.oy + 4 * (int)(q % t.my);
+        const int k = t.oz + 4 * (int)(q / t.my);
+        const long long l = ((long long)k * a.g.ny + j) * a.g.nx + i;
         float e[3];
-        residual(a, f, l, col.x, col.y, z, px, py, pz, e);
-        res[l] = e[0];
-        res[l + a.ps_psi] = e[1];
-        res[l + 2 * a.ps_psi] = e[2];
-        float x = e[0] * a.isx, y = e[1] * a.isy, zz = e[2] * a.isz;
-        float nrm = nan_canon(sqrtf(x * x + y * y + zz * zz));
-        sum += (double)nrm;
-        mx = __int_as_float(max(__float_as_int(mx), __float_as_int(nrm)));
-        px = qx;
-        py = qy;
-        pz = qz;
+        residual(a, f, l, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
+        const float nrm = nan_canon(err_norm(a, e));
+        best = __int_as_float(max(__float_as_int(best), __float_as_int(nrm)));
     }
+    best = warp_max_f(best);
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; ++w)
+            best = __int_as_float(max(__float_as_int(best), __float_as_int(wm[w])));
+        atomicMax(&st->lb, __float_as_uint(best));
+    }
+    __syncthreads();  // wm is free for the block's next item
 }
 
-// First measurement (body 0's error) of psi against f; the residual e = psi + f(x + psi) of
-// every voxel is kept in `res` for the body that follows.
-// Its last block also writes the loop's settings into the state (no separate init launch).
-__global__ void __launch_bounds__(256, 4) k_inv_measure(InvArgs a, const float* __restrict__ f,
-                                                     const float* __restrict__ psi,
-                                                     float* __restrict__ res,
-                                                     double* __restrict__ partials,
-                                                     unsigned int* __restrict__ counter,
-                                                     InvState* __restrict__ st,
-                                                     fw_invert_params prm,
-                                                     cudaGraphConditionalHandle handle,
-                                                     int use_handle) {
-    double sum = 0.0;
-    float mx = 0.0f;
-    measure_tile(a, blockIdx.x, blockIdx.y, blockIdx.z, f, psi, res, sum, mx);
-    const double count = (double)a.g.n;
-    const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
-    reduce_and_finish(sum, mx, partials, counter, bid, nblocks, [&](double s, double m) {
-        st->max_iterations = prm.max_iterations;
-        st->mean_tol = prm.mean_error_tolerance;
-        st->max_tol = prm.max_error_tolerance;
-        st->enforce = prm.enforce_boundary_condition;
-        st->mean = s / count;
-        st->max = m;
-        st->executed = 0;
-        st->k = 0;
-        st->go = prm.max_iterations > 0 ? 1 : 0;
-        if (use_handle) cudaGraphSetConditional(handle, st->go ? 1u : 0u);
-    });
+// The bound of the running body (also clears the previous body's deferred list, whose fix
+// kernel has run).
+__global__ void __launch_bounds__(256) k_inv_bound(InvArgs a, Lattice t, const float* __restrict__ f,
+                                                   const float* __restrict__ psi,
+                                                   InvState* __restrict__ st) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->ndefer = 0u;
+    if (!st->go) return;
+    bound_block(a, t, f, psi, st, blockIdx.x, gridDim.x);
 }
 
-// The sweep of virtual block vb of nvb (a grid-stride loop over the voxels, two a step): the
-// update of psi with eps and limit from the kept residual, faces to zero with `enforce`, and with
-// GATHER the next measurement into res, its sum and max added to sum / mx.
-template <bool GATHER>
-__device__ __forceinline__ void body_sweep(const InvArgs& a, unsigned int vb, unsigned int nvb,
-                                           const float* __restrict__ f, float* __restrict__ psi,
-                                           float* __restrict__ res, float eps, float limit,
-                                           bool enforce, double& sum, float& mx) {
-    const long long stride = (long long)nvb * blockDim.x;
-    // two voxels a step, `stride` apart: their loads are in flight together
-    for (long long l0 = (long long)vb * blockDim.x + threadIdx.x; l0 < a.g.n;
-         l0 += 2 * stride) {
-        float px[2], py[2], pz[2], ex[2], ey[2], ez[2];
-        int ii[2], jj[2], kk[2];
-        bool ok[2];
+// One step tile (bx, by, bz): the thread's column of at most kStepZ voxels is measured with psi
+// and e in registers; the tile's largest error decides whether it updates psi now (no voxel of
+// it can exceed eps * L <= the clamp) or keeps its errors in `res` for the fix kernel. Returns
+// whether the tile was deferred (uniform over the block).
+__device__ __forceinline__ bool step_tile(const InvArgs& a, int bx, int by, int bz,
+                                          const float* __restrict__ f, float* __restrict__ psi,
+                                          float* __restrict__ res, float eps, float safe,
+                                          bool enforce, double& sum, float& mx) {
+    __shared__ float wmax[8];  // one per warp of the 256-thread block
+    int x, y, z0, z1;
+    const bool have = column_of_tile(a.g.nx, a.g.ny, a.g.nz, kStepZ, bx, by, bz, x, y, z0, z1);
+    const long long sxy = (long long)a.g.nx * a.g.ny;
+    const long long l0 = (long long)z0 * sxy + (long long)y * a.g.nx + x;
+    float p[kStepZ][3], e[kStepZ][3];
+    float tmax = 0.0f;
+    if (have) {
 #pragma unroll
-        for (int v = 0; v < 2; ++v) {
-            long long l = l0 + v * stride;
-            ok[v] = l < a.g.n;
-            if (!ok[v]) continue;
-            voxel_ijk(l, a.g.nx, a.g.ny, ii[v], jj[v], kk[v]);
-            px[v] = psi[l];
-            py[v] = psi[l + a.ps_psi];
-            pz[v] = psi[l + 2 * a.ps_psi];
-            ex[v] = res[l];
-            ey[v] = res[l + a.ps_psi];
-            ez[v] = res[l + 2 * a.ps_psi];
-        }
-#pragma unroll
-        for (int v = 0; v < 2; ++v) {
-            if (!ok[v]) continue;
-            long long l = l0 + v * stride;
-            const int i = ii[v], j = jj[v], k = kk[v];
-            float sx = ex[v] * a.isx, sy = ey[v] * a.isy, sz = ez[v] * a.isz;
-            float nrm = sqrtf(sx * sx + sy * sy + sz * sz);
-            float ux = -ex[v], uy = -ey[v], uz = -ez[v];
-            if (nrm > limit) {
-                float fct = limit / nrm;
-                ux *= fct;
-                uy *= fct;
-                uz *= fct;
+        for (int q = 0; q < kStepZ; ++q) {
+            if (z0 + q < z1) {
+                const long long l = l0 + q * sxy;
+                p[q][0] = psi[l];
+                p[q][1] = psi[l + a.ps_psi];
+                p[q][2] = psi[l + 2 * a.ps_psi];
             }
-            px[v] = px[v] + ux * eps;
-            py[v] = py[v] + uy * eps;
-            pz[v] = pz[v] + uz * eps;
-            const bool face = i == 0 || j == 0 || k == 0 || i == a.g.nx - 1 ||
-                              j == a.g.ny - 1 || k == a.g.nz - 1;
-            if (enforce && face) px[v] = py[v] = pz[v] = 0.0f;
-            psi[l] = px[v];
-            psi[l + a.ps_psi] = py[v];
-            psi[l + 2 * a.ps_psi] = pz[v];
         }
-        if constexpr (GATHER) {
 #pragma unroll
-            for (int v = 0; v < 2; ++v) {
-                if (!ok[v]) continue;
-                long long l = l0 + v * stride;
-                float e[3];
-                residual(a, f, l, ii[v], jj[v], kk[v], px[v], py[v], pz[v], e);
-                res[l] = e[0];
-                res[l + a.ps_psi] = e[1];
-                res[l + 2 * a.ps_psi] = e[2];
-                float x = e[0] * a.isx, y = e[1] * a.isy, z = e[2] * a.isz;
-                float n2 = nan_canon(sqrtf(x * x + y * y + z * z));
-                sum += (double)n2;
-                mx = __int_as_float(max(__float_as_int(mx), __float_as_int(n2)));
+        for (int q = 0; q < kStepZ; ++q) {
+            if (z0 + q < z1) {
+                residual(a, f, l0 + q * sxy, x, y, z0 + q, p[q][0], p[q][1], p[q][2], e[q]);
+                const float nrm = nan_canon(err_norm(a, e[q]));
+                sum += (double)nrm;
+                tmax = __int_as_float(max(__float_as_int(tmax), __float_as_int(nrm)));
             }
         }
     }
+    const float w = warp_max_f(tmax);
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = w;
+    __syncthreads();
+    float tm = wmax[0];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) tm = __int_as_float(max(__float_as_int(tm), __float_as_int(wmax[q])));
+    __syncthreads();  // wmax is free for the block's next tile
+    mx = __int_as_float(max(__float_as_int(mx), __float_as_int(tmax)));
+    const bool now = tm <= safe;  // false when either is NaN
+    if (have) {
+#pragma unroll
+        for (int q = 0; q < kStepZ; ++q) {
+            if (z0 + q < z1) {
+                const long long l = l0 + q * sxy;
+                if (now) {
+                    // the clamp cannot apply: limit = eps * max >= eps * L >= every error here
+                    update_voxel(a, x, y, z0 + q, 0.0f, e[q], eps, 1.0f, enforce, p[q]);
+                    psi[l] = p[q][0];
+                    psi[l + a.ps_psi] = p[q][1];
+                    psi[l + 2 * a.ps_psi] = p[q][2];
+                } else {
+                    res[l] = e[q][0];
+                    res[l + a.ps_psi] = e[q][1];
+                    res[l + 2 * a.ps_psi] = e[q][2];
+                }
+            }
+        }
+    }
+    return !now;
 }
 
-// One body: the update with eps (0.75 on body 0, else 0.5) and limit eps * max of the last
-// measurement, from the residual that measurement kept in `res`; faces to zero; then -- when
-// the next body will run -- its measurement, whose residual replaces the voxel's in `res`.
-// Two kernels share the work, launched in this order every body: GATHER = false runs the body
-// when the loop stops after it (an elementwise sweep, no gather), GATHER = true when the loop
-// goes on (update and next measurement in one sweep). Each decides from the loop state, which
-// only the kernel that runs changes (in its last block), so exactly one of them works; kept
-// apart, the elementwise sweep keeps the gather's register footprint out of its occupancy.
-template <bool GATHER>
-__global__ void __launch_bounds__(256, 4) k_inv_body(InvArgs a, const float* __restrict__ f,
+// Block (bx, by, bzb) of body k's step: a.zchunk step tiles one above the other, measured against
+// f (sum and max added to sum / mx), updated at once or listed in `defer` (entries are tile
+// indices of the gx x gy x ceil(nz / kStepZ) tile grid).
+__device__ __forceinline__ void step_block(const InvArgs& a, int bx, int by, int bzb, int gx,
+                                           int gy, const float* __restrict__ f,
+                                           float* __restrict__ psi, float* __restrict__ res,
+                                           InvState* __restrict__ st,
+                                           unsigned int* __restrict__ defer, double& sum,
+                                           float& mx) {
+    const int kb = st->k;
+    const float eps = kb == 0 ? 0.75f : 0.5f;
+    const float safe = __fmul_rn(__fmul_rn(eps, __uint_as_float(st->lb)), kSafeMargin);
+    const bool enforce = st->enforce != 0;
+    const int gz = (a.g.nz + kStepZ - 1) / kStepZ;
+    const unsigned int cap = (unsigned int)(gx * gy * gz);  // the list holds every tile once
+    for (int m = 0; m < a.zchunk; ++m) {
+        const int tz = bzb * a.zchunk + m;
+        if (tz >= gz) break;  // uniform
+        const bool deferred =
+            step_tile(a, bx, by, tz, f, psi, res, eps, safe, enforce, sum, mx);
+        if (deferred && threadIdx.x == 0) {
+            const unsigned int at = atomicAdd(&st->ndefer, 1u);
+            if (at < cap) defer[at] = (unsigned int)(bx + gx * (by + gy * tz));
+        }
+    }
+}
+
+// The last block's record of body k (field_ops.rs:340-357): errors, bodies executed, the step
+// and clamp the fix kernel applies, and whether body k + 1 runs.
+__device__ __forceinline__ bool finish_step(InvState* __restrict__ st, double s, double m,
+                                            double count) {
+    const int kb = st->k;
+    const float eps = kb == 0 ? 0.75f : 0.5f;
+    const double mean = s / count;
+    const bool next = (kb + 1 < st->max_iterations) && m > st->max_tol && mean > st->mean_tol;
+    st->mean = mean;
+    st->max = m;
+    st->executed = kb + 1;
+    st->k = kb + 1;
+    st->eps = eps;
+    st->limit = eps * (float)m;
+    st->lb = 0u;
+    st->go = next ? 1 : 0;
+    return next;
+}
+
+// Body k of the loop: measurement of psi against f (its mean and max), the update of every tile
+// that cannot be clamped, and the list of the others. A block takes a.zchunk step tiles one above
+// the other (fewer block partials on big grids); the last block reduces the partials in a fixed
+// order, records the body and decides whether body k + 1 runs.
+__global__ void __launch_bounds__(256, FW_STEP_MIN_BLOCKS) k_inv_step(InvArgs a, const float* __restrict__ f,
                                                      float* __restrict__ psi,
                                                      float* __restrict__ res,
                                                      double* __restrict__ partials,
                                                      unsigned int* __restrict__ counter,
                                                      InvState* __restrict__ st,
+                                                     unsigned int* __restrict__ defer,
                                                      cudaGraphConditionalHandle handle,
                                                      int use_handle) {
-    const int go = st->go;
-    if (!go) {  // uniform: the state only changes in the last block of the grid that works
-        // keep a WHILE loop from spinning should its condition ever disagree with the state
-        if (use_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
+    if (!st->go) {  // uniform: the state only changes in the last block of a working grid
+        if (use_handle && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 &&
+            threadIdx.x == 0)
+            cudaGraphSetConditional(handle, 0u);
         return;
     }
-    const int kb = st->k;
-    const double mean = st->mean, mxe = st->max;
-    const bool next = (kb + 1 < st->max_iterations) && mxe > st->max_tol && mean > st->mean_tol;
-    if (next != GATHER) return;  // the other kernel of the pair runs this body
-    const float eps = kb == 0 ? 0.75f : 0.5f;
-    const float limit = eps * (float)mxe;
-    const bool enforce = st->enforce != 0;
     double sum = 0.0;
     float mx = 0.0f;
-    body_sweep<GATHER>(a, blockIdx.x, gridDim.x, f, psi, res, eps, limit, enforce, sum, mx);
-    const double count = (double)a.g.n;
-    reduce_and_finish(sum, mx, partials, counter, blockIdx.x, gridDim.x, [&](double s, double m) {
-        st->executed = kb + 1;
-        if (GATHER) {
-            st->mean = s / count;
-            st->max = m;
-            st->k = kb + 1;
-        }
-        st->go = GATHER ? 1 : 0;
-        if (use_handle) cudaGraphSetConditional(handle, GATHER ? 1u : 0u);
+    step_block(a, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, f, psi, res, st,
+               defer, sum, mx);
+    const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
+    reduce_and_finish(sum, mx, partials, counter, bid, nblocks, [&](double s, double m) {
+        const bool next = finish_step(st, s, m, (double)a.g.n);
+        if (use_handle) cudaGraphSetConditional(handle, next ? 1u : 0u);
     });
+}
+
+// The deferred tiles of the body that just ran, entries vb, vb + nvb, ... of the list: each
+// voxel's update from its kept error, with the clamp at eps * max (field_ops.rs:368-383). Each
+// voxel is written by one thread.
+__device__ __forceinline__ void fix_tiles(const InvArgs& a, float* __restrict__ psi,
+                                          const float* __restrict__ res,
+                                          const InvState* __restrict__ st,
+                                          const unsigned int* __restrict__ defer, unsigned int vb,
+                                          unsigned int nvb) {
+    const int gx = (a.g.nx + 31) / 32, gy = (a.g.ny + 7) / 8;
+    const unsigned int cap = (unsigned int)(gx * gy * ((a.g.nz + kStepZ - 1) / kStepZ));
+    const unsigned int n = min(st->ndefer, cap);
+    if (n == 0u) return;
+    const float eps = st->eps, limit = st->limit;
+    const bool enforce = st->enforce != 0;
+    const long long sxy = (long long)a.g.nx * a.g.ny;
+    for (unsigned int t = vb; t < n; t += nvb) {
+        int bx, by, bz;
+        tile_coords((int)defer[t], gx, gy, bx, by, bz);
+        int x, y, z0, z1;
+        if (!column_of_tile(a.g.nx, a.g.ny, a.g.nz, kStepZ, bx, by, bz, x, y, z0, z1)) continue;
+        for (int z = z0; z < z1; ++z) {
+            const long long l = (long long)z * sxy + (long long)y * a.g.nx + x;
+            const float e[3] = {res[l], res[l + a.ps_psi], res[l + 2 * a.ps_psi]};
+            float p[3] = {psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi]};
+            update_voxel(a, x, y, z, err_norm(a, e), e, eps, limit, enforce, p);
+            psi[l] = p[0];
+            psi[l + a.ps_psi] = p[1];
+            psi[l + 2 * a.ps_psi] = p[2];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 4) k_inv_fix(InvArgs a, float* __restrict__ psi,
+                                                    const float* __restrict__ res,
+                                                    const InvState* __restrict__ st,
+                                                    const unsigned int* __restrict__ defer) {
+    fix_tiles(a, psi, res, st, defer, blockIdx.x, gridDim.x);
 }
 
 // ---- batched inversions: every active subject of a batch, each with its own loop state ------
 //
 // Subject b's field, inverse and residual are at f / psi / res + b * stride, its partials at
-// partials + b * part_stride, its last-item counter at counter[b] and its loop state at
-// st[b * st_stride]. Tiles and virtual blocks are those of the single kernels, and a subject's
-// partials are reduced in the same order, so its loop takes the same decisions as alone. The
-// loop's condition is set afterwards by k_inv_any (any active subject still iterating).
+// partials + b * part_stride, its last-item counter at counter[b], its deferred list at
+// defer + b * defer_stride and its loop state at st[b * st_stride]. A subject's items are the
+// single kernels' blocks (the step's a.zchunk tiles each) and its partials are reduced in the
+// same order, so its loop takes the same decisions as alone. The loop's condition is set
+// afterwards by k_inv_any (any active subject still iterating).
 
-__global__ void __launch_bounds__(256, 4) k_inv_measure_batch(
-    InvArgs a, BatchList L, const float* __restrict__ f, const float* __restrict__ psi,
+__global__ void k_inv_init_batch(BatchList L, InvState* __restrict__ st, int st_stride,
+                                 fw_invert_params prm) {
+    const int n = *L.count;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        init_state(st + L.active[i] * st_stride, prm);
+}
+
+__global__ void __launch_bounds__(256) k_inv_bound_batch(InvArgs a, Lattice t, BatchList L,
+                                                         const float* __restrict__ f,
+                                                         const float* __restrict__ psi,
+                                                         long long stride,
+                                                         InvState* __restrict__ st,
+                                                         int st_stride) {
+    const int work = *L.count * L.tiles;
+    for (int w = blockIdx.x; w < work; w += gridDim.x) {
+        const int b = L.active[w / L.tiles];
+        const unsigned int vb = (unsigned int)(w % L.tiles);
+        InvState* sb = st + b * st_stride;
+        if (vb == 0 && threadIdx.x == 0) sb->ndefer = 0u;
+        if (!sb->go) continue;  // uniform
+        bound_block(a, t, f + b * stride, psi + b * stride, sb, vb, (unsigned int)L.tiles);
+    }
+}
+
+__global__ void __launch_bounds__(256, FW_STEP_MIN_BLOCKS) k_inv_step_batch(
+    InvArgs a, BatchList L, const float* __restrict__ f, float* __restrict__ psi,
     float* __restrict__ res, long long stride, double* __restrict__ partials,
     long long part_stride, unsigned int* __restrict__ counter, InvState* __restrict__ st,
-    int st_stride, fw_invert_params prm) {
+    int st_stride, unsigned int* __restrict__ defer, long long defer_stride) {
     const int work = *L.count * L.tiles;
     const int gx = (a.g.nx + 31) / 32, gy = (a.g.ny + 7) / 8;
     const double count = (double)a.g.n;
     for (int w = blockIdx.x; w < work; w += gridDim.x) {
         const int b = L.active[w / L.tiles], t = w % L.tiles;
-        int bx, by, bz;
-        tile_coords(t, gx, gy, bx, by, bz);
+        InvState* sb = st + b * st_stride;
+        // uniform over the block; the state only changes once every item of the subject is done
+        if (!sb->go) continue;
+        int bx, by, bzb;
+        tile_coords(t, gx, gy, bx, by, bzb);
         double sum = 0.0;
         float mx = 0.0f;
-        measure_tile(a, bx, by, bz, f + b * stride, psi + b * stride, res + b * stride, sum, mx);
-        InvState* sb = st + b * st_stride;
+        step_block(a, bx, by, bzb, gx, gy, f + b * stride, psi + b * stride, res + b * stride,
+                   sb, defer + b * defer_stride, sum, mx);
         reduce_and_finish(sum, mx, partials + b * part_stride, counter + b, (unsigned int)t,
-                          (unsigned int)L.tiles, [&](double sm, double m) {
-                              sb->max_iterations = prm.max_iterations;
-                              sb->mean_tol = prm.mean_error_tolerance;
-                              sb->max_tol = prm.max_error_tolerance;
-                              sb->enforce = prm.enforce_boundary_condition;
-                              sb->mean = sm / count;
-                              sb->max = m;
-                              sb->executed = 0;
-                              sb->k = 0;
-                              sb->go = prm.max_iterations > 0 ? 1 : 0;
-                          });
+                          (unsigned int)L.tiles,
+                          [&](double sm, double m) { finish_step(sb, sm, m, count); });
         __syncthreads();  // the next item reuses the reduction's shared memory
     }
 }
 
-// One body of every active subject (virtual block vb of L.tiles per subject): the kernel of the
-// pair that matches the subject's next step works, the other skips the subject.
-template <bool GATHER>
-__global__ void __launch_bounds__(256, 4) k_inv_body_batch(
-    InvArgs a, BatchList L, const float* __restrict__ f, float* __restrict__ psi,
-    float* __restrict__ res, long long stride, double* __restrict__ partials,
-    long long part_stride, unsigned int* __restrict__ counter, InvState* __restrict__ st,
-    int st_stride) {
+__global__ void __launch_bounds__(256, 4) k_inv_fix_batch(InvArgs a, BatchList L,
+                                                          float* __restrict__ psi,
+                                                          const float* __restrict__ res,
+                                                          long long stride,
+                                                          const InvState* __restrict__ st,
+                                                          int st_stride,
+                                                          const unsigned int* __restrict__ defer,
+                                                          long long defer_stride) {
     const int work = *L.count * L.tiles;
-    const double count = (double)a.g.n;
     for (int w = blockIdx.x; w < work; w += gridDim.x) {
         const int b = L.active[w / L.tiles];
-        const unsigned int vb = (unsigned int)(w % L.tiles);
-        InvState* sb = st + b * st_stride;
-        // uniform over the block; the state only changes once every item of the subject is done
-        if (!sb->go) continue;
-        const int kb = sb->k;
-        const double mean = sb->mean, mxe = sb->max;
-        const bool next = (kb + 1 < sb->max_iterations) && mxe > sb->max_tol && mean > sb->mean_tol;
-        if (next != GATHER) continue;
-        const float eps = kb == 0 ? 0.75f : 0.5f;
-        const float limit = eps * (float)mxe;
-        double sum = 0.0;
-        float mx = 0.0f;
-        body_sweep<GATHER>(a, vb, (unsigned int)L.tiles, f + b * stride, psi + b * stride,
-                           res + b * stride, eps, limit, sb->enforce != 0, sum, mx);
-        reduce_and_finish(sum, mx, partials + b * part_stride, counter + b, vb,
-                          (unsigned int)L.tiles, [&](double sm, double m) {
-                              sb->executed = kb + 1;
-                              if (GATHER) {
-                                  sb->mean = sm / count;
-                                  sb->max = m;
-                                  sb->k = kb + 1;
-                              }
-                              sb->go = GATHER ? 1 : 0;
-                          });
-        __syncthreads();
+        fix_tiles(a, psi + b * stride, res + b * stride, st + b * st_stride,
+                  defer + b * defer_stride, (unsigned int)(w % L.tiles), (unsigned int)L.tiles);
     }
 }
 
@@ -359,18 +497,6 @@ __global__ void k_inv_any(const InvState* __restrict__ st, int st_stride, BatchL
     for (int i = threadIdx.x; i < n; i += 32) any |= st[L.active[i] * st_stride].go;
     any = __any_sync(0xffffffffu, any);
     if (threadIdx.x == 0) cudaGraphSetConditional(handle, any ? 1u : 0u);
-}
-
-// Re-arms a finished loop for one more body from its last measurement (kernel timing).
-__global__ void k_inv_rearm(InvState* st, int max_iterations) {
-    st->go = 1;
-    st->k = 0;
-    st->max_iterations = max_iterations;
-}
-
-int enqueue_inversion_rearm(fw_ctx* ctx, InvState* st, int max_iterations) {
-    k_inv_rearm<<<1, 1, 0, ctx->stream>>>(st, max_iterations);
-    return check_launch(ctx, "k_inv_rearm");
 }
 
 static InvArgs inv_args(const fw_field* field, const fw_field* inverse) {
@@ -385,53 +511,90 @@ static InvArgs inv_args(const fw_field* field, const fw_field* inverse) {
     return a;
 }
 
-// The body streams psi and the residual (a flat grid-stride sweep, two voxels a step); only when
-// the loop goes on does it gather, and the measurement -- a gather of every voxel -- runs over
-// 32 x 8 column tiles marching along z (z chunks so that the grid fills the GPU a few blocks
-// deep per SM).
-// One wave of resident blocks (the body kernels keep 4 blocks of 256 threads on an SM; the sweep
-// loops over the rest): the kernel of a body pair that returns at once costs half as much as
-// with two waves, and the working one is as fast or faster.
-static unsigned int inv_blocks(fw_ctx* ctx, long long n) {
-    long long b = (n + 255) / 256;
-    return (unsigned int)std::max<long long>(1, std::min<long long>(b, 4LL * ctx->num_sms));
+// Step tiles per block on a grid: one unless the grid has more than about eight tiles an SM, then
+// up to four (the last block's fixed-order reduction reads two doubles a block).
+int inv_step_zchunk(const int64_t n[3], int num_sms) {
+    const long long tiles = ((n[0] + 31) / 32) * ((n[1] + 7) / 8) * ((n[2] + kStepZ - 1) / kStepZ);
+    return (int)std::max<long long>(1, std::min<long long>(FW_STEP_MAX_TILES, tiles / (8LL * num_sms)));
 }
 
-static dim3 inv_grid(fw_ctx* ctx, InvArgs& a) {
-    return column_grid(a.g.nx, a.g.ny, a.g.nz, ctx->num_sms, &a.zchunk);
+long long inv_step_tiles(const HostGrid& g) {
+    return (long long)((g.n[0] + 31) / 32) * ((g.n[1] + 7) / 8) * ((g.n[2] + kStepZ - 1) / kStepZ);
 }
 
-// Launches the whole inversion on the stream: init, first measurement and `bodies` body kernels
-// (each returns at once after the loop has ended). Used by graph capture with bodies = 0.
+// The step's grid: 32 x 8 columns, and along z blocks of a.zchunk step tiles.
+static dim3 step_grid(fw_ctx* ctx, InvArgs& a) {
+    const long long gx = (a.g.nx + 31) / 32, gy = (a.g.ny + 7) / 8;
+    const long long gz = (a.g.nz + kStepZ - 1) / kStepZ;
+    const int64_t n[3] = {a.g.nx, a.g.ny, a.g.nz};
+    a.zchunk = inv_step_zchunk(n, ctx->num_sms);
+    return dim3((unsigned int)gx, (unsigned int)gy, (unsigned int)((gz + a.zchunk - 1) / a.zchunk));
+}
+
+// Scratch of a body: the step's block partials (two doubles a block, at most one block a tile),
+// then its deferred list (one entry a tile).
+static unsigned int* defer_list(fw_ctx* ctx, const HostGrid& g) {
+    return reinterpret_cast<unsigned int*>(ctx->d_scratch + SLOT_PARTIALS + 2 * inv_step_tiles(g));
+}
+
+// Before the loop: scratch for its bodies and the loop's settings (the init kernel also sets the
+// WHILE node's condition in graph mode).
 int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
                              fw_field* res, const fw_invert_params& prm, InvState* st,
                              cudaGraphConditionalHandle handle, int use_handle) {
     FW_CHECK(res->grid.same(inverse->grid) && res->ps == inverse->ps,
              "invert: the residual buffer does not match the inverse");
-    InvArgs a = inv_args(field, inverse);
-    const dim3 blocks = inv_grid(ctx, a);
-    // block partials of the measurement's tiles and of the bodies' flat grid
-    const size_t parts = std::max<size_t>((size_t)blocks.x * blocks.y * blocks.z,
-                                          inv_blocks(ctx, a.g.n));
-    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + 2 * parts + 16));
-    k_inv_measure<<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
-                                                   ctx->d_scratch + SLOT_PARTIALS,
-                                                   ctx->d_counter + 2, st, prm, handle, use_handle);
-    return check_launch(ctx, "k_inv_measure");
+    FW_TRY(ensure_scratch(ctx, inv_scratch_doubles(field->grid)));
+    k_inv_init<<<1, 1, 0, ctx->stream>>>(st, prm, handle, use_handle);
+    return check_launch(ctx, "k_inv_init");
 }
 
+// One kernel of a body: 0 bound, 1 step, 2 fix (each returns at once when the loop has ended).
+static int launch_body_kernel(fw_ctx* ctx, const fw_field* field, fw_field* inverse,
+                              fw_field* res, InvState* st, int which,
+                              cudaGraphConditionalHandle handle, int use_handle) {
+    InvArgs a = inv_args(field, inverse);
+    const dim3 g = step_grid(ctx, a);
+    unsigned int* defer = defer_list(ctx, field->grid);
+    if (which == 0) {
+        const Lattice t = lattice_of(a.g);
+        const unsigned int nb = (unsigned int)std::max<long long>(
+            1, std::min<long long>((t.count() + 255) / 256, 4LL * ctx->num_sms));
+        k_inv_bound<<<nb, 256, 0, ctx->stream>>>(a, t, field->d, inverse->d, st);
+        return check_launch(ctx, "k_inv_bound");
+    }
+    if (which == 1) {
+        k_inv_step<<<g, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
+                                               ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 2,
+                                               st, defer, handle, use_handle);
+        return check_launch(ctx, "k_inv_step");
+    }
+    const unsigned int tiles = (unsigned int)inv_step_tiles(field->grid);
+    const unsigned int nf = std::max(1u, std::min(tiles, 2u * (unsigned int)ctx->num_sms));
+    k_inv_fix<<<nf, 256, 0, ctx->stream>>>(a, inverse->d, res->d, st, defer);
+    return check_launch(ctx, "k_inv_fix");
+}
+
+// One body: bound, step, fix.
 int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
                            InvState* st, cudaGraphConditionalHandle handle, int use_handle) {
-    InvArgs a = inv_args(field, inverse);
-    const unsigned int blocks = inv_blocks(ctx, a.g.n);
-    k_inv_body<false><<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
-                                                       ctx->d_scratch + SLOT_PARTIALS,
-                                                       ctx->d_counter + 2, st, handle, use_handle);
-    FW_TRY(check_launch(ctx, "k_inv_body"));
-    k_inv_body<true><<<blocks, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
-                                                      ctx->d_scratch + SLOT_PARTIALS,
-                                                      ctx->d_counter + 2, st, handle, use_handle);
-    return check_launch(ctx, "k_inv_body");
+    for (int which = 0; which < 3; ++which)
+        FW_TRY(launch_body_kernel(ctx, field, inverse, res, st, which, handle, use_handle));
+    return 0;
+}
+
+int enqueue_inversion_kernel(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
+                             InvState* st, int which) {
+    return launch_body_kernel(ctx, field, inverse, res, st, which, 0, 0);
+}
+
+size_t inv_scratch_doubles(const HostGrid& g) {
+    const size_t tiles = (size_t)inv_step_tiles(g);
+    return SLOT_PARTIALS + 2 * tiles + (tiles + 1) / 2 + 16;
+}
+
+long long inv_bound_voxels(const HostGrid& g) {
+    return lattice_of(dev_grid(g)).count();
 }
 
 static InvArgs inv_args_grid(const HostGrid& g, long long ps) {
@@ -446,36 +609,46 @@ static InvArgs inv_args_grid(const HostGrid& g, long long ps) {
     return a;
 }
 
-int inv_measure_tiles(const HostGrid& g, int zchunk) {
-    const long long gx = (g.n[0] + 31) / 32, gy = (g.n[1] + 7) / 8, gz = (g.n[2] + zchunk - 1) / zchunk;
-    return (int)(gx * gy * gz);
+int inv_step_blocks(const HostGrid& g, int zchunk) {
+    const long long gx = (g.n[0] + 31) / 32, gy = (g.n[1] + 7) / 8;
+    const long long gz = (g.n[2] + kStepZ - 1) / kStepZ;
+    return (int)(gx * gy * ((gz + zchunk - 1) / zchunk));
 }
 
-int inv_body_vblocks(fw_ctx* ctx, long long n) { return (int)inv_blocks(ctx, n); }
-
-int launch_inv_measure_batch(fw_ctx* ctx, const HostGrid& g, long long ps, int zchunk,
-                             const BatchList& L, int blocks, const float* f, const float* psi,
-                             float* res, long long stride, double* partials,
-                             long long part_stride, unsigned int* counter, InvState* st,
-                             int st_stride, const fw_invert_params& prm) {
-    InvArgs a = inv_args_grid(g, ps);
-    a.zchunk = zchunk;
-    k_inv_measure_batch<<<blocks, 256, 0, ctx->stream>>>(a, L, f, psi, res, stride, partials,
-                                                         part_stride, counter, st, st_stride, prm);
-    return check_launch(ctx, "k_inv_measure_batch");
+int inv_bound_vblocks(const HostGrid& g) {
+    return (int)std::max<long long>(1, (lattice_of(dev_grid(g)).count() + 255) / 256);
 }
 
-int launch_inv_body_batch(fw_ctx* ctx, const HostGrid& g, long long ps, const BatchList& L,
-                          int blocks, const float* f, float* psi, float* res, long long stride,
+int launch_inv_init_batch(fw_ctx* ctx, const BatchList& L, InvState* st, int st_stride,
+                          const fw_invert_params& prm) {
+    k_inv_init_batch<<<1, 256, 0, ctx->stream>>>(L, st, st_stride, prm);
+    return check_launch(ctx, "k_inv_init_batch");
+}
+
+int launch_inv_body_batch(fw_ctx* ctx, const HostGrid& g, long long ps, const InvBatchBody& w,
+                          const float* f, float* psi, float* res, long long stride,
                           double* partials, long long part_stride, unsigned int* counter,
-                          InvState* st, int st_stride) {
+                          InvState* st, int st_stride, unsigned int* defer,
+                          long long defer_stride, int which) {
     InvArgs a = inv_args_grid(g, ps);
-    k_inv_body_batch<false><<<blocks, 256, 0, ctx->stream>>>(a, L, f, psi, res, stride, partials,
-                                                             part_stride, counter, st, st_stride);
-    FW_TRY(check_launch(ctx, "k_inv_body_batch"));
-    k_inv_body_batch<true><<<blocks, 256, 0, ctx->stream>>>(a, L, f, psi, res, stride, partials,
-                                                            part_stride, counter, st, st_stride);
-    return check_launch(ctx, "k_inv_body_batch");
+    a.zchunk = w.zchunk;
+    if (which < 0 || which == 0) {
+        k_inv_bound_batch<<<w.bound_blocks, 256, 0, ctx->stream>>>(
+            a, lattice_of(a.g), w.bound, f, psi, stride, st, st_stride);
+        FW_TRY(check_launch(ctx, "k_inv_bound_batch"));
+    }
+    if (which < 0 || which == 1) {
+        k_inv_step_batch<<<w.step_blocks, 256, 0, ctx->stream>>>(
+            a, w.step, f, psi, res, stride, partials, part_stride, counter, st, st_stride, defer,
+            defer_stride);
+        FW_TRY(check_launch(ctx, "k_inv_step_batch"));
+    }
+    if (which < 0 || which == 2) {
+        k_inv_fix_batch<<<w.fix_blocks, 256, 0, ctx->stream>>>(a, w.fix, psi, res, stride, st,
+                                                               st_stride, defer, defer_stride);
+        FW_TRY(check_launch(ctx, "k_inv_fix_batch"));
+    }
+    return 0;
 }
 
 int launch_inv_any(fw_ctx* ctx, const InvState* st, int st_stride, const BatchList& L,

@@ -180,7 +180,7 @@ int add_while_node(cudaStream_t s, cudaGraphConditionalHandle handle, cudaGraph_
 
 namespace {
 
-// One inversion: in graph mode a WHILE node around the body kernel; in direct mode a host loop.
+// One inversion: in graph mode a WHILE node around the body kernels; in direct mode a host loop.
 int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inverse,
                    fw_field* res, InvState* st) {
     if (!graph) {
@@ -593,7 +593,7 @@ int check_status(int status, bool masked) {
 int kernels_per_iteration(const fw_syn_recipe* r, int mask_warps) {
     int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) +
             4 /*two-pass smoothing or max*/ + 2 /*compose*/ +
-            (r->total_field_variance > 0.0 ? 4 : 0) + 4 /*inversion measures*/ + 1 /*record*/ +
+            (r->total_field_variance > 0.0 ? 4 : 0) + 4 /*inversion inits*/ + 1 /*record*/ +
             mask_warps + (mask_warps == 2 ? 1 : 0) /*product*/;
     for (int c = 0; c < r->channels; ++c)
         if (r->channel_metrics[c] == FW_METRIC_MATTES) k += 6;  // 7 dense MI kernels, not 1 CC
@@ -663,7 +663,12 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
     int total_iters = 0;
     for (int l = 0; l < r->levels; ++l) total_iters += (int)r->iterations[l];
     // scratch for every reduction of the biggest level, before any capture
-    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)(1 << 20)));
+    {
+        HostGrid last;
+        FW_TRY(level_grid(r, fg, r->levels - 1, last));
+        FW_TRY(ensure_scratch(ctx, std::max<size_t>(SLOT_PARTIALS + (size_t)(1 << 20),
+                                                    inv_scratch_doubles(last))));
+    }
     RunScratch rs;
     FW_TRY(rs.init(ctx, C, std::max(total_iters, 1)));
     FW_TRY(upload_syn_dev(ctx, r, rs.d.syn, fixed_mask || moving_mask));
@@ -790,10 +795,10 @@ int syn_run_device(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* f
                 FW_CUDA(cudaMemcpy(all.data(), rs.d.trace, sizeof(fw_syn_iteration) * done,
                                    cudaMemcpyDeviceToHost));
             // the kernels the level graphs ran (direct launches are counted as they are made):
-            // every iteration's kernels, two per inversion body, one level init per level
+            // every iteration's kernels, three per inversion body, one level init per level
             for (int q = 0; q < done && graphs; ++q) {
                 for (int s = 0; s < 4; ++s)
-                    ctx->stats.kernel_launches += 2 * (uint64_t)all[q].inversions[s].iterations;
+                    ctx->stats.kernel_launches += 3 * (uint64_t)all[q].inversions[s].iterations;
                 ctx->stats.kernel_launches +=
                     kernels_per_iteration(r, (fixed_mask ? 1 : 0) + (moving_mask ? 1 : 0));
             }
@@ -897,7 +902,8 @@ int fw_syn_step_masked(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image*
     const HostGrid& g = f2m->grid;
     FW_CHECK(f2m_inv->grid.same(g) && m2m->grid.same(g) && m2m_inv->grid.same(g),
              "syn: the state fields differ in grid");
-    FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)(1 << 20)));
+    FW_TRY(ensure_scratch(ctx, std::max<size_t>(SLOT_PARTIALS + (size_t)(1 << 20),
+                                                inv_scratch_doubles(g))));
     Level L;
     L.channels = recipe->channels;
     L.fmask = fixed_mask;

@@ -643,7 +643,9 @@ typedef struct fw_batch_subject {
 
 /* The autotuner's choice for one level: z slices per tile of each tiled kernel family and the
  * persistent grid of each (blocks per SM), the time spent tuning, and whether it came from the
- * process-wide cache of earlier batches of the same shape. */
+ * process-wide cache of earlier batches of the same shape. The inversion body's fields:
+ * measure_zchunk = step tiles (4 slices each) per work item, as the single inversion plans them;
+ * measure_blocks_per_sm = the step kernel's grid; body_blocks_per_sm = the fix kernel's grid. */
 typedef struct fw_batch_tuning {
     int32_t level;
     int64_t grid_size[3];
@@ -656,7 +658,8 @@ typedef struct fw_batch_tuning {
     int32_t from_cache;
     double tune_ms;
     /* the tuned time of one launch over all subjects (ms; 0 when the shapes were not timed):
-     * moving-side warp, CC pair, smoothing pair, compose, inversion measure, inversion body */
+     * moving-side warp, CC pair, smoothing pair, compose, inversion step (after its bound),
+     * inversion body (bound, step and fix) */
     double kernel_ms[6];
 } fw_batch_tuning;
 
@@ -692,8 +695,9 @@ int fw_batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* recipe, const fw_image* c
 /* Times `reps` launches of each kernel of one SyN iteration on the grid of `fixed` with CUDA
  * events on the context's stream: mean ms per launch and algorithmic bytes per launch of
  * [0] warp, [1] CC pair, [2] Gaussian smoothing + max norm, [3] compose + scale,
- * [4] inversion measure (keeps the residual), [5] last inversion body (update from the kept
- * residual), [6] inversion body followed by the next measurement. */
+ * [4] one inversion body (its bound, step and fix kernels: measurement and update of every
+ * voxel), [5] the body's bound kernel alone (the error on one voxel in 64), [6] its fix kernel
+ * alone (the update of the tiles the step left for the clamp; bytes counts their voxels). */
 int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, int32_t radius,
                     double variance, int32_t reps, double ms[7], double bytes[7]);
 
