@@ -307,7 +307,7 @@ struct Run {
     BatchScalars sc;
     Buf partials;
     long long part_stride = 0;
-    Buf defer;                  // [B][defer_stride] deferred step tiles of each subject
+    Buf defer;                  // [B][defer_stride] deferred step warp parts of each subject
     long long defer_stride = 0;
 };
 
@@ -844,7 +844,7 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
             run.part_stride = pps;
             FW_TRY(run.partials.alloc(ctx, sizeof(double) * (size_t)pps * B));
         }
-        const long long dps = (inv_step_tiles(lg) + 63) / 64 * 64;
+        const long long dps = (inv_step_parts(lg) + 63) / 64 * 64;
         if (dps > run.defer_stride) {
             run.defer_stride = dps;
             FW_TRY(run.defer.alloc(ctx, sizeof(unsigned int) * (size_t)dps * B));

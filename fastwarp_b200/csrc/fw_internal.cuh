@@ -537,6 +537,8 @@ int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse
 int enqueue_inversion_kernel(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
                              InvState* st, int which);
 long long inv_step_tiles(const HostGrid& g);
+// Warp parts of the step's tiles on grid g (the capacity of a deferred list).
+long long inv_step_parts(const HostGrid& g);
 // Scratch doubles an inversion on grid g needs (block partials and the deferred-tile list).
 size_t inv_scratch_doubles(const HostGrid& g);
 long long inv_bound_voxels(const HostGrid& g);

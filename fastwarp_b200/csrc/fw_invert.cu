@@ -10,15 +10,16 @@
 // volume. A body is therefore three kernels:
 //   k_inv_bound  the error on a sparse lattice of voxels (one in 64): its maximum is a lower
 //                bound L on the body's maximum error;
-//   k_inv_step   the measurement over 32 x 8 x 4 column tiles, each thread keeping its column's
-//                psi and error in registers. No voxel of a tile whose largest error is at most
-//                eps * L can be clamped (eps * L <= eps * max), so such a tile updates psi in
-//                place at once; any other tile writes its errors to the residual field and
-//                enters a short list. A fixed-order reduction (the last block) gives the mean
-//                and max and decides whether another body runs;
-//   k_inv_fix    the listed tiles' updates, now with the clamp eps * max.
+//   k_inv_step   the measurement over 32 x 8 x 2 column tiles, each thread keeping its column's
+//                psi and error in registers. No voxel of a warp's part (32 columns of a row,
+//                2 slices) whose largest error is at most eps * L can be clamped (eps * L <=
+//                eps * max), so such a part updates psi in place at once; any other part writes
+//                its errors to the residual field and enters a short list. A fixed-order
+//                reduction (the last block) gives the mean and max and decides whether another
+//                body runs;
+//   k_inv_fix    the listed parts' updates, now with the clamp eps * max.
 // The update of every voxel is the same arithmetic on either path, so the result does not depend
-// on which tiles were deferred. The loop state lives in device memory, so the loop needs no host
+// on which parts were deferred. The loop state lives in device memory, so the loop needs no host
 // read-back: the SyN driver runs it inside a CUDA graph WHILE node whose condition the step's last
 // block sets. The batched kernels (many subjects, one launch) run the same body in two kernels:
 // a measurement that keeps the residual, then the update (with the next measurement when the
@@ -133,13 +134,16 @@ __device__ void reduce_and_finish(double sum, float mx, double* __restrict__ par
 // ---- one inversion body: bound, step, fix --------------------------------------------------
 
 #ifndef FW_STEP_Z
-#define FW_STEP_Z 4
+#define FW_STEP_Z 2
 #endif
 #ifndef FW_STEP_MIN_BLOCKS
-#define FW_STEP_MIN_BLOCKS 3
+#define FW_STEP_MIN_BLOCKS 4
 #endif
 #ifndef FW_STEP_MAX_TILES
-#define FW_STEP_MAX_TILES 4
+#define FW_STEP_MAX_TILES 8
+#endif
+#ifndef FW_BOUND_STRIDE
+#define FW_BOUND_STRIDE 4
 #endif
 constexpr int kStepZ = FW_STEP_Z;  // slices of a step tile (a thread's column stays in registers)
 // eps * L is lowered by this factor before tiles are compared with it: the bound and the step
@@ -171,20 +175,23 @@ __global__ void k_inv_init(InvState* __restrict__ st, fw_invert_params prm,
     if (use_handle) cudaGraphSetConditional(handle, st->go ? 1u : 0u);
 }
 
-// The lattice of the bound: voxels 1, 5, 9, ... along each axis (0 on an axis of one voxel).
+// The lattice of the bound: voxels 1, 1 + S, 1 + 2S, ... along each axis (0 on an axis of one
+// voxel), S = kBoundStride.
+constexpr int kBoundStride = FW_BOUND_STRIDE;
 struct Lattice {
     int ox, oy, oz, mx, my, mz;
     __host__ __device__ long long count() const { return (long long)mx * my * mz; }
 };
 
 static Lattice lattice_of(const DevGrid& g) {
+    constexpr int S = kBoundStride;
     Lattice t;
     t.ox = g.nx > 1 ? 1 : 0;
     t.oy = g.ny > 1 ? 1 : 0;
     t.oz = g.nz > 1 ? 1 : 0;
-    t.mx = (g.nx - t.ox + 3) / 4;
-    t.my = (g.ny - t.oy + 3) / 4;
-    t.mz = (g.nz - t.oz + 3) / 4;
+    t.mx = (g.nx - t.ox + S - 1) / S;
+    t.my = (g.ny - t.oy + S - 1) / S;
+    t.mz = (g.nz - t.oz + S - 1) / S;
     return t;
 }
 
@@ -202,9 +209,9 @@ __device__ __forceinline__ void bound_block(const InvArgs& a, const Lattice& t,
     for (long long s = (long long)vb * blockDim.x + threadIdx.x; s < m;
          s += (long long)nvb * blockDim.x) {
         const long long q = s / t.mx;
-        const int i = t.ox + 4 * (int)(s - q * t.mx);
-        const int j = t.oy + 4 * (int)(q % t.my);
-        const int k = t.oz + 4 * (int)(q / t.my);
+        const int i = t.ox + kBoundStride * (int)(s - q * t.mx);
+        const int j = t.oy + kBoundStride * (int)(q % t.my);
+        const int k = t.oz + kBoundStride * (int)(q / t.my);
         const long long l = ((long long)k * a.g.ny + j) * a.g.nx + i;
         float e[3];
         residual(a, f, l, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
@@ -232,15 +239,15 @@ __global__ void __launch_bounds__(256) k_inv_bound(InvArgs a, Lattice t, const f
     bound_block(a, t, f, psi, st, blockIdx.x, gridDim.x);
 }
 
-// One step tile (bx, by, bz): the thread's column of at most kStepZ voxels is measured with psi
-// and e in registers; the tile's largest error decides whether it updates psi now (no voxel of
-// it can exceed eps * L <= the clamp) or keeps its errors in `res` for the fix kernel. Returns
-// whether the tile was deferred (uniform over the block).
-__device__ __forceinline__ bool step_tile(const InvArgs& a, int bx, int by, int bz,
+// A warp's part of step tile (bx, by, bz) -- 32 columns of one row, kStepZ slices: each thread's
+// column is measured with psi and e in registers, and the warp's largest error decides whether it
+// updates psi now (no voxel of it can exceed eps * L <= the clamp) or keeps its errors in `res`
+// for the fix kernel. No block barrier: every warp decides alone. Returns whether the warp's
+// voxels were deferred (uniform over the warp).
+__device__ __forceinline__ bool step_warp(const InvArgs& a, int bx, int by, int bz,
                                           const float* __restrict__ f, float* __restrict__ psi,
                                           float* __restrict__ res, float eps, float safe,
                                           bool enforce, double& sum, float& mx) {
-    __shared__ float wmax[8];  // one per warp of the 256-thread block
     int x, y, z0, z1;
     const bool have = column_of_tile(a.g.nx, a.g.ny, a.g.nz, kStepZ, bx, by, bz, x, y, z0, z1);
     const long long sxy = (long long)a.g.nx * a.g.ny;
@@ -267,15 +274,8 @@ __device__ __forceinline__ bool step_tile(const InvArgs& a, int bx, int by, int 
             }
         }
     }
-    const float w = warp_max_f(tmax);
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = w;
-    __syncthreads();
-    float tm = wmax[0];
-#pragma unroll
-    for (int q = 1; q < 8; ++q) tm = __int_as_float(max(__float_as_int(tm), __float_as_int(wmax[q])));
-    __syncthreads();  // wmax is free for the block's next tile
     mx = __int_as_float(max(__float_as_int(mx), __float_as_int(tmax)));
-    const bool now = tm <= safe;  // false when either is NaN
+    const bool now = warp_max_f(tmax) <= safe;  // false when either is NaN
     if (have) {
 #pragma unroll
         for (int q = 0; q < kStepZ; ++q) {
@@ -299,10 +299,11 @@ __device__ __forceinline__ bool step_tile(const InvArgs& a, int bx, int by, int 
 }
 
 // Block (bx, by, bzb) of body k's step: a.zchunk step tiles one above the other, measured against
-// f (sum and max added to sum / mx), updated at once or listed in `defer` (entries are tile
-// indices of the gx x gy x ceil(nz / kStepZ) tile grid).
+// f (sum and max added to sum / mx), each warp's part updated at once or listed in `defer`
+// (entries index the warp parts of the grid: gx columns of 32, every row y, ceil(nz / kStepZ)
+// slices of kStepZ).
 __device__ __forceinline__ void step_block(const InvArgs& a, int bx, int by, int bzb, int gx,
-                                           int gy, const float* __restrict__ f,
+                                           const float* __restrict__ f,
                                            float* __restrict__ psi, float* __restrict__ res,
                                            InvState* __restrict__ st,
                                            unsigned int* __restrict__ defer, double& sum,
@@ -312,15 +313,17 @@ __device__ __forceinline__ void step_block(const InvArgs& a, int bx, int by, int
     const float safe = __fmul_rn(__fmul_rn(eps, __uint_as_float(st->lb)), kSafeMargin);
     const bool enforce = st->enforce != 0;
     const int gz = (a.g.nz + kStepZ - 1) / kStepZ;
-    const unsigned int cap = (unsigned int)(gx * gy * gz);  // the list holds every tile once
+    const int y = by * 8 + (threadIdx.x >> 5);
+    const unsigned int cap = (unsigned int)gx * (unsigned int)a.g.ny * (unsigned int)gz;
     for (int m = 0; m < a.zchunk; ++m) {
         const int tz = bzb * a.zchunk + m;
         if (tz >= gz) break;  // uniform
-        const bool deferred =
-            step_tile(a, bx, by, tz, f, psi, res, eps, safe, enforce, sum, mx);
-        if (deferred && threadIdx.x == 0) {
+        const bool deferred = step_warp(a, bx, by, tz, f, psi, res, eps, safe, enforce, sum, mx);
+        if (deferred && (threadIdx.x & 31) == 0 && y < a.g.ny) {
             const unsigned int at = atomicAdd(&st->ndefer, 1u);
-            if (at < cap) defer[at] = (unsigned int)(bx + gx * (by + gy * tz));
+            if (at < cap)
+                defer[at] = (unsigned int)bx +
+                            (unsigned int)gx * ((unsigned int)y + (unsigned int)a.g.ny * tz);
         }
     }
 }
@@ -365,8 +368,7 @@ __global__ void __launch_bounds__(256, FW_STEP_MIN_BLOCKS) k_inv_step(InvArgs a,
     }
     double sum = 0.0;
     float mx = 0.0f;
-    step_block(a, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, f, psi, res, st,
-               defer, sum, mx);
+    step_block(a, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, f, psi, res, st, defer, sum, mx);
     const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     const unsigned int nblocks = gridDim.x * gridDim.y * gridDim.z;
     reduce_and_finish(sum, mx, partials, counter, bid, nblocks, [&](double s, double m) {
@@ -375,26 +377,29 @@ __global__ void __launch_bounds__(256, FW_STEP_MIN_BLOCKS) k_inv_step(InvArgs a,
     });
 }
 
-// The deferred tiles of the body that just ran, entries vb, vb + nvb, ... of the list: each
-// voxel's update from its kept error, with the clamp at eps * max (field_ops.rs:368-383). Each
-// voxel is written by one thread.
+// The deferred warp parts of the body that just ran, entries vb * 8 + w, + 8 nvb, ... of the list
+// for warp w of the block: each voxel's update from its kept error, with the clamp at eps * max
+// (field_ops.rs:368-383). Each voxel is written by one thread.
 __device__ __forceinline__ void fix_tiles(const InvArgs& a, float* __restrict__ psi,
                                           const float* __restrict__ res,
                                           const InvState* __restrict__ st,
                                           const unsigned int* __restrict__ defer, unsigned int vb,
                                           unsigned int nvb) {
-    const int gx = (a.g.nx + 31) / 32, gy = (a.g.ny + 7) / 8;
-    const unsigned int cap = (unsigned int)(gx * gy * ((a.g.nz + kStepZ - 1) / kStepZ));
+    const unsigned int gx = (unsigned int)(a.g.nx + 31) / 32, ny = (unsigned int)a.g.ny;
+    const unsigned int cap = gx * ny * (unsigned int)((a.g.nz + kStepZ - 1) / kStepZ);
     const unsigned int n = min(st->ndefer, cap);
     if (n == 0u) return;
     const float eps = st->eps, limit = st->limit;
     const bool enforce = st->enforce != 0;
     const long long sxy = (long long)a.g.nx * a.g.ny;
-    for (unsigned int t = vb; t < n; t += nvb) {
-        int bx, by, bz;
-        tile_coords((int)defer[t], gx, gy, bx, by, bz);
-        int x, y, z0, z1;
-        if (!column_of_tile(a.g.nx, a.g.ny, a.g.nz, kStepZ, bx, by, bz, x, y, z0, z1)) continue;
+    const unsigned int warps = blockDim.x >> 5;
+    for (unsigned int t = vb * warps + (threadIdx.x >> 5); t < n; t += nvb * warps) {
+        const unsigned int id = defer[t];
+        const int x = (int)(id % gx) * 32 + (threadIdx.x & 31);
+        const unsigned int r = id / gx;
+        const int y = (int)(r % ny), z0 = (int)(r / ny) * kStepZ;
+        if (x >= a.g.nx) continue;
+        const int z1 = min(z0 + kStepZ, a.g.nz);
         for (int z = z0; z < z1; ++z) {
             const long long l = (long long)z * sxy + (long long)y * a.g.nx + x;
             const float e[3] = {res[l], res[l + a.ps_psi], res[l + 2 * a.ps_psi]};
@@ -464,7 +469,7 @@ __global__ void __launch_bounds__(256, FW_STEP_MIN_BLOCKS) k_inv_step_batch(
         tile_coords(t, gx, gy, bx, by, bzb);
         double sum = 0.0;
         float mx = 0.0f;
-        step_block(a, bx, by, bzb, gx, gy, f + b * stride, psi + b * stride, res + b * stride,
+        step_block(a, bx, by, bzb, gx, f + b * stride, psi + b * stride, res + b * stride,
                    sb, defer + b * defer_stride, sum, mx);
         reduce_and_finish(sum, mx, partials + b * part_stride, counter + b, (unsigned int)t,
                           (unsigned int)L.tiles,
@@ -518,6 +523,10 @@ int inv_step_zchunk(const int64_t n[3], int num_sms) {
     return (int)std::max<long long>(1, std::min<long long>(FW_STEP_MAX_TILES, tiles / (8LL * num_sms)));
 }
 
+long long inv_step_parts(const HostGrid& g) {
+    return (long long)((g.n[0] + 31) / 32) * g.n[1] * ((g.n[2] + kStepZ - 1) / kStepZ);
+}
+
 long long inv_step_tiles(const HostGrid& g) {
     return (long long)((g.n[0] + 31) / 32) * ((g.n[1] + 7) / 8) * ((g.n[2] + kStepZ - 1) / kStepZ);
 }
@@ -532,7 +541,7 @@ static dim3 step_grid(fw_ctx* ctx, InvArgs& a) {
 }
 
 // Scratch of a body: the step's block partials (two doubles a block, at most one block a tile),
-// then its deferred list (one entry a tile).
+// then its deferred list (one entry a warp part: 32 columns of a row, kStepZ slices).
 static unsigned int* defer_list(fw_ctx* ctx, const HostGrid& g) {
     return reinterpret_cast<unsigned int*>(ctx->d_scratch + SLOT_PARTIALS + 2 * inv_step_tiles(g));
 }
@@ -589,8 +598,8 @@ int enqueue_inversion_kernel(fw_ctx* ctx, const fw_field* field, fw_field* inver
 }
 
 size_t inv_scratch_doubles(const HostGrid& g) {
-    const size_t tiles = (size_t)inv_step_tiles(g);
-    return SLOT_PARTIALS + 2 * tiles + (tiles + 1) / 2 + 16;
+    const size_t tiles = (size_t)inv_step_tiles(g), parts = (size_t)inv_step_parts(g);
+    return SLOT_PARTIALS + 2 * tiles + (parts + 1) / 2 + 16;
 }
 
 long long inv_bound_voxels(const HostGrid& g) {

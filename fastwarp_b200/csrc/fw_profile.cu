@@ -98,7 +98,7 @@ int fw_time_kernels(fw_ctx* ctx, const fw_image* fixed, const fw_image* moving, 
                                     ctx->stream));
             FW_TRY(sync(ctx));
             std::memcpy(&h, ctx->h_pinned, sizeof(h));
-            deferred = (double)h.ndefer / (double)inv_step_tiles(g);
+            deferred = (double)h.ndefer / (double)inv_step_parts(g);
         }
         cudaEventRecord(ev.a, ctx->stream);
         for (int r = 0; r < reps && !rc; ++r) rc = launch();
