@@ -150,7 +150,7 @@ struct Tuning {
     int warp_zc = 16, warp_bps = 4;
     int comp_zc = 16, comp_bps = 4;
     int cc_zc = 0, cc_bps = 3;  // cc_zc 0: the whole column
-    int step_zc = 1, step_bps = 3;  // inversion step: tiles per block (planned, not tuned)
+    int step_zc = 1, step_bps = 3;  // inversion step: step tiles per work item, blocks per SM
     int fix_bps = 2;                 // inversion fix kernel
     int smooth_bps = 4;
     double tune_ms = 0.0;
@@ -562,21 +562,29 @@ int tune_level(Run& run, BatchLevel& L, Tuning& best) {
     // inverse, loop states of slot 0 kept iterating; then the whole body with the best grid
     FW_CUDA(cudaMemcpyAsync(L.dM.p, L.Fi.p, L.dM.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     const fw_invert_params forever = {1 << 30, -1.0, -1.0, 1};
-    best.step_zc = inv_step_zchunk(L.grid.n, sms);
-    run.plan.t.step_zc = best.step_zc;
     FW_TRY(launch_inv_init_batch(ctx, run.sc.list(1), run.sc.inv, 4, forever));
     bestms = DBL_MAX;
-    for (int bps : {2, 3}) {
-        run.plan.t.step_bps = bps;
-        const InvBatchBody w = body_plan(run, L);
-        // every step after its own bound (which also clears the deferred lists)
-        FW_TRY(time_launch(ctx, tm, reps, [&] {
-            FW_TRY(launch_batch_body(run, L, w, L.F, L.dM, 0, 0));
-            return launch_batch_body(run, L, w, L.F, L.dM, 0, 1);
-        }, &ms));
-        if (ms < bestms) bestms = ms, best.step_bps = bps;
+    // step tiles per work item: as the single step plans them, or twice as many (fewer items and
+    // partials per subject; the subject's mean is then summed in other groups, a last-bit change)
+    const int zc1 = inv_step_zchunk(L.grid.n, sms);
+    const long long gzs =  // step tiles along z
+        inv_step_tiles(L.grid) / (((L.grid.n[0] + 31) / 32) * ((L.grid.n[1] + 7) / 8));
+    for (int zc : {zc1, 2 * zc1}) {
+        if (zc != zc1 && zc > gzs) continue;
+        for (int bps : {2, 3, 4}) {
+            run.plan.t.step_zc = zc;
+            run.plan.t.step_bps = bps;
+            const InvBatchBody w = body_plan(run, L);
+            // every step after its own bound (which also clears the deferred lists)
+            FW_TRY(time_launch(ctx, tm, reps, [&] {
+                FW_TRY(launch_batch_body(run, L, w, L.F, L.dM, 0, 0));
+                return launch_batch_body(run, L, w, L.F, L.dM, 0, 1);
+            }, &ms));
+            if (ms < bestms) bestms = ms, best.step_bps = bps, best.step_zc = zc;
+        }
     }
     best.step_ms = bestms;
+    run.plan.t.step_zc = best.step_zc;
     run.plan.t.step_bps = best.step_bps;
     {
         const InvBatchBody w = body_plan(run, L);
@@ -875,7 +883,7 @@ int batch_syn_run(fw_ctx* ctx, const fw_syn_recipe* r, const fw_image* const* fi
             std::lock_guard<std::mutex> lock(g_tune_mu);
             g_tune[key] = t;
         }
-        t.step_zc = inv_step_zchunk(lg.n, ctx->num_sms);  // as the single step plans it
+        if (!t.cached && !tuning_enabled()) t.step_zc = inv_step_zchunk(lg.n, ctx->num_sms);
         run.plan.t = t;
         peak = std::max<uint64_t>(peak, ctx->live_bytes.load() - live0);
         double ms = 0.0;

@@ -533,6 +533,14 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
                              cudaGraphConditionalHandle handle, int use_handle);
 int enqueue_inversion_body(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
                            InvState* st, cudaGraphConditionalHandle handle, int use_handle);
+// Graph mode: scratch for an inversion's bodies without the init kernel, and the inits of up to
+// kMaxInitHandles inversions (their states and WHILE conditions) in one kernel that also clears
+// zero[0..nzero).
+constexpr int kMaxInitHandles = 4;
+int inversion_scratch(fw_ctx* ctx, const fw_field* field);
+int enqueue_inversion_inits(fw_ctx* ctx, InvState* st, int count, const fw_invert_params& prm,
+                            const cudaGraphConditionalHandle* handles, unsigned int* zero,
+                            int nzero);
 // One kernel of a body (0 bound, 1 step, 2 fix), for kernel timing.
 int enqueue_inversion_kernel(fw_ctx* ctx, const fw_field* field, fw_field* inverse, fw_field* res,
                              InvState* st, int which);

@@ -175,6 +175,22 @@ __global__ void k_inv_init(InvState* __restrict__ st, fw_invert_params prm,
     if (use_handle) cudaGraphSetConditional(handle, st->go ? 1u : 0u);
 }
 
+// Several inversions' settings in one launch: states st[0..count) and the conditions of their
+// WHILE nodes; it also clears zero[0..nzero) (the SyN level graph begins every iteration with it:
+// its four inversions' settings and the update maxima, in one node).
+struct InitHandles {
+    cudaGraphConditionalHandle h[kMaxInitHandles];
+};
+__global__ void k_inv_init_many(InvState* __restrict__ st, int count, fw_invert_params prm,
+                                InitHandles hs, unsigned int* __restrict__ zero, int nzero) {
+    const int i = threadIdx.x;
+    if (i < count) {
+        init_state(st + i, prm);
+        cudaGraphSetConditional(hs.h[i], st[i].go ? 1u : 0u);
+    }
+    if (i < nzero) zero[i] = 0u;
+}
+
 // The lattice of the bound: voxels 1, 1 + S, 1 + 2S, ... along each axis (0 on an axis of one
 // voxel), S = kBoundStride.
 constexpr int kBoundStride = FW_BOUND_STRIDE;
@@ -556,6 +572,23 @@ int enqueue_inversion_prefix(fw_ctx* ctx, const fw_field* field, fw_field* inver
     FW_TRY(ensure_scratch(ctx, inv_scratch_doubles(field->grid)));
     k_inv_init<<<1, 1, 0, ctx->stream>>>(st, prm, handle, use_handle);
     return check_launch(ctx, "k_inv_init");
+}
+
+// Scratch for the bodies of an inversion of `field` (before a capture: the graph holds the
+// pointers).
+int inversion_scratch(fw_ctx* ctx, const fw_field* field) {
+    return ensure_scratch(ctx, inv_scratch_doubles(field->grid));
+}
+
+int enqueue_inversion_inits(fw_ctx* ctx, InvState* st, int count, const fw_invert_params& prm,
+                            const cudaGraphConditionalHandle* handles, unsigned int* zero,
+                            int nzero) {
+    FW_CHECK(count >= 0 && count <= kMaxInitHandles && nzero >= 0 && nzero <= 32,
+             "inversion inits: too many loops");
+    InitHandles hs;
+    for (int i = 0; i < kMaxInitHandles; ++i) hs.h[i] = i < count ? handles[i] : 0;
+    k_inv_init_many<<<1, 32, 0, ctx->stream>>>(st, count, prm, hs, zero, nzero);
+    return check_launch(ctx, "k_inv_init_many");
 }
 
 // One kernel of a body: 0 bound, 1 step, 2 fix (each returns at once when the loop has ended).

@@ -11,7 +11,9 @@
 // Graph design: every buffer of a level is allocated once, so the kernel sequence of an
 // iteration is the same every time. The whole level is captured as ONE CUDA graph: an outer
 // WHILE node whose body is the iteration, with each of the four inversions an inner WHILE node
-// whose condition the inversion's last block sets (no host read-back inside the loop). A
+// whose condition the inversion step's last block sets (no host read-back inside the loop); the
+// iteration's first kernel sets the four loops' states and conditions and clears the update
+// maxima. A
 // single-thread record kernel at the end of the body runs the convergence monitor on the device,
 // writes the iteration record and sets the outer condition. The host launches one graph and
 // reads the records back once per level.
@@ -180,31 +182,30 @@ int add_while_node(cudaStream_t s, cudaGraphConditionalHandle handle, cudaGraph_
 
 namespace {
 
-// One inversion: in graph mode a WHILE node around the body kernels; in direct mode a host loop.
+// One inversion: in graph mode a WHILE node around the body kernels on `h` (the iteration's first
+// kernel set the loop's state and condition); in direct mode its init kernel and a host loop.
 int enqueue_invert(fw_ctx* ctx, bool graph, const fw_field* field, fw_field* inverse,
-                   fw_field* res, InvState* st) {
+                   fw_field* res, InvState* st, cudaGraphConditionalHandle h) {
     if (!graph) {
         FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, 0, 0));
-        InvState h;
+        InvState hs;
         for (int body = 0; body < kSynInvert.max_iterations; ++body) {
             FW_TRY(enqueue_inversion_body(ctx, field, inverse, res, st, 0, 0));
             FW_CUDA(cudaMemcpyAsync(ctx->h_pinned, st, sizeof(InvState), cudaMemcpyDeviceToHost,
                                     ctx->stream));
             FW_TRY(sync(ctx));
-            std::memcpy(&h, ctx->h_pinned, sizeof(h));
-            if (!h.go) break;
+            std::memcpy(&hs, ctx->h_pinned, sizeof(hs));
+            if (!hs.go) break;
         }
         return 0;
     }
-    // the handle lives in the graph being captured; the measure kernel sets it
+    FW_CHECK(res->grid.same(inverse->grid) && res->ps == inverse->ps,
+             "invert: the residual buffer does not match the inverse");
+    FW_TRY(inversion_scratch(ctx, field));
     cudaStreamCaptureStatus status;
     cudaGraph_t g;
     const cudaGraphNode_t* deps;
     size_t ndeps;
-    FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
-    cudaGraphConditionalHandle h;
-    FW_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    FW_TRY(enqueue_inversion_prefix(ctx, field, inverse, res, kSynInvert, st, h, 1));
     FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, &deps, &ndeps));
     cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
     p.conditional.handle = h;
@@ -237,7 +238,19 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
                       const std::vector<const fw_image*>& ms, const fw_affine* initial,
                       const RunDev& d) {
     const int C = L.channels;
-    FW_CUDA(cudaMemsetAsync(d.max_bits, 0, 2 * sizeof(unsigned int), ctx->stream));
+    // graph mode: one kernel begins the iteration -- the update maxima cleared, the four
+    // inversions' states and WHILE conditions set (their handles live in the graph being
+    // captured); direct mode: a memset, and each inversion's init kernel
+    cudaGraphConditionalHandle hinv[4] = {0, 0, 0, 0};
+    if (graph) {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t g;
+        FW_CUDA(cudaStreamGetCaptureInfo(ctx->stream, &status, nullptr, &g, nullptr, nullptr));
+        for (auto& h : hinv) FW_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+        FW_TRY(enqueue_inversion_inits(ctx, d.inv, 4, kSynInvert, hinv, d.max_bits, 2));
+    } else {
+        FW_CUDA(cudaMemsetAsync(d.max_bits, 0, 2 * sizeof(unsigned int), ctx->stream));
+    }
     if (C > 1) {
         FW_CUDA(cudaMemsetAsync(L.accF->d, 0, L.accF->bytes, ctx->stream));
         FW_CUDA(cudaMemsetAsync(L.accM->d, 0, L.accM->bytes, ctx->stream));
@@ -299,8 +312,9 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
         fw_field* inverse;
         unsigned int* max;
         InvState* st;
-    } sides[2] = {{gF, L.sF, L.F, L.Fi, d.max_bits, d.inv},
-                  {gM, L.sM, L.M, L.Mi, d.max_bits + 1, d.inv + 2}};
+        const cudaGraphConditionalHandle* h;
+    } sides[2] = {{gF, L.sF, L.F, L.Fi, d.max_bits, d.inv, hinv},
+                  {gM, L.sM, L.M, L.Mi, d.max_bits + 1, d.inv + 2, hinv + 2}};
     for (auto& s : sides) {
         const fw_field* u = s.g;
         if (r->update_field_variance > 0.0) {
@@ -317,8 +331,8 @@ int enqueue_iteration(fw_ctx* ctx, bool graph, const fw_syn_recipe* r, Level& L,
                                     ctx->stream));
         }
         // inverse = invert(field), then field = invert(inverse)
-        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, L.R, s.st));
-        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, L.R, s.st + 1));
+        FW_TRY(enqueue_invert(ctx, graph, s.field, s.inverse, L.R, s.st, s.h[0]));
+        FW_TRY(enqueue_invert(ctx, graph, s.inverse, s.field, L.R, s.st + 1, s.h[1]));
     }
     return 0;
 }
@@ -593,7 +607,7 @@ int check_status(int status, bool masked) {
 int kernels_per_iteration(const fw_syn_recipe* r, int mask_warps) {
     int k = r->channels * 3 + (r->channels > 1 ? 2 * r->channels + 2 : 0) +
             4 /*two-pass smoothing or max*/ + 2 /*compose*/ +
-            (r->total_field_variance > 0.0 ? 4 : 0) + 4 /*inversion inits*/ + 1 /*record*/ +
+            (r->total_field_variance > 0.0 ? 4 : 0) + 1 /*inversion inits*/ + 1 /*record*/ +
             mask_warps + (mask_warps == 2 ? 1 : 0) /*product*/;
     for (int c = 0; c < r->channels; ++c)
         if (r->channel_metrics[c] == FW_METRIC_MATTES) k += 6;  // 7 dense MI kernels, not 1 CC
