@@ -479,6 +479,7 @@ __global__ void __launch_bounds__(TX * TY, FW_CC_MIN_BLOCKS) k_cc_pair(CcArgs a,
                                                      double* __restrict__ partials,
                                                      unsigned int* __restrict__ counter,
                                                      double* __restrict__ result, int want_norms) {
+    pdl_wait();
     using L = Layout<R, TY, MK>;
     extern __shared__ __align__(16) unsigned char smem[];
     double* red = reinterpret_cast<double*>(smem + L::red_off);
@@ -564,10 +565,9 @@ int launch_r(fw_ctx* ctx, const CcArgs& a0, const float* f, const float* m, cons
     FW_TRY((plan_launch<R, TY, MK, Acc>(a, ctx->num_sms, &grid)));
     unsigned int nblocks = grid.x * grid.y * grid.z;
     FW_TRY(ensure_scratch(ctx, SLOT_PARTIALS + (size_t)L::NP * nblocks + 16));
-    k_cc_pair<R, TY, MK, Acc><<<grid, L::NT, L::bytes, ctx->stream>>>(
-        a, f, m, v, df, dm, ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 1, d_result,
-        want_norms);
-    return check_launch(ctx, "k_cc_pair");
+    return launch_pdl(ctx, "k_cc_pair", k_cc_pair<R, TY, MK, Acc>, grid, dim3(L::NT), L::bytes,
+                      a, f, m, v, df, dm, ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 1,
+                      d_result, want_norms);
 }
 
 // The window-sum arithmetic of the unmasked single-image CC pair (FW_CC_SUMS_*), process-wide.

@@ -3,6 +3,8 @@
 // (backend.rs:268-271), max and L2 norms (backend.rs:252-265).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
@@ -281,6 +283,14 @@ int host_stage(fw_ctx* ctx, size_t bytes, void** out) {
     return 0;
 }
 
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("FASTWARP_PDL");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 int check_launch(fw_ctx* ctx, const char* what) {
     ctx->stats.kernel_launches++;
     cudaError_t e = cudaGetLastError();
@@ -415,6 +425,7 @@ __global__ void __launch_bounds__(256) k_warp_t(WarpArgs a, int zchunk,
                                                 const float* __restrict__ u,
                                                 const float* __restrict__ src,
                                                 float* __restrict__ out) {
+    pdl_wait();
     int x, y, z0, z1;
     if (!column_of(a.g.nx, a.g.ny, a.g.nz, zchunk, x, y, z0, z1)) return;
     warp_column(a, x, y, z0, z1, u, src, out);
@@ -496,6 +507,7 @@ __global__ void __launch_bounds__(256) k_compose(FieldArgs a, int zchunk,
                                                  float* out,
                                                  const unsigned int* __restrict__ max_bits,
                                                  double step) {
+    pdl_wait();
     int i, j, z0, z1;
     if (!column_of(a.g.nx, a.g.ny, a.g.nz, zchunk, i, j, z0, z1)) return;
     compose_column(a, i, j, z0, z1, u, w, out, max_bits, step);
@@ -709,8 +721,8 @@ int launch_warp(fw_ctx* ctx, const fw_image* src, const fw_field* field, const f
     if (!pre && !mask) {
         int zchunk = 1;
         const dim3 grid = column_grid(a.g.nx, a.g.ny, a.g.nz, ctx->num_sms, &zchunk);
-        k_warp_t<<<grid, 256, 0, ctx->stream>>>(a, zchunk, field->d, src->d, out);
-        return check_launch(ctx, "k_warp_t");
+        return launch_pdl(ctx, "k_warp_t", k_warp_t, grid, dim3(256), 0, a, zchunk,
+                          (const float*)field->d, (const float*)src->d, out);
     }
     k_warp<<<blocks_for(n), 256, 0, ctx->stream>>>(a, field->d, pre ? pre->d : nullptr, src->d,
                                                    product, out);
@@ -722,9 +734,9 @@ int launch_compose(fw_ctx* ctx, const fw_field* disp, const fw_field* warping, f
     FieldArgs a{dev_grid(warping->grid), warping->ps};
     int zchunk = 1;
     const dim3 grid = column_grid(a.g.nx, a.g.ny, a.g.nz, ctx->num_sms, &zchunk);
-    k_compose<<<grid, 256, 0, ctx->stream>>>(a, zchunk, disp->d, warping->d, out->d,
-                                             d_scale_max_bits, step);
-    return check_launch(ctx, "k_compose");
+    return launch_pdl(ctx, "k_compose", k_compose, grid, dim3(256), 0, a, zchunk,
+                      (const float*)disp->d, (const float*)warping->d, out->d, d_scale_max_bits,
+                      step);
 }
 
 __global__ void k_image_product(const float* __restrict__ a, const float* __restrict__ b,

@@ -159,6 +159,33 @@ int new_image(fw_ctx* ctx, const HostGrid& g, fw_image** out);
 int new_field(fw_ctx* ctx, const HostGrid& g, fw_field** out);
 int sync(fw_ctx* ctx);
 int check_launch(fw_ctx* ctx, const char* what);
+
+// Programmatic dependent launch (sm_90+): a kernel launched by launch_pdl may be scheduled while
+// the kernel before it on the stream drains, so the launch latency of a chain of small kernels
+// (the coarse pyramid levels) overlaps the previous kernel's tail. Every such kernel calls
+// pdl_wait() before its first memory access: it returns once the previous kernel has completed
+// and its writes are visible, so the kernel sees exactly what an ordinary launch would (for an
+// ordinary launch it returns at once). FASTWARP_PDL=0 launches them without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+int launch_pdl(fw_ctx* ctx, const char* what, void (*kernel)(KArgs...), dim3 grid, dim3 block,
+               size_t smem, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return check_launch(ctx, what);
+}
 // The context's pinned staging buffer, at least `bytes` long; the caller synchronises the
 // stream before it writes the buffer again.
 int host_stage(fw_ctx* ctx, size_t bytes, void** out);

@@ -183,6 +183,7 @@ struct InitHandles {
 };
 __global__ void k_inv_init_many(InvState* __restrict__ st, int count, fw_invert_params prm,
                                 InitHandles hs, unsigned int* __restrict__ zero, int nzero) {
+    pdl_wait();
     const int i = threadIdx.x;
     if (i < count) {
         init_state(st + i, prm);
@@ -250,6 +251,7 @@ __device__ __forceinline__ void bound_block(const InvArgs& a, const Lattice& t,
 __global__ void __launch_bounds__(256) k_inv_bound(InvArgs a, Lattice t, const float* __restrict__ f,
                                                    const float* __restrict__ psi,
                                                    InvState* __restrict__ st) {
+    pdl_wait();
     if (blockIdx.x == 0 && threadIdx.x == 0) st->ndefer = 0u;
     if (!st->go) return;
     bound_block(a, t, f, psi, st, blockIdx.x, gridDim.x);
@@ -376,6 +378,7 @@ __global__ void __launch_bounds__(256, FW_STEP_MIN_BLOCKS) k_inv_step(InvArgs a,
                                                      unsigned int* __restrict__ defer,
                                                      cudaGraphConditionalHandle handle,
                                                      int use_handle) {
+    pdl_wait();
     if (!st->go) {  // uniform: the state only changes in the last block of a working grid
         if (use_handle && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 &&
             threadIdx.x == 0)
@@ -432,6 +435,7 @@ __global__ void __launch_bounds__(256, 4) k_inv_fix(InvArgs a, float* __restrict
                                                     const float* __restrict__ res,
                                                     const InvState* __restrict__ st,
                                                     const unsigned int* __restrict__ defer) {
+    pdl_wait();
     fix_tiles(a, psi, res, st, defer, blockIdx.x, gridDim.x);
 }
 
@@ -587,8 +591,8 @@ int enqueue_inversion_inits(fw_ctx* ctx, InvState* st, int count, const fw_inver
              "inversion inits: too many loops");
     InitHandles hs;
     for (int i = 0; i < kMaxInitHandles; ++i) hs.h[i] = i < count ? handles[i] : 0;
-    k_inv_init_many<<<1, 32, 0, ctx->stream>>>(st, count, prm, hs, zero, nzero);
-    return check_launch(ctx, "k_inv_init_many");
+    return launch_pdl(ctx, "k_inv_init_many", k_inv_init_many, dim3(1), dim3(32), 0, st, count,
+                      prm, hs, zero, nzero);
 }
 
 // One kernel of a body: 0 bound, 1 step, 2 fix (each returns at once when the loop has ended).
@@ -602,19 +606,18 @@ static int launch_body_kernel(fw_ctx* ctx, const fw_field* field, fw_field* inve
         const Lattice t = lattice_of(a.g);
         const unsigned int nb = (unsigned int)std::max<long long>(
             1, std::min<long long>((t.count() + 255) / 256, 4LL * ctx->num_sms));
-        k_inv_bound<<<nb, 256, 0, ctx->stream>>>(a, t, field->d, inverse->d, st);
-        return check_launch(ctx, "k_inv_bound");
+        return launch_pdl(ctx, "k_inv_bound", k_inv_bound, dim3(nb), dim3(256), 0, a, t,
+                          (const float*)field->d, (const float*)inverse->d, st);
     }
-    if (which == 1) {
-        k_inv_step<<<g, 256, 0, ctx->stream>>>(a, field->d, inverse->d, res->d,
-                                               ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 2,
-                                               st, defer, handle, use_handle);
-        return check_launch(ctx, "k_inv_step");
-    }
+    if (which == 1)
+        return launch_pdl(ctx, "k_inv_step", k_inv_step, g, dim3(256), 0, a,
+                          (const float*)field->d, inverse->d, res->d,
+                          ctx->d_scratch + SLOT_PARTIALS, ctx->d_counter + 2, st, defer, handle,
+                          use_handle);
     const unsigned int tiles = (unsigned int)inv_step_tiles(field->grid);
     const unsigned int nf = std::max(1u, std::min(tiles, 2u * (unsigned int)ctx->num_sms));
-    k_inv_fix<<<nf, 256, 0, ctx->stream>>>(a, inverse->d, res->d, st, defer);
-    return check_launch(ctx, "k_inv_fix");
+    return launch_pdl(ctx, "k_inv_fix", k_inv_fix, dim3(nf), dim3(256), 0, a, inverse->d,
+                      (const float*)res->d, (const InvState*)st, (const unsigned int*)defer);
 }
 
 // One body: bound, step, fix.

@@ -301,6 +301,7 @@ __device__ __forceinline__ void smooth_xy_tile(const SmoothArgs& a, int bx, int 
 template <int R>
 __global__ void __launch_bounds__(XY_NT) k_smooth_xy(SmoothArgs a, const float* __restrict__ in,
                                                      float* __restrict__ tmp, long long ps_tmp) {
+    pdl_wait();
     extern __shared__ __align__(16) float smem_xy[];
     smooth_xy_tile<R>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_xy, in, tmp, ps_tmp);
 }
@@ -389,6 +390,7 @@ __global__ void __launch_bounds__(256, R <= 6 ? 3 : 2) k_smooth_z(SmoothArgs a, 
                                                   long long ps_tmp, const float* in,
                                                   float* out,
                                                   unsigned int* __restrict__ max_bits) {
+    pdl_wait();
     float vmax = smooth_z_tile<R>(a, blockIdx.x, blockIdx.y, blockIdx.z, tmp, ps_tmp, in, out,
                                   max_bits != nullptr);
     if (max_bits) {
@@ -428,11 +430,12 @@ int launch_smooth_xyz(fw_ctx* ctx, const SmoothArgs& a, const fw_field* in, fw_f
     FW_CUDA(cudaFuncSetAttribute(k_smooth_xy<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)bytes));
     dim3 g1((a.g.nx + XY_T - 1) / XY_T, (a.g.ny + XY_T - 1) / XY_T, a.g.nz);
-    k_smooth_xy<R><<<g1, XY_NT, bytes, ctx->stream>>>(a, in->d, tmp->d, tmp->ps);
-    FW_TRY(check_launch(ctx, "k_smooth_xy"));
+    FW_TRY(launch_pdl(ctx, "k_smooth_xy", k_smooth_xy<R>, g1, dim3(XY_NT), bytes, a,
+                      (const float*)in->d, tmp->d, (long long)tmp->ps));
     dim3 g2((a.g.nz + Z_SEG - 1) / Z_SEG, (a.g.nx + 31) / 32, (a.g.ny + 7) / 8);
-    k_smooth_z<R><<<g2, 256, 0, ctx->stream>>>(a, tmp->d, tmp->ps, in->d, out->d, d_max_bits);
-    return check_launch(ctx, "k_smooth_z");
+    return launch_pdl(ctx, "k_smooth_z", k_smooth_z<R>, g2, dim3(256), 0, a,
+                      (const float*)tmp->d, (long long)tmp->ps, (const float*)in->d, out->d,
+                      d_max_bits);
 }
 
 template <int R>

@@ -47,6 +47,7 @@ __global__ void k_syn_record(SynDev* s, const double* __restrict__ cc,
                              const InvState* __restrict__ inv, fw_syn_iteration* trace,
                              int trace_cap, const volatile int* cancel,
                              cudaGraphConditionalHandle handle, int use_handle) {
+    pdl_wait();
     const int more = syn_record_step(s, cc, max_bits, inv, trace, trace_cap, cancel);
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
@@ -561,10 +562,10 @@ int run_level_graph(fw_ctx* ctx, const fw_syn_recipe* r, Level& L,
             if (!rc) {
                 // the context's cancel flag is read once per iteration: a cancel stops the
                 // level graph after the iteration in flight
-                k_syn_record<<<1, 1, 0, ctx->stream>>>(d.syn, d.cc, d.max_bits, d.inv,
-                                                      trace_dev_base, d.trace_cap,
-                                                      ctx->cancel_mapped_dev, h_it, 1);
-                rc = check_launch(ctx, "k_syn_record");
+                rc = launch_pdl(ctx, "k_syn_record", k_syn_record, dim3(1), dim3(1), 0, d.syn,
+                                (const double*)d.cc, (const unsigned int*)d.max_bits,
+                                (const InvState*)d.inv, trace_dev_base, d.trace_cap,
+                                ctx->cancel_mapped_dev, h_it, 1);
             }
             cudaGraph_t b2;
             e = cudaStreamEndCapture(ctx->stream, &b2);
