@@ -395,15 +395,15 @@ __device__ __forceinline__ void central_difference_voxel(const float* __restrict
     }
 }
 
-// Thread mapping of the gather sweeps (warp, compose, inversion): a block of 256 threads is a
-// 32 x 8 tile of (x, y) columns and each thread marches along z through `zchunk` slices, so the
-// trilinear gathers of neighbouring columns and consecutive slices meet in L1.
+// Thread mapping of the gather sweeps (warp, compose): a block of 256 threads is a 32 x 8 tile of
+// (x, y) columns and each thread marches along z through `zchunk` slices, so the trilinear
+// gathers of neighbouring columns and consecutive slices meet in L1 (the inversion step uses the
+// same columns, 2 slices a tile, fw_invert.cu).
 inline dim3 column_grid(int nx, int ny, int nz, int num_sms, int* zchunk) {
     dim3 g((unsigned int)((nx + 31) / 32), (unsigned int)((ny + 7) / 8), 1);
     const long long tiles = (long long)g.x * g.y;
     // about 16 blocks an SM: thin z chunks balance the SMs (measured on the 193 x 229 x 193
-    // finest level: 12 chunks against 5 made compose 17 %, warp 10 % and the inversion measure
-    // 4 % faster; past that the measure's per-block reductions start to cost)
+    // finest level: 12 chunks against 5 made compose 17 % and warp 10 % faster)
     const long long want = (16LL * num_sms + tiles - 1) / tiles;
     *zchunk = (int)((nz + (want > 1 ? want : 1) - 1) / (want > 1 ? want : 1));
     if (*zchunk < 1) *zchunk = 1;
