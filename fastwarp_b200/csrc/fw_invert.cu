@@ -21,9 +21,8 @@
 // The update of every voxel is the same arithmetic on either path, so the result does not depend
 // on which parts were deferred. The loop state lives in device memory, so the loop needs no host
 // read-back: the SyN driver runs it inside a CUDA graph WHILE node whose condition the step's last
-// block sets. The batched kernels (many subjects, one launch) run the same body in two kernels:
-// a measurement that keeps the residual, then the update (with the next measurement when the
-// loop goes on).
+// block sets. The batched kernels (many subjects, one launch each) run the same three kernels'
+// bodies over a work list of (subject, block) items.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -37,12 +36,12 @@ struct InvArgs {
     DevGrid g;
     long long ps_f, ps_psi;
     float isx, isy, isz;
-    int zchunk;  // slices a thread marches through
+    int zchunk;  // step tiles stacked in a block (k_inv_step)
 };
 
-__device__ __forceinline__ void residual(const InvArgs& a, const float* __restrict__ f,
-                                         long long l, int i, int j, int k, float px, float py,
-                                         float pz, float e[3]) {
+// e = psi + f(x + psi) at voxel (i, j, k) with psi = (px, py, pz) (field_ops.rs:346-351).
+__device__ __forceinline__ void residual(const InvArgs& a, const float* __restrict__ f, int i,
+                                         int j, int k, float px, float py, float pz, float e[3]) {
     // explicitly rounded (no contraction), in the reference's order: every kernel that measures
     // a voxel maps it to the same continuous index
     auto map = [&](int r, int base) {
@@ -151,7 +150,7 @@ constexpr int kStepZ = FW_STEP_Z;  // slices of a step tile (a thread's column s
 // the compiler contracting the norm's products differently in the two kernels (a last-bit change)
 constexpr float kSafeMargin = 0.999f;
 
-// The loop's settings before its first body (field_ops.rs:325-338: errors start at +inf, so the
+// The loop's settings before its first body (field_ops.rs:330-344: errors start at +inf, so the
 // first body runs whenever max_iterations > 0).
 __device__ __forceinline__ void init_state(InvState* __restrict__ st, const fw_invert_params& prm) {
     st->max_iterations = prm.max_iterations;
@@ -231,7 +230,7 @@ __device__ __forceinline__ void bound_block(const InvArgs& a, const Lattice& t,
         const int k = t.oz + kBoundStride * (int)(q / t.my);
         const long long l = ((long long)k * a.g.ny + j) * a.g.nx + i;
         float e[3];
-        residual(a, f, l, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
+        residual(a, f, i, j, k, psi[l], psi[l + a.ps_psi], psi[l + 2 * a.ps_psi], e);
         const float nrm = nan_canon(err_norm(a, e));
         best = __int_as_float(max(__float_as_int(best), __float_as_int(nrm)));
     }
@@ -285,7 +284,7 @@ __device__ __forceinline__ bool step_warp(const InvArgs& a, int bx, int by, int 
 #pragma unroll
         for (int q = 0; q < kStepZ; ++q) {
             if (z0 + q < z1) {
-                residual(a, f, l0 + q * sxy, x, y, z0 + q, p[q][0], p[q][1], p[q][2], e[q]);
+                residual(a, f, x, y, z0 + q, p[q][0], p[q][1], p[q][2], e[q]);
                 const float nrm = nan_canon(err_norm(a, e[q]));
                 sum += (double)nrm;
                 tmax = __int_as_float(max(__float_as_int(tmax), __float_as_int(nrm)));
@@ -346,7 +345,7 @@ __device__ __forceinline__ void step_block(const InvArgs& a, int bx, int by, int
     }
 }
 
-// The last block's record of body k (field_ops.rs:340-357): errors, bodies executed, the step
+// The last block's record of body k (field_ops.rs:339-355): errors, bodies executed, the step
 // and clamp the fix kernel applies, and whether body k + 1 runs.
 __device__ __forceinline__ bool finish_step(InvState* __restrict__ st, double s, double m,
                                             double count) {
